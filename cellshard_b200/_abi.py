@@ -1,0 +1,148 @@
+"""ctypes mirror of include/cellshard_b200.h.
+
+Structures follow the C layouts field for field (16-byte aligned structs get
+explicit tail padding so ctypes.sizeof matches the C sizeof; the layout test
+compiles the header with gcc and compares).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+u32 = C.c_uint32
+u64 = C.c_uint64
+vp = C.c_void_p
+sz = C.c_size_t
+
+LIB_PATH = Path(__file__).resolve().parent / "libcellshard_b200.so"
+
+
+class CompressedView(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("axis", u32),
+                ("majorPtr", vp), ("minorIdx", vp), ("val", vp), ("_pad", C.c_uint64)]
+
+
+class BlockedEllView(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("block_size", u32), ("ell_cols", u32),
+                ("blockColIdx", vp), ("val", vp), ("_pad", C.c_uint64)]
+
+
+class SlicedEllView(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("slice_count", u32), ("slice_rows", u32),
+                ("slice_row_offsets", vp), ("slice_widths", vp), ("slice_slot_offsets", vp),
+                ("col_idx", vp), ("val", vp)]
+
+
+class HostCompressed(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("axis", u32), ("flags", u32),
+                ("storage", vp), ("majorPtr", vp), ("minorIdx", vp), ("val", vp), ("_pad", C.c_uint64)]
+
+
+class HostBlockedEll(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("block_size", u32), ("ell_cols", u32),
+                ("flags", u32), ("storage", vp), ("blockColIdx", vp), ("val", vp)]
+
+
+class HostSlicedEll(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("slice_count", u32), ("flags", u32),
+                ("storage", vp), ("slice_row_offsets", vp), ("slice_widths", vp), ("col_idx", vp),
+                ("val", vp)]
+
+
+class BlockedEllTuneResult(C.Structure):
+    _fields_ = [("block_size", C.c_uint), ("fill_ratio", C.c_double), ("padded_bytes", sz)]
+
+
+class SlicedEllTuneResult(C.Structure):
+    _fields_ = [("slice_rows", C.c_uint), ("slice_count", C.c_uint), ("padded_slots", sz),
+                ("padded_bytes", sz), ("storage_ratio", C.c_double), ("slice_penalty", C.c_double),
+                ("score", C.c_double)]
+
+
+class RowFeatureMaskView(C.Structure):
+    _fields_ = [("row_keep", vp), ("feature_keep", vp), ("row_remap", vp), ("feature_remap", vp)]
+
+
+class GroupFilterParams(C.Structure):
+    _fields_ = [("min_total", C.c_float), ("min_detected_features", u32),
+                ("max_group_fraction", C.c_float), ("fraction_group_index", u32)]
+
+
+class GroupReduceOut(C.Structure):
+    _fields_ = [("row_totals", vp), ("detected_features", vp), ("max_values", vp), ("row_keep", vp),
+                ("group_counts", vp), ("group_percentages", vp)]
+
+
+class GroupMomentsParams(C.Structure):
+    _fields_ = [("group_count", u32), ("scheme", u32), ("ddof", u32), ("chunk_rows", u32)]
+
+
+class GroupMomentsOut(C.Structure):
+    _fields_ = [("sum", vp), ("sumsq", vp), ("mean", vp), ("var", vp), ("mean64", vp), ("var64", vp),
+                ("group_rows", vp), ("status", vp)]
+
+
+P = C.POINTER
+
+# name -> (restype, argtypes)
+PROTOTYPES: dict[str, tuple] = {
+    "cs_b200_abi_version": (C.c_int, []),
+    "cs_b200_last_error": (C.c_char_p, []),
+    "cs_b200_host_compressed_clear": (None, [P(HostCompressed)]),
+    "cs_b200_host_blocked_ell_clear": (None, [P(HostBlockedEll)]),
+    "cs_b200_host_sliced_ell_clear": (None, [P(HostSlicedEll)]),
+    "cs_b200_blocked_ell_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
+    "cs_b200_blocked_ell_shape": (C.c_int, [P(CompressedView), u32, vp, vp, sz, vp, vp]),
+    "cs_b200_blocked_ell_emit": (C.c_int, [P(CompressedView), P(BlockedEllView), vp, vp, sz, vp, vp]),
+    "cs_b200_blocked_ell_from_compressed": (C.c_int, [P(HostCompressed), C.c_uint, P(HostBlockedEll)]),
+    "cs_b200_choose_blocked_ell_block_size": (C.c_int, [P(HostCompressed), P(C.c_uint), C.c_uint,
+                                                         P(BlockedEllTuneResult)]),
+    "cs_b200_group_reduce_blocked_ell": (C.c_int, [P(BlockedEllView), vp, u32, P(RowFeatureMaskView),
+                                                   P(GroupFilterParams), P(GroupReduceOut), vp]),
+    "cs_b200_group_reduce_sliced_ell": (C.c_int, [P(SlicedEllView), vp, u32, P(RowFeatureMaskView),
+                                                  P(GroupFilterParams), P(GroupReduceOut), vp]),
+    "cs_b200_group_reduce_compressed": (C.c_int, [P(CompressedView), vp, u32, P(RowFeatureMaskView),
+                                                  P(GroupFilterParams), P(GroupReduceOut), vp]),
+    "cs_b200_reoptimize_scratch_bytes": (C.c_int, [u32, u32, P(sz)]),
+    "cs_b200_reoptimize_count": (C.c_int, [P(BlockedEllView), P(RowFeatureMaskView), u32, u32, vp, vp, sz, vp,
+                                           vp]),
+    "cs_b200_reoptimize_emit": (C.c_int, [P(BlockedEllView), P(RowFeatureMaskView), u32, u32, vp, vp, vp, vp]),
+    "cs_b200_group_moments_scratch_bytes": (C.c_int, [P(BlockedEllView), P(GroupMomentsParams), P(sz)]),
+    "cs_b200_group_moments_blocked_ell": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
+                                                    P(GroupMomentsOut), vp, sz, vp]),
+    "cs_b200_synth_csr": (C.c_int, [u32, u32, vp, vp, vp, vp, u32, vp, u64, vp, vp, vp]),
+}
+
+
+class CellShardError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: os.PathLike | None = None) -> C.CDLL:
+    """Loads libcellshard_b200.so; raises if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise CellShardError(
+            f"{p} is missing: build it with `python -m cellshard_b200.build` (nvcc, sm_100a); "
+            "there is no CPU fallback")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(ok: int, what: str) -> None:
+    if ok != 1:
+        msg = load().cs_b200_last_error()
+        raise CellShardError(f"{what} failed: {msg.decode() if msg else 'unknown error'}")

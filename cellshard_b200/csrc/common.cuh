@@ -1,0 +1,128 @@
+// Shared device/host helpers for libcellshard_b200.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/cellshard_b200.h"
+
+namespace csb {
+
+// ---------------------------------------------------------------------------
+// Error reporting: one message per host thread, read by cs_b200_last_error().
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+void clear_error();
+
+inline int cuda_ok(cudaError_t err, const char *what) {
+    if (err == cudaSuccess) return 1;
+    set_error("CUDA error at %s: %s", what, cudaGetErrorString(err));
+    return 0;
+}
+
+inline int launch_ok(const char *kernel) {
+    return cuda_ok(cudaGetLastError(), kernel);
+}
+
+inline cudaStream_t as_stream(cs_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs on the current device (cached per device ordinal).
+int sm_count();
+
+inline std::size_t align_up(std::size_t v, std::size_t a) { return (v + a - 1u) / a * a; }
+
+// Bump allocator over caller scratch; every sub-buffer is 256-byte aligned.
+struct scratch_carver {
+    char *base;
+    std::size_t cap;
+    std::size_t used;
+    __host__ scratch_carver(void *b, std::size_t c) : base((char *) b), cap(c), used(0) {}
+    template <typename T>
+    __host__ T *take(std::size_t count) {
+        used = align_up(used, 256);
+        T *p = (T *) (base ? base + used : nullptr);
+        used += count * sizeof(T);
+        return p;
+    }
+    __host__ bool fits() const { return used <= cap; }
+};
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float h2f(uint16_t bits) {
+    return __half2float(__ushort_as_half(bits));
+}
+
+// A fp16 value compares unequal to 0.0f unless it is +0 or -0 (NaN counts as
+// nonzero, as `__half2float(v) != 0.0f` does in the reference).
+__device__ __forceinline__ bool half_nonzero(uint16_t bits) { return (bits & 0x7fffu) != 0u; }
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ void status_or(uint32_t *status, uint32_t bits) {
+    if (status != nullptr && bits != 0u) atomicOr(status, bits);
+}
+
+// Streaming 16-byte load that does not allocate the line in L1 (value
+// streams are touched once).
+__device__ __forceinline__ uint4 ld_stream_v4(const void *p) {
+    uint4 r;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(p));
+    return r;
+}
+
+__device__ __forceinline__ void st_stream_v4(void *p, uint4 v) {
+    asm volatile("st.global.cs.v4.u32 [%0], {%1,%2,%3,%4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z),
+                 "r"(v.w)
+                 : "memory");
+}
+
+// Warp inclusive scan (all 32 lanes participate).
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
+    const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= (unsigned) o) v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan; blockDim.x must be a multiple of 32 (<= 1024)
+// and every thread must call it.  smem holds 33 words.  Safe to call back to
+// back (ends with a barrier after the shared reads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *smem, uint32_t &total) {
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t incl = warp_inclusive_scan(v);
+    if (lane == 31u) smem[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = lane < nw ? smem[lane] : 0u;
+        const uint32_t wi = warp_inclusive_scan(w);
+        if (lane < nw) smem[lane] = wi - w;
+        if (lane == 31u) smem[32] = wi;
+    }
+    __syncthreads();
+    const uint32_t r = smem[warp] + incl - v;
+    total = smem[32];
+    __syncthreads();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan of uint32 (three launches: tile sums, scan of
+// tile sums, tile-local scan + add).  out may alias in.  out[n] receives the
+// total when write_total is set (so out must hold n + 1 entries).
+// ---------------------------------------------------------------------------
+std::size_t scan_u32_scratch_bytes(std::size_t n);
+int scan_exclusive_u32(const uint32_t *in, uint32_t *out, std::size_t n, bool write_total, void *scratch,
+                       std::size_t scratch_bytes, cudaStream_t stream);
+
+} // namespace csb

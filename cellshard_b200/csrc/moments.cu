@@ -1,0 +1,659 @@
+// Row-label grouped per-feature moments over Blocked-ELL.
+//
+// For every kept row r with label g and every feature f:
+//     sum[g][f] += x,  sumsq[g][f] += x*x   (x = fp16 value widened to fp32)
+//
+// Plan (all stream-ordered, no host synchronisation):
+//   1. index     one warp per row block turns its ascending blockColIdx row
+//                into a bitmap over column blocks plus per-32-block prefix
+//                counts, so slot(rb, b) = prefix + popc(word & below(b)).
+//   2. sort      stable counting sort of kept rows by label (tile histograms,
+//                one-CTA group scan that also cuts each group's rows into
+//                chunks, tile-local ranked scatter).
+//   3. accumulate  grid (chunk, feature tile): each thread owns L consecutive
+//                features of one column block and streams its chunk's rows
+//                (all of one group), keeping its sums in registers; fp32 batch
+//                sums of kBatch rows are folded into hi/lo two-sum pairs.
+//                One partial (hi, lo) per (chunk, feature) goes to scratch.
+//   4. combine   per (group, feature): add the group's chunk partials (fp64 or
+//                fp32 by scheme), apply the feature mask, emit sum, sumsq,
+//                mean and variance.
+#include "common.cuh"
+
+#include <cstring>
+
+namespace csb {
+namespace {
+
+constexpr unsigned kTileRows = 1024;   // rows per sort tile
+constexpr unsigned kSortThreads = 256; // 8 warps x 128 rows
+constexpr unsigned kSortWarps = kSortThreads / 32;
+constexpr unsigned kAccThreads = 256;
+constexpr unsigned kBatch = 8;         // rows per fp32 batch sum
+constexpr unsigned kDefaultChunkRows = 2048;
+constexpr unsigned kMaxChunkRows = 8192;
+constexpr unsigned kIndexWarps = 4;
+constexpr unsigned kMaxIndexWords = 2048; // column blocks / 32 per row block
+
+struct chunk_desc {
+    uint32_t group;
+    uint32_t begin;
+    uint32_t end;
+    uint32_t pad;
+};
+
+struct moments_layout {
+    uint2 *index;              // [row_blocks * words]
+    uint32_t *tile_counts;     // [tiles * G]
+    uint32_t *group_offsets;   // [G + 1]
+    uint32_t *group_rows;      // [G]
+    uint32_t *chunk_first;     // [G + 1]
+    uint32_t *num_chunks;      // [1]
+    chunk_desc *chunks;        // [max_chunks]
+    uint32_t *sorted_rows;     // [rows]
+    float *partials;           // [max_chunks * 4 * cols]
+    std::size_t bytes;
+    uint32_t row_blocks, words, tiles, max_chunks, chunk_rows, col_blocks;
+};
+
+bool make_layout(const cs_blocked_ell_view *src, const cs_group_moments_params *p, void *base, std::size_t cap,
+                 moments_layout *lay) {
+    const uint32_t B = src->block_size;
+    lay->row_blocks = (src->rows + B - 1u) / B;
+    lay->col_blocks = (src->cols + B - 1u) / B;
+    lay->words = (lay->col_blocks + 31u) / 32u;
+    lay->tiles = (src->rows + kTileRows - 1u) / kTileRows;
+    lay->chunk_rows = p->chunk_rows == 0u ? kDefaultChunkRows : p->chunk_rows;
+    const std::size_t G = p->group_count;
+    lay->max_chunks = (uint32_t) ((src->rows + lay->chunk_rows - 1u) / lay->chunk_rows + G);
+    scratch_carver c(base, cap);
+    lay->index = c.take<uint2>((std::size_t) lay->row_blocks * lay->words + 1);
+    lay->tile_counts = c.take<uint32_t>((std::size_t) lay->tiles * G + 1);
+    lay->group_offsets = c.take<uint32_t>(G + 1);
+    lay->group_rows = c.take<uint32_t>(G);
+    lay->chunk_first = c.take<uint32_t>(G + 1);
+    lay->num_chunks = c.take<uint32_t>(1);
+    lay->chunks = c.take<chunk_desc>(lay->max_chunks);
+    lay->sorted_rows = c.take<uint32_t>((std::size_t) src->rows + 1);
+    lay->partials = c.take<float>((std::size_t) lay->max_chunks * 4u * src->cols + 1);
+    lay->bytes = c.used;
+    return c.fits();
+}
+
+// ---------------------------------------------------------------------------
+// 1. Column-block index per row block.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kIndexWarps * 32) moments_index_kernel(const uint32_t *__restrict__ block_col_idx,
+                                                                         uint32_t row_blocks, uint32_t width,
+                                                                         uint32_t col_blocks, uint32_t words,
+                                                                         uint2 *__restrict__ index,
+                                                                         uint32_t *status) {
+    extern __shared__ uint32_t bitmap_smem[];
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t *bits = bitmap_smem + (std::size_t) warp * words;
+    for (uint32_t rb = blockIdx.x * kIndexWarps + warp; rb < row_blocks; rb += gridDim.x * kIndexWarps) {
+        for (uint32_t w = lane; w < words; w += 32u) bits[w] = 0u;
+        __syncwarp();
+        const uint32_t *row = block_col_idx + (std::size_t) rb * width;
+        uint32_t bad = 0u;
+        for (uint32_t s = lane; s < width; s += 32u) {
+            const uint32_t bc = row[s];
+            if (bc != CS_INVALID_COL) {
+                if (bc >= col_blocks) {
+                    bad |= CS_STATUS_INDEX_RANGE;
+                } else {
+                    atomicOr(bits + (bc >> 5), 1u << (bc & 31u));
+                }
+                if (s > 0u) {
+                    const uint32_t prev = row[s - 1u];
+                    if (prev == CS_INVALID_COL || prev >= bc) bad |= CS_STATUS_BLOCK_COL_ORDER;
+                }
+            }
+        }
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        if (lane == 0u) status_or(status, bad);
+        __syncwarp();
+        uint32_t carry = 0u;
+        for (uint32_t w0 = 0; w0 < words; w0 += 32u) {
+            const uint32_t w = w0 + lane;
+            const uint32_t word = w < words ? bits[w] : 0u;
+            const uint32_t cnt = __popc(word);
+            uint32_t incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (unsigned) o) incl += t;
+            }
+            if (w < words) index[(std::size_t) rb * words + w] = make_uint2(word, carry + incl - cnt);
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Stable counting sort of kept rows by label.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t row_group(uint32_t r, uint32_t rows, const uint8_t *keep, const uint32_t *labels,
+                                              uint32_t G) {
+    if (r >= rows) return G;
+    if (keep != nullptr && keep[r] == 0u) return G;
+    const uint32_t g = labels != nullptr ? labels[r] : 0u;
+    return g < G ? g : G;
+}
+
+__global__ void __launch_bounds__(kSortThreads) moments_tile_hist_kernel(uint32_t rows, const uint8_t *__restrict__ keep,
+                                                                         const uint32_t *__restrict__ labels, uint32_t G,
+                                                                         uint32_t *__restrict__ tile_counts) {
+    extern __shared__ uint32_t hist[];
+    for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) hist[g] = 0u;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kTileRows;
+    for (uint32_t i = threadIdx.x; i < kTileRows; i += blockDim.x) {
+        const uint32_t g = row_group(base + i, rows, keep, labels, G);
+        if (g < G) atomicAdd(hist + g, 1u);
+    }
+    __syncthreads();
+    for (uint32_t g = threadIdx.x; g < G; g += blockDim.x)
+        tile_counts[(std::size_t) blockIdx.x * G + g] = hist[g];
+}
+
+// One warp per group: exclusive scan of the group's per-tile counts (in
+// place, group-relative) and the group's row total.
+__global__ void __launch_bounds__(256) moments_group_tiles_kernel(uint32_t tiles, uint32_t G,
+                                                                  uint32_t *__restrict__ tile_counts,
+                                                                  uint32_t *__restrict__ group_rows) {
+    const uint32_t g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const unsigned lane = threadIdx.x & 31u;
+    if (g >= G) return;
+    uint32_t carry = 0u;
+    for (uint32_t t0 = 0; t0 < tiles; t0 += 32u) {
+        const uint32_t t = t0 + lane;
+        const std::size_t k = (std::size_t) t * G + g;
+        const uint32_t c = t < tiles ? tile_counts[k] : 0u;
+        const uint32_t incl = warp_inclusive_scan(c);
+        if (t < tiles) tile_counts[k] = carry + incl - c;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0u) group_rows[g] = carry;
+}
+
+// One CTA: group offsets, chunk cutting (each chunk holds rows of one group).
+__global__ void __launch_bounds__(1024) moments_group_scan_kernel(uint32_t G, uint32_t chunk_rows, uint32_t max_chunks,
+                                                                  const uint32_t *__restrict__ group_rows,
+                                                                  uint32_t *__restrict__ group_offsets,
+                                                                  uint32_t *__restrict__ chunk_first,
+                                                                  uint32_t *__restrict__ num_chunks,
+                                                                  chunk_desc *__restrict__ chunks) {
+    __shared__ uint32_t smem[33];
+    uint32_t carry_rows = 0u, carry_chunks = 0u;
+    for (uint32_t g0 = 0; g0 < G; g0 += blockDim.x) {
+        const uint32_t g = g0 + threadIdx.x;
+        const uint32_t n = g < G ? group_rows[g] : 0u;
+        const uint32_t nc = g < G ? (n + chunk_rows - 1u) / chunk_rows : 0u;
+        uint32_t tot_n, tot_c;
+        const uint32_t ex_n = block_exclusive_scan(n, smem, tot_n);
+        const uint32_t ex_c = block_exclusive_scan(nc, smem, tot_c);
+        if (g < G) {
+            const uint32_t off = carry_rows + ex_n;
+            const uint32_t cf = carry_chunks + ex_c;
+            group_offsets[g] = off;
+            chunk_first[g] = cf;
+            for (uint32_t c = 0; c < nc; ++c) {
+                const uint32_t b = off + c * chunk_rows;
+                const uint32_t e = (c + 1u == nc) ? off + n : b + chunk_rows;
+                if (cf + c < max_chunks) chunks[cf + c] = chunk_desc{g, b, e, 0u};
+            }
+        }
+        carry_rows += tot_n;
+        carry_chunks += tot_c;
+    }
+    if (threadIdx.x == 0) {
+        group_offsets[G] = carry_rows;
+        chunk_first[G] = carry_chunks;
+        *num_chunks = carry_chunks;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) moments_tile_scatter_kernel(uint32_t rows,
+                                                                            const uint8_t *__restrict__ keep,
+                                                                            const uint32_t *__restrict__ labels,
+                                                                            uint32_t G,
+                                                                            const uint32_t *__restrict__ tile_base,
+                                                                            const uint32_t *__restrict__ group_offsets,
+                                                                            uint32_t *__restrict__ sorted_rows) {
+    extern __shared__ uint32_t warp_counts[]; // [kSortWarps][G]
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    for (uint32_t i = threadIdx.x; i < kSortWarps * G; i += blockDim.x) warp_counts[i] = 0u;
+    __syncthreads();
+    constexpr uint32_t rows_per_warp = kTileRows / kSortWarps;
+    const uint32_t wbase = blockIdx.x * kTileRows + warp * rows_per_warp;
+    uint32_t *my = warp_counts + (std::size_t) warp * G;
+    for (uint32_t b = 0; b < rows_per_warp; b += 32u) {
+        const uint32_t r = wbase + b + lane;
+        const uint32_t g = row_group(r, rows, keep, labels, G);
+        const uint32_t peers = __match_any_sync(0xffffffffu, g);
+        if (g < G && lane == (unsigned) (__ffs(peers) - 1)) my[g] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
+        uint32_t run = tile_base[(std::size_t) blockIdx.x * G + g] + group_offsets[g];
+        for (unsigned w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = warp_counts[(std::size_t) w * G + g];
+            warp_counts[(std::size_t) w * G + g] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    for (uint32_t b = 0; b < rows_per_warp; b += 32u) {
+        const uint32_t r = wbase + b + lane;
+        const uint32_t g = row_group(r, rows, keep, labels, G);
+        const uint32_t peers = __match_any_sync(0xffffffffu, g);
+        uint32_t base = 0u;
+        if (g < G) base = my[g];
+        __syncwarp();
+        if (g < G) {
+            sorted_rows[base + __popc(peers & lt)] = r;
+            if (lane == (unsigned) (__ffs(peers) - 1)) my[g] = base + __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Accumulation.
+// ---------------------------------------------------------------------------
+template <int L>
+struct vec_load;
+template <>
+struct vec_load<8> {
+    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
+        const uint4 v = ld_stream_v4(p);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[i]));
+            x[2 * i] = f.x;
+            x[2 * i + 1] = f.y;
+        }
+    }
+};
+template <>
+struct vec_load<4> {
+    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2 *>(p));
+        const uint32_t w[2] = {v.x, v.y};
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[i]));
+            x[2 * i] = f.x;
+            x[2 * i + 1] = f.y;
+        }
+    }
+};
+template <>
+struct vec_load<2> {
+    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
+        const uint32_t w = __ldg(reinterpret_cast<const unsigned int *>(p));
+        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w));
+        x[0] = f.x;
+        x[1] = f.y;
+    }
+};
+template <>
+struct vec_load<1> {
+    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
+        x[0] = h2f(__ldg(reinterpret_cast<const unsigned short *>(p)));
+    }
+};
+
+// Knuth two-sum folded into a running (hi, lo) pair.
+__device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float b) {
+    const float s = __fadd_rn(hi, b);
+    const float bb = __fsub_rn(s, hi);
+    const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+    hi = s;
+    lo = __fadd_rn(lo, err);
+}
+
+template <int L, bool COMP>
+__global__ void __launch_bounds__(kAccThreads) moments_accumulate_kernel(
+    const uint16_t *__restrict__ val, uint32_t ell_cols, uint32_t block_size, uint32_t col_blocks, uint32_t words,
+    uint32_t cols, const uint2 *__restrict__ index, const chunk_desc *__restrict__ chunks,
+    const uint32_t *__restrict__ num_chunks, const uint32_t *__restrict__ sorted_rows, float *__restrict__ partials) {
+    extern __shared__ uint2 chunk_rows_smem[]; // (row, row_block * words)
+    const uint32_t c = blockIdx.x;
+    if (c >= *num_chunks) return;
+    const chunk_desc d = chunks[c];
+    const uint32_t n = d.end - d.begin;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t r = sorted_rows[d.begin + i];
+        chunk_rows_smem[i] = make_uint2(r, (r / block_size) * words);
+    }
+    __syncthreads();
+
+    const uint32_t segs_per_block = block_size / L;
+    const uint32_t seg = blockIdx.y * kAccThreads + threadIdx.x;
+    const uint32_t b = seg / segs_per_block;
+    const uint32_t part = seg - b * segs_per_block;
+    const bool active = b < col_blocks;
+    const uint32_t w = b >> 5;
+    const uint32_t below = (1u << (b & 31u)) - 1u;
+    const uint32_t bitmask = 1u << (b & 31u);
+    const std::size_t lane_off = (std::size_t) part * L;
+
+    float s_hi[L], s_lo[L], q_hi[L], q_lo[L];
+#pragma unroll
+    for (int j = 0; j < L; ++j) s_hi[j] = s_lo[j] = q_hi[j] = q_lo[j] = 0.0f;
+
+    if (active) {
+        uint32_t i = 0;
+        for (; i + kBatch <= n; i += kBatch) {
+            float x[kBatch][L];
+#pragma unroll
+            for (unsigned u = 0; u < kBatch; ++u) {
+                const uint2 rr = chunk_rows_smem[i + u];
+                const uint32_t r = rr.x;
+                const uint2 e = __ldg(index + (std::size_t) rr.y + w);
+                if (e.x & bitmask) {
+                    const uint32_t slot = e.y + __popc(e.x & below);
+                    vec_load<L>::load(val + (std::size_t) r * ell_cols + (std::size_t) slot * block_size + lane_off,
+                                      x[u]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < L; ++j) x[u][j] = 0.0f;
+                }
+            }
+            if (COMP) {
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    float bs = 0.0f, bq = 0.0f;
+#pragma unroll
+                    for (unsigned u = 0; u < kBatch; ++u) {
+                        bs = __fadd_rn(bs, x[u][j]);
+                        bq = __fmaf_rn(x[u][j], x[u][j], bq);
+                    }
+                    two_sum_acc(s_hi[j], s_lo[j], bs);
+                    two_sum_acc(q_hi[j], q_lo[j], bq);
+                }
+            } else {
+#pragma unroll
+                for (unsigned u = 0; u < kBatch; ++u) {
+#pragma unroll
+                    for (int j = 0; j < L; ++j) {
+                        s_hi[j] = __fadd_rn(s_hi[j], x[u][j]);
+                        q_hi[j] = __fmaf_rn(x[u][j], x[u][j], q_hi[j]);
+                    }
+                }
+            }
+        }
+        for (; i < n; ++i) {
+            const uint2 rr = chunk_rows_smem[i];
+            const uint32_t r = rr.x;
+            const uint2 e = __ldg(index + (std::size_t) rr.y + w);
+            if (e.x & bitmask) {
+                float x[L];
+                const uint32_t slot = e.y + __popc(e.x & below);
+                vec_load<L>::load(val + (std::size_t) r * ell_cols + (std::size_t) slot * block_size + lane_off, x);
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    if (COMP) {
+                        two_sum_acc(s_hi[j], s_lo[j], x[j]);
+                        two_sum_acc(q_hi[j], q_lo[j], __fmul_rn(x[j], x[j]));
+                    } else {
+                        s_hi[j] = __fadd_rn(s_hi[j], x[j]);
+                        q_hi[j] = __fmaf_rn(x[j], x[j], q_hi[j]);
+                    }
+                }
+            }
+        }
+        const std::size_t f0 = (std::size_t) b * block_size + lane_off;
+        float *p = partials + (std::size_t) c * 4u * cols;
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            const std::size_t f = f0 + j;
+            if (f < cols) {
+                p[f] = s_hi[j];
+                p[cols + f] = s_lo[j];
+                p[2u * (std::size_t) cols + f] = q_hi[j];
+                p[3u * (std::size_t) cols + f] = q_lo[j];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 4. Combine.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) moments_combine_kernel(
+    uint32_t cols, uint32_t G, uint32_t scheme, uint32_t ddof, const uint32_t *__restrict__ chunk_first,
+    const uint32_t *__restrict__ group_rows, const float *__restrict__ partials, const uint8_t *__restrict__ feature_keep,
+    float *__restrict__ out_sum, float *__restrict__ out_sumsq, float *__restrict__ out_mean, float *__restrict__ out_var,
+    double *__restrict__ out_mean64, double *__restrict__ out_var64, uint32_t *__restrict__ out_group_rows) {
+    const uint32_t g = blockIdx.y;
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    if (f == 0 && out_group_rows != nullptr) out_group_rows[g] = group_rows[g];
+    if (f >= cols) return;
+    const uint32_t c0 = chunk_first[g], c1 = chunk_first[g + 1];
+    const uint32_t n = group_rows[g];
+    const bool kept = feature_keep == nullptr || feature_keep[f] != 0u;
+    const std::size_t o = (std::size_t) g * cols + f;
+    float rs = 0.0f, rq = 0.0f, rm = 0.0f, rv = 0.0f;
+    double dm = 0.0, dv = 0.0;
+    if (kept) {
+        if (scheme == CS_MOMENTS_TWOSUM_F64_COMBINE) {
+            double s = 0.0, q = 0.0;
+            for (uint32_t c = c0; c < c1; ++c) {
+                const float *p = partials + (std::size_t) c * 4u * cols;
+                s += (double) p[f] + (double) p[cols + f];
+                q += (double) p[2u * (std::size_t) cols + f] + (double) p[3u * (std::size_t) cols + f];
+            }
+            rs = (float) s;
+            rq = (float) q;
+            if (n > 0u) {
+                dm = s / (double) n;
+                if (n > ddof) {
+                    double m2 = q - s * dm;
+                    if (m2 < 0.0) m2 = 0.0;
+                    dv = m2 / (double) (n - ddof);
+                }
+            }
+            rm = (float) dm;
+            rv = (float) dv;
+        } else {
+            float s_hi = 0.0f, s_lo = 0.0f, q_hi = 0.0f, q_lo = 0.0f;
+            for (uint32_t c = c0; c < c1; ++c) {
+                const float *p = partials + (std::size_t) c * 4u * cols;
+                if (scheme == CS_MOMENTS_TWOSUM_F32) {
+                    two_sum_acc(s_hi, s_lo, p[f]);
+                    s_lo = __fadd_rn(s_lo, p[cols + f]);
+                    two_sum_acc(q_hi, q_lo, p[2u * (std::size_t) cols + f]);
+                    q_lo = __fadd_rn(q_lo, p[3u * (std::size_t) cols + f]);
+                } else {
+                    s_hi = __fadd_rn(s_hi, p[f]);
+                    q_hi = __fadd_rn(q_hi, p[2u * (std::size_t) cols + f]);
+                }
+            }
+            rs = __fadd_rn(s_hi, s_lo);
+            rq = __fadd_rn(q_hi, q_lo);
+            if (n > 0u) {
+                rm = __fdiv_rn(rs, (float) n);
+                if (n > ddof) {
+                    float m2 = __fsub_rn(rq, __fmul_rn(rs, rm));
+                    if (m2 < 0.0f) m2 = 0.0f;
+                    rv = __fdiv_rn(m2, (float) (n - ddof));
+                }
+            }
+            dm = rm;
+            dv = rv;
+        }
+    }
+    out_sum[o] = rs;
+    out_sumsq[o] = rq;
+    if (out_mean != nullptr) out_mean[o] = rm;
+    if (out_var != nullptr) out_var[o] = rv;
+    if (out_mean64 != nullptr) out_mean64[o] = dm;
+    if (out_var64 != nullptr) out_var64[o] = dv;
+}
+
+template <int L, bool COMP>
+int launch_accumulate(const cs_blocked_ell_view *src, const moments_layout &lay, cudaStream_t stream) {
+    const uint32_t segs = lay.col_blocks * (src->block_size / L);
+    dim3 grid(lay.max_chunks, (segs + kAccThreads - 1u) / kAccThreads);
+    const std::size_t smem = (std::size_t) lay.chunk_rows * sizeof(uint2);
+    auto kern = moments_accumulate_kernel<L, COMP>;
+    if (smem > 48u * 1024u &&
+        !cuda_ok(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem),
+                 "moments smem attribute"))
+        return 0;
+    kern<<<grid, kAccThreads, smem, stream>>>(src->val, src->ell_cols, src->block_size, lay.col_blocks, lay.words,
+                                              src->cols, lay.index, lay.chunks, lay.num_chunks, lay.sorted_rows,
+                                              lay.partials);
+    return launch_ok("moments_accumulate_kernel");
+}
+
+int validate(const cs_blocked_ell_view *src, const cs_group_moments_params *p) {
+    if (src == nullptr || p == nullptr) {
+        set_error("group_moments: null view or params");
+        return 0;
+    }
+    if (src->block_size == 0u || src->ell_cols % src->block_size != 0u) {
+        set_error("group_moments: block_size %u does not divide ell_cols %u", src->block_size, src->ell_cols);
+        return 0;
+    }
+    if (p->group_count == 0u || p->group_count > CS_MAX_MOMENT_GROUPS) {
+        set_error("group_moments: group_count %u outside [1, %u]", p->group_count, CS_MAX_MOMENT_GROUPS);
+        return 0;
+    }
+    if (p->scheme > CS_MOMENTS_TWOSUM_F64_COMBINE) {
+        set_error("group_moments: unknown scheme %u", p->scheme);
+        return 0;
+    }
+    if (p->chunk_rows > kMaxChunkRows) {
+        set_error("group_moments: chunk_rows %u above %u", p->chunk_rows, kMaxChunkRows);
+        return 0;
+    }
+    const uint32_t col_blocks = (src->cols + src->block_size - 1u) / src->block_size;
+    if ((col_blocks + 31u) / 32u > kMaxIndexWords) {
+        set_error("group_moments: %u column blocks exceed the index limit", col_blocks);
+        return 0;
+    }
+    return 1;
+}
+
+} // namespace
+} // namespace csb
+
+using namespace csb;
+
+extern "C" int cs_b200_group_moments_scratch_bytes(const cs_blocked_ell_view *src, const cs_group_moments_params *params,
+                                                   size_t *out_bytes) {
+    if (!validate(src, params) || out_bytes == nullptr) {
+        if (out_bytes == nullptr) set_error("group_moments_scratch_bytes: null output");
+        return 0;
+    }
+    moments_layout lay;
+    make_layout(src, params, nullptr, 0, &lay);
+    *out_bytes = lay.bytes;
+    return 1;
+}
+
+extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,
+                                                  const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
+                                                  const cs_group_moments_params *params,
+                                                  const cs_group_moments_out *out, void *d_scratch,
+                                                  size_t scratch_bytes, cs_stream_t s) {
+    if (!validate(src, params)) return 0;
+    if (out == nullptr || out->sum == nullptr || out->sumsq == nullptr) {
+        set_error("group_moments: sum and sumsq outputs are required");
+        return 0;
+    }
+    moments_layout lay;
+    if (!make_layout(src, params, d_scratch, scratch_bytes, &lay) || d_scratch == nullptr) {
+        set_error("group_moments: scratch too small (%zu bytes, need %zu)", scratch_bytes, lay.bytes);
+        return 0;
+    }
+    if (src->rows != 0u && src->ell_cols != 0u && (src->val == nullptr || src->blockColIdx == nullptr)) {
+        set_error("group_moments: null view arrays");
+        return 0;
+    }
+    cudaStream_t stream = as_stream(s);
+    const uint32_t G = params->group_count;
+    const uint32_t width = src->ell_cols / src->block_size;
+
+    if (lay.row_blocks != 0u && lay.words != 0u) {
+        if (width != 0u) {
+            const uint32_t blocks = (lay.row_blocks + kIndexWarps - 1u) / kIndexWarps;
+            const std::size_t smem = (std::size_t) kIndexWarps * lay.words * sizeof(uint32_t);
+            if (smem > 48u * 1024u &&
+                !cuda_ok(cudaFuncSetAttribute(moments_index_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int) smem),
+                         "index smem attribute"))
+                return 0;
+            moments_index_kernel<<<blocks, kIndexWarps * 32, smem, stream>>>(
+                src->blockColIdx, lay.row_blocks, width, lay.col_blocks, lay.words, lay.index, out->status);
+            if (!launch_ok("moments_index_kernel")) return 0;
+        } else if (!cuda_ok(cudaMemsetAsync(lay.index, 0, (std::size_t) lay.row_blocks * lay.words * sizeof(uint2),
+                                            stream),
+                            "index memset")) {
+            return 0;
+        }
+    }
+
+    const std::size_t sort_smem = (std::size_t) kSortWarps * G * sizeof(uint32_t);
+    if (lay.tiles != 0u) {
+        const std::size_t hist_smem = (std::size_t) G * sizeof(uint32_t);
+        moments_tile_hist_kernel<<<lay.tiles, kSortThreads, hist_smem, stream>>>(src->rows, d_row_keep, d_row_labels,
+                                                                                G, lay.tile_counts);
+        if (!launch_ok("moments_tile_hist_kernel")) return 0;
+    }
+    if (lay.tiles != 0u) {
+        moments_group_tiles_kernel<<<(G + 7u) / 8u, 256, 0, stream>>>(lay.tiles, G, lay.tile_counts, lay.group_rows);
+        if (!launch_ok("moments_group_tiles_kernel")) return 0;
+    } else if (!cuda_ok(cudaMemsetAsync(lay.group_rows, 0, (std::size_t) G * sizeof(uint32_t), stream),
+                        "group rows memset")) {
+        return 0;
+    }
+    moments_group_scan_kernel<<<1, 1024, 0, stream>>>(G, lay.chunk_rows, lay.max_chunks, lay.group_rows,
+                                                      lay.group_offsets, lay.chunk_first, lay.num_chunks, lay.chunks);
+    if (!launch_ok("moments_group_scan_kernel")) return 0;
+    if (lay.tiles != 0u) {
+        if (sort_smem > 48u * 1024u &&
+            !cuda_ok(cudaFuncSetAttribute(moments_tile_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) sort_smem),
+                     "scatter smem attribute"))
+            return 0;
+        moments_tile_scatter_kernel<<<lay.tiles, kSortThreads, sort_smem, stream>>>(
+            src->rows, d_row_keep, d_row_labels, G, lay.tile_counts, lay.group_offsets, lay.sorted_rows);
+        if (!launch_ok("moments_tile_scatter_kernel")) return 0;
+    }
+
+    if (lay.col_blocks != 0u && lay.max_chunks != 0u && src->cols != 0u) {
+        const bool comp = params->scheme != CS_MOMENTS_PLAIN_F32;
+        const uint32_t B = src->block_size;
+        const bool aligned16 = (reinterpret_cast<uintptr_t>(src->val) & 15u) == 0u;
+        int ok;
+        if (B % 8u == 0u && aligned16)
+            ok = comp ? launch_accumulate<8, true>(src, lay, stream) : launch_accumulate<8, false>(src, lay, stream);
+        else if (B % 4u == 0u && (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u)
+            ok = comp ? launch_accumulate<4, true>(src, lay, stream) : launch_accumulate<4, false>(src, lay, stream);
+        else if (B % 2u == 0u && (reinterpret_cast<uintptr_t>(src->val) & 3u) == 0u)
+            ok = comp ? launch_accumulate<2, true>(src, lay, stream) : launch_accumulate<2, false>(src, lay, stream);
+        else
+            ok = comp ? launch_accumulate<1, true>(src, lay, stream) : launch_accumulate<1, false>(src, lay, stream);
+        if (!ok) return 0;
+    }
+
+    if (src->cols != 0u || out->group_rows != nullptr) {
+        dim3 grid((src->cols + 255u) / 256u == 0u ? 1u : (src->cols + 255u) / 256u, G);
+        moments_combine_kernel<<<grid, 256, 0, stream>>>(src->cols, G, params->scheme, params->ddof, lay.chunk_first,
+                                                         lay.group_rows, lay.partials, d_feature_keep, out->sum,
+                                                         out->sumsq, out->mean, out->var, out->mean64, out->var64,
+                                                         out->group_rows);
+        if (!launch_ok("moments_combine_kernel")) return 0;
+    }
+    return 1;
+}

@@ -1,0 +1,154 @@
+"""Device-resident formats over torch tensors and the conversion launchers.
+
+Mirrors the reference's device views (include/CellShard/runtime/device/
+sharded_device.cuh:67-98): u32 arrays are held as torch.int32 tensors (same
+bits) and fp16 values as torch.float16.  Every function here calls the C ABI
+of libcellshard_b200.so; nothing computes on the host.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _abi
+
+COMPRESSED_BY_ROW = 0
+COMPRESSED_BY_COL = 1
+INVALID_COL = 0xFFFFFFFF
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("device tensor expected")
+    return t.data_ptr() if t.numel() > 0 else None
+
+
+def u32(t) -> torch.Tensor:
+    """int32 view of a uint32 array (numpy / tensor), moved to the current device."""
+    if isinstance(t, torch.Tensor):
+        return t if t.dtype == torch.int32 else t.to(torch.int32)
+    import numpy as np
+
+    a = np.ascontiguousarray(t, dtype=np.uint32).view(np.int32)
+    return torch.from_numpy(a.copy()).cuda()
+
+
+@dataclass
+class CSR:
+    rows: int
+    cols: int
+    ptr: torch.Tensor  # int32 [major + 1]
+    idx: torch.Tensor  # int32 [nnz]
+    val: torch.Tensor  # float16 [nnz]
+    axis: int = COMPRESSED_BY_ROW
+
+    @property
+    def nnz(self) -> int:
+        return int(self.idx.numel())
+
+    def view(self) -> _abi.CompressedView:
+        v = _abi.CompressedView()
+        v.rows, v.cols, v.nnz, v.axis = self.rows, self.cols, self.nnz, self.axis
+        v.majorPtr, v.minorIdx, v.val = ptr(self.ptr), ptr(self.idx), ptr(self.val)
+        return v
+
+
+@dataclass
+class BlockedELL:
+    rows: int
+    cols: int
+    block_size: int
+    ell_cols: int
+    bci: torch.Tensor  # int32 [row_blocks * ell_width]
+    val: torch.Tensor  # float16 [rows * ell_cols]
+    nnz: int = 0
+
+    @property
+    def row_blocks(self) -> int:
+        return (self.rows + self.block_size - 1) // self.block_size
+
+    @property
+    def ell_width(self) -> int:
+        return self.ell_cols // self.block_size if self.block_size else 0
+
+    def view(self) -> _abi.BlockedEllView:
+        v = _abi.BlockedEllView()
+        v.rows, v.cols, v.nnz, v.block_size, v.ell_cols = self.rows, self.cols, self.nnz, self.block_size, self.ell_cols
+        v.blockColIdx, v.val = ptr(self.bci), ptr(self.val)
+        return v
+
+
+@dataclass
+class SlicedELL:
+    rows: int
+    cols: int
+    nnz: int
+    slice_rows: int
+    slice_row_offsets: torch.Tensor  # int32 [S + 1]
+    slice_widths: torch.Tensor       # int32 [S]
+    slice_slot_offsets: torch.Tensor # int32 [S]
+    col_idx: torch.Tensor            # int32 [total_slots]
+    val: torch.Tensor                # float16 [total_slots]
+
+    @property
+    def slice_count(self) -> int:
+        return int(self.slice_widths.numel())
+
+    def view(self) -> _abi.SlicedEllView:
+        v = _abi.SlicedEllView()
+        v.rows, v.cols, v.nnz, v.slice_count, v.slice_rows = (self.rows, self.cols, self.nnz, self.slice_count,
+                                                              self.slice_rows)
+        v.slice_row_offsets, v.slice_widths = ptr(self.slice_row_offsets), ptr(self.slice_widths)
+        v.slice_slot_offsets, v.col_idx, v.val = ptr(self.slice_slot_offsets), ptr(self.col_idx), ptr(self.val)
+        return v
+
+
+def _scratch(nbytes: int) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device="cuda")
+
+
+def blocked_ell_shape(csr: CSR, block_size: int, keep_bitmaps: bool = True, stream=None):
+    """Shape pass; returns (ell_width, total_blocks, scratch, status) (synchronises)."""
+    lib = _abi.load()
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_blocked_ell_scratch_bytes(csr.rows, csr.cols, block_size, C.byref(nbytes)), "scratch")
+    scratch = _scratch(nbytes.value) if keep_bitmaps else None
+    shape = torch.zeros(2, dtype=torch.int64, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    v = csr.view()
+    _abi.check(lib.cs_b200_blocked_ell_shape(C.byref(v), block_size, ptr(shape), ptr(scratch),
+                                             nbytes.value if keep_bitmaps else 0, ptr(status), stream_handle(stream)),
+               "blocked_ell_shape")
+    sh = shape.cpu()
+    return int(sh[0]), int(sh[1]), scratch, status
+
+
+def blocked_ell_from_csr(csr: CSR, block_size: int, stream=None, check_status: bool = True) -> BlockedELL:
+    """Device CSR -> device Blocked-ELL (convert::blocked_ell_from_compressed on the GPU)."""
+    lib = _abi.load()
+    width, _total, scratch, status = blocked_ell_shape(csr, block_size, True, stream)
+    rb = (csr.rows + block_size - 1) // block_size
+    ell_cols = width * block_size
+    out = BlockedELL(csr.rows, csr.cols, block_size, ell_cols,
+                     torch.empty(rb * width, dtype=torch.int32, device="cuda"),
+                     torch.empty(csr.rows * ell_cols, dtype=torch.float16, device="cuda"), 0)
+    nnz = torch.zeros(1, dtype=torch.int32, device="cuda")
+    v, dv = csr.view(), out.view()
+    _abi.check(lib.cs_b200_blocked_ell_emit(C.byref(v), C.byref(dv), ptr(nnz), ptr(scratch), scratch.numel(),
+                                            ptr(status), stream_handle(stream)), "blocked_ell_emit")
+    out.nnz = int(nnz.cpu().view(torch.int32)[0]) & 0xFFFFFFFF
+    if check_status:
+        st = int(status.cpu()[0])
+        if st:
+            raise _abi.CellShardError(f"blocked_ell conversion flagged invalid input (status 0x{st:x})")
+    return out

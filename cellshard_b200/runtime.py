@@ -1,0 +1,173 @@
+"""Python mirror of the reference's mask_groups runtime
+(include/CellShard/runtime/mask_groups.cuh) over the C ABI.
+
+`compute_sparse_group_reduce*` keep the reference's argument meaning: group
+bitmasks per feature (<= 32 groups), a row/feature mask view, filter params,
+per-row outputs.  `compute_sparse_group_moments` is the row-label grouped
+per-feature moments entry point (no reference counterpart).  Results are
+device tensors; nothing here synchronises except where a value must be read.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _abi
+from .device import BlockedELL, CSR, SlicedELL, ptr, stream_handle
+
+MAX_MASK_GROUPS = 32
+MAX_MOMENT_GROUPS = 4096
+
+PLAIN_F32 = 0
+TWOSUM_F32 = 1
+TWOSUM_F64_COMBINE = 2
+
+
+@dataclass
+class FilterParams:
+    """runtime::sparse_group_filter_params (mask_groups.cuh:36-41)."""
+
+    min_total: float = 0.0
+    min_detected_features: int = 0
+    max_group_fraction: float = 1.0
+    fraction_group_index: int = 0
+
+    def c(self) -> _abi.GroupFilterParams:
+        return _abi.GroupFilterParams(self.min_total, self.min_detected_features, self.max_group_fraction,
+                                      self.fraction_group_index)
+
+
+def _mask_view(row_keep=None, feature_keep=None, row_remap=None, feature_remap=None) -> _abi.RowFeatureMaskView:
+    m = _abi.RowFeatureMaskView()
+    m.row_keep, m.feature_keep = ptr(row_keep), ptr(feature_keep)
+    m.row_remap, m.feature_remap = ptr(row_remap), ptr(feature_remap)
+    return m
+
+
+def compute_sparse_group_reduce(src, feature_group_masks: torch.Tensor | None, group_count: int,
+                                row_keep=None, feature_keep=None, filt: FilterParams | None = None, stream=None):
+    """Masked per-row feature-group reduction (runtime::compute_sparse_group_reduce and
+    compute_sparse_group_reduce_compressed_fallback, mask_groups.cu:811-918)."""
+    lib = _abi.load()
+    rows = src.rows
+    dev = "cuda"
+    res = {
+        "row_totals": torch.empty(rows, dtype=torch.float32, device=dev),
+        "detected_features": torch.empty(rows, dtype=torch.int32, device=dev),
+        "max_values": torch.empty(rows, dtype=torch.float32, device=dev),
+        "row_keep": torch.empty(rows, dtype=torch.uint8, device=dev),
+        "group_counts": torch.empty(rows * group_count, dtype=torch.float32, device=dev) if group_count else None,
+        "group_percentages": torch.empty(rows * group_count, dtype=torch.float32, device=dev) if group_count else None,
+    }
+    out = _abi.GroupReduceOut(ptr(res["row_totals"]), ptr(res["detected_features"]), ptr(res["max_values"]),
+                              ptr(res["row_keep"]), ptr(res["group_counts"]), ptr(res["group_percentages"]))
+    m = _mask_view(row_keep, feature_keep)
+    f = (filt or FilterParams()).c()
+    v = src.view()
+    if isinstance(src, BlockedELL):
+        fn, name = lib.cs_b200_group_reduce_blocked_ell, "group_reduce_blocked_ell"
+    elif isinstance(src, SlicedELL):
+        fn, name = lib.cs_b200_group_reduce_sliced_ell, "group_reduce_sliced_ell"
+    elif isinstance(src, CSR):
+        fn, name = lib.cs_b200_group_reduce_compressed, "group_reduce_compressed"
+    else:
+        raise TypeError(type(src))
+    _abi.check(fn(C.byref(v), ptr(feature_group_masks), group_count, C.byref(m), C.byref(f), C.byref(out),
+                  stream_handle(stream)), name)
+    return res
+
+
+def manual_reoptimize_masked_sparse(src: BlockedELL, row_keep=None, feature_keep=None, row_remap=None,
+                                    feature_remap=None, output_rows: int = 0, output_cols: int = 0, stream=None):
+    """Masked + remapped Blocked-ELL -> CSR (runtime::manual_reoptimize_masked_sparse,
+    mask_groups.cu:960-1034).  Synchronises once to size the output, as the reference does."""
+    lib = _abi.load()
+    out_rows = output_rows if output_rows else src.rows
+    out_cols = output_cols if output_cols else src.cols
+    m = _mask_view(row_keep, feature_keep, row_remap, feature_remap)
+    v = src.view()
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_reoptimize_scratch_bytes(src.rows, out_rows, C.byref(nbytes)), "reoptimize scratch")
+    scratch = torch.empty(max(nbytes.value, 16), dtype=torch.uint8, device="cuda")
+    major = torch.empty(out_rows + 1, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_reoptimize_count(C.byref(v), C.byref(m), out_rows, out_cols, ptr(major), ptr(scratch),
+                                            nbytes.value, ptr(status), s), "reoptimize_count")
+    nnz = int(major[out_rows].item()) & 0xFFFFFFFF
+    idx = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    val = torch.empty(nnz, dtype=torch.float16, device="cuda")
+    _abi.check(lib.cs_b200_reoptimize_emit(C.byref(v), C.byref(m), out_rows, out_cols, ptr(major), ptr(idx),
+                                           ptr(val), s), "reoptimize_emit")
+    st = int(status.item())
+    if st:
+        raise _abi.CellShardError(f"reoptimize flagged invalid input (status 0x{st:x})")
+    meta = {
+        "kept_rows": out_rows,
+        "kept_features": out_cols,
+        "live_nnz": nnz,
+        "bytes_before": src.rows * src.ell_cols * 2 + src.row_blocks * src.ell_width * 4,
+        "bytes_after": (out_rows + 1) * 4 + nnz * 6,
+    }
+    return CSR(out_rows, out_cols, major, idx, val), meta
+
+
+class MomentsWorkspace:
+    """Caller-held scratch for compute_sparse_group_moments (grows monotonically, like the
+    reference's sparse_group_reduce_workspace)."""
+
+    def __init__(self):
+        self.scratch: torch.Tensor | None = None
+
+    def reserve(self, nbytes: int) -> torch.Tensor:
+        if self.scratch is None or self.scratch.numel() < nbytes:
+            self.scratch = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device="cuda")
+        return self.scratch
+
+
+def group_moments_scratch_bytes(src: BlockedELL, group_count: int, scheme: int = TWOSUM_F64_COMBINE,
+                                ddof: int = 1, chunk_rows: int = 0) -> int:
+    lib = _abi.load()
+    p = _abi.GroupMomentsParams(group_count, scheme, ddof, chunk_rows)
+    v = src.view()
+    n = C.c_size_t()
+    _abi.check(lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(p), C.byref(n)), "moments scratch")
+    return n.value
+
+
+def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=None, feature_keep=None,
+                                 row_labels=None, scheme: int = TWOSUM_F64_COMBINE, ddof: int = 1,
+                                 chunk_rows: int = 0, workspace: MomentsWorkspace | None = None, out=None,
+                                 want_f64: bool = False, stream=None):
+    """Per-(group, feature) sum / sum of squares / mean / variance over kept rows of a
+    Blocked-ELL partition; returns a dict of device tensors ([G, cols])."""
+    lib = _abi.load()
+    G, cols = group_count, src.cols
+    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows)
+    v = src.view()
+    n = C.c_size_t()
+    _abi.check(lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(p), C.byref(n)), "moments scratch")
+    ws = workspace or MomentsWorkspace()
+    scratch = ws.reserve(n.value)
+    if out is None:
+        out = {
+            "sum": torch.empty((G, cols), dtype=torch.float32, device="cuda"),
+            "sumsq": torch.empty((G, cols), dtype=torch.float32, device="cuda"),
+            "mean": torch.empty((G, cols), dtype=torch.float32, device="cuda"),
+            "var": torch.empty((G, cols), dtype=torch.float32, device="cuda"),
+            "group_rows": torch.empty(G, dtype=torch.int32, device="cuda"),
+            "status": torch.zeros(1, dtype=torch.int32, device="cuda"),
+        }
+        if want_f64:
+            out["mean64"] = torch.empty((G, cols), dtype=torch.float64, device="cuda")
+            out["var64"] = torch.empty((G, cols), dtype=torch.float64, device="cuda")
+    o = _abi.GroupMomentsOut(ptr(out["sum"]), ptr(out["sumsq"]), ptr(out.get("mean")), ptr(out.get("var")),
+                             ptr(out.get("mean64")), ptr(out.get("var64")), ptr(out.get("group_rows")),
+                             ptr(out.get("status")))
+    _abi.check(lib.cs_b200_group_moments_blocked_ell(C.byref(v), ptr(row_keep), ptr(feature_keep), ptr(row_labels),
+                                                     C.byref(p), C.byref(o), ptr(scratch), scratch.numel(),
+                                                     stream_handle(stream)), "group_moments_blocked_ell")
+    return out

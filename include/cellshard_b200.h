@@ -1,0 +1,381 @@
+/*
+ * cellshard_b200.h -- C ABI of the B200-native CellShard sparse hot path.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * launches hand-written sm_100a kernels from libcellshard_b200.so.  Device
+ * pointers (prefix d_) must point to memory on the current CUDA device; host
+ * pointers are plain malloc'd or pinned memory.
+ *
+ * Conventions kept from the reference (tumlinso/CellShard 0.1.0):
+ *   - int return codes: 1 = success, 0 = failure (src/runtime/mask_groups.cu,
+ *     src/convert/*, src/bucket/*).  On failure cs_b200_last_error() holds a
+ *     one-line message for the calling host thread.
+ *   - raw launchers are stream-ordered and never synchronise; host-struct
+ *     convenience wrappers synchronise and return host-owned results.
+ *   - u32 local indices, fp16 values (passed here as uint16_t IEEE bits).
+ *
+ * Device-side input validation (bad block-column order, duplicate columns,
+ * out-of-range indices) cannot be reported by a return code without a sync,
+ * so launchers that validate take a nullable `uint32_t *d_status` word into
+ * which kernels OR CS_STATUS_* bits.  The caller clears it before the call
+ * and reads it after its own synchronisation point.
+ */
+#ifndef CELLSHARD_B200_H_
+#define CELLSHARD_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CS_B200_ABI_VERSION 1
+#define CS_ALIGN16 __attribute__((aligned(16)))
+#define CS_API __attribute__((visibility("default")))
+
+typedef struct CUstream_st *cs_stream_t; /* == cudaStream_t */
+
+enum {
+    CS_COMPRESSED_BY_ROW = 0, /* sparse::compressed_by_row (formats/compressed.cuh:11-14) */
+    CS_COMPRESSED_BY_COL = 1
+};
+
+#define CS_INVALID_COL 0xffffffffu   /* blocked_ell_invalid_col / sliced_ell_invalid_col */
+#define CS_MAX_MASK_GROUPS 32u       /* runtime::CELLSHARD_MAX_MASK_GROUPS (mask_groups.cuh:14) */
+#define CS_MAX_MOMENT_GROUPS 4096u   /* row-label groups of the moments reduction */
+
+/* Device status bits (OR'd by kernels into *d_status). */
+enum {
+    CS_STATUS_OK = 0u,
+    CS_STATUS_BLOCK_COL_ORDER = 1u << 0,    /* blockColIdx row not ascending / padding not trailing */
+    CS_STATUS_DUPLICATE_COL = 1u << 1,      /* a row repeats a column index */
+    CS_STATUS_INDEX_RANGE = 1u << 2,        /* an index is >= its dimension */
+    CS_STATUS_REMAP_COLLISION = 1u << 3,    /* two kept rows remap to one output row */
+    CS_STATUS_BAD_POINTERS = 1u << 4        /* a CSR row pointer decreases or exceeds nnz */
+};
+
+/* ------------------------------------------------------------------------ */
+/* Device views: field for field the reference's POD views                   */
+/* include/CellShard/runtime/device/sharded_device.cuh:67-98                 */
+/* ------------------------------------------------------------------------ */
+
+typedef struct CS_ALIGN16 cs_compressed_view {
+    uint32_t rows, cols, nnz, axis;
+    uint32_t *majorPtr;
+    uint32_t *minorIdx;
+    uint16_t *val;
+} cs_compressed_view;
+
+typedef struct CS_ALIGN16 cs_blocked_ell_view {
+    uint32_t rows, cols, nnz, block_size, ell_cols;
+    uint32_t *blockColIdx;
+    uint16_t *val;
+} cs_blocked_ell_view;
+
+typedef struct CS_ALIGN16 cs_sliced_ell_view {
+    uint32_t rows, cols, nnz, slice_count, slice_rows;
+    uint32_t *slice_row_offsets;
+    uint32_t *slice_widths;
+    uint32_t *slice_slot_offsets;
+    uint32_t *col_idx;
+    uint16_t *val;
+} cs_sliced_ell_view;
+
+/* Host-owned formats: field for field sparse::compressed, sparse::blocked_ell
+ * and sparse::sliced_ell (formats/compressed.cuh:24-37, blocked_ell.cuh:15-25,
+ * sliced_ell.cuh:16-28).  Results written by this library own one malloc'd
+ * packed block in `storage` laid out as the reference's sparse::allocate()
+ * lays it out, so the reference's sparse::clear() frees them. */
+typedef struct CS_ALIGN16 cs_host_compressed {
+    uint32_t rows, cols, nnz, axis, flags;
+    void *storage;
+    uint32_t *majorPtr;
+    uint32_t *minorIdx;
+    uint16_t *val;
+} cs_host_compressed;
+
+typedef struct CS_ALIGN16 cs_host_blocked_ell {
+    uint32_t rows, cols, nnz, block_size, ell_cols, flags;
+    void *storage;
+    uint32_t *blockColIdx;
+    uint16_t *val;
+} cs_host_blocked_ell;
+
+typedef struct CS_ALIGN16 cs_host_sliced_ell {
+    uint32_t rows, cols, nnz, slice_count, flags;
+    void *storage;
+    uint32_t *slice_row_offsets;
+    uint32_t *slice_widths;
+    uint32_t *col_idx;
+    uint16_t *val;
+} cs_host_sliced_ell;
+
+/* convert::blocked_ell_tune_result (blocked_ell_from_compressed.cuh:16-20) */
+typedef struct cs_blocked_ell_tune_result {
+    unsigned int block_size;
+    double fill_ratio;
+    size_t padded_bytes;
+} cs_blocked_ell_tune_result;
+
+/* convert::sliced_ell_tune_result (sliced_ell_from_blocked_ell.cuh:18-26) */
+typedef struct cs_sliced_ell_tune_result {
+    unsigned int slice_rows;
+    unsigned int slice_count;
+    size_t padded_slots;
+    size_t padded_bytes;
+    double storage_ratio;
+    double slice_penalty;
+    double score;
+} cs_sliced_ell_tune_result;
+
+/* Releases a host result written by this library (sparse::clear semantics:
+ * frees `storage` and zeroes the struct). */
+CS_API void cs_b200_host_compressed_clear(cs_host_compressed *m);
+CS_API void cs_b200_host_blocked_ell_clear(cs_host_blocked_ell *m);
+CS_API void cs_b200_host_sliced_ell_clear(cs_host_sliced_ell *m);
+
+/* runtime::row_feature_mask_view (mask_groups.cuh:29-34) */
+typedef struct CS_ALIGN16 cs_row_feature_mask_view {
+    const uint8_t *row_keep;
+    const uint8_t *feature_keep;
+    const uint32_t *row_remap;
+    const uint32_t *feature_remap;
+} cs_row_feature_mask_view;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Returns CS_B200_ABI_VERSION.  No reference counterpart. */
+CS_API int cs_b200_abi_version(void);
+
+/* Last error message of the calling host thread ("" if none).  Replaces the
+ * reference's fprintf(stderr) helpers (mask_groups.cu:44-48). */
+CS_API const char *cs_b200_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* CSR -> Blocked-ELL                                                         */
+/* replaces convert::blocked_ell_from_compressed and                          */
+/* convert::choose_blocked_ell_block_size (src/convert/                        */
+/* blocked_ell_from_compressed.cuh:33-91,157-190,258-347), which the           */
+/* reference runs as serial host loops.                                       */
+/* ------------------------------------------------------------------------ */
+
+/* Scratch of cs_b200_blocked_ell_shape when it keeps the per-row-block
+ * column-block bitmaps for cs_b200_blocked_ell_emit. */
+CS_API int cs_b200_blocked_ell_scratch_bytes(uint32_t rows, uint32_t cols, uint32_t block_size, size_t *out_bytes);
+
+/* Shape pass (detail::count_blocked_ell_shape_): d_shape[0] <- ell_width
+ * (max distinct column blocks over row blocks), d_shape[1] <- total distinct
+ * (row block, column block) pairs.  d_shape must be zeroed by the caller.
+ * d_scratch may be NULL (shape only, as the chooser needs). */
+CS_API int cs_b200_blocked_ell_shape(const cs_compressed_view *src,
+                              uint32_t block_size,
+                              uint64_t *d_shape,
+                              void *d_scratch,
+                              size_t scratch_bytes,
+                              uint32_t *d_status,
+                              cs_stream_t stream);
+
+/* Emit pass: dst->blockColIdx [row_blocks x ell_width] ascending with
+ * CS_INVALID_COL padding, dst->val [rows x ell_cols] with the value of column
+ * c of row r at r*ell_cols + slot*block_size + c%block_size and zeros
+ * elsewhere; *d_nnz += number of written values that are nonzero as fp32
+ * (the reference's dst->nnz).  d_scratch must hold the bitmaps of a
+ * preceding cs_b200_blocked_ell_shape with the same src and block_size.
+ * Repeated columns in a row resolve to the last one, as in the reference. */
+CS_API int cs_b200_blocked_ell_emit(const cs_compressed_view *src,
+                             const cs_blocked_ell_view *dst,
+                             uint32_t *d_nnz,
+                             const void *d_scratch,
+                             size_t scratch_bytes,
+                             uint32_t *d_status,
+                             cs_stream_t stream);
+
+/* Host convenience with the reference's signature and results:
+ * convert::blocked_ell_from_compressed(src, block_size, dst).  Synchronous. */
+CS_API int cs_b200_blocked_ell_from_compressed(const cs_host_compressed *src,
+                                        unsigned int block_size,
+                                        cs_host_blocked_ell *dst);
+
+/* convert::choose_blocked_ell_block_size: same candidates loop, same
+ * tie-breaking in double, shapes computed on the GPU.  Synchronous. */
+CS_API int cs_b200_choose_blocked_ell_block_size(const cs_host_compressed *src,
+                                          const unsigned int *candidates,
+                                          unsigned int candidate_count,
+                                          cs_blocked_ell_tune_result *out);
+
+/* ------------------------------------------------------------------------ */
+/* mask_groups: masked per-row feature-group reduction                        */
+/* replaces runtime::compute_sparse_group_reduce (mask_groups.cuh:185-204,     */
+/* mask_groups.cu:811-918)                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* runtime::sparse_group_filter_params (mask_groups.cuh:36-41) */
+typedef struct CS_ALIGN16 cs_group_filter_params {
+    float min_total;
+    uint32_t min_detected_features;
+    float max_group_fraction;
+    uint32_t fraction_group_index;
+} cs_group_filter_params;
+
+/* Output arrays of one reduction (runtime::sparse_group_reduce_result,
+ * mask_groups.cuh:43-52): rows entries each, group arrays rows x group_count,
+ * row-major.  group_counts / group_percentages may be NULL when group_count
+ * is 0. */
+typedef struct CS_ALIGN16 cs_group_reduce_out {
+    float *row_totals;
+    uint32_t *detected_features;
+    float *max_values;
+    uint8_t *row_keep;
+    float *group_counts;
+    float *group_percentages;
+} cs_group_reduce_out;
+
+/* compute_group_reduce_blocked_ell_kernel (mask_groups.cu:107-199) via
+ * compute_sparse_group_reduce(blocked_ell_view) (mask_groups.cu:811-845).
+ * d_feature_group_masks: [cols] uint32 bitmasks, or NULL for no groups. */
+CS_API int cs_b200_group_reduce_blocked_ell(const cs_blocked_ell_view *src,
+                                     const uint32_t *d_feature_group_masks,
+                                     uint32_t group_count,
+                                     const cs_row_feature_mask_view *masks,
+                                     const cs_group_filter_params *filter,
+                                     const cs_group_reduce_out *out,
+                                     cs_stream_t stream);
+
+/* compute_sparse_group_reduce(sliced_ell_view) (mask_groups.cu:847-881). */
+CS_API int cs_b200_group_reduce_sliced_ell(const cs_sliced_ell_view *src,
+                                    const uint32_t *d_feature_group_masks,
+                                    uint32_t group_count,
+                                    const cs_row_feature_mask_view *masks,
+                                    const cs_group_filter_params *filter,
+                                    const cs_group_reduce_out *out,
+                                    cs_stream_t stream);
+
+/* compute_sparse_group_reduce_compressed_fallback (mask_groups.cu:883-918). */
+CS_API int cs_b200_group_reduce_compressed(const cs_compressed_view *src,
+                                    const uint32_t *d_feature_group_masks,
+                                    uint32_t group_count,
+                                    const cs_row_feature_mask_view *masks,
+                                    const cs_group_filter_params *filter,
+                                    const cs_group_reduce_out *out,
+                                    cs_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* manual_reoptimize_masked_sparse: masked + remapped Blocked-ELL -> CSR      */
+/* (mask_groups.cuh:220-224, mask_groups.cu:383-462,960-1034)                 */
+/* ------------------------------------------------------------------------ */
+
+/* Scratch for cs_b200_reoptimize_count (per-row claim words + scan). */
+CS_API int cs_b200_reoptimize_scratch_bytes(uint32_t src_rows, uint32_t output_rows, size_t *out_bytes);
+
+/* Pass 1: d_major_ptr[output_rows + 1] <- exclusive scan of kept nonzeros per
+ * output row (count_masked_blocked_ell_rows_kernel + the serial scan at
+ * mask_groups.cu:383-424, here one parallel scan).  Rows whose remap target
+ * is >= output_rows are dropped, as in the reference.  Two kept source rows
+ * with one target set CS_STATUS_REMAP_COLLISION. */
+CS_API int cs_b200_reoptimize_count(const cs_blocked_ell_view *src,
+                             const cs_row_feature_mask_view *masks,
+                             uint32_t output_rows,
+                             uint32_t output_cols,
+                             uint32_t *d_major_ptr,
+                             void *d_scratch,
+                             size_t scratch_bytes,
+                             uint32_t *d_status,
+                             cs_stream_t stream);
+
+/* Pass 2: deterministic scatter (scatter_masked_blocked_ell_to_compressed_kernel,
+ * mask_groups.cu:426-462).  Within an output row the entries keep Blocked-ELL
+ * slot order, which is ascending source column for a sorted blockColIdx. */
+CS_API int cs_b200_reoptimize_emit(const cs_blocked_ell_view *src,
+                            const cs_row_feature_mask_view *masks,
+                            uint32_t output_rows,
+                            uint32_t output_cols,
+                            const uint32_t *d_major_ptr,
+                            uint32_t *d_minor_idx,
+                            uint16_t *d_val,
+                            cs_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Row-label grouped per-feature moments (no reference counterpart: the new   */
+/* entry point beside compute_sparse_group_reduce, same header style).        */
+/* ------------------------------------------------------------------------ */
+
+enum {
+    CS_MOMENTS_PLAIN_F32 = 0,          /* one fp32 running sum per (group, feature) */
+    CS_MOMENTS_TWOSUM_F32 = 1,         /* fp32 batch sums + two-sum compensation, fp32 combine */
+    CS_MOMENTS_TWOSUM_F64_COMBINE = 2  /* as 1, cross-chunk combine and variance in fp64 */
+};
+
+typedef struct CS_ALIGN16 cs_group_moments_params {
+    uint32_t group_count; /* G, 1..CS_MAX_MOMENT_GROUPS */
+    uint32_t scheme;      /* CS_MOMENTS_* */
+    uint32_t ddof;        /* variance divisor is n - ddof (0 or 1) */
+    uint32_t chunk_rows;  /* rows per work chunk, 0 = default */
+} cs_group_moments_params;
+
+/* All arrays are device memory, [G x cols] row-major unless noted.  Only sum
+ * and sumsq are required.  Features whose feature_keep is 0 report zeros. */
+typedef struct CS_ALIGN16 cs_group_moments_out {
+    float *sum;
+    float *sumsq;
+    float *mean;        /* nullable */
+    float *var;         /* nullable */
+    double *mean64;     /* nullable */
+    double *var64;      /* nullable */
+    uint32_t *group_rows; /* [G] kept rows per group, nullable */
+    uint32_t *status;     /* nullable device status word */
+} cs_group_moments_out;
+
+CS_API int cs_b200_group_moments_scratch_bytes(const cs_blocked_ell_view *src,
+                                        const cs_group_moments_params *params,
+                                        size_t *out_bytes);
+
+/* For every kept row r (d_row_keep[r] != 0, or all rows when NULL) with label
+ * g = d_row_labels[r] < G (all rows in group 0 when NULL), and every stored
+ * column f < cols: sum[g][f] += x, sumsq[g][f] += x*x, with x the fp16 value
+ * widened to fp32.  blockColIdx rows must be ascending with CS_INVALID_COL
+ * padding at the end (the layout cs_b200_blocked_ell_emit and
+ * convert::blocked_ell_from_compressed produce); other layouts set
+ * CS_STATUS_BLOCK_COL_ORDER.  Deterministic: the same inputs give the same
+ * bits regardless of stream contention. */
+CS_API int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
+                                      const uint8_t *d_row_keep,
+                                      const uint8_t *d_feature_keep,
+                                      const uint32_t *d_row_labels,
+                                      const cs_group_moments_params *params,
+                                      const cs_group_moments_out *out,
+                                      void *d_scratch,
+                                      size_t scratch_bytes,
+                                      cs_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic cell x gene data (no reference counterpart; feeds tests and the  */
+/* benchmark with seeded NB counts on Zipf-popular columns).                  */
+/* ------------------------------------------------------------------------ */
+
+/* Fills d_minor_idx / d_val of a CSR whose d_row_ptr[rows + 1] is given.
+ * Row r draws ptr[r+1]-ptr[r] distinct columns by successive sampling from
+ * the popularity CDF d_col_cdf[cols] (uint64 thresholds, rank order) mapped
+ * to columns through d_col_of_rank[cols], emitted ascending; value k of the
+ * row is the zero-truncated count drawn from d_val_cdf[val_cdf_len] (value
+ * i+1 for bucket i) times d_row_scale[r] (NULL = 1), rounded to fp16. */
+CS_API int cs_b200_synth_csr(uint32_t rows,
+                      uint32_t cols,
+                      const uint32_t *d_row_ptr,
+                      const uint64_t *d_col_cdf,
+                      const uint32_t *d_col_of_rank,
+                      const uint64_t *d_val_cdf,
+                      uint32_t val_cdf_len,
+                      const float *d_row_scale,
+                      uint64_t seed,
+                      uint32_t *d_minor_idx,
+                      uint16_t *d_val,
+                      cs_stream_t stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CELLSHARD_B200_H_ */

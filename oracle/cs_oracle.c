@@ -1,0 +1,660 @@
+/*
+ * TEST ORACLE ONLY -- CPU restatement of the reference's hot-path algorithms
+ * (see cs_oracle.h).  Plain C, serial unless a thread count is passed.  Used
+ * as the checker by tests/, __graft_entry__.smoke() and the CPU baseline leg
+ * of bench.py; libcellshard_b200 never calls it.
+ */
+#include "cs_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define INVALID_COL 0xffffffffu
+
+/* IEEE binary16 -> binary32, exact. */
+float cso_h2f(uint16_t h) {
+    const uint32_t sign = (uint32_t) (h & 0x8000u) << 16;
+    uint32_t exp = (h >> 10) & 0x1fu;
+    uint32_t man = h & 0x3ffu;
+    uint32_t bits;
+    if (exp == 0u) {
+        if (man == 0u) {
+            bits = sign;
+        } else { /* subnormal: normalise */
+            int e = -1;
+            do {
+                ++e;
+                man <<= 1;
+            } while ((man & 0x400u) == 0u);
+            bits = sign | ((uint32_t) (127 - 15 - e) << 23) | ((man & 0x3ffu) << 13);
+        }
+    } else if (exp == 31u) {
+        bits = sign | 0x7f800000u | (man << 13);
+    } else {
+        bits = sign | ((exp - 15u + 127u) << 23) | (man << 13);
+    }
+    float f;
+    memcpy(&f, &bits, sizeof(f));
+    return f;
+}
+
+static int half_nonzero(uint16_t h) { return (h & 0x7fffu) != 0u; }
+
+/* ------------------------------------------------------------------------ */
+/* mask_groups per-row reduce: for each participating row, values with        */
+/* column < cols, nonzero, feature kept (mask_groups.cu:155,255,338); group   */
+/* sums over the bits of each column's mask (:158-163); keep filter and      */
+/* percentages (:177-194); masked-out rows are zeroed (:81-105).             */
+/* Sums are accumulated in double and rounded once.                          */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    double sum;
+    float vmax;
+    uint32_t det;
+    double g[32];
+} row_state;
+
+static void rs_init(row_state *s) { memset(s, 0, sizeof(*s)); }
+
+static void rs_add(row_state *s, float v, uint32_t gene, const uint32_t *masks, uint32_t G) {
+    s->sum += v;
+    if (v > s->vmax) s->vmax = v;
+    s->det += 1u;
+    if (masks != NULL && G != 0u) {
+        uint32_t m = masks[gene];
+        for (uint32_t g = 0; g < 32u; ++g)
+            if (((m >> g) & 1u) && g < G) s->g[g] += v;
+    }
+}
+
+static void rs_emit(const row_state *s, uint32_t row, uint32_t G, float min_total, uint32_t min_det, float max_frac,
+                    uint32_t frac_idx, cso_reduce_out *o) {
+    const float total = (float) s->sum;
+    o->row_totals[row] = total;
+    o->max_values[row] = s->vmax;
+    o->detected[row] = s->det;
+    const float num = frac_idx < G ? (float) s->g[frac_idx] : 0.0f;
+    const float frac = total > 0.0f ? num / total : 0.0f;
+    o->row_keep[row] = (uint8_t) (total >= min_total && s->det >= min_det && frac <= max_frac);
+    if (o->group_counts != NULL && o->group_percentages != NULL) {
+        for (uint32_t g = 0; g < G; ++g) {
+            const float gs = (float) s->g[g];
+            o->group_counts[(size_t) row * G + g] = gs;
+            o->group_percentages[(size_t) row * G + g] = total > 0.0f ? (100.0f * gs) / total : 0.0f;
+        }
+    }
+}
+
+static void rs_empty(uint32_t row, uint32_t G, cso_reduce_out *o) {
+    o->row_totals[row] = 0.0f;
+    o->max_values[row] = 0.0f;
+    o->detected[row] = 0u;
+    o->row_keep[row] = 0u;
+    if (o->group_counts != NULL && o->group_percentages != NULL) {
+        for (uint32_t g = 0; g < G; ++g) {
+            o->group_counts[(size_t) row * G + g] = 0.0f;
+            o->group_percentages[(size_t) row * G + g] = 0.0f;
+        }
+    }
+}
+
+static int kept_feature(const uint8_t *fk, uint32_t c) { return fk == NULL || fk[c] != 0u; }
+
+int cso_group_reduce_csr(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                         const uint32_t *masks, uint32_t G, const uint8_t *row_keep, const uint8_t *fk,
+                         float min_total, uint32_t min_det, float max_frac, uint32_t frac_idx, cso_reduce_out *o) {
+    if (G > 32u) return 0;
+    for (uint32_t r = 0; r < rows; ++r) {
+        if (row_keep != NULL && row_keep[r] == 0u) {
+            rs_empty(r, G, o);
+            continue;
+        }
+        row_state s;
+        rs_init(&s);
+        for (uint32_t i = ptr[r]; i < ptr[r + 1u]; ++i) {
+            const uint32_t c = idx[i];
+            if (c < cols && half_nonzero(val[i]) && kept_feature(fk, c)) rs_add(&s, cso_h2f(val[i]), c, masks, G);
+        }
+        rs_emit(&s, r, G, min_total, min_det, max_frac, frac_idx, o);
+    }
+    return 1;
+}
+
+int cso_group_reduce_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                          const uint16_t *val, const uint32_t *masks, uint32_t G, const uint8_t *row_keep,
+                          const uint8_t *fk, float min_total, uint32_t min_det, float max_frac, uint32_t frac_idx,
+                          cso_reduce_out *o) {
+    if (G > 32u) return 0;
+    const uint32_t W = B != 0u ? ell_cols / B : 0u;
+    for (uint32_t r = 0; r < rows; ++r) {
+        if (row_keep != NULL && row_keep[r] == 0u) {
+            rs_empty(r, G, o);
+            continue;
+        }
+        row_state s;
+        rs_init(&s);
+        const uint32_t rb = B != 0u ? r / B : 0u;
+        for (uint32_t e = 0; e < ell_cols; ++e) {
+            const uint32_t slot = e / B;
+            const uint32_t bc = W != 0u ? bci[(size_t) rb * W + slot] : INVALID_COL;
+            const uint32_t gene = bc != INVALID_COL ? bc * B + e % B : cols;
+            const uint16_t h = val[(size_t) r * ell_cols + e];
+            if (gene < cols && half_nonzero(h) && kept_feature(fk, gene)) rs_add(&s, cso_h2f(h), gene, masks, G);
+        }
+        rs_emit(&s, r, G, min_total, min_det, max_frac, frac_idx, o);
+    }
+    return 1;
+}
+
+int cso_group_reduce_sell(uint32_t rows, uint32_t cols, uint32_t slice_count, uint32_t slice_rows,
+                          const uint32_t *offsets, const uint32_t *widths, const uint32_t *slot_offsets,
+                          const uint32_t *col_idx, const uint16_t *val, const uint32_t *masks, uint32_t G,
+                          const uint8_t *row_keep, const uint8_t *fk, float min_total, uint32_t min_det,
+                          float max_frac, uint32_t frac_idx, cso_reduce_out *o) {
+    if (G > 32u) return 0;
+    for (uint32_t r = 0; r < rows; ++r) {
+        if (row_keep != NULL && row_keep[r] == 0u) {
+            rs_empty(r, G, o);
+            continue;
+        }
+        row_state s;
+        rs_init(&s);
+        if (slice_count != 0u) {
+            uint32_t slice = 0u;
+            if (slice_rows != 0u) {
+                slice = r / slice_rows;
+                if (slice >= slice_count) slice = slice_count - 1u;
+            } else {
+                while (slice + 1u < slice_count && r >= offsets[slice + 1u]) ++slice; /* mask_groups.cu:243 */
+            }
+            const uint32_t w = widths[slice];
+            const size_t base = (size_t) slot_offsets[slice] + (size_t) (r - offsets[slice]) * w;
+            for (uint32_t k = 0; k < w; ++k) {
+                const uint32_t c = col_idx[base + k];
+                const uint16_t h = val[base + k];
+                if (c < cols && half_nonzero(h) && kept_feature(fk, c)) rs_add(&s, cso_h2f(h), c, masks, G);
+            }
+        }
+        rs_emit(&s, r, G, min_total, min_det, max_frac, frac_idx, o);
+    }
+    return 1;
+}
+
+long long cso_reoptimize_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                              const uint16_t *val, const uint8_t *row_keep, const uint8_t *fk,
+                              const uint32_t *row_remap, const uint32_t *feature_remap, uint32_t out_rows,
+                              uint32_t out_cols, uint32_t *major_ptr, uint32_t *minor_idx, uint16_t *out_val) {
+    const uint32_t W = B != 0u ? ell_cols / B : 0u;
+    int32_t *src_of = (int32_t *) malloc(((size_t) out_rows + 1u) * sizeof(int32_t));
+    if (src_of == NULL) return -2;
+    for (uint32_t i = 0; i < out_rows; ++i) src_of[i] = -1;
+    for (uint32_t r = 0; r < rows; ++r) {
+        if (row_keep != NULL && row_keep[r] == 0u) continue;
+        const uint32_t orow = row_remap != NULL ? row_remap[r] : r;
+        if (orow >= out_rows) continue;
+        if (src_of[orow] >= 0) {
+            free(src_of);
+            return -1;
+        }
+        src_of[orow] = (int32_t) r;
+    }
+    size_t nnz = 0;
+    for (uint32_t orow = 0; orow < out_rows; ++orow) {
+        major_ptr[orow] = (uint32_t) nnz;
+        const int32_t r = src_of[orow];
+        if (r < 0) continue;
+        const uint32_t rb = B != 0u ? (uint32_t) r / B : 0u;
+        for (uint32_t e = 0; e < ell_cols; ++e) {
+            const uint32_t slot = e / B;
+            const uint32_t bc = bci[(size_t) rb * W + slot];
+            if (bc == INVALID_COL) continue;
+            const uint32_t gene = bc * B + e % B;
+            const uint16_t h = val[(size_t) r * ell_cols + e];
+            if (!(gene < cols && half_nonzero(h) && kept_feature(fk, gene))) continue;
+            const uint32_t oc = feature_remap != NULL ? feature_remap[gene] : gene;
+            if (oc >= out_cols) continue;
+            minor_idx[nnz] = oc;
+            out_val[nnz] = h;
+            ++nnz;
+        }
+    }
+    major_ptr[out_rows] = (uint32_t) nnz;
+    free(src_of);
+    return (long long) nnz;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Grouped moments in FP64, row-partitioned over threads with private        */
+/* accumulators merged in thread order (deterministic).                      */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int kind; /* 0 = bell, 1 = csr */
+    uint32_t rows, cols, B, ell_cols;
+    const uint32_t *bci, *ptr, *idx;
+    const uint16_t *val;
+    const uint8_t *row_keep;
+    const uint32_t *labels;
+    uint32_t G;
+    uint32_t r0, r1;
+    double *s, *q;
+    uint32_t *n;
+} mom_task;
+
+static void *mom_worker(void *arg) {
+    mom_task *t = (mom_task *) arg;
+    const uint32_t W = t->B != 0u ? t->ell_cols / t->B : 0u;
+    for (uint32_t r = t->r0; r < t->r1; ++r) {
+        if (t->row_keep != NULL && t->row_keep[r] == 0u) continue;
+        const uint32_t g = t->labels != NULL ? t->labels[r] : 0u;
+        if (g >= t->G) continue;
+        t->n[g] += 1u;
+        double *s = t->s + (size_t) g * t->cols;
+        double *q = t->q + (size_t) g * t->cols;
+        if (t->kind == 0) {
+            const uint32_t rb = r / t->B;
+            const uint32_t *brow = t->bci + (size_t) rb * W;
+            const uint16_t *vrow = t->val + (size_t) r * t->ell_cols;
+            for (uint32_t slot = 0; slot < W; ++slot) {
+                const uint32_t bc = brow[slot];
+                if (bc == INVALID_COL) continue;
+                for (uint32_t l = 0; l < t->B; ++l) {
+                    const uint32_t f = bc * t->B + l;
+                    if (f >= t->cols) continue;
+                    const double x = cso_h2f(vrow[(size_t) slot * t->B + l]);
+                    s[f] += x;
+                    q[f] += x * x;
+                }
+            }
+        } else {
+            for (uint32_t i = t->ptr[r]; i < t->ptr[r + 1u]; ++i) {
+                const uint32_t f = t->idx[i];
+                if (f >= t->cols) continue;
+                const double x = cso_h2f(t->val[i]);
+                s[f] += x;
+                q[f] += x * x;
+            }
+        }
+    }
+    return NULL;
+}
+
+static int moments_run(mom_task proto, const uint8_t *fk, uint32_t ddof, double *sum, double *sumsq, double *mean,
+                       double *var, uint32_t *group_rows, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if ((uint32_t) nthreads > proto.rows && proto.rows > 0u) nthreads = (int) proto.rows;
+    if (nthreads < 1) nthreads = 1;
+    const size_t gc = (size_t) proto.G * proto.cols;
+    mom_task *tasks = (mom_task *) calloc((size_t) nthreads, sizeof(mom_task));
+    pthread_t *th = (pthread_t *) calloc((size_t) nthreads, sizeof(pthread_t));
+    if (tasks == NULL || th == NULL) return 0;
+    int ok = 1;
+    for (int t = 0; t < nthreads; ++t) {
+        tasks[t] = proto;
+        tasks[t].r0 = (uint32_t) (((uint64_t) proto.rows * (uint64_t) t) / (uint64_t) nthreads);
+        tasks[t].r1 = (uint32_t) (((uint64_t) proto.rows * (uint64_t) (t + 1)) / (uint64_t) nthreads);
+        tasks[t].s = (double *) calloc(gc + 1u, sizeof(double));
+        tasks[t].q = (double *) calloc(gc + 1u, sizeof(double));
+        tasks[t].n = (uint32_t *) calloc((size_t) proto.G + 1u, sizeof(uint32_t));
+        if (tasks[t].s == NULL || tasks[t].q == NULL || tasks[t].n == NULL) ok = 0;
+    }
+    if (ok) {
+        for (int t = 1; t < nthreads; ++t) pthread_create(&th[t], NULL, mom_worker, &tasks[t]);
+        mom_worker(&tasks[0]);
+        for (int t = 1; t < nthreads; ++t) pthread_join(th[t], NULL);
+        for (uint32_t g = 0; g < proto.G; ++g) {
+            uint32_t n = 0u;
+            for (int t = 0; t < nthreads; ++t) n += tasks[t].n[g];
+            if (group_rows != NULL) group_rows[g] = n;
+            for (uint32_t f = 0; f < proto.cols; ++f) {
+                const size_t k = (size_t) g * proto.cols + f;
+                double s = 0.0, q = 0.0;
+                for (int t = 0; t < nthreads; ++t) {
+                    s += tasks[t].s[k];
+                    q += tasks[t].q[k];
+                }
+                if (fk != NULL && fk[f] == 0u) s = q = 0.0;
+                double m = 0.0, v = 0.0;
+                if (n > 0u && (fk == NULL || fk[f] != 0u)) {
+                    m = s / (double) n;
+                    if (n > ddof) {
+                        double m2 = q - s * m;
+                        if (m2 < 0.0) m2 = 0.0;
+                        v = m2 / (double) (n - ddof);
+                    }
+                }
+                sum[k] = s;
+                sumsq[k] = q;
+                if (mean != NULL) mean[k] = m;
+                if (var != NULL) var[k] = v;
+            }
+        }
+    }
+    for (int t = 0; t < nthreads; ++t) {
+        free(tasks[t].s);
+        free(tasks[t].q);
+        free(tasks[t].n);
+    }
+    free(tasks);
+    free(th);
+    return ok;
+}
+
+int cso_group_moments_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                           const uint16_t *val, const uint8_t *row_keep, const uint8_t *fk, const uint32_t *labels,
+                           uint32_t G, uint32_t ddof, double *sum, double *sumsq, double *mean, double *var,
+                           uint32_t *group_rows, int nthreads) {
+    if (B == 0u || G == 0u) return 0;
+    mom_task p;
+    memset(&p, 0, sizeof(p));
+    p.kind = 0;
+    p.rows = rows;
+    p.cols = cols;
+    p.B = B;
+    p.ell_cols = ell_cols;
+    p.bci = bci;
+    p.val = val;
+    p.row_keep = row_keep;
+    p.labels = labels;
+    p.G = G;
+    return moments_run(p, fk, ddof, sum, sumsq, mean, var, group_rows, nthreads);
+}
+
+int cso_group_moments_csr(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx,
+                          const uint16_t *val, const uint8_t *row_keep, const uint8_t *fk, const uint32_t *labels,
+                          uint32_t G, uint32_t ddof, double *sum, double *sumsq, double *mean, double *var,
+                          uint32_t *group_rows, int nthreads) {
+    if (G == 0u) return 0;
+    mom_task p;
+    memset(&p, 0, sizeof(p));
+    p.kind = 1;
+    p.rows = rows;
+    p.cols = cols;
+    p.B = 1u;
+    p.ptr = ptr;
+    p.idx = idx;
+    p.val = val;
+    p.row_keep = row_keep;
+    p.labels = labels;
+    p.G = G;
+    return moments_run(p, fk, ddof, sum, sumsq, mean, var, group_rows, nthreads);
+}
+
+int cso_group_moments_bell_f32(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                               const uint16_t *val, const uint8_t *row_keep, const uint32_t *labels, uint32_t G,
+                               float *sum, float *sumsq) {
+    if (B == 0u) return 0;
+    const uint32_t W = ell_cols / B;
+    memset(sum, 0, (size_t) G * cols * sizeof(float));
+    memset(sumsq, 0, (size_t) G * cols * sizeof(float));
+    for (uint32_t r = 0; r < rows; ++r) {
+        if (row_keep != NULL && row_keep[r] == 0u) continue;
+        const uint32_t g = labels != NULL ? labels[r] : 0u;
+        if (g >= G) continue;
+        const uint32_t rb = r / B;
+        for (uint32_t slot = 0; slot < W; ++slot) {
+            const uint32_t bc = bci[(size_t) rb * W + slot];
+            if (bc == INVALID_COL) continue;
+            for (uint32_t l = 0; l < B; ++l) {
+                const uint32_t f = bc * B + l;
+                if (f >= cols) continue;
+                const float x = cso_h2f(val[(size_t) r * ell_cols + (size_t) slot * B + l]);
+                sum[(size_t) g * cols + f] += x;
+                sumsq[(size_t) g * cols + f] += x * x;
+            }
+        }
+    }
+    return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CSR -> Blocked-ELL (blocked_ell_from_compressed.cuh:33-91 shape with epoch */
+/* marks; :294-342 sorted unique block cols per row block, value scatter in  */
+/* CSR order, nnz = count of nonzero written values, :332-344).             */
+/* ------------------------------------------------------------------------ */
+static int cmp_u32(const void *a, const void *b) {
+    const uint32_t x = *(const uint32_t *) a, y = *(const uint32_t *) b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+int cso_blocked_ell_shape(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx, uint32_t B,
+                          uint32_t *ell_width, uint64_t *total_blocks) {
+    *ell_width = 0u;
+    *total_blocks = 0u;
+    if (rows == 0u || cols == 0u || B == 0u) return 1;
+    const uint32_t col_blocks = (cols + B - 1u) / B;
+    const uint32_t row_blocks = (rows + B - 1u) / B;
+    uint32_t *marks = (uint32_t *) calloc(col_blocks, sizeof(uint32_t));
+    if (marks == NULL) return 0;
+    uint32_t epoch = 1u;
+    for (uint32_t rb = 0; rb < row_blocks; ++rb) {
+        uint32_t unique = 0u;
+        const uint32_t r1 = rb * B + B < rows ? rb * B + B : rows;
+        for (uint32_t r = rb * B; r < r1; ++r)
+            for (uint32_t i = ptr[r]; i < ptr[r + 1u]; ++i) {
+                const uint32_t bc = idx[i] / B;
+                if (marks[bc] != epoch) {
+                    marks[bc] = epoch;
+                    ++unique;
+                }
+            }
+        *total_blocks += unique;
+        if (unique > *ell_width) *ell_width = unique;
+        ++epoch;
+    }
+    free(marks);
+    return 1;
+}
+
+uint32_t cso_blocked_ell_from_csr(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx,
+                                  const uint16_t *val, uint32_t B, uint32_t W, uint32_t *bci, uint16_t *out_val) {
+    const uint32_t row_blocks = (rows + B - 1u) / B;
+    const uint32_t col_blocks = (cols + B - 1u) / B;
+    const uint32_t ell_cols = W * B;
+    for (size_t i = 0; i < (size_t) row_blocks * W; ++i) bci[i] = INVALID_COL;
+    memset(out_val, 0, (size_t) rows * ell_cols * sizeof(uint16_t));
+    uint32_t *marks = (uint32_t *) calloc(col_blocks + 1u, sizeof(uint32_t));
+    uint32_t *slot_of = (uint32_t *) calloc(col_blocks + 1u, sizeof(uint32_t));
+    uint32_t *list = (uint32_t *) calloc(W + 1u, sizeof(uint32_t));
+    uint32_t epoch = 1u;
+    for (uint32_t rb = 0; rb < row_blocks; ++rb) {
+        uint32_t unique = 0u;
+        ++epoch;
+        const uint32_t r1 = rb * B + B < rows ? rb * B + B : rows;
+        for (uint32_t r = rb * B; r < r1; ++r)
+            for (uint32_t i = ptr[r]; i < ptr[r + 1u]; ++i) {
+                const uint32_t bc = idx[i] / B;
+                if (marks[bc] != epoch) {
+                    marks[bc] = epoch;
+                    list[unique++] = bc;
+                }
+            }
+        qsort(list, unique, sizeof(uint32_t), cmp_u32);
+        for (uint32_t s = 0; s < unique; ++s) {
+            bci[(size_t) rb * W + s] = list[s];
+            slot_of[list[s]] = s;
+        }
+        for (uint32_t r = rb * B; r < r1; ++r)
+            for (uint32_t i = ptr[r]; i < ptr[r + 1u]; ++i) {
+                const uint32_t c = idx[i];
+                out_val[(size_t) r * ell_cols + (size_t) slot_of[c / B] * B + c % B] = val[i];
+            }
+    }
+    uint32_t nnz = 0u;
+    for (size_t i = 0; i < (size_t) rows * ell_cols; ++i) nnz += half_nonzero(out_val[i]);
+    free(marks);
+    free(slot_of);
+    free(list);
+    return nnz;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CSR -> Sliced-ELL: uniform slices of clamp(slice_rows, 1, rows) rows,      */
+/* width = max row nnz in the slice (build_uniform_sliced_layout_,           */
+/* sliced_ell_from_blocked_ell.cuh:111-142), slot offsets = u32 running sum  */
+/* (sharded_device.cuh:716-723), entries copied into each row's first slots, */
+/* padding col 0xffffffff val 0 (sliced_ell.cuh:218-221, sliced_ell_from_   */
+/* compressed.cuh:125-140).                                                  */
+/* ------------------------------------------------------------------------ */
+static uint32_t clamp_slice(uint32_t rows, uint32_t h) {
+    if (rows == 0u) return 0u;
+    if (h < 1u) h = 1u;
+    return h < rows ? h : rows;
+}
+
+uint32_t cso_sliced_slice_count(uint32_t rows, uint32_t slice_rows) {
+    const uint32_t h = clamp_slice(rows, slice_rows);
+    return rows == 0u ? 0u : (rows + h - 1u) / h;
+}
+
+uint64_t cso_sliced_ell_layout(uint32_t rows, const uint32_t *ptr, uint32_t slice_rows, uint32_t *offsets,
+                               uint32_t *widths, uint32_t *slot_offsets) {
+    const uint32_t h = clamp_slice(rows, slice_rows);
+    const uint32_t S = cso_sliced_slice_count(rows, slice_rows);
+    offsets[0] = 0u;
+    uint32_t run = 0u;
+    uint64_t total = 0u;
+    for (uint32_t s = 0; s < S; ++s) {
+        const uint32_t r0 = s * h, r1 = r0 + h < rows ? r0 + h : rows;
+        uint32_t w = 0u;
+        for (uint32_t r = r0; r < r1; ++r) {
+            const uint32_t n = ptr[r + 1u] - ptr[r];
+            if (n > w) w = n;
+        }
+        offsets[s + 1u] = r1;
+        widths[s] = w;
+        slot_offsets[s] = run;
+        run += (r1 - r0) * w;
+        total += (uint64_t) (r1 - r0) * w;
+    }
+    return total;
+}
+
+void cso_sliced_ell_fill(uint32_t rows, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                         uint32_t slice_rows, const uint32_t *offsets, const uint32_t *widths,
+                         const uint32_t *slot_offsets, uint32_t *col_idx, uint16_t *out_val) {
+    const uint32_t S = cso_sliced_slice_count(rows, slice_rows);
+    for (uint32_t s = 0; s < S; ++s) {
+        const uint32_t w = widths[s];
+        for (uint32_t r = offsets[s]; r < offsets[s + 1u]; ++r) {
+            const size_t base = (size_t) slot_offsets[s] + (size_t) (r - offsets[s]) * w;
+            uint32_t k = 0u;
+            for (uint32_t i = ptr[r]; i < ptr[r + 1u]; ++i, ++k) {
+                col_idx[base + k] = idx[i];
+                out_val[base + k] = val[i];
+            }
+            for (; k < w; ++k) {
+                col_idx[base + k] = INVALID_COL;
+                out_val[base + k] = 0u;
+            }
+        }
+    }
+}
+
+uint64_t cso_sliced_padded_slots(uint32_t rows, const uint32_t *ptr, uint32_t candidate) {
+    const uint32_t h = clamp_slice(rows, candidate);
+    uint64_t padded = 0u;
+    for (uint32_t r0 = 0; r0 < rows; r0 += h) {
+        const uint32_t r1 = r0 + h < rows ? r0 + h : rows;
+        uint32_t w = 0u;
+        for (uint32_t r = r0; r < r1; ++r) {
+            const uint32_t n = ptr[r + 1u] - ptr[r];
+            if (n > w) w = n;
+        }
+        padded += (uint64_t) (r1 - r0) * w;
+    }
+    return padded;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Transpose: stable counting sort by column (rows ascending per column).    */
+/* ------------------------------------------------------------------------ */
+void cso_csr_transpose(uint32_t cDim, uint32_t uDim, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                       uint32_t *out_ptr, uint32_t *out_idx, uint16_t *out_val) {
+    memset(out_ptr, 0, ((size_t) uDim + 1u) * sizeof(uint32_t));
+    const uint32_t nnz = cDim ? ptr[cDim] : 0u;
+    for (uint32_t i = 0; i < nnz; ++i) out_ptr[idx[i] + 1u] += 1u;
+    for (uint32_t c = 0; c < uDim; ++c) out_ptr[c + 1u] += out_ptr[c];
+    uint32_t *head = (uint32_t *) malloc(((size_t) uDim + 1u) * sizeof(uint32_t));
+    memcpy(head, out_ptr, ((size_t) uDim + 1u) * sizeof(uint32_t));
+    for (uint32_t r = 0; r < cDim; ++r)
+        for (uint32_t i = ptr[r]; i < ptr[r + 1u]; ++i) {
+            const uint32_t d = head[idx[i]]++;
+            out_idx[d] = r;
+            out_val[d] = val[i];
+        }
+    free(head);
+}
+
+/* ------------------------------------------------------------------------ */
+/* nnz bucketing: counts (count_major_nnz.cuh), stable ascending sort by     */
+/* count with row ids as values (CUB SortPairs over all 32 key bits,         */
+/* major_nnz_raw.cuh:96-108), equal-count offsets where the first n % B      */
+/* buckets take one extra row (fill_equal_count_bucket_offsets.cuh:13-25).   */
+/* ------------------------------------------------------------------------ */
+static const uint32_t *g_sort_keys;
+static int cmp_by_key_then_id(const void *a, const void *b) {
+    const uint32_t x = *(const uint32_t *) a, y = *(const uint32_t *) b;
+    const uint32_t kx = g_sort_keys[x], ky = g_sort_keys[y];
+    if (kx != ky) return kx < ky ? -1 : 1;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+void cso_major_nnz_plan(const uint32_t *major_ptr, uint32_t n, uint32_t requested, uint32_t *major_nnz,
+                        uint32_t *sorted, uint32_t *order, uint32_t *bucket_offsets) {
+    if (n == 0u) {
+        if (bucket_offsets != NULL) bucket_offsets[0] = 0u;
+        return;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        major_nnz[i] = major_ptr[i + 1u] - major_ptr[i];
+        order[i] = i;
+    }
+    g_sort_keys = major_nnz;
+    qsort(order, n, sizeof(uint32_t), cmp_by_key_then_id);
+    for (uint32_t i = 0; i < n; ++i) sorted[i] = major_nnz[order[i]];
+    if (bucket_offsets != NULL) {
+        uint32_t B = requested < 1u ? 1u : requested;
+        if (B > n) B = n;
+        const uint32_t size = n / B, rem = n % B;
+        uint32_t off = 0u;
+        for (uint32_t b = 0; b < B; ++b) {
+            bucket_offsets[b] = off;
+            off += size + (b < rem ? 1u : 0u);
+        }
+        bucket_offsets[B] = n;
+    }
+}
+
+void cso_pow2_bins(const uint32_t *sorted, uint32_t n, uint32_t *bins) {
+    bins[0] = 0u;
+    for (uint32_t k = 1; k <= 32u; ++k) {
+        const uint64_t bound = (uint64_t) 1u << k;
+        uint32_t lo = 0u, hi = n;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2u;
+            if ((uint64_t) sorted[mid] < bound)
+                lo = mid + 1u;
+            else
+                hi = mid;
+        }
+        bins[k] = lo;
+    }
+    bins[33] = n;
+}
+
+void cso_rebuild(const uint32_t *ptr, const uint32_t *idx, const uint16_t *val, uint32_t n, const uint32_t *order,
+                 uint32_t *dst_ptr, uint32_t *dst_idx, uint16_t *dst_val, uint32_t *inverse) {
+    uint32_t run = 0u;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t src = order[i];
+        const uint32_t len = ptr[src + 1u] - ptr[src];
+        dst_ptr[i] = run;
+        memcpy(dst_idx + run, idx + ptr[src], (size_t) len * sizeof(uint32_t));
+        memcpy(dst_val + run, val + ptr[src], (size_t) len * sizeof(uint16_t));
+        run += len;
+        if (inverse != NULL) inverse[src] = i;
+    }
+    dst_ptr[n] = run;
+}

@@ -1,0 +1,103 @@
+/*
+ * TEST ORACLE ONLY.  CPU restatement of the reference's hot-path algorithms,
+ * used by tests/, __graft_entry__.smoke() and bench.py's CPU baseline as the
+ * checker.  The product (libcellshard_b200) never links or calls it.
+ * Each function cites the reference file:line it restates.
+ */
+#ifndef CS_ORACLE_H_
+#define CS_ORACLE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+float cso_h2f(uint16_t h);
+
+/* ---- mask_groups per-row reduce (src/runtime/mask_groups.cu:107-381) ---- */
+typedef struct cso_reduce_out {
+    float *row_totals;
+    uint32_t *detected;
+    float *max_values;
+    uint8_t *row_keep;
+    float *group_counts;      /* rows x G, nullable */
+    float *group_percentages; /* rows x G, nullable */
+} cso_reduce_out;
+
+int cso_group_reduce_csr(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                         const uint32_t *group_masks, uint32_t G, const uint8_t *row_keep, const uint8_t *feature_keep,
+                         float min_total, uint32_t min_detected, float max_fraction, uint32_t fraction_index,
+                         cso_reduce_out *out);
+int cso_group_reduce_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                          const uint16_t *val, const uint32_t *group_masks, uint32_t G, const uint8_t *row_keep,
+                          const uint8_t *feature_keep, float min_total, uint32_t min_detected, float max_fraction,
+                          uint32_t fraction_index, cso_reduce_out *out);
+int cso_group_reduce_sell(uint32_t rows, uint32_t cols, uint32_t slice_count, uint32_t slice_rows,
+                          const uint32_t *offsets, const uint32_t *widths, const uint32_t *slot_offsets,
+                          const uint32_t *col_idx, const uint16_t *val, const uint32_t *group_masks, uint32_t G,
+                          const uint8_t *row_keep, const uint8_t *feature_keep, float min_total,
+                          uint32_t min_detected, float max_fraction, uint32_t fraction_index, cso_reduce_out *out);
+
+/* ---- manual_reoptimize_masked_sparse (mask_groups.cu:383-462,960-1034) ---- */
+/* Writes major_ptr[out_rows+1]; minor_idx/val must hold rows*ell_cols entries.
+ * Within an output row entries follow Blocked-ELL slot order.  Returns nnz,
+ * or -1 when two kept rows map to one output row. */
+long long cso_reoptimize_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                              const uint16_t *val, const uint8_t *row_keep, const uint8_t *feature_keep,
+                              const uint32_t *row_remap, const uint32_t *feature_remap, uint32_t out_rows,
+                              uint32_t out_cols, uint32_t *major_ptr, uint32_t *minor_idx, uint16_t *out_val);
+
+/* ---- grouped moments, FP64 (no reference counterpart) ---- */
+/* Outputs [G x cols] doubles; group_rows[G].  nthreads >= 1 (row-partitioned). */
+int cso_group_moments_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                           const uint16_t *val, const uint8_t *row_keep, const uint8_t *feature_keep,
+                           const uint32_t *labels, uint32_t G, uint32_t ddof, double *sum, double *sumsq,
+                           double *mean, double *var, uint32_t *group_rows, int nthreads);
+int cso_group_moments_csr(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx,
+                          const uint16_t *val, const uint8_t *row_keep, const uint8_t *feature_keep,
+                          const uint32_t *labels, uint32_t G, uint32_t ddof, double *sum, double *sumsq, double *mean,
+                          double *var, uint32_t *group_rows, int nthreads);
+/* Plain fp32 running sums in row order (the "plain FP32" scheme's reference point). */
+int cso_group_moments_bell_f32(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                               const uint16_t *val, const uint8_t *row_keep, const uint32_t *labels, uint32_t G,
+                               float *sum, float *sumsq);
+
+/* ---- CSR -> Blocked-ELL (src/convert/blocked_ell_from_compressed.cuh:33-91,258-347) ---- */
+int cso_blocked_ell_shape(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx, uint32_t B,
+                          uint32_t *ell_width, uint64_t *total_blocks);
+/* bci[row_blocks*ell_width], val[rows*ell_width*B]; returns the nnz count. */
+uint32_t cso_blocked_ell_from_csr(uint32_t rows, uint32_t cols, const uint32_t *ptr, const uint32_t *idx,
+                                  const uint16_t *val, uint32_t B, uint32_t ell_width, uint32_t *bci,
+                                  uint16_t *out_val);
+
+/* ---- CSR -> Sliced-ELL (src/convert/sliced_ell_from_compressed.cuh:96-164,
+ *      sliced_ell_from_blocked_ell.cuh:64-142) ---- */
+uint32_t cso_sliced_slice_count(uint32_t rows, uint32_t slice_rows);
+/* offsets[S+1], widths[S], slot_offsets[S]; returns total slots. */
+uint64_t cso_sliced_ell_layout(uint32_t rows, const uint32_t *ptr, uint32_t slice_rows, uint32_t *offsets,
+                               uint32_t *widths, uint32_t *slot_offsets);
+void cso_sliced_ell_fill(uint32_t rows, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                         uint32_t slice_rows, const uint32_t *offsets, const uint32_t *widths,
+                         const uint32_t *slot_offsets, uint32_t *col_idx, uint16_t *out_val);
+/* evaluate_sliced_candidate_: padded slots for one candidate height. */
+uint64_t cso_sliced_padded_slots(uint32_t rows, const uint32_t *ptr, uint32_t candidate);
+
+/* ---- transpose: CSR (cDim x uDim) -> CSC, rows ascending in each column
+ *      (cusparseCsr2cscEx2 result used by compressed_transpose_raw.cuh:43-81) ---- */
+void cso_csr_transpose(uint32_t cDim, uint32_t uDim, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                       uint32_t *out_ptr, uint32_t *out_idx, uint16_t *out_val);
+
+/* ---- major-axis nnz bucketing (src/bucket/major_nnz_raw.cuh:64-120,188-250) ---- */
+void cso_major_nnz_plan(const uint32_t *major_ptr, uint32_t n, uint32_t requested, uint32_t *major_nnz,
+                        uint32_t *sorted, uint32_t *order, uint32_t *bucket_offsets);
+void cso_pow2_bins(const uint32_t *sorted, uint32_t n, uint32_t *bins /* 34 */);
+void cso_rebuild(const uint32_t *ptr, const uint32_t *idx, const uint16_t *val, uint32_t n, const uint32_t *order,
+                 uint32_t *dst_ptr, uint32_t *dst_idx, uint16_t *dst_val, uint32_t *inverse);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,351 @@
+"""TEST ORACLE ONLY: numpy wrappers over the C restatement (_build/libcs_oracle.so)
+and the reference bridges (_ref/libcs_ref.so, _ref/libcs_ref_gpu.so).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "_build" / "libcs_oracle.so"
+REF_LIB = HERE / "_ref" / "libcs_ref.so"
+REF_GPU_LIB = HERE / "_ref" / "libcs_ref_gpu.so"
+
+vp = C.c_void_p
+u32 = C.c_uint32
+
+
+def build_restatement() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE), "restate"], check=True)
+
+
+_o = None
+
+
+def lib() -> C.CDLL:
+    global _o
+    if _o is None:
+        if not ORACLE_LIB.exists() or ORACLE_LIB.stat().st_mtime < (HERE / "cs_oracle.c").stat().st_mtime:
+            build_restatement()
+        _o = C.CDLL(str(ORACLE_LIB))
+    return _o
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(vp)
+
+
+def h2f(bits: np.ndarray) -> np.ndarray:
+    return np.asarray(bits, dtype=np.uint16).view(np.float16).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# mask_groups per-row reduce
+# ---------------------------------------------------------------------------
+class ReduceOut(C.Structure):
+    _fields_ = [("row_totals", vp), ("detected", vp), ("max_values", vp), ("row_keep", vp),
+                ("group_counts", vp), ("group_percentages", vp)]
+
+
+def _reduce_outputs(rows, G):
+    res = {
+        "row_totals": np.zeros(rows, np.float32),
+        "detected_features": np.zeros(rows, np.uint32),
+        "max_values": np.zeros(rows, np.float32),
+        "row_keep": np.zeros(rows, np.uint8),
+        "group_counts": np.zeros(rows * G, np.float32) if G else None,
+        "group_percentages": np.zeros(rows * G, np.float32) if G else None,
+    }
+    out = ReduceOut(_p(res["row_totals"]), _p(res["detected_features"]), _p(res["max_values"]),
+                    _p(res["row_keep"]), _p(res["group_counts"]), _p(res["group_percentages"]))
+    return res, out
+
+
+def _f(filt):
+    return (C.c_float(filt[0]), u32(filt[1]), C.c_float(filt[2]), u32(filt[3]))
+
+
+def group_reduce_csr(rows, cols, ptr, idx, val, masks, G, row_keep, feature_keep, filt):
+    res, out = _reduce_outputs(rows, G)
+    ok = lib().cso_group_reduce_csr(u32(rows), u32(cols), _p(ptr), _p(idx), _p(val), _p(masks), u32(G),
+                                    _p(row_keep), _p(feature_keep), *_f(filt), C.byref(out))
+    assert ok == 1
+    return res
+
+
+def group_reduce_bell(rows, cols, B, ell_cols, bci, val, masks, G, row_keep, feature_keep, filt):
+    res, out = _reduce_outputs(rows, G)
+    ok = lib().cso_group_reduce_bell(u32(rows), u32(cols), u32(B), u32(ell_cols), _p(bci), _p(val), _p(masks),
+                                     u32(G), _p(row_keep), _p(feature_keep), *_f(filt), C.byref(out))
+    assert ok == 1
+    return res
+
+
+def group_reduce_sell(rows, cols, slice_rows, offsets, widths, slot_offsets, col_idx, val, masks, G, row_keep,
+                      feature_keep, filt):
+    res, out = _reduce_outputs(rows, G)
+    ok = lib().cso_group_reduce_sell(u32(rows), u32(cols), u32(len(widths)), u32(slice_rows), _p(offsets),
+                                     _p(widths), _p(slot_offsets), _p(col_idx), _p(val), _p(masks), u32(G),
+                                     _p(row_keep), _p(feature_keep), *_f(filt), C.byref(out))
+    assert ok == 1
+    return res
+
+
+def reoptimize_bell(rows, cols, B, ell_cols, bci, val, row_keep, feature_keep, row_remap, feature_remap, out_rows,
+                    out_cols):
+    cap = max(rows * ell_cols, 1)
+    major = np.zeros(out_rows + 1, np.uint32)
+    idx = np.zeros(cap, np.uint32)
+    v = np.zeros(cap, np.uint16)
+    f = lib().cso_reoptimize_bell
+    f.restype = C.c_longlong
+    n = f(u32(rows), u32(cols), u32(B), u32(ell_cols), _p(bci), _p(val), _p(row_keep), _p(feature_keep),
+          _p(row_remap), _p(feature_remap), u32(out_rows), u32(out_cols), _p(major), _p(idx), _p(v))
+    if n < 0:
+        raise ValueError("remap collision")
+    return major, idx[:n].copy(), v[:n].copy()
+
+
+# ---------------------------------------------------------------------------
+# grouped moments (FP64)
+# ---------------------------------------------------------------------------
+def group_moments_bell(rows, cols, B, ell_cols, bci, val, row_keep, feature_keep, labels, G, ddof=1,
+                       nthreads=1):
+    gc = G * cols
+    s, q, m, v = (np.zeros(gc, np.float64) for _ in range(4))
+    n = np.zeros(G, np.uint32)
+    ok = lib().cso_group_moments_bell(u32(rows), u32(cols), u32(B), u32(ell_cols), _p(bci), _p(val), _p(row_keep),
+                                      _p(feature_keep), _p(labels), u32(G), u32(ddof), _p(s), _p(q), _p(m), _p(v),
+                                      _p(n), C.c_int(nthreads))
+    assert ok == 1
+    shp = (G, cols)
+    return {"sum": s.reshape(shp), "sumsq": q.reshape(shp), "mean": m.reshape(shp), "var": v.reshape(shp),
+            "group_rows": n}
+
+
+def group_moments_csr(rows, cols, ptr, idx, val, row_keep, feature_keep, labels, G, ddof=1, nthreads=1):
+    gc = G * cols
+    s, q, m, v = (np.zeros(gc, np.float64) for _ in range(4))
+    n = np.zeros(G, np.uint32)
+    ok = lib().cso_group_moments_csr(u32(rows), u32(cols), _p(ptr), _p(idx), _p(val), _p(row_keep),
+                                     _p(feature_keep), _p(labels), u32(G), u32(ddof), _p(s), _p(q), _p(m), _p(v),
+                                     _p(n), C.c_int(nthreads))
+    assert ok == 1
+    shp = (G, cols)
+    return {"sum": s.reshape(shp), "sumsq": q.reshape(shp), "mean": m.reshape(shp), "var": v.reshape(shp),
+            "group_rows": n}
+
+
+# ---------------------------------------------------------------------------
+# conversions, transpose, bucketing (restatement)
+# ---------------------------------------------------------------------------
+def blocked_ell_shape(rows, cols, ptr, idx, B):
+    w = u32()
+    t = C.c_uint64()
+    assert lib().cso_blocked_ell_shape(u32(rows), u32(cols), _p(ptr), _p(idx), u32(B), C.byref(w), C.byref(t)) == 1
+    return w.value, t.value
+
+
+def blocked_ell_from_csr(rows, cols, ptr, idx, val, B):
+    W, _ = blocked_ell_shape(rows, cols, ptr, idx, B)
+    rb = (rows + B - 1) // B
+    bci = np.zeros(max(rb * W, 1), np.uint32)
+    out = np.zeros(max(rows * W * B, 1), np.uint16)
+    f = lib().cso_blocked_ell_from_csr
+    f.restype = u32
+    nnz = f(u32(rows), u32(cols), _p(ptr), _p(idx), _p(val), u32(B), u32(W), _p(bci), _p(out))
+    return {"ell_width": W, "ell_cols": W * B, "bci": bci[:rb * W], "val": out[:rows * W * B], "nnz": int(nnz)}
+
+
+def sliced_ell_from_csr(rows, ptr, idx, val, slice_rows):
+    f = lib().cso_sliced_slice_count
+    f.restype = u32
+    S = f(u32(rows), u32(slice_rows))
+    offsets = np.zeros(S + 1, np.uint32)
+    widths = np.zeros(max(S, 1), np.uint32)
+    slot_off = np.zeros(max(S, 1), np.uint32)
+    g = lib().cso_sliced_ell_layout
+    g.restype = C.c_uint64
+    total = g(u32(rows), _p(ptr), u32(slice_rows), _p(offsets), _p(widths), _p(slot_off))
+    col_idx = np.zeros(max(total, 1), np.uint32)
+    v = np.zeros(max(total, 1), np.uint16)
+    lib().cso_sliced_ell_fill(u32(rows), _p(ptr), _p(idx), _p(val), u32(slice_rows), _p(offsets), _p(widths),
+                              _p(slot_off), _p(col_idx), _p(v))
+    return {"slice_count": S, "offsets": offsets, "widths": widths[:S], "slot_offsets": slot_off[:S],
+            "col_idx": col_idx[:total], "val": v[:total], "total_slots": int(total)}
+
+
+def sliced_padded_slots(rows, ptr, candidate):
+    f = lib().cso_sliced_padded_slots
+    f.restype = C.c_uint64
+    return int(f(u32(rows), _p(ptr), u32(candidate)))
+
+
+def csr_transpose(cDim, uDim, ptr, idx, val):
+    nnz = int(ptr[cDim]) if cDim else 0
+    out_ptr = np.zeros(uDim + 1, np.uint32)
+    out_idx = np.zeros(max(nnz, 1), np.uint32)
+    out_val = np.zeros(max(nnz, 1), np.uint16)
+    lib().cso_csr_transpose(u32(cDim), u32(uDim), _p(ptr), _p(idx), _p(val), _p(out_ptr), _p(out_idx), _p(out_val))
+    return out_ptr, out_idx[:nnz], out_val[:nnz]
+
+
+def major_nnz_plan(major_ptr, n, requested):
+    nnz = np.zeros(max(n, 1), np.uint32)
+    srt = np.zeros(max(n, 1), np.uint32)
+    order = np.zeros(max(n, 1), np.uint32)
+    B = 1 if n == 0 else min(max(requested, 1), n)
+    offs = np.zeros(B + 1, np.uint32)
+    lib().cso_major_nnz_plan(_p(major_ptr), u32(n), u32(requested), _p(nnz), _p(srt), _p(order), _p(offs))
+    return nnz[:n], srt[:n], order[:n], offs
+
+
+def pow2_bins(sorted_nnz):
+    bins = np.zeros(34, np.uint32)
+    lib().cso_pow2_bins(_p(np.ascontiguousarray(sorted_nnz, np.uint32)), u32(len(sorted_nnz)), _p(bins))
+    return bins
+
+
+def rebuild(ptr, idx, val, n, order):
+    nnz = int(ptr[n]) if n else 0
+    dptr = np.zeros(n + 1, np.uint32)
+    didx = np.zeros(max(nnz, 1), np.uint32)
+    dval = np.zeros(max(nnz, 1), np.uint16)
+    inv = np.zeros(max(n, 1), np.uint32)
+    lib().cso_rebuild(_p(ptr), _p(idx), _p(val), u32(n), _p(order), _p(dptr), _p(didx), _p(dval), _p(inv))
+    return dptr, didx[:nnz], dval[:nnz], inv[:n]
+
+
+# ---------------------------------------------------------------------------
+# the reference's own code (compiled from its sources into _ref/)
+# ---------------------------------------------------------------------------
+class HostCompressed(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("axis", u32), ("flags", u32),
+                ("storage", vp), ("majorPtr", vp), ("minorIdx", vp), ("val", vp), ("_pad", C.c_uint64)]
+
+
+class HostBlockedEll(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("block_size", u32), ("ell_cols", u32),
+                ("flags", u32), ("storage", vp), ("blockColIdx", vp), ("val", vp)]
+
+
+class HostSlicedEll(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("slice_count", u32), ("flags", u32),
+                ("storage", vp), ("slice_row_offsets", vp), ("slice_widths", vp), ("col_idx", vp),
+                ("val", vp)]
+
+
+class BlockedTune(C.Structure):
+    _fields_ = [("block_size", C.c_uint), ("fill_ratio", C.c_double), ("padded_bytes", C.c_size_t)]
+
+
+class SlicedTune(C.Structure):
+    _fields_ = [("slice_rows", C.c_uint), ("slice_count", C.c_uint), ("padded_slots", C.c_size_t),
+                ("padded_bytes", C.c_size_t), ("storage_ratio", C.c_double), ("slice_penalty", C.c_double),
+                ("score", C.c_double)]
+
+
+_r = None
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref() -> C.CDLL:
+    global _r
+    if _r is None:
+        _r = C.CDLL(str(REF_LIB))
+    return _r
+
+
+def host_csr(rows, cols, ptr, idx, val):
+    h = HostCompressed()
+    h.rows, h.cols, h.nnz, h.axis = rows, cols, len(idx), 0
+    h.majorPtr, h.minorIdx, h.val = _p(ptr), _p(idx), _p(val)
+    return h
+
+
+def ref_blocked_ell_from_compressed(rows, cols, ptr, idx, val, B):
+    src = host_csr(rows, cols, ptr, idx, val)
+    dst = HostBlockedEll()
+    ok = ref().csref_blocked_ell_from_compressed(C.byref(src), C.c_uint(B), C.byref(dst))
+    if ok != 1:
+        return None
+    rb = (dst.rows + B - 1) // B
+    W = dst.ell_cols // B if B else 0
+    bci = np.ctypeslib.as_array(C.cast(dst.blockColIdx, C.POINTER(u32)), (rb * W,)).copy() if rb * W else \
+        np.zeros(0, np.uint32)
+    n = dst.rows * dst.ell_cols
+    v = np.ctypeslib.as_array(C.cast(dst.val, C.POINTER(C.c_uint16)), (n,)).copy() if n else np.zeros(0, np.uint16)
+    res = {"ell_cols": dst.ell_cols, "ell_width": W, "bci": bci, "val": v, "nnz": dst.nnz}
+    ref().csref_free(dst.storage)
+    return res
+
+
+def ref_choose_blocked_ell_block_size(rows, cols, ptr, idx, val, candidates):
+    src = host_csr(rows, cols, ptr, idx, val)
+    c = (C.c_uint * len(candidates))(*candidates)
+    out = BlockedTune()
+    ok = ref().csref_choose_blocked_ell_block_size(C.byref(src), c, C.c_uint(len(candidates)), C.byref(out))
+    return (out.block_size, out.fill_ratio, out.padded_bytes) if ok == 1 else None
+
+
+def ref_sliced_ell_from_compressed(rows, cols, ptr, idx, val, slice_rows):
+    src = host_csr(rows, cols, ptr, idx, val)
+    dst = HostSlicedEll()
+    ok = ref().csref_sliced_ell_from_compressed(C.byref(src), C.c_uint(slice_rows), C.byref(dst))
+    if ok != 1:
+        return None
+    S = dst.slice_count
+    f = ref().csref_sliced_total_slots
+    f.restype = u32
+    total = f(C.byref(dst))
+
+    def arr(p, n, t):
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(t)), (n,)).copy() if n else np.zeros(0, np.dtype(t))
+
+    res = {"slice_count": S, "offsets": arr(dst.slice_row_offsets, S + 1 if dst.storage else 0, u32),
+           "widths": arr(dst.slice_row_offsets and dst.slice_widths, S, u32),
+           "col_idx": arr(dst.col_idx, total, u32), "val": arr(dst.val, total, C.c_uint16), "nnz": dst.nnz,
+           "total_slots": int(total)}
+    if dst.storage:
+        ref().csref_free(dst.storage)
+    return res
+
+
+def ref_choose_sliced_ell_slice_rows(rows, cols, ptr, idx, val, candidates):
+    src = host_csr(rows, cols, ptr, idx, val)
+    c = (C.c_uint * len(candidates))(*candidates)
+    out = SlicedTune()
+    ok = ref().csref_choose_sliced_ell_slice_rows_from_compressed(C.byref(src), c, C.c_uint(len(candidates)),
+                                                                  C.byref(out))
+    if ok != 1:
+        return None
+    return {k: getattr(out, k) for k, _ in SlicedTune._fields_}
+
+
+_rg = None
+
+
+def ref_gpu_available() -> bool:
+    return REF_GPU_LIB.exists()
+
+
+def ref_gpu() -> C.CDLL:
+    global _rg
+    if _rg is None:
+        _rg = C.CDLL(str(REF_GPU_LIB))
+    return _rg
+
+
+def cpu_count() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1

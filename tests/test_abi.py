@@ -1,0 +1,123 @@
+"""C-ABI boundary checks that need no GPU: the library loads, exports every
+entry point the header declares, the ctypes mirrors match the C layouts, and
+host-side argument validation rejects bad calls with a message."""
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from cellshard_b200 import _abi
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "cellshard_b200.h"
+
+
+def declared_entry_points():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"CS_API\s+[\w\s\*]*?\b(cs_b200_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(cs_lib):
+    names = declared_entry_points()
+    assert len(names) >= 15
+    nm = subprocess.run(["nm", "-D", "--defined-only", str(_abi.LIB_PATH)], capture_output=True, text=True,
+                        check=True).stdout
+    exported = set(re.findall(r"\bT (cs_b200_\w+)", nm))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    for n in names:
+        getattr(cs_lib, n)
+    assert set(names) <= set(_abi.PROTOTYPES), sorted(set(names) - set(_abi.PROTOTYPES))
+
+
+LAYOUT_C = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "cellshard_b200.h"
+#define S(T) printf(#T " %zu\n", sizeof(T));
+#define O(T, f) printf(#T "." #f " %zu\n", offsetof(T, f));
+int main(void) {
+  S(cs_compressed_view) O(cs_compressed_view, val)
+  S(cs_blocked_ell_view) O(cs_blocked_ell_view, blockColIdx) O(cs_blocked_ell_view, val)
+  S(cs_sliced_ell_view) O(cs_sliced_ell_view, slice_row_offsets) O(cs_sliced_ell_view, val)
+  S(cs_host_compressed) O(cs_host_compressed, storage) O(cs_host_compressed, val)
+  S(cs_host_blocked_ell) O(cs_host_blocked_ell, storage) O(cs_host_blocked_ell, val)
+  S(cs_host_sliced_ell) O(cs_host_sliced_ell, storage) O(cs_host_sliced_ell, val)
+  S(cs_blocked_ell_tune_result) S(cs_sliced_ell_tune_result)
+  S(cs_row_feature_mask_view) S(cs_group_filter_params) S(cs_group_reduce_out)
+  S(cs_group_moments_params) S(cs_group_moments_out)
+  return 0;
+}
+"""
+
+PAIRS = {
+    "cs_compressed_view": _abi.CompressedView,
+    "cs_blocked_ell_view": _abi.BlockedEllView,
+    "cs_sliced_ell_view": _abi.SlicedEllView,
+    "cs_host_compressed": _abi.HostCompressed,
+    "cs_host_blocked_ell": _abi.HostBlockedEll,
+    "cs_host_sliced_ell": _abi.HostSlicedEll,
+    "cs_blocked_ell_tune_result": _abi.BlockedEllTuneResult,
+    "cs_sliced_ell_tune_result": _abi.SlicedEllTuneResult,
+    "cs_row_feature_mask_view": _abi.RowFeatureMaskView,
+    "cs_group_filter_params": _abi.GroupFilterParams,
+    "cs_group_reduce_out": _abi.GroupReduceOut,
+    "cs_group_moments_params": _abi.GroupMomentsParams,
+    "cs_group_moments_out": _abi.GroupMomentsOut,
+}
+
+
+def test_ctypes_layouts_match_c(tmp_path):
+    src = tmp_path / "layout.c"
+    src.write_text(LAYOUT_C)
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        k, v = line.split()
+        got[k] = int(v)
+    for cname, ct in PAIRS.items():
+        assert got[cname] == C.sizeof(ct), cname
+    assert got["cs_blocked_ell_view.val"] == _abi.BlockedEllView.val.offset
+    assert got["cs_sliced_ell_view.val"] == _abi.SlicedEllView.val.offset
+    assert got["cs_host_compressed.val"] == _abi.HostCompressed.val.offset
+    assert got["cs_host_sliced_ell.val"] == _abi.HostSlicedEll.val.offset
+
+
+def test_abi_version_and_host_validation(cs_lib):
+    assert cs_lib.cs_b200_abi_version() == 1
+    v = _abi.BlockedEllView()
+    v.rows, v.cols, v.block_size, v.ell_cols = 100, 64, 16, 64
+    n = C.c_size_t()
+    bad = _abi.GroupMomentsParams(0, 2, 1, 0)
+    assert cs_lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(bad), C.byref(n)) == 0
+    assert b"group_count" in cs_lib.cs_b200_last_error()
+    ok = _abi.GroupMomentsParams(8, 2, 1, 0)
+    assert cs_lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(ok), C.byref(n)) == 1
+    assert n.value > 100 * 4
+    v.ell_cols = 60  # not a multiple of the block size
+    assert cs_lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(ok), C.byref(n)) == 0
+    # more than 32 feature groups is rejected before any device work (mask_groups.cu:729,819)
+    v.ell_cols = 64
+    f = _abi.GroupFilterParams(0.0, 0, 1.0, 0)
+    out = _abi.GroupReduceOut(1, 1, 1, 1, 1, 1)
+    m = _abi.RowFeatureMaskView()
+    assert cs_lib.cs_b200_group_reduce_blocked_ell(C.byref(v), None, 33, C.byref(m), C.byref(f), C.byref(out),
+                                                   None) == 0
+    assert b"33" in cs_lib.cs_b200_last_error()
+    assert cs_lib.cs_b200_blocked_ell_scratch_bytes(10, 10, 0, C.byref(n)) == 0
+    assert cs_lib.cs_b200_blocked_ell_scratch_bytes(1000, 32768, 16, C.byref(n)) == 1
+    assert n.value >= 63 * 64 * 4
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    saved = _abi._lib
+    try:
+        _abi._lib = None
+        with pytest.raises(_abi.CellShardError, match="no CPU fallback"):
+            _abi.load(tmp_path / "absent.so")
+    finally:
+        _abi._lib = saved
