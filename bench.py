@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark: masked grouped per-feature moments on one Blocked-ELL partition.
+
+Workload (one step): 500,000 x 32,768 cell x gene matrix at ~4 % density
+(NB counts, Zipf gene popularity, fp16 values, u32 indices) stored as
+Blocked-ELL block 16 and resident in HBM; a request keeps a Bernoulli(0.7)
+row subset and 20,000 random features and assigns 64 uniform row labels; the
+step computes per-(group, feature) sum and sum of squares (fp32 with two-sum
+compensation, fp64 cross-chunk combine) plus mean and variance.
+
+  value  stored nnz of the kept rows / device time of the step, inputs resident
+  e2e    same metric through the one-shot C-ABI call with the request's masks
+         and labels copied from pinned host memory and the four G x C result
+         arrays copied back every step (the partition itself is staged once,
+         as device::stage_partition does in the reference)
+
+Multi-GPU: one process per GPU (torchrun), each rank an independent replica
+(the reduction needs no exchange for a single partition): weak scaling,
+value = all ranks' nnz / max-over-ranks time.
+
+`--impl reference` times the CPU implementation on the host cores instead
+(rank 0 only): the moments restatement (the reference has no CPU or GPU
+implementation of this reduction) over a bounded row sample whose
+Blocked-ELL comes from the reference's own convert::blocked_ell_from_compressed.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GROUPS = 64
+KEEP_FRAC = 0.7
+KEPT_FEATURES = 20_000
+BLOCK = 16
+FALLBACK_HBM_GBS = 6650.0
+# launches per step: index, tile hist, group tiles, group scan, tile scatter, accumulate, combine
+LAUNCHES_PER_STEP = 7
+# DRAM bytes (read + write) of one moments_accumulate_kernel launch per kept row, from the ncu
+# capture summarised in profiles/ (None until measured; then traffic = this x kept rows)
+NCU_DRAM_BYTES_PER_KEPT_ROW = None
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["cs_b200", "reference"], default="cs_b200")
+    p.add_argument("--rows", type=int, default=500_000)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def measured_peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.lines: list[str] = []
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(device_index), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# reference arm: CPU on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample(spec, tables, rows_wanted: int):
+    """(bell dict, kept rows, kept nnz) for the first rows of the workload, converted to
+    Blocked-ELL by the reference's own code (oracle/_ref) or, without it, the restatement."""
+    from cellshard_b200 import synth
+    from oracle import oracle
+
+    S = (rows_wanted // BLOCK) * BLOCK or BLOCK
+    ptr, idx, val = synth.host_rows(spec, tables, 0, S)
+    if oracle.ref_available():
+        b = oracle.ref_blocked_ell_from_compressed(S, spec.cols, ptr, idx, val, BLOCK)
+        conv = "reference convert::blocked_ell_from_compressed"
+    else:
+        b = oracle.blocked_ell_from_csr(S, spec.cols, ptr, idx, val, BLOCK)
+        conv = "restated blocked_ell_from_compressed"
+    return S, b, conv
+
+
+def time_cpu_moments(S, cols, b, rk, fk, lab, threads):
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    oracle.group_moments_bell(S, cols, BLOCK, b["ell_cols"], b["bci"], b["val"], rk[:S], fk, lab[:S], GROUPS,
+                              ddof=1, nthreads=threads)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    from cellshard_b200 import synth
+    from oracle import oracle
+
+    spec = synth.grouped_reduction_spec(args.rows)
+    tables = synth.host_tables(spec)
+    rk, fk, lab = synth.masks_and_labels(spec.rows, spec.cols, GROUPS, KEEP_FRAC, KEPT_FEATURES)
+    threads = min(64, oracle.cpu_count())
+    # calibrate the sample so one step is ~1-3 s of CPU work
+    S, b, conv = cpu_sample(spec, tables, 1024)
+    dt = time_cpu_moments(S, spec.cols, b, rk, fk, lab, threads)
+    target = max(1.0, min(3.0, 150.0 / max(1, args.steps + args.warmup)))
+    rows = int(min(spec.rows, max(BLOCK, S * target / max(dt, 1e-3))))
+    S, b, conv = cpu_sample(spec, tables, rows)
+    row_nnz = tables[0].astype(np.int64)
+    kept_nnz = int(row_nnz[:S][rk[:S] == 1].sum())
+    for _ in range(args.warmup):
+        time_cpu_moments(S, spec.cols, b, rk, fk, lab, threads)
+    times = [time_cpu_moments(S, spec.cols, b, rk, fk, lab, threads) for _ in range(args.steps)]
+    sec = float(np.mean(times))
+    v = kept_nnz / sec
+    sample = (f"first {S} of {spec.rows} rows ({kept_nnz} kept nnz), Blocked-ELL-16 from {conv}; "
+              f"FP64 grouped-moments restatement (the reference has no implementation of this reduction)")
+    line = {
+        "impl": "reference", "metric": "nnz/s", "value": v, "unit": "nnz/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic NB/Zipf (seeded)",
+        "config": workload_config(spec),
+        "cpu_baseline": {"value": v, "unit": "nnz/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(spec):
+    return {"workload": "masked grouped moments (sum, sumsq, mean, var) over a Blocked-ELL-16 partition",
+            "rows": spec.rows, "cols": spec.cols, "density": 0.04, "block_size": BLOCK, "groups": GROUPS,
+            "row_keep": KEEP_FRAC, "kept_features": KEPT_FEATURES,
+            "scheme": "fp32 two-sum, fp64 combine", "l2": "inputs larger than L2 (no flush needed)",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+# product arm
+# ---------------------------------------------------------------------------
+def run_product(args):
+    import torch
+
+    from cellshard_b200 import runtime, synth
+    from cellshard_b200.device import blocked_ell_from_csr
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    spec = synth.grouped_reduction_spec(args.rows)
+    tables = synth.host_tables(spec)
+    csr = synth.make_csr(spec)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    bell = blocked_ell_from_csr(csr, BLOCK)
+    c1.record()
+    torch.cuda.synchronize()
+    conversion_ms = c0.elapsed_time(c1)  # includes the host read of ell_width between the passes
+    del csr
+    torch.cuda.empty_cache()
+
+    rk, fk, lab = synth.masks_and_labels(spec.rows, spec.cols, GROUPS, KEEP_FRAC, KEPT_FEATURES)
+    row_nnz = tables[0].astype(np.int64)
+    kept_rows = int(rk.sum())
+    kept_nnz = int(row_nnz[rk == 1].sum())
+    d_rk = torch.from_numpy(rk).cuda()
+    d_fk = torch.from_numpy(fk).cuda()
+    d_lab = torch.from_numpy(lab.view(np.int32)).cuda()
+    ws = runtime.MomentsWorkspace()
+    out = {k: torch.empty((GROUPS, spec.cols), dtype=torch.float32, device="cuda")
+           for k in ("sum", "sumsq", "mean", "var")}
+    out["group_rows"] = torch.empty(GROUPS, dtype=torch.int32, device="cuda")
+    out["status"] = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def step(phases=runtime.PHASE_ALL):
+        runtime.compute_sparse_group_moments(bell, GROUPS, d_rk, d_fk, d_lab, workspace=ws, out=out, phases=phases)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if int(out["status"].item()) != 0:
+        raise RuntimeError(f"moments reported input status 0x{int(out['status'].item()):x}")
+
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ka = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kb = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e0.record()
+    for k in range(args.steps):
+        step(runtime.PHASE_PREPARE)
+        ka[k].record()
+        step(runtime.PHASE_ACCUMULATE)
+        kb[k].record()
+        step(runtime.PHASE_COMBINE)
+    e1.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    step_ms = e0.elapsed_time(e1) / args.steps
+    acc_ms = float(np.mean([a.elapsed_time(b) for a, b in zip(ka, kb)]))
+
+    # e2e through the one-shot C-ABI call with host buffers
+    e2e = None
+    if not args.no_e2e:
+        h_rk = torch.from_numpy(rk).pin_memory()
+        h_fk = torch.from_numpy(fk).pin_memory()
+        h_lab = torch.from_numpy(lab.view(np.int32)).pin_memory()
+        h_out = {k: torch.empty((GROUPS, spec.cols), dtype=torch.float32).pin_memory()
+                 for k in ("sum", "sumsq", "mean", "var")}
+        r_rk, r_fk, r_lab = torch.empty_like(d_rk), torch.empty_like(d_fk), torch.empty_like(d_lab)
+        h2d = rk.nbytes + fk.nbytes + lab.nbytes
+        d2h = sum(t.numel() * 4 for t in h_out.values())
+
+        def e2e_step():
+            r_rk.copy_(h_rk, non_blocking=True)
+            r_fk.copy_(h_fk, non_blocking=True)
+            r_lab.copy_(h_lab, non_blocking=True)
+            runtime.compute_sparse_group_moments(bell, GROUPS, r_rk, r_fk, r_lab, workspace=ws, out=out)
+            for k2, t2 in h_out.items():
+                t2.copy_(out[k2], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+
+        for _ in range(2):
+            e2e_step()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record()
+        torch.cuda.synchronize()
+        e2e_ms = f0.elapsed_time(f1) / args.steps
+        assert np.array_equal(h_out["sum"].numpy(), out["sum"].cpu().numpy())
+        e2e = {"ms": e2e_ms, "h2d": h2d, "d2h": d2h}
+    clk = clocks.stop()
+
+    if dist is not None:
+        t = torch.tensor([step_ms, acc_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, acc_ms = float(t[0]), float(t[1])
+        if e2e:
+            e2e["ms"] = float(t[2])
+
+    W = bell.ell_width
+    rb_kept = int(np.unique(np.flatnonzero(rk) // BLOCK).size)
+    chunks_per_group = [(n + 2047) // 2048 for n in np.bincount(lab[rk == 1], minlength=GROUPS)]
+    n_chunks = int(sum(chunks_per_group))
+    acc_bytes = kept_rows * bell.ell_cols * 2 + n_chunks * spec.cols * 16
+    step_bytes = (kept_rows * bell.ell_cols * 2 + rb_kept * W * 4 + spec.rows + spec.cols + 4 * spec.rows
+                  + GROUPS * spec.cols * 8)
+    peak, peak_kind = measured_peak()
+    achieved = acc_bytes / (acc_ms * 1e-3) / 1e9
+    value = world * kept_nnz / (step_ms * 1e-3)
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": "nnz/s", "value": value, "unit": "nnz/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic NB(mean 2, dispersion 0.5) counts on Zipf(1.1) genes, seeded, generated in HBM",
+            "config": workload_config(spec),
+            "hbm_gbs": step_bytes / (step_ms * 1e-3) / 1e9,
+            "roofline": {"bound": "hbm", "kernel": "moments_accumulate_kernel", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": (NCU_DRAM_BYTES_PER_KEPT_ROW * kept_rows
+                                     if NCU_DRAM_BYTES_PER_KEPT_ROW else None),
+                         "algorithmic_bytes": acc_bytes, "kernel_ms": acc_ms},
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "clocks": clk,
+            "extra": {"kept_rows": kept_rows, "kept_nnz": kept_nnz, "ell_cols": bell.ell_cols, "ell_width": W,
+                      "conversion_csr_to_blocked_ell_ms": conversion_ms, "chunks": n_chunks},
+        }
+        if e2e:
+            result["e2e"] = {"value": world * kept_nnz / (e2e["ms"] * 1e-3), "unit": "nnz/s",
+                             "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                             "ms_per_step": e2e["ms"]}
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, args.cpu_seconds)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+
+
+def cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, seconds):
+    """The FP64 moments restatement on the host cores over the first rows of the same
+    Blocked-ELL partition (copied back from HBM), sized to ~`seconds` of CPU time."""
+    from oracle import oracle
+
+    threads = min(64, oracle.cpu_count())
+    W = bell.ell_width
+
+    def sample(S):
+        bci = bell.bci[: (S // BLOCK) * W].cpu().numpy().view(np.uint32)
+        val = bell.val[: S * bell.ell_cols].cpu().numpy().view(np.uint16)
+        b = {"ell_cols": bell.ell_cols, "bci": bci, "val": val}
+        return time_cpu_moments(S, spec.cols, b, rk, fk, lab, threads)
+
+    S = 2048
+    dt = sample(S)
+    S2 = int(min(spec.rows, 65536, max(S, S * seconds / max(dt, 1e-3))))
+    S2 = (S2 // BLOCK) * BLOCK
+    dt = sample(S2) if S2 != S else dt
+    kept = int(row_nnz[:S2][rk[:S2] == 1].sum())
+    return {"value": kept / dt, "unit": "nnz/s", "cores": threads, "kind": "port",
+            "sample": f"first {S2} of {spec.rows} rows ({kept} kept nnz) of the same partition, FP64 restatement "
+                      f"of the grouped moments (no reference implementation exists), {dt:.2f} s"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world, rank, _ = dist_setup(args)
+        if rank != 0:
+            return
+        run_reference(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -309,6 +309,9 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(cs_blocked_ell_view 
         const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
         const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
         uint32_t run = EMIT ? major_ptr[out_row] : 0u;
+        // entries past the row's end (only possible when two rows remap to one
+        // output row, which the count pass flags) are dropped, never written
+        const uint32_t end = EMIT ? major_ptr[out_row + 1u] : 0u;
         for (uint32_t e0 = 0; e0 < src.ell_cols; e0 += 32u) {
             const uint32_t e = e0 + lane;
             uint32_t oc = 0u;
@@ -325,8 +328,10 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(cs_blocked_ell_view 
             const uint32_t ballot = __ballot_sync(0xffffffffu, k);
             if (EMIT && k) {
                 const uint32_t pos = run + __popc(ballot & ((1u << lane) - 1u));
-                minor_idx[pos] = oc;
-                out_val[pos] = h;
+                if (pos < end) {
+                    minor_idx[pos] = oc;
+                    out_val[pos] = h;
+                }
             }
             run += __popc(ballot);
         }

@@ -561,11 +561,10 @@ extern "C" int cs_b200_group_moments_scratch_bytes(const cs_blocked_ell_view *sr
     return 1;
 }
 
-extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,
-                                                  const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
-                                                  const cs_group_moments_params *params,
-                                                  const cs_group_moments_out *out, void *d_scratch,
-                                                  size_t scratch_bytes, cs_stream_t s) {
+static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep, const uint8_t *d_feature_keep,
+                       const uint32_t *d_row_labels, const cs_group_moments_params *params,
+                       const cs_group_moments_out *out, void *d_scratch, size_t scratch_bytes, cs_stream_t s,
+                       uint32_t phases) {
     if (!validate(src, params)) return 0;
     if (out == nullptr || out->sum == nullptr || out->sumsq == nullptr) {
         set_error("group_moments: sum and sumsq outputs are required");
@@ -584,7 +583,7 @@ extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
     const uint32_t G = params->group_count;
     const uint32_t width = src->ell_cols / src->block_size;
 
-    if (lay.row_blocks != 0u && lay.words != 0u) {
+    if ((phases & CS_MOMENTS_PHASE_PREPARE) && lay.row_blocks != 0u && lay.words != 0u) {
         if (width != 0u) {
             const uint32_t blocks = (lay.row_blocks + kIndexWarps - 1u) / kIndexWarps;
             const std::size_t smem = (std::size_t) kIndexWarps * lay.words * sizeof(uint32_t);
@@ -604,6 +603,7 @@ extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
     }
 
     const std::size_t sort_smem = (std::size_t) kSortWarps * G * sizeof(uint32_t);
+    if (phases & CS_MOMENTS_PHASE_PREPARE) {
     if (lay.tiles != 0u) {
         const std::size_t hist_smem = (std::size_t) G * sizeof(uint32_t);
         moments_tile_hist_kernel<<<lay.tiles, kSortThreads, hist_smem, stream>>>(src->rows, d_row_keep, d_row_labels,
@@ -630,8 +630,9 @@ extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
             src->rows, d_row_keep, d_row_labels, G, lay.tile_counts, lay.group_offsets, lay.sorted_rows);
         if (!launch_ok("moments_tile_scatter_kernel")) return 0;
     }
+    }
 
-    if (lay.col_blocks != 0u && lay.max_chunks != 0u && src->cols != 0u) {
+    if ((phases & CS_MOMENTS_PHASE_ACCUMULATE) && lay.col_blocks != 0u && lay.max_chunks != 0u && src->cols != 0u) {
         const bool comp = params->scheme != CS_MOMENTS_PLAIN_F32;
         const uint32_t B = src->block_size;
         const bool aligned16 = (reinterpret_cast<uintptr_t>(src->val) & 15u) == 0u;
@@ -647,7 +648,7 @@ extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
         if (!ok) return 0;
     }
 
-    if (src->cols != 0u || out->group_rows != nullptr) {
+    if ((phases & CS_MOMENTS_PHASE_COMBINE) && (src->cols != 0u || out->group_rows != nullptr)) {
         dim3 grid((src->cols + 255u) / 256u == 0u ? 1u : (src->cols + 255u) / 256u, G);
         moments_combine_kernel<<<grid, 256, 0, stream>>>(src->cols, G, params->scheme, params->ddof, lay.chunk_first,
                                                          lay.group_rows, lay.partials, d_feature_keep, out->sum,
@@ -656,4 +657,25 @@ extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
         if (!launch_ok("moments_combine_kernel")) return 0;
     }
     return 1;
+}
+
+extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,
+                                                  const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
+                                                  const cs_group_moments_params *params,
+                                                  const cs_group_moments_out *out, void *d_scratch,
+                                                  size_t scratch_bytes, cs_stream_t s) {
+    return moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, out, d_scratch, scratch_bytes, s,
+                       CS_MOMENTS_PHASE_ALL);
+}
+
+extern "C" int cs_b200_group_moments_phases(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,
+                                            const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
+                                            const cs_group_moments_params *params, const cs_group_moments_out *out,
+                                            void *d_scratch, size_t scratch_bytes, uint32_t phases, cs_stream_t s) {
+    if ((phases & ~(uint32_t) CS_MOMENTS_PHASE_ALL) != 0u) {
+        set_error("group_moments_phases: unknown phase bits 0x%x", phases);
+        return 0;
+    }
+    return moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, out, d_scratch, scratch_bytes, s,
+                       phases);
 }

@@ -21,6 +21,11 @@ from .device import BlockedELL, CSR, SlicedELL, ptr, stream_handle
 MAX_MASK_GROUPS = 32
 MAX_MOMENT_GROUPS = 4096
 
+PHASE_PREPARE = 1
+PHASE_ACCUMULATE = 2
+PHASE_COMBINE = 4
+PHASE_ALL = 7
+
 PLAIN_F32 = 0
 TWOSUM_F32 = 1
 TWOSUM_F64_COMBINE = 2
@@ -141,7 +146,7 @@ def group_moments_scratch_bytes(src: BlockedELL, group_count: int, scheme: int =
 def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=None, feature_keep=None,
                                  row_labels=None, scheme: int = TWOSUM_F64_COMBINE, ddof: int = 1,
                                  chunk_rows: int = 0, workspace: MomentsWorkspace | None = None, out=None,
-                                 want_f64: bool = False, stream=None):
+                                 want_f64: bool = False, phases: int = 7, stream=None):
     """Per-(group, feature) sum / sum of squares / mean / variance over kept rows of a
     Blocked-ELL partition; returns a dict of device tensors ([G, cols])."""
     lib = _abi.load()
@@ -167,7 +172,13 @@ def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=Non
     o = _abi.GroupMomentsOut(ptr(out["sum"]), ptr(out["sumsq"]), ptr(out.get("mean")), ptr(out.get("var")),
                              ptr(out.get("mean64")), ptr(out.get("var64")), ptr(out.get("group_rows")),
                              ptr(out.get("status")))
-    _abi.check(lib.cs_b200_group_moments_blocked_ell(C.byref(v), ptr(row_keep), ptr(feature_keep), ptr(row_labels),
-                                                     C.byref(p), C.byref(o), ptr(scratch), scratch.numel(),
-                                                     stream_handle(stream)), "group_moments_blocked_ell")
+    if phases == PHASE_ALL:
+        _abi.check(lib.cs_b200_group_moments_blocked_ell(C.byref(v), ptr(row_keep), ptr(feature_keep),
+                                                         ptr(row_labels), C.byref(p), C.byref(o), ptr(scratch),
+                                                         scratch.numel(), stream_handle(stream)),
+                   "group_moments_blocked_ell")
+    else:
+        _abi.check(lib.cs_b200_group_moments_phases(C.byref(v), ptr(row_keep), ptr(feature_keep), ptr(row_labels),
+                                                    C.byref(p), C.byref(o), ptr(scratch), scratch.numel(), phases,
+                                                    stream_handle(stream)), "group_moments_phases")
     return out

@@ -100,6 +100,59 @@ def host_tables(spec: MatrixSpec):
     return nnz, ptr.astype(np.uint32), col_cdf, col_of_rank, val_cdf, scale
 
 
+_COL_SALT = 0x636F6C756D6E73
+_VAL_SALT = 0x76616C7565737321
+
+
+def _splitmix64(z: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def _draw_u53(key: np.uint64, row: int, j: np.ndarray) -> np.ndarray:
+    return _splitmix64(key ^ ((np.uint64(row) << np.uint64(32)) | j.astype(np.uint64))) >> np.uint64(11)
+
+
+def host_rows(spec: MatrixSpec, tables, r0: int, r1: int):
+    """Rows [r0, r1) of the matrix cs_b200_synth_csr generates, computed on the host
+    with the same draws (bit-identical); returns (ptr, idx, val_bits)."""
+    nnz, rp, col_cdf, col_of_rank, val_cdf, scale = tables
+    cols = spec.cols
+    col_key = _splitmix64(np.array([spec.seed ^ _COL_SALT], np.uint64))[0]
+    val_key = _splitmix64(np.array([spec.seed ^ _VAL_SALT], np.uint64))[0]
+    max_draws = ((64 * cols + 1024) // 32) * 32
+    base = int(rp[r0])
+    ptr = (rp[r0:r1 + 1].astype(np.int64) - base).astype(np.uint32)
+    idx = np.empty(int(ptr[-1]), np.uint32)
+    val = np.empty(int(ptr[-1]), np.uint16)
+    for r in range(r0, r1):
+        need = min(int(nnz[r]), cols)
+        chosen = np.zeros(cols, bool)
+        count, j0 = 0, 0
+        while count < need and j0 < max_draws:
+            batch = min(max(256, 4 * (need - count)), max_draws - j0)
+            j = np.arange(j0, j0 + batch, dtype=np.uint64)
+            c = col_of_rank[np.searchsorted(col_cdf, _draw_u53(col_key, r, j), side="right")]
+            first = np.zeros(batch, bool)
+            first[np.unique(c, return_index=True)[1]] = True
+            acc = np.flatnonzero(first & ~chosen[c])[:need - count]
+            chosen[c[acc]] = True
+            count += len(acc)
+            j0 += batch
+        if count < need:
+            chosen[np.flatnonzero(~chosen)[:need - count]] = True
+        cs = np.flatnonzero(chosen).astype(np.uint32)
+        k = np.searchsorted(val_cdf, _draw_u53(val_key, r, np.arange(need, dtype=np.uint64)), side="right") + 1
+        sc = np.float32(scale[r]) if scale is not None else np.float32(1.0)
+        a, b = int(ptr[r - r0]), int(ptr[r - r0 + 1])
+        idx[a:b] = cs
+        val[a:b] = (k.astype(np.float32) * sc).astype(np.float16).view(np.uint16)
+    return ptr, idx, val
+
+
 def make_csr(spec: MatrixSpec, stream=None):
     """Generates the matrix on the current CUDA device; returns device.CSR."""
     import torch

@@ -350,6 +350,30 @@ CS_API int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
                                       size_t scratch_bytes,
                                       cs_stream_t stream);
 
+/* The same work split into its three stream-ordered phases, for callers that
+ * time or schedule them separately (the one-shot call above runs all three):
+ * PREPARE builds the column-block index and sorts the kept rows by label,
+ * ACCUMULATE streams the values (the dominant kernel), COMBINE adds the
+ * per-chunk partials and writes the outputs.  Consecutive phase calls must
+ * pass identical arguments and scratch. */
+enum {
+    CS_MOMENTS_PHASE_PREPARE = 1u,
+    CS_MOMENTS_PHASE_ACCUMULATE = 2u,
+    CS_MOMENTS_PHASE_COMBINE = 4u,
+    CS_MOMENTS_PHASE_ALL = 7u
+};
+
+CS_API int cs_b200_group_moments_phases(const cs_blocked_ell_view *src,
+                                        const uint8_t *d_row_keep,
+                                        const uint8_t *d_feature_keep,
+                                        const uint32_t *d_row_labels,
+                                        const cs_group_moments_params *params,
+                                        const cs_group_moments_out *out,
+                                        void *d_scratch,
+                                        size_t scratch_bytes,
+                                        uint32_t phases,
+                                        cs_stream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic cell x gene data (no reference counterpart; feeds tests and the  */
 /* benchmark with seeded NB counts on Zipf-popular columns).                  */
