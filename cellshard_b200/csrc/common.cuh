@@ -72,7 +72,7 @@ __device__ __forceinline__ void status_or(uint32_t *status, uint32_t bits) {
 // streams are touched once).
 __device__ __forceinline__ uint4 ld_stream_v4(const void *p) {
     uint4 r;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4];"
+    asm("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
                  : "l"(p));
     return r;

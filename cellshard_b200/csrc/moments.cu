@@ -265,49 +265,52 @@ __global__ void __launch_bounds__(kSortThreads) moments_tile_scatter_kernel(uint
 // ---------------------------------------------------------------------------
 // 3. Accumulation.
 // ---------------------------------------------------------------------------
+// Raw loads of L consecutive fp16 values (kept as packed words so a batch of
+// rows can be in flight before any conversion).
 template <int L>
-struct vec_load;
-template <>
-struct vec_load<8> {
-    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
+struct raw_vec {
+    static constexpr int W = (L + 1) / 2; // 32-bit words
+    uint32_t w[W];
+};
+
+template <int L>
+__device__ __forceinline__ void load_raw(const uint16_t *p, raw_vec<L> &r) {
+    if constexpr (L == 8) {
         const uint4 v = ld_stream_v4(p);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[i]));
-            x[2 * i] = f.x;
-            x[2 * i + 1] = f.y;
-        }
-    }
-};
-template <>
-struct vec_load<4> {
-    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
+        r.w[0] = v.x;
+        r.w[1] = v.y;
+        r.w[2] = v.z;
+        r.w[3] = v.w;
+    } else if constexpr (L == 4) {
         const uint2 v = __ldg(reinterpret_cast<const uint2 *>(p));
-        const uint32_t w[2] = {v.x, v.y};
+        r.w[0] = v.x;
+        r.w[1] = v.y;
+    } else if constexpr (L == 2) {
+        r.w[0] = __ldg(reinterpret_cast<const unsigned int *>(p));
+    } else {
+        r.w[0] = __ldg(reinterpret_cast<const unsigned short *>(p));
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void zero_raw(raw_vec<L> &r) {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[i]));
+    for (int i = 0; i < raw_vec<L>::W; ++i) r.w[i] = 0u;
+}
+
+template <int L>
+__device__ __forceinline__ void unpack(const raw_vec<L> &r, float *x) {
+    if constexpr (L == 1) {
+        x[0] = h2f((uint16_t) r.w[0]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < L / 2; ++i) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&r.w[i]));
             x[2 * i] = f.x;
             x[2 * i + 1] = f.y;
         }
     }
-};
-template <>
-struct vec_load<2> {
-    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
-        const uint32_t w = __ldg(reinterpret_cast<const unsigned int *>(p));
-        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w));
-        x[0] = f.x;
-        x[1] = f.y;
-    }
-};
-template <>
-struct vec_load<1> {
-    __device__ __forceinline__ static void load(const uint16_t *p, float *x) {
-        x[0] = h2f(__ldg(reinterpret_cast<const unsigned short *>(p)));
-    }
-};
+}
 
 // Knuth two-sum folded into a running (hi, lo) pair.
 __device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float b) {
@@ -319,7 +322,7 @@ __device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float b) {
 }
 
 template <int L, bool COMP>
-__global__ void __launch_bounds__(kAccThreads) moments_accumulate_kernel(
+__global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
     const uint16_t *__restrict__ val, uint32_t ell_cols, uint32_t block_size, uint32_t col_blocks, uint32_t words,
     uint32_t cols, const uint2 *__restrict__ index, const chunk_desc *__restrict__ chunks,
     const uint32_t *__restrict__ num_chunks, const uint32_t *__restrict__ sorted_rows, float *__restrict__ partials) {
@@ -338,7 +341,7 @@ __global__ void __launch_bounds__(kAccThreads) moments_accumulate_kernel(
     const uint32_t seg = blockIdx.y * kAccThreads + threadIdx.x;
     const uint32_t b = seg / segs_per_block;
     const uint32_t part = seg - b * segs_per_block;
-    const bool active = b < col_blocks;
+    if (b >= col_blocks) return;
     const uint32_t w = b >> 5;
     const uint32_t below = (1u << (b & 31u)) - 1u;
     const uint32_t bitmask = 1u << (b & 31u);
@@ -348,55 +351,77 @@ __global__ void __launch_bounds__(kAccThreads) moments_accumulate_kernel(
 #pragma unroll
     for (int j = 0; j < L; ++j) s_hi[j] = s_lo[j] = q_hi[j] = q_lo[j] = 0.0f;
 
-    if (active) {
-        uint32_t i = 0;
-        for (; i + kBatch <= n; i += kBatch) {
-            float x[kBatch][L];
+    // two-stage software pipeline: the index entries of batch i+1 are in
+    // flight while batch i's value loads are outstanding
+    uint2 e_next[kBatch];
+#pragma unroll
+    for (unsigned u = 0; u < kBatch; ++u)
+        e_next[u] = u < n ? __ldg(index + (std::size_t) chunk_rows_smem[u].y + w) : make_uint2(0u, 0u);
+    uint32_t i = 0;
+    for (; i + kBatch <= n; i += kBatch) {
+        raw_vec<L> raw[kBatch];
+#pragma unroll
+        for (unsigned u = 0; u < kBatch; ++u) {
+            const uint2 e = e_next[u];
+            if (e.x & bitmask) {
+                const uint32_t slot = e.y + __popc(e.x & below);
+                load_raw<L>(val + (std::size_t) chunk_rows_smem[i + u].x * ell_cols + (std::size_t) slot * block_size +
+                                lane_off,
+                            raw[u]);
+            } else {
+                zero_raw<L>(raw[u]);
+            }
+        }
+#pragma unroll
+        for (unsigned u = 0; u < kBatch; ++u) {
+            const uint32_t k = i + kBatch + u;
+            e_next[u] = k < n ? __ldg(index + (std::size_t) chunk_rows_smem[k].y + w) : make_uint2(0u, 0u);
+        }
+        if (COMP) {
+            float bs[L], bq[L];
+#pragma unroll
+            for (int j = 0; j < L; ++j) bs[j] = bq[j] = 0.0f;
 #pragma unroll
             for (unsigned u = 0; u < kBatch; ++u) {
-                const uint2 rr = chunk_rows_smem[i + u];
-                const uint32_t r = rr.x;
-                const uint2 e = __ldg(index + (std::size_t) rr.y + w);
-                if (e.x & bitmask) {
-                    const uint32_t slot = e.y + __popc(e.x & below);
-                    vec_load<L>::load(val + (std::size_t) r * ell_cols + (std::size_t) slot * block_size + lane_off,
-                                      x[u]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < L; ++j) x[u][j] = 0.0f;
-                }
-            }
-            if (COMP) {
+                float x[L];
+                unpack<L>(raw[u], x);
 #pragma unroll
                 for (int j = 0; j < L; ++j) {
-                    float bs = 0.0f, bq = 0.0f;
-#pragma unroll
-                    for (unsigned u = 0; u < kBatch; ++u) {
-                        bs = __fadd_rn(bs, x[u][j]);
-                        bq = __fmaf_rn(x[u][j], x[u][j], bq);
-                    }
-                    two_sum_acc(s_hi[j], s_lo[j], bs);
-                    two_sum_acc(q_hi[j], q_lo[j], bq);
+                    bs[j] = __fadd_rn(bs[j], x[j]);
+                    bq[j] = __fmaf_rn(x[j], x[j], bq[j]);
                 }
-            } else {
+            }
 #pragma unroll
-                for (unsigned u = 0; u < kBatch; ++u) {
+            for (int j = 0; j < L; ++j) {
+                two_sum_acc(s_hi[j], s_lo[j], bs[j]);
+                two_sum_acc(q_hi[j], q_lo[j], bq[j]);
+            }
+        } else {
 #pragma unroll
-                    for (int j = 0; j < L; ++j) {
-                        s_hi[j] = __fadd_rn(s_hi[j], x[u][j]);
-                        q_hi[j] = __fmaf_rn(x[u][j], x[u][j], q_hi[j]);
-                    }
+            for (unsigned u = 0; u < kBatch; ++u) {
+                float x[L];
+                unpack<L>(raw[u], x);
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    s_hi[j] = __fadd_rn(s_hi[j], x[j]);
+                    q_hi[j] = __fmaf_rn(x[j], x[j], q_hi[j]);
                 }
             }
         }
-        for (; i < n; ++i) {
-            const uint2 rr = chunk_rows_smem[i];
-            const uint32_t r = rr.x;
-            const uint2 e = __ldg(index + (std::size_t) rr.y + w);
+    }
+    // tail rows (fewer than a batch); their index entries are in e_next
+#pragma unroll
+    for (unsigned u = 0; u < kBatch; ++u) {
+        if (i + u < n) {
+            const uint2 e = e_next[u];
             if (e.x & bitmask) {
-                float x[L];
+                raw_vec<L> raw;
                 const uint32_t slot = e.y + __popc(e.x & below);
-                vec_load<L>::load(val + (std::size_t) r * ell_cols + (std::size_t) slot * block_size + lane_off, x);
+                load_raw<L>(val + (std::size_t) chunk_rows_smem[i + u].x * ell_cols + (std::size_t) slot * block_size +
+                                lane_off,
+                            raw);
+                float x[L];
+                unpack<L>(raw, x);
 #pragma unroll
                 for (int j = 0; j < L; ++j) {
                     if (COMP) {
@@ -409,17 +434,17 @@ __global__ void __launch_bounds__(kAccThreads) moments_accumulate_kernel(
                 }
             }
         }
-        const std::size_t f0 = (std::size_t) b * block_size + lane_off;
-        float *p = partials + (std::size_t) c * 4u * cols;
+    }
+    const std::size_t f0 = (std::size_t) b * block_size + lane_off;
+    float *p = partials + (std::size_t) c * 4u * cols;
 #pragma unroll
-        for (int j = 0; j < L; ++j) {
-            const std::size_t f = f0 + j;
-            if (f < cols) {
-                p[f] = s_hi[j];
-                p[cols + f] = s_lo[j];
-                p[2u * (std::size_t) cols + f] = q_hi[j];
-                p[3u * (std::size_t) cols + f] = q_lo[j];
-            }
+    for (int j = 0; j < L; ++j) {
+        const std::size_t f = f0 + j;
+        if (f < cols) {
+            p[f] = s_hi[j];
+            p[cols + f] = s_lo[j];
+            p[2u * (std::size_t) cols + f] = q_hi[j];
+            p[3u * (std::size_t) cols + f] = q_lo[j];
         }
     }
 }

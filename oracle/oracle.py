@@ -260,7 +260,16 @@ def ref_available() -> bool:
 def ref() -> C.CDLL:
     global _r
     if _r is None:
-        _r = C.CDLL(str(REF_LIB))
+        r = C.CDLL(str(REF_LIB))
+        r.csref_free.argtypes = [vp]
+        r.csref_free.restype = None
+        for name in ("csref_blocked_ell_from_compressed", "csref_sliced_ell_from_compressed"):
+            getattr(r, name).argtypes = [vp, C.c_uint, vp]
+        for name in ("csref_choose_blocked_ell_block_size", "csref_choose_sliced_ell_slice_rows_from_compressed"):
+            getattr(r, name).argtypes = [vp, vp, C.c_uint, vp]
+        r.csref_sliced_total_slots.argtypes = [vp]
+        r.csref_sliced_total_slots.restype = u32
+        _r = r
     return _r
 
 
@@ -340,7 +349,16 @@ def ref_gpu_available() -> bool:
 def ref_gpu() -> C.CDLL:
     global _rg
     if _rg is None:
-        _rg = C.CDLL(str(REF_GPU_LIB))
+        g = C.CDLL(str(REF_GPU_LIB))
+        for name in ("csrefgpu_group_reduce_blocked_ell", "csrefgpu_group_reduce_sliced_ell",
+                     "csrefgpu_group_reduce_compressed"):
+            getattr(g, name).argtypes = [vp, vp, u32, vp, vp, vp]
+        g.csrefgpu_reoptimize.argtypes = [vp, vp, u32, u32, vp, vp, vp, u32, vp]
+        g.csrefgpu_transpose.argtypes = [u32, u32, u32, vp, vp, vp, vp, vp, vp]
+        g.csrefgpu_major_nnz_plan.argtypes = [vp, u32, vp, vp, vp, vp, vp, u32]
+        g.csrefgpu_rebuild.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp]
+        g.csrefgpu_sliced_ell_from_compressed_cuda.argtypes = [vp, C.c_uint, vp]
+        _rg = g
     return _rg
 
 
