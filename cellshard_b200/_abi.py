@@ -99,6 +99,23 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_blocked_ell_from_compressed": (C.c_int, [P(HostCompressed), C.c_uint, P(HostBlockedEll)]),
     "cs_b200_choose_blocked_ell_block_size": (C.c_int, [P(HostCompressed), P(C.c_uint), C.c_uint,
                                                          P(BlockedEllTuneResult)]),
+    "cs_b200_sliced_ell_scratch_bytes": (C.c_int, [u32, u32, P(sz)]),
+    "cs_b200_sliced_ell_layout": (C.c_int, [P(CompressedView), u32, vp, vp, vp, vp, vp, sz, vp]),
+    "cs_b200_sliced_ell_emit": (C.c_int, [P(CompressedView), P(SlicedEllView), vp]),
+    "cs_b200_sliced_ell_candidates": (C.c_int, [P(CompressedView), vp, u32, vp, vp]),
+    "cs_b200_sliced_ell_from_compressed": (C.c_int, [P(HostCompressed), C.c_uint, P(HostSlicedEll)]),
+    "cs_b200_choose_sliced_ell_slice_rows_from_compressed": (C.c_int, [P(HostCompressed), P(C.c_uint), C.c_uint,
+                                                                        P(SlicedEllTuneResult)]),
+    "cs_b200_compressed_transpose_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
+    "cs_b200_build_compressed_transpose": (C.c_int, [u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "cs_b200_major_nnz_bucket_sort_scratch_bytes": (C.c_int, [u32, P(sz)]),
+    "cs_b200_major_nnz_bucket_scan_scratch_bytes": (C.c_int, [u32, P(sz)]),
+    "cs_b200_build_major_nnz_bucket_plan": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, vp, sz, vp]),
+    "cs_b200_build_shard_major_nnz_bucket_plan": (C.c_int, [vp, vp, u32, u32, vp, vp, vp, vp, vp, u32, vp, sz, vp]),
+    "cs_b200_pow2_nnz_bin_offsets": (C.c_int, [vp, u32, vp, vp]),
+    "cs_b200_rebuild_compressed_major_order": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "cs_b200_rebuild_bucketed_shard_compressed": (C.c_int, [vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp, vp, sz,
+                                                             vp]),
     "cs_b200_group_reduce_blocked_ell": (C.c_int, [P(BlockedEllView), vp, u32, P(RowFeatureMaskView),
                                                    P(GroupFilterParams), P(GroupReduceOut), vp]),
     "cs_b200_group_reduce_sliced_ell": (C.c_int, [P(SlicedEllView), vp, u32, P(RowFeatureMaskView),

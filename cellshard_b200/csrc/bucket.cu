@@ -1,0 +1,407 @@
+// Major-axis nnz bucketing.
+//
+// Plan (bucket::build_major_nnz_bucket_plan_raw, src/bucket/major_nnz_raw.cuh:64-120):
+//   major_nnz[i] = ptr[i+1] - ptr[i]; major_order_in = identity; a stable
+//   ascending sort of the counts with row ids as values (the reference runs
+//   CUB DeviceRadixSort::SortPairs over all 32 key bits) -> major_nnz_sorted,
+//   major_order_out; equal-count bucket offsets where the first n % B buckets
+//   take one extra row (fill_equal_count_bucket_offsets.cuh).
+//   Here the sort is an LSD radix sort of four 8-bit digit passes; each pass is
+//   a stable counting sort: per-tile digit histograms laid out digit-major so a
+//   single exclusive scan yields every (digit, tile) base, then an in-order
+//   ranked scatter (warp match on the digit + per-warp running counts).
+// Power-of-two bins (no reference function): bin k >= 1 holds counts in
+//   [2^k, 2^(k+1)), bin 0 holds 0 and 1; offsets are lower bounds in the sorted
+//   counts, so they are pinned by the sort.
+// Rebuild (rebuild_compressed_major_order_raw, major_nnz_raw.cuh:188-250): rows
+//   copied into sorted order with one warp per destination row.  The reference
+//   feeds counts already shifted by one slot into an exclusive scan, which
+//   yields dst_major_ptr = [0, 0, c0, c0+c1, ...] and overlapping rows; the row
+//   pointer here is the permuted CSR that rebuild is meant to produce.
+// Shard variants take per-part pointer tables and locate a row's part by
+// binary search over the part row offsets (find_offset_span semantics,
+// include/CellShard/core/offset_span.cuh:12-24).
+#include "common.cuh"
+
+namespace csb {
+namespace {
+
+constexpr unsigned kSortThreads = 256;
+constexpr unsigned kSortWarps = kSortThreads / 32;
+constexpr unsigned kTileKeys = 2048; // 8 warps x 256 keys
+constexpr unsigned kKeysPerWarp = kTileKeys / kSortWarps;
+constexpr unsigned kRadix = 256;
+
+__device__ __forceinline__ uint32_t find_part(uint32_t row, const uint32_t *offsets, uint32_t count) {
+    uint32_t lo = 0u, hi = count;
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (row < offsets[mid])
+            hi = mid;
+        else if (row >= offsets[mid + 1u])
+            lo = mid + 1u;
+        else
+            return mid;
+    }
+    return count;
+}
+
+// counts + identity; `parts` == nullptr for a single matrix
+__global__ void count_kernel(uint32_t n, const uint32_t *__restrict__ ptr, const uint32_t *const *__restrict__ parts,
+                             const uint32_t *__restrict__ part_offsets, uint32_t part_count,
+                             uint32_t *__restrict__ nnz, uint32_t *__restrict__ order_in) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t c;
+        if (parts == nullptr) {
+            c = ptr[i + 1u] - ptr[i];
+        } else {
+            const uint32_t p = find_part(i, part_offsets, part_count);
+            const uint32_t *pp = parts[p];
+            const uint32_t local = i - part_offsets[p];
+            c = pp[local + 1u] - pp[local];
+        }
+        nnz[i] = c;
+        order_in[i] = i;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t *__restrict__ keys, uint32_t n,
+                                                                  uint32_t shift, uint32_t tiles,
+                                                                  uint32_t *__restrict__ hist) {
+    __shared__ uint32_t h[kRadix];
+    h[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kTileKeys;
+    for (uint32_t i = threadIdx.x; i < kTileKeys; i += blockDim.x) {
+        const uint32_t k = base + i;
+        if (k < n) atomicAdd(h + ((keys[k] >> shift) & 0xffu), 1u);
+    }
+    __syncthreads();
+    hist[(std::size_t) threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint32_t *__restrict__ keys,
+                                                                     const uint32_t *__restrict__ vals, uint32_t n,
+                                                                     uint32_t shift, uint32_t tiles,
+                                                                     const uint32_t *__restrict__ base,
+                                                                     uint32_t *__restrict__ out_keys,
+                                                                     uint32_t *__restrict__ out_vals) {
+    __shared__ uint32_t wc[kSortWarps][kRadix];
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    for (uint32_t d = lane; d < kRadix; d += 32u) wc[warp][d] = 0u;
+    __syncwarp();
+    const uint32_t wbase = blockIdx.x * kTileKeys + warp * kKeysPerWarp;
+    for (uint32_t b = 0; b < kKeysPerWarp; b += 32u) {
+        const uint32_t k = wbase + b + lane;
+        const uint32_t d = k < n ? (keys[k] >> shift) & 0xffu : kRadix;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (d < kRadix && lane == (unsigned) (__ffs(peers) - 1)) wc[warp][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const uint32_t d = threadIdx.x; // kSortThreads == kRadix
+        uint32_t run = base[(std::size_t) d * tiles + blockIdx.x];
+        for (unsigned w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = wc[w][d];
+            wc[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    for (uint32_t b = 0; b < kKeysPerWarp; b += 32u) {
+        const uint32_t k = wbase + b + lane;
+        const uint32_t key = k < n ? keys[k] : 0u;
+        const uint32_t d = k < n ? (key >> shift) & 0xffu : kRadix;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t pos = 0u;
+        if (d < kRadix) pos = wc[warp][d] + __popc(peers & lt);
+        __syncwarp();
+        if (d < kRadix) {
+            out_keys[pos] = key;
+            out_vals[pos] = vals[k];
+            if (lane == (unsigned) (__ffs(peers) - 1)) wc[warp][d] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void equal_count_offsets_kernel(uint32_t n, uint32_t buckets, uint32_t *__restrict__ offsets) {
+    const uint32_t size = n / buckets, rem = n % buckets;
+    for (uint32_t b = threadIdx.x; b <= buckets; b += blockDim.x)
+        offsets[b] = b == buckets ? n : b * size + min(b, rem);
+}
+
+__global__ void pow2_bins_kernel(const uint32_t *__restrict__ sorted, uint32_t n, uint32_t *__restrict__ bins) {
+    const uint32_t k = threadIdx.x;
+    if (k > 33u) return;
+    if (k == 0u) {
+        bins[0] = 0u;
+        return;
+    }
+    if (k == 33u) {
+        bins[33] = n;
+        return;
+    }
+    const unsigned long long bound = 1ull << k;
+    uint32_t lo = 0u, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if ((unsigned long long) sorted[mid] < bound)
+            lo = mid + 1u;
+        else
+            hi = mid;
+    }
+    bins[k] = lo;
+}
+
+// dst counts in order (single matrix or shard)
+__global__ void gather_counts_kernel(uint32_t n, const uint32_t *__restrict__ order, const uint32_t *__restrict__ ptr,
+                                     const uint32_t *const *__restrict__ parts,
+                                     const uint32_t *__restrict__ part_offsets, uint32_t part_count,
+                                     uint32_t *__restrict__ counts, uint32_t *__restrict__ inverse) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = order[i];
+        uint32_t c;
+        if (parts == nullptr) {
+            c = ptr[s + 1u] - ptr[s];
+        } else {
+            const uint32_t p = find_part(s, part_offsets, part_count);
+            const uint32_t local = s - part_offsets[p];
+            c = parts[p][local + 1u] - parts[p][local];
+        }
+        counts[i] = c;
+        if (inverse != nullptr) inverse[s] = i;
+    }
+}
+
+__global__ void __launch_bounds__(256) segment_copy_kernel(uint32_t n, const uint32_t *__restrict__ order,
+                                                           const uint32_t *__restrict__ ptr,
+                                                           const uint32_t *__restrict__ idx,
+                                                           const uint16_t *__restrict__ val,
+                                                           const uint32_t *const *__restrict__ part_ptr,
+                                                           const uint32_t *const *__restrict__ part_idx,
+                                                           const uint16_t *const *__restrict__ part_val,
+                                                           const uint32_t *__restrict__ part_offsets,
+                                                           uint32_t part_count, const uint32_t *__restrict__ dst_ptr,
+                                                           uint32_t *__restrict__ dst_idx,
+                                                           uint16_t *__restrict__ dst_val) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint32_t i = blockIdx.x * 8u + (threadIdx.x >> 5); i < n; i += gridDim.x * 8u) {
+        const uint32_t s = order[i];
+        const uint32_t *sp = ptr;
+        const uint32_t *si = idx;
+        const uint16_t *sv = val;
+        uint32_t local = s;
+        if (part_ptr != nullptr) {
+            const uint32_t p = find_part(s, part_offsets, part_count);
+            local = s - part_offsets[p];
+            sp = part_ptr[p];
+            si = part_idx[p];
+            sv = part_val[p];
+        }
+        const uint32_t a = sp[local];
+        const uint32_t len = sp[local + 1u] - a;
+        const uint32_t d = dst_ptr[i];
+        for (uint32_t j = lane; j < len; j += 32u) {
+            dst_idx[d + j] = si[a + j];
+            dst_val[d + j] = sv[a + j];
+        }
+    }
+}
+
+unsigned grid1d(uint32_t n, uint32_t threads) {
+    uint32_t g = (n + threads - 1u) / threads;
+    const uint32_t cap = (uint32_t) sm_count() * 16u;
+    if (g > cap) g = cap;
+    return g == 0u ? 1u : g;
+}
+
+uint32_t clamp_buckets(uint32_t n, uint32_t requested) {
+    if (n == 0u) return 1u;
+    if (requested < 1u) return 1u;
+    return requested > n ? n : requested;
+}
+
+struct sort_layout {
+    uint32_t *tmp_keys, *tmp_vals, *hist;
+    void *scan_tmp;
+    std::size_t scan_bytes, bytes;
+    uint32_t tiles;
+};
+
+void make_sort_layout(uint32_t n, void *base, std::size_t cap, sort_layout *l) {
+    l->tiles = (n + kTileKeys - 1u) / kTileKeys;
+    scratch_carver c(base, cap);
+    l->tmp_keys = c.take<uint32_t>((std::size_t) n + 1u);
+    l->tmp_vals = c.take<uint32_t>((std::size_t) n + 1u);
+    l->hist = c.take<uint32_t>((std::size_t) l->tiles * kRadix + 1u);
+    l->scan_bytes = scan_u32_scratch_bytes((std::size_t) l->tiles * kRadix);
+    l->scan_tmp = c.take<char>(l->scan_bytes);
+    l->bytes = c.used;
+}
+
+// Stable ascending sort of keys (with values) into out_keys / out_vals.
+int radix_sort_pairs(const uint32_t *keys, const uint32_t *vals, uint32_t n, uint32_t *out_keys, uint32_t *out_vals,
+                     const sort_layout &l, cudaStream_t stream) {
+    const uint32_t *ik = keys, *iv = vals;
+    for (int pass = 0; pass < 4; ++pass) {
+        uint32_t *ok = (pass % 2 == 0) ? l.tmp_keys : out_keys;
+        uint32_t *ov = (pass % 2 == 0) ? l.tmp_vals : out_vals;
+        const uint32_t shift = 8u * (uint32_t) pass;
+        radix_hist_kernel<<<l.tiles, kSortThreads, 0, stream>>>(ik, n, shift, l.tiles, l.hist);
+        if (!launch_ok("radix_hist_kernel")) return 0;
+        if (!scan_exclusive_u32(l.hist, l.hist, (std::size_t) l.tiles * kRadix, false, l.scan_tmp, l.scan_bytes,
+                                stream))
+            return 0;
+        radix_scatter_kernel<<<l.tiles, kSortThreads, 0, stream>>>(ik, iv, n, shift, l.tiles, l.hist, ok, ov);
+        if (!launch_ok("radix_scatter_kernel")) return 0;
+        ik = ok;
+        iv = ov;
+    }
+    return 1;
+}
+
+int plan_common(uint32_t n, const uint32_t *ptr, const uint32_t *const *parts, const uint32_t *part_offsets,
+                uint32_t part_count, uint32_t *d_nnz, uint32_t *d_sorted, uint32_t *d_order_in, uint32_t *d_order_out,
+                uint32_t *d_offsets, uint32_t requested, void *tmp, std::size_t tmp_bytes, cudaStream_t stream) {
+    if (n == 0u) {
+        if (d_offsets != nullptr) return cuda_ok(cudaMemsetAsync(d_offsets, 0, 4, stream), "empty bucket offsets");
+        return 1;
+    }
+    sort_layout l;
+    make_sort_layout(n, tmp, tmp_bytes, &l);
+    if (tmp == nullptr || l.bytes > tmp_bytes) {
+        set_error("major_nnz_bucket_plan: sort scratch %zu < %zu bytes", tmp_bytes, l.bytes);
+        return 0;
+    }
+    count_kernel<<<grid1d(n, 256), 256, 0, stream>>>(n, ptr, parts, part_offsets, part_count, d_nnz, d_order_in);
+    if (!launch_ok("count_kernel")) return 0;
+    if (!radix_sort_pairs(d_nnz, d_order_in, n, d_sorted, d_order_out, l, stream)) return 0;
+    if (d_offsets != nullptr) {
+        equal_count_offsets_kernel<<<1, 256, 0, stream>>>(n, clamp_buckets(n, requested), d_offsets);
+        if (!launch_ok("equal_count_offsets_kernel")) return 0;
+    }
+    return 1;
+}
+
+int rebuild_common(uint32_t n, const uint32_t *order, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
+                   const uint32_t *const *pp, const uint32_t *const *pi, const uint16_t *const *pv,
+                   const uint32_t *part_offsets, uint32_t part_count, uint32_t *dst_ptr, uint32_t *dst_idx,
+                   uint16_t *dst_val, uint32_t *inverse, void *tmp, std::size_t tmp_bytes, cudaStream_t stream) {
+    if (n == 0u) return 1;
+    if (tmp == nullptr || tmp_bytes < scan_u32_scratch_bytes(n)) {
+        set_error("rebuild: scan scratch %zu < %zu bytes", tmp_bytes, scan_u32_scratch_bytes(n));
+        return 0;
+    }
+    gather_counts_kernel<<<grid1d(n, 256), 256, 0, stream>>>(n, order, ptr, pp, part_offsets, part_count, dst_ptr,
+                                                             inverse);
+    if (!launch_ok("gather_counts_kernel")) return 0;
+    if (!scan_exclusive_u32(dst_ptr, dst_ptr, n, true, tmp, tmp_bytes, stream)) return 0;
+    segment_copy_kernel<<<grid1d(n, 8), 256, 0, stream>>>(n, order, ptr, idx, val, pp, pi, pv, part_offsets,
+                                                          part_count, dst_ptr, dst_idx, dst_val);
+    return launch_ok("segment_copy_kernel");
+}
+
+} // namespace
+} // namespace csb
+
+using namespace csb;
+
+extern "C" int cs_b200_major_nnz_bucket_sort_scratch_bytes(uint32_t major_dim, size_t *out_bytes) {
+    if (out_bytes == nullptr) {
+        set_error("sort_scratch_bytes: null output");
+        return 0;
+    }
+    sort_layout l;
+    make_sort_layout(major_dim, nullptr, 0, &l);
+    *out_bytes = l.bytes;
+    return 1;
+}
+
+extern "C" int cs_b200_major_nnz_bucket_scan_scratch_bytes(uint32_t major_dim, size_t *out_bytes) {
+    if (out_bytes == nullptr) {
+        set_error("scan_scratch_bytes: null output");
+        return 0;
+    }
+    *out_bytes = scan_u32_scratch_bytes(major_dim);
+    return 1;
+}
+
+extern "C" int cs_b200_build_major_nnz_bucket_plan(const uint32_t *d_major_ptr, uint32_t major_dim,
+                                                   uint32_t *d_major_nnz, uint32_t *d_major_nnz_sorted,
+                                                   uint32_t *d_major_order_in, uint32_t *d_major_order_out,
+                                                   uint32_t *d_bucket_offsets, uint32_t requested_bucket_count,
+                                                   void *d_sort_tmp, size_t sort_tmp_bytes, cs_stream_t s) {
+    if (d_major_ptr == nullptr || d_major_nnz == nullptr || d_major_nnz_sorted == nullptr ||
+        d_major_order_in == nullptr || d_major_order_out == nullptr) {
+        set_error("build_major_nnz_bucket_plan: null device array");
+        return 0;
+    }
+    return plan_common(major_dim, d_major_ptr, nullptr, nullptr, 0u, d_major_nnz, d_major_nnz_sorted, d_major_order_in,
+                       d_major_order_out, d_bucket_offsets, requested_bucket_count, d_sort_tmp, sort_tmp_bytes,
+                       as_stream(s));
+}
+
+extern "C" int cs_b200_build_shard_major_nnz_bucket_plan(const uint32_t *const *d_part_major_ptr,
+                                                         const uint32_t *d_part_row_offsets, uint32_t part_count,
+                                                         uint32_t shard_rows, uint32_t *d_major_nnz,
+                                                         uint32_t *d_major_nnz_sorted, uint32_t *d_major_order_in,
+                                                         uint32_t *d_major_order_out, uint32_t *d_bucket_offsets,
+                                                         uint32_t requested_bucket_count, void *d_sort_tmp,
+                                                         size_t sort_tmp_bytes, cs_stream_t s) {
+    if (d_part_major_ptr == nullptr || d_part_row_offsets == nullptr || d_major_nnz == nullptr ||
+        d_major_nnz_sorted == nullptr || d_major_order_in == nullptr || d_major_order_out == nullptr) {
+        set_error("build_shard_major_nnz_bucket_plan: null device array");
+        return 0;
+    }
+    return plan_common(shard_rows, nullptr, d_part_major_ptr, d_part_row_offsets, part_count, d_major_nnz,
+                       d_major_nnz_sorted, d_major_order_in, d_major_order_out, d_bucket_offsets,
+                       requested_bucket_count, d_sort_tmp, sort_tmp_bytes, as_stream(s));
+}
+
+extern "C" int cs_b200_pow2_nnz_bin_offsets(const uint32_t *d_major_nnz_sorted, uint32_t major_dim,
+                                            uint32_t *d_bin_offsets, cs_stream_t s) {
+    if (d_bin_offsets == nullptr || (major_dim != 0u && d_major_nnz_sorted == nullptr)) {
+        set_error("pow2_nnz_bin_offsets: null device array");
+        return 0;
+    }
+    pow2_bins_kernel<<<1, 64, 0, as_stream(s)>>>(d_major_nnz_sorted, major_dim, d_bin_offsets);
+    return launch_ok("pow2_bins_kernel");
+}
+
+extern "C" int cs_b200_rebuild_compressed_major_order(const uint32_t *d_src_major_ptr, const uint32_t *d_src_minor_idx,
+                                                      const uint16_t *d_src_val, uint32_t major_dim,
+                                                      const uint32_t *d_major_order, uint32_t *d_dst_major_ptr,
+                                                      uint32_t *d_dst_minor_idx, uint16_t *d_dst_val,
+                                                      uint32_t *d_inverse_major_order, void *d_scan_tmp,
+                                                      size_t scan_tmp_bytes, cs_stream_t s) {
+    if (d_src_major_ptr == nullptr || d_src_minor_idx == nullptr || d_src_val == nullptr || d_major_order == nullptr ||
+        d_dst_major_ptr == nullptr || d_dst_minor_idx == nullptr || d_dst_val == nullptr) {
+        set_error("rebuild_compressed_major_order: null device array");
+        return 0;
+    }
+    return rebuild_common(major_dim, d_major_order, d_src_major_ptr, d_src_minor_idx, d_src_val, nullptr, nullptr,
+                          nullptr, nullptr, 0u, d_dst_major_ptr, d_dst_minor_idx, d_dst_val, d_inverse_major_order,
+                          d_scan_tmp, scan_tmp_bytes, as_stream(s));
+}
+
+extern "C" int cs_b200_rebuild_bucketed_shard_compressed(const uint32_t *const *d_part_major_ptr,
+                                                         const uint32_t *const *d_part_minor_idx,
+                                                         const uint16_t *const *d_part_val,
+                                                         const uint32_t *d_part_row_offsets, uint32_t part_count,
+                                                         uint32_t shard_rows, const uint32_t *d_major_order,
+                                                         uint32_t *d_dst_major_ptr, uint32_t *d_dst_minor_idx,
+                                                         uint16_t *d_dst_val, uint32_t *d_inverse_major_order,
+                                                         void *d_scan_tmp, size_t scan_tmp_bytes, cs_stream_t s) {
+    if (d_part_major_ptr == nullptr || d_part_minor_idx == nullptr || d_part_val == nullptr ||
+        d_part_row_offsets == nullptr || d_major_order == nullptr || d_dst_major_ptr == nullptr ||
+        d_dst_minor_idx == nullptr || d_dst_val == nullptr) {
+        set_error("rebuild_bucketed_shard_compressed: null device array");
+        return 0;
+    }
+    return rebuild_common(shard_rows, d_major_order, nullptr, nullptr, nullptr, d_part_major_ptr, d_part_minor_idx,
+                          d_part_val, d_part_row_offsets, part_count, d_dst_major_ptr, d_dst_minor_idx, d_dst_val,
+                          d_inverse_major_order, d_scan_tmp, scan_tmp_bytes, as_stream(s));
+}

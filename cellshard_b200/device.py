@@ -152,3 +152,90 @@ def blocked_ell_from_csr(csr: CSR, block_size: int, stream=None, check_status: b
         if st:
             raise _abi.CellShardError(f"blocked_ell conversion flagged invalid input (status 0x{st:x})")
     return out
+
+
+def sliced_ell_from_csr(csr: CSR, slice_rows: int, stream=None) -> SlicedELL:
+    """Device CSR -> device Sliced-ELL (convert::sliced_ell_from_compressed on the GPU).
+    Synchronises once to size the slot arrays."""
+    lib = _abi.load()
+    rows = csr.rows
+    h = max(1, min(slice_rows, rows)) if rows else 0
+    S = (rows + h - 1) // h if rows else 0
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_sliced_ell_scratch_bytes(rows, slice_rows, C.byref(nbytes)), "sliced scratch")
+    scratch = _scratch(nbytes.value)
+    offs = torch.empty(S + 1, dtype=torch.int32, device="cuda")
+    widths = torch.empty(max(S, 1), dtype=torch.int32, device="cuda")
+    slots = torch.empty(max(S, 1), dtype=torch.int32, device="cuda")
+    total = torch.zeros(1, dtype=torch.int64, device="cuda")
+    v = csr.view()
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_sliced_ell_layout(C.byref(v), slice_rows, ptr(offs), ptr(widths), ptr(slots), ptr(total),
+                                             ptr(scratch), nbytes.value, s), "sliced_ell_layout")
+    n_slots = int(total.item())
+    out = SlicedELL(rows, csr.cols, csr.nnz, h, offs, widths[:S], slots[:S],
+                    torch.empty(n_slots, dtype=torch.int32, device="cuda"),
+                    torch.empty(n_slots, dtype=torch.float16, device="cuda"))
+    dv = out.view()
+    _abi.check(lib.cs_b200_sliced_ell_emit(C.byref(v), C.byref(dv), s), "sliced_ell_emit")
+    return out
+
+
+def transpose(csr: CSR, stream=None, check_status: bool = True) -> CSR:
+    """build_compressed_transpose_raw on the GPU: a (cDim x uDim) compressed matrix ->
+    its (uDim x cDim) transpose, minor indices ascending in each major segment."""
+    lib = _abi.load()
+    cdim = csr.rows if csr.axis == COMPRESSED_BY_ROW else csr.cols
+    udim = csr.cols if csr.axis == COMPRESSED_BY_ROW else csr.rows
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_compressed_transpose_scratch_bytes(cdim, udim, csr.nnz, C.byref(nbytes)), "scratch")
+    scratch = _scratch(nbytes.value)
+    optr = torch.empty(udim + 1, dtype=torch.int32, device="cuda")
+    oidx = torch.empty(csr.nnz, dtype=torch.int32, device="cuda")
+    oval = torch.empty(csr.nnz, dtype=torch.float16, device="cuda")
+    _abi.check(lib.cs_b200_build_compressed_transpose(cdim, udim, csr.nnz, ptr(csr.ptr), ptr(csr.idx), ptr(csr.val),
+                                                      ptr(optr), None, ptr(oidx), ptr(oval), ptr(scratch),
+                                                      nbytes.value, stream_handle(stream)), "compressed_transpose")
+    if check_status:
+        st = int(scratch[:4].view(torch.int32).item())
+        if st:
+            raise _abi.CellShardError(f"transpose flagged invalid input (status 0x{st:x})")
+    axis = COMPRESSED_BY_COL if csr.axis == COMPRESSED_BY_ROW else COMPRESSED_BY_ROW
+    return CSR(csr.rows, csr.cols, optr, oidx, oval, axis)
+
+
+def major_nnz_plan(major_ptr: torch.Tensor, major_dim: int, buckets: int, stream=None) -> dict:
+    """bucket::build_major_nnz_bucket_plan_raw on the GPU plus power-of-two bins."""
+    lib = _abi.load()
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_major_nnz_bucket_sort_scratch_bytes(major_dim, C.byref(nbytes)), "sort scratch")
+    scratch = _scratch(nbytes.value)
+    n = max(major_dim, 1)
+    out = {k: torch.empty(n, dtype=torch.int32, device="cuda") for k in ("nnz", "sorted", "order_in", "order")}
+    nb = 1 if major_dim == 0 else min(max(buckets, 1), major_dim)
+    out["bucket_offsets"] = torch.empty(nb + 1, dtype=torch.int32, device="cuda")
+    out["pow2_bins"] = torch.empty(34, dtype=torch.int32, device="cuda")
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_build_major_nnz_bucket_plan(ptr(major_ptr), major_dim, ptr(out["nnz"]), ptr(out["sorted"]),
+                                                       ptr(out["order_in"]), ptr(out["order"]),
+                                                       ptr(out["bucket_offsets"]), buckets, ptr(scratch),
+                                                       nbytes.value, s), "major_nnz_bucket_plan")
+    _abi.check(lib.cs_b200_pow2_nnz_bin_offsets(ptr(out["sorted"]), major_dim, ptr(out["pow2_bins"]), s), "pow2 bins")
+    return out
+
+
+def rebuild_major_order(csr: CSR, order: torch.Tensor, stream=None):
+    """bucket::rebuild_compressed_major_order_raw on the GPU; returns (CSR, inverse)."""
+    lib = _abi.load()
+    n = csr.rows if csr.axis == COMPRESSED_BY_ROW else csr.cols
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_major_nnz_bucket_scan_scratch_bytes(n, C.byref(nbytes)), "scan scratch")
+    scratch = _scratch(nbytes.value)
+    dptr = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    didx = torch.empty(csr.nnz, dtype=torch.int32, device="cuda")
+    dval = torch.empty(csr.nnz, dtype=torch.float16, device="cuda")
+    inv = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    _abi.check(lib.cs_b200_rebuild_compressed_major_order(ptr(csr.ptr), ptr(csr.idx), ptr(csr.val), n, ptr(order),
+                                                          ptr(dptr), ptr(didx), ptr(dval), ptr(inv), ptr(scratch),
+                                                          nbytes.value, stream_handle(stream)), "rebuild")
+    return CSR(csr.rows, csr.cols, dptr, didx, dval, csr.axis), inv

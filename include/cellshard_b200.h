@@ -207,6 +207,165 @@ CS_API int cs_b200_choose_blocked_ell_block_size(const cs_host_compressed *src,
                                           cs_blocked_ell_tune_result *out);
 
 /* ------------------------------------------------------------------------ */
+/* CSR -> Sliced-ELL                                                          */
+/* replaces convert::sliced_ell_from_compressed[_cuda] and                    */
+/* choose_sliced_ell_slice_rows[_from_compressed] (src/convert/                */
+/* sliced_ell_from_compressed.cuh:20-45,86-254; sliced_ell_from_blocked_ell.cuh:*/
+/* 64-142,196-221), whose layout the reference computes on the host.          */
+/* ------------------------------------------------------------------------ */
+
+CS_API int cs_b200_sliced_ell_scratch_bytes(uint32_t rows, uint32_t slice_rows, size_t *out_bytes);
+
+/* Layout pass for uniform slices of clamp(slice_rows, 1, rows) rows:
+ * d_slice_row_offsets[S+1], d_slice_widths[S] (max row nnz of the slice),
+ * d_slice_slot_offsets[S] (u32 running sum of rows_in_slice * width), and
+ * d_total_slots[0] (u64, exact).  S = ceil(rows / clamp(slice_rows)). */
+CS_API int cs_b200_sliced_ell_layout(const cs_compressed_view *src,
+                                     uint32_t slice_rows,
+                                     uint32_t *d_slice_row_offsets,
+                                     uint32_t *d_slice_widths,
+                                     uint32_t *d_slice_slot_offsets,
+                                     uint64_t *d_total_slots,
+                                     void *d_scratch,
+                                     size_t scratch_bytes,
+                                     cs_stream_t stream);
+
+/* Emit pass: each row's entries in its first slots, CS_INVALID_COL / 0
+ * padding after them.  dst carries the layout and uniform slice_rows. */
+CS_API int cs_b200_sliced_ell_emit(const cs_compressed_view *src, const cs_sliced_ell_view *dst, cs_stream_t stream);
+
+/* d_padded_slots[k] <- sum over slices of rows_in_slice * max row nnz for
+ * candidate height candidates[k] (clamped to [1, rows]); at most 16. */
+CS_API int cs_b200_sliced_ell_candidates(const cs_compressed_view *src,
+                                         const uint32_t *candidates,
+                                         uint32_t count,
+                                         uint64_t *d_padded_slots,
+                                         cs_stream_t stream);
+
+/* Host convenience with the reference's signature and results:
+ * convert::sliced_ell_from_compressed(src, slice_rows, dst), CSR or CSC
+ * input.  Synchronous. */
+CS_API int cs_b200_sliced_ell_from_compressed(const cs_host_compressed *src,
+                                              unsigned int slice_rows,
+                                              cs_host_sliced_ell *dst);
+
+/* convert::choose_sliced_ell_slice_rows_from_compressed: same score,
+ * penalty and tie-breaking in host doubles, padded slots from the GPU. */
+CS_API int cs_b200_choose_sliced_ell_slice_rows_from_compressed(const cs_host_compressed *src,
+                                                                const unsigned int *candidates,
+                                                                unsigned int candidate_count,
+                                                                cs_sliced_ell_tune_result *out);
+
+/* ------------------------------------------------------------------------ */
+/* Compressed transpose                                                       */
+/* replaces convert::build_compressed_transpose_raw (src/convert/             */
+/* compressed_transpose_raw.cuh:14-123), same arguments.  The output equals   */
+/* the reference's cuSPARSE csr2cscEx2 path: row indices ascending inside     */
+/* each column; deterministic.  d_heads is accepted and unused.  Scratch word */
+/* 0 receives CS_STATUS bits (a row repeating a column sets                   */
+/* CS_STATUS_DUPLICATE_COL; such input has no defined transpose here).        */
+/* ------------------------------------------------------------------------ */
+
+CS_API int cs_b200_compressed_transpose_scratch_bytes(uint32_t cDim, uint32_t uDim, uint32_t nnz, size_t *out_bytes);
+
+CS_API int cs_b200_build_compressed_transpose(uint32_t cDim,
+                                              uint32_t uDim,
+                                              uint32_t nnz,
+                                              const uint32_t *d_cAxPtr,
+                                              const uint32_t *d_uAxIdx,
+                                              const uint16_t *d_val,
+                                              uint32_t *d_out_uAxPtr,
+                                              uint32_t *d_heads,
+                                              uint32_t *d_out_cAxIdx,
+                                              uint16_t *d_out_val,
+                                              void *d_scan_tmp,
+                                              size_t scan_bytes,
+                                              cs_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Major-axis nnz bucketing                                                   */
+/* replaces bucket::build_major_nnz_bucket_plan_raw,                          */
+/* build_shard_major_nnz_bucket_plan_raw, rebuild_compressed_major_order_raw, */
+/* rebuild_bucketed_shard_compressed_raw and their scratch queries            */
+/* (src/bucket/major_nnz_raw.cuh:34-320), same arguments.                     */
+/* ------------------------------------------------------------------------ */
+
+CS_API int cs_b200_major_nnz_bucket_sort_scratch_bytes(uint32_t major_dim, size_t *out_bytes);
+CS_API int cs_b200_major_nnz_bucket_scan_scratch_bytes(uint32_t major_dim, size_t *out_bytes);
+
+/* d_major_nnz[i] = ptr[i+1]-ptr[i]; d_major_order_in = identity;
+ * d_major_nnz_sorted / d_major_order_out = stable ascending sort of the
+ * counts; d_bucket_offsets (nullable) = clamp(requested, 1, major_dim) + 1
+ * equal-count offsets, the first major_dim % B buckets one row larger. */
+CS_API int cs_b200_build_major_nnz_bucket_plan(const uint32_t *d_major_ptr,
+                                               uint32_t major_dim,
+                                               uint32_t *d_major_nnz,
+                                               uint32_t *d_major_nnz_sorted,
+                                               uint32_t *d_major_order_in,
+                                               uint32_t *d_major_order_out,
+                                               uint32_t *d_bucket_offsets,
+                                               uint32_t requested_bucket_count,
+                                               void *d_sort_tmp,
+                                               size_t sort_tmp_bytes,
+                                               cs_stream_t stream);
+
+/* The same over many parts: row r of the shard is local row
+ * r - d_part_row_offsets[p] of part p (d_part_row_offsets[part_count+1]). */
+CS_API int cs_b200_build_shard_major_nnz_bucket_plan(const uint32_t *const *d_part_major_ptr,
+                                                     const uint32_t *d_part_row_offsets,
+                                                     uint32_t part_count,
+                                                     uint32_t shard_rows,
+                                                     uint32_t *d_major_nnz,
+                                                     uint32_t *d_major_nnz_sorted,
+                                                     uint32_t *d_major_order_in,
+                                                     uint32_t *d_major_order_out,
+                                                     uint32_t *d_bucket_offsets,
+                                                     uint32_t requested_bucket_count,
+                                                     void *d_sort_tmp,
+                                                     size_t sort_tmp_bytes,
+                                                     cs_stream_t stream);
+
+/* Power-of-two nnz bins over a sorted count array (no reference function):
+ * d_bin_offsets[34]; bin k in [0, 32] is [d_bin_offsets[k], d_bin_offsets[k+1]),
+ * holding counts in [2^k, 2^(k+1)) for k >= 1 and in [0, 2) for k = 0. */
+CS_API int cs_b200_pow2_nnz_bin_offsets(const uint32_t *d_major_nnz_sorted,
+                                        uint32_t major_dim,
+                                        uint32_t *d_bin_offsets,
+                                        cs_stream_t stream);
+
+/* Rows permuted into plan order: d_dst_major_ptr[major_dim+1] is the
+ * exclusive scan of the counts in plan order (the reference scans counts it
+ * has already shifted by one slot, giving [0, 0, c0, ...]; this returns the
+ * permuted CSR the function is documented to build); d_inverse (nullable). */
+CS_API int cs_b200_rebuild_compressed_major_order(const uint32_t *d_src_major_ptr,
+                                                  const uint32_t *d_src_minor_idx,
+                                                  const uint16_t *d_src_val,
+                                                  uint32_t major_dim,
+                                                  const uint32_t *d_major_order,
+                                                  uint32_t *d_dst_major_ptr,
+                                                  uint32_t *d_dst_minor_idx,
+                                                  uint16_t *d_dst_val,
+                                                  uint32_t *d_inverse_major_order,
+                                                  void *d_scan_tmp,
+                                                  size_t scan_tmp_bytes,
+                                                  cs_stream_t stream);
+
+CS_API int cs_b200_rebuild_bucketed_shard_compressed(const uint32_t *const *d_part_major_ptr,
+                                                     const uint32_t *const *d_part_minor_idx,
+                                                     const uint16_t *const *d_part_val,
+                                                     const uint32_t *d_part_row_offsets,
+                                                     uint32_t part_count,
+                                                     uint32_t shard_rows,
+                                                     const uint32_t *d_major_order,
+                                                     uint32_t *d_dst_major_ptr,
+                                                     uint32_t *d_dst_minor_idx,
+                                                     uint16_t *d_dst_val,
+                                                     uint32_t *d_inverse_major_order,
+                                                     void *d_scan_tmp,
+                                                     size_t scan_tmp_bytes,
+                                                     cs_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* mask_groups: masked per-row feature-group reduction                        */
 /* replaces runtime::compute_sparse_group_reduce (mask_groups.cuh:185-204,     */
 /* mask_groups.cu:811-918)                                                    */
