@@ -129,6 +129,8 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_group_moments_scratch_bytes": (C.c_int, [P(BlockedEllView), P(GroupMomentsParams), P(sz)]),
     "cs_b200_group_moments_blocked_ell": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
                                                     P(GroupMomentsOut), vp, sz, vp]),
+    "cs_b200_group_moments_blocked_ell_noalloc": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
+                                                            P(GroupMomentsOut), vp]),
     "cs_b200_group_moments_phases": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
                                                P(GroupMomentsOut), vp, sz, u32, vp]),
     "cs_b200_synth_csr": (C.c_int, [u32, u32, vp, vp, vp, vp, u32, vp, u64, vp, vp, vp]),

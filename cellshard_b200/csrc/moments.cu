@@ -684,6 +684,28 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
     return 1;
 }
 
+namespace csb {
+
+// Scratch bytes the moments reduction needs for (src, params); 0 when the
+// arguments are invalid (the error message is set).
+std::size_t group_moments_scratch_needed(const cs_blocked_ell_view *src, const cs_group_moments_params *params) {
+    if (!validate(src, params)) return 0;
+    moments_layout lay;
+    make_layout(src, params, nullptr, 0, &lay);
+    return lay.bytes;
+}
+
+// The full reduction over caller-provided scratch (used by the entry points
+// in this file and by the static-scratch entry point).
+int group_moments_launch(const cs_blocked_ell_view *src, const uint8_t *d_row_keep, const uint8_t *d_feature_keep,
+                         const uint32_t *d_row_labels, const cs_group_moments_params *params,
+                         const cs_group_moments_out *out, void *d_scratch, size_t scratch_bytes, cs_stream_t s) {
+    return moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, out, d_scratch, scratch_bytes, s,
+                       CS_MOMENTS_PHASE_ALL);
+}
+
+} // namespace csb
+
 extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,
                                                   const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
                                                   const cs_group_moments_params *params,

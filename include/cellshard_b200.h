@@ -509,6 +509,31 @@ CS_API int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
                                       size_t scratch_bytes,
                                       cs_stream_t stream);
 
+/* Size of the library-owned static scratch used by
+ * cs_b200_group_moments_blocked_ell_noalloc (64 MiB per GPU that loads it). */
+#define CS_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+/* No counterpart in the reference.  The same reduction for callers that must
+ * not allocate device memory (for example a plugin inside a process whose
+ * device memory is owned by another allocator or capped by a fixed budget,
+ * where cudaMalloc would synchronise the device mid-request and grow the
+ * footprint behind the owner's back).  It allocates nothing: its scratch is
+ * a fixed CS_NOALLOC_SCRATCH_BYTES device array inside the library, located
+ * once per device with cudaGetSymbolAddress on the first call on that device
+ * (make that first call before any stream capture).  Calls whose scratch need
+ * (cs_b200_group_moments_scratch_bytes) exceeds CS_NOALLOC_SCRATCH_BYTES
+ * return 0 with a message.  All calls share the array and it keeps the last
+ * call's contents (nothing needs clearing: every byte read is written earlier
+ * in the same call); calls that overlap on the GPU race on it, so the caller
+ * serialises them. */
+CS_API int cs_b200_group_moments_blocked_ell_noalloc(const cs_blocked_ell_view *src,
+                                                     const uint8_t *d_row_keep,
+                                                     const uint8_t *d_feature_keep,
+                                                     const uint32_t *d_row_labels,
+                                                     const cs_group_moments_params *params,
+                                                     const cs_group_moments_out *out,
+                                                     cs_stream_t stream);
+
 /* The same work split into its three stream-ordered phases, for callers that
  * time or schedule them separately (the one-shot call above runs all three):
  * PREPARE builds the column-block index and sorts the kept rows by label,
