@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", choices=["moments", "convert"], default="moments",
+                   help="moments: the headline reduction; convert: per-kernel conversion throughput")
     return p.parse_args()
 
 
@@ -391,8 +393,102 @@ def cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, seconds):
                       f"of the grouped moments (no reference implementation exists), {dt:.2f} s"}
 
 
+def run_convert(args):
+    """Conversion kernels on the same 500,000 x 32,768 matrix: CSR -> Blocked-ELL-16,
+    CSR -> Sliced-ELL (h 32), stable transpose, nnz plan + rebuild.  One JSON line per
+    operation with device time (CUDA events, mean of --steps after --warmup) and
+    algorithmic GB/s."""
+    import ctypes as C
+
+    import torch
+
+    from cellshard_b200 import _abi, synth
+    from cellshard_b200.device import (blocked_ell_from_csr, blocked_ell_shape, major_nnz_plan,
+                                       rebuild_major_order, sliced_ell_from_csr, transpose, ptr, stream_handle)
+
+    torch.cuda.set_device(0)
+    spec = synth.grouped_reduction_spec(args.rows)
+    csr = synth.make_csr(spec)
+    R, Cc, nnz = spec.rows, spec.cols, csr.nnz
+    peak, _ = measured_peak()
+    lib = _abi.load()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for a, b in ev:
+            a.record()
+            fn()
+            b.record()
+        torch.cuda.synchronize()
+        return float(np.mean([a.elapsed_time(b) for a, b in ev]))
+
+    lines = []
+
+    def emit(op, ms, nbytes, extra=None):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        d = {"workload": "convert", "op": op, "ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs,
+             "peak_gbs": peak, "frac": gbs / peak, "nnz_per_s": nnz / (ms * 1e-3), "rows": R, "cols": Cc, "nnz": nnz}
+        if extra:
+            d.update(extra)
+        lines.append(d)
+        print(json.dumps(d), flush=True)
+
+    # Blocked-ELL: shape (with bitmaps) and emit timed separately
+    B = BLOCK
+    width, _tot, scratch, status = blocked_ell_shape(csr, B)
+    rb = (R + B - 1) // B
+    bell = blocked_ell_from_csr(csr, B)
+    v = csr.view()
+    shape_t = torch.zeros(2, dtype=torch.int64, device="cuda")
+    ms_shape = timed(lambda: lib.cs_b200_blocked_ell_shape(C.byref(v), B, ptr(shape_t), ptr(scratch), scratch.numel(),
+                                                           ptr(status), stream_handle()))
+    emit("blocked_ell_shape", ms_shape, 4 * (R + 1) + 4 * nnz)
+    dv = bell.view()
+    nnz_t = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ms_emit = timed(lambda: lib.cs_b200_blocked_ell_emit(C.byref(v), C.byref(dv), ptr(nnz_t), ptr(scratch),
+                                                         scratch.numel(), ptr(status), stream_handle()))
+    emit("blocked_ell_emit", ms_emit, 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4,
+         {"ell_cols": bell.ell_cols})
+    del bell
+    torch.cuda.empty_cache()
+    # Sliced-ELL at h = 32: layout + emit (the layout's total needs one host read)
+    sell = sliced_ell_from_csr(csr, 32)
+    S = sell.slice_count
+    total = int(sell.col_idx.numel())
+    sv = sell.view()
+    ms_sell = timed(lambda: lib.cs_b200_sliced_ell_emit(C.byref(v), C.byref(sv), stream_handle()))
+    emit("sliced_ell_emit", ms_sell, 4 * (R + 1) + 6 * nnz + 6 * total + 4 * (2 * S + 1), {"total_slots": total})
+    del sell
+    torch.cuda.empty_cache()
+    # transpose
+    nb = C.c_size_t()
+    lib.cs_b200_compressed_transpose_scratch_bytes(R, Cc, nnz, C.byref(nb))
+    tscr = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+    optr = torch.empty(Cc + 1, dtype=torch.int32, device="cuda")
+    oidx = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    oval = torch.empty(nnz, dtype=torch.float16, device="cuda")
+    ms_t = timed(lambda: lib.cs_b200_build_compressed_transpose(R, Cc, nnz, ptr(csr.ptr), ptr(csr.idx), ptr(csr.val),
+                                                               ptr(optr), None, ptr(oidx), ptr(oval), ptr(tscr),
+                                                               nb.value, stream_handle()))
+    emit("transpose", ms_t, 4 * (R + 1) + 6 * nnz + 4 * (Cc + 1) + 6 * nnz)
+    del oidx, oval, tscr
+    torch.cuda.empty_cache()
+    # nnz plan (+ pow2 bins) and rebuild
+    ms_p = timed(lambda: major_nnz_plan(csr.ptr, R, 64))
+    emit("nnz_plan", ms_p, 4 * (R + 1) + 12 * R + 4 * 65)
+    plan = major_nnz_plan(csr.ptr, R, 64)
+    ms_r = timed(lambda: rebuild_major_order(csr, plan["order"]))
+    emit("rebuild", ms_r, 6 * nnz + 4 * (R + 1) + 6 * nnz + 4 * (R + 1) + 4 * R)
+
+
 def main():
     args = parse()
+    if args.workload == "convert":
+        run_convert(args)
+        return
     if args.impl == "reference":
         world, rank, _ = dist_setup(args)
         if rank != 0:

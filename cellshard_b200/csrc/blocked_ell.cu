@@ -60,14 +60,30 @@ __global__ void __launch_bounds__(kShapeWarps * 32) bell_shape_kernel(
             bad |= CS_STATUS_BAD_POINTERS;
         } else {
             const uint32_t b = ptr[r0], e = ptr[r1];
-            for (uint32_t i = b + lane; i < e; i += 32u) {
-                const uint32_t c = idx[i];
+            auto mark = [&](uint32_t c) {
                 if (c >= cols) {
                     bad |= CS_STATUS_INDEX_RANGE;
-                    continue;
+                    return;
                 }
                 const uint32_t bc = div_b(c, B, shift);
                 atomicOr(bits + (bc >> 5), 1u << (bc & 31u));
+            };
+            // scalar head to a 16-byte boundary, 16-byte body, scalar tail
+            const bool vec = (reinterpret_cast<uintptr_t>(idx) & 15u) == 0u;
+            const uint32_t head_end = vec ? min(e, (b + 3u) & ~3u) : e;
+            for (uint32_t i = b + lane; i < head_end; i += 32u) mark(idx[i]);
+            if (vec) {
+                const uint32_t nvec = (e - head_end) >> 2;
+                const uint4 *v4 = reinterpret_cast<const uint4 *>(idx + head_end);
+#pragma unroll 4
+                for (uint32_t k = lane; k < nvec; k += 32u) {
+                    const uint4 q = __ldg(v4 + k);
+                    mark(q.x);
+                    mark(q.y);
+                    mark(q.z);
+                    mark(q.w);
+                }
+                for (uint32_t i = head_end + (nvec << 2) + lane; i < e; i += 32u) mark(idx[i]);
             }
         }
         __syncwarp();
@@ -213,6 +229,168 @@ __global__ void __launch_bounds__(kEmitThreads) bell_emit_kernel(
     }
 }
 
+
+// Emit with shared-memory row staging and bulk (TMA) stores.  A CTA takes
+// whole row blocks (the block's column index is loaded once for its B rows)
+// and owns NBUF row buffers (~64 KB in total, three CTAs per SM): a row is
+// scattered into a zeroed buffer by the threads, then one thread hands the
+// whole padded row to the copy engine and the CTA moves on while it streams
+// out.  A buffer is re-zeroed only after the bulk store that read it has
+// finished reading.  Rows whose columns are not strictly increasing are
+// redone in CSR order by one thread (the reference's overwrite order).
+template <int NBUF>
+__global__ void __launch_bounds__(kEmitThreads, 3) bell_emit_tma_kernel(
+    const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ idx, const uint16_t *__restrict__ val, uint32_t rows,
+    uint32_t cols, uint32_t nnz, uint32_t B, int shift, uint32_t words, uint32_t width, uint32_t ell_cols,
+    const uint32_t *__restrict__ bitmaps, uint32_t *__restrict__ out_bci, uint16_t *__restrict__ out_val,
+    uint32_t *__restrict__ d_nnz, uint32_t *status) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    constexpr int PF = 8; // entries per thread prefetched for the next row
+    const uint32_t row_bytes = ell_cols * 2u;
+    const uint32_t stride = (row_bytes + 127u) & ~127u;
+    uint2 *ix = reinterpret_cast<uint2 *>(tma_smem + (std::size_t) NBUF * stride);
+    uint32_t *rp = reinterpret_cast<uint32_t *>(ix + words); // [B + 1] row pointers of the block
+    __shared__ uint32_t count_smem;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t row_blocks = (rows + B - 1u) / B;
+    for (uint32_t k = threadIdx.x * 16u; k < NBUF * stride; k += blockDim.x * 16u)
+        *reinterpret_cast<uint4 *>(tma_smem + k) = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t my_nnz = 0u, bad = 0u, iter = 0u;
+    uint32_t nc[PF];
+    uint16_t nv[PF];
+    auto prefetch = [&](uint32_t a, uint32_t e) {
+#pragma unroll
+        for (int k = 0; k < PF; ++k) {
+            const uint32_t i = a + threadIdx.x + (uint32_t) k * kEmitThreads;
+            nc[k] = i < e ? __ldg(idx + i) : 0xffffffffu;
+            nv[k] = i < e ? __ldg(reinterpret_cast<const unsigned short *>(val) + i) : (uint16_t) 0u;
+        }
+    };
+    for (uint32_t rb = blockIdx.x; rb < row_blocks; rb += gridDim.x) {
+        const uint32_t r_beg = rb * B, r_end = min(rows, rb * B + B);
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t carry = 0u;
+            for (uint32_t w0 = 0; w0 < words; w0 += 32u) {
+                const uint32_t w = w0 + lane;
+                const uint32_t word = w < words ? bitmaps[(std::size_t) rb * words + w] : 0u;
+                const uint32_t c = __popc(word);
+                const uint32_t incl = warp_inclusive_scan(c);
+                if (w < words) ix[w] = make_uint2(word, carry + incl - c);
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0u) count_smem = carry;
+        }
+        for (uint32_t r = threadIdx.x; r <= r_end - r_beg; r += blockDim.x) rp[r] = ptr[r_beg + r];
+        __syncthreads();
+        const uint32_t count = count_smem;
+        if (count > width) bad |= CS_STATUS_INDEX_RANGE;
+        if (out_bci != nullptr) {
+            uint32_t *row_bci = out_bci + (std::size_t) rb * width;
+            for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+                uint32_t word = ix[w].x;
+                uint32_t pos = ix[w].y;
+                while (word != 0u) {
+                    const uint32_t bit = __ffs(word) - 1u;
+                    if (pos < width) row_bci[pos] = w * 32u + bit;
+                    ++pos;
+                    word &= word - 1u;
+                }
+            }
+            for (uint32_t s2 = count + threadIdx.x; s2 < width; s2 += blockDim.x) row_bci[s2] = CS_INVALID_COL;
+        }
+        {
+            const uint32_t a0 = rp[0], e0 = rp[1];
+            prefetch(a0, (e0 < a0 || e0 > nnz) ? a0 : e0);
+        }
+        for (uint32_t r = r_beg; r < r_end; ++r, ++iter) {
+            uint32_t cc[PF];
+            uint16_t cv[PF];
+#pragma unroll
+            for (int k = 0; k < PF; ++k) {
+                cc[k] = nc[k];
+                cv[k] = nv[k];
+            }
+            const uint32_t a = rp[r - r_beg], e = rp[r - r_beg + 1u];
+            const bool ptr_bad = e < a || e > nnz;
+            if (ptr_bad) bad |= CS_STATUS_BAD_POINTERS;
+            if (r + 1u < r_end) {
+                const uint32_t a1 = rp[r - r_beg + 1u], e1 = rp[r - r_beg + 2u];
+                prefetch(a1, (e1 < a1 || e1 > nnz) ? a1 : e1);
+            }
+            uint16_t *buf = reinterpret_cast<uint16_t *>(tma_smem + (std::size_t) (iter % NBUF) * stride);
+            if (iter >= (uint32_t) NBUF) {
+                if (threadIdx.x == 0) bulk_wait_read<NBUF - 1>();
+                __syncthreads();
+                for (uint32_t k = threadIdx.x * 8u; k < ell_cols; k += blockDim.x * 8u)
+                    *reinterpret_cast<uint4 *>(buf + k) = make_uint4(0u, 0u, 0u, 0u);
+                __syncthreads();
+            }
+            int unordered = 0;
+            uint32_t row_nnz = 0u;
+            auto place = [&](uint32_t i, uint32_t c, uint16_t v) {
+                if (c >= cols) return;
+                const uint32_t bc = div_b(c, B, shift);
+                const uint2 x = ix[bc >> 5];
+                const uint32_t slot = x.y + __popc(x.x & ((1u << (bc & 31u)) - 1u));
+                if (slot >= width) return;
+                buf[slot * B + (c - bc * B)] = v;
+                row_nnz += half_nonzero(v);
+            };
+            if (!ptr_bad) {
+#pragma unroll
+                for (int k = 0; k < PF; ++k) {
+                    const uint32_t i = a + threadIdx.x + (uint32_t) k * kEmitThreads;
+                    // the next entry belongs to the next lane (or, for lane 31, the next warp)
+                    uint32_t nxt = __shfl_down_sync(0xffffffffu, cc[k], 1);
+                    if (lane == 31u && i + 1u < e) nxt = __ldg(idx + i + 1u);
+                    if (i < e) {
+                        if (i + 1u < e && cc[k] >= nxt) unordered = 1;
+                        place(i, cc[k], cv[k]);
+                    }
+                }
+                for (uint32_t i = a + PF * kEmitThreads + threadIdx.x; i < e; i += blockDim.x) {
+                    const uint32_t c = __ldg(idx + i);
+                    if (i + 1u < e && c >= __ldg(idx + i + 1u)) unordered = 1;
+                    place(i, c, val[i]);
+                }
+            }
+            if (__syncthreads_or(unordered)) {
+                for (uint32_t k = threadIdx.x * 8u; k < ell_cols; k += blockDim.x * 8u)
+                    *reinterpret_cast<uint4 *>(buf + k) = make_uint4(0u, 0u, 0u, 0u);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    for (uint32_t i = a; i < e; ++i) {
+                        const uint32_t c = idx[i];
+                        if (c >= cols) continue;
+                        const uint32_t bc = div_b(c, B, shift);
+                        const uint2 x = ix[bc >> 5];
+                        const uint32_t slot = x.y + __popc(x.x & ((1u << (bc & 31u)) - 1u));
+                        if (slot < width) buf[slot * B + (c - bc * B)] = val[i];
+                    }
+                }
+                __syncthreads();
+                row_nnz = 0u;
+                for (uint32_t k = threadIdx.x; k < ell_cols; k += blockDim.x) row_nnz += half_nonzero(buf[k]);
+            }
+            my_nnz += row_nnz;
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                bulk_store_s2g(out_val + (std::size_t) r * ell_cols, buf, row_bytes);
+                bulk_commit();
+            }
+        }
+    }
+    if (threadIdx.x == 0) bulk_wait_all();
+    my_nnz = __reduce_add_sync(0xffffffffu, my_nnz);
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (lane == 0u) {
+        if (my_nnz != 0u) atomicAdd(d_nnz, my_nnz);
+        status_or(status, bad);
+    }
+}
+
 int pow2_shift(uint32_t B) {
     if (B == 0u || (B & (B - 1u)) != 0u) return -1;
     int s = 0;
@@ -278,6 +456,35 @@ int blocked_ell_emit_launch(const cs_compressed_view *src, const cs_blocked_ell_
     const uint32_t words = col_words(src->cols, B);
     const uint32_t width = dst->ell_cols / B;
     if (src->rows == 0u || dst->ell_cols == 0u) return 1;
+    // bulk-store path: whole padded rows in shared memory, 16-byte aligned rows
+    const std::size_t row_bytes = (std::size_t) dst->ell_cols * 2u;
+    const std::size_t stride = (row_bytes + 127u) & ~(std::size_t) 127u;
+    const bool tma_ok = (dst->ell_cols % 8u) == 0u && (reinterpret_cast<uintptr_t>(dst->val) & 15u) == 0u &&
+                        dst->ell_cols <= kSegHalves;
+    if (tma_ok) {
+        const int nbuf = stride <= 8192u ? 8 : (stride <= 16384u ? 4 : (stride <= 32768u ? 2 : 1));
+        const std::size_t tsmem =
+            (std::size_t) nbuf * stride + (std::size_t) words * sizeof(uint2) + ((std::size_t) B + 1u) * 4u;
+        if (tsmem <= 72u * 1024u) {
+            const uint32_t row_blocks = (src->rows + B - 1u) / B;
+            uint32_t tgrid = (uint32_t) sm_count() * 3u;
+            if (tgrid > row_blocks) tgrid = row_blocks;
+            auto launch = [&](auto kern) {
+                if (!cuda_ok(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) tsmem),
+                             "bell_emit_tma smem attribute"))
+                    return 0;
+                kern<<<tgrid, kEmitThreads, tsmem, stream>>>(src->majorPtr, src->minorIdx, src->val, src->rows,
+                                                              src->cols, src->nnz, B, pow2_shift(B), words, width,
+                                                              dst->ell_cols, bitmaps, dst->blockColIdx, dst->val,
+                                                              d_nnz, d_status);
+                return launch_ok("bell_emit_tma_kernel");
+            };
+            if (nbuf == 8) return launch(bell_emit_tma_kernel<8>);
+            if (nbuf == 4) return launch(bell_emit_tma_kernel<4>);
+            if (nbuf == 2) return launch(bell_emit_tma_kernel<2>);
+            return launch(bell_emit_tma_kernel<1>);
+        }
+    }
     const std::size_t smem = (std::size_t) kSegHalves * sizeof(uint16_t) + (std::size_t) words * sizeof(uint2);
     if (!cuda_ok(cudaFuncSetAttribute(bell_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem),
                  "bell_emit smem attribute"))

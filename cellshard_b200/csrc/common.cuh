@@ -116,6 +116,50 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
     return r;
 }
 
+// Lanes holding the same BITS-bit digit as this lane (this lane included),
+// among lanes whose `valid` is set; 0 for an invalid lane.  Built from one
+// ballot per digit bit (the multisplit construction), cheaper than a general
+// match for small digits.
+template <int BITS>
+__device__ __forceinline__ uint32_t warp_match_digit(uint32_t d, bool valid) {
+    uint32_t m = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < BITS; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? bb : ~bb;
+    }
+    return valid ? m : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// Bulk (TMA) copies shared -> global.  Sizes and both addresses must be
+// multiples of 16 bytes.  Generic-proxy shared-memory writes must be fenced
+// with fence_proxy_async_smem() (by the writing threads, then a barrier)
+// before the bulk copy reads them.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_store_s2g(void *gdst, const void *ssrc, uint32_t bytes) {
+    const uint32_t s = (uint32_t) __cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(s), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Waits until at most N of this thread's committed bulk groups are still
+// reading shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Waits until all of this thread's committed bulk groups have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // Device-wide exclusive scan of uint32 (three launches: tile sums, scan of
 // tile sums, tile-local scan + add).  out may alias in.  out[n] receives the

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kIndexWarps * 32) moments_index_kernel(const u
                                                                          uint32_t row_blocks, uint32_t width,
                                                                          uint32_t col_blocks, uint32_t words,
                                                                          uint2 *__restrict__ index,
-                                                                         uint32_t *status) {
+                                                                         uint32_t *status, bool vec4) {
     extern __shared__ uint32_t bitmap_smem[];
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t *bits = bitmap_smem + (std::size_t) warp * words;
@@ -96,19 +96,34 @@ __global__ void __launch_bounds__(kIndexWarps * 32) moments_index_kernel(const u
         __syncwarp();
         const uint32_t *row = block_col_idx + (std::size_t) rb * width;
         uint32_t bad = 0u;
-        for (uint32_t s = lane; s < width; s += 32u) {
-            const uint32_t bc = row[s];
-            if (bc != CS_INVALID_COL) {
-                if (bc >= col_blocks) {
-                    bad |= CS_STATUS_INDEX_RANGE;
-                } else {
-                    atomicOr(bits + (bc >> 5), 1u << (bc & 31u));
+        auto mark = [&](uint32_t bc, uint32_t prev, bool has_prev) {
+            if (bc == CS_INVALID_COL) return;
+            if (bc >= col_blocks)
+                bad |= CS_STATUS_INDEX_RANGE;
+            else
+                atomicOr(bits + (bc >> 5), 1u << (bc & 31u));
+            if (has_prev && (prev == CS_INVALID_COL || prev >= bc)) bad |= CS_STATUS_BLOCK_COL_ORDER;
+        };
+        if (vec4) {
+            // 4 entries per lane per step; the entry before a lane's first one is
+            // the previous lane's last (or the previous step's lane 31)
+            uint32_t carry = CS_INVALID_COL;
+            for (uint32_t s0 = 0; s0 < width; s0 += 128u) {
+                const uint32_t s = s0 + lane * 4u;
+                uint4 q = make_uint4(CS_INVALID_COL, CS_INVALID_COL, CS_INVALID_COL, CS_INVALID_COL);
+                if (s < width) q = __ldg(reinterpret_cast<const uint4 *>(row + s));
+                uint32_t before = __shfl_up_sync(0xffffffffu, q.w, 1);
+                if (lane == 0u) before = carry;
+                if (s < width) {
+                    mark(q.x, before, s > 0u);
+                    mark(q.y, q.x, true);
+                    mark(q.z, q.y, true);
+                    mark(q.w, q.z, true);
                 }
-                if (s > 0u) {
-                    const uint32_t prev = row[s - 1u];
-                    if (prev == CS_INVALID_COL || prev >= bc) bad |= CS_STATUS_BLOCK_COL_ORDER;
-                }
+                carry = __shfl_sync(0xffffffffu, q.w, 31);
             }
+        } else {
+            for (uint32_t s = lane; s < width; s += 32u) mark(row[s], s > 0u ? row[s - 1u] : 0u, s > 0u);
         }
         bad = __reduce_or_sync(0xffffffffu, bad);
         if (lane == 0u) status_or(status, bad);
@@ -618,7 +633,8 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
                          "index smem attribute"))
                 return 0;
             moments_index_kernel<<<blocks, kIndexWarps * 32, smem, stream>>>(
-                src->blockColIdx, lay.row_blocks, width, lay.col_blocks, lay.words, lay.index, out->status);
+                src->blockColIdx, lay.row_blocks, width, lay.col_blocks, lay.words, lay.index, out->status,
+                (width % 4u) == 0u && (reinterpret_cast<uintptr_t>(src->blockColIdx) & 15u) == 0u);
             if (!launch_ok("moments_index_kernel")) return 0;
         } else if (!cuda_ok(cudaMemsetAsync(lay.index, 0, (std::size_t) lay.row_blocks * lay.words * sizeof(uint2),
                                             stream),

@@ -49,15 +49,17 @@ def test_transpose_generated_and_roundtrip(cuda, orc):
     assert np.array_equal(np_u16(back.val), val)
 
 
-def test_transpose_flags_duplicate_columns(cuda):
-    from cellshard_b200 import _abi
+def test_transpose_keeps_repeated_columns_in_row_order(cuda, orc):
+    """A row repeating a column keeps both entries, in CSR order (stable)."""
     from cellshard_b200.device import transpose
 
-    ptr = np.array([0, 3, 4], np.uint32)
-    idx = np.array([1, 1, 2, 0], np.uint32)
-    val = np.array([1, 2, 3, 4], np.float16).view(np.uint16)
-    with pytest.raises(_abi.CellShardError, match="status"):
-        transpose(to_device_csr(2, 3, ptr, idx, val))
+    ptr = np.array([0, 3, 4, 6], np.uint32)
+    idx = np.array([1, 1, 2, 0, 2, 1], np.uint32)
+    val = np.array([1, 2, 3, 4, 5, 6], np.float16).view(np.uint16)
+    t = transpose(to_device_csr(3, 3, ptr, idx, val))
+    rptr, ridx, rval = orc.csr_transpose(3, 3, ptr, idx, val)
+    assert np.array_equal(np_u32(t.ptr), rptr) and np.array_equal(np_u32(t.idx), ridx)
+    assert np.array_equal(np_u16(t.val), rval)
 
 
 @ref_gpu
