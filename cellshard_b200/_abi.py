@@ -84,6 +84,28 @@ class GroupMomentsOut(C.Structure):
                 ("group_rows", vp), ("status", vp)]
 
 
+class BatchPart(C.Structure):
+    _fields_ = [("src", CompressedView), ("bucket_count", u32), ("pad0", u32 * 3), ("d_major_nnz", vp),
+                ("d_sorted_nnz", vp), ("d_order", vp), ("d_bucket_offsets", vp), ("d_pow2_offsets", vp),
+                ("_pad", C.c_uint64)]
+
+
+class BatchTiles(C.Structure):
+    _fields_ = [("layout_rows", u32), ("emit_rows", u32), ("emit_lanes", u32), ("ctas_per_sm", u32)]
+
+
+class BatchSlicedResult(C.Structure):
+    _fields_ = [("status", u32), ("slice_rows", u32), ("slice_count", u32), ("plan_status", u32),
+                ("total_slots", u64), ("arena_offset", u64), ("arena_bytes", u64), ("score", C.c_double),
+                ("view", SlicedEllView)]
+
+
+BATCH_DEFERRED = 1 << 8
+BATCH_WAIT_TIMEOUT = 1 << 9
+BATCH_TOO_LARGE = 1 << 10
+BATCH_NO_CANDIDATE = 1 << 11
+BATCH_EXCEEDS_ARENA = 1 << 12
+
 P = C.POINTER
 
 # name -> (restype, argtypes)
@@ -134,6 +156,13 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_group_moments_phases": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
                                                P(GroupMomentsOut), vp, sz, u32, vp]),
     "cs_b200_synth_csr": (C.c_int, [u32, u32, vp, vp, vp, vp, u32, vp, u64, vp, vp, vp]),
+    "cs_b200_batch_sliced_create": (C.c_int, [P(BatchPart), u32, P(u32), u32, vp, u64, P(BatchTiles), P(vp)]),
+    "cs_b200_batch_sliced_autotune": (C.c_int, [vp, vp, P(BatchTiles)]),
+    "cs_b200_batch_sliced_run": (C.c_int, [vp, vp]),
+    "cs_b200_batch_sliced_results": (C.c_int, [vp, P(BatchSlicedResult), P(u32), P(u32), vp]),
+    "cs_b200_batch_sliced_next_wave": (C.c_int, [vp, vp, u64, P(u32)]),
+    "cs_b200_batch_sliced_tiles": (C.c_int, [vp, P(BatchTiles), P(u32), P(u32)]),
+    "cs_b200_batch_sliced_destroy": (None, [vp]),
 }
 
 

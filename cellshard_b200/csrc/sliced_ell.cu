@@ -18,6 +18,7 @@
 //           height: one launch accumulates it for every candidate; the score
 //           arithmetic stays in host doubles, in the reference's order.
 #include "common.cuh"
+#include "emit_rows.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -113,6 +114,27 @@ __global__ void __launch_bounds__(kWarps * 32) sell_emit_kernel(const uint32_t *
     }
 }
 
+// Vectorised emit: one group of GL lanes per row (rows_per_warp = 32 / GL).
+template <unsigned GL>
+__global__ void __launch_bounds__(kWarps * 32) sell_emit_vec_kernel(const uint32_t *__restrict__ ptr,
+                                                                    const uint32_t *__restrict__ idx,
+                                                                    const uint16_t *__restrict__ val, uint32_t rows,
+                                                                    uint32_t h, const uint32_t *__restrict__ widths,
+                                                                    const uint32_t *__restrict__ slot_offsets,
+                                                                    uint32_t *__restrict__ col_idx,
+                                                                    uint16_t *__restrict__ out_val) {
+    constexpr unsigned RPW = 32u / GL;
+    const unsigned lane = threadIdx.x & 31u, gl = lane % GL;
+    const uint32_t warp0 = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    for (uint32_t r = warp0 * RPW + lane / GL; r < rows; r += gridDim.x * kWarps * RPW) {
+        const uint32_t s = r / h;
+        const uint32_t w = widths[s];
+        const std::size_t base = (std::size_t) slot_offsets[s] + (std::size_t) (r - s * h) * w;
+        const uint32_t a = ptr[r];
+        sell_emit_row_vec<GL>(idx, val, a, ptr[r + 1u] - a, w, base, col_idx, out_val, gl);
+    }
+}
+
 unsigned grid_for(uint32_t items) {
     uint32_t g = (items + kWarps - 1u) / kWarps;
     const uint32_t cap = (uint32_t) sm_count() * 32u;
@@ -171,10 +193,25 @@ int sliced_layout_launch(const cs_compressed_view *src, uint32_t slice_rows, uin
 int sliced_emit_launch(const cs_compressed_view *src, const cs_sliced_ell_view *dst, cudaStream_t stream) {
     if (src->rows == 0u) return 1;
     const uint32_t h = clamp_rows(src->rows, dst->slice_rows);
-    sell_emit_kernel<<<grid_for(src->rows), kWarps * 32, 0, stream>>>(src->majorPtr, src->minorIdx, src->val,
-                                                                      src->rows, h, dst->slice_widths,
-                                                                      dst->slice_slot_offsets, dst->col_idx, dst->val);
-    return launch_ok("sell_emit_kernel");
+    const bool aligned = ((uintptr_t) dst->col_idx & 15u) == 0u && ((uintptr_t) dst->val & 7u) == 0u;
+    if (!aligned) {
+        sell_emit_kernel<<<grid_for(src->rows), kWarps * 32, 0, stream>>>(src->majorPtr, src->minorIdx, src->val,
+                                                                          src->rows, h, dst->slice_widths,
+                                                                          dst->slice_slot_offsets, dst->col_idx,
+                                                                          dst->val);
+        return launch_ok("sell_emit_kernel");
+    }
+    // rows narrower than a warp's 128 slots share the warp
+    const double mean_nnz = (double) src->nnz / (double) src->rows;
+    if (mean_nnz >= 96.0)
+        sell_emit_vec_kernel<32><<<grid_for(src->rows), kWarps * 32, 0, stream>>>(
+            src->majorPtr, src->minorIdx, src->val, src->rows, h, dst->slice_widths, dst->slice_slot_offsets,
+            dst->col_idx, dst->val);
+    else
+        sell_emit_vec_kernel<8><<<grid_for((src->rows + 3u) / 4u), kWarps * 32, 0, stream>>>(
+            src->majorPtr, src->minorIdx, src->val, src->rows, h, dst->slice_widths, dst->slice_slot_offsets,
+            dst->col_idx, dst->val);
+    return launch_ok("sell_emit_vec_kernel");
 }
 
 } // namespace csb

@@ -582,6 +582,83 @@ CS_API int cs_b200_synth_csr(uint32_t rows,
                       uint16_t *d_val,
                       cs_stream_t stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched conversion of many uneven partitions (no reference counterpart:  */
+/* the reference converts one partition per call, sliced_ell_from_          */
+/* compressed.cuh:96-254, and plans one per call, major_nnz_raw.cuh:64-120). */
+/* Per partition the results equal choose_sliced_ell_slice_rows_from_       */
+/* compressed + sliced_ell_from_compressed at the chosen height, and        */
+/* build_major_nnz_bucket_plan_raw, bit for bit.  All partitions of a wave   */
+/* run in ONE persistent launch fed by a device work queue, replayed from a  */
+/* CUDA graph; output blocks are taken from a caller arena first-fit in      */
+/* partition order, and partitions that do not fit are deferred to the next  */
+/* wave.                                                                     */
+/* ------------------------------------------------------------------------ */
+#define CS_BATCH_MAX_CANDIDATES 4
+
+enum {
+    CS_BATCH_DEFERRED = 1u << 8,      /* output did not fit the wave's arena */
+    CS_BATCH_WAIT_TIMEOUT = 1u << 9,  /* a bounded device wait ran out; item skipped */
+    CS_BATCH_TOO_LARGE = 1u << 10,    /* padded slots exceed the u32 slot offsets */
+    CS_BATCH_NO_CANDIDATE = 1u << 11,
+    CS_BATCH_EXCEEDS_ARENA = 1u << 12 /* the partition's block alone is larger than the arena */
+};
+
+typedef struct CS_ALIGN16 cs_batch_part {
+    cs_compressed_view src;     /* device CSR (row-compressed) */
+    uint32_t bucket_count;      /* requested nnz buckets; plan skipped if d_major_nnz is NULL */
+    uint32_t pad0[3];
+    uint32_t *d_major_nnz;      /* [rows] row nnz */
+    uint32_t *d_sorted_nnz;     /* [rows] ascending */
+    uint32_t *d_order;          /* [rows] stable: ties keep row order */
+    uint32_t *d_bucket_offsets; /* [clamp(bucket_count, 1, rows) + 1]; [1] if rows == 0 */
+    uint32_t *d_pow2_offsets;   /* [34] or NULL: bin k = nnz in [2^k, 2^(k+1)), bin 0 also 0 */
+} cs_batch_part;
+
+/* Launch-shape knobs picked by cs_b200_batch_sliced_autotune. */
+typedef struct cs_batch_tiles {
+    uint32_t layout_rows; /* rows per layout item (multiple of 32) */
+    uint32_t emit_rows;   /* rows per emit item */
+    uint32_t emit_lanes;  /* lanes per row in the emit: 32, 16, 8 or 4 (rows per warp 1..8) */
+    uint32_t ctas_per_sm; /* 0 = as many as fit */
+} cs_batch_tiles;
+
+typedef struct CS_ALIGN16 cs_batch_sliced_result {
+    uint32_t status;        /* 0, or CS_BATCH_* bits */
+    uint32_t slice_rows;    /* chosen height (clamped to [1, rows]) */
+    uint32_t slice_count;
+    uint32_t plan_status;
+    uint64_t total_slots;
+    uint64_t arena_offset;  /* byte offset of the partition's block in its wave's arena */
+    uint64_t arena_bytes;
+    double score;           /* the chooser's score of the chosen height */
+    cs_sliced_ell_view view; /* device view into the arena */
+} cs_batch_sliced_result;
+
+typedef struct cs_batch_plan cs_batch_plan;
+
+/* Builds the queue, descriptors and the CUDA graph for wave 1 (all
+ * partitions).  d_arena must be 256-byte aligned; tiles NULL = defaults.
+ * 1..CS_BATCH_MAX_CANDIDATES non-zero candidate heights. */
+CS_API int cs_b200_batch_sliced_create(const cs_batch_part *parts, uint32_t count, const uint32_t *candidates,
+                                       uint32_t candidate_count, void *d_arena, uint64_t arena_bytes,
+                                       const cs_batch_tiles *tiles, cs_batch_plan **out);
+/* Times the tile candidates on this batch (each a full wave) and keeps the
+ * fastest; cached per process by batch shape. */
+CS_API int cs_b200_batch_sliced_autotune(cs_batch_plan *plan, cs_stream_t stream, cs_batch_tiles *chosen);
+/* One wave: one graph launch (a state reset and the persistent kernel). */
+CS_API int cs_b200_batch_sliced_run(cs_batch_plan *plan, cs_stream_t stream);
+/* Copies every partition's result record to the host (synchronises). */
+CS_API int cs_b200_batch_sliced_results(cs_batch_plan *plan, cs_batch_sliced_result *h_results, uint32_t *deferred,
+                                        uint32_t *error_bits, cs_stream_t stream);
+/* The partitions deferred by the last wave become the next wave, with a new
+ * (or the same, once its blocks are consumed) arena. */
+CS_API int cs_b200_batch_sliced_next_wave(cs_batch_plan *plan, void *d_arena, uint64_t arena_bytes,
+                                          uint32_t *wave_size);
+CS_API int cs_b200_batch_sliced_tiles(const cs_batch_plan *plan, cs_batch_tiles *out, uint32_t *grid,
+                                      uint32_t *items);
+CS_API void cs_b200_batch_sliced_destroy(cs_batch_plan *plan);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

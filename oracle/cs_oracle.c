@@ -226,8 +226,11 @@ long long cso_reoptimize_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t
 }
 
 /* ------------------------------------------------------------------------ */
-/* Grouped moments in FP64, row-partitioned over threads with private        */
-/* accumulators merged in thread order (deterministic).                      */
+/* Grouped moments in FP64, feature-partitioned over threads: each thread     */
+/* owns a column range and walks every kept row in ascending order, so every  */
+/* (group, feature) sum is taken in row order -- the result does not depend   */
+/* on the thread count, and no thread holds a private G x C copy.  Rows whose */
+/* columns are ascending are entered by binary search; others are filtered.   */
 /* ------------------------------------------------------------------------ */
 typedef struct {
     int kind; /* 0 = bell, 1 = csr */
@@ -236,45 +239,97 @@ typedef struct {
     const uint16_t *val;
     const uint8_t *row_keep;
     const uint32_t *labels;
-    uint32_t G;
-    uint32_t r0, r1;
-    double *s, *q;
-    uint32_t *n;
+    const uint8_t *sorted; /* per row (csr) or row block (bell): columns ascending */
+    uint32_t G, ddof;
+    const uint8_t *fk;
+    const uint32_t *group_rows;
+    uint32_t f0, f1; /* owned features; multiples of B (bell) except at cols */
+    double *sum, *sumsq, *mean, *var;
 } mom_task;
+
+static uint32_t lower_bound_u32(const uint32_t *a, uint32_t n, uint32_t x) {
+    uint32_t lo = 0u, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (a[mid] < x)
+            lo = mid + 1u;
+        else
+            hi = mid;
+    }
+    return lo;
+}
 
 static void *mom_worker(void *arg) {
     mom_task *t = (mom_task *) arg;
     const uint32_t W = t->B != 0u ? t->ell_cols / t->B : 0u;
-    for (uint32_t r = t->r0; r < t->r1; ++r) {
+    for (uint32_t g = 0; g < t->G; ++g)
+        for (uint32_t f = t->f0; f < t->f1; ++f) {
+            t->sum[(size_t) g * t->cols + f] = 0.0;
+            t->sumsq[(size_t) g * t->cols + f] = 0.0;
+        }
+    for (uint32_t r = 0; r < t->rows; ++r) {
         if (t->row_keep != NULL && t->row_keep[r] == 0u) continue;
         const uint32_t g = t->labels != NULL ? t->labels[r] : 0u;
         if (g >= t->G) continue;
-        t->n[g] += 1u;
-        double *s = t->s + (size_t) g * t->cols;
-        double *q = t->q + (size_t) g * t->cols;
+        double *s = t->sum + (size_t) g * t->cols;
+        double *q = t->sumsq + (size_t) g * t->cols;
         if (t->kind == 0) {
             const uint32_t rb = r / t->B;
             const uint32_t *brow = t->bci + (size_t) rb * W;
             const uint16_t *vrow = t->val + (size_t) r * t->ell_cols;
-            for (uint32_t slot = 0; slot < W; ++slot) {
+            uint32_t slot = t->sorted[rb] ? lower_bound_u32(brow, W, t->f0 / t->B) : 0u;
+            for (; slot < W; ++slot) {
                 const uint32_t bc = brow[slot];
-                if (bc == INVALID_COL) continue;
+                if (bc == INVALID_COL) {
+                    if (t->sorted[rb]) break;
+                    continue;
+                }
+                if ((uint64_t) bc * t->B >= t->f1) {
+                    if (t->sorted[rb]) break;
+                    continue;
+                }
                 for (uint32_t l = 0; l < t->B; ++l) {
                     const uint32_t f = bc * t->B + l;
-                    if (f >= t->cols) continue;
+                    if (f >= t->cols || f < t->f0 || f >= t->f1) continue;
                     const double x = cso_h2f(vrow[(size_t) slot * t->B + l]);
                     s[f] += x;
                     q[f] += x * x;
                 }
             }
         } else {
-            for (uint32_t i = t->ptr[r]; i < t->ptr[r + 1u]; ++i) {
+            const uint32_t a = t->ptr[r], e = t->ptr[r + 1u];
+            uint32_t i = t->sorted[r] ? a + lower_bound_u32(t->idx + a, e - a, t->f0) : a;
+            for (; i < e; ++i) {
                 const uint32_t f = t->idx[i];
-                if (f >= t->cols) continue;
+                if (f < t->f0 || f >= t->f1) {
+                    if (t->sorted[r] && f >= t->f1) break;
+                    continue;
+                }
                 const double x = cso_h2f(t->val[i]);
                 s[f] += x;
                 q[f] += x * x;
             }
+        }
+    }
+    for (uint32_t g = 0; g < t->G; ++g) {
+        const uint32_t n = t->group_rows[g];
+        for (uint32_t f = t->f0; f < t->f1; ++f) {
+            const size_t k = (size_t) g * t->cols + f;
+            double sv = t->sum[k], qv = t->sumsq[k];
+            if (t->fk != NULL && t->fk[f] == 0u) sv = qv = 0.0;
+            double m = 0.0, v = 0.0;
+            if (n > 0u && (t->fk == NULL || t->fk[f] != 0u)) {
+                m = sv / (double) n;
+                if (n > t->ddof) {
+                    double m2 = qv - sv * m;
+                    if (m2 < 0.0) m2 = 0.0;
+                    v = m2 / (double) (n - t->ddof);
+                }
+            }
+            t->sum[k] = sv;
+            t->sumsq[k] = qv;
+            if (t->mean != NULL) t->mean[k] = m;
+            if (t->var != NULL) t->var[k] = v;
         }
     }
     return NULL;
@@ -282,63 +337,61 @@ static void *mom_worker(void *arg) {
 
 static int moments_run(mom_task proto, const uint8_t *fk, uint32_t ddof, double *sum, double *sumsq, double *mean,
                        double *var, uint32_t *group_rows, int nthreads) {
+    const uint32_t unit = proto.kind == 0 ? proto.B : 1u;
+    const uint32_t units = (proto.cols + unit - 1u) / unit;
     if (nthreads < 1) nthreads = 1;
-    if ((uint32_t) nthreads > proto.rows && proto.rows > 0u) nthreads = (int) proto.rows;
+    if ((uint32_t) nthreads > units && units > 0u) nthreads = (int) units;
     if (nthreads < 1) nthreads = 1;
-    const size_t gc = (size_t) proto.G * proto.cols;
+    uint32_t *n = (uint32_t *) calloc((size_t) proto.G + 1u, sizeof(uint32_t));
+    const size_t nsorted = proto.kind == 0 ? ((size_t) proto.rows + proto.B - 1u) / proto.B : proto.rows;
+    uint8_t *sorted = (uint8_t *) malloc(nsorted + 1u);
     mom_task *tasks = (mom_task *) calloc((size_t) nthreads, sizeof(mom_task));
     pthread_t *th = (pthread_t *) calloc((size_t) nthreads, sizeof(pthread_t));
-    if (tasks == NULL || th == NULL) return 0;
-    int ok = 1;
+    if (n == NULL || sorted == NULL || tasks == NULL || th == NULL) {
+        free(n);
+        free(sorted);
+        free(tasks);
+        free(th);
+        return 0;
+    }
+    for (uint32_t r = 0; r < proto.rows; ++r) {
+        if (proto.row_keep != NULL && proto.row_keep[r] == 0u) continue;
+        const uint32_t g = proto.labels != NULL ? proto.labels[r] : 0u;
+        if (g < proto.G) n[g] += 1u;
+    }
+    const uint32_t W = proto.kind == 0 ? proto.ell_cols / proto.B : 0u;
+    for (size_t u = 0; u < nsorted; ++u) {
+        const uint32_t *a = proto.kind == 0 ? proto.bci + u * W : proto.idx + proto.ptr[u];
+        const uint32_t len = proto.kind == 0 ? W : proto.ptr[u + 1u] - proto.ptr[u];
+        uint8_t ok = 1u;
+        for (uint32_t j = 1; j < len && ok; ++j) ok = a[j - 1u] <= a[j];
+        sorted[u] = ok;
+    }
     for (int t = 0; t < nthreads; ++t) {
         tasks[t] = proto;
-        tasks[t].r0 = (uint32_t) (((uint64_t) proto.rows * (uint64_t) t) / (uint64_t) nthreads);
-        tasks[t].r1 = (uint32_t) (((uint64_t) proto.rows * (uint64_t) (t + 1)) / (uint64_t) nthreads);
-        tasks[t].s = (double *) calloc(gc + 1u, sizeof(double));
-        tasks[t].q = (double *) calloc(gc + 1u, sizeof(double));
-        tasks[t].n = (uint32_t *) calloc((size_t) proto.G + 1u, sizeof(uint32_t));
-        if (tasks[t].s == NULL || tasks[t].q == NULL || tasks[t].n == NULL) ok = 0;
+        tasks[t].sorted = sorted;
+        tasks[t].fk = fk;
+        tasks[t].ddof = ddof;
+        tasks[t].group_rows = n;
+        const uint64_t u0 = (uint64_t) units * (uint64_t) t / (uint64_t) nthreads;
+        const uint64_t u1 = (uint64_t) units * (uint64_t) (t + 1) / (uint64_t) nthreads;
+        tasks[t].f0 = (uint32_t) (u0 * unit < proto.cols ? u0 * unit : proto.cols);
+        tasks[t].f1 = (uint32_t) (u1 * unit < proto.cols ? u1 * unit : proto.cols);
+        tasks[t].sum = sum;
+        tasks[t].sumsq = sumsq;
+        tasks[t].mean = mean;
+        tasks[t].var = var;
     }
-    if (ok) {
-        for (int t = 1; t < nthreads; ++t) pthread_create(&th[t], NULL, mom_worker, &tasks[t]);
-        mom_worker(&tasks[0]);
-        for (int t = 1; t < nthreads; ++t) pthread_join(th[t], NULL);
-        for (uint32_t g = 0; g < proto.G; ++g) {
-            uint32_t n = 0u;
-            for (int t = 0; t < nthreads; ++t) n += tasks[t].n[g];
-            if (group_rows != NULL) group_rows[g] = n;
-            for (uint32_t f = 0; f < proto.cols; ++f) {
-                const size_t k = (size_t) g * proto.cols + f;
-                double s = 0.0, q = 0.0;
-                for (int t = 0; t < nthreads; ++t) {
-                    s += tasks[t].s[k];
-                    q += tasks[t].q[k];
-                }
-                if (fk != NULL && fk[f] == 0u) s = q = 0.0;
-                double m = 0.0, v = 0.0;
-                if (n > 0u && (fk == NULL || fk[f] != 0u)) {
-                    m = s / (double) n;
-                    if (n > ddof) {
-                        double m2 = q - s * m;
-                        if (m2 < 0.0) m2 = 0.0;
-                        v = m2 / (double) (n - ddof);
-                    }
-                }
-                sum[k] = s;
-                sumsq[k] = q;
-                if (mean != NULL) mean[k] = m;
-                if (var != NULL) var[k] = v;
-            }
-        }
-    }
-    for (int t = 0; t < nthreads; ++t) {
-        free(tasks[t].s);
-        free(tasks[t].q);
-        free(tasks[t].n);
-    }
+    for (int t = 1; t < nthreads; ++t) pthread_create(&th[t], NULL, mom_worker, &tasks[t]);
+    mom_worker(&tasks[0]);
+    for (int t = 1; t < nthreads; ++t) pthread_join(th[t], NULL);
+    if (group_rows != NULL)
+        for (uint32_t g = 0; g < proto.G; ++g) group_rows[g] = n[g];
+    free(n);
+    free(sorted);
     free(tasks);
     free(th);
-    return ok;
+    return 1;
 }
 
 int cso_group_moments_bell(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,

@@ -49,6 +49,8 @@ int main(void) {
   S(cs_blocked_ell_tune_result) S(cs_sliced_ell_tune_result)
   S(cs_row_feature_mask_view) S(cs_group_filter_params) S(cs_group_reduce_out)
   S(cs_group_moments_params) S(cs_group_moments_out)
+  S(cs_batch_part) O(cs_batch_part, d_major_nnz) O(cs_batch_part, d_pow2_offsets)
+  S(cs_batch_tiles) S(cs_batch_sliced_result) O(cs_batch_sliced_result, view)
   return 0;
 }
 """
@@ -67,6 +69,9 @@ PAIRS = {
     "cs_group_reduce_out": _abi.GroupReduceOut,
     "cs_group_moments_params": _abi.GroupMomentsParams,
     "cs_group_moments_out": _abi.GroupMomentsOut,
+    "cs_batch_part": _abi.BatchPart,
+    "cs_batch_tiles": _abi.BatchTiles,
+    "cs_batch_sliced_result": _abi.BatchSlicedResult,
 }
 
 
@@ -85,6 +90,9 @@ def test_ctypes_layouts_match_c(tmp_path):
     assert got["cs_sliced_ell_view.val"] == _abi.SlicedEllView.val.offset
     assert got["cs_host_compressed.val"] == _abi.HostCompressed.val.offset
     assert got["cs_host_sliced_ell.val"] == _abi.HostSlicedEll.val.offset
+    assert got["cs_batch_part.d_major_nnz"] == _abi.BatchPart.d_major_nnz.offset
+    assert got["cs_batch_part.d_pow2_offsets"] == _abi.BatchPart.d_pow2_offsets.offset
+    assert got["cs_batch_sliced_result.view"] == _abi.BatchSlicedResult.view.offset
 
 
 def test_abi_version_and_host_validation(cs_lib):
