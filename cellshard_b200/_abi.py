@@ -161,6 +161,7 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_batch_sliced_run": (C.c_int, [vp, vp]),
     "cs_b200_batch_sliced_results": (C.c_int, [vp, P(BatchSlicedResult), P(u32), P(u32), vp]),
     "cs_b200_batch_sliced_next_wave": (C.c_int, [vp, vp, u64, P(u32)]),
+    "cs_b200_batch_sliced_reset": (C.c_int, [vp, vp, u64]),
     "cs_b200_batch_sliced_tiles": (C.c_int, [vp, P(BatchTiles), P(u32), P(u32)]),
     "cs_b200_batch_sliced_destroy": (None, [vp]),
 }

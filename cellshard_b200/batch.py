@@ -139,6 +139,13 @@ class BatchSlicedConverter:
                                                            C.byref(n)), "batch_sliced_next_wave")
         return n.value
 
+    def reset(self, arena: torch.Tensor | None = None) -> None:
+        """All partitions form the next wave again."""
+        if arena is not None:
+            self.arena = arena
+        _abi.check(self.lib.cs_b200_batch_sliced_reset(self.handle, self.arena.data_ptr(), self.arena.numel()),
+                   "batch_sliced_reset")
+
     def raw_results(self):
         res = (_abi.BatchSlicedResult * max(len(self.parts), 1))()
         d, e = _abi.u32(), _abi.u32()

@@ -889,6 +889,18 @@ extern "C" int cs_b200_batch_sliced_next_wave(cs_batch_plan *plan, void *d_arena
     return build_wave(plan);
 }
 
+extern "C" int cs_b200_batch_sliced_reset(cs_batch_plan *plan, void *d_arena, uint64_t arena_bytes) {
+    if (plan == nullptr || d_arena == nullptr || ((uintptr_t) d_arena & 255u) != 0u) {
+        set_error("batch_sliced_reset: null plan or unaligned arena");
+        return 0;
+    }
+    plan->wave.clear();
+    for (uint32_t i = 0; i < plan->count; ++i) plan->wave.push_back(i);
+    plan->arena = static_cast<unsigned char *>(d_arena);
+    plan->arena_bytes = arena_bytes;
+    return build_wave(plan);
+}
+
 extern "C" int cs_b200_batch_sliced_autotune(cs_batch_plan *plan, cs_stream_t s, cs_batch_tiles *chosen) {
     if (plan == nullptr) {
         set_error("batch_sliced_autotune: no plan");

@@ -655,6 +655,8 @@ CS_API int cs_b200_batch_sliced_results(cs_batch_plan *plan, cs_batch_sliced_res
  * (or the same, once its blocks are consumed) arena. */
 CS_API int cs_b200_batch_sliced_next_wave(cs_batch_plan *plan, void *d_arena, uint64_t arena_bytes,
                                           uint32_t *wave_size);
+/* Every partition becomes the next wave again (e.g. to rerun the batch). */
+CS_API int cs_b200_batch_sliced_reset(cs_batch_plan *plan, void *d_arena, uint64_t arena_bytes);
 CS_API int cs_b200_batch_sliced_tiles(const cs_batch_plan *plan, cs_batch_tiles *out, uint32_t *grid,
                                       uint32_t *items);
 CS_API void cs_b200_batch_sliced_destroy(cs_batch_plan *plan);

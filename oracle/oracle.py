@@ -186,6 +186,27 @@ def sliced_padded_slots(rows, ptr, candidate):
     return int(f(u32(rows), _p(ptr), u32(candidate)))
 
 
+def choose_sliced_slice_rows(rows, nnz, ptr, candidates):
+    """Restated convert::choose_sliced_ell_slice_rows_from_compressed
+    (src/convert/sliced_ell_from_blocked_ell.cuh:64-109,196-221): per candidate
+    h clamped to [1, rows], score = padded_slots / nnz + 0.25 * slices / rows;
+    lower score (1e-12 slack), then fewer padded bytes, then larger h.
+    Returns (h, score, padded_bytes)."""
+    best = None
+    for h in candidates:
+        if h == 0:
+            continue
+        hh = max(1, min(h, rows))
+        S = (rows + hh - 1) // hh
+        padded = sliced_padded_slots(rows, ptr, hh)
+        nbytes = padded * 6 + (2 * S + 1) * 4
+        score = (1.0 if nnz == 0 else padded / nnz) + 0.25 * (S / rows)
+        if (best is None or score + 1e-12 < best[1] or (score <= best[1] + 1e-12 and nbytes < best[2])
+                or (score <= best[1] + 1e-12 and nbytes == best[2] and hh > best[0])):
+            best = (hh, score, nbytes)
+    return best
+
+
 def csr_transpose(cDim, uDim, ptr, idx, val):
     nnz = int(ptr[cDim]) if cDim else 0
     out_ptr = np.zeros(uDim + 1, np.uint32)

@@ -35,17 +35,7 @@ def _device(parts):
 
 
 def _choose(orc, rows, nnz, ptr, cands):
-    best = None
-    for h in cands:
-        hh = max(1, min(h, rows))
-        S = (rows + hh - 1) // hh
-        padded = orc.sliced_padded_slots(rows, ptr, hh)
-        nbytes = padded * 6 + (2 * S + 1) * 4
-        score = (1.0 if nnz == 0 else padded / nnz) + 0.25 * (S / rows)
-        if (best is None or score + 1e-12 < best[1] or (score <= best[1] + 1e-12 and nbytes < best[2])
-                or (score <= best[1] + 1e-12 and nbytes == best[2] and hh > best[0])):
-            best = (hh, score, nbytes)
-    return best
+    return orc.choose_sliced_slice_rows(rows, nnz, ptr, cands)
 
 
 def _check_part(orc, hp, res, bucket_count=16):
@@ -140,6 +130,13 @@ def test_batch_waves_defer_and_finish(cuda, orc):
         assert waves < len(hp) + 1
         conv.next_wave(torch.empty_like(conv.arena))
     assert waves > 1 and len(done) == len(hp)
+    # reset: every partition forms one wave again in an arena that holds them all
+    conv.reset(torch.empty(sum(b) + 4096, dtype=torch.uint8, device="cuda"))
+    conv.run()
+    results, deferred, err = conv.results()
+    assert deferred == 0 and err == 0
+    for h, r in zip(hp, results):
+        _check_part(orc, h, r)
     # a partition larger than the whole arena is refused, not deferred forever
     tiny = BatchSlicedConverter(dev[:2], CANDS, arena_bytes=4096)
     tiny.run()
