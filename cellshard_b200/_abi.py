@@ -100,6 +100,26 @@ class BatchSlicedResult(C.Structure):
                 ("view", SlicedEllView)]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [("scratch_budget_bytes", u64), ("max_inflight", u32), ("chunk_rows", u32), ("idle_exit_us", u32),
+                ("ctas_per_sm", u32)]
+
+
+class ServeRequest(C.Structure):
+    _fields_ = [("group_count", u32), ("scheme", u32), ("ddof", u32), ("flags", u32), ("row_keep", vp),
+                ("row_labels", vp), ("feature_keep", vp), ("sum", vp), ("sumsq", vp), ("mean", vp), ("var", vp),
+                ("group_rows", vp)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("admitted", u64), ("completed", u64), ("pending", u64), ("kernel_launches", u64),
+                ("scratch_in_use", u64), ("scratch_budget", u64), ("device_error", u32), ("pad", u32)]
+
+
+SERVE_DEVICE_INPUTS = 1
+SERVE_DEVICE_OUTPUTS = 2
+SERVE_QUEUED, SERVE_RUNNING, SERVE_DONE = 0, 1, 2
+
 BATCH_DEFERRED = 1 << 8
 BATCH_WAIT_TIMEOUT = 1 << 9
 BATCH_TOO_LARGE = 1 << 10
@@ -164,6 +184,15 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_batch_sliced_reset": (C.c_int, [vp, vp, u64]),
     "cs_b200_batch_sliced_tiles": (C.c_int, [vp, P(BatchTiles), P(u32), P(u32)]),
     "cs_b200_batch_sliced_destroy": (None, [vp]),
+    "cs_b200_serve_open": (C.c_int, [P(BlockedEllView), u32, P(ServeConfig), P(vp)]),
+    "cs_b200_serve_submit": (C.c_int, [vp, P(ServeRequest), P(u64)]),
+    "cs_b200_serve_poll": (C.c_int, [vp, u64, P(u32), P(C.c_double)]),
+    "cs_b200_serve_wait": (C.c_int, [vp, u64, u32, P(C.c_double)]),
+    "cs_b200_serve_release": (C.c_int, [vp, u64]),
+    "cs_b200_serve_stats": (C.c_int, [vp, P(ServeStats)]),
+    "cs_b200_serve_run_trace": (C.c_int, [vp, P(ServeRequest), P(u32), P(C.c_double), u32, P(C.c_double),
+                                          P(C.c_double)]),
+    "cs_b200_serve_close": (None, [vp]),
 }
 
 

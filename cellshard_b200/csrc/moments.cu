@@ -19,6 +19,7 @@
 //                fp32 by scheme), apply the feature mask, emit sum, sumsq,
 //                mean and variance.
 #include "common.cuh"
+#include "moments_device.cuh"
 
 #include <cstring>
 
@@ -280,62 +281,6 @@ __global__ void __launch_bounds__(kSortThreads) moments_tile_scatter_kernel(uint
 // ---------------------------------------------------------------------------
 // 3. Accumulation.
 // ---------------------------------------------------------------------------
-// Raw loads of L consecutive fp16 values (kept as packed words so a batch of
-// rows can be in flight before any conversion).
-template <int L>
-struct raw_vec {
-    static constexpr int W = (L + 1) / 2; // 32-bit words
-    uint32_t w[W];
-};
-
-template <int L>
-__device__ __forceinline__ void load_raw(const uint16_t *p, raw_vec<L> &r) {
-    if constexpr (L == 8) {
-        const uint4 v = ld_stream_v4(p);
-        r.w[0] = v.x;
-        r.w[1] = v.y;
-        r.w[2] = v.z;
-        r.w[3] = v.w;
-    } else if constexpr (L == 4) {
-        const uint2 v = __ldg(reinterpret_cast<const uint2 *>(p));
-        r.w[0] = v.x;
-        r.w[1] = v.y;
-    } else if constexpr (L == 2) {
-        r.w[0] = __ldg(reinterpret_cast<const unsigned int *>(p));
-    } else {
-        r.w[0] = __ldg(reinterpret_cast<const unsigned short *>(p));
-    }
-}
-
-template <int L>
-__device__ __forceinline__ void zero_raw(raw_vec<L> &r) {
-#pragma unroll
-    for (int i = 0; i < raw_vec<L>::W; ++i) r.w[i] = 0u;
-}
-
-template <int L>
-__device__ __forceinline__ void unpack(const raw_vec<L> &r, float *x) {
-    if constexpr (L == 1) {
-        x[0] = h2f((uint16_t) r.w[0]);
-    } else {
-#pragma unroll
-        for (int i = 0; i < L / 2; ++i) {
-            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&r.w[i]));
-            x[2 * i] = f.x;
-            x[2 * i + 1] = f.y;
-        }
-    }
-}
-
-// Knuth two-sum folded into a running (hi, lo) pair.
-__device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float b) {
-    const float s = __fadd_rn(hi, b);
-    const float bb = __fsub_rn(s, hi);
-    const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bb)), __fsub_rn(b, bb));
-    hi = s;
-    lo = __fadd_rn(lo, err);
-}
-
 template <int L, bool COMP>
 __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
     const uint16_t *__restrict__ val, uint32_t ell_cols, uint32_t block_size, uint32_t col_blocks, uint32_t words,
@@ -701,6 +646,32 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
 }
 
 namespace csb {
+
+// Column-block index of a Blocked-ELL partition (index[rb * words + w] =
+// (occupancy bits of column blocks 32w..32w+31, slots before them)), as the
+// moments prepare phase builds it; used by the serving loop, which keeps one
+// per staged partition.  words = ceil(ceil(cols / block_size) / 32).
+int build_column_block_index(const cs_blocked_ell_view *src, uint2 *index, uint32_t *status, cudaStream_t stream) {
+    const uint32_t B = src->block_size;
+    const uint32_t row_blocks = (src->rows + B - 1u) / B;
+    const uint32_t col_blocks = (src->cols + B - 1u) / B;
+    const uint32_t words = (col_blocks + 31u) / 32u;
+    if (row_blocks == 0u || words == 0u) return 1;
+    const uint32_t width = src->ell_cols / B;
+    if (width == 0u)
+        return cuda_ok(cudaMemsetAsync(index, 0, (std::size_t) row_blocks * words * sizeof(uint2), stream),
+                       "index memset");
+    const uint32_t blocks = (row_blocks + kIndexWarps - 1u) / kIndexWarps;
+    const std::size_t smem = (std::size_t) kIndexWarps * words * sizeof(uint32_t);
+    if (smem > 48u * 1024u &&
+        !cuda_ok(cudaFuncSetAttribute(moments_index_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem),
+                 "index smem attribute"))
+        return 0;
+    moments_index_kernel<<<blocks, kIndexWarps * 32, smem, stream>>>(
+        src->blockColIdx, row_blocks, width, col_blocks, words, index, status,
+        (width % 4u) == 0u && (reinterpret_cast<uintptr_t>(src->blockColIdx) & 15u) == 0u);
+    return launch_ok("moments_index_kernel");
+}
 
 // Scratch bytes the moments reduction needs for (src, params); 0 when the
 // arguments are invalid (the error message is set).

@@ -661,6 +661,74 @@ CS_API int cs_b200_batch_sliced_tiles(const cs_batch_plan *plan, cs_batch_tiles 
                                       uint32_t *items);
 CS_API void cs_b200_batch_sliced_destroy(cs_batch_plan *plan);
 
+/* ------------------------------------------------------------------------ */
+/* Serving: masked grouped moments requests over staged Blocked-ELL          */
+/* partitions (no reference counterpart).  A device-resident persistent      */
+/* kernel runs every admitted request as a dataflow of work items (label     */
+/* histogram, scan, stable scatter, chunk accumulation, combine) that it     */
+/* appends to its own device queue; the host scheduler admits requests from  */
+/* a FIFO when a slot and their scratch fit the HBM budget, copies inputs    */
+/* and results on a copy stream that overlaps the kernel, and relaunches the */
+/* kernel after it exits on idle.  Results per request are the same bits     */
+/* alone and in any mix.                                                      */
+/* ------------------------------------------------------------------------ */
+typedef struct cs_server cs_server;
+
+typedef struct cs_serve_config {
+    uint64_t scratch_budget_bytes; /* HBM for admitted requests (0 = 16 GiB) */
+    uint32_t max_inflight;         /* request slots (0 = 32, at most 256) */
+    uint32_t chunk_rows;           /* rows per accumulation chunk (0 = 2048, at most 2048) */
+    uint32_t idle_exit_us;         /* the persistent kernel exits after this idle time (0 = 20000) */
+    uint32_t ctas_per_sm;          /* 0 = occupancy */
+} cs_serve_config;
+
+enum {
+    CS_SERVE_DEVICE_INPUTS = 1u,  /* row_keep / row_labels / feature_keep are device pointers */
+    CS_SERVE_DEVICE_OUTPUTS = 2u  /* outputs are device pointers (no copy back) */
+};
+
+enum { CS_SERVE_QUEUED = 0u, CS_SERVE_RUNNING = 1u, CS_SERVE_DONE = 2u };
+
+/* One request over the concatenation of the staged partitions (global rows
+ * in partition order).  Host inputs and outputs must stay valid until the
+ * request is done; pinned memory makes their copies asynchronous. */
+typedef struct cs_serve_request {
+    uint32_t group_count;           /* 1..1024 */
+    uint32_t scheme;                /* CS_MOMENTS_* */
+    uint32_t ddof;
+    uint32_t flags;                 /* CS_SERVE_* */
+    const uint8_t *row_keep;        /* [total rows] or NULL = all */
+    const uint32_t *row_labels;     /* [total rows] or NULL = group 0; labels >= group_count are skipped */
+    const uint8_t *feature_keep;    /* [cols] or NULL = all */
+    float *sum, *sumsq;             /* [group_count x cols], required */
+    float *mean, *var;              /* [group_count x cols] or NULL */
+    uint32_t *group_rows;           /* [group_count] or NULL */
+} cs_serve_request;
+
+typedef struct cs_serve_stats {
+    uint64_t admitted, completed, pending, kernel_launches;
+    uint64_t scratch_in_use, scratch_budget;
+    uint32_t device_error, pad;
+} cs_serve_stats;
+
+CS_API int cs_b200_serve_open(const cs_blocked_ell_view *parts, uint32_t count, const cs_serve_config *config,
+                              cs_server **out);
+/* Queues a request (non-blocking); rejects one whose scratch exceeds the budget. */
+CS_API int cs_b200_serve_submit(cs_server *server, const cs_serve_request *request, uint64_t *ticket);
+CS_API int cs_b200_serve_poll(cs_server *server, uint64_t ticket, uint32_t *state, double *latency_ms);
+/* Blocks until the ticket is done (results copied back); latency = submit -> done. */
+CS_API int cs_b200_serve_wait(cs_server *server, uint64_t ticket, uint32_t timeout_ms, double *latency_ms);
+/* Forgets a finished ticket. */
+CS_API int cs_b200_serve_release(cs_server *server, uint64_t ticket);
+CS_API int cs_b200_serve_stats(cs_server *server, cs_serve_stats *out);
+/* Submits requests[req_index[i]] at arrival_s[i] seconds after the call
+ * (open-loop arrivals), waits for all, returns per-request latency and the
+ * makespan. */
+CS_API int cs_b200_serve_run_trace(cs_server *server, const cs_serve_request *requests, const uint32_t *req_index,
+                                   const double *arrival_s, uint32_t n, double *latency_ms, double *makespan_s);
+/* Finishes admitted work (bounded), stops the kernel and frees everything. */
+CS_API void cs_b200_serve_close(cs_server *server);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -51,6 +51,7 @@ int main(void) {
   S(cs_group_moments_params) S(cs_group_moments_out)
   S(cs_batch_part) O(cs_batch_part, d_major_nnz) O(cs_batch_part, d_pow2_offsets)
   S(cs_batch_tiles) S(cs_batch_sliced_result) O(cs_batch_sliced_result, view)
+  S(cs_serve_config) S(cs_serve_request) O(cs_serve_request, group_rows) S(cs_serve_stats)
   return 0;
 }
 """
@@ -72,6 +73,9 @@ PAIRS = {
     "cs_batch_part": _abi.BatchPart,
     "cs_batch_tiles": _abi.BatchTiles,
     "cs_batch_sliced_result": _abi.BatchSlicedResult,
+    "cs_serve_config": _abi.ServeConfig,
+    "cs_serve_request": _abi.ServeRequest,
+    "cs_serve_stats": _abi.ServeStats,
 }
 
 
@@ -93,6 +97,7 @@ def test_ctypes_layouts_match_c(tmp_path):
     assert got["cs_batch_part.d_major_nnz"] == _abi.BatchPart.d_major_nnz.offset
     assert got["cs_batch_part.d_pow2_offsets"] == _abi.BatchPart.d_pow2_offsets.offset
     assert got["cs_batch_sliced_result.view"] == _abi.BatchSlicedResult.view.offset
+    assert got["cs_serve_request.group_rows"] == _abi.ServeRequest.group_rows.offset
 
 
 def test_abi_version_and_host_validation(cs_lib):
