@@ -113,7 +113,8 @@ class ServeRequest(C.Structure):
 
 class ServeStats(C.Structure):
     _fields_ = [("admitted", u64), ("completed", u64), ("pending", u64), ("kernel_launches", u64),
-                ("scratch_in_use", u64), ("scratch_budget", u64), ("device_error", u32), ("pad", u32)]
+                ("scratch_in_use", u64), ("scratch_budget", u64), ("device_error", u32), ("pad", u32),
+                ("items", u64 * 8), ("item_ns", u64 * 8)]
 
 
 SERVE_DEVICE_INPUTS = 1
@@ -191,7 +192,7 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_serve_release": (C.c_int, [vp, u64]),
     "cs_b200_serve_stats": (C.c_int, [vp, P(ServeStats)]),
     "cs_b200_serve_run_trace": (C.c_int, [vp, P(ServeRequest), P(u32), P(C.c_double), u32, P(C.c_double),
-                                          P(C.c_double)]),
+                                          P(C.c_double), P(C.c_double)]),
     "cs_b200_serve_close": (None, [vp]),
 }
 

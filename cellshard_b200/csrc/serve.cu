@@ -1,8 +1,11 @@
 // Serving loop for masked grouped moments over staged Blocked-ELL partitions.
 //
-// A device-resident persistent kernel pulls work items from two rings: a
-// device ring that the kernel itself appends to, and a host ring in mapped
-// pinned memory that the host scheduler appends request starts to.  Every
+// A device-resident persistent kernel pulls work items from two rings in
+// device memory: a device ring that the kernel itself appends to, and a host
+// ring that the host scheduler appends request starts to with ordered copies
+// (item, sequence word, tail) on a control stream.  Nothing the kernel polls
+// lives in host memory: hundreds of resident CTAs polling over PCIe would
+// starve the result copies.  Every
 // request runs as a dataflow of items; the item that completes a stage
 // appends the next stage's items, so no item ever waits for another:
 //
@@ -63,6 +66,7 @@ constexpr uint32_t kServeBatch = 8;
 constexpr uint32_t kSeqSpin = 1u << 22;
 constexpr unsigned long long kDevRing = 1ull << 22;
 constexpr unsigned long long kHostRing = 1ull << 14;
+constexpr unsigned long long kOrphans = 1ull << 12;
 
 enum : uint32_t { IT_START = 1u, IT_HIST, IT_SCAN, IT_SCATTER, IT_ACC, IT_COMBINE };
 
@@ -106,9 +110,14 @@ struct sparams {
     uint32_t col_blocks, words, tiles, pad;
     sreq *reqs;
     squeue dq, hq;
-    const volatile uint32_t *stop; // mapped
+    const volatile uint32_t *stop; // device memory, written by the host at close
     uint32_t *error;
     unsigned long long idle_ns;
+    unsigned long long *prof; // [16]: items per kind [0..7], device ns per kind [8..15]
+    unsigned long long *orph_head, *orph_tail; // tickets left by CTAs that exited on idle
+    unsigned long long *orph, *orph_seq;       // [kOrphans]
+    uint32_t *idle_ctas;                       // CTAs of this launch waiting for work
+    uint32_t *closing;                         // set once every CTA was idle: all exit
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -562,23 +571,89 @@ __device__ void do_combine(const sparams &P, ssmem &sm, uint32_t q, uint32_t g, 
     }
 }
 
+// one thread: take a ticket left by an exited CTA, if any
+__device__ bool claim_orphan(const sparams &P, unsigned long long &ticket) {
+    // retry until one is taken or none is left, so a launch's CTAs hold every
+    // orphaned ticket before any of them takes a fresh one
+    unsigned long long h = ld_acq_gpu64(P.orph_head);
+    while (true) {
+        if (h >= ld_acq_gpu64(P.orph_tail)) return false;
+        const unsigned long long seen = atomicCAS(P.orph_head, h, h + 1ull);
+        if (seen == h) break;
+        h = seen;
+    }
+    const unsigned long long slot = h & (kOrphans - 1ull);
+    for (uint32_t it = 0; it < kSeqSpin; ++it) {
+        if (ld_acq_gpu64(P.orph_seq + slot) == h + 1ull) {
+            ticket = __ldcg(P.orph + slot);
+            return true;
+        }
+        __nanosleep(64);
+    }
+    atomicOr(P.error, 8u); // an exiting CTA reserved an orphan slot and never filled it
+    return false;
+}
+
 __global__ void __launch_bounds__(kSThreads, 2) serve_kernel(sparams P) {
     extern __shared__ __align__(16) unsigned char serve_dyn[];
     __shared__ ssmem sm;
-    unsigned long long idle_since = 0ull;
+    // Device-ring items are taken by ticket: a CTA takes the next ring index
+    // with one atomicAdd (no compare-and-swap race between hundreds of CTAs)
+    // and waits for that slot's sequence word; tickets may run ahead of the
+    // tail, so waiting CTAs are served in order as items are appended.  The
+    // host ring (request starts only) is polled by compare-and-swap while a
+    // CTA waits on its ticket.  Exit is all-or-nothing: a CTA leaves only
+    // once every CTA of the launch has been idle for idle_ns (then it raises
+    // `closing` and the others follow), or on stop, or after a hard bound of
+    // 8 x idle_ns; its unfilled ticket goes to the orphan ring, which the next
+    // launch's CTAs drain before taking fresh tickets, so no item is lost.
+    unsigned long long idle_since = 0ull, ticket = 0ull;
+    bool have_ticket = false;
     while (true) {
         if (threadIdx.x == 0) {
             uint4 it = make_uint4(0u, 0u, 0u, 0u);
             bool got = false;
+            if (!have_ticket) {
+                if (!claim_orphan(P, ticket)) ticket = atomicAdd(P.dq.head, 1ull);
+                have_ticket = true;
+            }
+            atomicAdd(P.idle_ctas, 1u);
             while (true) {
-                got = try_pop(P.dq, false, it, P.error) || try_pop(P.hq, true, it, P.error);
-                if (got) break;
+                const unsigned long long slot = ticket & P.dq.mask;
+                if (ld_acq_gpu64(P.dq.seq + slot) == ticket + 1ull) {
+                    it = ld_volatile_v4(P.dq.slots + slot);
+                    have_ticket = false;
+                    got = true;
+                    break;
+                }
+                if (try_pop(P.hq, true, it, P.error)) {
+                    got = true;
+                    break;
+                }
                 const unsigned long long now = globaltimer();
                 if (idle_since == 0ull) idle_since = now;
-                if (*P.stop != 0u || now - idle_since > P.idle_ns) break;
-                __nanosleep(500);
+                const unsigned long long idle = now - idle_since;
+                bool leave = *P.stop != 0u || *reinterpret_cast<volatile uint32_t *>(P.closing) != 0u ||
+                             idle > 8ull * P.idle_ns;
+                if (!leave && idle > P.idle_ns &&
+                    *reinterpret_cast<volatile uint32_t *>(P.idle_ctas) >= gridDim.x) {
+                    atomicExch(P.closing, 1u);
+                    leave = true;
+                }
+                if (leave) {
+                    const unsigned long long k = atomicAdd(P.orph_tail, 1ull);
+                    P.orph[k & (kOrphans - 1ull)] = ticket;
+                    __threadfence();
+                    st_rel_gpu64(P.orph_seq + (k & (kOrphans - 1ull)), k + 1ull);
+                    have_ticket = false;
+                    break;
+                }
+                __nanosleep(200);
             }
-            if (got) idle_since = 0ull;
+            if (got) {
+                atomicSub(P.idle_ctas, 1u);
+                idle_since = 0ull;
+            }
             sm.item = got ? it : make_uint4(0u, 0u, 0u, 0u);
         }
         __syncthreads();
@@ -591,6 +666,7 @@ __global__ void __launch_bounds__(kSThreads, 2) serve_kernel(sparams P) {
             reinterpret_cast<uint4 *>(&sm.req)[threadIdx.x] = __ldcg(reinterpret_cast<const uint4 *>(P.reqs + q) +
                                                                        threadIdx.x);
         __syncthreads();
+        const unsigned long long t_item = threadIdx.x == 0 ? globaltimer() : 0ull;
         switch (kind) {
         case IT_START: do_start(P, sm, q); break;
         case IT_HIST: do_hist(P, sm, reinterpret_cast<uint32_t *>(serve_dyn), q, it.y); break;
@@ -601,6 +677,10 @@ __global__ void __launch_bounds__(kSThreads, 2) serve_kernel(sparams P) {
         default: atomicOr(P.error, 4u); break;
         }
         __syncthreads();
+        if (threadIdx.x == 0 && kind < 8u) {
+            atomicAdd(P.prof + kind, 1ull);
+            atomicAdd(P.prof + 8u + kind, globaltimer() - t_item);
+        }
     }
 }
 
@@ -630,7 +710,7 @@ struct ticket_rec {
     uint32_t max_chunks = 0;
     uint32_t state = CS_SERVE_QUEUED;
     uint32_t status = 0;
-    clk::time_point t_submit, t_admit, t_done;
+    clk::time_point t_submit, t_admit, t_start, t_device_done, t_done;
 };
 
 struct slot_rec {
@@ -668,13 +748,17 @@ struct cs_server {
     uint32_t *d_done = nullptr;
     uint32_t *h_zero = nullptr;   // pinned zeros
     // rings
-    unsigned long long *d_heads = nullptr; // [0] device ring head, [1] device ring tail, [2] host ring head
+    unsigned long long *d_heads = nullptr; // [0] device ring head, [1] tail, [2] host ring head, [3..4] orphans,
+                                           // [5] idle CTAs, [6] closing
     uint4 *d_dslots = nullptr;
     unsigned long long *d_dseq = nullptr;
-    uint4 *h_hslots = nullptr;
-    unsigned long long *h_hseq = nullptr;
-    unsigned long long *h_htail = nullptr; // mapped
-    uint32_t *h_stop = nullptr;            // mapped
+    uint4 *d_hslots = nullptr;             // host ring in device memory
+    unsigned long long *d_hseq = nullptr;
+    unsigned long long *d_htail = nullptr; // [0] tail, [1] stop word
+    unsigned char *h_push = nullptr;       // pinned staging of host-ring writes (32 B per slot)
+    cudaStream_t pstream = nullptr;        // control stream for host-ring writes
+    unsigned long long *d_prof = nullptr;
+    unsigned long long *d_orph = nullptr; // [2 * kOrphans]: tickets, sequence words
     uint32_t *d_error = nullptr;
     unsigned long long host_tail = 0;
     // requests
@@ -779,16 +863,17 @@ bool launch_kernel(cs_server *s) {
     P.tiles = s->tiles;
     P.reqs = s->d_reqs;
     P.dq = squeue{s->d_heads + 0, s->d_heads + 1, s->d_dslots, s->d_dseq, kDevRing - 1ull};
-    unsigned long long *htail = nullptr;
-    uint4 *hslots = nullptr;
-    unsigned long long *hseq = nullptr;
-    uint32_t *stop = nullptr;
-    cudaHostGetDevicePointer((void **) &htail, s->h_htail, 0);
-    cudaHostGetDevicePointer((void **) &hslots, s->h_hslots, 0);
-    cudaHostGetDevicePointer((void **) &hseq, s->h_hseq, 0);
-    cudaHostGetDevicePointer((void **) &stop, s->h_stop, 0);
-    P.hq = squeue{s->d_heads + 2, htail, hslots, hseq, kHostRing - 1ull};
-    P.stop = stop;
+    P.hq = squeue{s->d_heads + 2, s->d_htail, s->d_hslots, s->d_hseq, kHostRing - 1ull};
+    P.stop = reinterpret_cast<const volatile uint32_t *>(s->d_htail + 1);
+    P.prof = s->d_prof;
+    P.orph_head = s->d_heads + 3;
+    P.orph_tail = s->d_heads + 4;
+    P.orph = s->d_orph;
+    P.orph_seq = s->d_orph + kOrphans;
+    P.idle_ctas = reinterpret_cast<uint32_t *>(s->d_heads + 5);
+    P.closing = reinterpret_cast<uint32_t *>(s->d_heads + 6);
+    // a new launch starts with no idle CTAs and no exit in progress
+    cudaMemcpyAsync(s->d_heads + 5, s->h_zero, 16, cudaMemcpyHostToDevice, s->kstream);
     P.error = s->d_error;
     P.idle_ns = (unsigned long long) (s->cfg.idle_exit_us ? s->cfg.idle_exit_us : 20000u) * 1000ull;
     serve_kernel<<<s->grid, kSThreads, kServeDynSmem, s->kstream>>>(P);
@@ -801,20 +886,21 @@ bool launch_kernel(cs_server *s) {
 
 bool kernel_running(cs_server *s) { return s->kernel_launched && cudaEventQuery(s->kdone) == cudaErrorNotReady; }
 
+// item, then its sequence word, then the tail: three copies in stream order,
+// each complete before the next starts, so a consumer that sees the tail sees
+// the item.  The staging slot is reused only kHostRing pushes later.
 void push_host_item(cs_server *s, uint4 item) {
     const unsigned long long k = s->host_tail;
     const unsigned long long slot = k & (kHostRing - 1ull);
-    volatile uint4 *vs = s->h_hslots + slot;
-    vs->x = item.x;
-    vs->y = item.y;
-    vs->z = item.z;
-    vs->w = item.w;
-    std::atomic_thread_fence(std::memory_order_seq_cst);
-    reinterpret_cast<volatile unsigned long long *>(s->h_hseq)[slot] = k + 1ull;
-    std::atomic_thread_fence(std::memory_order_seq_cst);
-    s->host_tail = k + 1ull;
-    *reinterpret_cast<volatile unsigned long long *>(s->h_htail) = s->host_tail;
-    std::atomic_thread_fence(std::memory_order_seq_cst);
+    unsigned char *st = s->h_push + slot * 32u;
+    std::memcpy(st, &item, 16);
+    const unsigned long long seq = k + 1ull;
+    std::memcpy(st + 16, &seq, 8);
+    std::memcpy(st + 24, &seq, 8);
+    cudaMemcpyAsync(s->d_hslots + slot, st, 16, cudaMemcpyHostToDevice, s->pstream);
+    cudaMemcpyAsync(s->d_hseq + slot, st + 16, 8, cudaMemcpyHostToDevice, s->pstream);
+    cudaMemcpyAsync(s->d_htail, st + 24, 8, cudaMemcpyHostToDevice, s->pstream);
+    s->host_tail = seq;
 }
 
 // admission of the queue head; returns false when it does not fit now
@@ -911,10 +997,12 @@ void sched_loop(cs_server *s) {
                 busy = true;
                 if (sr.state == SLOT_COPY_IN && cudaEventQuery(sr.ev) == cudaSuccess) {
                     push_host_item(s, make_uint4(IT_START | ((uint32_t) i << 8), 0u, 0u, 0u));
+                    s->tickets[sr.ticket].t_start = clk::now();
                     sr.state = SLOT_RUNNING;
                 } else if (sr.state == SLOT_RUNNING &&
                            reinterpret_cast<volatile uint32_t *>(s->h_done)[i] != 0u) {
                     ticket_rec &t = s->tickets[sr.ticket];
+                    t.t_device_done = clk::now();
                     const cs_serve_request &r = t.req;
                     if ((r.flags & CS_SERVE_DEVICE_OUTPUTS) == 0u) {
                         const std::size_t gc = (std::size_t) r.group_count * s->cols * 4u;
@@ -1035,17 +1123,21 @@ extern "C" int cs_b200_serve_open(const cs_blocked_ell_view *parts, uint32_t cou
              cuda_ok(cudaMalloc(&s->d_dslots, sizeof(uint4) * kDevRing), "serve ring") &&
              cuda_ok(cudaMalloc(&s->d_dseq, 8u * kDevRing), "serve ring seq") &&
              cuda_ok(cudaMemset(s->d_dseq, 0, 8u * kDevRing), "ring seq clear") &&
-             cuda_ok(cudaHostAlloc(&s->h_hslots, sizeof(uint4) * kHostRing, cudaHostAllocMapped), "host ring") &&
-             cuda_ok(cudaHostAlloc(&s->h_hseq, 8u * kHostRing, cudaHostAllocMapped), "host ring seq") &&
-             cuda_ok(cudaHostAlloc(&s->h_htail, 64, cudaHostAllocMapped), "host ring tail") &&
-             cuda_ok(cudaHostAlloc(&s->h_stop, 64, cudaHostAllocMapped), "stop word") &&
+             cuda_ok(cudaMalloc(&s->d_hslots, sizeof(uint4) * kHostRing), "host ring") &&
+             cuda_ok(cudaMalloc(&s->d_hseq, 8u * kHostRing), "host ring seq") &&
+             cuda_ok(cudaMemset(s->d_hseq, 0, 8u * kHostRing), "host ring seq clear") &&
+             cuda_ok(cudaMalloc(&s->d_htail, 64), "host ring tail") &&
+             cuda_ok(cudaMemset(s->d_htail, 0, 64), "host ring tail clear") &&
+             cuda_ok(cudaHostAlloc(&s->h_push, 32u * kHostRing, cudaHostAllocDefault), "host ring staging") &&
+             cuda_ok(cudaStreamCreateWithFlags(&s->pstream, cudaStreamNonBlocking), "serve control stream") &&
+             cuda_ok(cudaMalloc(&s->d_prof, 16u * 8u), "serve profile") &&
+             cuda_ok(cudaMalloc(&s->d_orph, 16u * kOrphans), "serve orphans") &&
+             cuda_ok(cudaMemset(s->d_orph, 0, 16u * kOrphans), "serve orphans clear") &&
+             cuda_ok(cudaMemset(s->d_prof, 0, 16u * 8u), "serve profile clear") &&
              cuda_ok(cudaMalloc(&s->d_error, 4), "serve error") && cuda_ok(cudaMemset(s->d_error, 0, 4), "error");
     if (ok) {
         std::memset(s->h_zero, 0, 64);
         std::memset(s->h_done, 0, 4u * S);
-        std::memset(s->h_hseq, 0, 8u * kHostRing);
-        std::memset(s->h_htail, 0, 64);
-        std::memset(s->h_stop, 0, 64);
         s->pool_bytes = s->cfg.scratch_budget_bytes;
         ok = cuda_ok(cudaMalloc(&s->pool, s->pool_bytes), "serve scratch pool");
         if (ok) s->free_blocks[0] = s->pool_bytes;
@@ -1178,13 +1270,20 @@ extern "C" int cs_b200_serve_stats(cs_server *s, cs_serve_stats *out) {
     out->scratch_in_use = s->pool_used;
     out->scratch_budget = s->pool_bytes;
     uint32_t err = 0u;
+    unsigned long long prof[16] = {0};
     cudaMemcpy(&err, s->d_error, 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(prof, s->d_prof, sizeof(prof), cudaMemcpyDeviceToHost);
     out->device_error = err;
+    for (int k = 0; k < 8; ++k) {
+        out->items[k] = prof[k];
+        out->item_ns[k] = prof[8 + k];
+    }
     return 1;
 }
 
 extern "C" int cs_b200_serve_run_trace(cs_server *s, const cs_serve_request *reqs, const uint32_t *req_index,
-                                       const double *arrival_s, uint32_t n, double *latency_ms, double *makespan_s) {
+                                       const double *arrival_s, uint32_t n, double *latency_ms, double *makespan_s,
+                                       double *phase_ms) {
     if (s == nullptr || reqs == nullptr || req_index == nullptr || arrival_s == nullptr) {
         set_error("serve_run_trace: null argument");
         return 0;
@@ -1202,11 +1301,22 @@ extern "C" int cs_b200_serve_run_trace(cs_server *s, const cs_serve_request *req
     }
     for (uint32_t i = 0; i < n; ++i) {
         double ms = 0.0;
-        if (!cs_b200_serve_wait(s, tk[i], 600000u, &ms)) return 0;
+        if (!cs_b200_serve_wait(s, tk[i], 120000u, &ms)) return 0;
         if (latency_ms) latency_ms[i] = ms;
     }
     const auto t1 = clk::now();
     if (makespan_s) *makespan_s = std::chrono::duration<double>(t1 - t0).count();
+    if (phase_ms) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t i = 0; i < n; ++i) {
+            const ticket_rec &t = s->tickets[tk[i]];
+            auto ms = [&](clk::time_point x) { return std::chrono::duration<double, std::milli>(x - t.t_submit).count(); };
+            phase_ms[4 * i + 0] = ms(t.t_admit);
+            phase_ms[4 * i + 1] = ms(t.t_start);
+            phase_ms[4 * i + 2] = ms(t.t_device_done);
+            phase_ms[4 * i + 3] = ms(t.t_done);
+        }
+    }
     for (uint32_t i = 0; i < n; ++i) cs_b200_serve_release(s, tk[i]);
     return 1;
 }
@@ -1227,7 +1337,11 @@ extern "C" void cs_b200_serve_close(cs_server *s) {
         s->quit.store(true);
         s->sched.join();
     }
-    if (s->h_stop) *reinterpret_cast<volatile uint32_t *>(s->h_stop) = 1u;
+    if (s->d_htail && s->h_zero && s->pstream) {
+        s->h_zero[8] = 1u;
+        cudaMemcpyAsync(s->d_htail + 1, s->h_zero + 8, 4, cudaMemcpyHostToDevice, s->pstream);
+        cudaStreamSynchronize(s->pstream);
+    }
     if (s->kstream) cudaStreamSynchronize(s->kstream);
     if (s->cstream) cudaStreamSynchronize(s->cstream);
     for (auto &sr : s->slots)
@@ -1241,10 +1355,13 @@ extern "C" void cs_b200_serve_close(cs_server *s) {
     if (s->d_heads) cudaFree(s->d_heads);
     if (s->d_dslots) cudaFree(s->d_dslots);
     if (s->d_dseq) cudaFree(s->d_dseq);
-    if (s->h_hslots) cudaFreeHost(s->h_hslots);
-    if (s->h_hseq) cudaFreeHost(s->h_hseq);
-    if (s->h_htail) cudaFreeHost(s->h_htail);
-    if (s->h_stop) cudaFreeHost(s->h_stop);
+    if (s->d_hslots) cudaFree(s->d_hslots);
+    if (s->d_hseq) cudaFree(s->d_hseq);
+    if (s->d_htail) cudaFree(s->d_htail);
+    if (s->h_push) cudaFreeHost(s->h_push);
+    if (s->d_prof) cudaFree(s->d_prof);
+    if (s->d_orph) cudaFree(s->d_orph);
+    if (s->pstream) cudaStreamDestroy(s->pstream);
     if (s->d_error) cudaFree(s->d_error);
     if (s->pool) cudaFree(s->pool);
     if (s->kdone) cudaEventDestroy(s->kdone);

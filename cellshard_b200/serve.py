@@ -93,14 +93,22 @@ class Server:
     def stats(self) -> dict:
         st = _abi.ServeStats()
         _abi.check(self.lib.cs_b200_serve_stats(self.handle, C.byref(st)), "serve_stats")
-        return {k: getattr(st, k) for k, _ in _abi.ServeStats._fields_ if k != "pad"}
+        out = {k: getattr(st, k) for k, _ in _abi.ServeStats._fields_ if k not in ("pad", "items", "item_ns")}
+        kinds = ["none", "start", "hist", "scan", "scatter", "acc", "combine", "other"]
+        out["items"] = {kinds[k]: int(st.items[k]) for k in range(1, 7)}
+        out["item_ms"] = {kinds[k]: st.item_ns[k] / 1e6 for k in range(1, 7)}
+        return out
 
-    def run_trace(self, requests: list[Request], req_index, arrival_s) -> tuple[np.ndarray, float]:
+    def run_trace(self, requests: list[Request], req_index, arrival_s):
+        """Open-loop arrivals; returns (latency ms [n], makespan s, phase ms [n, 4]: admitted,
+        started, device done, results on the host -- each measured from submit)."""
         n = len(req_index)
         arr = (_abi.ServeRequest * len(requests))(*[r.c for r in requests])
         idx = (_abi.u32 * n)(*[int(i) for i in req_index])
         at = (C.c_double * n)(*[float(a) for a in arrival_s])
         lat = (C.c_double * n)()
+        ph = (C.c_double * (4 * n))()
         mk = C.c_double()
-        _abi.check(self.lib.cs_b200_serve_run_trace(self.handle, arr, idx, at, n, lat, C.byref(mk)), "run_trace")
-        return np.frombuffer(lat, dtype=np.float64).copy(), mk.value
+        _abi.check(self.lib.cs_b200_serve_run_trace(self.handle, arr, idx, at, n, lat, C.byref(mk), ph), "run_trace")
+        return (np.frombuffer(lat, dtype=np.float64).copy(), mk.value,
+                np.frombuffer(ph, dtype=np.float64).reshape(n, 4).copy())

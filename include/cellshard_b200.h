@@ -709,6 +709,8 @@ typedef struct cs_serve_stats {
     uint64_t admitted, completed, pending, kernel_launches;
     uint64_t scratch_in_use, scratch_budget;
     uint32_t device_error, pad;
+    uint64_t items[8];   /* work items run, by kind (1 start, 2 hist, 3 scan, 4 scatter, 5 acc, 6 combine) */
+    uint64_t item_ns[8]; /* device time spent in them (sum over CTAs) */
 } cs_serve_stats;
 
 CS_API int cs_b200_serve_open(const cs_blocked_ell_view *parts, uint32_t count, const cs_serve_config *config,
@@ -722,10 +724,13 @@ CS_API int cs_b200_serve_wait(cs_server *server, uint64_t ticket, uint32_t timeo
 CS_API int cs_b200_serve_release(cs_server *server, uint64_t ticket);
 CS_API int cs_b200_serve_stats(cs_server *server, cs_serve_stats *out);
 /* Submits requests[req_index[i]] at arrival_s[i] seconds after the call
- * (open-loop arrivals), waits for all, returns per-request latency and the
- * makespan. */
+ * (open-loop arrivals), waits for all, returns per-request latency, the
+ * makespan and (phase_ms, nullable, 4 per request) the times from submit to
+ * admission, to the start item, to the device finishing, to results on the
+ * host. */
 CS_API int cs_b200_serve_run_trace(cs_server *server, const cs_serve_request *requests, const uint32_t *req_index,
-                                   const double *arrival_s, uint32_t n, double *latency_ms, double *makespan_s);
+                                   const double *arrival_s, uint32_t n, double *latency_ms, double *makespan_s,
+                                   double *phase_ms);
 /* Finishes admitted work (bounded), stops the kernel and frees everything. */
 CS_API void cs_b200_serve_close(cs_server *server);
 
