@@ -100,6 +100,11 @@ class BatchSlicedResult(C.Structure):
                 ("view", SlicedEllView)]
 
 
+class PartitionRecord(C.Structure):
+    _fields_ = [("allocation", vp), ("allocation_bytes", sz), ("view", vp), ("a0", vp), ("a1", vp), ("a2", vp),
+                ("a3", vp), ("device_id", C.c_int), ("format", u32), ("host_view", C.c_ubyte * 64)]
+
+
 class ServeConfig(C.Structure):
     _fields_ = [("scratch_budget_bytes", u64), ("max_inflight", u32), ("chunk_rows", u32), ("idle_exit_us", u32),
                 ("ctas_per_sm", u32)]
@@ -185,6 +190,13 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_batch_sliced_reset": (C.c_int, [vp, vp, u64]),
     "cs_b200_batch_sliced_tiles": (C.c_int, [vp, P(BatchTiles), P(u32), P(u32)]),
     "cs_b200_batch_sliced_destroy": (None, [vp]),
+    "cs_b200_device_partition_bytes_compressed": (C.c_int, [P(HostCompressed), P(sz)]),
+    "cs_b200_device_partition_bytes_blocked_ell": (C.c_int, [P(HostBlockedEll), P(sz)]),
+    "cs_b200_device_partition_bytes_sliced_ell": (C.c_int, [P(HostSlicedEll), P(sz)]),
+    "cs_b200_upload_compressed": (C.c_int, [P(HostCompressed), P(PartitionRecord), vp]),
+    "cs_b200_upload_blocked_ell": (C.c_int, [P(HostBlockedEll), P(PartitionRecord), vp]),
+    "cs_b200_upload_sliced_ell": (C.c_int, [P(HostSlicedEll), P(PartitionRecord), vp]),
+    "cs_b200_release_partition": (C.c_int, [P(PartitionRecord)]),
     "cs_b200_serve_open": (C.c_int, [P(BlockedEllView), u32, P(ServeConfig), P(vp)]),
     "cs_b200_serve_submit": (C.c_int, [vp, P(ServeRequest), P(u64)]),
     "cs_b200_serve_poll": (C.c_int, [vp, u64, P(u32), P(C.c_double)]),

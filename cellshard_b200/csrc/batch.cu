@@ -226,8 +226,7 @@ __device__ void do_choose(const bparams &P, bsmem &sm, uint32_t pi) {
     const bool ready = sm.flag != 0u;
     __syncthreads();
     const uint32_t rows = p.rows;
-    // padded slots per candidate
-    unsigned long long padded[CS_BATCH_MAX_CANDIDATES] = {0ull, 0ull, 0ull, 0ull};
+    // padded slots per candidate (per-warp partial sums)
     if (ready) {
 #pragma unroll
         for (uint32_t k = 0; k < CS_BATCH_MAX_CANDIDATES; ++k) {
@@ -257,7 +256,6 @@ __device__ void do_choose(const bparams &P, bsmem &sm, uint32_t pi) {
                 if (h == 0u) continue;
                 unsigned long long slots = 0ull;
                 for (unsigned w = 0; w < kBWarps; ++w) slots += sm.red[w][k];
-                padded[k] = slots;
                 const uint32_t S = (rows + h - 1u) / h;
                 const unsigned long long bytes = slots * 6ull + ((unsigned long long) S * 2ull + 1ull) * 4ull;
                 // the reference's score in IEEE doubles, no contraction:

@@ -58,7 +58,6 @@ namespace {
 constexpr unsigned kSThreads = 256;
 constexpr unsigned kSWarps = kSThreads / 32;
 constexpr uint32_t kServeTile = 8192;        // rows per HIST / SCATTER tile
-constexpr uint32_t kServeFeatTile = kSThreads * 8u; // features per ACC item (8 per thread)
 constexpr uint32_t kServeCombFeat = 2048;    // features per COMBINE item
 constexpr uint32_t kServeMaxGroups = 1024;
 constexpr uint32_t kServeMaxChunkRows = 2048;

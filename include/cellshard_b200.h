@@ -583,6 +583,38 @@ CS_API int cs_b200_synth_csr(uint32_t rows,
                       cs_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Partition staging: replaces device::upload / release for the compressed,   */
+/* Blocked-ELL and Sliced-ELL formats and device_partition_bytes              */
+/* (runtime/device/sharded_device.cuh:343-756, 959-991, 1050-1083).  One      */
+/* packed device allocation per partition: the device view descriptor, then   */
+/* the payload arrays on 256-byte boundaries.  The upload synchronises the    */
+/* given stream before returning, as device::upload does.  The Sliced-ELL     */
+/* view gets its uniform slice height and u32 slot offsets on upload.         */
+/* ------------------------------------------------------------------------ */
+enum { CS_FORMAT_COMPRESSED = 1u, CS_FORMAT_BLOCKED_ELL = 2u, CS_FORMAT_SLICED_ELL = 3u };
+
+/* device::partition_record (sharded_device.cuh:22-35) for one partition */
+typedef struct CS_ALIGN16 cs_partition_record {
+    void *allocation;          /* the packed device block (cudaMalloc) */
+    size_t allocation_bytes;
+    void *view;                /* device address of the cs_*_view at the block start */
+    void *a0, *a1, *a2, *a3;   /* payload arrays (device) */
+    int device_id;
+    uint32_t format;           /* CS_FORMAT_* */
+    unsigned char host_view[64]; /* host copy of the device view (a cs_*_view) */
+} cs_partition_record;
+
+CS_API int cs_b200_device_partition_bytes_compressed(const cs_host_compressed *src, size_t *out_bytes);
+CS_API int cs_b200_device_partition_bytes_blocked_ell(const cs_host_blocked_ell *src, size_t *out_bytes);
+CS_API int cs_b200_device_partition_bytes_sliced_ell(const cs_host_sliced_ell *src, size_t *out_bytes);
+CS_API int cs_b200_upload_compressed(const cs_host_compressed *src, cs_partition_record *record, cs_stream_t stream);
+CS_API int cs_b200_upload_blocked_ell(const cs_host_blocked_ell *src, cs_partition_record *record,
+                                      cs_stream_t stream);
+CS_API int cs_b200_upload_sliced_ell(const cs_host_sliced_ell *src, cs_partition_record *record, cs_stream_t stream);
+/* device::release: frees the block on its device and zeroes the record. */
+CS_API int cs_b200_release_partition(cs_partition_record *record);
+
+/* ------------------------------------------------------------------------ */
 /* Batched conversion of many uneven partitions (no reference counterpart:  */
 /* the reference converts one partition per call, sliced_ell_from_          */
 /* compressed.cuh:96-254, and plans one per call, major_nnz_raw.cuh:64-120). */

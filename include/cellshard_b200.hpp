@@ -1,0 +1,858 @@
+/*
+ * cellshard_b200.hpp -- C++ drop-in shim over the C ABI of cellshard_b200.h.
+ *
+ * Host code written against the reference's C++ API (namespaces
+ * cellshard::{sparse, device, convert, bucket, runtime}) includes this header
+ * instead of the reference's headers for the hot path and keeps its calls:
+ * the types below are field for field the reference's (same names, same
+ * layouts, __half values), and every function keeps the reference's name,
+ * argument order and meaning and its return convention (int 1/0, or
+ * cudaError_t for the device:: staging calls).  A translation unit includes
+ * either this header or the reference's, not both.
+ *
+ * Reference declarations mirrored here:
+ *   formats/compressed.cuh:24-37, blocked_ell.cuh:15-25, sliced_ell.cuh:16-28
+ *   runtime/device/sharded_device.cuh:22-35,67-98,343-991,1050-1083
+ *   src/convert/blocked_ell_from_compressed.cuh:157-190,258-347
+ *   src/convert/sliced_ell_from_compressed.cuh:96-164,
+ *       sliced_ell_from_blocked_ell.cuh:18-26,196-221
+ *   src/convert/compressed_transpose_raw.cuh:14-123
+ *   src/bucket/major_nnz_raw.cuh:12-320, src/bucket/operators/major_nnz.cuh:11-213
+ *   include/CellShard/runtime/mask_groups.cuh:14-224
+ * Not mirrored (out of this library's scope): the fleet (multi-GPU) entry
+ * points, sharded<T> host containers and their shard-level staging, the COO
+ * and DIA formats.
+ */
+#ifndef CELLSHARD_B200_HPP_
+#define CELLSHARD_B200_HPP_
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+
+#include "cellshard_b200.h"
+
+namespace cellshard {
+
+namespace types {
+using dim_t = unsigned int;
+using nnz_t = unsigned int;
+using idx_t = unsigned int;
+using ptr_t = unsigned int;
+using u32 = std::uint32_t;
+} // namespace types
+
+namespace real {
+using storage_t = __half;
+} // namespace real
+
+// ---------------------------------------------------------------------------
+// sparse:: host formats
+// ---------------------------------------------------------------------------
+namespace sparse {
+
+enum : types::u32 { compressed_by_row = 0u, compressed_by_col = 1u };
+enum : types::u32 { blocked_ell_invalid_col = 0xffffffffu, sliced_ell_invalid_col = 0xffffffffu };
+
+struct alignas(16) compressed {
+    types::dim_t rows;
+    types::dim_t cols;
+    types::nnz_t nnz;
+    types::u32 axis;
+    types::u32 flags;
+    void *storage;
+    types::ptr_t *majorPtr;
+    types::idx_t *minorIdx;
+    real::storage_t *val;
+};
+
+struct alignas(16) blocked_ell {
+    types::dim_t rows;
+    types::dim_t cols;
+    types::nnz_t nnz;
+    types::u32 block_size;
+    types::u32 ell_cols;
+    types::u32 flags;
+    void *storage;
+    types::idx_t *blockColIdx;
+    real::storage_t *val;
+};
+
+struct alignas(16) sliced_ell {
+    types::dim_t rows;
+    types::dim_t cols;
+    types::nnz_t nnz;
+    types::u32 slice_count;
+    types::u32 flags;
+    void *storage;
+    types::u32 *slice_row_offsets;
+    types::u32 *slice_widths;
+    types::idx_t *col_idx;
+    real::storage_t *val;
+};
+
+static_assert(sizeof(compressed) == sizeof(cs_host_compressed) &&
+                  offsetof(compressed, val) == offsetof(cs_host_compressed, val),
+              "sparse::compressed layout");
+static_assert(sizeof(blocked_ell) == sizeof(cs_host_blocked_ell) &&
+                  offsetof(blocked_ell, val) == offsetof(cs_host_blocked_ell, val),
+              "sparse::blocked_ell layout");
+static_assert(sizeof(sliced_ell) == sizeof(cs_host_sliced_ell) &&
+                  offsetof(sliced_ell, val) == offsetof(cs_host_sliced_ell, val),
+              "sparse::sliced_ell layout");
+
+inline void init(compressed *m) { std::memset(m, 0, sizeof(*m)); }
+inline void init(blocked_ell *m) { std::memset(m, 0, sizeof(*m)); }
+inline void init(sliced_ell *m) { std::memset(m, 0, sizeof(*m)); }
+// Results written by this library own one packed malloc'd block in `storage`.
+inline void clear(compressed *m) { cs_b200_host_compressed_clear(reinterpret_cast<cs_host_compressed *>(m)); }
+inline void clear(blocked_ell *m) { cs_b200_host_blocked_ell_clear(reinterpret_cast<cs_host_blocked_ell *>(m)); }
+inline void clear(sliced_ell *m) { cs_b200_host_sliced_ell_clear(reinterpret_cast<cs_host_sliced_ell *>(m)); }
+
+} // namespace sparse
+
+// ---------------------------------------------------------------------------
+// device:: views and single-partition staging
+// ---------------------------------------------------------------------------
+namespace device {
+
+struct alignas(16) compressed_view {
+    unsigned int rows, cols, nnz, axis;
+    unsigned int *majorPtr;
+    unsigned int *minorIdx;
+    __half *val;
+};
+
+struct alignas(16) blocked_ell_view {
+    unsigned int rows, cols, nnz, block_size, ell_cols;
+    unsigned int *blockColIdx;
+    __half *val;
+};
+
+struct alignas(16) sliced_ell_view {
+    unsigned int rows, cols, nnz, slice_count, slice_rows;
+    unsigned int *slice_row_offsets;
+    unsigned int *slice_widths;
+    unsigned int *slice_slot_offsets;
+    unsigned int *col_idx;
+    __half *val;
+};
+
+static_assert(sizeof(compressed_view) == sizeof(cs_compressed_view), "compressed_view layout");
+static_assert(sizeof(blocked_ell_view) == sizeof(cs_blocked_ell_view), "blocked_ell_view layout");
+static_assert(sizeof(sliced_ell_view) == sizeof(cs_sliced_ell_view), "sliced_ell_view layout");
+
+// One staged partition: `view` is the device address of the view descriptor
+// at the start of the packed block; `host_view` its host copy.
+template <typename MatrixT>
+struct alignas(16) partition_record {
+    cs_partition_record rec;
+};
+
+namespace detail {
+inline cudaError_t staged(int ok) {
+    if (ok) return cudaSuccess;
+    const cudaError_t e = cudaGetLastError();
+    return e != cudaSuccess ? e : cudaErrorInvalidValue;
+}
+} // namespace detail
+
+inline std::size_t device_partition_bytes(const sparse::compressed *src) {
+    size_t n = 0;
+    return cs_b200_device_partition_bytes_compressed(reinterpret_cast<const cs_host_compressed *>(src), &n) ? n : 0;
+}
+inline std::size_t device_partition_bytes(const sparse::blocked_ell *src) {
+    size_t n = 0;
+    return cs_b200_device_partition_bytes_blocked_ell(reinterpret_cast<const cs_host_blocked_ell *>(src), &n) ? n
+                                                                                                               : 0;
+}
+inline std::size_t device_partition_bytes(const sparse::sliced_ell *src) {
+    size_t n = 0;
+    return cs_b200_device_partition_bytes_sliced_ell(reinterpret_cast<const cs_host_sliced_ell *>(src), &n) ? n : 0;
+}
+
+inline cudaError_t upload_async(const sparse::compressed *src, partition_record<sparse::compressed> *record,
+                                cudaStream_t stream) {
+    return detail::staged(cs_b200_upload_compressed(reinterpret_cast<const cs_host_compressed *>(src), &record->rec,
+                                                    reinterpret_cast<cs_stream_t>(stream)));
+}
+inline cudaError_t upload_async(const sparse::blocked_ell *src, partition_record<sparse::blocked_ell> *record,
+                                cudaStream_t stream) {
+    return detail::staged(cs_b200_upload_blocked_ell(reinterpret_cast<const cs_host_blocked_ell *>(src),
+                                                     &record->rec, reinterpret_cast<cs_stream_t>(stream)));
+}
+inline cudaError_t upload_async(const sparse::sliced_ell *src, partition_record<sparse::sliced_ell> *record,
+                                cudaStream_t stream) {
+    return detail::staged(cs_b200_upload_sliced_ell(reinterpret_cast<const cs_host_sliced_ell *>(src), &record->rec,
+                                                    reinterpret_cast<cs_stream_t>(stream)));
+}
+template <typename MatrixT>
+inline cudaError_t upload(const MatrixT *src, partition_record<MatrixT> *record) {
+    return upload_async(src, record, (cudaStream_t) 0);
+}
+template <typename MatrixT>
+inline cudaError_t release(partition_record<MatrixT> *record) {
+    return detail::staged(cs_b200_release_partition(&record->rec));
+}
+// The staged view, usable on the host side of a launch.
+template <typename ViewT, typename MatrixT>
+inline ViewT staged_view(const partition_record<MatrixT> *record) {
+    ViewT v;
+    std::memcpy(&v, record->rec.host_view, sizeof(v));
+    return v;
+}
+
+} // namespace device
+
+// ---------------------------------------------------------------------------
+// convert::
+// ---------------------------------------------------------------------------
+namespace convert {
+
+struct blocked_ell_tune_result {
+    unsigned int block_size;
+    double fill_ratio;
+    std::size_t padded_bytes;
+};
+
+struct sliced_ell_tune_result {
+    unsigned int slice_rows;
+    unsigned int slice_count;
+    std::size_t padded_slots;
+    std::size_t padded_bytes;
+    double storage_ratio;
+    double slice_penalty;
+    double score;
+};
+
+static_assert(sizeof(blocked_ell_tune_result) == sizeof(cs_blocked_ell_tune_result), "tune layout");
+static_assert(sizeof(sliced_ell_tune_result) == sizeof(cs_sliced_ell_tune_result), "tune layout");
+
+inline int blocked_ell_from_compressed(const sparse::compressed *src, unsigned int block_size,
+                                       sparse::blocked_ell *dst) {
+    return cs_b200_blocked_ell_from_compressed(reinterpret_cast<const cs_host_compressed *>(src), block_size,
+                                               reinterpret_cast<cs_host_blocked_ell *>(dst));
+}
+
+inline int choose_blocked_ell_block_size(const sparse::compressed *src, const unsigned int *candidates,
+                                         unsigned int candidate_count, blocked_ell_tune_result *out) {
+    return cs_b200_choose_blocked_ell_block_size(reinterpret_cast<const cs_host_compressed *>(src), candidates,
+                                                 candidate_count, reinterpret_cast<cs_blocked_ell_tune_result *>(out));
+}
+
+inline int sliced_ell_from_compressed(const sparse::compressed *src, unsigned int slice_rows,
+                                      sparse::sliced_ell *dst) {
+    return cs_b200_sliced_ell_from_compressed(reinterpret_cast<const cs_host_compressed *>(src), slice_rows,
+                                              reinterpret_cast<cs_host_sliced_ell *>(dst));
+}
+// The reference's GPU route has the same contract (host in, host out).
+inline int sliced_ell_from_compressed_cuda(const sparse::compressed *src, unsigned int slice_rows,
+                                           sparse::sliced_ell *dst) {
+    return sliced_ell_from_compressed(src, slice_rows, dst);
+}
+
+inline int choose_sliced_ell_slice_rows_from_compressed(const sparse::compressed *src, const unsigned int *candidates,
+                                                        unsigned int candidate_count, sliced_ell_tune_result *out) {
+    return cs_b200_choose_sliced_ell_slice_rows_from_compressed(
+        reinterpret_cast<const cs_host_compressed *>(src), candidates, candidate_count,
+        reinterpret_cast<cs_sliced_ell_tune_result *>(out));
+}
+
+inline std::size_t compressed_transpose_scratch_bytes(types::dim_t cDim, types::dim_t uDim, types::nnz_t nnz) {
+    size_t n = 0;
+    return cs_b200_compressed_transpose_scratch_bytes(cDim, uDim, nnz, &n) ? n : 0;
+}
+
+inline int build_compressed_transpose_raw(types::dim_t cDim, types::dim_t uDim, types::nnz_t nnz,
+                                          const types::ptr_t *d_cAxPtr, const types::idx_t *d_uAxIdx,
+                                          const real::storage_t *d_val, types::ptr_t *d_out_uAxPtr,
+                                          types::ptr_t *d_heads, types::idx_t *d_out_cAxIdx,
+                                          real::storage_t *d_out_val, void *d_scan_tmp, std::size_t scan_bytes,
+                                          cudaStream_t stream) {
+    return cs_b200_build_compressed_transpose(cDim, uDim, nnz, d_cAxPtr, d_uAxIdx,
+                                              reinterpret_cast<const uint16_t *>(d_val), d_out_uAxPtr, d_heads,
+                                              d_out_cAxIdx, reinterpret_cast<uint16_t *>(d_out_val), d_scan_tmp,
+                                              scan_bytes, reinterpret_cast<cs_stream_t>(stream));
+}
+inline int build_transpose_cs_from_cs_raw(types::dim_t cDim, types::dim_t uDim, types::nnz_t nnz,
+                                          const types::ptr_t *p, const types::idx_t *i, const real::storage_t *v,
+                                          types::ptr_t *op, types::ptr_t *heads, types::idx_t *oi,
+                                          real::storage_t *ov, void *tmp, std::size_t bytes, cudaStream_t s) {
+    return build_compressed_transpose_raw(cDim, uDim, nnz, p, i, v, op, heads, oi, ov, tmp, bytes, s);
+}
+
+} // namespace convert
+
+// ---------------------------------------------------------------------------
+// bucket::
+// ---------------------------------------------------------------------------
+namespace bucket {
+
+struct alignas(16) major_nnz_bucket_plan_view {
+    types::dim_t major_dim;
+    types::idx_t bucket_count;
+    const types::idx_t *major_order;
+    const types::idx_t *major_nnz_sorted;
+    const types::idx_t *bucket_offsets;
+    const types::idx_t *inverse_major_order;
+};
+
+inline std::size_t major_nnz_bucket_sort_scratch_bytes(types::dim_t major_dim) {
+    size_t n = 0;
+    return cs_b200_major_nnz_bucket_sort_scratch_bytes(major_dim, &n) ? n : 0;
+}
+inline std::size_t major_nnz_bucket_scan_scratch_bytes(types::dim_t major_dim) {
+    size_t n = 0;
+    return cs_b200_major_nnz_bucket_scan_scratch_bytes(major_dim, &n) ? n : 0;
+}
+
+inline int build_major_nnz_bucket_plan_raw(const types::ptr_t *d_major_ptr, types::dim_t major_dim,
+                                           types::idx_t *d_major_nnz, types::idx_t *d_major_nnz_sorted,
+                                           types::idx_t *d_major_order_in, types::idx_t *d_major_order_out,
+                                           types::idx_t *d_bucket_offsets, types::idx_t requested_bucket_count,
+                                           void *d_sort_tmp, std::size_t sort_tmp_bytes, cudaStream_t stream) {
+    return cs_b200_build_major_nnz_bucket_plan(d_major_ptr, major_dim, d_major_nnz, d_major_nnz_sorted,
+                                               d_major_order_in, d_major_order_out, d_bucket_offsets,
+                                               requested_bucket_count, d_sort_tmp, sort_tmp_bytes,
+                                               reinterpret_cast<cs_stream_t>(stream));
+}
+
+inline int rebuild_compressed_major_order_raw(const types::ptr_t *d_src_major_ptr, const types::idx_t *d_src_minor_idx,
+                                              const real::storage_t *d_src_val, types::dim_t major_dim,
+                                              const types::idx_t *d_major_order, types::ptr_t *d_dst_major_ptr,
+                                              types::idx_t *d_dst_minor_idx, real::storage_t *d_dst_val,
+                                              types::idx_t *d_inverse_major_order, void *d_scan_tmp,
+                                              std::size_t scan_tmp_bytes, cudaStream_t stream) {
+    return cs_b200_rebuild_compressed_major_order(d_src_major_ptr, d_src_minor_idx,
+                                                  reinterpret_cast<const uint16_t *>(d_src_val), major_dim,
+                                                  d_major_order, d_dst_major_ptr, d_dst_minor_idx,
+                                                  reinterpret_cast<uint16_t *>(d_dst_val), d_inverse_major_order,
+                                                  d_scan_tmp, scan_tmp_bytes, reinterpret_cast<cs_stream_t>(stream));
+}
+
+// Caller-held workspace (operators/major_nnz.cuh:11-44): buffers grow
+// monotonically; result views alias it until the next call or clear().
+struct alignas(16) compressed_major_bucket_workspace {
+    int device;
+    cudaStream_t stream;
+    types::dim_t major_capacity;
+    types::nnz_t nnz_capacity;
+    types::idx_t bucket_capacity;
+    std::size_t sort_capacity;
+    std::size_t scan_capacity;
+    void *d_major_block;
+    void *d_rebuilt_block;
+    types::idx_t *d_major_nnz;
+    types::idx_t *d_major_nnz_sorted;
+    types::idx_t *d_major_order_in;
+    types::idx_t *d_major_order_out;
+    types::idx_t *d_inverse_major_order;
+    types::idx_t *d_bucket_offsets;
+    types::ptr_t *d_rebuilt_major_ptr;
+    types::idx_t *d_rebuilt_minor_idx;
+    real::storage_t *d_rebuilt_val;
+    void *d_sort_tmp;
+    void *d_scan_tmp;
+};
+
+struct alignas(16) compressed_major_bucket_result {
+    device::compressed_view rebuilt;
+    major_nnz_bucket_plan_view plan;
+};
+
+inline void init(compressed_major_bucket_workspace *ws) {
+    std::memset(ws, 0, sizeof(*ws));
+    ws->device = -1;
+}
+
+inline void clear(compressed_major_bucket_workspace *ws) {
+    if (ws->d_major_block) cudaFree(ws->d_major_block);
+    if (ws->d_rebuilt_block) cudaFree(ws->d_rebuilt_block);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+    init(ws);
+}
+
+inline int setup(compressed_major_bucket_workspace *ws, int device) {
+    init(ws);
+    ws->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return 0;
+    return cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) == cudaSuccess;
+}
+
+namespace detail {
+inline std::size_t up256(std::size_t x) { return (x + 255u) / 256u * 256u; }
+} // namespace detail
+
+inline int reserve(compressed_major_bucket_workspace *ws, types::dim_t major_dim, types::nnz_t nnz,
+                   types::idx_t bucket_count) {
+    const std::size_t sort_bytes = major_nnz_bucket_sort_scratch_bytes(major_dim);
+    const std::size_t scan_bytes = major_nnz_bucket_scan_scratch_bytes(major_dim);
+    if (major_dim > ws->major_capacity || bucket_count > ws->bucket_capacity || sort_bytes > ws->sort_capacity ||
+        scan_bytes > ws->scan_capacity) {
+        if (ws->d_major_block) cudaFree(ws->d_major_block);
+        ws->d_major_block = nullptr;
+        const std::size_t m = detail::up256(((std::size_t) major_dim + 1u) * 4u);
+        const std::size_t b = detail::up256(((std::size_t) bucket_count + 2u) * 4u);
+        const std::size_t total = 5u * m + b + detail::up256(sort_bytes) + detail::up256(scan_bytes);
+        if (cudaMalloc(&ws->d_major_block, total) != cudaSuccess) return 0;
+        unsigned char *p = static_cast<unsigned char *>(ws->d_major_block);
+        ws->d_major_nnz = reinterpret_cast<types::idx_t *>(p);
+        ws->d_major_nnz_sorted = reinterpret_cast<types::idx_t *>(p + m);
+        ws->d_major_order_in = reinterpret_cast<types::idx_t *>(p + 2u * m);
+        ws->d_major_order_out = reinterpret_cast<types::idx_t *>(p + 3u * m);
+        ws->d_inverse_major_order = reinterpret_cast<types::idx_t *>(p + 4u * m);
+        ws->d_bucket_offsets = reinterpret_cast<types::idx_t *>(p + 5u * m);
+        ws->d_sort_tmp = p + 5u * m + b;
+        ws->d_scan_tmp = p + 5u * m + b + detail::up256(sort_bytes);
+        ws->major_capacity = major_dim;
+        ws->bucket_capacity = bucket_count;
+        ws->sort_capacity = sort_bytes;
+        ws->scan_capacity = scan_bytes;
+    }
+    if (nnz > ws->nnz_capacity || major_dim > ws->major_capacity || !ws->d_rebuilt_block) {
+        if (ws->d_rebuilt_block) cudaFree(ws->d_rebuilt_block);
+        ws->d_rebuilt_block = nullptr;
+        const std::size_t m = detail::up256(((std::size_t) major_dim + 1u) * 4u);
+        const std::size_t i = detail::up256((std::size_t) nnz * 4u + 4u);
+        const std::size_t v = detail::up256((std::size_t) nnz * 2u + 2u);
+        if (cudaMalloc(&ws->d_rebuilt_block, m + i + v) != cudaSuccess) return 0;
+        unsigned char *p = static_cast<unsigned char *>(ws->d_rebuilt_block);
+        ws->d_rebuilt_major_ptr = reinterpret_cast<types::ptr_t *>(p);
+        ws->d_rebuilt_minor_idx = reinterpret_cast<types::idx_t *>(p + m);
+        ws->d_rebuilt_val = reinterpret_cast<real::storage_t *>(p + m + i);
+        ws->nnz_capacity = nnz;
+    }
+    return 1;
+}
+
+inline int build_plan(const device::compressed_view *src, types::idx_t requested_bucket_count,
+                      compressed_major_bucket_workspace *ws, major_nnz_bucket_plan_view *out) {
+    if (src == nullptr || ws == nullptr || out == nullptr) return 0;
+    const types::dim_t major_dim = src->axis == sparse::compressed_by_col ? src->cols : src->rows;
+    const types::idx_t B = major_dim == 0u ? 1u
+                                           : (requested_bucket_count < 1u ? 1u
+                                                                          : (requested_bucket_count > major_dim
+                                                                                 ? major_dim
+                                                                                 : requested_bucket_count));
+    if (!reserve(ws, major_dim, src->nnz, B)) return 0;
+    if (!build_major_nnz_bucket_plan_raw(src->majorPtr, major_dim, ws->d_major_nnz, ws->d_major_nnz_sorted,
+                                         ws->d_major_order_in, ws->d_major_order_out, ws->d_bucket_offsets,
+                                         requested_bucket_count, ws->d_sort_tmp, ws->sort_capacity, ws->stream))
+        return 0;
+    out->major_dim = major_dim;
+    out->bucket_count = B;
+    out->major_order = ws->d_major_order_out;
+    out->major_nnz_sorted = ws->d_major_nnz_sorted;
+    out->bucket_offsets = ws->d_bucket_offsets;
+    out->inverse_major_order = nullptr;
+    return 1;
+}
+
+inline int rebuild(const device::compressed_view *src, const major_nnz_bucket_plan_view *plan,
+                   compressed_major_bucket_workspace *ws, compressed_major_bucket_result *out) {
+    if (src == nullptr || plan == nullptr || ws == nullptr || out == nullptr) return 0;
+    if (!reserve(ws, plan->major_dim, src->nnz, plan->bucket_count)) return 0;
+    if (!rebuild_compressed_major_order_raw(src->majorPtr, src->minorIdx, src->val, plan->major_dim,
+                                            plan->major_order, ws->d_rebuilt_major_ptr, ws->d_rebuilt_minor_idx,
+                                            ws->d_rebuilt_val, ws->d_inverse_major_order, ws->d_scan_tmp,
+                                            ws->scan_capacity, ws->stream))
+        return 0;
+    out->rebuilt = *src;
+    out->rebuilt.majorPtr = ws->d_rebuilt_major_ptr;
+    out->rebuilt.minorIdx = ws->d_rebuilt_minor_idx;
+    out->rebuilt.val = ws->d_rebuilt_val;
+    out->plan = *plan;
+    out->plan.inverse_major_order = ws->d_inverse_major_order;
+    return 1;
+}
+
+inline int build_bucketed_major_view(const device::compressed_view *src, types::idx_t requested_bucket_count,
+                                     compressed_major_bucket_workspace *ws, compressed_major_bucket_result *out) {
+    major_nnz_bucket_plan_view plan;
+    if (!build_plan(src, requested_bucket_count, ws, &plan)) return 0;
+    return rebuild(src, &plan, ws, out);
+}
+
+} // namespace bucket
+
+// ---------------------------------------------------------------------------
+// runtime:: mask_groups
+// ---------------------------------------------------------------------------
+namespace runtime {
+
+static constexpr unsigned int CELLSHARD_MAX_MASK_GROUPS = CS_MAX_MASK_GROUPS;
+
+enum sparse_mask_layout : std::uint32_t {
+    sparse_mask_layout_unknown = 0u,
+    sparse_mask_layout_blocked_ell = 1u,
+    sparse_mask_layout_sliced_ell = 2u,
+    sparse_mask_layout_compressed = 3u
+};
+
+struct alignas(16) group_mask_config_view {
+    unsigned int group_count;
+    const char *const *group_names;
+    const std::uint32_t *feature_group_masks;
+};
+
+struct alignas(16) row_feature_mask_view {
+    const unsigned char *row_keep;
+    const unsigned char *feature_keep;
+    const unsigned int *row_remap;
+    const unsigned int *feature_remap;
+};
+
+struct alignas(16) sparse_group_filter_params {
+    float min_total;
+    unsigned int min_detected_features;
+    float max_group_fraction;
+    unsigned int fraction_group_index;
+};
+
+struct alignas(16) sparse_group_reduce_result {
+    unsigned int rows;
+    unsigned int group_count;
+    float *row_totals;
+    unsigned int *detected_features;
+    float *max_values;
+    unsigned char *row_keep;
+    float *group_counts;
+    float *group_percentages;
+};
+
+struct alignas(16) sparse_group_reduce_workspace {
+    int device;
+    cudaStream_t stream;
+    int owns_stream;
+    unsigned int rows_capacity;
+    unsigned int cols_capacity;
+    unsigned int group_capacity;
+    unsigned int values_capacity;
+    void *row_block;
+    void *feature_block;
+    void *scratch_block;
+    std::size_t scratch_bytes;
+    float *row_totals;
+    unsigned int *detected_features;
+    float *max_values;
+    unsigned char *row_keep;
+    float *group_counts;
+    float *group_percentages;
+    std::uint32_t *feature_group_masks;
+};
+
+struct alignas(16) masked_sparse_reoptimize_config {
+    unsigned int output_rows;
+    unsigned int output_cols;
+    unsigned int requested_bucket_count;
+    unsigned int output_block_size;
+    sparse_mask_layout requested_layout;
+};
+
+struct alignas(16) masked_sparse_reoptimize_metadata {
+    unsigned int kept_rows;
+    unsigned int kept_features;
+    unsigned int live_nnz;
+    unsigned long long bytes_before;
+    unsigned long long bytes_after;
+    sparse_mask_layout output_layout;
+};
+
+struct alignas(16) masked_sparse_reoptimize_result {
+    device::compressed_view compressed;
+    device::blocked_ell_view blocked_ell;
+    masked_sparse_reoptimize_metadata metadata;
+};
+
+struct alignas(16) masked_sparse_reoptimize_workspace {
+    int device;
+    cudaStream_t stream;
+    int owns_stream;
+    void *private_workspace;
+};
+
+struct alignas(16) auto_reoptimize_prediction_input {
+    float density_change;
+    float row_drop_ratio;
+    float feature_drop_ratio;
+    float layout_padding_change;
+    float estimated_rebuild_cost_ms;
+    unsigned int expected_reuse_count;
+};
+
+struct alignas(16) auto_reoptimize_prediction {
+    unsigned int should_reoptimize;
+    float estimated_net_gain_ms;
+};
+
+// The reference's predictor is a stub that never asks for a reoptimization
+// (mask_groups.cu:526-532); kept with the same answer.
+inline int predict_masked_sparse_reoptimization(const auto_reoptimize_prediction_input *input,
+                                                auto_reoptimize_prediction *out) {
+    if (input == nullptr || out == nullptr) return 0;
+    out->should_reoptimize = 0u;
+    out->estimated_net_gain_ms = 0.0f;
+    return 1;
+}
+
+inline void init(sparse_group_reduce_workspace *ws) {
+    std::memset(ws, 0, sizeof(*ws));
+    ws->device = -1;
+}
+
+inline void clear(sparse_group_reduce_workspace *ws) {
+    if (ws == nullptr) return;
+    if (ws->row_block) cudaFree(ws->row_block);
+    if (ws->feature_block) cudaFree(ws->feature_block);
+    if (ws->scratch_block) cudaFree(ws->scratch_block);
+    if (ws->owns_stream && ws->stream) cudaStreamDestroy(ws->stream);
+    init(ws);
+}
+
+inline int setup(sparse_group_reduce_workspace *ws, int device, cudaStream_t stream = (cudaStream_t) 0) {
+    if (ws == nullptr) return 0;
+    ws->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return 0;
+    if (stream != (cudaStream_t) 0) {
+        ws->stream = stream;
+        ws->owns_stream = 0;
+        return 1;
+    }
+    if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return 0;
+    ws->owns_stream = 1;
+    return 1;
+}
+
+namespace detail {
+inline std::size_t up256(std::size_t x) { return (x + 255u) / 256u * 256u; }
+} // namespace detail
+
+// Sizes the per-row outputs for `rows` x `group_count` and the feature masks
+// for `cols`; buffers grow monotonically (mask_groups.cu:620-700).
+inline int reserve(sparse_group_reduce_workspace *ws, unsigned int rows, unsigned int cols, unsigned int values,
+                   unsigned int group_count) {
+    if (ws == nullptr || group_count > CELLSHARD_MAX_MASK_GROUPS) return 0;
+    if (rows > ws->rows_capacity || group_count > ws->group_capacity || ws->row_block == nullptr) {
+        const unsigned int R = rows > ws->rows_capacity ? rows : ws->rows_capacity;
+        const unsigned int G = group_count > ws->group_capacity ? group_count : ws->group_capacity;
+        const std::size_t r4 = detail::up256((std::size_t) R * 4u + 4u), r1 = detail::up256((std::size_t) R + 1u);
+        const std::size_t rg = detail::up256((std::size_t) R * G * 4u + 4u);
+        void *p = nullptr;
+        if (cudaMalloc(&p, 3u * r4 + r1 + 2u * rg) != cudaSuccess) return 0;
+        if (ws->row_block) cudaFree(ws->row_block);
+        ws->row_block = p;
+        unsigned char *b = static_cast<unsigned char *>(p);
+        ws->row_totals = reinterpret_cast<float *>(b);
+        ws->detected_features = reinterpret_cast<unsigned int *>(b + r4);
+        ws->max_values = reinterpret_cast<float *>(b + 2u * r4);
+        ws->row_keep = b + 3u * r4;
+        ws->group_counts = reinterpret_cast<float *>(b + 3u * r4 + r1);
+        ws->group_percentages = reinterpret_cast<float *>(b + 3u * r4 + r1 + rg);
+        ws->rows_capacity = R;
+        ws->group_capacity = G;
+    }
+    if (cols > ws->cols_capacity || ws->feature_block == nullptr) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, detail::up256((std::size_t) cols * 4u + 4u)) != cudaSuccess) return 0;
+        if (ws->feature_block) {
+            if (ws->cols_capacity != 0u)
+                cudaMemcpy(p, ws->feature_block, (std::size_t) ws->cols_capacity * 4u, cudaMemcpyDeviceToDevice);
+            cudaFree(ws->feature_block);
+        }
+        ws->feature_block = p;
+        ws->feature_group_masks = static_cast<std::uint32_t *>(p);
+        ws->cols_capacity = cols;
+    }
+    if (values > ws->values_capacity) ws->values_capacity = values;
+    return 1;
+}
+
+inline int upload_feature_group_masks(sparse_group_reduce_workspace *ws, unsigned int cols,
+                                      const std::uint32_t *host_masks) {
+    if (ws == nullptr || host_masks == nullptr) return 0;
+    if (!reserve(ws, ws->rows_capacity, cols, ws->values_capacity, ws->group_capacity)) return 0;
+    return cudaMemcpy(ws->feature_group_masks, host_masks, (std::size_t) cols * 4u, cudaMemcpyHostToDevice) ==
+           cudaSuccess;
+}
+
+namespace detail {
+inline int bind(sparse_group_reduce_workspace *ws, unsigned int rows, unsigned int G,
+                sparse_group_reduce_result *out) {
+    out->rows = rows;
+    out->group_count = G;
+    out->row_totals = ws->row_totals;
+    out->detected_features = ws->detected_features;
+    out->max_values = ws->max_values;
+    out->row_keep = ws->row_keep;
+    out->group_counts = G ? ws->group_counts : nullptr;
+    out->group_percentages = G ? ws->group_percentages : nullptr;
+    return 1;
+}
+
+template <typename ViewT, typename CView, typename Fn>
+inline int reduce(const ViewT *src, sparse_group_reduce_workspace *ws, const group_mask_config_view *groups,
+                  const row_feature_mask_view *masks, const sparse_group_filter_params *filter,
+                  sparse_group_reduce_result *out, unsigned int values, Fn fn) {
+    if (src == nullptr || ws == nullptr || out == nullptr) return 0;
+    const unsigned int G = groups ? groups->group_count : 0u;
+    if (G > CELLSHARD_MAX_MASK_GROUPS || !reserve(ws, src->rows, src->cols, values, G)) return 0;
+    const std::uint32_t *fm = G == 0u ? nullptr
+                                      : (groups->feature_group_masks ? groups->feature_group_masks
+                                                                     : ws->feature_group_masks);
+    cs_group_reduce_out o{ws->row_totals, ws->detected_features, ws->max_values, ws->row_keep,
+                          G ? ws->group_counts : nullptr, G ? ws->group_percentages : nullptr};
+    static const row_feature_mask_view no_masks{nullptr, nullptr, nullptr, nullptr};
+    if (!fn(reinterpret_cast<const CView *>(src), fm, G,
+            reinterpret_cast<const cs_row_feature_mask_view *>(masks ? masks : &no_masks),
+            reinterpret_cast<const cs_group_filter_params *>(filter), &o, reinterpret_cast<cs_stream_t>(ws->stream)))
+        return 0;
+    return bind(ws, src->rows, G, out);
+}
+} // namespace detail
+
+inline int compute_sparse_group_reduce(const device::blocked_ell_view *src, sparse_group_reduce_workspace *ws,
+                                       const group_mask_config_view *groups, const row_feature_mask_view *masks,
+                                       const sparse_group_filter_params *filter, sparse_group_reduce_result *out) {
+    return detail::reduce<device::blocked_ell_view, cs_blocked_ell_view>(
+        src, ws, groups, masks, filter, out, src ? src->rows * src->ell_cols : 0u, cs_b200_group_reduce_blocked_ell);
+}
+
+inline int compute_sparse_group_reduce(const device::sliced_ell_view *src, sparse_group_reduce_workspace *ws,
+                                       const group_mask_config_view *groups, const row_feature_mask_view *masks,
+                                       const sparse_group_filter_params *filter, sparse_group_reduce_result *out) {
+    return detail::reduce<device::sliced_ell_view, cs_sliced_ell_view>(src, ws, groups, masks, filter, out, 0u,
+                                                                       cs_b200_group_reduce_sliced_ell);
+}
+
+inline int compute_sparse_group_reduce_compressed_fallback(const device::compressed_view *src,
+                                                           sparse_group_reduce_workspace *ws,
+                                                           const group_mask_config_view *groups,
+                                                           const row_feature_mask_view *masks,
+                                                           const sparse_group_filter_params *filter,
+                                                           sparse_group_reduce_result *out) {
+    return detail::reduce<device::compressed_view, cs_compressed_view>(src, ws, groups, masks, filter, out,
+                                                                       src ? src->nnz : 0u,
+                                                                       cs_b200_group_reduce_compressed);
+}
+
+inline void init(masked_sparse_reoptimize_workspace *ws) {
+    std::memset(ws, 0, sizeof(*ws));
+    ws->device = -1;
+}
+
+namespace detail {
+struct reopt_private {
+    void *scratch;
+    std::size_t scratch_bytes;
+    void *out_block;
+    std::size_t out_bytes;
+    std::uint32_t *status;
+};
+} // namespace detail
+
+inline void clear(masked_sparse_reoptimize_workspace *ws) {
+    if (ws == nullptr) return;
+    auto *pv = static_cast<detail::reopt_private *>(ws->private_workspace);
+    if (pv) {
+        if (pv->scratch) cudaFree(pv->scratch);
+        if (pv->out_block) cudaFree(pv->out_block);
+        if (pv->status) cudaFree(pv->status);
+        delete pv;
+    }
+    if (ws->owns_stream && ws->stream) cudaStreamDestroy(ws->stream);
+    init(ws);
+}
+
+inline int setup(masked_sparse_reoptimize_workspace *ws, int device, cudaStream_t stream = (cudaStream_t) 0) {
+    if (ws == nullptr) return 0;
+    ws->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return 0;
+    if (stream != (cudaStream_t) 0) {
+        ws->stream = stream;
+        ws->owns_stream = 0;
+    } else {
+        if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return 0;
+        ws->owns_stream = 1;
+    }
+    if (ws->private_workspace == nullptr) {
+        auto *pv = new detail::reopt_private{};
+        if (cudaMalloc((void **) &pv->status, 4) != cudaSuccess) {
+            delete pv;
+            return 0;
+        }
+        ws->private_workspace = pv;
+    }
+    return 1;
+}
+
+// Masked + remapped Blocked-ELL -> CSR.  Synchronises once to size the output
+// (as the reference does); the result aliases the workspace.  Entries of an
+// output row keep Blocked-ELL slot order; two kept rows remapped to one
+// output row are rejected.
+inline int manual_reoptimize_masked_sparse(const device::blocked_ell_view *src, const row_feature_mask_view *masks,
+                                           const masked_sparse_reoptimize_config *config,
+                                           masked_sparse_reoptimize_workspace *ws,
+                                           masked_sparse_reoptimize_result *out) {
+    if (src == nullptr || ws == nullptr || out == nullptr || ws->private_workspace == nullptr) return 0;
+    auto *pv = static_cast<detail::reopt_private *>(ws->private_workspace);
+    const unsigned int out_rows = config && config->output_rows ? config->output_rows : src->rows;
+    const unsigned int out_cols = config && config->output_cols ? config->output_cols : src->cols;
+    static const row_feature_mask_view no_masks{nullptr, nullptr, nullptr, nullptr};
+    const auto *m = reinterpret_cast<const cs_row_feature_mask_view *>(masks ? masks : &no_masks);
+    const auto *v = reinterpret_cast<const cs_blocked_ell_view *>(src);
+    const cs_stream_t s = reinterpret_cast<cs_stream_t>(ws->stream);
+    size_t need = 0;
+    if (!cs_b200_reoptimize_scratch_bytes(src->rows, out_rows, &need)) return 0;
+    const std::size_t ptr_bytes = detail::up256(((std::size_t) out_rows + 1u) * 4u);
+    if (need + ptr_bytes > pv->scratch_bytes) {
+        if (pv->scratch) cudaFree(pv->scratch);
+        pv->scratch = nullptr;
+        if (cudaMalloc(&pv->scratch, need + ptr_bytes) != cudaSuccess) return 0;
+        pv->scratch_bytes = need + ptr_bytes;
+    }
+    auto *major = static_cast<std::uint32_t *>(pv->scratch);
+    void *scr = static_cast<unsigned char *>(pv->scratch) + ptr_bytes;
+    if (cudaMemsetAsync(pv->status, 0, 4, ws->stream) != cudaSuccess) return 0;
+    if (!cs_b200_reoptimize_count(v, m, out_rows, out_cols, major, scr, need, pv->status, s)) return 0;
+    std::uint32_t nnz = 0, status = 0;
+    if (cudaMemcpyAsync(&nnz, major + out_rows, 4, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&status, pv->status, 4, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ws->stream) != cudaSuccess || status != 0u)
+        return 0;
+    const std::size_t need_out = ptr_bytes + detail::up256((std::size_t) nnz * 4u + 4u) +
+                                 detail::up256((std::size_t) nnz * 2u + 2u);
+    if (need_out > pv->out_bytes) {
+        if (pv->out_block) cudaFree(pv->out_block);
+        pv->out_block = nullptr;
+        if (cudaMalloc(&pv->out_block, need_out) != cudaSuccess) return 0;
+        pv->out_bytes = need_out;
+    }
+    unsigned char *ob = static_cast<unsigned char *>(pv->out_block);
+    auto *optr = reinterpret_cast<std::uint32_t *>(ob);
+    auto *oidx = reinterpret_cast<std::uint32_t *>(ob + ptr_bytes);
+    auto *oval = reinterpret_cast<__half *>(ob + ptr_bytes + detail::up256((std::size_t) nnz * 4u + 4u));
+    if (cudaMemcpyAsync(optr, major, ((std::size_t) out_rows + 1u) * 4u, cudaMemcpyDeviceToDevice, ws->stream) !=
+            cudaSuccess ||
+        !cs_b200_reoptimize_emit(v, m, out_rows, out_cols, optr, oidx, reinterpret_cast<uint16_t *>(oval), s))
+        return 0;
+    std::memset(out, 0, sizeof(*out));
+    out->compressed = device::compressed_view{out_rows, out_cols, nnz, sparse::compressed_by_row, optr, oidx, oval};
+    out->metadata.kept_rows = out_rows;
+    out->metadata.kept_features = out_cols;
+    out->metadata.live_nnz = nnz;
+    const unsigned int rb = src->block_size ? (src->rows + src->block_size - 1u) / src->block_size : 0u;
+    out->metadata.bytes_before = (unsigned long long) src->rows * src->ell_cols * 2ull +
+                                 (unsigned long long) rb * (src->block_size ? src->ell_cols / src->block_size : 0u) *
+                                     4ull;
+    out->metadata.bytes_after = ((unsigned long long) out_rows + 1ull) * 4ull + (unsigned long long) nnz * 6ull;
+    out->metadata.output_layout = sparse_mask_layout_compressed;
+    return 1;
+}
+
+} // namespace runtime
+} // namespace cellshard
+
+#endif /* CELLSHARD_B200_HPP_ */

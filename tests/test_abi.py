@@ -52,6 +52,7 @@ int main(void) {
   S(cs_batch_part) O(cs_batch_part, d_major_nnz) O(cs_batch_part, d_pow2_offsets)
   S(cs_batch_tiles) S(cs_batch_sliced_result) O(cs_batch_sliced_result, view)
   S(cs_serve_config) S(cs_serve_request) O(cs_serve_request, group_rows) S(cs_serve_stats)
+  S(cs_partition_record) O(cs_partition_record, host_view)
   return 0;
 }
 """
@@ -76,6 +77,7 @@ PAIRS = {
     "cs_serve_config": _abi.ServeConfig,
     "cs_serve_request": _abi.ServeRequest,
     "cs_serve_stats": _abi.ServeStats,
+    "cs_partition_record": _abi.PartitionRecord,
 }
 
 
@@ -98,6 +100,7 @@ def test_ctypes_layouts_match_c(tmp_path):
     assert got["cs_batch_part.d_pow2_offsets"] == _abi.BatchPart.d_pow2_offsets.offset
     assert got["cs_batch_sliced_result.view"] == _abi.BatchSlicedResult.view.offset
     assert got["cs_serve_request.group_rows"] == _abi.ServeRequest.group_rows.offset
+    assert got["cs_partition_record.host_view"] == _abi.PartitionRecord.host_view.offset
 
 
 def test_abi_version_and_host_validation(cs_lib):

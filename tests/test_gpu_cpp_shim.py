@@ -1,0 +1,136 @@
+"""The C++ drop-in shim (include/cellshard_b200.hpp): a C++ program written
+the way reference host code is written (cellshard::runtime / device /
+convert / bucket calls, workspaces, device::upload staging) is compiled
+against the shim and the library, run on the GPU, and its results checked:
+the mask_groups known answers of the reference's runtime test, and the
+restatement for the conversion, chooser, bucketing, reoptimize and transpose
+calls on the same inputs."""
+
+import json
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+KA = json.loads((ROOT / "tests" / "golden" / "mask_groups_known_answers.json").read_text())
+
+
+def _inputs_text():
+    lines = [f"rows {KA['rows']}", f"cols {KA['cols']}", "group_masks " + " ".join(map(str, KA["group_masks"])),
+             "row_keep " + " ".join(map(str, KA["row_keep"])), "feature_keep " + " ".join(map(str, KA["feature_keep"])),
+             f"group_count {KA['group_count']}", "filter " + " ".join(map(str, KA["filter"]))]
+    for sec in ("blocked", "compressed", "sliced", "reoptimize"):
+        for k, v in KA[sec].items():
+            lines.append(f"{sec}.{k} " + (" ".join(map(str, v)) if isinstance(v, list) else str(v)))
+    return "\n".join(lines) + "\n"
+
+
+@pytest.fixture(scope="module")
+def shim_out(cuda, tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    d = tmp_path_factory.mktemp("shim")
+    exe = d / "shim_runtime_test"
+    lib = ROOT / "cellshard_b200"
+    subprocess.run([nvcc, "-std=c++17", "-Wno-deprecated-gpu-targets", "-I", str(ROOT / "include"), "-o", str(exe),
+                    str(ROOT / "tests" / "cpp" / "shim_runtime_test.cpp"), "-L", str(lib), "-lcellshard_b200",
+                    "-Xlinker", f"-rpath,{lib}"], check=True)
+    inp = d / "inputs.txt"
+    inp.write_text(_inputs_text())
+    p = subprocess.run([str(exe), str(inp)], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    out = {}
+    for line in p.stdout.splitlines():
+        parts = line.split()
+        out[parts[0]] = np.array([float(x) for x in parts[1:]])
+    return out
+
+
+def close(a, b, tol=1e-3):
+    return abs(float(a) - float(b)) <= tol
+
+
+def test_shim_mask_groups_known_answers(shim_out):
+    o = shim_out
+    e = KA["expect_blocked"]
+    assert all(close(a, b) for a, b in zip(o["blocked.row_totals"], e["row_totals"]))
+    assert list(o["blocked.detected"]) == e["detected"] and list(o["blocked.keep"]) == e["keep"]
+    for k, v in e["group_counts"].items():
+        assert close(o["blocked.group_counts"][int(k)], v)
+    for k, v in e["group_percentages"].items():
+        assert close(o["blocked.group_percentages"][int(k)], v)
+    assert close(o["no_groups.row_totals"][0], 15) and o["no_groups.detected"][0] == 3
+    assert "no_groups.group_counts" not in o
+    assert o["null_filter"][0] == 0
+    assert close(o["compressed.row_totals"][2], 7) and close(o["compressed.group_counts"][8], 2)
+    assert close(o["sliced.row_totals"][0], 8) and close(o["sliced.row_totals"][3], 18)
+    assert list(o["sliced.view"]) == [KA["sliced"]["slice_rows"], len(KA["sliced"]["widths"])]
+    assert list(o["sliced.slot_offsets"]) == KA["sliced"]["slot_offsets"]
+    er = KA["expect_reoptimize"]
+    assert list(o["reoptimize.meta"]) == [er["kept_rows"], er["kept_features"], er["live_nnz"]]
+    assert o["done"][0] == 0
+
+
+def test_shim_matches_c_abi_path(shim_out, cuda):
+    """The shim adds no arithmetic: its reduce outputs equal the C-ABI path's."""
+    import torch
+
+    from cellshard_b200 import runtime
+    from cellshard_b200.device import BlockedELL
+
+    b = KA["blocked"]
+    bell = BlockedELL(KA["rows"], KA["cols"], b["block_size"], b["ell_cols"],
+                      torch.tensor(b["block_cols"], dtype=torch.int32, device="cuda"),
+                      torch.tensor(b["values"], dtype=torch.float16, device="cuda"))
+    f = KA["filter"]
+    r = runtime.compute_sparse_group_reduce(
+        bell, torch.tensor(np.array(KA["group_masks"], np.uint32).view(np.int32), device="cuda"), 3,
+        torch.tensor(KA["row_keep"], dtype=torch.uint8, device="cuda"),
+        torch.tensor(KA["feature_keep"], dtype=torch.uint8, device="cuda"), runtime.FilterParams(*f))
+    torch.cuda.synchronize()
+    assert np.array_equal(r["row_totals"].cpu().numpy(), shim_out["blocked.row_totals"].astype(np.float32))
+    assert np.array_equal(r["group_counts"].cpu().numpy().ravel(),
+                          shim_out["blocked.group_counts"].astype(np.float32))
+    assert np.array_equal(r["group_percentages"].cpu().numpy().ravel(),
+                          shim_out["blocked.group_percentages"].astype(np.float32))
+
+
+def test_shim_convert_bucket_transpose_reoptimize(shim_out, orc):
+    o = shim_out
+    c = KA["compressed"]
+    rows, cols = KA["rows"], KA["cols"]
+    ptr = np.array(c["ptr"], np.uint32)
+    idx = np.array(c["idx"], np.uint32)
+    val = np.array(c["values"], np.float16).view(np.uint16)
+    ref = orc.blocked_ell_from_csr(rows, cols, ptr, idx, val, 2)
+    assert list(o["convert.blocked"][:2]) == [2, ref["ell_cols"]] and o["convert.blocked"][2] == ref["nnz"]
+    assert np.array_equal(o["convert.block_cols"].astype(np.uint32), ref["bci"])
+    assert np.array_equal(o["convert.values"].astype(np.float16).view(np.uint16), ref["val"])
+    h, score, _ = orc.choose_sliced_slice_rows(rows, int(ptr[-1]), ptr, (16, 32, 64))
+    assert o["convert.slice_choice"][0] == h and o["convert.slice_choice"][3] == score
+    _nnz, _srt, order, offs = orc.major_nnz_plan(ptr, rows, 2)
+    assert np.array_equal(o["bucket.order"].astype(np.uint32), order)
+    assert np.array_equal(o["bucket.offsets"].astype(np.uint32), offs)
+    rptr, _ridx, _rval, rinv = orc.rebuild(ptr, idx, val, rows, order)
+    assert np.array_equal(o["bucket.rebuilt_ptr"].astype(np.uint32), rptr)
+    assert np.array_equal(o["bucket.inverse"].astype(np.uint32), rinv)
+    tptr, tidx, tval = orc.csr_transpose(rows, cols, ptr, idx, val)
+    assert np.array_equal(o["transpose.ptr"].astype(np.uint32), tptr)
+    assert np.array_equal(o["transpose.idx"].astype(np.uint32), tidx)
+    assert np.array_equal(o["transpose.val"].astype(np.float16).view(np.uint16), tval)
+    rr = KA["reoptimize"]
+    b = KA["blocked"]
+    major, ridx, rval = orc.reoptimize_bell(rows, cols, b["block_size"], b["ell_cols"],
+                                            np.array(b["block_cols"], np.uint32),
+                                            np.array(b["values"], np.float16).view(np.uint16),
+                                            np.array(KA["row_keep"], np.uint8), np.array(KA["feature_keep"], np.uint8),
+                                            np.array(rr["row_remap"], np.uint32),
+                                            np.array(rr["feature_remap"], np.uint32), rr["output_rows"],
+                                            rr["output_cols"])
+    assert np.array_equal(o["reoptimize.ptr"].astype(np.uint32), major)
+    assert np.array_equal(o["reoptimize.idx"].astype(np.uint32), ridx)
+    assert np.array_equal(o["reoptimize.val"].astype(np.float16).view(np.uint16), rval)
