@@ -20,6 +20,7 @@ namespace {
 
 constexpr unsigned kRowWarps = 8;
 constexpr unsigned kRowThreads = kRowWarps * 32;
+constexpr uint32_t kStagePairs = 128; // per-warp (feature, value) staging in the Blocked-ELL reduce
 
 struct row_acc {
     float sum;
@@ -40,6 +41,34 @@ __device__ __forceinline__ void add_value(row_acc &a, float v, uint32_t gene, co
     a.detected += 1u;
     if (acc_col != nullptr) {
         uint32_t m = group_masks[gene];
+        while (m != 0u) {
+            const uint32_t g = __ffs(m) - 1u;
+            if (g < group_count) acc_col[g * 32u] += v;
+            m &= m - 1u;
+        }
+    }
+}
+
+// Bit q set when fp16 value q of the 8 packed in v (low half first) is
+// nonzero (either sign of zero counts as zero).
+__device__ __forceinline__ uint32_t nonzero_bits(const uint4 &v) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    uint32_t b = 0u;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t m = __vsetne2(w[i] & 0x7fff7fffu, 0u); // 1 in each nonzero half
+        b |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * i);
+    }
+    return b;
+}
+
+// add_value with the column's group mask already loaded.
+__device__ __forceinline__ void add_value_masked(row_acc &a, float v, uint32_t m, uint32_t group_count,
+                                                 float *acc_col) {
+    a.sum += v;
+    a.vmax = fmaxf(a.vmax, v);
+    a.detected += 1u;
+    if (acc_col != nullptr) {
         while (m != 0u) {
             const uint32_t g = __ffs(m) - 1u;
             if (g < group_count) acc_col[g * 32u] += v;
@@ -127,6 +156,9 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_bell_kernel(cs_block
     extern __shared__ float gr_smem[];
     const bool groups = group_masks != nullptr && group_count != 0u;
     float *acc_col = warp_acc_column(gr_smem, groups);
+    // staging pairs follow the accumulator columns (if any)
+    uint2 *stage = reinterpret_cast<uint2 *>(gr_smem + (groups ? kRowWarps * 1024u : 0u)) +
+                   (threadIdx.x >> 5) * kStagePairs;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t B = src.block_size;
     const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
@@ -141,19 +173,67 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_bell_kernel(cs_block
         const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
         const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
         if (VEC) {
-            for (uint32_t e0 = lane * 8u; e0 < src.ell_cols; e0 += 256u) {
-                const uint32_t slot = e0 / B;
-                const uint32_t bc = bci[slot];
-                if (bc == CS_INVALID_COL) continue;
-                const uint4 v = ld_stream_v4(vrow + e0);
-                const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
-                const uint32_t gene0 = bc * B + (e0 - slot * B);
+            // U 16-byte vectors of values in flight per lane, loaded whether or
+            // not their slot is padding (they lie inside the row) so no value
+            // load waits for its block column.  The lane's nonzero values of
+            // the U vectors become a 32-bit mask; the warp compacts them
+            // (exclusive scan of the lanes' counts) into a per-warp staging
+            // buffer of (value, feature) pairs and then works through the pairs
+            // 32 at a time with every lane busy, instead of every lane stepping
+            // through all its slots while most of them hold zeros.
+            constexpr unsigned U = 4;
+            for (uint32_t base = lane * 8u; base < src.ell_cols; base += 256u * U) {
+                uint4 v[U];
+                uint32_t bc[U], gene0[U];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const uint16_t h = (uint16_t) (w4[q >> 1] >> ((q & 1) * 16));
-                    const uint32_t gene = gene0 + q;
-                    if (half_nonzero(h) && gene < src.cols && feature_kept(masks.feature_keep, gene))
-                        add_value(a, h2f(h), gene, group_masks, group_count, acc_col);
+                for (unsigned u = 0; u < U; ++u) {
+                    const uint32_t e0 = base + u * 256u;
+                    const bool in = e0 < src.ell_cols;
+                    v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
+                    bc[u] = in ? __ldg(bci + e0 / B) : CS_INVALID_COL;
+                }
+                // the feature flags are checked per staged value, not per vector
+                uint32_t nzall = 0u;
+#pragma unroll
+                for (unsigned u = 0; u < U; ++u) {
+                    const uint32_t e0 = base + u * 256u;
+                    gene0[u] = bc[u] * B + (e0 % B);
+                    if (bc[u] == CS_INVALID_COL) continue;
+                    uint32_t nz = nonzero_bits(v[u]);
+                    if (nz != 0u && gene0[u] + 8u > src.cols) {
+                        const uint32_t lim = gene0[u] < src.cols ? src.cols - gene0[u] : 0u; // < 8 here
+                        nz &= (1u << lim) - 1u;
+                    }
+                    nzall |= nz << (8u * u);
+                }
+                const uint32_t cnt = __popc(nzall);
+                const uint32_t incl = warp_inclusive_scan(cnt);
+                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                const uint32_t excl = incl - cnt;
+                for (uint32_t p0 = 0; p0 < total; p0 += kStagePairs) {
+                    uint32_t bits = nzall, k = excl;
+                    while (bits != 0u && k < p0 + kStagePairs) {
+                        const uint32_t bitpos = __ffs(bits) - 1u;
+                        bits &= bits - 1u;
+                        if (k >= p0) {
+                            const uint32_t u = bitpos >> 3, q = bitpos & 7u;
+                            const uint4 vu = u < 2u ? (u == 0u ? v[0] : v[1]) : (u == 2u ? v[2] : v[3]);
+                            const uint32_t g0 = u < 2u ? (u == 0u ? gene0[0] : gene0[1])
+                                                       : (u == 2u ? gene0[2] : gene0[3]);
+                            const uint32_t wq = q < 4u ? (q < 2u ? vu.x : vu.y) : (q < 6u ? vu.z : vu.w);
+                            stage[k - p0] = make_uint2(g0 + q, (wq >> ((q & 1u) * 16u)) & 0xffffu);
+                        }
+                        ++k;
+                    }
+                    __syncwarp();
+                    const uint32_t n = min(kStagePairs, total - p0);
+                    for (uint32_t i = lane; i < n; i += 32u) {
+                        const uint2 pr = stage[i];
+                        if (!feature_kept(masks.feature_keep, pr.x)) continue;
+                        const uint32_t m = acc_col != nullptr ? __ldg(group_masks + pr.x) : 0u;
+                        add_value_masked(a, h2f((uint16_t) pr.y), m, group_count, acc_col);
+                    }
+                    __syncwarp();
                 }
             }
         } else {
@@ -363,7 +443,8 @@ extern "C" int cs_b200_group_reduce_blocked_ell(const cs_blocked_ell_view *src, 
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
     const bool vec = src->block_size != 0u && src->block_size % 8u == 0u &&
                      (reinterpret_cast<uintptr_t>(src->val) & 15u) == 0u;
-    const std::size_t smem = group_smem(d_feature_group_masks, group_count);
+    const std::size_t smem = group_smem(d_feature_group_masks, group_count) +
+                             (vec ? (std::size_t) kRowWarps * kStagePairs * sizeof(uint2) : 0u);
     if (vec)
         group_reduce_bell_kernel<true><<<row_grid(src->rows), kRowThreads, smem, as_stream(s)>>>(
             *src, d_feature_group_masks, group_count, m, *filter, *out);

@@ -379,6 +379,10 @@ def ref_gpu() -> C.CDLL:
         g.csrefgpu_major_nnz_plan.argtypes = [vp, u32, vp, vp, vp, vp, vp, u32]
         g.csrefgpu_rebuild.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp]
         g.csrefgpu_sliced_ell_from_compressed_cuda.argtypes = [vp, C.c_uint, vp]
+        fp = C.POINTER(C.c_float)
+        g.csrefgpu_transpose_timed.argtypes = [u32, u32, u32, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, fp]
+        g.csrefgpu_major_nnz_plan_timed.argtypes = [vp, u32, vp, vp, vp, vp, vp, u32, C.c_int, C.c_int, fp]
+        g.csrefgpu_group_reduce_blocked_ell_timed.argtypes = [vp, vp, u32, vp, vp, C.c_int, C.c_int, fp]
         _rg = g
     return _rg
 

@@ -11,6 +11,9 @@
 //   bucket::build_major_nnz_bucket_plan_raw (src/bucket/major_nnz_raw.cuh:64)
 //   bucket::rebuild_compressed_major_order_raw (src/bucket/major_nnz_raw.cuh:188)
 //   convert::sliced_ell_from_compressed_cuda (src/convert/sliced_ell_from_compressed.cuh:166)
+// The *_timed variants allocate once, run `warmup` untimed calls, then time
+// `reps` calls of the reference function alone with CUDA events on its
+// stream, for the reference GPU points beside this library's kernels.
 #include <CellShard/runtime/mask_groups.cuh>
 
 #include "src/bucket/major_nnz_raw.cuh"
@@ -214,6 +217,111 @@ int csrefgpu_sliced_ell_from_compressed_cuda(const cs_host_compressed *src, unsi
     sparse::init(&d);
     const int ok = convert::sliced_ell_from_compressed_cuda(&s, slice_rows, &d, 0, (cudaStream_t) 0);
     std::memcpy(dst, &d, sizeof(d));
+    return ok;
+}
+
+} // extern "C"
+
+namespace {
+struct ev_timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ev_timer() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~ev_timer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+template <typename Call>
+int time_calls(Call call, cudaStream_t stream, int warmup, int reps, float *ms_per_call) {
+    int ok = 1;
+    for (int i = 0; i < warmup && ok; ++i) ok = call();
+    if (ok) ok = cudaStreamSynchronize(stream) == cudaSuccess;
+    ev_timer t;
+    cudaEventRecord(t.a, stream);
+    for (int i = 0; i < reps && ok; ++i) ok = call();
+    cudaEventRecord(t.b, stream);
+    if (ok) ok = cudaEventSynchronize(t.b) == cudaSuccess;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, t.a, t.b);
+    *ms_per_call = reps > 0 ? ms / (float) reps : 0.0f;
+    return ok;
+}
+} // namespace
+
+extern "C" {
+
+int csrefgpu_transpose_timed(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uint32_t *d_ptr, const uint32_t *d_idx,
+                             const uint16_t *d_val, uint32_t *d_out_ptr, uint32_t *d_out_idx, uint16_t *d_out_val,
+                             int warmup, int reps, float *ms_per_call) {
+    cusparseHandle_t handle = 0;
+    std::size_t lib_bytes = 0;
+    if (!convert::cusparse_utils::acquire((cudaStream_t) 0, &handle)) return 0;
+    if (cusparseCsr2cscEx2_bufferSize(handle, (int) cDim, (int) uDim, (int) nnz, d_val,
+                                      reinterpret_cast<const int *>(d_ptr), reinterpret_cast<const int *>(d_idx),
+                                      d_out_val, reinterpret_cast<int *>(d_out_ptr),
+                                      reinterpret_cast<int *>(d_out_idx), CUDA_R_16F, CUSPARSE_ACTION_NUMERIC,
+                                      CUSPARSE_INDEX_BASE_ZERO, CUSPARSE_CSR2CSC_ALG1,
+                                      &lib_bytes) != CUSPARSE_STATUS_SUCCESS)
+        return 0;
+    void *scratch = nullptr;
+    uint32_t *heads = nullptr;
+    const std::size_t bytes = lib_bytes < 256u ? 256u : lib_bytes;
+    if (cudaMalloc(&scratch, bytes) != cudaSuccess) return 0;
+    if (cudaMalloc((void **) &heads, ((std::size_t) uDim + 1u) * 4u) != cudaSuccess) {
+        cudaFree(scratch);
+        return 0;
+    }
+    const int ok = time_calls(
+        [&] {
+            return convert::build_compressed_transpose_raw(cDim, uDim, nnz, d_ptr, d_idx,
+                                                           reinterpret_cast<const __half *>(d_val), d_out_ptr, heads,
+                                                           d_out_idx, reinterpret_cast<__half *>(d_out_val), scratch,
+                                                           bytes, (cudaStream_t) 0);
+        },
+        (cudaStream_t) 0, warmup, reps, ms_per_call);
+    cudaFree(heads);
+    cudaFree(scratch);
+    return ok;
+}
+
+int csrefgpu_major_nnz_plan_timed(const uint32_t *d_major_ptr, uint32_t major_dim, uint32_t *d_major_nnz,
+                                  uint32_t *d_sorted, uint32_t *d_order_in, uint32_t *d_order_out,
+                                  uint32_t *d_offsets, uint32_t requested, int warmup, int reps, float *ms_per_call) {
+    std::size_t bytes = 0;
+    if (!bucket::major_nnz_bucket_sort_scratch_bytes(major_dim, &bytes)) return 0;
+    void *tmp = nullptr;
+    if (cudaMalloc(&tmp, bytes < 256u ? 256u : bytes) != cudaSuccess) return 0;
+    const int ok = time_calls(
+        [&] {
+            return bucket::build_major_nnz_bucket_plan_raw(d_major_ptr, major_dim, d_major_nnz, d_sorted, d_order_in,
+                                                           d_order_out, d_offsets, requested, tmp, bytes,
+                                                           (cudaStream_t) 0);
+        },
+        (cudaStream_t) 0, warmup, reps, ms_per_call);
+    cudaFree(tmp);
+    return ok;
+}
+
+int csrefgpu_group_reduce_blocked_ell_timed(const cs_blocked_ell_view *src, const uint32_t *d_masks,
+                                            uint32_t group_count, const cs_row_feature_mask_view *m,
+                                            const cs_group_filter_params *f, int warmup, int reps,
+                                            float *ms_per_call) {
+    runtime::sparse_group_reduce_workspace ws;
+    runtime::init(&ws);
+    if (!runtime::setup(&ws, 0)) return 0;
+    runtime::group_mask_config_view groups{group_count, nullptr, d_masks};
+    runtime::row_feature_mask_view mv = masks_of(m);
+    runtime::sparse_group_filter_params filter{f->min_total, f->min_detected_features, f->max_group_fraction,
+                                               f->fraction_group_index};
+    runtime::sparse_group_reduce_result res{};
+    const device::blocked_ell_view *v = reinterpret_cast<const device::blocked_ell_view *>(src);
+    const int ok = time_calls([&] { return runtime::compute_sparse_group_reduce(v, &ws, &groups, &mv, &filter, &res); },
+                              ws.stream, warmup, reps, ms_per_call);
+    runtime::clear(&ws);
     return ok;
 }
 
