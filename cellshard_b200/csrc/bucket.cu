@@ -6,10 +6,17 @@
 //   CUB DeviceRadixSort::SortPairs over all 32 key bits) -> major_nnz_sorted,
 //   major_order_out; equal-count bucket offsets where the first n % B buckets
 //   take one extra row (fill_equal_count_bucket_offsets.cuh).
-//   Here the sort is an LSD radix sort of four 8-bit digit passes; each pass is
-//   a stable counting sort: per-tile digit histograms laid out digit-major so a
-//   single exclusive scan yields every (digit, tile) base, then an in-order
-//   ranked scatter (warp match on the digit + per-warp running counts).
+//   Here the sort is an LSD radix sort of 8-bit digit passes in the onesweep
+//   style: the counting kernel also builds the global digit histograms of all
+//   four passes (they depend only on the keys, not on their order) and the
+//   largest count; each pass is one kernel whose CTAs take tiles in start
+//   order, rank their keys stably (warp match on the digit + per-warp running
+//   counts), find each digit's offset among earlier tiles by a decoupled
+//   look-back over the tiles' published counts, and scatter.  Passes 3 and 4
+//   return at once when every count is below 2^16 (the keys are then sorted
+//   after two passes).  Look-back waits are bounded; one that runs out sets
+//   word 0 of the sort scratch (a status word, CS_STATUS_* style; 1 = a wait
+//   ran out).
 // Power-of-two bins (no reference function): bin k >= 1 holds counts in
 //   [2^k, 2^(k+1)), bin 0 holds 0 and 1; offsets are lower bounds in the sorted
 //   counts, so they are pinned by the sort.
@@ -46,10 +53,24 @@ __device__ __forceinline__ uint32_t find_part(uint32_t row, const uint32_t *offs
     return count;
 }
 
-// counts + identity; `parts` == nullptr for a single matrix
-__global__ void count_kernel(uint32_t n, const uint32_t *__restrict__ ptr, const uint32_t *const *__restrict__ parts,
-                             const uint32_t *__restrict__ part_offsets, uint32_t part_count,
-                             uint32_t *__restrict__ nnz, uint32_t *__restrict__ order_in) {
+// counts + identity + global digit histograms of the 4 passes + max count
+__global__ void __launch_bounds__(256) count_hist_kernel(uint32_t n, const uint32_t *__restrict__ ptr,
+                                                         const uint32_t *const *__restrict__ parts,
+                                                         const uint32_t *__restrict__ part_offsets,
+                                                         uint32_t part_count, uint32_t *__restrict__ nnz,
+                                                         uint32_t *__restrict__ order_in, uint32_t *__restrict__ ghist,
+                                                         uint32_t *__restrict__ max_key, uint32_t buckets,
+                                                         uint32_t *__restrict__ offsets) {
+    __shared__ uint32_t h[4][kRadix];
+    // equal-count bucket offsets (fill_equal_count_bucket_offsets) by block 0
+    if (blockIdx.x == 0u && offsets != nullptr) {
+        const uint32_t size = n / buckets, rem = n % buckets;
+        for (uint32_t b = threadIdx.x; b <= buckets; b += blockDim.x)
+            offsets[b] = b == buckets ? n : b * size + min(b, rem);
+    }
+    for (uint32_t i = threadIdx.x; i < 4u * kRadix; i += blockDim.x) (&h[0][0])[i] = 0u;
+    __syncthreads();
+    uint32_t mx = 0u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t c;
         if (parts == nullptr) {
@@ -62,46 +83,97 @@ __global__ void count_kernel(uint32_t n, const uint32_t *__restrict__ ptr, const
         }
         nnz[i] = c;
         order_in[i] = i;
+        mx = max(mx, c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) atomicAdd(&h[q][(c >> (8 * q)) & 0xffu], 1u);
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31u) == 0u && mx != 0u) atomicMax(max_key, mx);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 4u * kRadix; i += blockDim.x) {
+        const uint32_t v = (&h[0][0])[i];
+        if (v != 0u) atomicAdd(ghist + i, v);
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t *__restrict__ keys, uint32_t n,
-                                                                  uint32_t shift, uint32_t tiles,
-                                                                  uint32_t *__restrict__ hist) {
-    __shared__ uint32_t h[kRadix];
-    h[threadIdx.x] = 0u;
-    __syncthreads();
-    const uint32_t base = blockIdx.x * kTileKeys;
-    for (uint32_t i = threadIdx.x; i < kTileKeys; i += blockDim.x) {
-        const uint32_t k = base + i;
-        if (k < n) atomicAdd(h + ((keys[k] >> shift) & 0xffu), 1u);
-    }
-    __syncthreads();
-    hist[(std::size_t) threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+constexpr unsigned long long kLookAggregate = 1ull << 62;
+constexpr unsigned long long kLookInclusive = 2ull << 62;
+constexpr unsigned long long kLookValue = (1ull << 62) - 1ull;
+constexpr uint32_t kLookSpin = 1u << 22;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
 }
 
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint32_t *__restrict__ keys,
-                                                                     const uint32_t *__restrict__ vals, uint32_t n,
-                                                                     uint32_t shift, uint32_t tiles,
-                                                                     const uint32_t *__restrict__ base,
-                                                                     uint32_t *__restrict__ out_keys,
-                                                                     uint32_t *__restrict__ out_vals) {
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// One stable counting-sort pass over digit (key >> shift) & 255.  vals ==
+// nullptr means the identity (the row ids).  Tiles are taken in start order so
+// every look-back target belongs to a CTA that is already running.
+__global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
+    const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, uint32_t n, uint32_t shift,
+    const uint32_t *__restrict__ ghist, unsigned long long *__restrict__ look, uint32_t *__restrict__ tile_counter,
+    const uint32_t *__restrict__ max_key, uint32_t skip_below, uint32_t *__restrict__ out_keys,
+    uint32_t *__restrict__ out_vals, uint32_t *__restrict__ status) {
     __shared__ uint32_t wc[kSortWarps][kRadix];
+    __shared__ uint32_t scan33[33];
+    __shared__ uint32_t tile_s;
+    if (skip_below != 0u && *max_key < skip_below) return; // uniform: the pass changes nothing
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
     for (uint32_t d = lane; d < kRadix; d += 32u) wc[warp][d] = 0u;
-    __syncwarp();
-    const uint32_t wbase = blockIdx.x * kTileKeys + warp * kKeysPerWarp;
-    for (uint32_t b = 0; b < kKeysPerWarp; b += 32u) {
-        const uint32_t k = wbase + b + lane;
-        const uint32_t d = k < n ? (keys[k] >> shift) & 0xffu : kRadix;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (d < kRadix && lane == (unsigned) (__ffs(peers) - 1)) wc[warp][d] += __popc(peers);
+    __syncthreads();
+    const uint32_t t = tile_s;
+    const uint32_t wbase = t * kTileKeys + warp * kKeysPerWarp;
+    uint32_t kk[kKeysPerWarp / 32u], pk[kKeysPerWarp / 32u];
+#pragma unroll
+    for (uint32_t b = 0; b < kKeysPerWarp / 32u; ++b) {
+        const uint32_t k = wbase + b * 32u + lane;
+        kk[b] = k < n ? __ldcg(keys + k) : 0u;
+        const uint32_t d = k < n ? (kk[b] >> shift) & 0xffu : kRadix;
+        pk[b] = __match_any_sync(0xffffffffu, d);
+        if (d < kRadix && lane == (unsigned) (__ffs(pk[b]) - 1)) wc[warp][d] += __popc(pk[b]);
         __syncwarp();
     }
     __syncthreads();
     {
         const uint32_t d = threadIdx.x; // kSortThreads == kRadix
-        uint32_t run = base[(std::size_t) d * tiles + blockIdx.x];
+        uint32_t cnt = 0u;
+#pragma unroll
+        for (unsigned w = 0; w < kSortWarps; ++w) cnt += wc[w][d];
+        unsigned long long *mine = look + (std::size_t) t * kRadix + d;
+        uint32_t excl = 0u;
+        if (t == 0u) {
+            st_release_u64(mine, kLookInclusive | cnt);
+        } else {
+            st_release_u64(mine, kLookAggregate | cnt);
+            bool ok = true;
+            for (uint32_t j = t; j-- > 0u;) {
+                unsigned long long v = 0ull;
+                uint32_t it = 0u;
+                while (((v = ld_acquire_u64(look + (std::size_t) j * kRadix + d)) & ~kLookValue) == 0ull) {
+                    if (++it >= kLookSpin) {
+                        ok = false;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                if (!ok) break;
+                excl += (uint32_t) (v & kLookValue);
+                if (v & kLookInclusive) break;
+            }
+            if (!ok) atomicOr(status, 1u);
+            st_release_u64(mine, kLookInclusive | (unsigned long long) (excl + cnt));
+        }
+        // global base of digit d: exclusive scan of the pass's digit totals
+        uint32_t tot;
+        const uint32_t gbase = block_exclusive_scan(ghist[d], scan33, tot);
+        uint32_t run = gbase + excl;
+#pragma unroll
         for (unsigned w = 0; w < kSortWarps; ++w) {
             const uint32_t c = wc[w][d];
             wc[w][d] = run;
@@ -110,27 +182,20 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint3
     }
     __syncthreads();
     const unsigned lt = (1u << lane) - 1u;
-    for (uint32_t b = 0; b < kKeysPerWarp; b += 32u) {
-        const uint32_t k = wbase + b + lane;
-        const uint32_t key = k < n ? keys[k] : 0u;
-        const uint32_t d = k < n ? (key >> shift) & 0xffu : kRadix;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+#pragma unroll
+    for (uint32_t b = 0; b < kKeysPerWarp / 32u; ++b) {
+        const uint32_t k = wbase + b * 32u + lane;
+        const uint32_t d = k < n ? (kk[b] >> shift) & 0xffu : kRadix;
         uint32_t pos = 0u;
-        if (d < kRadix) pos = wc[warp][d] + __popc(peers & lt);
+        if (d < kRadix) pos = wc[warp][d] + __popc(pk[b] & lt);
         __syncwarp();
         if (d < kRadix) {
-            out_keys[pos] = key;
-            out_vals[pos] = vals[k];
-            if (lane == (unsigned) (__ffs(peers) - 1)) wc[warp][d] += __popc(peers);
+            out_keys[pos] = kk[b];
+            out_vals[pos] = vals != nullptr ? __ldcg(vals + k) : k;
+            if (lane == (unsigned) (__ffs(pk[b]) - 1)) wc[warp][d] += __popc(pk[b]);
         }
         __syncwarp();
     }
-}
-
-__global__ void equal_count_offsets_kernel(uint32_t n, uint32_t buckets, uint32_t *__restrict__ offsets) {
-    const uint32_t size = n / buckets, rem = n % buckets;
-    for (uint32_t b = threadIdx.x; b <= buckets; b += blockDim.x)
-        offsets[b] = b == buckets ? n : b * size + min(b, rem);
 }
 
 __global__ void pow2_bins_kernel(const uint32_t *__restrict__ sorted, uint32_t n, uint32_t *__restrict__ bins) {
@@ -225,42 +290,30 @@ uint32_t clamp_buckets(uint32_t n, uint32_t requested) {
 }
 
 struct sort_layout {
-    uint32_t *tmp_keys, *tmp_vals, *hist;
-    void *scan_tmp;
-    std::size_t scan_bytes, bytes;
+    uint32_t *status;             // word 0 of the scratch
+    uint32_t *max_key;
+    uint32_t *tile_counters;      // [4]
+    uint32_t *ghist;              // [4][256]
+    unsigned long long *look;     // [4][tiles][256]
+    uint32_t *tmp_keys, *tmp_vals;
+    std::size_t clear_bytes, bytes;
     uint32_t tiles;
 };
 
 void make_sort_layout(uint32_t n, void *base, std::size_t cap, sort_layout *l) {
     l->tiles = (n + kTileKeys - 1u) / kTileKeys;
     scratch_carver c(base, cap);
+    // status, max, counters and histograms first, then the look-back words:
+    // one memset clears them all
+    l->status = c.take<uint32_t>(8);
+    l->max_key = l->status + 1;
+    l->tile_counters = l->status + 2;
+    l->ghist = c.take<uint32_t>(4u * kRadix);
+    l->look = c.take<unsigned long long>((std::size_t) 4u * l->tiles * kRadix);
+    l->clear_bytes = c.used;
     l->tmp_keys = c.take<uint32_t>((std::size_t) n + 1u);
     l->tmp_vals = c.take<uint32_t>((std::size_t) n + 1u);
-    l->hist = c.take<uint32_t>((std::size_t) l->tiles * kRadix + 1u);
-    l->scan_bytes = scan_u32_scratch_bytes((std::size_t) l->tiles * kRadix);
-    l->scan_tmp = c.take<char>(l->scan_bytes);
     l->bytes = c.used;
-}
-
-// Stable ascending sort of keys (with values) into out_keys / out_vals.
-int radix_sort_pairs(const uint32_t *keys, const uint32_t *vals, uint32_t n, uint32_t *out_keys, uint32_t *out_vals,
-                     const sort_layout &l, cudaStream_t stream) {
-    const uint32_t *ik = keys, *iv = vals;
-    for (int pass = 0; pass < 4; ++pass) {
-        uint32_t *ok = (pass % 2 == 0) ? l.tmp_keys : out_keys;
-        uint32_t *ov = (pass % 2 == 0) ? l.tmp_vals : out_vals;
-        const uint32_t shift = 8u * (uint32_t) pass;
-        radix_hist_kernel<<<l.tiles, kSortThreads, 0, stream>>>(ik, n, shift, l.tiles, l.hist);
-        if (!launch_ok("radix_hist_kernel")) return 0;
-        if (!scan_exclusive_u32(l.hist, l.hist, (std::size_t) l.tiles * kRadix, false, l.scan_tmp, l.scan_bytes,
-                                stream))
-            return 0;
-        radix_scatter_kernel<<<l.tiles, kSortThreads, 0, stream>>>(ik, iv, n, shift, l.tiles, l.hist, ok, ov);
-        if (!launch_ok("radix_scatter_kernel")) return 0;
-        ik = ok;
-        iv = ov;
-    }
-    return 1;
 }
 
 int plan_common(uint32_t n, const uint32_t *ptr, const uint32_t *const *parts, const uint32_t *part_offsets,
@@ -276,12 +329,22 @@ int plan_common(uint32_t n, const uint32_t *ptr, const uint32_t *const *parts, c
         set_error("major_nnz_bucket_plan: sort scratch %zu < %zu bytes", tmp_bytes, l.bytes);
         return 0;
     }
-    count_kernel<<<grid1d(n, 256), 256, 0, stream>>>(n, ptr, parts, part_offsets, part_count, d_nnz, d_order_in);
-    if (!launch_ok("count_kernel")) return 0;
-    if (!radix_sort_pairs(d_nnz, d_order_in, n, d_sorted, d_order_out, l, stream)) return 0;
-    if (d_offsets != nullptr) {
-        equal_count_offsets_kernel<<<1, 256, 0, stream>>>(n, clamp_buckets(n, requested), d_offsets);
-        if (!launch_ok("equal_count_offsets_kernel")) return 0;
+    if (!cuda_ok(cudaMemsetAsync(l.status, 0, l.clear_bytes, stream), "plan scratch clear")) return 0;
+    count_hist_kernel<<<grid1d(n, 256), 256, 0, stream>>>(n, ptr, parts, part_offsets, part_count, d_nnz, d_order_in,
+                                                          l.ghist, l.max_key, clamp_buckets(n, requested), d_offsets);
+    if (!launch_ok("count_hist_kernel")) return 0;
+    // passes 0 and 1 always run (they leave the result in the output arrays);
+    // passes 2 and 3 only when some count reaches 2^16
+    const uint32_t *ik = d_nnz, *iv = nullptr;
+    for (uint32_t pass = 0; pass < 4u; ++pass) {
+        uint32_t *ok = (pass % 2u == 0u) ? l.tmp_keys : d_sorted;
+        uint32_t *ov = (pass % 2u == 0u) ? l.tmp_vals : d_order_out;
+        onesweep_pass_kernel<<<l.tiles, kSortThreads, 0, stream>>>(
+            ik, iv, n, 8u * pass, l.ghist + pass * kRadix, l.look + (std::size_t) pass * l.tiles * kRadix,
+            l.tile_counters + pass, l.max_key, pass >= 2u ? (1u << 16) : 0u, ok, ov, l.status);
+        if (!launch_ok("onesweep_pass_kernel")) return 0;
+        ik = ok;
+        iv = ov;
     }
     return 1;
 }
