@@ -383,6 +383,8 @@ def ref_gpu() -> C.CDLL:
         g.csrefgpu_transpose_timed.argtypes = [u32, u32, u32, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, fp]
         g.csrefgpu_major_nnz_plan_timed.argtypes = [vp, u32, vp, vp, vp, vp, vp, u32, C.c_int, C.c_int, fp]
         g.csrefgpu_group_reduce_blocked_ell_timed.argtypes = [vp, vp, u32, vp, vp, C.c_int, C.c_int, fp]
+        g.csrefgpu_group_reduce_sliced_ell_timed.argtypes = [vp, vp, u32, vp, vp, C.c_int, C.c_int, fp]
+        g.csrefgpu_group_reduce_compressed_timed.argtypes = [vp, vp, u32, vp, vp, C.c_int, C.c_int, fp]
         _rg = g
     return _rg
 

@@ -325,4 +325,42 @@ int csrefgpu_group_reduce_blocked_ell_timed(const cs_blocked_ell_view *src, cons
     return ok;
 }
 
+
+int csrefgpu_group_reduce_sliced_ell_timed(const cs_sliced_ell_view *src, const uint32_t *d_masks,
+                                           uint32_t group_count, const cs_row_feature_mask_view *m,
+                                           const cs_group_filter_params *f, int warmup, int reps, float *ms_per_call) {
+    runtime::sparse_group_reduce_workspace ws;
+    runtime::init(&ws);
+    if (!runtime::setup(&ws, 0)) return 0;
+    runtime::group_mask_config_view groups{group_count, nullptr, d_masks};
+    runtime::row_feature_mask_view mv = masks_of(m);
+    runtime::sparse_group_filter_params filter{f->min_total, f->min_detected_features, f->max_group_fraction,
+                                               f->fraction_group_index};
+    runtime::sparse_group_reduce_result res{};
+    const device::sliced_ell_view *v = reinterpret_cast<const device::sliced_ell_view *>(src);
+    const int ok = time_calls([&] { return runtime::compute_sparse_group_reduce(v, &ws, &groups, &mv, &filter, &res); },
+                              ws.stream, warmup, reps, ms_per_call);
+    runtime::clear(&ws);
+    return ok;
+}
+
+int csrefgpu_group_reduce_compressed_timed(const cs_compressed_view *src, const uint32_t *d_masks,
+                                           uint32_t group_count, const cs_row_feature_mask_view *m,
+                                           const cs_group_filter_params *f, int warmup, int reps, float *ms_per_call) {
+    runtime::sparse_group_reduce_workspace ws;
+    runtime::init(&ws);
+    if (!runtime::setup(&ws, 0)) return 0;
+    runtime::group_mask_config_view groups{group_count, nullptr, d_masks};
+    runtime::row_feature_mask_view mv = masks_of(m);
+    runtime::sparse_group_filter_params filter{f->min_total, f->min_detected_features, f->max_group_fraction,
+                                               f->fraction_group_index};
+    runtime::sparse_group_reduce_result res{};
+    const device::compressed_view *v = reinterpret_cast<const device::compressed_view *>(src);
+    const int ok = time_calls(
+        [&] { return runtime::compute_sparse_group_reduce_compressed_fallback(v, &ws, &groups, &mv, &filter, &res); },
+        ws.stream, warmup, reps, ms_per_call);
+    runtime::clear(&ws);
+    return ok;
+}
+
 } // extern "C"

@@ -90,10 +90,8 @@ def test_reference_gpu_points(cuda, orc):
         assert torch.equal(a, b)
     out["nnz_plan_ms"] = {"ours": ms, "reference_cub": ms_ref.value}
 
-    # mask_groups reduce over Blocked-ELL-16: this library's kernel vs the reference's
-    bell = blocked_ell_from_csr(csr, 16)
-    del csr
-    torch.cuda.empty_cache()
+    # mask_groups reduce over the compressed, Sliced-ELL and Blocked-ELL forms:
+    # this library's kernels vs the reference's
     rng = np.random.default_rng(5)
     G = 8
     masks = (rng.integers(0, 1 << G, Cc) & rng.integers(0, 2, Cc) * 0xFF).astype(np.uint32)
@@ -101,10 +99,45 @@ def test_reference_gpu_points(cuda, orc):
     rk = torch.from_numpy((rng.random(R) < 0.7).astype(np.uint8)).cuda()
     fk = torch.from_numpy((rng.random(Cc) < 0.6).astype(np.uint8)).cuda()
     filt = runtime.FilterParams(10.0, 5, 0.9, 0)
-    ours = runtime.compute_sparse_group_reduce(bell, d_masks, G, rk, fk, filt)
-    ms = _time_ours(lambda: runtime.compute_sparse_group_reduce(bell, d_masks, G, rk, fk, filt))
     mv = _abi.RowFeatureMaskView(ptr(rk), ptr(fk), None, None)
     fp = filt.c()
+
+    def compare(ours, bridge, v):
+        ref = {k: torch.empty_like(t) for k, t in ours.items() if t is not None}
+        ro = _abi.GroupReduceOut(ptr(ref["row_totals"]), ptr(ref["detected_features"]), ptr(ref["max_values"]),
+                                 ptr(ref["row_keep"]), ptr(ref["group_counts"]), ptr(ref["group_percentages"]))
+        assert bridge(C.byref(v), ptr(d_masks), G, C.byref(mv), C.byref(fp), C.byref(ro)) == 1
+        torch.cuda.synchronize()
+        for k in ("row_totals", "detected_features", "max_values", "row_keep", "group_counts"):
+            assert torch.equal(ours[k], ref[k]), k
+
+    ours = runtime.compute_sparse_group_reduce(csr, d_masks, G, rk, fk, filt)
+    ms = _time_ours(lambda: runtime.compute_sparse_group_reduce(csr, d_masks, G, rk, fk, filt))
+    v = csr.view()
+    assert rg.csrefgpu_group_reduce_compressed_timed(C.byref(v), ptr(d_masks), G, C.byref(mv), C.byref(fp), 2, REPS,
+                                                     C.byref(ms_ref)) == 1
+    compare(ours, rg.csrefgpu_group_reduce_compressed, v)
+    out["mask_groups_reduce_compressed_ms"] = {"ours": ms, "reference": ms_ref.value}
+
+    from cellshard_b200.device import sliced_ell_from_csr
+
+    sell = sliced_ell_from_csr(csr, 32)
+    ours = runtime.compute_sparse_group_reduce(sell, d_masks, G, rk, fk, filt)
+    ms = _time_ours(lambda: runtime.compute_sparse_group_reduce(sell, d_masks, G, rk, fk, filt))
+    v = sell.view()
+    assert rg.csrefgpu_group_reduce_sliced_ell_timed(C.byref(v), ptr(d_masks), G, C.byref(mv), C.byref(fp), 2, REPS,
+                                                     C.byref(ms_ref)) == 1
+    compare(ours, rg.csrefgpu_group_reduce_sliced_ell, v)
+    out["mask_groups_reduce_sliced_ms"] = {"ours": ms, "reference": ms_ref.value,
+                                           "bytes": int(sell.col_idx.numel()) * 6}
+    del sell
+    torch.cuda.empty_cache()
+
+    bell = blocked_ell_from_csr(csr, 16)
+    del csr
+    torch.cuda.empty_cache()
+    ours = runtime.compute_sparse_group_reduce(bell, d_masks, G, rk, fk, filt)
+    ms = _time_ours(lambda: runtime.compute_sparse_group_reduce(bell, d_masks, G, rk, fk, filt))
     v = bell.view()
     assert rg.csrefgpu_group_reduce_blocked_ell_timed(C.byref(v), ptr(d_masks), G, C.byref(mv), C.byref(fp), 2, REPS,
                                                       C.byref(ms_ref)) == 1
