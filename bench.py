@@ -62,9 +62,11 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["moments", "convert", "batched", "serving"], default="moments",
+    p.add_argument("--workload", choices=["moments", "convert", "mask_groups", "batched", "serving"],
+                   default="moments",
                    help="moments: the headline reduction; convert: per-kernel conversion throughput; "
-                        "batched: 256 uneven partitions -> Sliced-ELL + nnz plans in one persistent launch")
+                        "mask_groups: the masked group reduce over the compressed, Sliced-ELL and Blocked-ELL "
+                        "forms; batched: 256 uneven partitions -> Sliced-ELL + nnz plans in one persistent launch")
     p.add_argument("--parts", type=int, default=256, help="batched: partitions")
     p.add_argument("--total-rows", type=int, default=8_000_000, help="batched: rows over all partitions")
     p.add_argument("--resident-gb", type=float, default=135.0, help="serving: resident Blocked-ELL bytes")
@@ -491,6 +493,76 @@ def run_convert(args):
     emit("rebuild", ms_r, 6 * nnz + 4 * (R + 1) + 6 * nnz + 4 * (R + 1) + 4 * R)
 
 
+def run_mask_groups(args):
+    """mask_groups reduce (row totals, maxima, detected counts, 8 feature-group sums,
+    keep decision) over the grouped-reduction matrix held as CSR, Sliced-ELL (h 32) and
+    Blocked-ELL-16, with 70 % of rows and 60 % of features kept.  One JSON line per
+    format: device time (CUDA events, mean of --steps after --warmup) and algorithmic
+    GB/s = the stored entries / slots of the kept rows, each row's metadata and flag,
+    the column tables and the outputs, each counted once."""
+    import torch
+
+    from cellshard_b200 import runtime, synth
+    from cellshard_b200.device import blocked_ell_from_csr, sliced_ell_from_csr
+
+    torch.cuda.set_device(0)
+    spec = synth.grouped_reduction_spec(args.rows)
+    csr = synth.make_csr(spec)
+    R, Cc, nnz = spec.rows, spec.cols, csr.nnz
+    peak, _ = measured_peak()
+    rng = np.random.default_rng(5)
+    G = 8
+    masks = (rng.integers(0, 1 << G, Cc) & rng.integers(0, 2, Cc) * 0xFF).astype(np.uint32)
+    gm = torch.from_numpy(masks.view(np.int32)).cuda()
+    rk_h = rng.random(R) < 0.7
+    rk = torch.from_numpy(rk_h.astype(np.uint8)).cuda()
+    fk = torch.from_numpy((rng.random(Cc) < 0.6).astype(np.uint8)).cuda()
+    filt = runtime.FilterParams(10.0, 5, 0.9, 0)
+    kept = torch.from_numpy(rk_h).cuda()
+    row_nnz = (csr.ptr[1:] - csr.ptr[:-1]).long()
+    common = R + Cc * 5 + R * 13 + R * G * 8  # row flags, column tables, outputs
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for a, b in ev:
+            a.record()
+            fn()
+            b.record()
+        torch.cuda.synchronize()
+        return float(np.mean([a.elapsed_time(b) for a, b in ev]))
+
+    def emit(fmt, ms, nbytes, extra=None):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        d = {"workload": "mask_groups", "format": fmt, "ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs,
+             "peak_gbs": peak, "frac": gbs / peak, "rows": R, "cols": Cc, "nnz": nnz, "groups": G,
+             "kept_rows": int(rk_h.sum())}
+        if extra:
+            d.update(extra)
+        print(json.dumps(d), flush=True)
+
+    ms = timed(lambda: runtime.compute_sparse_group_reduce(csr, gm, G, rk, fk, filt))
+    emit("compressed", ms, common + 4 * (R + 1) + 6 * int(row_nnz[kept].sum()))
+    sell = sliced_ell_from_csr(csr, 32)
+    widths = sell.slice_widths.long().repeat_interleave(32)[:R]
+    ms = timed(lambda: runtime.compute_sparse_group_reduce(sell, gm, G, rk, fk, filt))
+    emit("sliced_ell", ms, common + 4 * 3 * sell.slice_count + 6 * int(widths[kept].sum()),
+         {"total_slots": int(sell.col_idx.numel())})
+    del sell
+    torch.cuda.empty_cache()
+    bell = blocked_ell_from_csr(csr, BLOCK)
+    del csr
+    torch.cuda.empty_cache()
+    W = bell.ell_cols // BLOCK
+    kept_blocks = int(kept.view(-1)[: (R // BLOCK) * BLOCK].view(-1, BLOCK).any(1).sum()) + (
+        int(kept[(R // BLOCK) * BLOCK:].any()) if R % BLOCK else 0)
+    ms = timed(lambda: runtime.compute_sparse_group_reduce(bell, gm, G, rk, fk, filt))
+    emit("blocked_ell", ms, common + 2 * bell.ell_cols * int(rk_h.sum()) + 4 * W * kept_blocks,
+         {"ell_cols": bell.ell_cols})
+
+
 BATCH_CANDIDATES = (16, 32, 64)
 BATCH_BUCKETS = 16
 
@@ -815,6 +887,9 @@ def main():
         return
     if args.workload == "convert":
         run_convert(args)
+        return
+    if args.workload == "mask_groups":
+        run_mask_groups(args)
         return
     if args.workload == "batched":
         run_batched(args)

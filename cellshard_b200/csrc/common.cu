@@ -31,6 +31,16 @@ int sm_count() {
     return g_sm_count[dev];
 }
 
+unsigned resident_grid(const void *kernel, unsigned threads, std::size_t smem, std::size_t needed) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (int) threads, smem) != cudaSuccess ||
+        per_sm <= 0)
+        per_sm = 1;
+    std::size_t g = (std::size_t) sm_count() * (std::size_t) per_sm;
+    if (g > needed) g = needed;
+    return g == 0u ? 1u : (unsigned) g;
+}
+
 // ---------------------------------------------------------------------------
 // Scan: 256 threads x 16 items = 4096 items per tile.
 // ---------------------------------------------------------------------------

@@ -33,6 +33,11 @@ inline cudaStream_t as_stream(cs_stream_t s) { return reinterpret_cast<cudaStrea
 // Number of SMs on the current device (cached per device ordinal).
 int sm_count();
 
+// Blocks of `kernel` resident on the whole device at once (SMs x blocks per
+// SM for this block size and dynamic shared memory), at most `needed` and
+// at least 1: a grid-stride kernel launched with it runs in a single wave.
+unsigned resident_grid(const void *kernel, unsigned threads, std::size_t smem, std::size_t needed);
+
 inline std::size_t align_up(std::size_t v, std::size_t a) { return (v + a - 1u) / a * a; }
 
 // Bump allocator over caller scratch; every sub-buffer is 256-byte aligned.
@@ -75,6 +80,12 @@ __device__ __forceinline__ uint4 ld_stream_v4(const void *p) {
     asm("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
                  : "l"(p));
+    return r;
+}
+
+__device__ __forceinline__ uint2 ld_stream_v2(const void *p) {
+    uint2 r;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.v2.u32 {%0,%1}, [%2];" : "=r"(r.x), "=r"(r.y) : "l"(p));
     return r;
 }
 
@@ -130,6 +141,23 @@ __device__ __forceinline__ uint32_t warp_match_digit(uint32_t d, bool valid) {
         m &= bit ? bb : ~bb;
     }
     return valid ? m : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// 16-byte asynchronous copies global -> shared (per thread; completion is
+// tracked per thread in commit groups).  Both addresses 16-byte aligned.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_16(void *sdst, const void *gsrc) {
+    const uint32_t s = (uint32_t) __cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// Waits until at most N of this thread's committed groups are pending.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // ---------------------------------------------------------------------------

@@ -22,31 +22,30 @@ constexpr unsigned kRowWarps = 8;
 constexpr unsigned kRowThreads = kRowWarps * 32;
 constexpr uint32_t kStagePairs = 128; // per-warp (feature, value) staging in the Blocked-ELL reduce
 
+// Per-lane running values of one row.  The group sums live in registers:
+// GR (8, 16 or 32, or 0 without groups) accumulators updated with one
+// predicated add per group for every value, so lanes whose masks have
+// different numbers of bits do not serialise the warp on a per-bit loop.
+// They reach shared memory once per row (finish_row).
+template <unsigned GR>
 struct row_acc {
     float sum;
     float vmax;
     uint32_t detected;
+    float g[GR != 0u ? GR : 1u];
 };
+
+template <unsigned GR>
+__device__ __forceinline__ void init_acc(row_acc<GR> &a) {
+    a.sum = 0.0f;
+    a.vmax = 0.0f;
+    a.detected = 0u;
+#pragma unroll
+    for (unsigned k = 0; k < (GR != 0u ? GR : 1u); ++k) a.g[k] = 0.0f;
+}
 
 __device__ __forceinline__ bool feature_kept(const uint8_t *feature_keep, uint32_t c) {
     return feature_keep == nullptr || feature_keep[c] != 0u;
-}
-
-// Adds one participating value.  acc_col is this lane's column of the warp's
-// [32 groups x 32 lanes] accumulator, or null when there are no groups.
-__device__ __forceinline__ void add_value(row_acc &a, float v, uint32_t gene, const uint32_t *group_masks,
-                                          uint32_t group_count, float *acc_col) {
-    a.sum += v;
-    a.vmax = fmaxf(a.vmax, v);
-    a.detected += 1u;
-    if (acc_col != nullptr) {
-        uint32_t m = group_masks[gene];
-        while (m != 0u) {
-            const uint32_t g = __ffs(m) - 1u;
-            if (g < group_count) acc_col[g * 32u] += v;
-            m &= m - 1u;
-        }
-    }
 }
 
 // Bit q set when fp16 value q of the 8 packed in v (low half first) is
@@ -62,25 +61,40 @@ __device__ __forceinline__ uint32_t nonzero_bits(const uint4 &v) {
     return b;
 }
 
-// add_value with the column's group mask already loaded.
-__device__ __forceinline__ void add_value_masked(row_acc &a, float v, uint32_t m, uint32_t group_count,
-                                                 float *acc_col) {
+// Adds one participating value whose column has group mask m.  Bits at or
+// above the call's group count land in accumulators that are never written
+// out, so they are ignored as the reference ignores them.
+template <unsigned GR>
+__device__ __forceinline__ void add_value_masked(row_acc<GR> &a, float v, uint32_t m) {
     a.sum += v;
     a.vmax = fmaxf(a.vmax, v);
     a.detected += 1u;
-    if (acc_col != nullptr) {
-        while (m != 0u) {
-            const uint32_t g = __ffs(m) - 1u;
-            if (g < group_count) acc_col[g * 32u] += v;
-            m &= m - 1u;
-        }
+    if constexpr (GR != 0u) {
+#pragma unroll
+        for (unsigned k = 0; k < GR; ++k)
+            if ((m >> k) & 1u) a.g[k] += v;
     }
 }
 
+template <unsigned GR>
+__device__ __forceinline__ void add_value(row_acc<GR> &a, float v, uint32_t gene, const uint32_t *group_masks) {
+    add_value_masked(a, v, GR != 0u ? __ldg(group_masks + gene) : 0u);
+}
+
 // Warp epilogue shared by the three formats (mask_groups.cu:171-194).
-__device__ __forceinline__ void finish_row(uint32_t row, row_acc a, float *acc_col, uint32_t group_count,
-                                           const cs_group_filter_params &filter, const cs_group_reduce_out &out) {
+// acc_col is this lane's column of the warp's [group_count x 32 lanes]
+// shared block (null without groups): the lanes' group sums are written
+// there and each group's 32 partial sums are added by lane `group`.
+template <unsigned GR>
+__device__ __forceinline__ void finish_row(uint32_t row, const row_acc<GR> &a, float *acc_col,
+                                           uint32_t group_count, const cs_group_filter_params &filter,
+                                           const cs_group_reduce_out &out) {
     const unsigned lane = threadIdx.x & 31u;
+    if constexpr (GR != 0u) {
+#pragma unroll
+        for (unsigned k = 0; k < GR; ++k)
+            if (k < group_count) acc_col[k * 32u] = a.g[k];
+    }
     float sum = a.sum;
     float vmax = a.vmax;
     uint32_t det = a.detected;
@@ -133,20 +147,180 @@ __device__ __forceinline__ void empty_row(uint32_t row, uint32_t group_count, co
     }
 }
 
-__device__ __forceinline__ float *warp_acc_column(float *smem, bool groups) {
+// Each warp owns group_count rows of 32 lane columns (group_count <= 32), so
+// a call with few groups leaves most of the SM's shared memory to L1, where
+// the column mask and feature tables are gathered from.
+__device__ __forceinline__ float *warp_acc_column(float *smem, bool groups, uint32_t group_count) {
     if (!groups) return nullptr;
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    return smem + (std::size_t) warp * 1024u + lane; // [group][lane] -> g * 32 + lane
+    return smem + (std::size_t) warp * group_count * 32u + lane; // [group][lane] -> g * 32 + lane
 }
 
-__device__ __forceinline__ void zero_acc(float *acc_col) {
-    if (acc_col == nullptr) return;
-#pragma unroll 8
-    for (unsigned g = 0; g < 32u; ++g) acc_col[g * 32u] = 0.0f;
+// One stored (column, value) pair of a compressed or Sliced-ELL row.
+template <unsigned GR>
+__device__ __forceinline__ void add_entry(row_acc<GR> &a, uint32_t col, uint32_t h, uint32_t cols,
+                                          const uint8_t *feature_keep, const uint32_t *group_masks) {
+    if (col < cols && (h & 0x7fffu) != 0u && feature_kept(feature_keep, col))
+        add_value(a, h2f((uint16_t) h), col, group_masks);
+}
+
+// Reduces the entries [b, e) of one row held as parallel column / fp16 arrays
+// (a CSR row, or one Sliced-ELL row's slots).  The body moves through aligned
+// quads: per lane U 16-byte column vectors and U 8-byte value vectors are in
+// flight before any is used, and the column flags and group masks of all 4U
+// entries are gathered before the accumulation.  The unaligned head (< 4
+// entries) runs on lanes 0-2 and the tail (< 4) on lanes 3-5.  Requires idx
+// 16-byte and val 8-byte aligned.
+template <unsigned U, unsigned GR>
+__device__ __forceinline__ void reduce_span(const uint32_t *__restrict__ idx, const uint16_t *__restrict__ val,
+                                            std::size_t b, std::size_t e, uint32_t cols,
+                                            const uint8_t *__restrict__ feature_keep,
+                                            const uint32_t *__restrict__ group_masks, row_acc<GR> &a) {
+    const unsigned lane = threadIdx.x & 31u;
+    const std::size_t a4 = min(e, (b + 3u) & ~(std::size_t) 3u);
+    const std::size_t e4 = max(a4, e & ~(std::size_t) 3u);
+    {
+        const std::size_t i = lane < 3u ? b + lane : e4 + (lane - 3u);
+        if (lane < 3u ? i < a4 : (lane < 6u && i < e))
+            add_entry(a, __ldg(idx + i), __ldg(val + i), cols, feature_keep, group_masks);
+    }
+    const std::size_t q_end = e4 >> 2;
+    for (std::size_t q = (a4 >> 2) + lane; q < q_end; q += 32u * U) {
+        uint4 c[U];
+        uint2 h[U];
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            const std::size_t qi = q + 32u * u;
+            const bool in = qi < q_end;
+            c[u] = in ? ld_stream_v4(idx + qi * 4u) : make_uint4(cols, cols, cols, cols);
+            h[u] = in ? ld_stream_v2(val + qi * 4u) : make_uint2(0u, 0u);
+        }
+        uint32_t col[4 * U], hv[4 * U], m[4 * U];
+        bool ok[4 * U];
+        bool any = false;
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            col[4 * u + 0] = c[u].x;
+            col[4 * u + 1] = c[u].y;
+            col[4 * u + 2] = c[u].z;
+            col[4 * u + 3] = c[u].w;
+            hv[4 * u + 0] = h[u].x & 0xffffu;
+            hv[4 * u + 1] = h[u].x >> 16;
+            hv[4 * u + 2] = h[u].y & 0xffffu;
+            hv[4 * u + 3] = h[u].y >> 16;
+            any = any || ((h[u].x | h[u].y) & 0x7fff7fffu) != 0u;
+        }
+        // quads of zeros (Sliced-ELL padding past a row's end) skip the gathers
+        if (!any) continue;
+#pragma unroll
+        for (unsigned j = 0; j < 4 * U; ++j) {
+            ok[j] = col[j] < cols && (hv[j] & 0x7fffu) != 0u;
+            ok[j] = ok[j] && (feature_keep == nullptr || __ldg(feature_keep + col[j]) != 0u);
+            m[j] = ok[j] && GR != 0u ? __ldg(group_masks + col[j]) : 0u;
+        }
+#pragma unroll
+        for (unsigned j = 0; j < 4 * U; ++j)
+            if (ok[j]) add_value_masked(a, h2f((uint16_t) hv[j]), m[j]);
+    }
+}
+
+// One Blocked-ELL row, warp-wide (reads, accumulation and outputs).
+template <bool VEC, unsigned GR>
+__device__ __forceinline__ void bell_row(const cs_blocked_ell_view &src, uint32_t row,
+                                         const uint32_t *__restrict__ group_masks, uint32_t group_count,
+                                         const cs_row_feature_mask_view &masks, const cs_group_filter_params &filter,
+                                         const cs_group_reduce_out &out, float *acc_col, uint2 *stage) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t B = src.block_size;
+    const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
+    if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
+        empty_row(row, group_count, out);
+        return;
+    }
+    row_acc<GR> a;
+    init_acc(a);
+    const uint32_t rb = B != 0u ? row / B : 0u;
+    const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
+    const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
+    if (VEC) {
+        // U 16-byte vectors of values in flight per lane, loaded whether or
+        // not their slot is padding (they lie inside the row) so no value
+        // load waits for its block column.  The lane's nonzero values of
+        // the U vectors become a 32-bit mask; the warp compacts them
+        // (exclusive scan of the lanes' counts) into a per-warp staging
+        // buffer of (value, feature) pairs and then works through the pairs
+        // 32 at a time with every lane busy, instead of every lane stepping
+        // through all its slots while most of them hold zeros.
+        constexpr unsigned U = 4;
+        for (uint32_t base = lane * 8u; base < src.ell_cols; base += 256u * U) {
+            uint4 v[U];
+            uint32_t bc[U], gene0[U];
+    #pragma unroll
+            for (unsigned u = 0; u < U; ++u) {
+                const uint32_t e0 = base + u * 256u;
+                const bool in = e0 < src.ell_cols;
+                v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
+                bc[u] = in ? __ldg(bci + e0 / B) : CS_INVALID_COL;
+            }
+            // the feature flags are checked per staged value, not per vector
+            uint32_t nzall = 0u;
+    #pragma unroll
+            for (unsigned u = 0; u < U; ++u) {
+                const uint32_t e0 = base + u * 256u;
+                gene0[u] = bc[u] * B + (e0 % B);
+                if (bc[u] == CS_INVALID_COL) continue;
+                uint32_t nz = nonzero_bits(v[u]);
+                if (nz != 0u && gene0[u] + 8u > src.cols) {
+                    const uint32_t lim = gene0[u] < src.cols ? src.cols - gene0[u] : 0u; // < 8 here
+                    nz &= (1u << lim) - 1u;
+                }
+                nzall |= nz << (8u * u);
+            }
+            const uint32_t cnt = __popc(nzall);
+            const uint32_t incl = warp_inclusive_scan(cnt);
+            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+            const uint32_t excl = incl - cnt;
+            for (uint32_t p0 = 0; p0 < total; p0 += kStagePairs) {
+                uint32_t bits = nzall, k = excl;
+                while (bits != 0u && k < p0 + kStagePairs) {
+                    const uint32_t bitpos = __ffs(bits) - 1u;
+                    bits &= bits - 1u;
+                    if (k >= p0) {
+                        const uint32_t u = bitpos >> 3, q = bitpos & 7u;
+                        const uint4 vu = u < 2u ? (u == 0u ? v[0] : v[1]) : (u == 2u ? v[2] : v[3]);
+                        const uint32_t g0 = u < 2u ? (u == 0u ? gene0[0] : gene0[1])
+                                                   : (u == 2u ? gene0[2] : gene0[3]);
+                        const uint32_t wq = q < 4u ? (q < 2u ? vu.x : vu.y) : (q < 6u ? vu.z : vu.w);
+                        stage[k - p0] = make_uint2(g0 + q, (wq >> ((q & 1u) * 16u)) & 0xffffu);
+                    }
+                    ++k;
+                }
+                __syncwarp();
+                const uint32_t n = min(kStagePairs, total - p0);
+                for (uint32_t i = lane; i < n; i += 32u) {
+                    const uint2 pr = stage[i];
+                    if (!feature_kept(masks.feature_keep, pr.x)) continue;
+                    const uint32_t m = GR != 0u ? __ldg(group_masks + pr.x) : 0u;
+                    add_value_masked(a, h2f((uint16_t) pr.y), m);
+                }
+                __syncwarp();
+            }
+        }
+    } else {
+        for (uint32_t e = lane; e < src.ell_cols; e += 32u) {
+            const uint32_t slot = e / B;
+            const uint32_t bc = W != 0u ? bci[slot] : CS_INVALID_COL;
+            const uint32_t gene = bc != CS_INVALID_COL ? bc * B + (e - slot * B) : src.cols;
+            const uint16_t h = vrow[e];
+            if (half_nonzero(h) && gene < src.cols && feature_kept(masks.feature_keep, gene))
+                add_value(a, h2f(h), gene, group_masks);
+        }
+    }
     __syncwarp();
+    finish_row(row, a, acc_col, group_count, filter, out);
 }
 
-template <bool VEC>
+template <bool VEC, unsigned GR>
 __global__ void __launch_bounds__(kRowThreads) group_reduce_bell_kernel(cs_blocked_ell_view src,
                                                                          const uint32_t *__restrict__ group_masks,
                                                                          uint32_t group_count,
@@ -154,101 +328,12 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_bell_kernel(cs_block
                                                                          cs_group_filter_params filter,
                                                                          cs_group_reduce_out out) {
     extern __shared__ float gr_smem[];
-    const bool groups = group_masks != nullptr && group_count != 0u;
-    float *acc_col = warp_acc_column(gr_smem, groups);
+    float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
     // staging pairs follow the accumulator columns (if any)
-    uint2 *stage = reinterpret_cast<uint2 *>(gr_smem + (groups ? kRowWarps * 1024u : 0u)) +
+    uint2 *stage = reinterpret_cast<uint2 *>(gr_smem + (GR != 0u ? kRowWarps * group_count * 32u : 0u)) +
                    (threadIdx.x >> 5) * kStagePairs;
-    const unsigned lane = threadIdx.x & 31u;
-    const uint32_t B = src.block_size;
-    const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
-    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
-        if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
-            empty_row(row, group_count, out);
-            continue;
-        }
-        zero_acc(acc_col);
-        row_acc a{0.0f, 0.0f, 0u};
-        const uint32_t rb = B != 0u ? row / B : 0u;
-        const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
-        const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
-        if (VEC) {
-            // U 16-byte vectors of values in flight per lane, loaded whether or
-            // not their slot is padding (they lie inside the row) so no value
-            // load waits for its block column.  The lane's nonzero values of
-            // the U vectors become a 32-bit mask; the warp compacts them
-            // (exclusive scan of the lanes' counts) into a per-warp staging
-            // buffer of (value, feature) pairs and then works through the pairs
-            // 32 at a time with every lane busy, instead of every lane stepping
-            // through all its slots while most of them hold zeros.
-            constexpr unsigned U = 4;
-            for (uint32_t base = lane * 8u; base < src.ell_cols; base += 256u * U) {
-                uint4 v[U];
-                uint32_t bc[U], gene0[U];
-#pragma unroll
-                for (unsigned u = 0; u < U; ++u) {
-                    const uint32_t e0 = base + u * 256u;
-                    const bool in = e0 < src.ell_cols;
-                    v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
-                    bc[u] = in ? __ldg(bci + e0 / B) : CS_INVALID_COL;
-                }
-                // the feature flags are checked per staged value, not per vector
-                uint32_t nzall = 0u;
-#pragma unroll
-                for (unsigned u = 0; u < U; ++u) {
-                    const uint32_t e0 = base + u * 256u;
-                    gene0[u] = bc[u] * B + (e0 % B);
-                    if (bc[u] == CS_INVALID_COL) continue;
-                    uint32_t nz = nonzero_bits(v[u]);
-                    if (nz != 0u && gene0[u] + 8u > src.cols) {
-                        const uint32_t lim = gene0[u] < src.cols ? src.cols - gene0[u] : 0u; // < 8 here
-                        nz &= (1u << lim) - 1u;
-                    }
-                    nzall |= nz << (8u * u);
-                }
-                const uint32_t cnt = __popc(nzall);
-                const uint32_t incl = warp_inclusive_scan(cnt);
-                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-                const uint32_t excl = incl - cnt;
-                for (uint32_t p0 = 0; p0 < total; p0 += kStagePairs) {
-                    uint32_t bits = nzall, k = excl;
-                    while (bits != 0u && k < p0 + kStagePairs) {
-                        const uint32_t bitpos = __ffs(bits) - 1u;
-                        bits &= bits - 1u;
-                        if (k >= p0) {
-                            const uint32_t u = bitpos >> 3, q = bitpos & 7u;
-                            const uint4 vu = u < 2u ? (u == 0u ? v[0] : v[1]) : (u == 2u ? v[2] : v[3]);
-                            const uint32_t g0 = u < 2u ? (u == 0u ? gene0[0] : gene0[1])
-                                                       : (u == 2u ? gene0[2] : gene0[3]);
-                            const uint32_t wq = q < 4u ? (q < 2u ? vu.x : vu.y) : (q < 6u ? vu.z : vu.w);
-                            stage[k - p0] = make_uint2(g0 + q, (wq >> ((q & 1u) * 16u)) & 0xffffu);
-                        }
-                        ++k;
-                    }
-                    __syncwarp();
-                    const uint32_t n = min(kStagePairs, total - p0);
-                    for (uint32_t i = lane; i < n; i += 32u) {
-                        const uint2 pr = stage[i];
-                        if (!feature_kept(masks.feature_keep, pr.x)) continue;
-                        const uint32_t m = acc_col != nullptr ? __ldg(group_masks + pr.x) : 0u;
-                        add_value_masked(a, h2f((uint16_t) pr.y), m, group_count, acc_col);
-                    }
-                    __syncwarp();
-                }
-            }
-        } else {
-            for (uint32_t e = lane; e < src.ell_cols; e += 32u) {
-                const uint32_t slot = e / B;
-                const uint32_t bc = W != 0u ? bci[slot] : CS_INVALID_COL;
-                const uint32_t gene = bc != CS_INVALID_COL ? bc * B + (e - slot * B) : src.cols;
-                const uint16_t h = vrow[e];
-                if (half_nonzero(h) && gene < src.cols && feature_kept(masks.feature_keep, gene))
-                    add_value(a, h2f(h), gene, group_masks, group_count, acc_col);
-            }
-        }
-        __syncwarp();
-        finish_row(row, a, acc_col, group_count, filter, out);
-    }
+    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps)
+        bell_row<VEC, GR>(src, row, group_masks, group_count, masks, filter, out, acc_col, stage);
 }
 
 __device__ __forceinline__ uint32_t find_slice(const cs_sliced_ell_view &src, uint32_t row) {
@@ -266,6 +351,9 @@ __device__ __forceinline__ uint32_t find_slice(const cs_sliced_ell_view &src, ui
     return lo;
 }
 
+// VEC: col_idx 16-byte and val 8-byte aligned; the row's slots go through
+// reduce_span.  Padding slots hold a column >= cols and are skipped there.
+template <bool VEC, unsigned GR, unsigned U = 2>
 __global__ void __launch_bounds__(kRowThreads) group_reduce_sell_kernel(cs_sliced_ell_view src,
                                                                          const uint32_t *__restrict__ group_masks,
                                                                          uint32_t group_count,
@@ -273,16 +361,15 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_sell_kernel(cs_slice
                                                                          cs_group_filter_params filter,
                                                                          cs_group_reduce_out out) {
     extern __shared__ float gr_smem[];
-    const bool groups = group_masks != nullptr && group_count != 0u;
-    float *acc_col = warp_acc_column(gr_smem, groups);
+    float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
     const unsigned lane = threadIdx.x & 31u;
     for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
         if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
             empty_row(row, group_count, out);
             continue;
         }
-        zero_acc(acc_col);
-        row_acc a{0.0f, 0.0f, 0u};
+        row_acc<GR> a;
+        init_acc(a);
         uint32_t width = 0u;
         std::size_t slot_base = 0u;
         if (src.slice_count != 0u) {
@@ -291,17 +378,20 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_sell_kernel(cs_slice
             slot_base = (std::size_t) src.slice_slot_offsets[slice] +
                         (std::size_t) (row - src.slice_row_offsets[slice]) * width;
         }
-        for (uint32_t k = lane; k < width; k += 32u) {
-            const uint32_t col = src.col_idx[slot_base + k];
-            const uint16_t h = src.val[slot_base + k];
-            if (col < src.cols && half_nonzero(h) && feature_kept(masks.feature_keep, col))
-                add_value(a, h2f(h), col, group_masks, group_count, acc_col);
+        if (VEC) {
+            reduce_span<U>(src.col_idx, src.val, slot_base, slot_base + width, src.cols, masks.feature_keep,
+                           group_masks, a);
+        } else {
+            for (uint32_t k = lane; k < width; k += 32u)
+                add_entry(a, src.col_idx[slot_base + k], src.val[slot_base + k], src.cols, masks.feature_keep,
+                          group_masks);
         }
         __syncwarp();
         finish_row(row, a, acc_col, group_count, filter, out);
     }
 }
 
+template <bool VEC, unsigned GR, unsigned U = 2>
 __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_kernel(cs_compressed_view src,
                                                                         const uint32_t *__restrict__ group_masks,
                                                                         uint32_t group_count,
@@ -309,27 +399,429 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_kernel(cs_compre
                                                                         cs_group_filter_params filter,
                                                                         cs_group_reduce_out out) {
     extern __shared__ float gr_smem[];
-    const bool groups = group_masks != nullptr && group_count != 0u;
-    float *acc_col = warp_acc_column(gr_smem, groups);
+    float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
     const unsigned lane = threadIdx.x & 31u;
     for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
         if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
             empty_row(row, group_count, out);
             continue;
         }
-        zero_acc(acc_col);
-        row_acc a{0.0f, 0.0f, 0u};
+        row_acc<GR> a;
+        init_acc(a);
         const uint32_t b = src.majorPtr[row], e = src.majorPtr[row + 1u];
-        for (uint32_t i = b + lane; i < e; i += 32u) {
-            const uint32_t col = src.minorIdx[i];
-            const uint16_t h = src.val[i];
-            if (col < src.cols && half_nonzero(h) && feature_kept(masks.feature_keep, col))
-                add_value(a, h2f(h), col, group_masks, group_count, acc_col);
+        if (VEC) {
+            reduce_span<U>(src.minorIdx, src.val, b, e, src.cols, masks.feature_keep, group_masks, a);
+        } else {
+            for (uint32_t i = b + lane; i < e; i += 32u)
+                add_entry(a, src.minorIdx[i], src.val[i], src.cols, masks.feature_keep, group_masks);
         }
         __syncwarp();
         finish_row(row, a, acc_col, group_count, filter, out);
     }
 }
+
+// ---------------------------------------------------------------------------
+// Blocked-ELL-16 reduce on the tensor cores.
+//
+// For one 16-row block and one 16-column slot, the block rows' group sums are
+// a small product
+//     D[n][grp] += sum_c V[n][c] * M[c][grp]
+// with V[n][c] the slot's fp16 value of block row n, column c, and
+// M[c][grp] = 1 when column c is inside the matrix, kept by the feature mask
+// and in group grp.  One warp owns one row block and issues, per slot, one
+// mma.m16n8k16 (fp16 operands, fp32 accumulators) per 8 groups, one whose B
+// is the kept-column indicator (column 0 of D = the row totals) and one
+// whose A is the nonzero indicator of the values (column 0 of D = the
+// detected counts).  Products are v * 1 or v * 0, so the sums are fp32 sums
+// of the values, as in the per-row path (addition order differs; integer data
+// gives identical results).  The slot's 16 columns are dealt to the lanes as
+// 4 consecutive columns per lane (lane = 4g + t reads columns 4t..4t+3 of
+// block rows g and g + 8), the fragments' k order permuted: physical column
+// 4t + {0,1,2,3} stands for k = 2t, 2t+1, 2t+8, 2t+9 in both operands.
+// Maxima come from the same values with packed-half max.  A non-finite value
+// turns its row total non-finite (0 * inf and 1 * inf alike), and such row
+// blocks are redone by the per-row path.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mma_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                          uint32_t b0, uint32_t b1) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t hmax2_bits(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("max.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// 1.0 in each half that is nonzero or NaN (either sign of zero gives 0.0).
+__device__ __forceinline__ uint32_t nonzero_unit_pair(uint32_t x) {
+    uint32_t d;
+    asm("set.neu.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(x), "r"(0u));
+    return d;
+}
+
+// (without groups, G is the constant 0 and its comparisons fold away)
+#pragma nv_diag_suppress 186
+// NT: tiles of 8 groups (0 without groups); GR: accumulators of the per-row
+// path that takes row blocks with non-finite values.
+template <unsigned NT, unsigned GR, unsigned U>
+__global__ void __launch_bounds__(kRowThreads) group_reduce_bell16_mma_kernel(
+    cs_blocked_ell_view src, const uint32_t *__restrict__ group_masks, uint32_t group_count,
+    cs_row_feature_mask_view masks, cs_group_filter_params filter, cs_group_reduce_out out) {
+    extern __shared__ float gr_smem[];
+    const bool groups = GR != 0u;
+    const uint32_t G = groups ? group_count : 0u;
+    float *acc_col = warp_acc_column(gr_smem, groups, group_count);
+    uint2 *stage = reinterpret_cast<uint2 *>(gr_smem + (groups ? kRowWarps * group_count * 32u : 0u)) +
+                   (threadIdx.x >> 5) * kStagePairs;
+    const unsigned lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
+    const uint32_t W = src.ell_cols >> 4;
+    const uint32_t row_blocks = (src.rows + 15u) >> 4;
+    const uint32_t gmask = G >= 32u ? 0xffffffffu : (1u << G) - 1u;
+    const uint32_t unit_n0 = g == 0u ? 0x3c00u : 0u; // B column 0 only
+    for (uint32_t rb = blockIdx.x * kRowWarps + (threadIdx.x >> 5); rb < row_blocks; rb += gridDim.x * kRowWarps) {
+        uint32_t rowh[2];
+        bool kept[2];
+#pragma unroll
+        for (unsigned h = 0; h < 2u; ++h) {
+            rowh[h] = rb * 16u + 8u * h + g;
+            kept[h] = rowh[h] < src.rows && (masks.row_keep == nullptr || masks.row_keep[rowh[h]] != 0u);
+        }
+        float dg[NT > 0u ? NT : 1u][4], dt[4] = {0.0f, 0.0f, 0.0f, 0.0f}, dd[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (unsigned nt = 0; nt < (NT > 0u ? NT : 1u); ++nt)
+#pragma unroll
+            for (unsigned q = 0; q < 4u; ++q) dg[nt][q] = 0.0f;
+        uint32_t mx[2] = {0u, 0u};
+        if (__any_sync(0xffffffffu, kept[0] || kept[1])) {
+            const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
+            const uint16_t *vr[2];
+#pragma unroll
+            for (unsigned h = 0; h < 2u; ++h)
+                vr[h] = src.val + (std::size_t) (kept[h] ? rowh[h] : 0u) * src.ell_cols + 4u * t;
+            for (uint32_t s0 = 0; s0 < W; s0 += 32u) {
+                const uint32_t n = min(32u, W - s0);
+                const uint32_t my_bc = lane < n ? __ldg(bci + s0 + lane) : CS_INVALID_COL;
+                for (uint32_t j0 = 0; j0 < n; j0 += U) {
+                    uint2 x[U][2];
+                    uint32_t bc[U];
+#pragma unroll
+                    for (unsigned u = 0; u < U; ++u) {
+                        bc[u] = __shfl_sync(0xffffffffu, my_bc, (j0 + u) & 31u);
+                        if (j0 + u >= n) bc[u] = CS_INVALID_COL;
+                        const std::size_t off = (std::size_t) (s0 + j0 + u) * 16u;
+#pragma unroll
+                        for (unsigned h = 0; h < 2u; ++h)
+                            x[u][h] = bc[u] != CS_INVALID_COL && kept[h] ? ld_stream_v2(vr[h] + off)
+                                                                        : make_uint2(0u, 0u);
+                    }
+#pragma unroll
+                    for (unsigned u = 0; u < U; ++u) {
+                        if (bc[u] == CS_INVALID_COL) continue; // warp-uniform
+                        // this lane's 4 columns: in range and kept (kw bytes), group bits
+                        const uint32_t c0 = bc[u] * 16u + 4u * t;
+                        uint32_t mk[4], kw;
+                        if (c0 + 4u <= src.cols) {
+                            const uint4 m4 = NT > 0u ? __ldg(reinterpret_cast<const uint4 *>(group_masks + c0))
+                                                     : make_uint4(0u, 0u, 0u, 0u);
+                            mk[0] = m4.x, mk[1] = m4.y, mk[2] = m4.z, mk[3] = m4.w;
+                            kw = masks.feature_keep != nullptr
+                                     ? __ldg(reinterpret_cast<const uint32_t *>(masks.feature_keep + c0))
+                                     : 0x01010101u;
+                        } else {
+                            kw = 0u;
+#pragma unroll
+                            for (unsigned j = 0; j < 4u; ++j) {
+                                const bool in = c0 + j < src.cols;
+                                mk[j] = in && NT > 0u ? __ldg(group_masks + c0 + j) : 0u;
+                                kw |= (in && feature_kept(masks.feature_keep, c0 + j) ? 1u : 0u) << (8u * j);
+                            }
+                        }
+                        const uint32_t kv = __vsetne4(kw, 0u);                  // 1 per kept column byte
+                        const uint32_t kb_lo = __byte_perm(kv, 0u, 0x4140u);     // columns 4t, 4t+1 -> bits 0, 16
+                        const uint32_t kb_hi = __byte_perm(kv, 0u, 0x4342u);     // columns 4t+2, 4t+3
+                        const uint32_t km_lo = kb_lo * 0xffffu, km_hi = kb_hi * 0xffffu;
+                        const uint32_t a0 = x[u][0].x, a1 = x[u][1].x, a2 = x[u][0].y, a3 = x[u][1].y;
+                        mma_16816(dt, a0, a1, a2, a3, kb_lo * unit_n0, kb_hi * unit_n0);
+                        mma_16816(dd, nonzero_unit_pair(a0), nonzero_unit_pair(a1), nonzero_unit_pair(a2),
+                                  nonzero_unit_pair(a3), kb_lo * unit_n0, kb_hi * unit_n0);
+#pragma unroll
+                        for (unsigned nt = 0; nt < NT; ++nt) {
+                            // group 8nt + g of columns (4t, 4t+1) and (4t+2, 4t+3), as bits 0 and 16
+                            const uint32_t sh = (8u * nt + g) & 15u;
+                            const uint32_t sel = nt < 2u ? 0x5410u : 0x7632u;
+                            const uint32_t p01 = __byte_perm(mk[0] & gmask, mk[1] & gmask, sel);
+                            const uint32_t p23 = __byte_perm(mk[2] & gmask, mk[3] & gmask, sel);
+                            mma_16816(dg[nt], a0, a1, a2, a3, ((p01 >> sh) & kb_lo) * 0x3c00u,
+                                      ((p23 >> sh) & kb_hi) * 0x3c00u);
+                        }
+                        mx[0] = hmax2_bits(mx[0], hmax2_bits(a0 & km_lo, a2 & km_hi));
+                        mx[1] = hmax2_bits(mx[1], hmax2_bits(a1 & km_lo, a3 & km_hi));
+                    }
+                }
+            }
+        }
+        // D fragments of lane (g, t): [0] = D[g][2t], [1] = D[g][2t+1],
+        // [2] = D[g+8][2t], [3] = D[g+8][2t+1]; totals and counts are column 0.
+        const unsigned quad0 = lane & ~3u;
+        float tot[2], cnt[2];
+        tot[0] = __shfl_sync(0xffffffffu, dt[0], quad0);
+        tot[1] = __shfl_sync(0xffffffffu, dt[2], quad0);
+        cnt[0] = __shfl_sync(0xffffffffu, dd[0], quad0);
+        cnt[1] = __shfl_sync(0xffffffffu, dd[2], quad0);
+        if (__any_sync(0xffffffffu, !isfinite(tot[0]) || !isfinite(tot[1]))) {
+            for (uint32_t r = 0; r < 16u; ++r)
+                if (rb * 16u + r < src.rows)
+                    bell_row<true, GR>(src, rb * 16u + r, group_masks, group_count, masks, filter, out, acc_col,
+                                       stage);
+            continue;
+        }
+        // fraction numerator: group F of rows g, g + 8 sits in lane (g, (F & 7) >> 1)
+        const uint32_t F = filter.fraction_group_index;
+        float fr[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (unsigned nt = 0; nt < NT; ++nt)
+            if (F < G && (F >> 3) == nt) {
+                fr[0] = (F & 1u) ? dg[nt][1] : dg[nt][0];
+                fr[1] = (F & 1u) ? dg[nt][3] : dg[nt][2];
+            }
+        const unsigned src_f = quad0 | ((F & 7u) >> 1);
+        fr[0] = __shfl_sync(0xffffffffu, fr[0], src_f);
+        fr[1] = __shfl_sync(0xffffffffu, fr[1], src_f);
+#pragma unroll
+        for (unsigned h = 0; h < 2u; ++h) {
+            float vmax = fmaxf(h2f((uint16_t) (mx[h] & 0xffffu)), h2f((uint16_t) (mx[h] >> 16)));
+            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, 1));
+            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, 2));
+            const uint32_t row = rowh[h];
+            if (t == h && row < src.rows) {
+                const float sum = tot[h];
+                const uint32_t det = (uint32_t) cnt[h];
+                out.row_totals[row] = sum;
+                out.max_values[row] = vmax + 0.0f;
+                out.detected_features[row] = det;
+                const float frac = sum > 0.0f ? __fdiv_rn(F < G ? fr[h] : 0.0f, sum) : 0.0f;
+                out.row_keep[row] = (uint8_t) (kept[h] && sum >= filter.min_total &&
+                                               det >= filter.min_detected_features &&
+                                               frac <= filter.max_group_fraction);
+            }
+            if (groups && out.group_counts != nullptr && out.group_percentages != nullptr && row < src.rows) {
+#pragma unroll
+                for (unsigned nt = 0; nt < NT; ++nt) {
+#pragma unroll
+                    for (unsigned q = 0; q < 2u; ++q) {
+                        const uint32_t grp = 8u * nt + 2u * t + q;
+                        if (grp < G) {
+                            const float gs = dg[nt][2u * h + q];
+                            const std::size_t o = (std::size_t) row * G + grp;
+                            out.group_counts[o] = gs;
+                            out.group_percentages[o] = tot[h] > 0.0f ? __fdiv_rn(__fmul_rn(100.0f, gs), tot[h])
+                                                                     : 0.0f;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Pipelined form for up to 15 groups and a column table that fits shared
+// memory.  Each CTA first builds a u16 entry per column in shared memory
+// (bit 15: in the matrix and kept; bits 0..G-1: the column's groups if
+// kept), so the per-slot column lookups are shared-memory reads.  The values
+// reach shared memory through 16-byte asynchronous copies, STAGES stages of 8
+// slots (16 rows x 256 bytes) per warp, so the bytes in flight do not depend
+// on registers; rows the row mask drops are not copied.  A stage row is
+// padded by 32 bytes, which puts the 8-byte fragment reads of a half-warp on
+// distinct banks.  Row blocks with non-finite values use the per-row path,
+// its shared memory taken from the warp's (then idle) stage buffers.
+constexpr unsigned kPipeWarps = 16;
+constexpr unsigned kPipeSlots = 8;
+constexpr unsigned kPipeRowStride = kPipeSlots * 32u + 32u;
+constexpr unsigned kPipeStageBytes = 16u * kPipeRowStride;
+constexpr unsigned kPipeStages = 2;
+
+template <unsigned STAGES>
+constexpr std::size_t pipe_warp_bytes() { return (std::size_t) STAGES * kPipeStageBytes; }
+
+std::size_t pipe_table_bytes(uint32_t cols) { return align_up(((std::size_t) cols + 15u) / 16u * 32u, 16u); }
+
+template <unsigned STAGES>
+std::size_t pipe_smem_bytes(uint32_t cols) { return kPipeWarps * pipe_warp_bytes<STAGES>() + pipe_table_bytes(cols); }
+
+template <unsigned NT, unsigned GR, unsigned STAGES>
+__global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_kernel(
+    cs_blocked_ell_view src, const uint32_t *__restrict__ group_masks, uint32_t group_count,
+    cs_row_feature_mask_view masks, cs_group_filter_params filter, cs_group_reduce_out out) {
+    extern __shared__ __align__(16) unsigned char pipe_smem[];
+    constexpr unsigned RS = kPipeRowStride;
+    const bool groups = GR != 0u;
+    const uint32_t G = groups ? group_count : 0u;
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
+    unsigned char *buf = pipe_smem + (std::size_t) warp * pipe_warp_bytes<STAGES>();
+    uint16_t *table = reinterpret_cast<uint16_t *>(pipe_smem + kPipeWarps * pipe_warp_bytes<STAGES>());
+    // per-row fallback: accumulator block and pair staging inside this warp's stage buffers
+    float *acc_col = groups ? reinterpret_cast<float *>(buf) + lane : nullptr;
+    uint2 *stage = reinterpret_cast<uint2 *>(buf + (std::size_t) G * 32u * sizeof(float));
+    const uint32_t col_blocks = (src.cols + 15u) >> 4;
+    const uint32_t gmask = (1u << G) - 1u;
+    for (uint32_t c = threadIdx.x; c < col_blocks * 16u; c += blockDim.x) {
+        uint32_t e = 0u;
+        if (c < src.cols && feature_kept(masks.feature_keep, c))
+            e = 0x8000u | (NT > 0u ? __ldg(group_masks + c) & gmask : 0u);
+        table[c] = (uint16_t) e;
+    }
+    __syncthreads();
+    const uint32_t W = src.ell_cols >> 4;
+    const uint32_t nstages = (W + kPipeSlots - 1u) / kPipeSlots;
+    const uint32_t row_blocks = (src.rows + 15u) >> 4;
+    const uint32_t unit_n0 = g == 0u ? 0x3c00u : 0u;
+    for (uint32_t rb = blockIdx.x * kPipeWarps + warp; rb < row_blocks; rb += gridDim.x * kPipeWarps) {
+        // rows of the block the row mask keeps (bit r = block row r)
+        const uint32_t r16 = rb * 16u + (lane & 15u);
+        const bool lane_keep = lane < 16u && r16 < src.rows && (masks.row_keep == nullptr || masks.row_keep[r16] != 0u);
+        const uint32_t keep16 = __ballot_sync(0xffffffffu, lane_keep);
+        const bool kept[2] = {((keep16 >> g) & 1u) != 0u, ((keep16 >> (g + 8u)) & 1u) != 0u};
+        float dg[NT > 0u ? NT : 1u][4], dt[4] = {0.0f, 0.0f, 0.0f, 0.0f}, dd[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (unsigned nt = 0; nt < (NT > 0u ? NT : 1u); ++nt)
+#pragma unroll
+            for (unsigned q = 0; q < 4u; ++q) dg[nt][q] = 0.0f;
+        uint32_t mx[2] = {0u, 0u};
+        if (keep16 != 0u) {
+            const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
+            // rows the mask drops are never copied: zero them in every stage once
+            for (unsigned i = lane; i < STAGES * 16u * 16u; i += 32u) {
+                const unsigned r = (i >> 4) & 15u;
+                if (!((keep16 >> r) & 1u))
+                    *reinterpret_cast<uint4 *>(buf + (i >> 8) * kPipeStageBytes + r * RS + (i & 15u) * 16u) =
+                        make_uint4(0u, 0u, 0u, 0u);
+            }
+            // this lane's copies: 16-byte piece (lane & 15) of stage rows (lane >> 4) + 2i
+            const unsigned piece = lane & 15u;
+            const uint16_t *gsrc = src.val + (std::size_t) rb * 16u * src.ell_cols + piece * 8u;
+            auto issue = [&](uint32_t k) {
+                if (k < nstages && k * kPipeSlots + piece / 2u < W) {
+                    unsigned char *dst = buf + (k % STAGES) * kPipeStageBytes + piece * 16u;
+                    const uint16_t *from = gsrc + (std::size_t) k * kPipeSlots * 16u;
+#pragma unroll
+                    for (unsigned i = 0; i < 8u; ++i) {
+                        const unsigned r = (lane >> 4) + 2u * i;
+                        if ((keep16 >> r) & 1u) cp_async_16(dst + r * RS, from + (std::size_t) r * src.ell_cols);
+                    }
+                }
+                cp_async_commit();
+            };
+#pragma unroll
+            for (unsigned p = 0; p + 1u < STAGES; ++p) issue(p);
+            // block columns of slots [32w, 32w + 32) one per lane, the next window loaded ahead
+            uint32_t my_bc = lane < W ? __ldg(bci + lane) : CS_INVALID_COL;
+            uint32_t next_bc = 32u + lane < W ? __ldg(bci + 32u + lane) : CS_INVALID_COL;
+            for (uint32_t k = 0; k < nstages; ++k) {
+                issue(k + STAGES - 1u);
+                cp_async_wait<STAGES - 1>();
+                __syncwarp();
+                const unsigned char *sb = buf + (k % STAGES) * kPipeStageBytes + 8u * t;
+                const uint32_t nslots = min(kPipeSlots, W - k * kPipeSlots);
+                if (k % 4u == 0u && k != 0u) {
+                    my_bc = next_bc;
+                    const uint32_t s = k * kPipeSlots + 32u + lane;
+                    next_bc = s < W ? __ldg(bci + s) : CS_INVALID_COL;
+                }
+#pragma unroll
+                for (unsigned j = 0; j < kPipeSlots; ++j) {
+                    const uint32_t bc = __shfl_sync(0xffffffffu, my_bc, ((k % 4u) * kPipeSlots + j) & 31u);
+                    if (j >= nslots || bc >= col_blocks) continue; // warp-uniform (padding or outside)
+                    // this lane's 4 columns: two u16 entries per word (columns 4t, 4t+1 and 4t+2, 4t+3)
+                    const uint2 te = *reinterpret_cast<const uint2 *>(table + bc * 16u + 4u * t);
+                    const uint32_t kb_lo = (te.x >> 15) & 0x00010001u, kb_hi = (te.y >> 15) & 0x00010001u;
+                    const uint32_t km_lo = kb_lo * 0xffffu, km_hi = kb_hi * 0xffffu;
+                    const uint2 lo = *reinterpret_cast<const uint2 *>(sb + g * RS + j * 32u);
+                    const uint2 hi = *reinterpret_cast<const uint2 *>(sb + (g + 8u) * RS + j * 32u);
+                    const uint32_t a0 = lo.x, a1 = hi.x, a2 = lo.y, a3 = hi.y;
+                    mma_16816(dt, a0, a1, a2, a3, kb_lo * unit_n0, kb_hi * unit_n0);
+                    mma_16816(dd, nonzero_unit_pair(a0), nonzero_unit_pair(a1), nonzero_unit_pair(a2),
+                              nonzero_unit_pair(a3), kb_lo * unit_n0, kb_hi * unit_n0);
+                    if constexpr (NT > 0u)
+                        mma_16816(dg[0], a0, a1, a2, a3, ((te.x >> g) & 0x00010001u) * 0x3c00u,
+                                  ((te.y >> g) & 0x00010001u) * 0x3c00u);
+                    if constexpr (NT > 1u)
+                        mma_16816(dg[NT - 1u], a0, a1, a2, a3, ((te.x >> (g + 8u)) & 0x00010001u) * 0x3c00u,
+                                  ((te.y >> (g + 8u)) & 0x00010001u) * 0x3c00u);
+                    mx[0] = hmax2_bits(mx[0], hmax2_bits(a0 & km_lo, a2 & km_hi));
+                    mx[1] = hmax2_bits(mx[1], hmax2_bits(a1 & km_lo, a3 & km_hi));
+                }
+                __syncwarp();
+            }
+            cp_async_wait<0>();
+            __syncwarp();
+        }
+        const unsigned quad0 = lane & ~3u;
+        float tot[2], cnt[2];
+        tot[0] = __shfl_sync(0xffffffffu, dt[0], quad0);
+        tot[1] = __shfl_sync(0xffffffffu, dt[2], quad0);
+        cnt[0] = __shfl_sync(0xffffffffu, dd[0], quad0);
+        cnt[1] = __shfl_sync(0xffffffffu, dd[2], quad0);
+        if (__any_sync(0xffffffffu, !isfinite(tot[0]) || !isfinite(tot[1]))) {
+            for (uint32_t r = 0; r < 16u; ++r)
+                if (rb * 16u + r < src.rows)
+                    bell_row<true, GR>(src, rb * 16u + r, group_masks, group_count, masks, filter, out, acc_col,
+                                       stage);
+            __syncwarp();
+            continue;
+        }
+        const uint32_t F = filter.fraction_group_index;
+        float fr[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (unsigned nt = 0; nt < NT; ++nt)
+            if (F < G && (F >> 3) == nt) {
+                fr[0] = (F & 1u) ? dg[nt][1] : dg[nt][0];
+                fr[1] = (F & 1u) ? dg[nt][3] : dg[nt][2];
+            }
+        const unsigned src_f = quad0 | ((F & 7u) >> 1);
+        fr[0] = __shfl_sync(0xffffffffu, fr[0], src_f);
+        fr[1] = __shfl_sync(0xffffffffu, fr[1], src_f);
+#pragma unroll
+        for (unsigned h = 0; h < 2u; ++h) {
+            float vmax = fmaxf(h2f((uint16_t) (mx[h] & 0xffffu)), h2f((uint16_t) (mx[h] >> 16)));
+            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, 1));
+            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, 2));
+            const uint32_t row = rb * 16u + 8u * h + g;
+            if (t == h && row < src.rows) {
+                const float sum = tot[h];
+                const uint32_t det = (uint32_t) cnt[h];
+                out.row_totals[row] = sum;
+                out.max_values[row] = vmax + 0.0f;
+                out.detected_features[row] = det;
+                const float frac = sum > 0.0f ? __fdiv_rn(F < G ? fr[h] : 0.0f, sum) : 0.0f;
+                out.row_keep[row] = (uint8_t) (kept[h] && sum >= filter.min_total &&
+                                               det >= filter.min_detected_features &&
+                                               frac <= filter.max_group_fraction);
+            }
+            if (groups && out.group_counts != nullptr && out.group_percentages != nullptr && row < src.rows) {
+#pragma unroll
+                for (unsigned nt = 0; nt < NT; ++nt) {
+#pragma unroll
+                    for (unsigned q = 0; q < 2u; ++q) {
+                        const uint32_t grp = 8u * nt + 2u * t + q;
+                        if (grp < G) {
+                            const float gs = dg[nt][2u * h + q];
+                            const std::size_t o = (std::size_t) row * G + grp;
+                            out.group_counts[o] = gs;
+                            out.group_percentages[o] = tot[h] > 0.0f ? __fdiv_rn(__fmul_rn(100.0f, gs), tot[h])
+                                                                     : 0.0f;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+#pragma nv_diag_default 186
 
 unsigned row_grid(uint32_t rows) {
     uint32_t g = (rows + kRowWarps - 1u) / kRowWarps;
@@ -357,7 +849,7 @@ int check_common(uint32_t group_count, const cs_group_filter_params *filter, con
 }
 
 std::size_t group_smem(const uint32_t *masks, uint32_t group_count) {
-    return (masks != nullptr && group_count != 0u) ? kRowWarps * 1024u * sizeof(float) : 0u;
+    return (masks != nullptr && group_count != 0u) ? kRowWarps * group_count * 32u * sizeof(float) : 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -406,9 +898,9 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(cs_blocked_ell_view 
                 }
             }
             const uint32_t ballot = __ballot_sync(0xffffffffu, k);
-            if (EMIT && k) {
+            if constexpr (EMIT) {
                 const uint32_t pos = run + __popc(ballot & ((1u << lane) - 1u));
-                if (pos < end) {
+                if (k && pos < end) {
                     minor_idx[pos] = oc;
                     out_val[pos] = h;
                 }
@@ -421,6 +913,32 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(cs_blocked_ell_view 
         }
     }
 }
+
+// Group accumulator registers a call needs: none, 8, 16 or 32.
+unsigned group_regs(const uint32_t *masks, uint32_t group_count) {
+    if (masks == nullptr || group_count == 0u) return 0u;
+    return group_count <= 8u ? 8u : group_count <= 16u ? 16u : 32u;
+}
+
+template <typename View>
+using reduce_kernel_t = void (*)(View, const uint32_t *, uint32_t, cs_row_feature_mask_view, cs_group_filter_params,
+                                 cs_group_reduce_out);
+
+// Tensor-core Blocked-ELL-16 kernel for a group count: tiles of 8 groups and
+// the per-row fallback's accumulators.
+template <unsigned U>
+reduce_kernel_t<cs_blocked_ell_view> bell16_mma_kernel(uint32_t groups) {
+    switch ((groups + 7u) / 8u) {
+    case 0: return group_reduce_bell16_mma_kernel<0u, 0u, U>;
+    case 1: return group_reduce_bell16_mma_kernel<1u, 8u, U>;
+    case 2: return group_reduce_bell16_mma_kernel<2u, 16u, U>;
+    case 3: return group_reduce_bell16_mma_kernel<3u, 32u, U>;
+    default: return group_reduce_bell16_mma_kernel<4u, 32u, U>;
+    }
+}
+
+#define CS_PICK_REDUCE(KERNEL, VEC, GR)                                                                          \
+    ((GR) == 0u ? KERNEL<VEC, 0u> : (GR) == 8u ? KERNEL<VEC, 8u> : (GR) == 16u ? KERNEL<VEC, 16u> : KERNEL<VEC, 32u>)
 
 } // namespace
 } // namespace csb
@@ -445,12 +963,48 @@ extern "C" int cs_b200_group_reduce_blocked_ell(const cs_blocked_ell_view *src, 
                      (reinterpret_cast<uintptr_t>(src->val) & 15u) == 0u;
     const std::size_t smem = group_smem(d_feature_group_masks, group_count) +
                              (vec ? (std::size_t) kRowWarps * kStagePairs * sizeof(uint2) : 0u);
-    if (vec)
-        group_reduce_bell_kernel<true><<<row_grid(src->rows), kRowThreads, smem, as_stream(s)>>>(
-            *src, d_feature_group_masks, group_count, m, *filter, *out);
-    else
-        group_reduce_bell_kernel<false><<<row_grid(src->rows), kRowThreads, smem, as_stream(s)>>>(
-            *src, d_feature_group_masks, group_count, m, *filter, *out);
+    const unsigned gr = group_regs(d_feature_group_masks, group_count);
+    const bool mma = vec && src->block_size == 16u &&
+                     (gr == 0u || (reinterpret_cast<uintptr_t>(d_feature_group_masks) & 15u) == 0u) &&
+                     (m.feature_keep == nullptr || (reinterpret_cast<uintptr_t>(m.feature_keep) & 3u) == 0u);
+    const uint32_t G = gr != 0u ? group_count : 0u;
+    if (vec && src->block_size == 16u && G <= 15u) {
+        // pipelined tensor-core kernel when the column table fits shared memory
+        int dev = 0, optin = 0;
+        const std::size_t psmem = pipe_smem_bytes<kPipeStages>(src->cols);
+        if (cuda_ok(cudaGetDevice(&dev), "group_reduce_blocked_ell device") &&
+            cuda_ok(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                    "group_reduce_blocked_ell shared memory limit") &&
+            psmem <= (std::size_t) optin) {
+            const reduce_kernel_t<cs_blocked_ell_view> k =
+                G == 0u ? group_reduce_bell16_pipe_kernel<0u, 0u, kPipeStages>
+                        : G <= 8u ? group_reduce_bell16_pipe_kernel<1u, 8u, kPipeStages>
+                                  : group_reduce_bell16_pipe_kernel<2u, 16u, kPipeStages>;
+            if (!cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(k),
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int) psmem),
+                         "group_reduce_bell16_pipe_kernel shared memory"))
+                return 0;
+            const uint32_t row_blocks = (src->rows + 15u) / 16u;
+            const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kPipeWarps * 32u, psmem,
+                                                (row_blocks + kPipeWarps - 1u) / kPipeWarps);
+            k<<<grid, kPipeWarps * 32u, psmem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter,
+                                                                *out);
+            return launch_ok("group_reduce_bell16_pipe_kernel");
+        }
+    }
+    if (mma) {
+        const reduce_kernel_t<cs_blocked_ell_view> k = bell16_mma_kernel<4u>(G);
+        const uint32_t row_blocks = (src->rows + 15u) / 16u;
+        const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, smem,
+                                            (row_blocks + kRowWarps - 1u) / kRowWarps);
+        k<<<grid, kRowThreads, smem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter, *out);
+        return launch_ok("group_reduce_bell16_mma_kernel");
+    }
+    const reduce_kernel_t<cs_blocked_ell_view> k = vec ? CS_PICK_REDUCE(group_reduce_bell_kernel, true, gr)
+                                                       : CS_PICK_REDUCE(group_reduce_bell_kernel, false, gr);
+    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, smem,
+                                        (src->rows + kRowWarps - 1u) / kRowWarps);
+    k<<<grid, kRowThreads, smem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter, *out);
     return launch_ok("group_reduce_bell_kernel");
 }
 
@@ -464,8 +1018,15 @@ extern "C" int cs_b200_group_reduce_sliced_ell(const cs_sliced_ell_view *src, co
     }
     if (src->rows == 0u) return 1;
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
-    group_reduce_sell_kernel<<<row_grid(src->rows), kRowThreads, group_smem(d_feature_group_masks, group_count),
-                               as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter, *out);
+    const bool vec = (reinterpret_cast<uintptr_t>(src->col_idx) & 15u) == 0u &&
+                     (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u;
+    const std::size_t smem = group_smem(d_feature_group_masks, group_count);
+    const unsigned gr = group_regs(d_feature_group_masks, group_count);
+    const reduce_kernel_t<cs_sliced_ell_view> k = vec ? CS_PICK_REDUCE(group_reduce_sell_kernel, true, gr)
+                                                      : CS_PICK_REDUCE(group_reduce_sell_kernel, false, gr);
+    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, smem,
+                                        (src->rows + kRowWarps - 1u) / kRowWarps);
+    k<<<grid, kRowThreads, smem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter, *out);
     return launch_ok("group_reduce_sell_kernel");
 }
 
@@ -483,8 +1044,15 @@ extern "C" int cs_b200_group_reduce_compressed(const cs_compressed_view *src, co
     }
     if (src->rows == 0u) return 1;
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
-    group_reduce_csr_kernel<<<row_grid(src->rows), kRowThreads, group_smem(d_feature_group_masks, group_count),
-                              as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter, *out);
+    const bool vec = (reinterpret_cast<uintptr_t>(src->minorIdx) & 15u) == 0u &&
+                     (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u;
+    const std::size_t smem = group_smem(d_feature_group_masks, group_count);
+    const unsigned gr = group_regs(d_feature_group_masks, group_count);
+    const reduce_kernel_t<cs_compressed_view> k = vec ? CS_PICK_REDUCE(group_reduce_csr_kernel, true, gr)
+                                                      : CS_PICK_REDUCE(group_reduce_csr_kernel, false, gr);
+    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, smem,
+                                        (src->rows + kRowWarps - 1u) / kRowWarps);
+    k<<<grid, kRowThreads, smem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter, *out);
     return launch_ok("group_reduce_csr_kernel");
 }
 

@@ -253,3 +253,135 @@ def test_random_vs_reference_kernels(cuda, orc, seed):
         assert np.max(np.abs(p.astype(np.int64) - q.astype(np.int64))) <= 2, fn
         diff = np.flatnonzero(mine["row_keep"] != ref["row_keep"])
         assert len(diff) <= 2, (fn, diff)  # fast-math fraction right at the threshold
+
+
+def _shifted(t):
+    """The same values starting one element past an aligned allocation, so
+    the kernels take their unaligned (per-entry) path."""
+    import torch
+
+    buf = torch.empty(t.numel() + 1, dtype=t.dtype, device=t.device)
+    buf[1:] = t
+    return buf[1:]
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_unaligned_views_match_vector_path(cuda, orc, seed):
+    """Compressed and Sliced-ELL reduces over 16-byte-aligned arrays (quad
+    loads, ragged heads and tails) and over arrays shifted by one element
+    (per-entry loads) agree with each other and with the restatement."""
+    from dataclasses import replace
+
+    import torch
+
+    from cellshard_b200 import runtime
+    from cellshard_b200.device import SlicedELL
+
+    rows, cols, G = 640, 515, 9
+    ptr, idx, val, masks, rk, fk = _random_inputs(rows, cols, seed)
+    filt = runtime.FilterParams(3.0, 2, 0.5, 2)
+    fa = (3.0, 2, 0.5, 2)
+    csr = to_device_csr(rows, cols, ptr, idx, val)
+    gm, drk, dfk = t(masks, "u32"), t(rk, "u8"), t(fk, "u8")
+    o = orc.group_reduce_csr(rows, cols, ptr, idx, val, masks, G, rk, fk, fa)
+    a = host(runtime.compute_sparse_group_reduce(csr, gm, G, drk, dfk, filt))
+    csr_u = replace(csr, idx=_shifted(csr.idx), val=_shifted(csr.val))
+    assert csr_u.idx.data_ptr() % 16 != 0
+    u = host(runtime.compute_sparse_group_reduce(csr_u, gm, G, drk, dfk, filt))
+    _cmp(a, o)
+    _cmp(u, o)
+    s = orc.sliced_ell_from_csr(rows, ptr, idx, val, 32)
+    sell = SlicedELL(rows, cols, len(idx), 32, t(s["offsets"], "u32"), t(s["widths"], "u32"),
+                     t(s["slot_offsets"], "u32"), t(s["col_idx"], "u32"),
+                     torch.from_numpy(s["val"].view(np.float16).copy()).cuda())
+    o = orc.group_reduce_sell(rows, cols, 32, s["offsets"], s["widths"], s["slot_offsets"], s["col_idx"], s["val"],
+                              masks, G, rk, fk, fa)
+    _cmp(host(runtime.compute_sparse_group_reduce(sell, gm, G, drk, dfk, filt)), o)
+    sell_u = replace(sell, col_idx=_shifted(sell.col_idx), val=_shifted(sell.val))
+    _cmp(host(runtime.compute_sparse_group_reduce(sell_u, gm, G, drk, dfk, filt)), o)
+
+
+def _bell_case(rows, cols, G, seed, integer, density=0.08):
+    ptr, idx, val = random_csr(rows, cols, density, seed, 0.1, integer)
+    rng = np.random.default_rng(seed + 100)
+    masks = rng.integers(0, 2 ** 32, cols, dtype=np.uint64).astype(np.uint32)
+    masks[rng.random(cols) < 0.3] = 0
+    rk = (rng.random(rows) < 0.75).astype(np.uint8)
+    fk = (rng.random(cols) < 0.8).astype(np.uint8)
+    return ptr, idx, val, masks, rk, fk
+
+
+def _cmp_nan(r, o, exact=True):
+    """_cmp for outputs that may hold NaN / inf (equal NaNs count as equal)."""
+    assert np.array_equal(r["detected_features"].view(np.uint32), o["detected_features"])
+    assert np.array_equal(r["row_keep"], o["row_keep"])
+    for k in ("row_totals", "max_values", "group_counts", "group_percentages"):
+        if r[k] is None:
+            assert o[k] is None or o[k].size == 0
+            continue
+        if exact or k == "max_values":
+            assert np.array_equal(r[k], o[k], equal_nan=True), k
+        else:
+            assert np.allclose(r[k], o[k], rtol=1e-5, atol=1e-3, equal_nan=True), k
+
+
+@pytest.mark.parametrize("G,rows,cols,integer,masked", [
+    (0, 700, 300, True, True),      # totals only (pipelined tensor-core kernel)
+    (5, 700, 300, True, False),     # no row / feature masks
+    (12, 700, 515, True, True),     # two group tiles, last column block partial
+    (12, 700, 515, False, True),
+    (16, 700, 300, True, True),     # register tensor-core kernel
+    (24, 333, 333, True, True),
+    (32, 700, 300, True, True),
+    (32, 700, 300, False, True),
+    (8, 48, 50000, True, True),     # column table too large for shared memory
+])
+def test_bell16_tensor_core_paths(cuda, orc, G, rows, cols, integer, masked):
+    """Blocked-ELL-16 reduces on the tensor-core kernels (every group-count
+    class, partial last column block, padding slots, rows not a multiple of 16)
+    against the restatement."""
+    from cellshard_b200 import runtime
+    from cellshard_b200.device import blocked_ell_from_csr
+
+    ptr, idx, val, masks, rk, fk = _bell_case(rows, cols, G, 11 + G, integer,
+                                              density=0.08 if cols < 10000 else 0.002)
+    bell = blocked_ell_from_csr(to_device_csr(rows, cols, ptr, idx, val), 16)
+    filt = runtime.FilterParams(3.0, 2, 0.5, min(G - 1, 9) if G else 0)
+    fa = (3.0, 2, 0.5, min(G - 1, 9) if G else 0)
+    gm = t(masks, "u32") if G else None
+    r = host(runtime.compute_sparse_group_reduce(bell, gm, G, t(rk, "u8") if masked else None,
+                                                 t(fk, "u8") if masked else None, filt))
+    o = orc.group_reduce_bell(rows, cols, 16, bell.ell_cols, np_u32(bell.bci), bell.val.cpu().numpy().view(np.uint16),
+                              masks if G else None, G, rk if masked else None, fk if masked else None, fa)
+    _cmp_nan(r, o, integer)
+
+
+@pytest.mark.parametrize("G", [3, 12, 20])
+def test_bell16_nonfinite_rows_take_per_row_path(cuda, orc, G):
+    """inf / NaN values (in kept and dropped columns) give the reference's
+    per-value results: their row blocks are redone on the per-row path."""
+    import torch
+
+    from cellshard_b200 import runtime
+    from cellshard_b200.device import blocked_ell_from_csr
+
+    rows, cols = 200, 300
+    ptr, idx, val, masks, rk, fk = _bell_case(rows, cols, G, 3, True)
+    val = val.copy()
+    special = np.array([np.inf, -np.inf, np.nan], np.float16).view(np.uint16)
+    rng = np.random.default_rng(9)
+    for p in rng.choice(len(val), size=6, replace=False):
+        val[p] = special[p % 3]
+    bell = blocked_ell_from_csr(to_device_csr(rows, cols, ptr, idx, val), 16)
+    filt = runtime.FilterParams(3.0, 2, 0.5, 1)
+    r = host(runtime.compute_sparse_group_reduce(bell, t(masks, "u32"), G, t(rk, "u8"), t(fk, "u8"), filt))
+    o = orc.group_reduce_bell(rows, cols, 16, bell.ell_cols, np_u32(bell.bci), bell.val.cpu().numpy().view(np.uint16),
+                              masks, G, rk, fk, (3.0, 2, 0.5, 1))
+    assert not np.all(np.isfinite(o["row_totals"]))
+    _cmp_nan(r, o)
+    # the per-row kernel (values not 16-byte aligned) agrees
+    from dataclasses import replace
+
+    r2 = host(runtime.compute_sparse_group_reduce(replace(bell, val=_shifted(bell.val)), t(masks, "u32"), G,
+                                                  t(rk, "u8"), t(fk, "u8"), filt))
+    _cmp_nan(r2, o)
