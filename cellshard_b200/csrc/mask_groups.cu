@@ -456,6 +456,14 @@ __device__ __forceinline__ uint32_t hmax2_bits(uint32_t a, uint32_t b) {
     return d;
 }
 
+// 0xffff in each half whose bit 15 is set, 0 in the others (prmt with the
+// sign-replicating selector: each byte takes the sign of the half's high byte).
+__device__ __forceinline__ uint32_t half_sign_mask(uint32_t x) {
+    uint32_t d;
+    asm("prmt.b32 %0, %1, 0, 0xbb99;" : "=r"(d) : "r"(x));
+    return d;
+}
+
 // 1.0 in each half that is nonzero or NaN (either sign of zero gives 0.0).
 __device__ __forceinline__ uint32_t nonzero_unit_pair(uint32_t x) {
     uint32_t d;
@@ -678,7 +686,7 @@ __global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_k
     const uint32_t W = src.ell_cols >> 4;
     const uint32_t nstages = (W + kPipeSlots - 1u) / kPipeSlots;
     const uint32_t row_blocks = (src.rows + 15u) >> 4;
-    const uint32_t unit_n0 = g == 0u ? 0x3c00u : 0u;
+    const uint32_t unit_n0 = g == 0u ? 0x3c003c00u : 0u; // 1.0 pairs in B column 0 only
     for (uint32_t rb = blockIdx.x * kPipeWarps + warp; rb < row_blocks; rb += gridDim.x * kPipeWarps) {
         // rows of the block the row mask keeps (bit r = block row r)
         const uint32_t r16 = rb * 16u + (lane & 15u);
@@ -737,14 +745,14 @@ __global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_k
                     if (j >= nslots || bc >= col_blocks) continue; // warp-uniform (padding or outside)
                     // this lane's 4 columns: two u16 entries per word (columns 4t, 4t+1 and 4t+2, 4t+3)
                     const uint2 te = *reinterpret_cast<const uint2 *>(table + bc * 16u + 4u * t);
-                    const uint32_t kb_lo = (te.x >> 15) & 0x00010001u, kb_hi = (te.y >> 15) & 0x00010001u;
-                    const uint32_t km_lo = kb_lo * 0xffffu, km_hi = kb_hi * 0xffffu;
+                    const uint32_t km_lo = half_sign_mask(te.x), km_hi = half_sign_mask(te.y);
+                    const uint32_t bt_lo = km_lo & unit_n0, bt_hi = km_hi & unit_n0;
                     const uint2 lo = *reinterpret_cast<const uint2 *>(sb + g * RS + j * 32u);
                     const uint2 hi = *reinterpret_cast<const uint2 *>(sb + (g + 8u) * RS + j * 32u);
                     const uint32_t a0 = lo.x, a1 = hi.x, a2 = lo.y, a3 = hi.y;
-                    mma_16816(dt, a0, a1, a2, a3, kb_lo * unit_n0, kb_hi * unit_n0);
+                    mma_16816(dt, a0, a1, a2, a3, bt_lo, bt_hi);
                     mma_16816(dd, nonzero_unit_pair(a0), nonzero_unit_pair(a1), nonzero_unit_pair(a2),
-                              nonzero_unit_pair(a3), kb_lo * unit_n0, kb_hi * unit_n0);
+                              nonzero_unit_pair(a3), bt_lo, bt_hi);
                     if constexpr (NT > 0u)
                         mma_16816(dg[0], a0, a1, a2, a3, ((te.x >> g) & 0x00010001u) * 0x3c00u,
                                   ((te.y >> g) & 0x00010001u) * 0x3c00u);
