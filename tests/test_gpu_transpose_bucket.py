@@ -62,6 +62,24 @@ def test_transpose_keeps_repeated_columns_in_row_order(cuda, orc):
     assert np.array_equal(np_u16(t.val), rval)
 
 
+@pytest.mark.parametrize("rows,cols,density,unsorted,dups", [
+    (3000, 20000, 0.01, 0, 0),    # many pass-1 buckets, uneven rows
+    (130, 4096, 0.3, 0, 0),       # dense rows
+    (2000, 9000, 0.02, 7, 0),     # some rows unsorted
+    (500, 300, 0.05, 0, 4),       # repeated columns
+])
+def test_transpose_shapes_unsorted_and_repeated(cuda, orc, rows, cols, density, unsorted, dups):
+    """Stable transpose of sorted, unsorted and column-repeating rows."""
+    from cellshard_b200.device import transpose
+
+    ptr, idx, val = random_csr(rows, cols, density, 21, 0.15, unsorted_rows=unsorted, dup_rows=dups)
+    t = transpose(to_device_csr(rows, cols, ptr, idx, val))
+    rptr, ridx, rval = orc.csr_transpose(rows, cols, ptr, idx, val)
+    assert np.array_equal(np_u32(t.ptr), rptr)
+    assert np.array_equal(np_u32(t.idx), ridx)
+    assert np.array_equal(np_u16(t.val), rval)
+
+
 @ref_gpu
 def test_transpose_vs_reference_cusparse(cuda, orc):
     import torch
