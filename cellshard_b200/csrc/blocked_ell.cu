@@ -75,14 +75,29 @@ __global__ void __launch_bounds__(kShapeWarps * 32) bell_shape_kernel(
             if (vec) {
                 const uint32_t nvec = (e - head_end) >> 2;
                 const uint4 *v4 = reinterpret_cast<const uint4 *>(idx + head_end);
+                // the four columns of a vector usually share a bitmap word (rows are
+                // mostly sorted): their bits are OR-ed locally, one atomic per word run
+                auto mark4 = [&](const uint4 &q) {
+                    const uint32_t c[4] = {q.x, q.y, q.z, q.w};
+                    uint32_t word = 0xffffffffu, m = 0u;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (c[k] >= cols) {
+                            bad |= CS_STATUS_INDEX_RANGE;
+                            continue;
+                        }
+                        const uint32_t bc = div_b(c[k], B, shift);
+                        if ((bc >> 5) != word) {
+                            if (m != 0u) atomicOr(bits + word, m);
+                            word = bc >> 5;
+                            m = 0u;
+                        }
+                        m |= 1u << (bc & 31u);
+                    }
+                    if (m != 0u) atomicOr(bits + word, m);
+                };
 #pragma unroll 4
-                for (uint32_t k = lane; k < nvec; k += 32u) {
-                    const uint4 q = __ldg(v4 + k);
-                    mark(q.x);
-                    mark(q.y);
-                    mark(q.z);
-                    mark(q.w);
-                }
+                for (uint32_t k = lane; k < nvec; k += 32u) mark4(__ldg(v4 + k));
                 for (uint32_t i = head_end + (nvec << 2) + lane; i < e; i += 32u) mark(idx[i]);
             }
         }

@@ -269,9 +269,27 @@ __global__ void __launch_bounds__(256) segment_copy_kernel(uint32_t n, const uin
         const uint32_t a = sp[local];
         const uint32_t len = sp[local + 1u] - a;
         const uint32_t d = dst_ptr[i];
-        for (uint32_t j = lane; j < len; j += 32u) {
-            dst_idx[d + j] = si[a + j];
-            dst_val[d + j] = sv[a + j];
+        // four coalesced loads per array in flight per lane before the stores
+        constexpr unsigned U = 4;
+        for (uint32_t j0 = 0; j0 < len; j0 += 32u * U) {
+            uint32_t iv[U];
+            uint16_t vv[U];
+#pragma unroll
+            for (unsigned u = 0; u < U; ++u) {
+                const uint32_t j = j0 + u * 32u + lane;
+                if (j < len) {
+                    iv[u] = __ldcs(si + a + j);
+                    vv[u] = __ldcs(reinterpret_cast<const unsigned short *>(sv) + a + j);
+                }
+            }
+#pragma unroll
+            for (unsigned u = 0; u < U; ++u) {
+                const uint32_t j = j0 + u * 32u + lane;
+                if (j < len) {
+                    dst_idx[d + j] = iv[u];
+                    dst_val[d + j] = vv[u];
+                }
+            }
         }
     }
 }
