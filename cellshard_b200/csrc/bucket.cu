@@ -269,8 +269,8 @@ __global__ void __launch_bounds__(256) segment_copy_kernel(uint32_t n, const uin
         const uint32_t a = sp[local];
         const uint32_t len = sp[local + 1u] - a;
         const uint32_t d = dst_ptr[i];
-        // four coalesced loads per array in flight per lane before the stores
-        constexpr unsigned U = 4;
+        // eight coalesced loads per array in flight per lane before the stores
+        constexpr unsigned U = 8;
         for (uint32_t j0 = 0; j0 < len; j0 += 32u * U) {
             uint32_t iv[U];
             uint16_t vv[U];
