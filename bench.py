@@ -404,7 +404,8 @@ def cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, seconds):
 
 def run_convert(args):
     """Conversion kernels on the same 500,000 x 32,768 matrix: CSR -> Blocked-ELL-16,
-    CSR -> Sliced-ELL (h 32), stable transpose, nnz plan + rebuild.  One JSON line per
+    Blocked-ELL-16 -> Sliced-ELL (h 32), CSR -> Sliced-ELL (h 32), stable transpose,
+    nnz plan + rebuild.  One JSON line per
     operation with device time (CUDA events, mean of --steps after --warmup) and
     algorithmic GB/s."""
     import ctypes as C
@@ -461,7 +462,26 @@ def run_convert(args):
                                                          scratch.numel(), ptr(status), stream_handle()))
     emit("blocked_ell_emit", ms_emit, 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4,
          {"ell_cols": bell.ell_cols})
-    del bell
+    # Blocked-ELL -> Sliced-ELL (h 32): live-entry row pointers (count + scan), then the emit;
+    # both read the whole value array (the layout needs every row's count before any slot)
+    from cellshard_b200.device import blocked_ell_row_ptr, sliced_ell_from_blocked_ell
+
+    bv = bell.view()
+    bell_bytes = R * bell.ell_cols * 2 + rb * width * 4
+    rbytes = C.c_size_t()
+    lib.cs_b200_blocked_ell_row_ptr_scratch_bytes(R, C.byref(rbytes))
+    rscr = torch.empty(max(rbytes.value, 16), dtype=torch.uint8, device="cuda")
+    rp = torch.empty(R + 1, dtype=torch.int32, device="cuda")
+    ms_rp = timed(lambda: lib.cs_b200_blocked_ell_row_ptr(C.byref(bv), ptr(rp), ptr(rscr), rbytes.value,
+                                                          stream_handle()))
+    emit("blocked_ell_row_ptr", ms_rp, bell_bytes + 4 * (R + 1))
+    sfb = sliced_ell_from_blocked_ell(bell, 32)
+    sfv = sfb.view()
+    total_fb = int(sfb.col_idx.numel())
+    ms_sfb = timed(lambda: lib.cs_b200_sliced_ell_emit_from_blocked_ell(C.byref(bv), C.byref(sfv), stream_handle()))
+    emit("sliced_ell_emit_from_blocked_ell", ms_sfb, bell_bytes + 6 * total_fb + 4 * (2 * sfb.slice_count + 1),
+         {"total_slots": total_fb})
+    del bell, sfb, rscr, rp
     torch.cuda.empty_cache()
     # Sliced-ELL at h = 32: layout + emit (the layout's total needs one host read)
     sell = sliced_ell_from_csr(csr, 32)

@@ -197,4 +197,13 @@ std::size_t scan_u32_scratch_bytes(std::size_t n);
 int scan_exclusive_u32(const uint32_t *in, uint32_t *out, std::size_t n, bool write_total, void *scratch,
                        std::size_t scratch_bytes, cudaStream_t stream);
 
+// Sliced-ELL pieces shared by the CSR and Blocked-ELL sources (sliced_ell.cu).
+int sliced_layout_launch(const cs_compressed_view *src, uint32_t slice_rows, uint32_t *d_offsets, uint32_t *d_widths,
+                         uint32_t *d_slot_offsets, uint64_t *d_total, void *scratch, std::size_t scratch_bytes,
+                         cudaStream_t stream);
+int choose_sliced_rows_core(const cs_compressed_view *v, uint32_t nnz, const unsigned int *candidates,
+                            unsigned int candidate_count, cs_sliced_ell_tune_result *out, cudaStream_t stream);
+int host_sliced_alloc(cs_host_sliced_ell *dst, uint32_t rows, uint32_t cols, uint32_t nnz, uint32_t S,
+                      uint64_t total_slots);
+
 } // namespace csb

@@ -278,6 +278,39 @@ extern "C" int cs_b200_sliced_ell_candidates(const cs_compressed_view *src, cons
 
 namespace {
 
+// Host result packed as sparse::allocate(sliced_ell) (sliced_ell.cuh:165-224):
+// offsets, widths, column indices, values in one malloc'd block.
+} // namespace
+
+int csb::host_sliced_alloc(cs_host_sliced_ell *dst, uint32_t rows, uint32_t cols, uint32_t nnz, uint32_t S,
+                           uint64_t total_slots) {
+    cs_b200_host_sliced_ell_clear(dst);
+    dst->rows = rows;
+    dst->cols = cols;
+    dst->nnz = nnz;
+    const std::size_t offsets_bytes = ((std::size_t) S + 1u) * 4u;
+    const std::size_t widths_offset = align_up(offsets_bytes, 4);
+    const std::size_t widths_bytes = (std::size_t) S * 4u;
+    const std::size_t col_offset = align_up(widths_offset + widths_bytes, 4);
+    const std::size_t col_bytes = (std::size_t) total_slots * 4u;
+    const std::size_t val_offset = align_up(col_offset + col_bytes, 2);
+    const std::size_t total_bytes = val_offset + (std::size_t) total_slots * 2u;
+    char *storage = (char *) std::malloc(total_bytes);
+    if (storage == nullptr) {
+        set_error("sliced_ell host allocation failed");
+        return 0;
+    }
+    dst->slice_count = S;
+    dst->storage = storage;
+    dst->slice_row_offsets = (uint32_t *) storage;
+    dst->slice_widths = (uint32_t *) (storage + widths_offset);
+    dst->col_idx = (uint32_t *) (storage + col_offset);
+    dst->val = (uint16_t *) (storage + val_offset);
+    return 1;
+}
+
+namespace {
+
 // CSC input: the reference's CPU path (sliced_ell_from_compressed.cuh:144-163)
 // appends each column's entries to its rows in column order, i.e. the stable
 // transpose; it is staged through the GPU transpose here.
@@ -347,7 +380,15 @@ extern "C" int cs_b200_choose_sliced_ell_slice_rows_from_compressed(const cs_hos
     if (!cuda_ok(cudaStreamCreateWithFlags(&g.s, cudaStreamNonBlocking), "stream create")) return 0;
     row_source rs;
     if (!stage_rows(src, &rs, g.s)) return 0;
-    const uint32_t rows = src->rows;
+    return choose_sliced_rows_core(&rs.view, src->nnz, candidates, candidate_count, out, g.s);
+}
+
+// evaluate_sliced_candidate_ + choose_sliced_ell_slice_rows
+// (sliced_ell_from_blocked_ell.cuh:64-109,196-221) over the row pointers of a
+// device view; nnz is the source's nnz field (the storage ratio's divisor).
+int csb::choose_sliced_rows_core(const cs_compressed_view *v, uint32_t nnz, const unsigned int *candidates,
+                                 unsigned int candidate_count, cs_sliced_ell_tune_result *out, cudaStream_t stream) {
+    const uint32_t rows = v->rows;
     cs_sliced_ell_tune_result best{};
     best.slice_rows = 0u;
     best.score = __builtin_inf();
@@ -362,7 +403,7 @@ extern "C" int cs_b200_choose_sliced_ell_slice_rows_from_compressed(const cs_hos
         }
         if (n == 0u) break;
         uint64_t padded[kMaxCandidates] = {0};
-        if (rows != 0u && !padded_slots_host(&rs.view, live, n, padded, g.s)) return 0;
+        if (rows != 0u && !padded_slots_host(v, live, n, padded, stream)) return 0;
         for (unsigned int k = 0; k < n; ++k) {
             cs_sliced_ell_tune_result c{};
             if (rows == 0u) {
@@ -380,7 +421,7 @@ extern "C" int cs_b200_choose_sliced_ell_slice_rows_from_compressed(const cs_hos
                 c.slice_count = S;
                 c.padded_slots = (std::size_t) padded[k];
                 c.padded_bytes = c.padded_slots * 6u + ((std::size_t) S * 2u + 1u) * 4u;
-                c.storage_ratio = src->nnz == 0u ? 1.0 : (double) c.padded_slots / (double) src->nnz;
+                c.storage_ratio = nnz == 0u ? 1.0 : (double) c.padded_slots / (double) nnz;
                 c.slice_penalty = 0.25 * ((double) S / (double) rows);
                 c.score = c.storage_ratio + c.slice_penalty;
             }
@@ -430,30 +471,10 @@ extern "C" int cs_b200_sliced_ell_from_compressed(const cs_host_compressed *src,
         set_error("sliced_ell_from_compressed: %llu slots overflow the u32 slot index", (unsigned long long) total_slots);
         return 0;
     }
-    // host allocation packed as sparse::allocate(sliced_ell) (sliced_ell.cuh:165-224)
-    cs_b200_host_sliced_ell_clear(dst);
-    dst->rows = src->rows;
-    dst->cols = src->cols;
-    dst->nnz = src->nnz;
+    if (!host_sliced_alloc(dst, src->rows, src->cols, src->nnz, S, total_slots)) return 0;
     const std::size_t offsets_bytes = ((std::size_t) S + 1u) * 4u;
-    const std::size_t widths_offset = align_up(offsets_bytes, 4);
     const std::size_t widths_bytes = (std::size_t) S * 4u;
-    const std::size_t col_offset = align_up(widths_offset + widths_bytes, 4);
     const std::size_t col_bytes = (std::size_t) total_slots * 4u;
-    const std::size_t val_offset = align_up(col_offset + col_bytes, 2);
-    const std::size_t total_bytes = val_offset + (std::size_t) total_slots * 2u;
-    dst->slice_count = S;
-    char *storage = (char *) std::malloc(total_bytes);
-    if (storage == nullptr) {
-        set_error("sliced_ell_from_compressed: host allocation failed");
-        dst->slice_count = 0;
-        return 0;
-    }
-    dst->storage = storage;
-    dst->slice_row_offsets = (uint32_t *) storage;
-    dst->slice_widths = (uint32_t *) (storage + widths_offset);
-    dst->col_idx = (uint32_t *) (storage + col_offset);
-    dst->val = (uint16_t *) (storage + val_offset);
     bool ok = true;
     if (S == 0u) {
         dst->slice_row_offsets[0] = 0u;

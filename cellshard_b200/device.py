@@ -181,6 +181,52 @@ def sliced_ell_from_csr(csr: CSR, slice_rows: int, stream=None) -> SlicedELL:
     return out
 
 
+def blocked_ell_row_ptr(bell: BlockedELL, stream=None) -> torch.Tensor:
+    """Row pointers of a device Blocked-ELL's live entries (count_blocked_ell_row_nnz_,
+    src/convert/sliced_ell_from_blocked_ell.cuh:36-62, prefix-summed on the GPU)."""
+    lib = _abi.load()
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_blocked_ell_row_ptr_scratch_bytes(bell.rows, C.byref(nbytes)), "row_ptr scratch")
+    scratch = _scratch(nbytes.value)
+    rp = torch.empty(bell.rows + 1, dtype=torch.int32, device="cuda")
+    v = bell.view()
+    _abi.check(lib.cs_b200_blocked_ell_row_ptr(C.byref(v), ptr(rp), ptr(scratch), nbytes.value, stream_handle(stream)),
+               "blocked_ell_row_ptr")
+    return rp
+
+
+def sliced_ell_from_blocked_ell(bell: BlockedELL, slice_rows: int, stream=None) -> SlicedELL:
+    """Device Blocked-ELL -> device Sliced-ELL (convert::sliced_ell_from_blocked_ell on the
+    GPU): live-entry row pointers, the CSR layout pass over them, then the emit.
+    Synchronises once to size the slot arrays."""
+    lib = _abi.load()
+    rows = bell.rows
+    h = max(1, min(slice_rows, rows)) if rows else 0
+    S = (rows + h - 1) // h if rows else 0
+    rp = blocked_ell_row_ptr(bell, stream)
+    rv = _abi.CompressedView()
+    rv.rows, rv.cols, rv.nnz, rv.axis = rows, bell.cols, bell.nnz, COMPRESSED_BY_ROW
+    rv.majorPtr = ptr(rp)
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_sliced_ell_scratch_bytes(rows, slice_rows, C.byref(nbytes)), "sliced scratch")
+    scratch = _scratch(nbytes.value)
+    offs = torch.empty(S + 1, dtype=torch.int32, device="cuda")
+    widths = torch.empty(max(S, 1), dtype=torch.int32, device="cuda")
+    slots = torch.empty(max(S, 1), dtype=torch.int32, device="cuda")
+    total = torch.zeros(1, dtype=torch.int64, device="cuda")
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_sliced_ell_layout(C.byref(rv), slice_rows, ptr(offs), ptr(widths), ptr(slots), ptr(total),
+                                             ptr(scratch), nbytes.value, s), "sliced_ell_layout")
+    n_slots = int(total.item())
+    out = SlicedELL(rows, bell.cols, bell.nnz, h, offs, widths[:S], slots[:S],
+                    torch.empty(n_slots, dtype=torch.int32, device="cuda"),
+                    torch.empty(n_slots, dtype=torch.float16, device="cuda"))
+    bv, dv = bell.view(), out.view()
+    _abi.check(lib.cs_b200_sliced_ell_emit_from_blocked_ell(C.byref(bv), C.byref(dv), s),
+               "sliced_ell_emit_from_blocked_ell")
+    return out
+
+
 def transpose(csr: CSR, stream=None, check_status: bool = True) -> CSR:
     """build_compressed_transpose_raw on the GPU: a (cDim x uDim) compressed matrix ->
     its (uDim x cDim) transpose, minor indices ascending in each major segment."""

@@ -257,6 +257,50 @@ CS_API int cs_b200_choose_sliced_ell_slice_rows_from_compressed(const cs_host_co
                                                                 cs_sliced_ell_tune_result *out);
 
 /* ------------------------------------------------------------------------ */
+/* Blocked-ELL -> Sliced-ELL                                                  */
+/* replaces convert::sliced_ell_from_blocked_ell[_cuda],                      */
+/* choose_sliced_ell_slice_rows_from_blocked_ell and the host row count       */
+/* count_blocked_ell_row_nnz_ (src/convert/sliced_ell_from_blocked_ell.cuh:    */
+/* 36-62,146-190,223-364).  A row's entries are its live values in slot then  */
+/* lane order: valid block column, column < cols, value != 0 as a float.      */
+/* ------------------------------------------------------------------------ */
+
+CS_API int cs_b200_blocked_ell_row_ptr_scratch_bytes(uint32_t rows, size_t *out_bytes);
+
+/* d_row_ptr[rows + 1] <- exclusive prefix of the rows' live-entry counts
+ * (count_blocked_ell_row_nnz_, :36-62).  A cs_compressed_view with these
+ * row pointers (minorIdx / val unused) is a valid input of
+ * cs_b200_sliced_ell_layout and cs_b200_sliced_ell_candidates, which then
+ * give the reference's uniform layout (build_uniform_sliced_layout_,
+ * :111-142) and candidate padding for this Blocked-ELL. */
+CS_API int cs_b200_blocked_ell_row_ptr(const cs_blocked_ell_view *src,
+                                       uint32_t *d_row_ptr,
+                                       void *d_scratch,
+                                       size_t scratch_bytes,
+                                       cs_stream_t stream);
+
+/* Emit (emit_sliced_ell_from_blocked_ell_kernel, :146-190): each row's live
+ * entries in its first slots, CS_INVALID_COL / 0 padding after them.  dst
+ * carries the layout and the uniform slice_rows. */
+CS_API int cs_b200_sliced_ell_emit_from_blocked_ell(const cs_blocked_ell_view *src,
+                                                    const cs_sliced_ell_view *dst,
+                                                    cs_stream_t stream);
+
+/* Host convenience with the reference's signature and results:
+ * convert::sliced_ell_from_blocked_ell(src, slice_rows, dst) (:233-276; the
+ * result carries src->nnz, as the reference's does).  Synchronous. */
+CS_API int cs_b200_sliced_ell_from_blocked_ell(const cs_host_blocked_ell *src,
+                                               unsigned int slice_rows,
+                                               cs_host_sliced_ell *dst);
+
+/* convert::choose_sliced_ell_slice_rows_from_blocked_ell (:223-231): the
+ * chooser's score over the live-entry counts, storage ratio over src->nnz. */
+CS_API int cs_b200_choose_sliced_ell_slice_rows_from_blocked_ell(const cs_host_blocked_ell *src,
+                                                                 const unsigned int *candidates,
+                                                                 unsigned int candidate_count,
+                                                                 cs_sliced_ell_tune_result *out);
+
+/* ------------------------------------------------------------------------ */
 /* Compressed transpose                                                       */
 /* replaces convert::build_compressed_transpose_raw (src/convert/             */
 /* compressed_transpose_raw.cuh:14-123), same arguments.  The output equals   */

@@ -261,6 +261,48 @@ inline int choose_sliced_ell_slice_rows_from_compressed(const sparse::compressed
         reinterpret_cast<cs_sliced_ell_tune_result *>(out));
 }
 
+// src/convert/sliced_ell_from_blocked_ell.cuh:223-395
+inline int choose_sliced_ell_slice_rows_from_blocked_ell(const sparse::blocked_ell *src,
+                                                         const unsigned int *candidates,
+                                                         unsigned int candidate_count, sliced_ell_tune_result *out) {
+    return cs_b200_choose_sliced_ell_slice_rows_from_blocked_ell(
+        reinterpret_cast<const cs_host_blocked_ell *>(src), candidates, candidate_count,
+        reinterpret_cast<cs_sliced_ell_tune_result *>(out));
+}
+
+inline int sliced_ell_from_blocked_ell(const sparse::blocked_ell *src, unsigned int slice_rows,
+                                       sparse::sliced_ell *dst) {
+    return cs_b200_sliced_ell_from_blocked_ell(reinterpret_cast<const cs_host_blocked_ell *>(src), slice_rows,
+                                               reinterpret_cast<cs_host_sliced_ell *>(dst));
+}
+// The reference's GPU route has the same contract (host in, host out); the
+// device and stream arguments select nothing here (the current device runs it).
+inline int sliced_ell_from_blocked_ell_cuda(const sparse::blocked_ell *src, unsigned int slice_rows,
+                                            sparse::sliced_ell *dst, int device = 0, cudaStream_t stream = 0) {
+    (void) device;
+    (void) stream;
+    return sliced_ell_from_blocked_ell(src, slice_rows, dst);
+}
+
+inline int sliced_ell_from_blocked_ell_auto(const sparse::blocked_ell *src, const unsigned int *candidates,
+                                            unsigned int candidate_count, sparse::sliced_ell *dst,
+                                            sliced_ell_tune_result *picked = 0) {
+    sliced_ell_tune_result tune{};
+    if (!choose_sliced_ell_slice_rows_from_blocked_ell(src, candidates, candidate_count, &tune)) return 0;
+    if (!sliced_ell_from_blocked_ell(src, tune.slice_rows == 0u ? 1u : tune.slice_rows, dst)) return 0;
+    if (picked != 0) *picked = tune;
+    return 1;
+}
+
+inline int sliced_ell_from_blocked_ell_cuda_auto(const sparse::blocked_ell *src, const unsigned int *candidates,
+                                                 unsigned int candidate_count, sparse::sliced_ell *dst,
+                                                 int device = 0, cudaStream_t stream = 0,
+                                                 sliced_ell_tune_result *picked = 0) {
+    (void) device;
+    (void) stream;
+    return sliced_ell_from_blocked_ell_auto(src, candidates, candidate_count, dst, picked);
+}
+
 inline std::size_t compressed_transpose_scratch_bytes(types::dim_t cDim, types::dim_t uDim, types::nnz_t nnz) {
     size_t n = 0;
     return cs_b200_compressed_transpose_scratch_bytes(cDim, uDim, nnz, &n) ? n : 0;

@@ -605,6 +605,40 @@ void cso_sliced_ell_fill(uint32_t rows, const uint32_t *ptr, const uint32_t *idx
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Blocked-ELL -> its live entries as CSR, the input of the Sliced-ELL layout  */
+/* and fill above: per row, slots in order, lanes in order, an entry when the  */
+/* slot's block column is valid, the column is < cols and the value is nonzero */
+/* as a float (count_blocked_ell_row_nnz_ and the emit loop,                  */
+/* sliced_ell_from_blocked_ell.cuh:36-62,146-190).  With ptr == NULL only the  */
+/* row counts are written (into row_nnz) and the total returned.              */
+/* ------------------------------------------------------------------------ */
+uint64_t cso_bell_live_csr(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                           const uint16_t *val, uint32_t *ptr, uint32_t *idx, uint16_t *out_val) {
+    const uint32_t W = B != 0u ? ell_cols / B : 0u;
+    uint64_t n = 0u;
+    if (ptr != NULL) ptr[0] = 0u;
+    for (uint32_t r = 0; r < rows; ++r) {
+        const uint32_t rb = B != 0u ? r / B : 0u;
+        for (uint32_t s = 0; s < W; ++s) {
+            const uint32_t bc = bci[(size_t) rb * W + s];
+            if (bc == INVALID_COL) continue;
+            for (uint32_t l = 0; l < B; ++l) {
+                const uint32_t c = bc * B + l;
+                const uint16_t h = val[(size_t) r * ell_cols + (size_t) s * B + l];
+                if (c >= cols || cso_h2f(h) == 0.0f) continue;
+                if (idx != NULL) {
+                    idx[n] = c;
+                    out_val[n] = h;
+                }
+                ++n;
+            }
+        }
+        if (ptr != NULL) ptr[r + 1u] = (uint32_t) n;
+    }
+    return n;
+}
+
 uint64_t cso_sliced_padded_slots(uint32_t rows, const uint32_t *ptr, uint32_t candidate) {
     const uint32_t h = clamp_slice(rows, candidate);
     uint64_t padded = 0u;

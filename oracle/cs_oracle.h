@@ -83,6 +83,8 @@ void cso_sliced_ell_fill(uint32_t rows, const uint32_t *ptr, const uint32_t *idx
                          const uint32_t *slot_offsets, uint32_t *col_idx, uint16_t *out_val);
 /* evaluate_sliced_candidate_: padded slots for one candidate height. */
 uint64_t cso_sliced_padded_slots(uint32_t rows, const uint32_t *ptr, uint32_t candidate);
+uint64_t cso_bell_live_csr(uint32_t rows, uint32_t cols, uint32_t B, uint32_t ell_cols, const uint32_t *bci,
+                           const uint16_t *val, uint32_t *ptr, uint32_t *idx, uint16_t *out_val);
 
 /* ---- transpose: CSR (cDim x uDim) -> CSC, rows ascending in each column
  *      (cusparseCsr2cscEx2 result used by compressed_transpose_raw.cuh:43-81) ---- */

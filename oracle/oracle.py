@@ -180,6 +180,30 @@ def sliced_ell_from_csr(rows, ptr, idx, val, slice_rows):
             "col_idx": col_idx[:total], "val": v[:total], "total_slots": int(total)}
 
 
+def bell_live_csr(rows, cols, B, ell_cols, bci, val):
+    """Restated count_blocked_ell_row_nnz_ + the emit order of
+    convert::sliced_ell_from_blocked_ell (src/convert/sliced_ell_from_blocked_ell.cuh:36-62,
+    251-270): the Blocked-ELL's live entries (valid slot, column < cols, value != 0
+    as a float) per row, slots then lanes in order, as CSR."""
+    f = lib().cso_bell_live_csr
+    f.restype = C.c_uint64
+    n = f(u32(rows), u32(cols), u32(B), u32(ell_cols), _p(bci), _p(val), None, None, None)
+    ptr = np.zeros(rows + 1, np.uint32)
+    idx = np.zeros(max(n, 1), np.uint32)
+    v = np.zeros(max(n, 1), np.uint16)
+    f(u32(rows), u32(cols), u32(B), u32(ell_cols), _p(bci), _p(val), _p(ptr), _p(idx), _p(v))
+    return ptr, idx[:n], v[:n]
+
+
+def sliced_ell_from_bell(rows, cols, B, ell_cols, bci, val, slice_rows):
+    """Restated convert::sliced_ell_from_blocked_ell (sliced_ell_from_blocked_ell.cuh:233-276):
+    the uniform layout and fill of the live entries."""
+    ptr, idx, v = bell_live_csr(rows, cols, B, ell_cols, bci, val)
+    r = sliced_ell_from_csr(rows, ptr, idx, v, slice_rows)
+    r["row_ptr"] = ptr
+    return r
+
+
 def sliced_padded_slots(rows, ptr, candidate):
     f = lib().cso_sliced_padded_slots
     f.restype = C.c_uint64
@@ -290,6 +314,8 @@ def ref() -> C.CDLL:
             getattr(r, name).argtypes = [vp, vp, C.c_uint, vp]
         r.csref_sliced_total_slots.argtypes = [vp]
         r.csref_sliced_total_slots.restype = u32
+        r.csref_sliced_ell_from_blocked_ell.argtypes = [vp, C.c_uint, vp]
+        r.csref_choose_sliced_ell_slice_rows_from_blocked_ell.argtypes = [vp, vp, C.c_uint, vp]
         _r = r
     return _r
 
@@ -347,6 +373,47 @@ def ref_sliced_ell_from_compressed(rows, cols, ptr, idx, val, slice_rows):
     if dst.storage:
         ref().csref_free(dst.storage)
     return res
+
+
+def host_bell(rows, cols, nnz, B, ell_cols, bci, val):
+    h = HostBlockedEll()
+    h.rows, h.cols, h.nnz, h.block_size, h.ell_cols = rows, cols, nnz, B, ell_cols
+    h.blockColIdx, h.val = _p(bci), _p(val)
+    return h
+
+
+def _sliced_result(dst):
+    S = dst.slice_count
+    total = ref().csref_sliced_total_slots(C.byref(dst))
+
+    def arr(p, n, t):
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(t)), (n,)).copy() if n else np.zeros(0, np.dtype(t))
+
+    res = {"slice_count": S, "offsets": arr(dst.slice_row_offsets, S + 1 if dst.storage else 0, u32),
+           "widths": arr(dst.slice_widths, S, u32), "col_idx": arr(dst.col_idx, total, u32),
+           "val": arr(dst.val, total, C.c_uint16), "nnz": dst.nnz, "total_slots": int(total)}
+    if dst.storage:
+        ref().csref_free(dst.storage)
+    return res
+
+
+def ref_sliced_ell_from_blocked_ell(rows, cols, nnz, B, ell_cols, bci, val, slice_rows):
+    """convert::sliced_ell_from_blocked_ell of the reference, run on the host."""
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    dst = HostSlicedEll()
+    ok = ref().csref_sliced_ell_from_blocked_ell(C.byref(src), C.c_uint(slice_rows), C.byref(dst))
+    return _sliced_result(dst) if ok == 1 else None
+
+
+def ref_choose_sliced_ell_slice_rows_from_blocked_ell(rows, cols, nnz, B, ell_cols, bci, val, candidates):
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    c = (C.c_uint * len(candidates))(*candidates)
+    out = SlicedTune()
+    ok = ref().csref_choose_sliced_ell_slice_rows_from_blocked_ell(C.byref(src), c, C.c_uint(len(candidates)),
+                                                                   C.byref(out))
+    if ok != 1:
+        return None
+    return {k: getattr(out, k) for k, _ in SlicedTune._fields_}
 
 
 def ref_choose_sliced_ell_slice_rows(rows, cols, ptr, idx, val, candidates):

@@ -5,12 +5,15 @@
 // libcs_ref.so by oracle/Makefile.  Nothing is copied: this file only calls
 // convert::blocked_ell_from_compressed (src/convert/blocked_ell_from_compressed.cuh:258),
 // convert::choose_blocked_ell_block_size (:157),
-// convert::sliced_ell_from_compressed (src/convert/sliced_ell_from_compressed.cuh:96) and
-// convert::choose_sliced_ell_slice_rows_from_compressed (:86).
+// convert::sliced_ell_from_compressed (src/convert/sliced_ell_from_compressed.cuh:96),
+// convert::choose_sliced_ell_slice_rows_from_compressed (:86),
+// convert::sliced_ell_from_blocked_ell (src/convert/sliced_ell_from_blocked_ell.cuh:233) and
+// convert::choose_sliced_ell_slice_rows_from_blocked_ell (:223).
 // The static_asserts pin the C ABI structs of include/cellshard_b200.h to the
 // reference's format structs and device views, field for field.
 #include "src/convert/blocked_ell_from_compressed.cuh"
 #include "src/convert/sliced_ell_from_compressed.cuh"
+#include "src/convert/sliced_ell_from_blocked_ell.cuh"
 
 #include "cellshard_b200.h"
 
@@ -64,9 +67,60 @@ void to_ref(const cs_host_compressed *s, sparse::compressed *d) {
     d->val = reinterpret_cast<real::storage_t *>(s->val);
 }
 
+void to_ref_bell(const cs_host_blocked_ell *s, sparse::blocked_ell *d) {
+    sparse::init(d, s->rows, s->cols, s->nnz, s->block_size, s->ell_cols);
+    d->blockColIdx = s->blockColIdx;
+    d->val = reinterpret_cast<real::storage_t *>(s->val);
+}
+
+void from_ref_sliced(const sparse::sliced_ell &d, cs_host_sliced_ell *dst) {
+    dst->rows = d.rows;
+    dst->cols = d.cols;
+    dst->nnz = d.nnz;
+    dst->slice_count = d.slice_count;
+    dst->flags = d.flags;
+    dst->storage = d.storage;
+    dst->slice_row_offsets = d.slice_row_offsets;
+    dst->slice_widths = d.slice_widths;
+    dst->col_idx = d.col_idx;
+    dst->val = reinterpret_cast<uint16_t *>(d.val);
+}
+
+void from_ref_tune(const convert::sliced_ell_tune_result &r, cs_sliced_ell_tune_result *out) {
+    out->slice_rows = r.slice_rows;
+    out->slice_count = r.slice_count;
+    out->padded_slots = r.padded_slots;
+    out->padded_bytes = r.padded_bytes;
+    out->storage_ratio = r.storage_ratio;
+    out->slice_penalty = r.slice_penalty;
+    out->score = r.score;
+}
+
 } // namespace
 
 extern "C" {
+
+int csref_sliced_ell_from_blocked_ell(const cs_host_blocked_ell *src, unsigned int slice_rows,
+                                      cs_host_sliced_ell *dst) {
+    sparse::blocked_ell s;
+    to_ref_bell(src, &s);
+    sparse::sliced_ell d;
+    sparse::init(&d);
+    const int ok = convert::sliced_ell_from_blocked_ell(&s, slice_rows, &d);
+    from_ref_sliced(d, dst);
+    return ok;
+}
+
+int csref_choose_sliced_ell_slice_rows_from_blocked_ell(const cs_host_blocked_ell *src,
+                                                        const unsigned int *candidates, unsigned int count,
+                                                        cs_sliced_ell_tune_result *out) {
+    sparse::blocked_ell s;
+    to_ref_bell(src, &s);
+    convert::sliced_ell_tune_result r{};
+    const int ok = convert::choose_sliced_ell_slice_rows_from_blocked_ell(&s, candidates, count, &r);
+    from_ref_tune(r, out);
+    return ok;
+}
 
 int csref_blocked_ell_from_compressed(const cs_host_compressed *src, unsigned int block_size,
                                       cs_host_blocked_ell *dst) {

@@ -8,7 +8,8 @@
    as data.
 2. ref_conversions.npz -- outputs of the reference's own conversion code
    (convert::blocked_ell_from_compressed, choose_blocked_ell_block_size,
-   sliced_ell_from_compressed, choose_sliced_ell_slice_rows_from_compressed),
+   sliced_ell_from_compressed, choose_sliced_ell_slice_rows_from_compressed,
+   sliced_ell_from_blocked_ell, choose_sliced_ell_slice_rows_from_blocked_ell),
    compiled from the reference sources into oracle/_ref/libcs_ref.so by
    oracle/Makefile, on seeded small CSR inputs.  Needs the reference tree
    (only here, not on the GPU machine).
@@ -102,6 +103,8 @@ BLOCK_SIZES = [1, 2, 3, 4, 8, 16]
 SLICE_ROWS = [1, 3, 16, 32, 64]
 BLOCK_CANDIDATES = [4, 8, 16, 32]
 SLICE_CANDIDATES = [8, 16, 32, 64]
+BELL_TO_SELL_BLOCKS = [3, 4, 16]
+BELL_TO_SELL_ROWS = [3, 32]
 
 
 def ref_conversions() -> dict:
@@ -134,6 +137,26 @@ def ref_conversions() -> dict:
         out[f"{name}/choose_sell"] = np.array([s["slice_rows"], s["slice_count"], s["padded_slots"],
                                                s["padded_bytes"]], np.uint64)
         out[f"{name}/choose_sell_f"] = np.array([s["storage_ratio"], s["slice_penalty"], s["score"]], np.float64)
+        # Blocked-ELL -> Sliced-ELL on the reference's own Blocked-ELL of this case; the
+        # B = 4 matrix also gets a -0.0 and a NaN value (zero and live as floats)
+        for B in BELL_TO_SELL_BLOCKS:
+            key = f"{name}/bell{B}"
+            bci, bval = out[f"{key}/bci"], out[f"{key}/val"].copy()
+            ell_cols, bnnz = (int(x) for x in out[f"{key}/meta"])
+            if B == 4 and bval.size >= 2:
+                bval[0], bval[bval.size // 2] = 0x8000, 0x7E00
+                out[f"{key}/val_special"] = bval
+            for h in BELL_TO_SELL_ROWS:
+                r = oracle.ref_sliced_ell_from_blocked_ell(rows, cols, bnnz, B, ell_cols, bci, bval, h)
+                k2 = f"{key}/sell{h}"
+                out[f"{k2}/widths"] = r["widths"]
+                out[f"{k2}/col_idx"] = r["col_idx"]
+                out[f"{k2}/val"] = r["val"]
+                out[f"{k2}/meta"] = np.array([r["slice_count"], r["nnz"], r["total_slots"]], np.uint64)
+            t = oracle.ref_choose_sliced_ell_slice_rows_from_blocked_ell(rows, cols, bnnz, B, ell_cols, bci, bval,
+                                                                         SLICE_CANDIDATES)
+            out[f"{key}/choose_sell"] = np.array([t["slice_rows"], t["slice_count"], t["padded_slots"],
+                                                  t["padded_bytes"]], np.uint64)
     return out
 
 

@@ -136,6 +136,37 @@ def test_restated_sliced_ell_matches_reference_vectors(orc, gold):
     assert checked >= 20
 
 
+def _bell_cases(gold):
+    for n, rows, cols, ptr, idx, val in _cases(gold):
+        for B in (3, 4, 16):
+            key = f"{n}/bell{B}"
+            if f"{key}/sell3/meta" not in gold.files:
+                continue
+            ell_cols, nnz = (int(x) for x in gold[f"{key}/meta"])
+            bval = gold[f"{key}/val_special"] if f"{key}/val_special" in gold.files else gold[f"{key}/val"]
+            yield n, key, rows, cols, nnz, B, ell_cols, gold[f"{key}/bci"], bval
+
+
+def test_restated_bell_to_sliced_matches_reference_vectors(orc, gold):
+    """convert::sliced_ell_from_blocked_ell of the reference on its own
+    Blocked-ELL outputs (with a -0.0 and a NaN planted in the B = 4 matrices)."""
+    checked = 0
+    for n, key, rows, cols, nnz, B, ell_cols, bci, bval in _bell_cases(gold):
+        for hgt in (3, 32):
+            S, rnnz, total = (int(x) for x in gold[f"{key}/sell{hgt}/meta"])
+            r = orc.sliced_ell_from_bell(rows, cols, B, ell_cols, bci, bval, hgt)
+            assert rnnz == nnz, key  # the reference carries the source's nnz field
+            assert r["slice_count"] == S and r["total_slots"] == total, (key, hgt)
+            assert np.array_equal(r["widths"], gold[f"{key}/sell{hgt}/widths"]), (key, hgt)
+            assert np.array_equal(r["col_idx"], gold[f"{key}/sell{hgt}/col_idx"]), (key, hgt)
+            assert np.array_equal(r["val"], gold[f"{key}/sell{hgt}/val"]), (key, hgt)
+            checked += 1
+        hr, S, padded, pbytes = (int(x) for x in gold[f"{key}/choose_sell"])
+        live_ptr, _, _ = orc.bell_live_csr(rows, cols, B, ell_cols, bci, bval)
+        assert orc.choose_sliced_slice_rows(rows, nnz, live_ptr, (8, 16, 32, 64))[0] == hr, key
+    assert checked >= 30
+
+
 def test_restated_sliced_chooser_matches_reference_vectors(orc, gold):
     for n, rows, cols, ptr, idx, val in _cases(gold):
         hr, S, padded, pbytes = (int(x) for x in gold[f"{n}/choose_sell"])
