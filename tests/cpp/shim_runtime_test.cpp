@@ -215,6 +215,25 @@ int main(int argc, char **argv) {
         for (unsigned i = 0; i < conv.rows * conv.ell_cols; ++i) std::printf(" %g", __half2float(conv.val[i]));
         std::printf("\n");
     }
+    {
+        // Blocked-ELL -> Sliced-ELL with the slice height chosen from 2 / 4 / 8
+        const unsigned bcands[3] = {2u, 4u, 8u};
+        cs::sparse::sliced_ell sconv;
+        cs::sparse::init(&sconv);
+        cs::convert::sliced_ell_tune_result picked;
+        if (!cs::convert::sliced_ell_from_blocked_ell_auto(&conv, bcands, 3u, &sconv, &picked))
+            return fail(20, "sliced_ell_from_blocked_ell_auto");
+        unsigned total = 0u;
+        for (unsigned s = 0; s < sconv.slice_count; ++s)
+            total += (sconv.slice_row_offsets[s + 1u] - sconv.slice_row_offsets[s]) * sconv.slice_widths[s];
+        std::printf("convert.sell_from_bell %u %u %u\n", picked.slice_rows, sconv.slice_count, sconv.nnz);
+        std::printf("convert.sell_from_bell.col");
+        for (unsigned i = 0; i < total; ++i) std::printf(" %u", sconv.col_idx[i]);
+        std::printf("\nconvert.sell_from_bell.val");
+        for (unsigned i = 0; i < total; ++i) std::printf(" %g", __half2float(sconv.val[i]));
+        std::printf("\n");
+        cs::sparse::clear(&sconv);
+    }
     cs::sparse::clear(&conv);
     const unsigned cands[3] = {16u, 32u, 64u};
     cs::convert::sliced_ell_tune_result tune;

@@ -110,6 +110,13 @@ def test_shim_convert_bucket_transpose_reoptimize(shim_out, orc):
     assert list(o["convert.blocked"][:2]) == [2, ref["ell_cols"]] and o["convert.blocked"][2] == ref["nnz"]
     assert np.array_equal(o["convert.block_cols"].astype(np.uint32), ref["bci"])
     assert np.array_equal(o["convert.values"].astype(np.float16).view(np.uint16), ref["val"])
+    # Blocked-ELL (B = 2) -> Sliced-ELL at the height the chooser picks from 2 / 4 / 8
+    lp, _, _ = orc.bell_live_csr(rows, cols, 2, ref["ell_cols"], ref["bci"], ref["val"])
+    hb = orc.choose_sliced_slice_rows(rows, ref["nnz"], lp, (2, 4, 8))[0]
+    sb = orc.sliced_ell_from_bell(rows, cols, 2, ref["ell_cols"], ref["bci"], ref["val"], hb)
+    assert list(o["convert.sell_from_bell"]) == [hb, sb["slice_count"], ref["nnz"]]
+    assert np.array_equal(o["convert.sell_from_bell.col"].astype(np.uint32), sb["col_idx"])
+    assert np.array_equal(o["convert.sell_from_bell.val"].astype(np.float16).view(np.uint16), sb["val"])
     h, score, _ = orc.choose_sliced_slice_rows(rows, int(ptr[-1]), ptr, (16, 32, 64))
     assert o["convert.slice_choice"][0] == h and o["convert.slice_choice"][3] == score
     _nnz, _srt, order, offs = orc.major_nnz_plan(ptr, rows, 2)
