@@ -160,6 +160,11 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_sliced_ell_from_blocked_ell": (C.c_int, [P(HostBlockedEll), C.c_uint, P(HostSlicedEll)]),
     "cs_b200_choose_sliced_ell_slice_rows_from_blocked_ell": (C.c_int, [P(HostBlockedEll), P(C.c_uint), C.c_uint,
                                                                          P(SlicedEllTuneResult)]),
+    "cs_b200_filter_blocked_ell_scratch_bytes": (C.c_int, [u32, u32, P(sz)]),
+    "cs_b200_filter_blocked_ell_count": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
+                                                    vp, sz, vp, vp]),
+    "cs_b200_filter_blocked_ell_emit": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
+                                                   vp, vp]),
     "cs_b200_compressed_transpose_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
     "cs_b200_build_compressed_transpose": (C.c_int, [u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "cs_b200_major_nnz_bucket_sort_scratch_bytes": (C.c_int, [u32, P(sz)]),

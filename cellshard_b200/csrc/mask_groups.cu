@@ -15,6 +15,8 @@
 // end of the row) instead of shared-memory float atomics.
 #include "common.cuh"
 
+#include <cstring>
+
 namespace csb {
 namespace {
 
@@ -871,23 +873,55 @@ __device__ __forceinline__ bool reopt_keep(const cs_blocked_ell_view &src, const
     return oc < output_cols;
 }
 
+// The Blocked-ELL partitions of one shard, rows concatenated in order (the
+// reference's part_views / part_row_offsets, repack/kernels/sharded_blocked_ell.cuh:
+// 13-21); a single view is a one-part table.
+struct reopt_parts {
+    cs_blocked_ell_view v[CS_MAX_REPACK_PARTS];
+    uint32_t row_off[CS_MAX_REPACK_PARTS + 1];
+    uint32_t count;
+};
+
+__device__ __forceinline__ uint32_t part_of_row(const reopt_parts &p, uint32_t row) {
+    uint32_t lo = 0u, hi = p.count - 1u; // last part whose first row is <= row
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (p.row_off[mid] <= row)
+            lo = mid;
+        else
+            hi = mid - 1u;
+    }
+    return lo;
+}
+
+// Count (EMIT false: per output row its kept entries, a claim per output row,
+// and when kept != null the kept rows and their slots) or scatter (EMIT true).
 template <bool EMIT>
-__global__ void __launch_bounds__(kRowThreads) reopt_kernel(cs_blocked_ell_view src, cs_row_feature_mask_view masks,
-                                                            uint32_t output_rows, uint32_t output_cols,
-                                                            uint32_t *__restrict__ major_ptr,
+__global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constant__ reopt_parts parts,
+                                                            cs_row_feature_mask_view masks, uint32_t output_rows,
+                                                            uint32_t output_cols, uint32_t *__restrict__ major_ptr,
                                                             uint32_t *__restrict__ claims,
                                                             uint32_t *__restrict__ minor_idx,
-                                                            uint16_t *__restrict__ out_val, uint32_t *status) {
+                                                            uint16_t *__restrict__ out_val, uint32_t *status,
+                                                            unsigned long long *__restrict__ kept) {
     const unsigned lane = threadIdx.x & 31u;
-    const uint32_t B = src.block_size;
-    const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
-    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
+    const uint32_t rows = parts.row_off[parts.count];
+    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < rows; row += gridDim.x * kRowWarps) {
         if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) continue;
+        const uint32_t part = part_of_row(parts, row);
+        const cs_blocked_ell_view &src = parts.v[part];
+        const uint32_t local = row - parts.row_off[part];
+        if (!EMIT && kept != nullptr && lane == 0u) {
+            atomicAdd(kept, 1ull);
+            atomicAdd(kept + 1, (unsigned long long) src.ell_cols);
+        }
         const uint32_t out_row = masks.row_remap != nullptr ? masks.row_remap[row] : row;
         if (out_row >= output_rows) continue;
-        const uint32_t rb = B != 0u ? row / B : 0u;
+        const uint32_t B = src.block_size;
+        const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
+        const uint32_t rb = B != 0u ? local / B : 0u;
         const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
-        const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
+        const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
         uint32_t run = EMIT ? major_ptr[out_row] : 0u;
         // entries past the row's end (only possible when two rows remap to one
         // output row, which the count pass flags) are dropped, never written
@@ -1075,6 +1109,78 @@ extern "C" int cs_b200_reoptimize_scratch_bytes(uint32_t src_rows, uint32_t outp
     return 1;
 }
 
+namespace csb {
+namespace {
+
+bool make_parts(const cs_blocked_ell_view *views, uint32_t count, reopt_parts *p, const char *who) {
+    if (views == nullptr || count == 0u || count > CS_MAX_REPACK_PARTS) {
+        set_error("%s: 1..%u partition views required", who, CS_MAX_REPACK_PARTS);
+        return false;
+    }
+    std::memset(p, 0, sizeof(*p));
+    uint64_t rows = 0u;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (views[k].block_size == 0u && views[k].ell_cols != 0u) {
+            set_error("%s: partition %u has a zero block size", who, k);
+            return false;
+        }
+        p->v[k] = views[k];
+        p->row_off[k] = (uint32_t) rows;
+        rows += views[k].rows;
+    }
+    if (rows > 0xffffffffull) {
+        set_error("%s: shard rows overflow 32 bits", who);
+        return false;
+    }
+    p->row_off[count] = (uint32_t) rows;
+    p->count = count;
+    return true;
+}
+
+int reopt_count_launch(const reopt_parts &parts, const cs_row_feature_mask_view *masks, uint32_t output_rows,
+                       uint32_t output_cols, uint32_t *d_major_ptr, uint64_t *d_kept, void *d_scratch,
+                       std::size_t scratch_bytes, uint32_t *d_status, cudaStream_t stream, const char *who) {
+    const uint32_t rows = parts.row_off[parts.count];
+    size_t need = 0;
+    cs_b200_reoptimize_scratch_bytes(rows, output_rows, &need);
+    if (d_scratch == nullptr || scratch_bytes < need) {
+        set_error("%s: scratch %zu < %zu", who, scratch_bytes, need);
+        return 0;
+    }
+    uint32_t *claims = (uint32_t *) d_scratch;
+    void *scan_scratch = (char *) d_scratch + align_up((std::size_t) output_rows * sizeof(uint32_t) + 16u, 256);
+    if (!cuda_ok(cudaMemsetAsync(d_major_ptr, 0, ((std::size_t) output_rows + 1u) * sizeof(uint32_t), stream),
+                 "memset major_ptr") ||
+        !cuda_ok(cudaMemsetAsync(claims, 0, (std::size_t) output_rows * sizeof(uint32_t) + 4u, stream),
+                 "memset claims") ||
+        (d_kept != nullptr && !cuda_ok(cudaMemsetAsync(d_kept, 0, 16, stream), "memset kept")))
+        return 0;
+    const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
+    if (rows != 0u && (output_rows != 0u || d_kept != nullptr)) {
+        reopt_kernel<false><<<row_grid(rows), kRowThreads, 0, stream>>>(
+            parts, m, output_rows, output_cols, d_major_ptr, claims, nullptr, nullptr, d_status,
+            reinterpret_cast<unsigned long long *>(d_kept));
+        if (!launch_ok("reopt_count_kernel")) return 0;
+    }
+    return scan_exclusive_u32(d_major_ptr, d_major_ptr, output_rows, true, scan_scratch,
+                              scan_u32_scratch_bytes(output_rows), stream);
+}
+
+int reopt_emit_launch(const reopt_parts &parts, const cs_row_feature_mask_view *masks, uint32_t output_rows,
+                      uint32_t output_cols, const uint32_t *d_major_ptr, uint32_t *d_minor_idx, uint16_t *d_val,
+                      cudaStream_t stream) {
+    const uint32_t rows = parts.row_off[parts.count];
+    if (rows == 0u || output_rows == 0u) return 1;
+    const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
+    reopt_kernel<true><<<row_grid(rows), kRowThreads, 0, stream>>>(parts, m, output_rows, output_cols,
+                                                                   const_cast<uint32_t *>(d_major_ptr), nullptr,
+                                                                   d_minor_idx, d_val, nullptr, nullptr);
+    return launch_ok("reopt_emit_kernel");
+}
+
+} // namespace
+} // namespace csb
+
 extern "C" int cs_b200_reoptimize_count(const cs_blocked_ell_view *src, const cs_row_feature_mask_view *masks,
                                         uint32_t output_rows, uint32_t output_cols, uint32_t *d_major_ptr,
                                         void *d_scratch, size_t scratch_bytes, uint32_t *d_status, cs_stream_t s) {
@@ -1082,33 +1188,10 @@ extern "C" int cs_b200_reoptimize_count(const cs_blocked_ell_view *src, const cs
         set_error("reoptimize_count: null view or major_ptr");
         return 0;
     }
-    if (src->block_size == 0u && src->ell_cols != 0u) {
-        set_error("reoptimize_count: zero block size");
-        return 0;
-    }
-    size_t need = 0;
-    cs_b200_reoptimize_scratch_bytes(src->rows, output_rows, &need);
-    if (d_scratch == nullptr || scratch_bytes < need) {
-        set_error("reoptimize_count: scratch %zu < %zu", scratch_bytes, need);
-        return 0;
-    }
-    cudaStream_t stream = as_stream(s);
-    uint32_t *claims = (uint32_t *) d_scratch;
-    void *scan_scratch = (char *) d_scratch + align_up((std::size_t) output_rows * sizeof(uint32_t) + 16u, 256);
-    if (!cuda_ok(cudaMemsetAsync(d_major_ptr, 0, ((std::size_t) output_rows + 1u) * sizeof(uint32_t), stream),
-                 "memset major_ptr") ||
-        !cuda_ok(cudaMemsetAsync(claims, 0, (std::size_t) output_rows * sizeof(uint32_t) + 4u, stream),
-                 "memset claims"))
-        return 0;
-    const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
-    if (src->rows != 0u && output_rows != 0u) {
-        reopt_kernel<false><<<row_grid(src->rows), kRowThreads, 0, stream>>>(*src, m, output_rows, output_cols,
-                                                                            d_major_ptr, claims, nullptr, nullptr,
-                                                                            d_status);
-        if (!launch_ok("reopt_count_kernel")) return 0;
-    }
-    return scan_exclusive_u32(d_major_ptr, d_major_ptr, output_rows, true, scan_scratch,
-                              scan_u32_scratch_bytes(output_rows), stream);
+    reopt_parts parts;
+    if (!make_parts(src, 1u, &parts, "reoptimize_count")) return 0;
+    return reopt_count_launch(parts, masks, output_rows, output_cols, d_major_ptr, nullptr, d_scratch, scratch_bytes,
+                              d_status, as_stream(s), "reoptimize_count");
 }
 
 extern "C" int cs_b200_reoptimize_emit(const cs_blocked_ell_view *src, const cs_row_feature_mask_view *masks,
@@ -1118,9 +1201,39 @@ extern "C" int cs_b200_reoptimize_emit(const cs_blocked_ell_view *src, const cs_
         set_error("reoptimize_emit: null view or major_ptr");
         return 0;
     }
-    if (src->rows == 0u || output_rows == 0u) return 1;
-    const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
-    reopt_kernel<true><<<row_grid(src->rows), kRowThreads, 0, as_stream(s)>>>(
-        *src, m, output_rows, output_cols, const_cast<uint32_t *>(d_major_ptr), nullptr, d_minor_idx, d_val, nullptr);
-    return launch_ok("reopt_emit_kernel");
+    reopt_parts parts;
+    if (!make_parts(src, 1u, &parts, "reoptimize_emit")) return 0;
+    return reopt_emit_launch(parts, masks, output_rows, output_cols, d_major_ptr, d_minor_idx, d_val, as_stream(s));
+}
+
+extern "C" int cs_b200_filter_blocked_ell_scratch_bytes(uint32_t shard_rows, uint32_t output_rows, size_t *out_bytes) {
+    return cs_b200_reoptimize_scratch_bytes(shard_rows, output_rows, out_bytes);
+}
+
+extern "C" int cs_b200_filter_blocked_ell_count(const cs_blocked_ell_view *parts, uint32_t part_count,
+                                                const cs_row_feature_mask_view *masks, uint32_t output_rows,
+                                                uint32_t output_cols, uint32_t *d_major_ptr, uint64_t *d_kept,
+                                                void *d_scratch, size_t scratch_bytes, uint32_t *d_status,
+                                                cs_stream_t s) {
+    if (d_major_ptr == nullptr) {
+        set_error("filter_blocked_ell_count: null major_ptr");
+        return 0;
+    }
+    reopt_parts p;
+    if (!make_parts(parts, part_count, &p, "filter_blocked_ell_count")) return 0;
+    return reopt_count_launch(p, masks, output_rows, output_cols, d_major_ptr, d_kept, d_scratch, scratch_bytes,
+                              d_status, as_stream(s), "filter_blocked_ell_count");
+}
+
+extern "C" int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts, uint32_t part_count,
+                                               const cs_row_feature_mask_view *masks, uint32_t output_rows,
+                                               uint32_t output_cols, const uint32_t *d_major_ptr,
+                                               uint32_t *d_minor_idx, uint16_t *d_val, cs_stream_t s) {
+    if (d_major_ptr == nullptr) {
+        set_error("filter_blocked_ell_emit: null major_ptr");
+        return 0;
+    }
+    reopt_parts p;
+    if (!make_parts(parts, part_count, &p, "filter_blocked_ell_emit")) return 0;
+    return reopt_emit_launch(p, masks, output_rows, output_cols, d_major_ptr, d_minor_idx, d_val, as_stream(s));
 }

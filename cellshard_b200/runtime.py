@@ -120,6 +120,62 @@ def manual_reoptimize_masked_sparse(src: BlockedELL, row_keep=None, feature_keep
     return CSR(out_rows, out_cols, major, idx, val), meta
 
 
+def filter_blocked_ell_to_compressed(parts, output_rows: int, output_cols: int, keep_rows=None, keep_cols=None,
+                                     row_remap=None, col_remap=None, stream=None):
+    """Filtered Blocked-ELL -> CSR over the partitions of one shard, rows concatenated in
+    order (convert::filter_blocked_ell_to_compressed, src/convert/
+    filtered_blocked_ell_to_compressed.cuh:264-382, and the filter stage of
+    repack::build_repacked_shard_blocked_ell).  Synchronises once to size the output.
+    Returns (CSR, stats) with the reference's stats fields; kept_rows / kept_row_slots
+    count every kept source row (the repack operator's figures)."""
+    lib = _abi.load()
+    parts = list(parts) if isinstance(parts, (list, tuple)) else [parts]
+    views = (_abi.BlockedEllView * len(parts))(*[p.view() for p in parts])
+    shard_rows = sum(p.rows for p in parts)
+    m = _mask_view(keep_rows, keep_cols, row_remap, col_remap)
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_filter_blocked_ell_scratch_bytes(shard_rows, output_rows, C.byref(nbytes)), "scratch")
+    scratch = torch.empty(max(nbytes.value, 16), dtype=torch.uint8, device="cuda")
+    major = torch.empty(output_rows + 1, dtype=torch.int32, device="cuda")
+    kept = torch.zeros(2, dtype=torch.int64, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_filter_blocked_ell_count(views, len(parts), C.byref(m), output_rows, output_cols,
+                                                    ptr(major), ptr(kept), ptr(scratch), nbytes.value, ptr(status),
+                                                    s), "filter_blocked_ell_count")
+    nnz = int(major[output_rows].item()) & 0xFFFFFFFF
+    idx = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    val = torch.empty(nnz, dtype=torch.float16, device="cuda")
+    _abi.check(lib.cs_b200_filter_blocked_ell_emit(views, len(parts), C.byref(m), output_rows, output_cols,
+                                                   ptr(major), ptr(idx), ptr(val), s), "filter_blocked_ell_emit")
+    st = int(status.item())
+    if st:
+        raise _abi.CellShardError(f"filter flagged invalid input (status 0x{st:x})")
+    kept_rows, kept_slots = (int(x) for x in kept.tolist())
+    dead = max(kept_slots - nnz, 0)
+    stats = {"kept_rows": kept_rows, "output_rows": output_rows, "output_cols": output_cols, "live_nnz": nnz,
+             "kept_row_slots": kept_slots, "dead_slots": dead,
+             "live_fill_ratio": 1.0 if kept_slots == 0 else nnz / kept_slots, "dead_value_bytes": dead * 2}
+    return CSR(output_rows, output_cols, major, idx, val), stats
+
+
+def build_repacked_blocked_ell(parts, output_rows: int, output_cols: int, block_size: int, bucket_count: int,
+                               keep_rows=None, keep_cols=None, row_remap=None, col_remap=None, stream=None):
+    """repack::build_repacked_shard_blocked_ell (src/repack/operators/sharded_blocked_ell.cuh:
+    393-726) over a list of partitions: filter -> CSR, nnz bucket plan and row rebuild,
+    then the rebuilt CSR as Blocked-ELL of block_size.  Returns
+    (filtered CSR, plan, rebuilt CSR, Blocked-ELL, stats)."""
+    from .device import blocked_ell_from_csr, major_nnz_plan, rebuild_major_order
+
+    filtered, stats = filter_blocked_ell_to_compressed(parts, output_rows, output_cols, keep_rows, keep_cols,
+                                                       row_remap, col_remap, stream)
+    plan = major_nnz_plan(filtered.ptr, output_rows, bucket_count, stream)
+    rebuilt, _inverse = rebuild_major_order(filtered, plan["order"], stream)
+    bell = blocked_ell_from_csr(rebuilt, block_size, stream)
+    stats["ell_width"] = bell.ell_width
+    return filtered, plan, rebuilt, bell, stats
+
+
 class MomentsWorkspace:
     """Caller-held scratch for compute_sparse_group_moments (grows monotonically, like the
     reference's sparse_group_reduce_workspace)."""

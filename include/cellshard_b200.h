@@ -501,6 +501,49 @@ CS_API int cs_b200_reoptimize_emit(const cs_blocked_ell_view *src,
                             cs_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Filtered Blocked-ELL -> CSR over the partitions of one shard               */
+/* replaces convert::filter_blocked_ell_to_compressed (src/convert/           */
+/* filtered_blocked_ell_to_compressed.cuh:264-382) and the filter stage of    */
+/* repack::build_repacked_shard_blocked_ell (src/repack/operators/            */
+/* sharded_blocked_ell.cuh:393-566, kernels/sharded_blocked_ell.cuh:23-138).  */
+/* parts: host array of device views, rows concatenated in order (the         */
+/* reference's part_views / part_row_offsets); row masks and remaps index the */
+/* shard's rows.  The entries kept are those of the masked reoptimize above.  */
+/* ------------------------------------------------------------------------ */
+
+#define CS_MAX_REPACK_PARTS 64u
+
+CS_API int cs_b200_filter_blocked_ell_scratch_bytes(uint32_t shard_rows, uint32_t output_rows, size_t *out_bytes);
+
+/* d_major_ptr[output_rows + 1] <- row pointers of the filtered CSR (the live
+ * nnz is d_major_ptr[output_rows]); d_kept (nullable, u64[2]) <- kept rows
+ * and their Blocked-ELL slots (the reference's d_kept_rows /
+ * d_kept_row_slots).  The reference exclusive-scans counts already stored one
+ * slot up, so its pointers read [0, 0, c0, c0 + c1, ...]; these are the CSR
+ * row pointers the functions document. */
+CS_API int cs_b200_filter_blocked_ell_count(const cs_blocked_ell_view *parts,
+                                            uint32_t part_count,
+                                            const cs_row_feature_mask_view *masks,
+                                            uint32_t output_rows,
+                                            uint32_t output_cols,
+                                            uint32_t *d_major_ptr,
+                                            uint64_t *d_kept,
+                                            void *d_scratch,
+                                            size_t scratch_bytes,
+                                            uint32_t *d_status,
+                                            cs_stream_t stream);
+
+CS_API int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts,
+                                           uint32_t part_count,
+                                           const cs_row_feature_mask_view *masks,
+                                           uint32_t output_rows,
+                                           uint32_t output_cols,
+                                           const uint32_t *d_major_ptr,
+                                           uint32_t *d_minor_idx,
+                                           uint16_t *d_val,
+                                           cs_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Row-label grouped per-feature moments (no reference counterpart: the new   */
 /* entry point beside compute_sparse_group_reduce, same header style).        */
 /* ------------------------------------------------------------------------ */

@@ -43,6 +43,7 @@ using nnz_t = unsigned int;
 using idx_t = unsigned int;
 using ptr_t = unsigned int;
 using u32 = std::uint32_t;
+using u64 = std::uint64_t;
 } // namespace types
 
 namespace real {
@@ -519,6 +520,397 @@ inline int build_bucketed_major_view(const device::compressed_view *src, types::
 }
 
 } // namespace bucket
+
+// ---------------------------------------------------------------------------
+// convert:: filtered Blocked-ELL -> CSR (src/convert/filtered_blocked_ell_to_compressed.cuh)
+// ---------------------------------------------------------------------------
+namespace convert {
+
+struct alignas(16) filtered_blocked_ell_stats {
+    types::dim_t kept_rows;
+    types::dim_t output_rows;
+    types::dim_t output_cols;
+    types::nnz_t live_nnz;
+    types::u64 kept_row_slots;
+    types::u64 dead_slots;
+    double live_fill_ratio;
+    std::size_t dead_value_bytes;
+};
+
+struct alignas(16) filtered_blocked_ell_result {
+    device::compressed_view filtered;
+    bucket::compressed_major_bucket_result bucketed;
+    filtered_blocked_ell_stats stats;
+    int has_bucketed;
+};
+
+struct alignas(16) filtered_blocked_ell_workspace {
+    int device;
+    cudaStream_t stream;
+    int owns_stream;
+    types::dim_t rows_capacity;
+    types::dim_t filtered_rows_capacity;
+    types::nnz_t nnz_capacity;
+    void *d_counts_block;   // row pointers, kept counters, status
+    void *d_values_block;   // filtered column indices and values
+    void *d_scan_tmp;
+    std::size_t d_scan_tmp_bytes;
+    types::ptr_t *d_filtered_major_ptr;
+    types::idx_t *d_filtered_minor_idx;
+    real::storage_t *d_filtered_val;
+    unsigned long long *d_kept; // kept rows, kept row slots
+    std::uint32_t *d_status;
+    bucket::compressed_major_bucket_workspace bucket_ws;
+};
+
+inline void init(filtered_blocked_ell_workspace *ws) {
+    std::memset(ws, 0, sizeof(*ws));
+    ws->device = -1;
+    bucket::init(&ws->bucket_ws);
+}
+
+inline void clear(filtered_blocked_ell_workspace *ws) {
+    if (ws->device >= 0) cudaSetDevice(ws->device);
+    bucket::clear(&ws->bucket_ws);
+    if (ws->d_scan_tmp) cudaFree(ws->d_scan_tmp);
+    if (ws->d_values_block) cudaFree(ws->d_values_block);
+    if (ws->d_counts_block) cudaFree(ws->d_counts_block);
+    if (ws->owns_stream && ws->stream) cudaStreamDestroy(ws->stream);
+    init(ws);
+}
+
+inline int setup(filtered_blocked_ell_workspace *ws, int device, cudaStream_t stream = 0) {
+    clear(ws);
+    if (cudaSetDevice(device) != cudaSuccess) return 0;
+    ws->device = device;
+    if (stream == 0) {
+        if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return 0;
+        ws->owns_stream = 1;
+    } else {
+        ws->stream = stream;
+    }
+    return bucket::setup(&ws->bucket_ws, device);
+}
+
+inline int reserve(filtered_blocked_ell_workspace *ws, types::dim_t src_rows, types::dim_t filtered_rows,
+                   types::dim_t /*filtered_cols*/, types::nnz_t max_nnz, types::u64 /*total_values*/) {
+    if (cudaSetDevice(ws->device >= 0 ? ws->device : 0) != cudaSuccess) return 0;
+    size_t scan = 0;
+    if (!cs_b200_filter_blocked_ell_scratch_bytes(src_rows, filtered_rows, &scan)) return 0;
+    if (filtered_rows + 1u > ws->filtered_rows_capacity + 1u || !ws->d_counts_block) {
+        if (ws->d_counts_block) cudaFree(ws->d_counts_block);
+        ws->d_counts_block = nullptr;
+        const std::size_t ptr_bytes = bucket::detail::up256(((std::size_t) filtered_rows + 1u) * 4u);
+        if (cudaMalloc(&ws->d_counts_block, ptr_bytes + 256u) != cudaSuccess) return 0;
+        unsigned char *p = static_cast<unsigned char *>(ws->d_counts_block);
+        ws->d_filtered_major_ptr = reinterpret_cast<types::ptr_t *>(p);
+        ws->d_kept = reinterpret_cast<unsigned long long *>(p + ptr_bytes);
+        ws->d_status = reinterpret_cast<std::uint32_t *>(p + ptr_bytes + 64u);
+        ws->filtered_rows_capacity = filtered_rows;
+    }
+    if (max_nnz > ws->nnz_capacity || !ws->d_values_block) {
+        if (ws->d_values_block) cudaFree(ws->d_values_block);
+        ws->d_values_block = nullptr;
+        const std::size_t idx_bytes = bucket::detail::up256((std::size_t) max_nnz * 4u + 4u);
+        if (cudaMalloc(&ws->d_values_block, idx_bytes + (std::size_t) max_nnz * 2u + 16u) != cudaSuccess) return 0;
+        ws->d_filtered_minor_idx = static_cast<types::idx_t *>(ws->d_values_block);
+        ws->d_filtered_val = reinterpret_cast<real::storage_t *>(static_cast<unsigned char *>(ws->d_values_block) +
+                                                                 idx_bytes);
+        ws->nnz_capacity = max_nnz;
+    }
+    if (scan > ws->d_scan_tmp_bytes || !ws->d_scan_tmp) {
+        if (ws->d_scan_tmp) cudaFree(ws->d_scan_tmp);
+        ws->d_scan_tmp = nullptr;
+        if (cudaMalloc(&ws->d_scan_tmp, scan) != cudaSuccess) return 0;
+        ws->d_scan_tmp_bytes = scan;
+    }
+    ws->rows_capacity = src_rows;
+    return 1;
+}
+
+namespace detail {
+// Count + emit over a shard's partitions (host array of views); live nnz and
+// kept counters come back to the host, as the reference reads them.
+inline int filter_parts(const cs_blocked_ell_view *views, std::uint32_t part_count, types::dim_t output_rows,
+                        types::dim_t output_cols, const unsigned char *d_keep_rows, const unsigned char *d_keep_cols,
+                        const types::idx_t *d_row_remap, const types::idx_t *d_col_remap, types::nnz_t max_nnz,
+                        filtered_blocked_ell_workspace *ws, unsigned int *live_nnz, unsigned long long kept[2]) {
+    types::dim_t rows = 0;
+    for (std::uint32_t k = 0; k < part_count; ++k) rows += views[k].rows;
+    if (!reserve(ws, rows, output_rows, output_cols, max_nnz, 0u)) return 0;
+    cs_row_feature_mask_view m{d_keep_rows, d_keep_cols, d_row_remap, d_col_remap};
+    const cs_stream_t s = reinterpret_cast<cs_stream_t>(ws->stream);
+    if (cudaMemsetAsync(ws->d_status, 0, 4, ws->stream) != cudaSuccess) return 0;
+    if (!cs_b200_filter_blocked_ell_count(views, part_count, &m, output_rows, output_cols, ws->d_filtered_major_ptr,
+                                          reinterpret_cast<std::uint64_t *>(ws->d_kept), ws->d_scan_tmp,
+                                          ws->d_scan_tmp_bytes, ws->d_status, s))
+        return 0;
+    std::uint32_t status = 0u;
+    if (cudaMemcpyAsync(live_nnz, ws->d_filtered_major_ptr + output_rows, 4, cudaMemcpyDeviceToHost, ws->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(kept, ws->d_kept, 16, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&status, ws->d_status, 4, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ws->stream) != cudaSuccess)
+        return 0;
+    if (status != 0u || *live_nnz > max_nnz) return 0;
+    if (*live_nnz == 0u) return 1;
+    return cs_b200_filter_blocked_ell_emit(views, part_count, &m, output_rows, output_cols, ws->d_filtered_major_ptr,
+                                           ws->d_filtered_minor_idx,
+                                           reinterpret_cast<std::uint16_t *>(ws->d_filtered_val), s);
+}
+} // namespace detail
+
+// filtered_blocked_ell_to_compressed.cuh:264-382; stats as the reference fills
+// them there (kept_rows = output_rows, kept_row_slots = kept_rows * ell_cols)
+inline int filter_blocked_ell_to_compressed(const device::blocked_ell_view *src, types::dim_t output_rows,
+                                            types::dim_t output_cols, const unsigned char *d_keep_rows,
+                                            const unsigned char *d_keep_cols, const types::idx_t *d_row_remap,
+                                            const types::idx_t *d_col_remap, filtered_blocked_ell_workspace *ws,
+                                            filtered_blocked_ell_result *out) {
+    if (src == nullptr || ws == nullptr) return 0;
+    filtered_blocked_ell_result local{};
+    unsigned int live = 0u;
+    unsigned long long kept[2] = {0ull, 0ull};
+    if (output_rows != 0u && output_cols != 0u) {
+        const cs_blocked_ell_view v = *reinterpret_cast<const cs_blocked_ell_view *>(src);
+        if (!detail::filter_parts(&v, 1u, output_rows, output_cols, d_keep_rows, d_keep_cols, d_row_remap,
+                                  d_col_remap, src->nnz, ws, &live, kept))
+            return 0;
+    } else if (!reserve(ws, src->rows, output_rows, output_cols, src->nnz, 0u)) {
+        return 0;
+    }
+    local.filtered.rows = output_rows;
+    local.filtered.cols = output_cols;
+    local.filtered.nnz = live;
+    local.filtered.axis = sparse::compressed_by_row;
+    local.filtered.majorPtr = ws->d_filtered_major_ptr;
+    local.filtered.minorIdx = ws->d_filtered_minor_idx;
+    local.filtered.val = ws->d_filtered_val;
+    const types::u64 slots = (output_rows != 0u && output_cols != 0u) ? (types::u64) output_rows * src->ell_cols : 0u;
+    local.stats.kept_rows = output_rows;
+    local.stats.output_rows = output_rows;
+    local.stats.output_cols = output_cols;
+    local.stats.live_nnz = live;
+    local.stats.kept_row_slots = slots;
+    local.stats.dead_slots = slots > live ? slots - live : 0u;
+    local.stats.live_fill_ratio = slots == 0u ? 1.0 : (double) live / (double) slots;
+    local.stats.dead_value_bytes = (std::size_t) local.stats.dead_slots * sizeof(real::storage_t);
+    local.has_bucketed = 0;
+    if (out != nullptr) *out = local;
+    return 1;
+}
+
+// :384-412
+inline int build_bucketed_filtered_blocked_ell_major_view(const device::blocked_ell_view *src,
+                                                          types::dim_t output_rows, types::dim_t output_cols,
+                                                          const unsigned char *d_keep_rows,
+                                                          const unsigned char *d_keep_cols,
+                                                          const types::idx_t *d_row_remap,
+                                                          const types::idx_t *d_col_remap,
+                                                          types::idx_t requested_bucket_count,
+                                                          filtered_blocked_ell_workspace *ws,
+                                                          filtered_blocked_ell_result *out) {
+    filtered_blocked_ell_result local{};
+    if (ws == nullptr) return 0;
+    if (!filter_blocked_ell_to_compressed(src, output_rows, output_cols, d_keep_rows, d_keep_cols, d_row_remap,
+                                          d_col_remap, ws, &local))
+        return 0;
+    if (cudaStreamSynchronize(ws->stream) != cudaSuccess) return 0;
+    if (!bucket::build_bucketed_major_view(&local.filtered, requested_bucket_count, &ws->bucket_ws, &local.bucketed))
+        return 0;
+    local.has_bucketed = 1;
+    if (out != nullptr) *out = local;
+    return 1;
+}
+
+} // namespace convert
+
+// ---------------------------------------------------------------------------
+// repack:: (src/repack/operators/sharded_blocked_ell.cuh).  The reference takes
+// a sharded_device<blocked_ell> state and a shard id; sharded<> containers are
+// not part of this library, so the shard is passed as its partitions' device
+// views in row order (what the reference gathers into part_views).
+// ---------------------------------------------------------------------------
+namespace repack {
+
+struct alignas(16) sharded_blocked_ell_repack_config {
+    types::dim_t output_rows;
+    types::dim_t output_cols;
+    types::u32 block_size;
+    types::idx_t requested_bucket_count;
+};
+
+struct alignas(16) sharded_blocked_ell_repack_stats {
+    types::dim_t kept_rows;
+    types::dim_t output_rows;
+    types::dim_t output_cols;
+    types::nnz_t live_nnz;
+    types::u64 kept_row_slots;
+    types::u64 dead_slots;
+    double live_fill_ratio;
+    std::size_t dead_value_bytes;
+    types::u32 ell_width;
+};
+
+struct alignas(16) sharded_blocked_ell_repack_result {
+    device::compressed_view filtered;
+    bucket::compressed_major_bucket_result bucketed;
+    device::blocked_ell_view rebuilt;
+    bucket::major_nnz_bucket_plan_view bucket_plan;
+    sharded_blocked_ell_repack_stats stats;
+    unsigned long shard_id;
+};
+
+struct alignas(16) sharded_blocked_ell_repack_workspace {
+    int device;
+    cudaStream_t stream;
+    convert::filtered_blocked_ell_workspace filter_ws; // filtered CSR + bucket workspace
+    void *d_shape_block;                              // shape words, emitted nnz, status
+    void *d_bell_scratch;
+    std::size_t bell_scratch_bytes;
+    void *d_rebuilt_storage;
+    std::size_t rebuilt_storage_capacity_bytes;
+    types::idx_t *d_rebuilt_block_cols;
+    real::storage_t *d_rebuilt_val;
+};
+
+inline void init(sharded_blocked_ell_repack_workspace *ws) {
+    std::memset(ws, 0, sizeof(*ws));
+    ws->device = -1;
+    convert::init(&ws->filter_ws);
+}
+
+inline void clear(sharded_blocked_ell_repack_workspace *ws) {
+    convert::clear(&ws->filter_ws);
+    if (ws->d_rebuilt_storage) cudaFree(ws->d_rebuilt_storage);
+    if (ws->d_bell_scratch) cudaFree(ws->d_bell_scratch);
+    if (ws->d_shape_block) cudaFree(ws->d_shape_block);
+    init(ws);
+}
+
+inline int setup(sharded_blocked_ell_repack_workspace *ws, int device, cudaStream_t stream = 0) {
+    clear(ws);
+    if (!convert::setup(&ws->filter_ws, device, stream)) return 0;
+    ws->device = device;
+    ws->stream = ws->filter_ws.stream;
+    return cudaMalloc(&ws->d_shape_block, 256) == cudaSuccess;
+}
+
+// sharded_blocked_ell.cuh:393-726: filter the shard's partitions to CSR, bucket
+// its rows by nnz and rebuild them in bucket order, then the rebuilt CSR as
+// Blocked-ELL of cfg->block_size in workspace memory.
+inline int build_repacked_blocked_ell_parts(const device::blocked_ell_view *const *part_views,
+                                            unsigned long part_count, unsigned long shard_id,
+                                            const sharded_blocked_ell_repack_config *cfg,
+                                            const unsigned char *d_keep_rows, const unsigned char *d_keep_cols,
+                                            const types::idx_t *d_row_remap, const types::idx_t *d_col_remap,
+                                            sharded_blocked_ell_repack_workspace *ws,
+                                            sharded_blocked_ell_repack_result *out) {
+    if (part_views == nullptr || cfg == nullptr || ws == nullptr || out == nullptr || cfg->block_size == 0u ||
+        part_count == 0u || part_count > CS_MAX_REPACK_PARTS)
+        return 0;
+    cs_blocked_ell_view views[CS_MAX_REPACK_PARTS];
+    types::nnz_t shard_nnz = 0u;
+    for (unsigned long k = 0; k < part_count; ++k) {
+        if (part_views[k] == nullptr) return 0;
+        views[k] = *reinterpret_cast<const cs_blocked_ell_view *>(part_views[k]);
+        shard_nnz += part_views[k]->nnz;
+    }
+    sharded_blocked_ell_repack_result local{};
+    local.shard_id = shard_id;
+    unsigned int live = 0u;
+    unsigned long long kept[2] = {0ull, 0ull};
+    if (!convert::detail::filter_parts(views, (std::uint32_t) part_count, cfg->output_rows, cfg->output_cols,
+                                       d_keep_rows, d_keep_cols, d_row_remap, d_col_remap, shard_nnz, &ws->filter_ws,
+                                       &live, kept))
+        return 0;
+    convert::filtered_blocked_ell_workspace &fw = ws->filter_ws;
+    local.filtered.rows = cfg->output_rows;
+    local.filtered.cols = cfg->output_cols;
+    local.filtered.nnz = live;
+    local.filtered.axis = sparse::compressed_by_row;
+    local.filtered.majorPtr = fw.d_filtered_major_ptr;
+    local.filtered.minorIdx = fw.d_filtered_minor_idx;
+    local.filtered.val = fw.d_filtered_val;
+    local.stats.kept_rows = (types::dim_t) kept[0];
+    local.stats.output_rows = cfg->output_rows;
+    local.stats.output_cols = cfg->output_cols;
+    local.stats.live_nnz = live;
+    local.stats.kept_row_slots = kept[1];
+    local.stats.dead_slots = kept[1] > live ? kept[1] - live : 0u;
+    local.stats.live_fill_ratio = kept[1] == 0u ? 1.0 : (double) live / (double) kept[1];
+    local.stats.dead_value_bytes = (std::size_t) local.stats.dead_slots * sizeof(real::storage_t);
+    local.rebuilt.rows = cfg->output_rows;
+    local.rebuilt.cols = cfg->output_cols;
+    local.rebuilt.nnz = live;
+    local.rebuilt.block_size = cfg->block_size;
+    if (cfg->output_rows == 0u || cfg->output_cols == 0u || live == 0u) {
+        // as the reference: the filtered CSR doubles as the bucketed view, one bucket
+        local.bucketed.rebuilt = local.filtered;
+        local.bucketed.plan.major_dim = cfg->output_rows;
+        local.bucketed.plan.bucket_count = 1u;
+        local.bucket_plan = local.bucketed.plan;
+        *out = local;
+        return 1;
+    }
+    if (cudaStreamSynchronize(ws->stream) != cudaSuccess) return 0;
+    if (!bucket::build_bucketed_major_view(&local.filtered, cfg->requested_bucket_count, &fw.bucket_ws,
+                                           &local.bucketed) ||
+        cudaStreamSynchronize(fw.bucket_ws.stream) != cudaSuccess)
+        return 0;
+    local.bucket_plan = local.bucketed.plan;
+    // the rebuilt CSR as Blocked-ELL: shape (ell width), then the emit
+    const cs_compressed_view cv = *reinterpret_cast<const cs_compressed_view *>(&local.bucketed.rebuilt);
+    size_t sb = 0;
+    if (!cs_b200_blocked_ell_scratch_bytes(cv.rows, cv.cols, cfg->block_size, &sb)) return 0;
+    if (sb > ws->bell_scratch_bytes || !ws->d_bell_scratch) {
+        if (ws->d_bell_scratch) cudaFree(ws->d_bell_scratch);
+        ws->d_bell_scratch = nullptr;
+        if (cudaMalloc(&ws->d_bell_scratch, sb) != cudaSuccess) return 0;
+        ws->bell_scratch_bytes = sb;
+    }
+    unsigned long long *d_shape = static_cast<unsigned long long *>(ws->d_shape_block);
+    std::uint32_t *d_nnz = reinterpret_cast<std::uint32_t *>(d_shape + 2);
+    std::uint32_t *d_status = d_nnz + 1;
+    const cs_stream_t s = reinterpret_cast<cs_stream_t>(ws->stream);
+    unsigned long long shape[2] = {0ull, 0ull};
+    std::uint32_t status = 0u;
+    if (cudaMemsetAsync(ws->d_shape_block, 0, 32, ws->stream) != cudaSuccess ||
+        !cs_b200_blocked_ell_shape(&cv, cfg->block_size, reinterpret_cast<std::uint64_t *>(d_shape),
+                                   ws->d_bell_scratch, ws->bell_scratch_bytes, d_status, s) ||
+        cudaMemcpyAsync(shape, d_shape, 16, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&status, d_status, 4, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ws->stream) != cudaSuccess || status != 0u)
+        return 0;
+    const types::u32 ell_width = (types::u32) shape[0];
+    const types::u32 B = cfg->block_size;
+    const std::size_t row_blocks = ((std::size_t) cv.rows + B - 1u) / B;
+    const std::size_t idx_bytes = bucket::detail::up256(row_blocks * ell_width * 4u + 4u);
+    const std::size_t total = idx_bytes + (std::size_t) cv.rows * ell_width * B * 2u + 16u;
+    if (total > ws->rebuilt_storage_capacity_bytes || !ws->d_rebuilt_storage) {
+        if (ws->d_rebuilt_storage) cudaFree(ws->d_rebuilt_storage);
+        ws->d_rebuilt_storage = nullptr;
+        if (cudaMalloc(&ws->d_rebuilt_storage, total) != cudaSuccess) return 0;
+        ws->rebuilt_storage_capacity_bytes = total;
+    }
+    ws->d_rebuilt_block_cols = static_cast<types::idx_t *>(ws->d_rebuilt_storage);
+    ws->d_rebuilt_val = reinterpret_cast<real::storage_t *>(static_cast<unsigned char *>(ws->d_rebuilt_storage) +
+                                                            idx_bytes);
+    local.rebuilt.ell_cols = ell_width * B;
+    local.rebuilt.blockColIdx = ell_width ? ws->d_rebuilt_block_cols : nullptr;
+    local.rebuilt.val = ell_width ? ws->d_rebuilt_val : nullptr;
+    local.stats.ell_width = ell_width;
+    if (ell_width != 0u) {
+        const cs_blocked_ell_view dv = *reinterpret_cast<const cs_blocked_ell_view *>(&local.rebuilt);
+        if (!cs_b200_blocked_ell_emit(&cv, &dv, d_nnz, ws->d_bell_scratch, ws->bell_scratch_bytes, d_status, s) ||
+            cudaStreamSynchronize(ws->stream) != cudaSuccess)
+            return 0;
+    }
+    *out = local;
+    return 1;
+}
+
+} // namespace repack
 
 // ---------------------------------------------------------------------------
 // runtime:: mask_groups

@@ -438,6 +438,7 @@ def ref_gpu() -> C.CDLL:
     global _rg
     if _rg is None:
         g = C.CDLL(str(REF_GPU_LIB))
+        g.csrefgpu_filter_blocked_ell.argtypes = [vp, u32, u32, vp, vp, vp]
         for name in ("csrefgpu_group_reduce_blocked_ell", "csrefgpu_group_reduce_sliced_ell",
                      "csrefgpu_group_reduce_compressed"):
             getattr(g, name).argtypes = [vp, vp, u32, vp, vp, vp]

@@ -19,6 +19,7 @@
 #include "src/bucket/major_nnz_raw.cuh"
 #include "src/convert/compressed_transpose_raw.cuh"
 #include "src/convert/sliced_ell_from_compressed.cuh"
+#include "src/convert/filtered_blocked_ell_to_compressed.cuh"
 
 #include "cellshard_b200.h"
 
@@ -203,6 +204,26 @@ int csrefgpu_rebuild(const uint32_t *d_ptr, const uint32_t *d_idx, const uint16_
                                                         (cudaStream_t) 0);
     if (ok) ok = cudaDeviceSynchronize() == cudaSuccess;
     cudaFree(tmp);
+    return ok;
+}
+
+// convert::filter_blocked_ell_to_compressed (filtered_blocked_ell_to_compressed.cuh:264-382):
+// its row pointers (output_rows + 1) into d_major_ptr_out and its nnz field.
+int csrefgpu_filter_blocked_ell(const cs_blocked_ell_view *src, uint32_t output_rows, uint32_t output_cols,
+                                const cs_row_feature_mask_view *m, uint32_t *d_major_ptr_out, uint32_t *live_nnz_out) {
+    convert::filtered_blocked_ell_workspace ws;
+    convert::init(&ws);
+    if (!convert::setup(&ws, 0)) return 0;
+    convert::filtered_blocked_ell_result r{};
+    const device::blocked_ell_view *v = reinterpret_cast<const device::blocked_ell_view *>(src);
+    int ok = convert::filter_blocked_ell_to_compressed(v, output_rows, output_cols, m->row_keep, m->feature_keep,
+                                                       m->row_remap, m->feature_remap, &ws, &r);
+    if (ok)
+        ok = cudaStreamSynchronize(ws.stream) == cudaSuccess &&
+             cudaMemcpy(d_major_ptr_out, r.filtered.majorPtr, ((std::size_t) output_rows + 1u) * 4u,
+                        cudaMemcpyDeviceToDevice) == cudaSuccess;
+    *live_nnz_out = r.filtered.nnz;
+    convert::clear(&ws);
     return ok;
 }
 

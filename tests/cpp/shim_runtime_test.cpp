@@ -121,6 +121,7 @@ int main(int argc, char **argv) {
     hb.ell_cols = ell_cols;
     hb.blockColIdx = bci.data();
     hb.val = bval.data();
+    for (const auto &x : bval) hb.nnz += __half2float(x) != 0.0f ? 1u : 0u; // the stored nonzeros
     cs::device::partition_record<cs::sparse::blocked_ell> rb;
     if (cs::device::upload(&hb, &rb) != cudaSuccess) return fail(5, "upload blocked_ell");
     std::printf("blocked.partition_bytes %zu %zu\n", cs::device::device_partition_bytes(&hb),
@@ -201,6 +202,40 @@ int main(int argc, char **argv) {
     print_dev("reoptimize.ptr", rres.compressed.majorPtr, rres.compressed.rows + 1u);
     print_dev("reoptimize.idx", rres.compressed.minorIdx, rres.compressed.nnz);
     print_dev_half("reoptimize.val", rres.compressed.val, rres.compressed.nnz);
+
+    // filtered Blocked-ELL -> CSR and the repack (one partition, block size 2, 2 buckets)
+    {
+        const unsigned orows = (unsigned) in["reoptimize.output_rows"][0];
+        const unsigned ocols = (unsigned) in["reoptimize.output_cols"][0];
+        cs::convert::filtered_blocked_ell_workspace fws;
+        cs::convert::init(&fws);
+        if (!cs::convert::setup(&fws, 0)) return fail(21, "filter setup");
+        cs::convert::filtered_blocked_ell_result fres;
+        if (!cs::convert::build_bucketed_filtered_blocked_ell_major_view(&bview, orows, ocols, d_rk, d_fk, d_rr, d_fr,
+                                                                         2u, &fws, &fres))
+            return fail(22, "filter + bucket");
+        cudaStreamSynchronize(fws.bucket_ws.stream);
+        std::printf("filter.meta %u %u %d\n", fres.filtered.nnz, fres.stats.kept_rows, fres.has_bucketed);
+        print_dev("filter.ptr", fres.filtered.majorPtr, orows + 1u);
+        print_dev("filter.idx", fres.filtered.minorIdx, fres.filtered.nnz);
+        print_dev("filter.bucket_order", fres.bucketed.plan.major_order, orows);
+        cs::convert::clear(&fws);
+
+        cs::repack::sharded_blocked_ell_repack_workspace pws;
+        cs::repack::init(&pws);
+        if (!cs::repack::setup(&pws, 0)) return fail(23, "repack setup");
+        const cs::device::blocked_ell_view *pv[1] = {&bview};
+        const cs::repack::sharded_blocked_ell_repack_config pcfg{orows, ocols, 2u, 2u};
+        cs::repack::sharded_blocked_ell_repack_result pres;
+        if (!cs::repack::build_repacked_blocked_ell_parts(pv, 1ul, 0ul, &pcfg, d_rk, d_fk, d_rr, d_fr, &pws, &pres))
+            return fail(24, "repack");
+        std::printf("repack.meta %u %u %u %u\n", pres.stats.kept_rows, pres.stats.live_nnz, pres.stats.ell_width,
+                    pres.rebuilt.ell_cols);
+        print_dev("repack.block_cols", pres.rebuilt.blockColIdx,
+                  ((orows + 1u) / 2u) * pres.stats.ell_width);
+        print_dev_half("repack.values", pres.rebuilt.val, orows * pres.rebuilt.ell_cols);
+        cs::repack::clear(&pws);
+    }
 
     // host conversion + chooser through convert::
     cs::sparse::blocked_ell conv;

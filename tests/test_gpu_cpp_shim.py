@@ -138,6 +138,18 @@ def test_shim_convert_bucket_transpose_reoptimize(shim_out, orc):
                                             np.array(rr["row_remap"], np.uint32),
                                             np.array(rr["feature_remap"], np.uint32), rr["output_rows"],
                                             rr["output_cols"])
+    # filter (= the masked reoptimize's entries) -> bucket plan -> rebuild -> Blocked-ELL-2
+    assert list(o["filter.meta"]) == [len(ridx), rr["output_rows"], 1]
+    assert np.array_equal(o["filter.ptr"].astype(np.uint32), major)
+    assert np.array_equal(o["filter.idx"].astype(np.uint32), ridx)
+    _n, _s, order2, _o = orc.major_nnz_plan(major, rr["output_rows"], 2)
+    assert np.array_equal(o["filter.bucket_order"].astype(np.uint32), order2)
+    bp, bi, bv, _inv = orc.rebuild(major, ridx, rval, rr["output_rows"], order2)
+    rep = orc.blocked_ell_from_csr(rr["output_rows"], rr["output_cols"], bp, bi, bv, 2)
+    kept_src = int(np.count_nonzero(np.array(KA["row_keep"])))
+    assert list(o["repack.meta"]) == [kept_src, len(ridx), rep["ell_width"], rep["ell_cols"]]
+    assert np.array_equal(o["repack.block_cols"].astype(np.uint32), rep["bci"])
+    assert np.array_equal(o["repack.values"].astype(np.float16).view(np.uint16), rep["val"])
     assert np.array_equal(o["reoptimize.ptr"].astype(np.uint32), major)
     assert np.array_equal(o["reoptimize.idx"].astype(np.uint32), ridx)
     assert np.array_equal(o["reoptimize.val"].astype(np.float16).view(np.uint16), rval)
