@@ -481,7 +481,27 @@ def run_convert(args):
     ms_sfb = timed(lambda: lib.cs_b200_sliced_ell_emit_from_blocked_ell(C.byref(bv), C.byref(sfv), stream_handle()))
     emit("sliced_ell_emit_from_blocked_ell", ms_sfb, bell_bytes + 6 * total_fb + 4 * (2 * sfb.slice_count + 1),
          {"total_slots": total_fb})
-    del bell, sfb, rscr, rp
+    del sfb, rscr, rp
+    torch.cuda.empty_cache()
+    # filtered Blocked-ELL -> CSR (70 % rows, 60 % features kept) and the whole repack
+    # (filter, nnz plan over 64 buckets, row rebuild, CSR -> Blocked-ELL-16)
+    from cellshard_b200 import runtime
+
+    g = np.random.default_rng(9)
+    rk_h = g.random(R) < 0.7
+    rk = torch.from_numpy(rk_h.astype(np.uint8)).cuda()
+    fk = torch.from_numpy((g.random(Cc) < 0.6).astype(np.uint8)).cuda()
+    filt_csr, fstats = runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk)
+    del filt_csr
+    ms_f = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk))
+    emit("filter_blocked_ell_to_compressed", ms_f,
+         2 * int(rk_h.sum()) * bell.ell_cols + rb * width * 4 + R + Cc + 4 * (R + 1) + 6 * fstats["live_nnz"],
+         {"live_nnz": fstats["live_nnz"], "note": "count + emit with one host read of the live nnz; bytes are the "
+                                                  "kept rows' values, tables, row pointers and the CSR written"})
+    ms_rp2 = timed(lambda: runtime.build_repacked_blocked_ell([bell], R, Cc, BLOCK, 64, rk, fk))
+    emit("repack_blocked_ell", ms_rp2, 0, {"note": "filter + nnz plan + rebuild + CSR -> Blocked-ELL-16 with host "
+                                                   "reads of sizes between stages; time only"})
+    del bell
     torch.cuda.empty_cache()
     # Sliced-ELL at h = 32: layout + emit (the layout's total needs one host read)
     sell = sliced_ell_from_csr(csr, 32)

@@ -14,6 +14,7 @@
 // shared-memory columns (no atomics; one 32-way column sum per group at the
 // end of the row) instead of shared-memory float atomics.
 #include "common.cuh"
+#include "bell_vec.cuh"
 
 #include <cstring>
 
@@ -926,6 +927,42 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
         // entries past the row's end (only possible when two rows remap to one
         // output row, which the count pass flags) are dropped, never written
         const uint32_t end = EMIT ? major_ptr[out_row + 1u] : 0u;
+        if (B % 8u == 0u && B != 0u && (reinterpret_cast<uintptr_t>(src.val) & 15u) == 0u) {
+            // a 16-byte value vector per lane, four 256-value steps in flight; the
+            // feature flag and remap are read only for the live values, and a warp
+            // scan of the kept counts ranks them in slot order
+            constexpr unsigned kRs = 4;
+            for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
+                uint4 v[kRs];
+                uint32_t bcs[kRs];
+                load_steps(vrow, bci, B, src.ell_cols, b0, v, bcs);
+#pragma unroll
+                for (unsigned u = 0; u < kRs; ++u) {
+                    const uint32_t gene0 = bcs[u] * B + (b0 + u * 256u) % B;
+                    const uint32_t live = live_bits8(v[u]) & in_range8(bcs[u], gene0, src.cols);
+                    uint32_t keep = 0u;
+                    for (uint32_t bb = live; bb != 0u; bb &= bb - 1u) {
+                        const uint32_t q = __ffs(bb) - 1u, c = gene0 + q;
+                        if (!feature_kept(masks.feature_keep, c)) continue;
+                        const uint32_t oc = masks.feature_remap != nullptr ? masks.feature_remap[c] : c;
+                        if (oc < output_cols) keep |= 1u << q;
+                    }
+                    const uint32_t cnt = __popc(keep);
+                    const uint32_t incl = warp_inclusive_scan(cnt);
+                    if constexpr (EMIT) {
+                        uint32_t pos = run + incl - cnt;
+                        for (uint32_t bb = keep; bb != 0u; bb &= bb - 1u, ++pos) {
+                            const uint32_t q = __ffs(bb) - 1u, c = gene0 + q;
+                            if (pos < end) {
+                                minor_idx[pos] = masks.feature_remap != nullptr ? masks.feature_remap[c] : c;
+                                out_val[pos] = half_of(v[u], q);
+                            }
+                        }
+                    }
+                    run += __shfl_sync(0xffffffffu, incl, 31);
+                }
+            }
+        } else
         for (uint32_t e0 = 0; e0 < src.ell_cols; e0 += 32u) {
             const uint32_t e = e0 + lane;
             uint32_t oc = 0u;

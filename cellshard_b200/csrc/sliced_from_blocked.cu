@@ -18,6 +18,7 @@
 //                 run + rank, slot order preserved; padding (CS_INVALID_COL,
 //                 0) fills the rest of the row's width.
 #include "common.cuh"
+#include "bell_vec.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -34,43 +35,6 @@ unsigned grid_rows(uint32_t rows) {
     const uint32_t cap = (uint32_t) sm_count() * 16u;
     if (g > cap) g = cap;
     return g == 0u ? 1u : g;
-}
-
-// Bit q set when fp16 value q of the 8 in v is nonzero as a float (NaN counts).
-__device__ __forceinline__ uint32_t live_bits8(const uint4 &v) {
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    uint32_t b = 0u;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const uint32_t m = __vsetne2(w[i] & 0x7fff7fffu, 0u);
-        b |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * i);
-    }
-    return b;
-}
-
-// Columns gene0 .. gene0 + 7 of a vector inside slot bc: the mask of those
-// that exist (valid block column, column < cols).
-__device__ __forceinline__ uint32_t in_range8(uint32_t bc, uint32_t gene0, uint32_t cols) {
-    if (bc == CS_INVALID_COL || gene0 >= cols) return 0u;
-    return gene0 + 8u <= cols ? 0xffu : (1u << (cols - gene0)) - 1u;
-}
-
-__device__ __forceinline__ uint16_t half_of(const uint4 &v, uint32_t q) {
-    const uint32_t w = q < 4u ? (q < 2u ? v.x : v.y) : (q < 6u ? v.z : v.w);
-    return (uint16_t) (w >> ((q & 1u) * 16u));
-}
-
-// kSteps 16-byte value vectors of one lane (256 values apart) and their block
-// columns; positions past the row give zeros and CS_INVALID_COL.
-__device__ __forceinline__ void load_steps(const uint16_t *vrow, const uint32_t *bci, uint32_t B, uint32_t ell_cols,
-                                           uint32_t first, uint4 (&v)[kSteps], uint32_t (&bc)[kSteps]) {
-#pragma unroll
-    for (unsigned u = 0; u < kSteps; ++u) {
-        const uint32_t e0 = first + u * 256u;
-        const bool in = e0 < ell_cols;
-        v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
-        bc[u] = in ? __ldg(bci + e0 / B) : CS_INVALID_COL;
-    }
 }
 
 // VEC: block size a multiple of 8 and values 16-byte aligned.
