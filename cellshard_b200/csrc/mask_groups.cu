@@ -834,13 +834,6 @@ __global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_k
 
 #pragma nv_diag_default 186
 
-unsigned row_grid(uint32_t rows) {
-    uint32_t g = (rows + kRowWarps - 1u) / kRowWarps;
-    const uint32_t cap = (uint32_t) sm_count() * 16u;
-    if (g > cap) g = cap;
-    return g == 0u ? 1u : g;
-}
-
 int check_common(uint32_t group_count, const cs_group_filter_params *filter, const cs_group_reduce_out *out,
                  const char *who) {
     if (filter == nullptr || out == nullptr) {
@@ -904,17 +897,35 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
                                                             uint32_t *__restrict__ claims,
                                                             uint32_t *__restrict__ minor_idx,
                                                             uint16_t *__restrict__ out_val, uint32_t *status,
-                                                            unsigned long long *__restrict__ kept) {
+                                                            unsigned long long *__restrict__ kept,
+                                                            uint32_t keep_words) {
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t rows = parts.row_off[parts.count];
+    // keep_words != 0: the feature flags as a bitmap in shared memory (bit c of
+    // word c / 32), so a vector's 8 consecutive columns are checked at once
+    extern __shared__ uint32_t reopt_keep_bits[];
+    const uint32_t *kbits = keep_words != 0u ? reopt_keep_bits : nullptr;
+    uint32_t kcols = 0u; // columns the flags cover: the widest part
+    for (uint32_t k = 0; k < parts.count; ++k) kcols = max(kcols, parts.v[k].cols);
+    for (uint32_t w = threadIdx.x; w < keep_words; w += blockDim.x) {
+        uint32_t word = 0u;
+        const uint32_t c0 = w * 32u;
+#pragma unroll 4
+        for (uint32_t k = 0; k < 32u; ++k)
+            if (c0 + k < kcols) word |= (masks.feature_keep[c0 + k] != 0u ? 1u : 0u) << k;
+        reopt_keep_bits[w] = word;
+    }
+    if (keep_words != 0u) __syncthreads();
+    uint32_t warp_kept_rows = 0u;       // count pass: kept rows of this warp and their slots,
+    unsigned long long warp_kept_slots = 0u; // added to the totals once at the end
     for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < rows; row += gridDim.x * kRowWarps) {
         if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) continue;
         const uint32_t part = part_of_row(parts, row);
         const cs_blocked_ell_view &src = parts.v[part];
         const uint32_t local = row - parts.row_off[part];
-        if (!EMIT && kept != nullptr && lane == 0u) {
-            atomicAdd(kept, 1ull);
-            atomicAdd(kept + 1, (unsigned long long) src.ell_cols);
+        if (!EMIT) {
+            warp_kept_rows += 1u;
+            warp_kept_slots += src.ell_cols;
         }
         const uint32_t out_row = masks.row_remap != nullptr ? masks.row_remap[row] : row;
         if (out_row >= output_rows) continue;
@@ -932,6 +943,7 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
             // feature flag and remap are read only for the live values, and a warp
             // scan of the kept counts ranks them in slot order
             constexpr unsigned kRs = 4;
+            uint32_t lane_count = 0u;
             for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
                 uint4 v[kRs];
                 uint32_t bcs[kRs];
@@ -939,17 +951,23 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
 #pragma unroll
                 for (unsigned u = 0; u < kRs; ++u) {
                     const uint32_t gene0 = bcs[u] * B + (b0 + u * 256u) % B;
-                    const uint32_t live = live_bits8(v[u]) & in_range8(bcs[u], gene0, src.cols);
+                    uint32_t live = live_bits8(v[u]) & in_range8(bcs[u], gene0, src.cols);
+                    // gene0 is a multiple of 8: its 8 flags sit in one bitmap word
+                    if (kbits != nullptr && live != 0u) live &= kbits[gene0 >> 5] >> (gene0 & 31u);
                     uint32_t keep = 0u;
-                    for (uint32_t bb = live; bb != 0u; bb &= bb - 1u) {
-                        const uint32_t q = __ffs(bb) - 1u, c = gene0 + q;
-                        if (!feature_kept(masks.feature_keep, c)) continue;
-                        const uint32_t oc = masks.feature_remap != nullptr ? masks.feature_remap[c] : c;
-                        if (oc < output_cols) keep |= 1u << q;
+                    if (masks.feature_remap == nullptr && (kbits != nullptr || masks.feature_keep == nullptr)) {
+                        keep = live & in_range8(bcs[u], gene0, output_cols);
+                    } else {
+                        for (uint32_t bb = live; bb != 0u; bb &= bb - 1u) {
+                            const uint32_t q = __ffs(bb) - 1u, c = gene0 + q;
+                            if (kbits == nullptr && !feature_kept(masks.feature_keep, c)) continue;
+                            const uint32_t oc = masks.feature_remap != nullptr ? masks.feature_remap[c] : c;
+                            if (oc < output_cols) keep |= 1u << q;
+                        }
                     }
                     const uint32_t cnt = __popc(keep);
-                    const uint32_t incl = warp_inclusive_scan(cnt);
                     if constexpr (EMIT) {
+                        const uint32_t incl = warp_inclusive_scan(cnt);
                         uint32_t pos = run + incl - cnt;
                         for (uint32_t bb = keep; bb != 0u; bb &= bb - 1u, ++pos) {
                             const uint32_t q = __ffs(bb) - 1u, c = gene0 + q;
@@ -958,10 +976,13 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
                                 out_val[pos] = half_of(v[u], q);
                             }
                         }
+                        run += __shfl_sync(0xffffffffu, incl, 31);
+                    } else {
+                        lane_count += cnt; // the count pass needs only the row total
                     }
-                    run += __shfl_sync(0xffffffffu, incl, 31);
                 }
             }
+            if constexpr (!EMIT) run = __reduce_add_sync(0xffffffffu, lane_count);
         } else
         for (uint32_t e0 = 0; e0 < src.ell_cols; e0 += 32u) {
             const uint32_t e = e0 + lane;
@@ -990,6 +1011,10 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
             major_ptr[out_row] = run;
             if (atomicAdd(claims + out_row, 1u) != 0u) status_or(status, CS_STATUS_REMAP_COLLISION);
         }
+    }
+    if (!EMIT && kept != nullptr && lane == 0u && warp_kept_rows != 0u) {
+        atomicAdd(kept, (unsigned long long) warp_kept_rows);
+        atomicAdd(kept + 1, warp_kept_slots);
     }
 }
 
@@ -1174,6 +1199,17 @@ bool make_parts(const cs_blocked_ell_view *views, uint32_t count, reopt_parts *p
     return true;
 }
 
+// Words of the shared feature bitmap: the flags of every column of every part
+// (up to 12,288 words = 48 KB of dynamic shared memory), 0 without flags or
+// beyond that width (the kernel then reads the flags per column).
+uint32_t keep_bitmap_words(const reopt_parts &parts, const cs_row_feature_mask_view &m) {
+    if (m.feature_keep == nullptr) return 0u;
+    uint32_t cols = 0u;
+    for (uint32_t k = 0; k < parts.count; ++k) cols = parts.v[k].cols > cols ? parts.v[k].cols : cols;
+    const uint32_t words = (cols + 31u) / 32u;
+    return words <= 12288u ? words : 0u;
+}
+
 int reopt_count_launch(const reopt_parts &parts, const cs_row_feature_mask_view *masks, uint32_t output_rows,
                        uint32_t output_cols, uint32_t *d_major_ptr, uint64_t *d_kept, void *d_scratch,
                        std::size_t scratch_bytes, uint32_t *d_status, cudaStream_t stream, const char *who) {
@@ -1194,9 +1230,13 @@ int reopt_count_launch(const reopt_parts &parts, const cs_row_feature_mask_view 
         return 0;
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
     if (rows != 0u && (output_rows != 0u || d_kept != nullptr)) {
-        reopt_kernel<false><<<row_grid(rows), kRowThreads, 0, stream>>>(
-            parts, m, output_rows, output_cols, d_major_ptr, claims, nullptr, nullptr, d_status,
-            reinterpret_cast<unsigned long long *>(d_kept));
+        const uint32_t kw = keep_bitmap_words(parts, m);
+        const auto k = reopt_kernel<false>;
+        const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, kw * 4u,
+                                            (rows + kRowWarps - 1u) / kRowWarps);
+        k<<<grid, kRowThreads, kw * 4u, stream>>>(parts, m, output_rows, output_cols, d_major_ptr, claims, nullptr,
+                                                 nullptr, d_status, reinterpret_cast<unsigned long long *>(d_kept),
+                                                 kw);
         if (!launch_ok("reopt_count_kernel")) return 0;
     }
     return scan_exclusive_u32(d_major_ptr, d_major_ptr, output_rows, true, scan_scratch,
@@ -1209,9 +1249,12 @@ int reopt_emit_launch(const reopt_parts &parts, const cs_row_feature_mask_view *
     const uint32_t rows = parts.row_off[parts.count];
     if (rows == 0u || output_rows == 0u) return 1;
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
-    reopt_kernel<true><<<row_grid(rows), kRowThreads, 0, stream>>>(parts, m, output_rows, output_cols,
-                                                                   const_cast<uint32_t *>(d_major_ptr), nullptr,
-                                                                   d_minor_idx, d_val, nullptr, nullptr);
+    const uint32_t kw = keep_bitmap_words(parts, m);
+    const auto k = reopt_kernel<true>;
+    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, kw * 4u,
+                                        (rows + kRowWarps - 1u) / kRowWarps);
+    k<<<grid, kRowThreads, kw * 4u, stream>>>(parts, m, output_rows, output_cols, const_cast<uint32_t *>(d_major_ptr),
+                                             nullptr, d_minor_idx, d_val, nullptr, nullptr, kw);
     return launch_ok("reopt_emit_kernel");
 }
 
