@@ -402,6 +402,110 @@ def cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, seconds):
                       f"of the grouped moments (no reference implementation exists), {dt:.2f} s"}
 
 
+def bucket_cpu_baseline(bell, sell, chosen: int, seconds: float = 10.0):
+    """The reference's own execution-bucketing builder (oracle/_ref, host code) on the
+    first rows of the same matrix, at the bucket count the device chose; rows/s."""
+    from oracle import oracle
+
+    if not oracle.ref_bucket_available():
+        return None
+    if bell is not None:
+        B, W = bell.block_size, bell.ell_width
+        rows = min(bell.rows, max(B, (1 << 30) // max(1, 2 * bell.ell_cols)) // B * B)  # about 1 GB of values
+        bci = bell.bci[:(rows // B) * W].cpu().numpy().view(np.uint32)
+        val = bell.val[:rows * bell.ell_cols].cpu().numpy().view(np.uint16)
+        run = lambda: oracle.ref_build_bucketed_bell(rows, bell.cols, 0, B, bell.ell_cols, bci, val, chosen)
+        sample = f"first {rows} rows (Blocked-ELL-{B}), build_bucketed_execution_partition at {chosen} buckets"
+    else:
+        offs = sell.slice_row_offsets.cpu().numpy().view(np.uint32)
+        widths = sell.slice_widths.cpu().numpy().view(np.uint32)
+        slots = sell.slice_slot_offsets.cpu().numpy().view(np.uint32)
+        per = max(1, (1 << 28) // max(1, int(widths.max(initial=1)) * sell.slice_rows * 6))
+        S = min(len(widths), per)
+        rows = int(offs[S])
+        end = int(slots[S]) if S < len(widths) else int(sell.col_idx.numel())
+        col = sell.col_idx[:end].cpu().numpy().view(np.uint32)
+        val = sell.val[:end].cpu().numpy().view(np.uint16)
+        run = lambda: oracle.ref_build_bucketed_sell(rows, sell.cols, 0, offs[:S + 1], widths[:S], col, val, chosen)
+        sample = f"first {rows} rows (Sliced-ELL h {sell.slice_rows}), build_bucketed_sliced_execution_partition " \
+                 f"at {chosen} buckets"
+    n, t0 = 0, time.perf_counter()
+    while True:
+        run()
+        n += 1
+        if time.perf_counter() - t0 > seconds or n >= 20:
+            break
+    dt = (time.perf_counter() - t0) / n
+    return {"value": rows / dt, "unit": "rows/s", "cores": 1, "kind": "reference", "sample": sample}
+
+
+def bucket_lines(lib, timed, emit, bell, sell):
+    """Execution bucketing lines: the plan (counts, sort, cuts, choice of 1..8 buckets;
+    ends with one small device->host read) and the fill, timed separately; the fill's
+    algorithmic bytes are the source's index array, its valid values, the segments
+    written and the row / column maps."""
+    import ctypes as C
+
+    import torch
+
+    from cellshard_b200 import _abi
+    from cellshard_b200.device import ptr, stream_handle
+
+    nb = C.c_size_t()
+    plan = _abi.ExecBucketPlan()
+    if bell is not None:
+        R, B, W, RB = bell.rows, bell.block_size, bell.ell_width, bell.row_blocks
+        lib.cs_b200_bucketed_blocked_ell_scratch_bytes(R, B, 8, C.byref(nb))
+        scr = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+        v = bell.view()
+        plan_fn = lambda: lib.cs_b200_bucketed_blocked_ell_plan(C.byref(v), 0, ptr(scr), nb.value, C.byref(plan), None,
+                                                                stream_handle())
+        _abi.check(plan_fn(), "bucketed plan")
+        idx = torch.empty(max(plan.index_entries, 1), dtype=torch.int32, device="cuda")
+        val = torch.empty(max(plan.value_entries, 1), dtype=torch.float16, device="cuda")
+        maps = torch.empty(2 * R + 2 * bell.cols, dtype=torch.int32, device="cuda")
+        fill_fn = lambda: lib.cs_b200_bucketed_blocked_ell_fill(
+            C.byref(v), ptr(scr), C.byref(plan), ptr(idx), ptr(val), ptr(maps), ptr(maps[R:]), ptr(maps[2 * R:]),
+            ptr(maps[2 * R + bell.cols:]), stream_handle())
+        valid = (bell.bci.view(RB, W) != -1).sum(1).to(torch.int64)
+        rows_rb = torch.full((RB,), B, dtype=torch.int64, device="cuda")
+        rows_rb[-1] = R - (RB - 1) * B
+        live_values = int((valid * rows_rb).sum().item()) * B
+        fill_bytes = RB * W * 4 + 2 * live_values + 2 * plan.value_entries + 4 * plan.index_entries + 8 * R + \
+            8 * bell.cols
+        name, cols = "bucketed_blocked_ell", bell.cols
+    else:
+        R = sell.rows
+        lib.cs_b200_bucketed_sliced_ell_scratch_bytes(R, 8, C.byref(nb))
+        scr = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+        v = sell.view()
+        plan_fn = lambda: lib.cs_b200_bucketed_sliced_ell_plan(C.byref(v), 0, ptr(scr), nb.value, C.byref(plan), None,
+                                                               stream_handle())
+        _abi.check(plan_fn(), "bucketed plan")
+        idx = torch.empty(max(plan.index_entries, 1), dtype=torch.int32, device="cuda")
+        val = torch.empty(max(plan.value_entries, 1), dtype=torch.float16, device="cuda")
+        maps = torch.empty(2 * R, dtype=torch.int32, device="cuda")
+        fill_fn = lambda: lib.cs_b200_bucketed_sliced_ell_fill(C.byref(v), ptr(scr), C.byref(plan), ptr(idx), ptr(val),
+                                                               ptr(maps), ptr(maps[R:]), stream_handle())
+        total = int(sell.col_idx.numel())
+        fill_bytes = 4 * total + 2 * sell.nnz + 6 * plan.index_entries + 8 * R + 4 * (2 * sell.slice_count + 1)
+        name, cols = "bucketed_sliced_ell", sell.cols
+    ms_plan = timed(plan_fn)
+    extra = {"segments": plan.segment_count, "bucket_count": plan.bucket_count, "bytes": plan.bytes,
+             "original_bytes": plan.original_bytes}
+    emit(name + "_plan", ms_plan, 0, dict(extra, note="time only: counts, stable sort, cuts and the 1..8 choice, "
+                                                      "one device->host read"))
+    _abi.check(fill_fn(), "bucketed fill")
+    ms_fill = timed(fill_fn)
+    cpu = bucket_cpu_baseline(bell, sell, plan.bucket_count)
+    ex = dict(extra, rows_per_s=R / ((ms_plan + ms_fill) * 1e-3), cols=cols)
+    if cpu is not None:
+        ex["cpu_baseline"] = cpu
+    emit(name + "_fill", ms_fill, fill_bytes, ex)
+    del idx, val, maps, scr
+    torch.cuda.empty_cache()
+
+
 def run_convert(args):
     """Conversion kernels on the same 500,000 x 32,768 matrix: CSR -> Blocked-ELL-16,
     Blocked-ELL-16 -> Sliced-ELL (h 32), CSR -> Sliced-ELL (h 32), stable transpose,
@@ -501,6 +605,8 @@ def run_convert(args):
     ms_rp2 = timed(lambda: runtime.build_repacked_blocked_ell([bell], R, Cc, BLOCK, 64, rk, fk))
     emit("repack_blocked_ell", ms_rp2, 0, {"note": "filter + nnz plan + rebuild + CSR -> Blocked-ELL-16 with host "
                                                    "reads of sizes between stages; time only"})
+    # execution bucketing of the Blocked-ELL-16 (bucket count chosen in 1..8, then the fill)
+    bucket_lines(lib, timed, emit, bell, None)
     del bell
     torch.cuda.empty_cache()
     # Sliced-ELL at h = 32: layout + emit (the layout's total needs one host read)
@@ -510,6 +616,7 @@ def run_convert(args):
     sv = sell.view()
     ms_sell = timed(lambda: lib.cs_b200_sliced_ell_emit(C.byref(v), C.byref(sv), stream_handle()))
     emit("sliced_ell_emit", ms_sell, 4 * (R + 1) + 6 * nnz + 6 * total + 4 * (2 * S + 1), {"total_slots": total})
+    bucket_lines(lib, timed, emit, None, sell)
     del sell
     torch.cuda.empty_cache()
     # transpose

@@ -51,6 +51,28 @@ class HostSlicedEll(C.Structure):
                 ("val", vp)]
 
 
+class HostBucketedBlockedEll(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("segment_count", u32), ("segments", vp),
+                ("segment_row_offsets", vp), ("exec_to_canonical_rows", vp), ("canonical_to_exec_rows", vp),
+                ("exec_to_canonical_cols", vp), ("canonical_to_exec_cols", vp)]
+
+
+class HostBucketedSlicedEll(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("segment_count", u32), ("segments", vp),
+                ("segment_row_offsets", vp), ("exec_to_canonical_rows", vp), ("canonical_to_exec_rows", vp),
+                ("canonical_slice_count", u32), ("canonical_slice_row_offsets", vp),
+                ("canonical_slice_widths", vp)]
+
+
+class ExecBucketPlan(C.Structure):
+    _fields_ = [("segment_count", u32), ("bucket_count", u32), ("units", u32), ("block_size", u32),
+                ("bytes", u64), ("original_bytes", u64), ("index_entries", u64), ("value_entries", u64)]
+
+
+class ExecBucketSegments(C.Structure):
+    _fields_ = [("max_segments", u32), ("unit_offsets", vp), ("row_offsets", vp), ("widths", vp)]
+
+
 class BlockedEllTuneResult(C.Structure):
     _fields_ = [("block_size", C.c_uint), ("fill_ratio", C.c_double), ("padded_bytes", sz)]
 
@@ -165,6 +187,23 @@ PROTOTYPES: dict[str, tuple] = {
                                                     vp, sz, vp, vp]),
     "cs_b200_filter_blocked_ell_emit": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
                                                    vp, vp]),
+    "cs_b200_bucketed_blocked_ell_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
+    "cs_b200_bucketed_blocked_ell_plan": (C.c_int, [P(BlockedEllView), u32, vp, sz, P(ExecBucketPlan),
+                                                     P(ExecBucketSegments), vp]),
+    "cs_b200_bucketed_blocked_ell_fill": (C.c_int, [P(BlockedEllView), vp, P(ExecBucketPlan), vp, vp, vp, vp, vp,
+                                                     vp, vp]),
+    "cs_b200_bucketed_sliced_ell_scratch_bytes": (C.c_int, [u32, u32, P(sz)]),
+    "cs_b200_bucketed_sliced_ell_plan": (C.c_int, [P(SlicedEllView), u32, vp, sz, P(ExecBucketPlan),
+                                                    P(ExecBucketSegments), vp]),
+    "cs_b200_bucketed_sliced_ell_fill": (C.c_int, [P(SlicedEllView), vp, P(ExecBucketPlan), vp, vp, vp, vp, vp]),
+    "cs_b200_build_bucketed_blocked_ell_partition": (C.c_int, [P(HostBucketedBlockedEll), P(HostBlockedEll), u32,
+                                                                P(u64)]),
+    "cs_b200_choose_bucket_count_for_part": (C.c_int, [P(HostBlockedEll), P(u32), P(u64)]),
+    "cs_b200_host_bucketed_blocked_ell_clear": (None, [P(HostBucketedBlockedEll)]),
+    "cs_b200_build_bucketed_sliced_ell_partition": (C.c_int, [P(HostBucketedSlicedEll), P(HostSlicedEll), u32,
+                                                               P(u64)]),
+    "cs_b200_choose_bucket_count_for_sliced_part": (C.c_int, [P(HostSlicedEll), P(u32), P(u64)]),
+    "cs_b200_host_bucketed_sliced_ell_clear": (None, [P(HostBucketedSlicedEll)]),
     "cs_b200_compressed_transpose_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
     "cs_b200_build_compressed_transpose": (C.c_int, [u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "cs_b200_major_nnz_bucket_sort_scratch_bytes": (C.c_int, [u32, P(sz)]),

@@ -334,6 +334,47 @@ void make_sort_layout(uint32_t n, void *base, std::size_t cap, sort_layout *l) {
     l->bytes = c.used;
 }
 
+// Digit histograms of the 4 passes and the largest key, for keys given as is
+// (the sort_pairs_u32 entry below).
+__global__ void __launch_bounds__(256) key_hist_kernel(uint32_t n, const uint32_t *__restrict__ keys,
+                                                       uint32_t *__restrict__ ghist, uint32_t *__restrict__ max_key) {
+    __shared__ uint32_t h[4][kRadix];
+    for (uint32_t i = threadIdx.x; i < 4u * kRadix; i += blockDim.x) (&h[0][0])[i] = 0u;
+    __syncthreads();
+    uint32_t mx = 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = keys[i];
+        mx = max(mx, c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) atomicAdd(&h[q][(c >> (8 * q)) & 0xffu], 1u);
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31u) == 0u && mx != 0u) atomicMax(max_key, mx);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 4u * kRadix; i += blockDim.x) {
+        const uint32_t v = (&h[0][0])[i];
+        if (v != 0u) atomicAdd(ghist + i, v);
+    }
+}
+
+int run_passes(const uint32_t *keys, const uint32_t *vals, uint32_t n, uint32_t *out_keys, uint32_t *out_vals,
+               const sort_layout &l, cudaStream_t stream) {
+    // passes 0 and 1 always run (they leave the result in the output arrays);
+    // passes 2 and 3 only when some key reaches 2^16
+    const uint32_t *ik = keys, *iv = vals;
+    for (uint32_t pass = 0; pass < 4u; ++pass) {
+        uint32_t *ok = (pass % 2u == 0u) ? l.tmp_keys : out_keys;
+        uint32_t *ov = (pass % 2u == 0u) ? l.tmp_vals : out_vals;
+        onesweep_pass_kernel<<<l.tiles, kSortThreads, 0, stream>>>(
+            ik, iv, n, 8u * pass, l.ghist + pass * kRadix, l.look + (std::size_t) pass * l.tiles * kRadix,
+            l.tile_counters + pass, l.max_key, pass >= 2u ? (1u << 16) : 0u, ok, ov, l.status);
+        if (!launch_ok("onesweep_pass_kernel")) return 0;
+        ik = ok;
+        iv = ov;
+    }
+    return 1;
+}
+
 int plan_common(uint32_t n, const uint32_t *ptr, const uint32_t *const *parts, const uint32_t *part_offsets,
                 uint32_t part_count, uint32_t *d_nnz, uint32_t *d_sorted, uint32_t *d_order_in, uint32_t *d_order_out,
                 uint32_t *d_offsets, uint32_t requested, void *tmp, std::size_t tmp_bytes, cudaStream_t stream) {
@@ -351,20 +392,7 @@ int plan_common(uint32_t n, const uint32_t *ptr, const uint32_t *const *parts, c
     count_hist_kernel<<<grid1d(n, 256), 256, 0, stream>>>(n, ptr, parts, part_offsets, part_count, d_nnz, d_order_in,
                                                           l.ghist, l.max_key, clamp_buckets(n, requested), d_offsets);
     if (!launch_ok("count_hist_kernel")) return 0;
-    // passes 0 and 1 always run (they leave the result in the output arrays);
-    // passes 2 and 3 only when some count reaches 2^16
-    const uint32_t *ik = d_nnz, *iv = nullptr;
-    for (uint32_t pass = 0; pass < 4u; ++pass) {
-        uint32_t *ok = (pass % 2u == 0u) ? l.tmp_keys : d_sorted;
-        uint32_t *ov = (pass % 2u == 0u) ? l.tmp_vals : d_order_out;
-        onesweep_pass_kernel<<<l.tiles, kSortThreads, 0, stream>>>(
-            ik, iv, n, 8u * pass, l.ghist + pass * kRadix, l.look + (std::size_t) pass * l.tiles * kRadix,
-            l.tile_counters + pass, l.max_key, pass >= 2u ? (1u << 16) : 0u, ok, ov, l.status);
-        if (!launch_ok("onesweep_pass_kernel")) return 0;
-        ik = ok;
-        iv = ov;
-    }
-    return 1;
+    return run_passes(d_nnz, nullptr, n, d_sorted, d_order_out, l, stream);
 }
 
 int rebuild_common(uint32_t n, const uint32_t *order, const uint32_t *ptr, const uint32_t *idx, const uint16_t *val,
@@ -386,6 +414,28 @@ int rebuild_common(uint32_t n, const uint32_t *order, const uint32_t *ptr, const
 }
 
 } // namespace
+
+std::size_t sort_pairs_u32_scratch_bytes(uint32_t n) {
+    sort_layout l;
+    make_sort_layout(n, nullptr, 0, &l);
+    return l.bytes;
+}
+
+int sort_pairs_u32(const uint32_t *keys, const uint32_t *vals, uint32_t n, uint32_t *out_keys, uint32_t *out_vals,
+                   void *tmp, std::size_t tmp_bytes, cudaStream_t stream) {
+    if (n == 0u) return 1;
+    sort_layout l;
+    make_sort_layout(n, tmp, tmp_bytes, &l);
+    if (tmp == nullptr || l.bytes > tmp_bytes) {
+        set_error("sort_pairs_u32: sort scratch %zu < %zu bytes", tmp_bytes, l.bytes);
+        return 0;
+    }
+    if (!cuda_ok(cudaMemsetAsync(l.status, 0, l.clear_bytes, stream), "sort scratch clear")) return 0;
+    key_hist_kernel<<<grid1d(n, 256), 256, 0, stream>>>(n, keys, l.ghist, l.max_key);
+    if (!launch_ok("key_hist_kernel")) return 0;
+    return run_passes(keys, vals, n, out_keys, out_vals, l, stream);
+}
+
 } // namespace csb
 
 using namespace csb;

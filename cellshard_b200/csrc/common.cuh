@@ -197,6 +197,46 @@ std::size_t scan_u32_scratch_bytes(std::size_t n);
 int scan_exclusive_u32(const uint32_t *in, uint32_t *out, std::size_t n, bool write_total, void *scratch,
                        std::size_t scratch_bytes, cudaStream_t stream);
 
+// Stable ascending sort of n uint32 keys carrying uint32 values (vals nullptr:
+// the indices 0..n-1), LSD radix in 8-bit digit passes (bucket.cu).  Word 0
+// of the scratch is a status word (1 = a bounded look-back wait ran out).
+std::size_t sort_pairs_u32_scratch_bytes(uint32_t n);
+int sort_pairs_u32(const uint32_t *keys, const uint32_t *vals, uint32_t n, uint32_t *out_keys, uint32_t *out_vals,
+                   void *tmp, std::size_t tmp_bytes, cudaStream_t stream);
+
+// Owned device memory and stream for the synchronous host entry points.
+struct dmem {
+    void *p = nullptr;
+    dmem() = default;
+    dmem(const dmem &) = delete;
+    dmem &operator=(const dmem &) = delete;
+    ~dmem() {
+        if (p) cudaFree(p);
+    }
+    bool alloc(std::size_t n, const char *what) { return cuda_ok(cudaMalloc(&p, n == 0 ? 16 : n), what) != 0; }
+};
+
+struct own_stream {
+    cudaStream_t s = nullptr;
+    own_stream() = default;
+    own_stream(const own_stream &) = delete;
+    own_stream &operator=(const own_stream &) = delete;
+    ~own_stream() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+// Host Blocked-ELL staged on the device (the reference's upload_async), and
+// the shape check of a device Blocked-ELL view (sliced_from_blocked.cu).
+struct staged_bell {
+    dmem bci, val;
+    cs_blocked_ell_view view{};
+};
+int stage_bell(const cs_host_blocked_ell *src, staged_bell *st, cudaStream_t stream);
+int check_bell(const cs_blocked_ell_view *src, const char *who);
+// Host-owned Blocked-ELL packed as sparse::allocate lays it out (blocked_ell.cu).
+int host_blocked_ell_allocate(cs_host_blocked_ell *m);
+
 // Sliced-ELL pieces shared by the CSR and Blocked-ELL sources (sliced_ell.cu).
 int sliced_layout_launch(const cs_compressed_view *src, uint32_t slice_rows, uint32_t *d_offsets, uint32_t *d_widths,
                          uint32_t *d_slot_offsets, uint64_t *d_total, void *scratch, std::size_t scratch_bytes,

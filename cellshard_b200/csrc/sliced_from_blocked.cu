@@ -160,6 +160,8 @@ bool bell_vec(const cs_blocked_ell_view *src) {
     return src->block_size % 8u == 0u && (reinterpret_cast<uintptr_t>(src->val) & 15u) == 0u;
 }
 
+} // namespace
+
 int check_bell(const cs_blocked_ell_view *src, const char *who) {
     if (src == nullptr) {
         set_error("%s: null view", who);
@@ -173,27 +175,6 @@ int check_bell(const cs_blocked_ell_view *src, const char *who) {
     }
     return 1;
 }
-
-struct dmem {
-    void *p = nullptr;
-    ~dmem() {
-        if (p) cudaFree(p);
-    }
-    bool alloc(std::size_t n, const char *what) { return cuda_ok(cudaMalloc(&p, n == 0 ? 16 : n), what) != 0; }
-};
-
-struct own_stream {
-    cudaStream_t s = nullptr;
-    ~own_stream() {
-        if (s) cudaStreamDestroy(s);
-    }
-};
-
-// Host Blocked-ELL staged on the device (the reference's upload_async).
-struct staged_bell {
-    dmem bci, val;
-    cs_blocked_ell_view view{};
-};
 
 int stage_bell(const cs_host_blocked_ell *src, staged_bell *st, cudaStream_t stream) {
     const uint32_t B = src->block_size;
@@ -211,8 +192,6 @@ int stage_bell(const cs_host_blocked_ell *src, staged_bell *st, cudaStream_t str
                                    (uint32_t *) st->bci.p, (uint16_t *) st->val.p};
     return 1;
 }
-
-} // namespace
 
 std::size_t bell_row_ptr_scratch(uint32_t rows) { return scan_u32_scratch_bytes(rows); }
 

@@ -285,3 +285,103 @@ def rebuild_major_order(csr: CSR, order: torch.Tensor, stream=None):
                                                           ptr(dptr), ptr(didx), ptr(dval), ptr(inv), ptr(scratch),
                                                           nbytes.value, stream_handle(stream)), "rebuild")
     return CSR(csr.rows, csr.cols, dptr, didx, dval, csr.axis), inv
+
+
+@dataclass
+class BucketedPartition:
+    """Execution-bucketed partition on the device (cellshard::bucketed_blocked_ell_partition /
+    bucketed_sliced_ell_partition, io/csh5/api.cuh:316-327,394-406): the segments as device
+    views over shared back-to-back buffers, the exec <-> canonical row maps and, for
+    Blocked-ELL, the identity column maps."""
+    plan: dict
+    segments: list
+    segment_row_offsets: list
+    exec_to_canonical_rows: torch.Tensor
+    canonical_to_exec_rows: torch.Tensor
+    exec_to_canonical_cols: torch.Tensor | None = None
+    canonical_to_exec_cols: torch.Tensor | None = None
+    idx: torch.Tensor | None = None
+    val: torch.Tensor | None = None
+
+
+def _plan_dict(p: _abi.ExecBucketPlan) -> dict:
+    return {k: getattr(p, k) for k, _ in _abi.ExecBucketPlan._fields_}
+
+
+def _segments_arrays(room: int):
+    import numpy as np
+
+    arrs = [np.zeros(room + 1, np.uint32), np.zeros(room + 1, np.uint32), np.zeros(room, np.uint32)]
+    segs = _abi.ExecBucketSegments()
+    segs.max_segments = room
+    segs.unit_offsets, segs.row_offsets, segs.widths = (a.ctypes.data for a in arrs)
+    return segs, arrs
+
+
+def bucketed_blocked_ell(bell: BlockedELL, requested: int, stream=None) -> BucketedPartition:
+    """build_bucketed_blocked_ell_partition on the GPU (requested 0: choose_bucket_count_for_part's
+    count).  Synchronises once, after the plan, to size the segments."""
+    lib = _abi.load()
+    RB = bell.row_blocks if bell.rows else 0
+    room = max(1, min(max(requested, 8), max(RB, 1)))
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_bucketed_blocked_ell_scratch_bytes(bell.rows, bell.block_size, room, C.byref(nbytes)),
+               "bucketed scratch")
+    scratch = _scratch(nbytes.value)
+    plan = _abi.ExecBucketPlan()
+    segs, (unit_off, row_off, widths) = _segments_arrays(room)
+    v = bell.view()
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_bucketed_blocked_ell_plan(C.byref(v), requested, ptr(scratch), nbytes.value,
+                                                     C.byref(plan), C.byref(segs), s), "bucketed_blocked_ell_plan")
+    S, B = plan.segment_count, bell.block_size
+    bci = torch.empty(max(plan.index_entries, 1), dtype=torch.int32, device="cuda")
+    val = torch.empty(max(plan.value_entries, 1), dtype=torch.float16, device="cuda")
+    maps = torch.empty(2 * bell.rows + 2 * bell.cols + 1, dtype=torch.int32, device="cuda")
+    r, c = bell.rows, bell.cols
+    e2c, c2e, e2cc, c2ec = maps[:r], maps[r:2 * r], maps[2 * r:2 * r + c], maps[2 * r + c:2 * r + 2 * c]
+    _abi.check(lib.cs_b200_bucketed_blocked_ell_fill(C.byref(v), ptr(scratch), C.byref(plan), bci.data_ptr(),
+                                                     val.data_ptr(), ptr(e2c), ptr(c2e), ptr(e2cc), ptr(c2ec), s),
+               "bucketed_blocked_ell_fill")
+    segments, io, vo = [], 0, 0
+    for k in range(S):
+        nrb, w, rows = int(unit_off[k + 1] - unit_off[k]), int(widths[k]), int(row_off[k + 1] - row_off[k])
+        segments.append(BlockedELL(rows, bell.cols, B, w * B, bci[io:io + nrb * w], val[vo:vo + rows * w * B], 0))
+        io += nrb * w
+        vo += rows * w * B
+    return BucketedPartition(_plan_dict(plan), segments, [int(x) for x in row_off[:S + 1]], e2c, c2e, e2cc, c2ec,
+                             bci, val)
+
+
+def bucketed_sliced_ell(sell: SlicedELL, requested: int, stream=None) -> BucketedPartition:
+    """build_bucketed_sliced_ell_partition on the GPU (requested 0: choose_bucket_count_for_sliced_part's
+    count); each segment is a one-slice Sliced-ELL."""
+    lib = _abi.load()
+    rows = sell.rows
+    room = max(1, min(max(requested, 8), max(rows, 1)))
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_bucketed_sliced_ell_scratch_bytes(rows, room, C.byref(nbytes)), "bucketed scratch")
+    scratch = _scratch(nbytes.value)
+    plan = _abi.ExecBucketPlan()
+    segs, (unit_off, row_off, widths) = _segments_arrays(room)
+    v = sell.view()
+    s = stream_handle(stream)
+    _abi.check(lib.cs_b200_bucketed_sliced_ell_plan(C.byref(v), requested, ptr(scratch), nbytes.value,
+                                                    C.byref(plan), C.byref(segs), s), "bucketed_sliced_ell_plan")
+    S = plan.segment_count
+    col = torch.empty(max(plan.index_entries, 1), dtype=torch.int32, device="cuda")
+    val = torch.empty(max(plan.value_entries, 1), dtype=torch.float16, device="cuda")
+    maps = torch.empty(2 * rows + 1, dtype=torch.int32, device="cuda")
+    e2c, c2e = maps[:rows], maps[rows:2 * rows]
+    _abi.check(lib.cs_b200_bucketed_sliced_ell_fill(C.byref(v), ptr(scratch), C.byref(plan), col.data_ptr(),
+                                                    val.data_ptr(), ptr(e2c), ptr(c2e), s), "bucketed_sliced_ell_fill")
+    segments, o = [], 0
+    for k in range(S):
+        n, w = int(unit_off[k + 1] - unit_off[k]), int(widths[k])
+        z = torch.zeros(1, dtype=torch.int32, device="cuda")
+        segments.append(SlicedELL(n, sell.cols, 0, n, torch.tensor([0, n], dtype=torch.int32, device="cuda"),
+                                  torch.tensor([w], dtype=torch.int32, device="cuda"), z,
+                                  col[o:o + n * w], val[o:o + n * w]))
+        o += n * w
+    return BucketedPartition(_plan_dict(plan), segments, [int(x) for x in row_off[:S + 1]], e2c, c2e, None, None,
+                             col, val)

@@ -544,6 +544,135 @@ CS_API int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts,
                                            cs_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Execution bucketing of one partition (the persisted execution layout)      */
+/* replaces build_bucketed_blocked_ell_partition / build_bucketed_sliced_ell_ */
+/* partition (include/CellShard/io/csh5/api.cuh:726-733, src/io/csh5/runtime/ */
+/* fetch.cc:332-344 -> src/io/csh5/execution_builders_part.hh:1011-1596) and  */
+/* choose_bucket_count_for_part / choose_bucket_count_for_sliced_part (:1249, */
+/* :1572).  Blocked-ELL: row blocks stably sorted by their valid block        */
+/* columns (a partial last row block stays last), equal row-block cuts, each  */
+/* segment as wide as its widest row block, neighbouring equal widths merged  */
+/* only when all are equal.  Sliced-ELL: rows stably sorted by live slots,    */
+/* cut by the reference's byte-minimising dynamic programme into single-slice */
+/* segments.  Both fall back to one segment when the cut layout packs no      */
+/* smaller than the source.  Valid slots are compacted to the front of each   */
+/* destination row (block); padding is the invalid column with zero values.   */
+/* ------------------------------------------------------------------------ */
+
+/* cellshard::bucketed_blocked_ell_partition (io/csh5/api.cuh:316-327) */
+typedef struct cs_host_bucketed_blocked_ell {
+    uint32_t rows, cols, nnz, segment_count;
+    cs_host_blocked_ell *segments;
+    uint32_t *segment_row_offsets;
+    uint32_t *exec_to_canonical_rows;
+    uint32_t *canonical_to_exec_rows;
+    uint32_t *exec_to_canonical_cols;
+    uint32_t *canonical_to_exec_cols;
+} cs_host_bucketed_blocked_ell;
+
+/* cellshard::bucketed_sliced_ell_partition (io/csh5/api.cuh:394-406) */
+typedef struct cs_host_bucketed_sliced_ell {
+    uint32_t rows, cols, nnz, segment_count;
+    cs_host_sliced_ell *segments;
+    uint32_t *segment_row_offsets;
+    uint32_t *exec_to_canonical_rows;
+    uint32_t *canonical_to_exec_rows;
+    uint32_t canonical_slice_count;
+    uint32_t *canonical_slice_row_offsets;
+    uint32_t *canonical_slice_widths;
+} cs_host_bucketed_sliced_ell;
+
+/* A planned layout.  Segments are stored back to back: segment s's index
+ * entries (block-column indices or column indices) start at the sum of the
+ * earlier segments' index entries, its values likewise. */
+typedef struct cs_exec_bucket_plan {
+    uint32_t segment_count;
+    uint32_t bucket_count;   /* the requested count it was built for (the chosen one when 0 was asked) */
+    uint32_t units;          /* row blocks (Blocked-ELL) or rows (Sliced-ELL) */
+    uint32_t block_size;     /* Blocked-ELL block size, 1 for Sliced-ELL */
+    uint64_t bytes;          /* bucketed_bytes_out: packed bytes of the kept layout */
+    uint64_t original_bytes; /* packed bytes of the source part */
+    uint64_t index_entries;  /* all segments */
+    uint64_t value_entries;  /* all segments */
+} cs_exec_bucket_plan;
+
+/* Host arrays of a plan: room for max_segments entries (+1 for offsets),
+ * max_segments >= min(max(requested, 8), units). */
+typedef struct cs_exec_bucket_segments {
+    uint32_t max_segments;
+    uint32_t *unit_offsets;  /* [S + 1] row blocks (Blocked-ELL) or rows (Sliced-ELL) of each segment */
+    uint32_t *row_offsets;   /* [S + 1] execution rows of each segment */
+    uint32_t *widths;        /* [S] width in blocks (Blocked-ELL) or slots (Sliced-ELL) */
+} cs_exec_bucket_segments;
+
+CS_API int cs_b200_bucketed_blocked_ell_scratch_bytes(uint32_t rows, uint32_t block_size, uint32_t max_segments,
+                                                      size_t *out_bytes);
+/* Plans on the device (valid-slot counts, the stable sort, the cuts and the
+ * byte fallback) and synchronises the stream to return the plan.
+ * requested 0 picks the count in 1..min(8, row blocks) with fewest packed
+ * bytes (ties to the smaller), as choose_bucket_count_for_part. */
+CS_API int cs_b200_bucketed_blocked_ell_plan(const cs_blocked_ell_view *part,
+                                             uint32_t requested,
+                                             void *d_scratch,
+                                             size_t scratch_bytes,
+                                             cs_exec_bucket_plan *plan,
+                                             cs_exec_bucket_segments *segments,
+                                             cs_stream_t stream);
+/* Copies the part into the planned segments and writes the row maps and the
+ * identity column maps (each of the four maps nullable). */
+CS_API int cs_b200_bucketed_blocked_ell_fill(const cs_blocked_ell_view *part,
+                                             const void *d_scratch,
+                                             const cs_exec_bucket_plan *plan,
+                                             uint32_t *d_seg_block_col_idx,
+                                             uint16_t *d_seg_val,
+                                             uint32_t *d_exec_to_canonical_rows,
+                                             uint32_t *d_canonical_to_exec_rows,
+                                             uint32_t *d_exec_to_canonical_cols,
+                                             uint32_t *d_canonical_to_exec_cols,
+                                             cs_stream_t stream);
+
+CS_API int cs_b200_bucketed_sliced_ell_scratch_bytes(uint32_t rows, uint32_t max_segments, size_t *out_bytes);
+/* Live-slot counts and the stable sort on the device; the split (a
+ * sequential dynamic programme over the sorted widths, as the reference's)
+ * runs on the host over the widths copied back.  requested 0 chooses as
+ * choose_bucket_count_for_sliced_part. */
+CS_API int cs_b200_bucketed_sliced_ell_plan(const cs_sliced_ell_view *part,
+                                            uint32_t requested,
+                                            void *d_scratch,
+                                            size_t scratch_bytes,
+                                            cs_exec_bucket_plan *plan,
+                                            cs_exec_bucket_segments *segments,
+                                            cs_stream_t stream);
+CS_API int cs_b200_bucketed_sliced_ell_fill(const cs_sliced_ell_view *part,
+                                            const void *d_scratch,
+                                            const cs_exec_bucket_plan *plan,
+                                            uint32_t *d_seg_col_idx,
+                                            uint16_t *d_seg_val,
+                                            uint32_t *d_exec_to_canonical_rows,
+                                            uint32_t *d_canonical_to_exec_rows,
+                                            cs_stream_t stream);
+
+/* The reference's host signatures: H2D, plan + fill on the device, D2H into
+ * host structs packed as the reference allocates them (its clear() frees
+ * them).  bucketed_bytes_out nullable. */
+CS_API int cs_b200_build_bucketed_blocked_ell_partition(cs_host_bucketed_blocked_ell *out,
+                                                        const cs_host_blocked_ell *part,
+                                                        uint32_t requested_bucket_count,
+                                                        uint64_t *bucketed_bytes_out);
+CS_API int cs_b200_choose_bucket_count_for_part(const cs_host_blocked_ell *part,
+                                                uint32_t *bucket_count_out,
+                                                uint64_t *bucketed_bytes_out);
+CS_API void cs_b200_host_bucketed_blocked_ell_clear(cs_host_bucketed_blocked_ell *part);
+CS_API int cs_b200_build_bucketed_sliced_ell_partition(cs_host_bucketed_sliced_ell *out,
+                                                       const cs_host_sliced_ell *part,
+                                                       uint32_t requested_bucket_count,
+                                                       uint64_t *bucketed_bytes_out);
+CS_API int cs_b200_choose_bucket_count_for_sliced_part(const cs_host_sliced_ell *part,
+                                                       uint32_t *bucket_count_out,
+                                                       uint64_t *bucketed_bytes_out);
+CS_API void cs_b200_host_bucketed_sliced_ell_clear(cs_host_bucketed_sliced_ell *part);
+
+/* ------------------------------------------------------------------------ */
 /* Row-label grouped per-feature moments (no reference counterpart: the new   */
 /* entry point beside compute_sparse_group_reduce, same header style).        */
 /* ------------------------------------------------------------------------ */

@@ -745,3 +745,353 @@ void cso_rebuild(const uint32_t *ptr, const uint32_t *idx, const uint16_t *val, 
     }
     dst_ptr[n] = run;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Execution bucketing of one Blocked-ELL part                               */
+/* (src/io/csh5/execution_builders_part.hh:1018-1272).  Row blocks are       */
+/* ordered by their count of valid block columns (a stable ascending sort    */
+/* that leaves a partial last row block in place), cut into equal row-block  */
+/* ranges whose width is their widest member, and copied with the valid      */
+/* slots compacted to the front of each row block.                           */
+/* ------------------------------------------------------------------------ */
+#define CSO_INVALID 0xffffffffu
+
+static uint32_t bell_rb_rows(uint32_t rows, uint32_t B, uint32_t rb) {
+    const uint64_t begin = (uint64_t) rb * B;
+    if (begin >= rows) return 0u;
+    return rows - begin < B ? (uint32_t) (rows - begin) : B;
+}
+
+uint64_t cso_packed_blocked_ell_bytes(uint32_t rows, uint32_t ell_cols, uint32_t B) {
+    /* io/pack/packfile.cuh:110-116: 16-byte disk header, two u32 words, the
+     * block column indices and the fp16 values */
+    const uint64_t rb = B == 0u ? 0u : ((uint64_t) rows + B - 1u) / B;
+    const uint64_t w = B == 0u ? 0u : ell_cols / B;
+    return 16u + 8u + rb * w * 4u + (uint64_t) rows * ell_cols * 2u;
+}
+
+uint32_t cso_bell_exec_layout(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t requested,
+                              uint32_t *order, uint32_t *widths, uint32_t *seg_rb, uint32_t *seg_w) {
+    const uint32_t RB = B == 0u ? 0u : (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    seg_rb[0] = 0u;
+    if (RB == 0u) return 0u;
+    for (uint32_t rb = 0; rb < RB; ++rb) {
+        uint32_t n = 0u;
+        for (uint32_t s = 0; s < W; ++s) n += bci[(size_t) rb * W + s] != CSO_INVALID;
+        order[rb] = rb;
+        widths[rb] = n;
+    }
+    const uint32_t sortable = bell_rb_rows(rows, B, RB - 1u) != B ? RB - 1u : RB;
+    g_sort_keys = widths;
+    qsort(order, sortable, sizeof(uint32_t), cmp_by_key_then_id);
+    const uint32_t nb = requested < 1u ? 1u : (requested > RB ? RB : requested);
+    for (uint32_t b = 0; b < nb; ++b) {
+        /* u32 products, as written in the reference */
+        const uint32_t lo = (b * RB) / nb, hi = ((b + 1u) * RB) / nb;
+        uint32_t w = 0u;
+        for (uint32_t p = lo; p < hi; ++p)
+            if (widths[order[p]] > w) w = widths[order[p]];
+        seg_w[b] = w;
+        seg_rb[b + 1u] = hi;
+    }
+    if (nb > 1u) {
+        uint32_t same = 1u;
+        for (uint32_t b = 1; b < nb; ++b) same &= seg_w[b] == seg_w[0];
+        if (same) {
+            seg_rb[1] = RB;
+            return 1u;
+        }
+    }
+    return nb;
+}
+
+static uint32_t bell_seg_rows(uint32_t rows, uint32_t B, const uint32_t *order, uint32_t lo, uint32_t hi) {
+    uint32_t n = 0u;
+    for (uint32_t p = lo; p < hi; ++p) n += bell_rb_rows(rows, B, order[p]);
+    return n;
+}
+
+uint32_t cso_bell_exec_build_layout(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t requested,
+                                    uint32_t *order, uint32_t *widths, uint32_t *seg_rb, uint32_t *seg_w,
+                                    uint64_t *bytes) {
+    uint32_t S = cso_bell_exec_layout(rows, B, W, bci, requested, order, widths, seg_rb, seg_w);
+    uint64_t cand = 0u;
+    for (uint32_t s = 0; s < S; ++s)
+        cand += cso_packed_blocked_ell_bytes(bell_seg_rows(rows, B, order, seg_rb[s], seg_rb[s + 1u]), seg_w[s] * B, B);
+    const uint64_t orig = cso_packed_blocked_ell_bytes(rows, W * B, B);
+    if (S > 1u && cand >= orig) {
+        S = cso_bell_exec_layout(rows, B, W, bci, 1u, order, widths, seg_rb, seg_w);
+        cand = orig;
+    }
+    if (bytes != NULL) *bytes = cand;
+    return S;
+}
+
+void cso_bell_exec_fill(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, const uint16_t *val,
+                        const uint32_t *order, uint32_t S, const uint32_t *seg_rb, const uint32_t *seg_w,
+                        uint32_t *seg_bci, uint16_t *seg_val, uint32_t *exec_to_canonical,
+                        uint32_t *canonical_to_exec) {
+    const size_t src_ell = (size_t) W * B;
+    size_t bci_off = 0u, val_off = 0u;
+    uint32_t exec_row = 0u;
+    for (uint32_t s = 0; s < S; ++s) {
+        const uint32_t lo = seg_rb[s], hi = seg_rb[s + 1u], dw = seg_w[s];
+        const size_t dst_ell = (size_t) dw * B;
+        const uint32_t seg_rows = bell_seg_rows(rows, B, order, lo, hi);
+        for (size_t i = 0; i < (size_t) (hi - lo) * dw; ++i) seg_bci[bci_off + i] = CSO_INVALID;
+        memset(seg_val + val_off, 0, (size_t) seg_rows * dst_ell * sizeof(uint16_t));
+        for (uint32_t p = lo; p < hi; ++p) {
+            const uint32_t dst_rb = p - lo, src_rb = order[p], n = bell_rb_rows(rows, B, src_rb);
+            for (uint32_t r = 0; r < n; ++r) {
+                exec_to_canonical[exec_row + r] = src_rb * B + r;
+                canonical_to_exec[src_rb * B + r] = exec_row + r;
+            }
+            uint32_t slot = 0u;
+            for (uint32_t k = 0; k < W; ++k) {
+                const uint32_t c = bci[(size_t) src_rb * W + k];
+                if (c == CSO_INVALID) continue;
+                seg_bci[bci_off + (size_t) dst_rb * dw + slot] = c;
+                for (uint32_t r = 0; r < n; ++r)
+                    memcpy(seg_val + val_off + ((size_t) dst_rb * B + r) * dst_ell + (size_t) slot * B,
+                           val + ((size_t) src_rb * B + r) * src_ell + (size_t) k * B, (size_t) B * sizeof(uint16_t));
+                ++slot;
+            }
+            exec_row += n;
+        }
+        bci_off += (size_t) (hi - lo) * dw;
+        val_off += (size_t) seg_rows * dst_ell;
+    }
+}
+
+int cso_bell_choose_bucket_count(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t *count,
+                                 uint64_t *bytes) {
+    const uint32_t RB = B == 0u ? 0u : (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    const uint32_t top = RB < 8u ? (RB < 1u ? 1u : RB) : 8u;
+    uint32_t *order = (uint32_t *) malloc(((size_t) RB + 1u) * 2u * sizeof(uint32_t));
+    uint32_t seg_rb[9], seg_w[8];
+    uint32_t best = 1u;
+    uint64_t best_bytes = UINT64_MAX;
+    if (order == NULL) return 0;
+    for (uint32_t b = 1; b <= top; ++b) {
+        uint64_t x = 0u;
+        cso_bell_exec_build_layout(rows, B, W, bci, b, order, order + RB + 1u, seg_rb, seg_w, &x);
+        if (x < best_bytes) {
+            best_bytes = x;
+            best = b;
+        }
+    }
+    free(order);
+    *count = best;
+    *bytes = best_bytes;
+    return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Execution bucketing of one Sliced-ELL part                                */
+/* (src/io/csh5/execution_builders_part.hh:1274-1596).  Rows are ordered by  */
+/* their live slot count (stable, ascending) and split into at most the      */
+/* requested number of single-slice segments by a dynamic programme that     */
+/* minimises packed bytes (fixed segment bytes + 6 bytes per slot, a segment  */
+/* as wide as its last row), solved with a monotone convex-hull of lines;    */
+/* neighbouring segments of equal width are merged.                          */
+/* ------------------------------------------------------------------------ */
+uint64_t cso_packed_sliced_ell_bytes(uint32_t slice_count, uint64_t total_slots) {
+    /* io/pack/packfile.cu:179-188: 13-byte header, one u32, slice offsets,
+     * slice widths, column indices and fp16 values */
+    return 13u + 4u + ((uint64_t) slice_count + 1u) * 4u + (uint64_t) slice_count * 4u + total_slots * 6u;
+}
+
+static uint32_t sell_find_slice(uint32_t rows, uint32_t S, const uint32_t *offsets, uint32_t row) {
+    if (row >= rows) return S;
+    for (uint32_t s = 0; s < S; ++s)
+        if (row < offsets[s + 1u]) return s;
+    return S;
+}
+
+typedef struct {
+    int64_t slope, intercept;
+    uint32_t cut;
+} cso_line;
+
+static int64_t line_at(const cso_line *l, uint32_t x) { return l->intercept + l->slope * (int64_t) x; }
+
+static int line_redundant(const cso_line *a, const cso_line *m, const cso_line *b) {
+    const __int128 left = (__int128) (b->intercept - a->intercept) * (__int128) (a->slope - m->slope);
+    const __int128 right = (__int128) (m->intercept - a->intercept) * (__int128) (a->slope - b->slope);
+    return left <= right;
+}
+
+/* sorted_widths[rows] (ascending); seg_row[S+1], seg_w[S] sized for
+ * min(requested, rows) segments.  Returns S, or -1 when no split exists. */
+int cso_sell_exec_dp(uint32_t rows, const uint32_t *sorted_widths, uint32_t requested, uint32_t *seg_row,
+                     uint32_t *seg_w) {
+    const uint32_t K = requested < 1u ? 1u : (requested > rows ? (rows < 1u ? 1u : rows) : requested);
+    const uint64_t fixed = cso_packed_sliced_ell_bytes(1u, 0u), slot = 6u, inf = UINT64_MAX / 4u;
+    seg_row[0] = 0u;
+    if (rows == 0u) return 0;
+    uint64_t *prev = (uint64_t *) malloc(((size_t) rows + 1u) * sizeof(uint64_t));
+    uint64_t *curr = (uint64_t *) malloc(((size_t) rows + 1u) * sizeof(uint64_t));
+    uint32_t *cuts = (uint32_t *) calloc(((size_t) K + 1u) * ((size_t) rows + 1u), sizeof(uint32_t));
+    cso_line *hull = (cso_line *) malloc(((size_t) rows + 1u) * sizeof(cso_line));
+    uint32_t *raw_off = (uint32_t *) malloc(((size_t) K + 1u) * sizeof(uint32_t));
+    uint32_t *raw_w = (uint32_t *) malloc(((size_t) K + 1u) * sizeof(uint32_t));
+    int out = -1;
+    if (!prev || !curr || !cuts || !hull || !raw_off || !raw_w) goto done;
+    for (uint32_t i = 0; i <= rows; ++i) prev[i] = inf;
+    prev[0] = 0u;
+    for (uint32_t k = 1; k <= K; ++k) {
+        size_t n = 0u, head = 0u;
+        for (uint32_t i = 0; i <= rows; ++i) curr[i] = inf;
+        if (prev[k - 1u] != inf) {
+            hull[n].slope = -(int64_t) slot * (int64_t) (k - 1u);
+            hull[n].intercept = (int64_t) prev[k - 1u];
+            hull[n].cut = k - 1u;
+            ++n;
+        }
+        for (uint32_t r = k; r <= rows; ++r) {
+            const uint32_t w = sorted_widths[r - 1u];
+            while (head + 1u < n && line_at(&hull[head + 1u], w) < line_at(&hull[head], w)) ++head;
+            if (head < n) {
+                curr[r] = fixed + slot * (uint64_t) w * (uint64_t) r + (uint64_t) line_at(&hull[head], w);
+                cuts[(size_t) k * (rows + 1u) + r] = hull[head].cut;
+            }
+            if (prev[r] != inf) {
+                const cso_line l = {-(int64_t) slot * (int64_t) r, (int64_t) prev[r], r};
+                while (n >= head + 2u && line_redundant(&hull[n - 2u], &hull[n - 1u], &l)) --n;
+                hull[n++] = l;
+            }
+        }
+        uint64_t *t = prev;
+        prev = curr;
+        curr = t;
+    }
+    if (prev[rows] == inf) goto done;
+    {
+        uint32_t r = rows;
+        raw_off[K] = rows;
+        for (uint32_t k = K; k != 0u; --k) {
+            const uint32_t begin = cuts[(size_t) k * (rows + 1u) + r];
+            raw_off[k - 1u] = begin;
+            raw_w[k - 1u] = sorted_widths[r - 1u];
+            r = begin;
+        }
+        uint32_t S = 0u;
+        for (uint32_t k = 0; k < K; ++k) {
+            if (S != 0u && seg_w[S - 1u] == raw_w[k]) {
+                seg_row[S] = raw_off[k + 1u];
+            } else {
+                seg_w[S] = raw_w[k];
+                seg_row[S + 1u] = raw_off[k + 1u];
+                ++S;
+            }
+        }
+        out = (int) S;
+    }
+done:
+    free(prev);
+    free(curr);
+    free(cuts);
+    free(hull);
+    free(raw_off);
+    free(raw_w);
+    return out;
+}
+
+/* order[rows], row_widths[rows] (canonical row index) and the DP split;
+ * *bytes = bucketed bytes after the fallback to one segment
+ * (build_bucketed_sliced_execution_partition:1547-1570).  Returns S or -1. */
+int cso_sell_exec_build_layout(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
+                               const uint32_t *col_idx, uint32_t requested, uint32_t *order, uint32_t *row_widths,
+                               uint32_t *sorted_widths, uint32_t *seg_row, uint32_t *seg_w, uint64_t *bytes) {
+    uint64_t total = 0u;
+    for (uint32_t s = 0; s < S_src; ++s) total += (uint64_t) (offsets[s + 1u] - offsets[s]) * widths[s];
+    for (uint32_t r = 0; r < rows; ++r) {
+        const uint32_t s = sell_find_slice(rows, S_src, offsets, r);
+        uint32_t n = 0u;
+        if (s < S_src) {
+            uint64_t base = 0u;
+            for (uint32_t t = 0; t < s; ++t) base += (uint64_t) (offsets[t + 1u] - offsets[t]) * widths[t];
+            base += (uint64_t) (r - offsets[s]) * widths[s];
+            for (uint32_t k = 0; k < widths[s]; ++k) n += col_idx[base + k] != CSO_INVALID;
+        }
+        order[r] = r;
+        row_widths[r] = n;
+    }
+    g_sort_keys = row_widths;
+    qsort(order, rows, sizeof(uint32_t), cmp_by_key_then_id);
+    for (uint32_t r = 0; r < rows; ++r) sorted_widths[r] = row_widths[order[r]];
+    int S = cso_sell_exec_dp(rows, sorted_widths, requested, seg_row, seg_w);
+    if (S < 0) return -1;
+    uint64_t cand = 0u;
+    for (int s = 0; s < S; ++s) {
+        const uint32_t n = seg_row[s + 1] - seg_row[s];
+        cand += cso_packed_sliced_ell_bytes(n != 0u ? 1u : 0u, (uint64_t) n * seg_w[s]);
+    }
+    const uint64_t orig = cso_packed_sliced_ell_bytes(S_src, total);
+    if (S > 1 && cand >= orig) {
+        S = cso_sell_exec_dp(rows, sorted_widths, 1u, seg_row, seg_w);
+        cand = orig;
+    }
+    if (bytes != NULL) *bytes = cand;
+    return S;
+}
+
+void cso_sell_exec_fill(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
+                        const uint32_t *col_idx, const uint16_t *val, const uint32_t *order, uint32_t S,
+                        const uint32_t *seg_row, const uint32_t *seg_w, uint32_t *seg_col, uint16_t *seg_val,
+                        uint32_t *exec_to_canonical, uint32_t *canonical_to_exec) {
+    size_t off = 0u;
+    for (uint32_t s = 0; s < S; ++s) {
+        const uint32_t w = seg_w[s];
+        for (uint32_t p = seg_row[s]; p < seg_row[s + 1u]; ++p) {
+            const uint32_t row = order[p], src = sell_find_slice(rows, S_src, offsets, row);
+            uint32_t *dc = seg_col + off + (size_t) (p - seg_row[s]) * w;
+            uint16_t *dv = seg_val + off + (size_t) (p - seg_row[s]) * w;
+            for (uint32_t k = 0; k < w; ++k) {
+                dc[k] = CSO_INVALID;
+                dv[k] = 0u;
+            }
+            if (src < S_src) {
+                uint64_t base = 0u;
+                for (uint32_t t = 0; t < src; ++t) base += (uint64_t) (offsets[t + 1u] - offsets[t]) * widths[t];
+                base += (uint64_t) (row - offsets[src]) * widths[src];
+                uint32_t d = 0u;
+                for (uint32_t k = 0; k < widths[src]; ++k) {
+                    if (col_idx[base + k] == CSO_INVALID) continue;
+                    dc[d] = col_idx[base + k];
+                    dv[d] = val[base + k];
+                    ++d;
+                }
+            }
+            exec_to_canonical[p] = row;
+            canonical_to_exec[row] = p;
+        }
+        off += (size_t) (seg_row[s + 1u] - seg_row[s]) * w;
+    }
+}
+
+int cso_sell_choose_bucket_count(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
+                                 const uint32_t *col_idx, uint32_t *count, uint64_t *bytes) {
+    const uint32_t top = rows < 8u ? (rows < 1u ? 1u : rows) : 8u;
+    uint32_t *buf = (uint32_t *) malloc(((size_t) rows + 1u) * 3u * sizeof(uint32_t));
+    uint32_t seg_row[9], seg_w[8];
+    uint32_t best = 1u;
+    uint64_t best_bytes = UINT64_MAX;
+    if (buf == NULL) return 0;
+    for (uint32_t b = 1; b <= top; ++b) {
+        uint64_t x = 0u;
+        if (cso_sell_exec_build_layout(rows, S_src, offsets, widths, col_idx, b, buf, buf + rows + 1u,
+                                       buf + 2u * ((size_t) rows + 1u), seg_row, seg_w, &x) < 0) {
+            free(buf);
+            return 0;
+        }
+        if (x < best_bytes) {
+            best_bytes = x;
+            best = b;
+        }
+    }
+    free(buf);
+    *count = best;
+    *bytes = best_bytes;
+    return 1;
+}

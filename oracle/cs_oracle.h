@@ -98,6 +98,40 @@ void cso_pow2_bins(const uint32_t *sorted, uint32_t n, uint32_t *bins /* 34 */);
 void cso_rebuild(const uint32_t *ptr, const uint32_t *idx, const uint16_t *val, uint32_t n, const uint32_t *order,
                  uint32_t *dst_ptr, uint32_t *dst_idx, uint16_t *dst_val, uint32_t *inverse);
 
+/* ---- execution bucketing (src/io/csh5/execution_builders_part.hh:1018-1596) ---- */
+/* packed_blocked_ell_bytes (io/pack/packfile.cuh:110-116), fp16 values. */
+uint64_t cso_packed_blocked_ell_bytes(uint32_t rows, uint32_t ell_cols, uint32_t B);
+/* packed_sliced_ell_bytes (src/io/pack/packfile.cu:179-188), fp16 values. */
+uint64_t cso_packed_sliced_ell_bytes(uint32_t slice_count, uint64_t total_slots);
+/* Blocked-ELL: order[RB], widths[RB]; seg_rb[S+1], seg_w[S] with room for
+ * min(requested, RB) segments.  Returns S (build_execution_bucket_layout). */
+uint32_t cso_bell_exec_layout(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t requested,
+                              uint32_t *order, uint32_t *widths, uint32_t *seg_rb, uint32_t *seg_w);
+/* The layout build_bucketed_execution_partition keeps, and its byte count. */
+uint32_t cso_bell_exec_build_layout(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t requested,
+                                    uint32_t *order, uint32_t *widths, uint32_t *seg_rb, uint32_t *seg_w,
+                                    uint64_t *bytes);
+/* Segments packed back to back: seg_bci [sum RB_s * w_s], seg_val [sum rows_s * w_s * B]. */
+void cso_bell_exec_fill(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, const uint16_t *val,
+                        const uint32_t *order, uint32_t S, const uint32_t *seg_rb, const uint32_t *seg_w,
+                        uint32_t *seg_bci, uint16_t *seg_val, uint32_t *exec_to_canonical,
+                        uint32_t *canonical_to_exec);
+int cso_bell_choose_bucket_count(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t *count,
+                                 uint64_t *bytes);
+/* Sliced-ELL: the split of ascending widths into <= requested segments. */
+int cso_sell_exec_dp(uint32_t rows, const uint32_t *sorted_widths, uint32_t requested, uint32_t *seg_row,
+                     uint32_t *seg_w);
+int cso_sell_exec_build_layout(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
+                               const uint32_t *col_idx, uint32_t requested, uint32_t *order, uint32_t *row_widths,
+                               uint32_t *sorted_widths, uint32_t *seg_row, uint32_t *seg_w, uint64_t *bytes);
+/* Segments packed back to back: seg_col / seg_val [sum rows_s * w_s]. */
+void cso_sell_exec_fill(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
+                        const uint32_t *col_idx, const uint16_t *val, const uint32_t *order, uint32_t S,
+                        const uint32_t *seg_row, const uint32_t *seg_w, uint32_t *seg_col, uint16_t *seg_val,
+                        uint32_t *exec_to_canonical, uint32_t *canonical_to_exec);
+int cso_sell_choose_bucket_count(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
+                                 const uint32_t *col_idx, uint32_t *count, uint64_t *bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,5 +1,6 @@
 """TEST ORACLE ONLY: numpy wrappers over the C restatement (_build/libcs_oracle.so)
-and the reference bridges (_ref/libcs_ref.so, _ref/libcs_ref_gpu.so).
+and the reference bridges (_ref/libcs_ref.so, _ref/libcs_ref_gpu.so,
+_ref/libcs_ref_bucket.so).
 """
 
 from __future__ import annotations
@@ -266,6 +267,86 @@ def rebuild(ptr, idx, val, n, order):
     return dptr, didx[:nnz], dval[:nnz], inv[:n]
 
 
+
+# ---------------------------------------------------------------------------
+# execution bucketing (src/io/csh5/execution_builders_part.hh:1011-1596)
+# ---------------------------------------------------------------------------
+def _seg_room(units, requested):
+    return max(1, min(max(requested, 8), max(units, 1)))
+
+
+def bell_bucketed(rows, B, ell_cols, bci, val, requested):
+    """build_bucketed_execution_partition restated: the kept layout, its bytes
+    and the segments' contents packed back to back."""
+    o = lib()
+    W = ell_cols // B if B else 0
+    RB = (rows + B - 1) // B if B else 0
+    room = _seg_room(RB, requested)
+    order, widths = np.zeros(max(RB, 1), np.uint32), np.zeros(max(RB, 1), np.uint32)
+    seg_rb, seg_w = np.zeros(room + 1, np.uint32), np.zeros(room, np.uint32)
+    nbytes = C.c_uint64()
+    o.cso_bell_exec_build_layout.restype = u32
+    S = o.cso_bell_exec_build_layout(u32(rows), u32(B), u32(W), _p(np.ascontiguousarray(bci, np.uint32)),
+                                     u32(requested), _p(order), _p(widths), _p(seg_rb), _p(seg_w), C.byref(nbytes))
+    seg_rows = []
+    for s in range(S):
+        n = sum(min(B, rows - int(rb) * B) for rb in order[seg_rb[s]:seg_rb[s + 1]])
+        seg_rows.append(n)
+    n_idx = sum(int(seg_rb[s + 1] - seg_rb[s]) * int(seg_w[s]) for s in range(S))
+    n_val = sum(seg_rows[s] * int(seg_w[s]) * B for s in range(S))
+    seg_bci, seg_val = np.zeros(max(n_idx, 1), np.uint32), np.zeros(max(n_val, 1), np.uint16)
+    e2c, c2e = np.zeros(max(rows, 1), np.uint32), np.zeros(max(rows, 1), np.uint32)
+    o.cso_bell_exec_fill.restype = None
+    o.cso_bell_exec_fill(u32(rows), u32(B), u32(W), _p(np.ascontiguousarray(bci, np.uint32)),
+                         _p(np.ascontiguousarray(val, np.uint16)), _p(order), u32(S), _p(seg_rb), _p(seg_w),
+                         _p(seg_bci), _p(seg_val), _p(e2c), _p(c2e))
+    return {"segment_count": S, "bytes": nbytes.value, "order": order[:RB], "widths": widths[:RB],
+            "seg_rb": seg_rb[:S + 1], "seg_w": seg_w[:S], "seg_rows": np.array(seg_rows, np.uint32),
+            "seg_bci": seg_bci[:n_idx], "seg_val": seg_val[:n_val], "e2c": e2c[:rows], "c2e": c2e[:rows]}
+
+
+def bell_choose_bucket_count(rows, B, ell_cols, bci):
+    count, nbytes = C.c_uint32(), C.c_uint64()
+    assert lib().cso_bell_choose_bucket_count(u32(rows), u32(B), u32(ell_cols // B if B else 0),
+                                              _p(np.ascontiguousarray(bci, np.uint32)), C.byref(count),
+                                              C.byref(nbytes)) == 1
+    return count.value, nbytes.value
+
+
+def _sell_args(offsets, widths, col_idx):
+    return (_p(np.ascontiguousarray(offsets, np.uint32)), _p(np.ascontiguousarray(widths, np.uint32)),
+            _p(np.ascontiguousarray(col_idx, np.uint32)))
+
+
+def sell_bucketed(rows, offsets, widths, col_idx, val, requested):
+    """build_bucketed_sliced_execution_partition restated."""
+    o = lib()
+    S_src = len(widths)
+    room = _seg_room(rows, requested)
+    order, rw, sw = (np.zeros(max(rows, 1), np.uint32) for _ in range(3))
+    seg_row, seg_w = np.zeros(room + 1, np.uint32), np.zeros(room, np.uint32)
+    nbytes = C.c_uint64()
+    S = o.cso_sell_exec_build_layout(u32(rows), u32(S_src), *_sell_args(offsets, widths, col_idx), u32(requested),
+                                     _p(order), _p(rw), _p(sw), _p(seg_row), _p(seg_w), C.byref(nbytes))
+    assert S >= 0
+    n = sum(int(seg_row[s + 1] - seg_row[s]) * int(seg_w[s]) for s in range(S))
+    seg_col, seg_val = np.zeros(max(n, 1), np.uint32), np.zeros(max(n, 1), np.uint16)
+    e2c, c2e = np.zeros(max(rows, 1), np.uint32), np.zeros(max(rows, 1), np.uint32)
+    o.cso_sell_exec_fill.restype = None
+    o.cso_sell_exec_fill(u32(rows), u32(S_src), *_sell_args(offsets, widths, col_idx),
+                         _p(np.ascontiguousarray(val, np.uint16)), _p(order), u32(S), _p(seg_row), _p(seg_w),
+                         _p(seg_col), _p(seg_val), _p(e2c), _p(c2e))
+    return {"segment_count": S, "bytes": nbytes.value, "order": order[:rows], "row_widths": rw[:rows],
+            "seg_row": seg_row[:S + 1], "seg_w": seg_w[:S], "seg_col": seg_col[:n], "seg_val": seg_val[:n],
+            "e2c": e2c[:rows], "c2e": c2e[:rows]}
+
+
+def sell_choose_bucket_count(rows, offsets, widths, col_idx):
+    count, nbytes = C.c_uint32(), C.c_uint64()
+    assert lib().cso_sell_choose_bucket_count(u32(rows), u32(len(widths)), *_sell_args(offsets, widths, col_idx),
+                                              C.byref(count), C.byref(nbytes)) == 1
+    return count.value, nbytes.value
+
 # ---------------------------------------------------------------------------
 # the reference's own code (compiled from its sources into _ref/)
 # ---------------------------------------------------------------------------
@@ -455,6 +536,142 @@ def ref_gpu() -> C.CDLL:
         g.csrefgpu_group_reduce_compressed_timed.argtypes = [vp, vp, u32, vp, vp, C.c_int, C.c_int, fp]
         _rg = g
     return _rg
+
+
+# ---------------------------------------------------------------------------
+# the reference's execution-bucketing builders (_ref/libcs_ref_bucket.so)
+# ---------------------------------------------------------------------------
+REF_BUCKET_LIB = HERE / "_ref" / "libcs_ref_bucket.so"
+
+
+class HostBucketedBell(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("segment_count", u32), ("segments", vp),
+                ("segment_row_offsets", vp), ("exec_to_canonical_rows", vp), ("canonical_to_exec_rows", vp),
+                ("exec_to_canonical_cols", vp), ("canonical_to_exec_cols", vp)]
+
+
+class HostBucketedSell(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("segment_count", u32), ("segments", vp),
+                ("segment_row_offsets", vp), ("exec_to_canonical_rows", vp), ("canonical_to_exec_rows", vp),
+                ("canonical_slice_count", u32), ("canonical_slice_row_offsets", vp),
+                ("canonical_slice_widths", vp)]
+
+
+_rb = None
+
+
+def ref_bucket_available() -> bool:
+    return REF_BUCKET_LIB.exists()
+
+
+def ref_bucket() -> C.CDLL:
+    global _rb
+    if _rb is None:
+        b = C.CDLL(str(REF_BUCKET_LIB))
+        b.csrefb_build_bucketed_blocked_ell.argtypes = [vp, u32, vp, vp]
+        b.csrefb_build_bucketed_sliced_ell.argtypes = [vp, u32, vp, vp]
+        b.csrefb_choose_bucket_count_for_part.argtypes = [vp, vp, vp]
+        b.csrefb_choose_bucket_count_for_sliced_part.argtypes = [vp, vp, vp]
+        for name in ("csrefb_clear_bucketed_blocked_ell", "csrefb_clear_bucketed_sliced_ell"):
+            getattr(b, name).argtypes = [vp]
+            getattr(b, name).restype = None
+        _rb = b
+    return _rb
+
+
+def _arr(p, n, t):
+    return np.ctypeslib.as_array(C.cast(p, C.POINTER(t)), (n,)).copy() if n and p else np.zeros(0, np.dtype(t))
+
+
+def read_bucketed_bell(out):
+    """Host bucketed Blocked-ELL struct -> dict (reference layout)."""
+    S, rows, cols = out.segment_count, out.rows, out.cols
+    segs = []
+    base = C.cast(out.segments, C.POINTER(HostBlockedEll)) if S else None
+    for s in range(S):
+        m = base[s]
+        B = m.block_size
+        rb = (m.rows + B - 1) // B if B else 0
+        w = m.ell_cols // B if B else 0
+        segs.append({"rows": m.rows, "cols": m.cols, "nnz": m.nnz, "block_size": B, "ell_cols": m.ell_cols,
+                     "bci": _arr(m.blockColIdx, rb * w, u32), "val": _arr(m.val, m.rows * m.ell_cols, C.c_uint16)})
+    return {"rows": rows, "cols": cols, "nnz": out.nnz, "segment_count": S, "segments": segs,
+            "segment_row_offsets": _arr(out.segment_row_offsets, S + 1, u32),
+            "e2c": _arr(out.exec_to_canonical_rows, rows, u32), "c2e": _arr(out.canonical_to_exec_rows, rows, u32),
+            "e2c_cols": _arr(out.exec_to_canonical_cols, cols, u32),
+            "c2e_cols": _arr(out.canonical_to_exec_cols, cols, u32)}
+
+
+def read_bucketed_sell(out):
+    S, rows = out.segment_count, out.rows
+    segs = []
+    base = C.cast(out.segments, C.POINTER(HostSlicedEll)) if S else None
+    for s in range(S):
+        m = base[s]
+        offs = _arr(m.slice_row_offsets, m.slice_count + 1, u32) if m.slice_count else np.zeros(1, np.uint32)
+        widths = _arr(m.slice_widths, m.slice_count, u32)
+        total = int(sum(int(offs[i + 1] - offs[i]) * int(widths[i]) for i in range(m.slice_count)))
+        segs.append({"rows": m.rows, "cols": m.cols, "nnz": m.nnz, "slice_count": m.slice_count,
+                     "offsets": offs, "widths": widths, "col_idx": _arr(m.col_idx, total, u32),
+                     "val": _arr(m.val, total, C.c_uint16)})
+    cs = out.canonical_slice_count
+    return {"rows": rows, "cols": out.cols, "nnz": out.nnz, "segment_count": S, "segments": segs,
+            "segment_row_offsets": _arr(out.segment_row_offsets, S + 1, u32),
+            "e2c": _arr(out.exec_to_canonical_rows, rows, u32), "c2e": _arr(out.canonical_to_exec_rows, rows, u32),
+            "canonical_slice_count": cs, "canonical_slice_row_offsets": _arr(out.canonical_slice_row_offsets,
+                                                                             cs + 1, u32),
+            "canonical_slice_widths": _arr(out.canonical_slice_widths, cs, u32)}
+
+
+def host_sell(rows, cols, nnz, offsets, widths, col_idx, val):
+    h = HostSlicedEll()
+    h.rows, h.cols, h.nnz, h.slice_count = rows, cols, nnz, len(widths)
+    h.slice_row_offsets, h.slice_widths, h.col_idx, h.val = _p(offsets), _p(widths), _p(col_idx), _p(val)
+    return h
+
+
+def ref_build_bucketed_bell(rows, cols, nnz, B, ell_cols, bci, val, requested):
+    """build_bucketed_blocked_ell_partition of the reference, on the host."""
+    bci, val = np.ascontiguousarray(bci, np.uint32), np.ascontiguousarray(val, np.uint16)
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    out, nbytes = HostBucketedBell(), C.c_uint64()
+    ok = ref_bucket().csrefb_build_bucketed_blocked_ell(C.byref(src), requested, C.byref(out), C.byref(nbytes))
+    res = read_bucketed_bell(out) if ok == 1 else None
+    ref_bucket().csrefb_clear_bucketed_blocked_ell(C.byref(out))
+    if res is not None:
+        res["bytes"] = nbytes.value
+    return res
+
+
+def ref_choose_bucket_count_for_part(rows, cols, nnz, B, ell_cols, bci, val):
+    bci, val = np.ascontiguousarray(bci, np.uint32), np.ascontiguousarray(val, np.uint16)
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    count, nbytes = C.c_uint32(), C.c_uint64()
+    assert ref_bucket().csrefb_choose_bucket_count_for_part(C.byref(src), C.byref(count), C.byref(nbytes)) == 1
+    return count.value, nbytes.value
+
+
+def ref_build_bucketed_sell(rows, cols, nnz, offsets, widths, col_idx, val, requested):
+    arrs = [np.ascontiguousarray(a, np.uint32) for a in (offsets, widths, col_idx)]
+    val = np.ascontiguousarray(val, np.uint16)
+    src = host_sell(rows, cols, nnz, *arrs, val)
+    out, nbytes = HostBucketedSell(), C.c_uint64()
+    ok = ref_bucket().csrefb_build_bucketed_sliced_ell(C.byref(src), requested, C.byref(out), C.byref(nbytes))
+    res = read_bucketed_sell(out) if ok == 1 else None
+    ref_bucket().csrefb_clear_bucketed_sliced_ell(C.byref(out))
+    if res is not None:
+        res["bytes"] = nbytes.value
+    return res
+
+
+def ref_choose_bucket_count_for_sliced_part(rows, cols, nnz, offsets, widths, col_idx, val):
+    arrs = [np.ascontiguousarray(a, np.uint32) for a in (offsets, widths, col_idx)]
+    val = np.ascontiguousarray(val, np.uint16)
+    src = host_sell(rows, cols, nnz, *arrs, val)
+    count, nbytes = C.c_uint32(), C.c_uint64()
+    assert ref_bucket().csrefb_choose_bucket_count_for_sliced_part(C.byref(src), C.byref(count),
+                                                                   C.byref(nbytes)) == 1
+    return count.value, nbytes.value
 
 
 def cpu_count() -> int:

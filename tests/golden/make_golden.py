@@ -13,6 +13,12 @@
    compiled from the reference sources into oracle/_ref/libcs_ref.so by
    oracle/Makefile, on seeded small CSR inputs.  Needs the reference tree
    (only here, not on the GPU machine).
+3. ref_bucketing.npz -- outputs of the reference's execution-bucketing
+   builders (build_bucketed_execution_partition, choose_bucket_count_for_part,
+   build_bucketed_sliced_execution_partition,
+   choose_bucket_count_for_sliced_part, src/io/csh5/execution_builders_part.hh)
+   compiled into oracle/_ref/libcs_ref_bucket.so, on the Blocked-ELL and
+   Sliced-ELL matrices of the conversion cases.
 """
 
 from __future__ import annotations
@@ -160,14 +166,69 @@ def ref_conversions() -> dict:
     return out
 
 
+BUCKET_BLOCKS = [4, 16]
+BUCKET_SLICES = [3, 32]
+BUCKET_REQUESTS = [1, 2, 3, 8]
+
+
+def ref_bucketing(conv: dict) -> dict:
+    """The reference's bucketed partitions of the conversion cases' own Blocked-ELL
+    and Sliced-ELL matrices (taken from `conv`)."""
+    from oracle import oracle
+
+    out = {}
+    names = sorted({k.split("/")[0] for k in conv})
+    for name in names:
+        rows, cols = (int(x) for x in conv[f"{name}/shape"])
+        for B in BUCKET_BLOCKS:
+            key = f"{name}/bell{B}"
+            bci, bval = conv[f"{key}/bci"], conv[f"{key}/val"]
+            ell_cols, bnnz = (int(x) for x in conv[f"{key}/meta"])
+            for req in BUCKET_REQUESTS:
+                r = oracle.ref_build_bucketed_bell(rows, cols, bnnz, B, ell_cols, bci, bval, req)
+                k2 = f"{key}/bucket{req}"
+                segs = r["segments"]
+                out[f"{k2}/meta"] = np.array([r["segment_count"], r["bytes"]], np.uint64)
+                out[f"{k2}/seg"] = np.array([[g["rows"], g["ell_cols"], g["nnz"]] for g in segs], np.uint32)
+                out[f"{k2}/bci"] = np.concatenate([g["bci"] for g in segs] + [np.zeros(0, np.uint32)])
+                out[f"{k2}/val"] = np.concatenate([g["val"] for g in segs] + [np.zeros(0, np.uint16)])
+                out[f"{k2}/e2c"] = r["e2c"]
+            out[f"{key}/choose"] = np.array(oracle.ref_choose_bucket_count_for_part(rows, cols, bnnz, B, ell_cols,
+                                                                                   bci, bval), np.uint64)
+        for h in BUCKET_SLICES:
+            key = f"{name}/sell{h}"
+            if f"{key}/widths" not in conv:
+                continue
+            offs, widths, col, val = (conv[f"{key}/{f}"] for f in ("offsets", "widths", "col_idx", "val"))
+            nnz = int(conv[f"{key}/meta"][1])
+            for req in BUCKET_REQUESTS:
+                r = oracle.ref_build_bucketed_sell(rows, cols, nnz, offs, widths, col, val, req)
+                k2 = f"{key}/bucket{req}"
+                segs = r["segments"]
+                out[f"{k2}/meta"] = np.array([r["segment_count"], r["bytes"]], np.uint64)
+                out[f"{k2}/seg"] = np.array([[g["rows"], int(g["widths"][0]) if g["slice_count"] else 0, g["nnz"]]
+                                             for g in segs], np.uint32)
+                out[f"{k2}/col_idx"] = np.concatenate([g["col_idx"] for g in segs] + [np.zeros(0, np.uint32)])
+                out[f"{k2}/val"] = np.concatenate([g["val"] for g in segs] + [np.zeros(0, np.uint16)])
+                out[f"{k2}/e2c"] = r["e2c"]
+            out[f"{key}/choose"] = np.array(oracle.ref_choose_bucket_count_for_sliced_part(rows, cols, nnz, offs,
+                                                                                          widths, col, val), np.uint64)
+    return out
+
+
 def main() -> None:
     (HERE / "mask_groups_known_answers.json").write_text(json.dumps(known_answers(), indent=1) + "\n")
     from oracle import oracle
 
     if not oracle.ref_available():
         raise SystemExit("oracle/_ref/libcs_ref.so missing: run `make -C oracle ref` with the reference tree present")
-    np.savez_compressed(HERE / "ref_conversions.npz", **ref_conversions())
-    print("wrote", HERE / "mask_groups_known_answers.json", HERE / "ref_conversions.npz")
+    conv = ref_conversions()
+    np.savez_compressed(HERE / "ref_conversions.npz", **conv)
+    if not oracle.ref_bucket_available():
+        raise SystemExit("oracle/_ref/libcs_ref_bucket.so missing: run `make -C oracle ref`")
+    np.savez_compressed(HERE / "ref_bucketing.npz", **ref_bucketing(conv))
+    print("wrote", HERE / "mask_groups_known_answers.json", HERE / "ref_conversions.npz",
+          HERE / "ref_bucketing.npz")
 
 
 if __name__ == "__main__":

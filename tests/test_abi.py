@@ -53,6 +53,9 @@ int main(void) {
   S(cs_batch_tiles) S(cs_batch_sliced_result) O(cs_batch_sliced_result, view)
   S(cs_serve_config) S(cs_serve_request) O(cs_serve_request, group_rows) S(cs_serve_stats)
   S(cs_partition_record) O(cs_partition_record, host_view)
+  S(cs_host_bucketed_blocked_ell) O(cs_host_bucketed_blocked_ell, canonical_to_exec_cols)
+  S(cs_host_bucketed_sliced_ell) O(cs_host_bucketed_sliced_ell, canonical_slice_widths)
+  S(cs_exec_bucket_plan) O(cs_exec_bucket_plan, value_entries) S(cs_exec_bucket_segments)
   return 0;
 }
 """
@@ -78,6 +81,10 @@ PAIRS = {
     "cs_serve_request": _abi.ServeRequest,
     "cs_serve_stats": _abi.ServeStats,
     "cs_partition_record": _abi.PartitionRecord,
+    "cs_host_bucketed_blocked_ell": _abi.HostBucketedBlockedEll,
+    "cs_host_bucketed_sliced_ell": _abi.HostBucketedSlicedEll,
+    "cs_exec_bucket_plan": _abi.ExecBucketPlan,
+    "cs_exec_bucket_segments": _abi.ExecBucketSegments,
 }
 
 
@@ -98,6 +105,11 @@ def test_ctypes_layouts_match_c(tmp_path):
     assert got["cs_host_sliced_ell.val"] == _abi.HostSlicedEll.val.offset
     assert got["cs_batch_part.d_major_nnz"] == _abi.BatchPart.d_major_nnz.offset
     assert got["cs_batch_part.d_pow2_offsets"] == _abi.BatchPart.d_pow2_offsets.offset
+    assert got["cs_host_bucketed_blocked_ell.canonical_to_exec_cols"] == \
+        _abi.HostBucketedBlockedEll.canonical_to_exec_cols.offset
+    assert got["cs_host_bucketed_sliced_ell.canonical_slice_widths"] == \
+        _abi.HostBucketedSlicedEll.canonical_slice_widths.offset
+    assert got["cs_exec_bucket_plan.value_entries"] == _abi.ExecBucketPlan.value_entries.offset
     assert got["cs_batch_sliced_result.view"] == _abi.BatchSlicedResult.view.offset
     assert got["cs_serve_request.group_rows"] == _abi.ServeRequest.group_rows.offset
     assert got["cs_partition_record.host_view"] == _abi.PartitionRecord.host_view.offset
