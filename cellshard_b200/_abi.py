@@ -204,6 +204,10 @@ PROTOTYPES: dict[str, tuple] = {
                                                                P(u64)]),
     "cs_b200_choose_bucket_count_for_sliced_part": (C.c_int, [P(HostSlicedEll), P(u32), P(u64)]),
     "cs_b200_host_bucketed_sliced_ell_clear": (None, [P(HostBucketedSlicedEll)]),
+    "cs_b200_blocked_ell_bucket_plan_scratch_bytes": (C.c_int, [u32, u32, P(sz)]),
+    "cs_b200_blocked_ell_bucket_plan": (C.c_int, [P(BlockedEllView), vp, vp, vp, sz, vp]),
+    "cs_b200_choose_bucket_count_from_plan": (C.c_int, [P(BlockedEllView), vp, vp, vp, vp, vp]),
+    "cs_b200_choose_ingest_bucket_count_for_part": (C.c_int, [P(HostBlockedEll), C.c_int, P(u32)]),
     "cs_b200_compressed_transpose_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
     "cs_b200_build_compressed_transpose": (C.c_int, [u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "cs_b200_major_nnz_bucket_sort_scratch_bytes": (C.c_int, [u32, P(sz)]),

@@ -411,8 +411,15 @@ __global__ void __launch_bounds__(kFillThreads) bell_exec_fill_kernel(
     }
 }
 
-int bell_geometry(const cs_blocked_ell_view *part, bell_geom *g) {
-    if (!check_bell(part, "bucketed_blocked_ell")) return 0;
+int bell_geometry(const cs_blocked_ell_view *part, bell_geom *g, bool need_values = true) {
+    if (need_values) {
+        if (!check_bell(part, "bucketed_blocked_ell")) return 0;
+    } else if (part == nullptr || (part->rows != 0u && part->ell_cols != 0u &&
+                                   (part->block_size == 0u || part->ell_cols % part->block_size != 0u ||
+                                    part->blockColIdx == nullptr))) {
+        set_error("blocked_ell_bucket_plan: block size must divide ell_cols and the block columns be set");
+        return 0;
+    }
     if (part->rows != 0u && part->block_size == 0u) {
         set_error("bucketed_blocked_ell: zero block size");
         return 0;
@@ -850,6 +857,137 @@ int sell_fill(const cs_sliced_ell_view *part, const void *scratch, const cs_exec
     return launch_ok("sell_exec_fill_kernel");
 }
 
+// ---------------------------------------------------------------------------
+// Ingest-time bucket-count choice
+// ---------------------------------------------------------------------------
+// Row-block key of bucket::build_plan (blocked_ell_bucket.cuh:78-95): the
+// valid width, and a hash folded over the valid block columns in slot order
+// (h ^= c + 0x9e3779b9 + (h << 6) + (h >> 2); h *= 16777619; from 2166136261).
+// One warp per row block: the columns of each 32-slot step are broadcast by
+// shuffle and every lane folds the same chain.
+__global__ void __launch_bounds__(256) bell_rb_key_kernel(const cs_blocked_ell_view src, uint32_t RB,
+                                                          uint32_t *__restrict__ widths,
+                                                          uint32_t *__restrict__ hashes) {
+    const uint32_t lane = threadIdx.x & 31u, W = src.ell_cols / src.block_size;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rb < RB; rb += warps) {
+        const uint32_t *row = src.blockColIdx + (std::size_t) rb * W;
+        uint32_t n = 0u, h = 2166136261u;
+        for (uint32_t k0 = 0; k0 < W; k0 += 32u) {
+            const uint32_t k = k0 + lane;
+            const uint32_t c = k < W ? __ldg(row + k) : kInvalid;
+            unsigned m = __ballot_sync(0xffffffffu, c != kInvalid);
+            n += __popc(m);
+            while (m != 0u) {
+                const uint32_t x = __shfl_sync(0xffffffffu, c, __ffs(m) - 1);
+                m &= m - 1u;
+                h ^= x + 0x9e3779b9u + (h << 6) + (h >> 2);
+                h *= 16777619u;
+            }
+        }
+        if (lane == 0u) {
+            widths[rb] = n;
+            hashes[rb] = h;
+        }
+    }
+}
+
+__global__ void gather_u32_kernel(uint32_t n, const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx,
+                                  uint32_t *__restrict__ dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
+}
+
+// choose_bucket_count_for_part of the ingest path (convert_layout_support_part.hh:
+// 116-181): for 1..min(8, RB) buckets of equal row-block ranges over the plan
+// order, idx + values of width = the range's last sorted width, plus both row
+// maps and the offsets; a count must beat the source's packed bytes.
+__global__ void __launch_bounds__(256) ingest_choose_kernel(uint32_t rows, uint32_t B, uint32_t W, uint32_t RB,
+                                                            const uint32_t *__restrict__ order,
+                                                            const uint32_t *__restrict__ width_sorted,
+                                                            uint32_t *__restrict__ out_count,
+                                                            unsigned long long *__restrict__ out_bytes) {
+    __shared__ uint32_t partial_pos;
+    const uint32_t last_rows = RB == 0u ? 0u : rows - (RB - 1u) * B;
+    if (threadIdx.x == 0u) partial_pos = kInvalid;
+    __syncthreads();
+    if (RB > 1u && last_rows != B)
+        for (uint32_t p = threadIdx.x; p < RB; p += blockDim.x)
+            if (order[p] == RB - 1u) partial_pos = p;
+    __syncthreads();
+    if (threadIdx.x != 0u) return;
+    uint64_t best = packed_bell_bytes(rows, (uint64_t) W * B, B);
+    uint32_t best_b = 1u;
+    if (RB > 1u) {
+        const uint32_t top = RB < kChooseMax ? RB : kChooseMax;
+        for (uint32_t nb = 1; nb <= top; ++nb) {
+            uint64_t bytes = 0u;
+            for (uint32_t b = 0; b < nb; ++b) {
+                const uint32_t lo = (b * RB) / nb, hi = ((b + 1u) * RB) / nb;
+                if (hi <= lo) continue;
+                const uint32_t w = width_sorted[hi - 1u];
+                uint32_t seg_rows = (hi - lo) * B;
+                if (partial_pos >= lo && partial_pos < hi) seg_rows -= B - last_rows;
+                bytes += (uint64_t) (hi - lo) * w * 4u;
+                bytes += (uint64_t) seg_rows * w * B * 2u;
+            }
+            bytes += (uint64_t) rows * 8u + ((uint64_t) nb + 1u) * 4u;
+            if (bytes < best) {
+                best = bytes;
+                best_b = nb;
+            }
+        }
+    }
+    *out_count = best_b;
+    *out_bytes = best;
+}
+
+struct plan_scratch {
+    uint32_t *widths, *hashes, *order1, *hash_sorted, *w1;
+    void *sort_tmp;
+    std::size_t sort_bytes, bytes;
+};
+
+void carve_plan(void *base, uint32_t RB, plan_scratch *x) {
+    scratch_carver c(base, ~std::size_t(0));
+    x->widths = c.take<uint32_t>((std::size_t) RB + 1u);
+    x->hashes = c.take<uint32_t>((std::size_t) RB + 1u);
+    x->order1 = c.take<uint32_t>((std::size_t) RB + 1u);
+    x->hash_sorted = c.take<uint32_t>((std::size_t) RB + 1u);
+    x->w1 = c.take<uint32_t>((std::size_t) RB + 1u);
+    x->sort_bytes = sort_pairs_u32_scratch_bytes(RB);
+    x->sort_tmp = c.take<char>(x->sort_bytes);
+    x->bytes = c.used;
+}
+
+// bucket::build_plan: keys, then a stable sort by the 64-bit key as two
+// stable 32-bit passes (hash, then width), which orders equal keys by row
+// block as the reference's 64-bit radix sort does.
+int bucket_plan(const cs_blocked_ell_view *part, uint32_t *order, uint32_t *width_sorted, void *scratch,
+                std::size_t scratch_bytes, cudaStream_t stream) {
+    bell_geom g;
+    if (!bell_geometry(part, &g, false)) return 0;
+    plan_scratch x;
+    carve_plan(nullptr, g.RB, &x);
+    if (scratch == nullptr || scratch_bytes < x.bytes) {
+        set_error("blocked_ell_bucket_plan: scratch %zu < %zu bytes", scratch_bytes, x.bytes);
+        return 0;
+    }
+    if (g.RB == 0u) return 1;
+    if (order == nullptr || width_sorted == nullptr) {
+        set_error("blocked_ell_bucket_plan: null outputs");
+        return 0;
+    }
+    carve_plan(scratch, g.RB, &x);
+    bell_rb_key_kernel<<<resident_grid((const void *) bell_rb_key_kernel, 256, 0, ((std::size_t) g.RB + 7u) / 8u), 256,
+                         0, stream>>>(*part, g.RB, x.widths, x.hashes);
+    if (!launch_ok("bell_rb_key_kernel")) return 0;
+    if (!sort_pairs_u32(x.hashes, nullptr, g.RB, x.hash_sorted, x.order1, x.sort_tmp, x.sort_bytes, stream)) return 0;
+    gather_u32_kernel<<<resident_grid((const void *) gather_u32_kernel, 256, 0, ((std::size_t) g.RB + 255u) / 256u), 256,
+                        0, stream>>>(g.RB, x.widths, x.order1, x.w1);
+    if (!launch_ok("gather_u32_kernel")) return 0;
+    return sort_pairs_u32(x.w1, x.order1, g.RB, width_sorted, order, x.sort_tmp, x.sort_bytes, stream);
+}
+
 std::size_t scratch_for(uint32_t units, uint32_t max_segments) {
     exec_scratch x;
     const uint32_t b = max_segments > kChooseMax ? max_segments : kChooseMax;
@@ -912,6 +1050,77 @@ extern "C" int cs_b200_bucketed_sliced_ell_fill(const cs_sliced_ell_view *part, 
                                                 uint32_t *d_canonical_to_exec_rows, cs_stream_t s) {
     return sell_fill(part, d_scratch, plan, d_seg_col_idx, d_seg_val, d_exec_to_canonical_rows,
                      d_canonical_to_exec_rows, as_stream(s));
+}
+
+extern "C" int cs_b200_blocked_ell_bucket_plan_scratch_bytes(uint32_t rows, uint32_t block_size, size_t *out_bytes) {
+    if (out_bytes == nullptr || (rows != 0u && block_size == 0u)) {
+        set_error("blocked_ell_bucket_plan_scratch_bytes: null output or zero block size");
+        return 0;
+    }
+    plan_scratch x;
+    carve_plan(nullptr, rows == 0u ? 0u : (uint32_t) (((uint64_t) rows + block_size - 1u) / block_size), &x);
+    *out_bytes = x.bytes;
+    return 1;
+}
+
+extern "C" int cs_b200_blocked_ell_bucket_plan(const cs_blocked_ell_view *part, uint32_t *d_row_block_order,
+                                               uint32_t *d_row_block_width_sorted, void *d_scratch,
+                                               size_t scratch_bytes, cs_stream_t s) {
+    return bucket_plan(part, d_row_block_order, d_row_block_width_sorted, d_scratch, scratch_bytes, as_stream(s));
+}
+
+extern "C" int cs_b200_choose_bucket_count_from_plan(const cs_blocked_ell_view *part,
+                                                     const uint32_t *d_row_block_order,
+                                                     const uint32_t *d_row_block_width_sorted,
+                                                     uint32_t *d_bucket_count, uint64_t *d_estimated_bytes,
+                                                     cs_stream_t s) {
+    bell_geom g;
+    if (!bell_geometry(part, &g, false)) return 0;
+    if (d_bucket_count == nullptr || d_estimated_bytes == nullptr ||
+        (g.RB > 1u && (d_row_block_order == nullptr || d_row_block_width_sorted == nullptr))) {
+        set_error("choose_bucket_count_from_plan: null argument");
+        return 0;
+    }
+    ingest_choose_kernel<<<1, 256, 0, as_stream(s)>>>(g.rows, g.B, g.W, g.RB, d_row_block_order,
+                                                     d_row_block_width_sorted, d_bucket_count,
+                                                     (unsigned long long *) d_estimated_bytes);
+    return launch_ok("ingest_choose_kernel");
+}
+
+extern "C" int cs_b200_choose_ingest_bucket_count_for_part(const cs_host_blocked_ell *part, int device,
+                                                           uint32_t *bucket_count_out) {
+    if (part == nullptr || bucket_count_out == nullptr || (part->rows != 0u && part->block_size == 0u)) {
+        set_error("choose_ingest_bucket_count_for_part: null argument or zero block size");
+        return 0;
+    }
+    const uint32_t B = part->block_size;
+    const uint32_t RB = part->rows == 0u ? 0u : (uint32_t) (((uint64_t) part->rows + B - 1u) / B);
+    if (RB <= 1u) {
+        *bucket_count_out = 1u;
+        return 1;
+    }
+    if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return 0;
+    own_stream g;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&g.s, cudaStreamNonBlocking), "stream create")) return 0;
+    // the plan reads the block column indices only (the reference uploads just those)
+    const std::size_t idx_bytes = (std::size_t) RB * (part->ell_cols / B) * 4u;
+    plan_scratch x;
+    carve_plan(nullptr, RB, &x);
+    dmem bci, scratch, out;
+    if (!bci.alloc(idx_bytes, "bucket plan idx") || !scratch.alloc(x.bytes, "bucket plan scratch") ||
+        !out.alloc(((std::size_t) RB * 2u + 4u) * 4u, "bucket plan out"))
+        return 0;
+    if (idx_bytes != 0u &&
+        !cuda_ok(cudaMemcpyAsync(bci.p, part->blockColIdx, idx_bytes, cudaMemcpyHostToDevice, g.s), "H2D idx"))
+        return 0;
+    const cs_blocked_ell_view v{part->rows, part->cols, part->nnz, B, part->ell_cols, (uint32_t *) bci.p, nullptr};
+    uint32_t *order = (uint32_t *) out.p, *ws = order + RB, *res = ws + RB;
+    if (!bucket_plan(&v, order, ws, scratch.p, x.bytes, g.s)) return 0;
+    ingest_choose_kernel<<<1, 256, 0, g.s>>>(v.rows, B, v.ell_cols / B, RB, order, ws, res,
+                                            (unsigned long long *) (res + 2));
+    if (!launch_ok("ingest_choose_kernel")) return 0;
+    return cuda_ok(cudaMemcpyAsync(bucket_count_out, res, 4, cudaMemcpyDeviceToHost, g.s), "D2H count") &&
+           cuda_ok(cudaStreamSynchronize(g.s), "sync choose");
 }
 
 // ---------------------------------------------------------------------------

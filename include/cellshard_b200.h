@@ -652,6 +652,33 @@ CS_API int cs_b200_bucketed_sliced_ell_fill(const cs_sliced_ell_view *part,
                                             uint32_t *d_canonical_to_exec_rows,
                                             cs_stream_t stream);
 
+/* The ingest-time choice (bucket::build_plan, src/bucket/operators/
+ * blocked_ell_bucket.cuh:149-210, and choose_bucket_count_for_part,
+ * include/CellShard/ingest/internal/dataset/internal/convert_layout_support_part.hh:
+ * 116-181): row blocks stably sorted by (valid width << 32 | hash of their
+ * valid block columns); for 1..min(8, row blocks) equal cuts, an estimate of
+ * index + value + row-map + offset bytes; the count must beat the source's
+ * packed bytes (else 1).  Reads the block column indices only. */
+CS_API int cs_b200_blocked_ell_bucket_plan_scratch_bytes(uint32_t rows, uint32_t block_size, size_t *out_bytes);
+CS_API int cs_b200_blocked_ell_bucket_plan(const cs_blocked_ell_view *part,
+                                           uint32_t *d_row_block_order,
+                                           uint32_t *d_row_block_width_sorted,
+                                           void *d_scratch,
+                                           size_t scratch_bytes,
+                                           cs_stream_t stream);
+/* d_bucket_count <- the count; d_estimated_bytes <- its estimate, or the
+ * source's packed bytes when no count beats them. */
+CS_API int cs_b200_choose_bucket_count_from_plan(const cs_blocked_ell_view *part,
+                                                 const uint32_t *d_row_block_order,
+                                                 const uint32_t *d_row_block_width_sorted,
+                                                 uint32_t *d_bucket_count,
+                                                 uint64_t *d_estimated_bytes,
+                                                 cs_stream_t stream);
+/* The ingest chooser's host signature (part in host memory, device ordinal). */
+CS_API int cs_b200_choose_ingest_bucket_count_for_part(const cs_host_blocked_ell *part,
+                                                       int device,
+                                                       uint32_t *bucket_count_out);
+
 /* The reference's host signatures: H2D, plan + fill on the device, D2H into
  * host structs packed as the reference allocates them (its clear() frees
  * them).  bucketed_bytes_out nullable. */

@@ -19,6 +19,10 @@
  *   src/convert/compressed_transpose_raw.cuh:14-123
  *   src/bucket/major_nnz_raw.cuh:12-320, src/bucket/operators/major_nnz.cuh:11-213
  *   include/CellShard/runtime/mask_groups.cuh:14-224
+ *   include/CellShard/io/csh5/api.cuh:316-436,726-733 (bucketed partitions),
+ *       src/io/csh5/execution_builders_part.hh:1249-1272,1572-1596,
+ *       src/bucket/operators/blocked_ell_bucket.cuh:11-210,
+ *       include/CellShard/ingest/internal/dataset/internal/convert_layout_support_part.hh:143-181
  * Not mirrored (out of this library's scope): the fleet (multi-GPU) entry
  * points, sharded<T> host containers and their shard-level staging, the COO
  * and DIA formats.
@@ -32,6 +36,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include "cellshard_b200.h"
 
@@ -1287,6 +1292,194 @@ inline int manual_reoptimize_masked_sparse(const device::blocked_ell_view *src, 
 }
 
 } // namespace runtime
+
+// ---------------------------------------------------------------------------
+// Execution bucketing of one partition (io/csh5/api.cuh:316-436,726-733)
+// ---------------------------------------------------------------------------
+struct bucketed_blocked_ell_partition {
+    types::u32 rows;
+    types::u32 cols;
+    types::u32 nnz;
+    types::u32 segment_count;
+    sparse::blocked_ell *segments;
+    types::u32 *segment_row_offsets;
+    types::u32 *exec_to_canonical_rows;
+    types::u32 *canonical_to_exec_rows;
+    types::u32 *exec_to_canonical_cols;
+    types::u32 *canonical_to_exec_cols;
+};
+
+struct bucketed_sliced_ell_partition {
+    types::u32 rows;
+    types::u32 cols;
+    types::u32 nnz;
+    types::u32 segment_count;
+    sparse::sliced_ell *segments;
+    types::u32 *segment_row_offsets;
+    types::u32 *exec_to_canonical_rows;
+    types::u32 *canonical_to_exec_rows;
+    types::u32 canonical_slice_count;
+    types::u32 *canonical_slice_row_offsets;
+    types::u32 *canonical_slice_widths;
+};
+
+static_assert(sizeof(bucketed_blocked_ell_partition) == sizeof(cs_host_bucketed_blocked_ell) &&
+                  offsetof(bucketed_blocked_ell_partition, canonical_to_exec_cols) ==
+                      offsetof(cs_host_bucketed_blocked_ell, canonical_to_exec_cols),
+              "bucketed_blocked_ell_partition layout");
+static_assert(sizeof(bucketed_sliced_ell_partition) == sizeof(cs_host_bucketed_sliced_ell) &&
+                  offsetof(bucketed_sliced_ell_partition, canonical_slice_widths) ==
+                      offsetof(cs_host_bucketed_sliced_ell, canonical_slice_widths),
+              "bucketed_sliced_ell_partition layout");
+
+inline void init(bucketed_blocked_ell_partition *p) { std::memset(p, 0, sizeof(*p)); }
+inline void init(bucketed_sliced_ell_partition *p) { std::memset(p, 0, sizeof(*p)); }
+inline void clear(bucketed_blocked_ell_partition *p) {
+    cs_b200_host_bucketed_blocked_ell_clear(reinterpret_cast<cs_host_bucketed_blocked_ell *>(p));
+}
+inline void clear(bucketed_sliced_ell_partition *p) {
+    cs_b200_host_bucketed_sliced_ell_clear(reinterpret_cast<cs_host_bucketed_sliced_ell *>(p));
+}
+
+inline int build_bucketed_blocked_ell_partition(bucketed_blocked_ell_partition *out, const sparse::blocked_ell *part,
+                                                std::uint32_t requested_bucket_count,
+                                                std::uint64_t *bucketed_bytes_out) {
+    return cs_b200_build_bucketed_blocked_ell_partition(reinterpret_cast<cs_host_bucketed_blocked_ell *>(out),
+                                                        reinterpret_cast<const cs_host_blocked_ell *>(part),
+                                                        requested_bucket_count, bucketed_bytes_out);
+}
+
+inline int build_bucketed_sliced_ell_partition(bucketed_sliced_ell_partition *out, const sparse::sliced_ell *part,
+                                               std::uint32_t requested_bucket_count,
+                                               std::uint64_t *bucketed_bytes_out) {
+    return cs_b200_build_bucketed_sliced_ell_partition(reinterpret_cast<cs_host_bucketed_sliced_ell *>(out),
+                                                       reinterpret_cast<const cs_host_sliced_ell *>(part),
+                                                       requested_bucket_count, bucketed_bytes_out);
+}
+
+inline int choose_bucket_count_for_part(const sparse::blocked_ell *part, std::uint32_t *bucket_count_out,
+                                        std::uint64_t *bucketed_bytes_out) {
+    return cs_b200_choose_bucket_count_for_part(reinterpret_cast<const cs_host_blocked_ell *>(part), bucket_count_out,
+                                                bucketed_bytes_out);
+}
+
+inline int choose_bucket_count_for_sliced_part(const sparse::sliced_ell *part, std::uint32_t *bucket_count_out,
+                                               std::uint64_t *bucketed_bytes_out) {
+    return cs_b200_choose_bucket_count_for_sliced_part(reinterpret_cast<const cs_host_sliced_ell *>(part),
+                                                       bucket_count_out, bucketed_bytes_out);
+}
+
+namespace bucket {
+
+// blocked_ell_bucket.cuh:11-29: the plan comes back to the host, the
+// workspace owns a stream and grows its device buffers.
+struct blocked_ell_bucket_plan {
+    std::vector<std::uint32_t> row_block_order;
+    std::vector<std::uint32_t> row_block_width_sorted;
+};
+
+struct blocked_ell_bucket_workspace {
+    int device;
+    cudaStream_t stream;
+    std::uint32_t row_block_capacity;
+    std::uint32_t slot_capacity;
+    std::size_t sort_bytes;
+    types::idx_t *d_block_col_idx;
+    std::uint32_t *d_order;
+    std::uint32_t *d_width_sorted;
+    void *d_sort_tmp;
+};
+
+inline void init(blocked_ell_bucket_workspace *ws) {
+    if (ws == nullptr) return;
+    std::memset(ws, 0, sizeof(*ws));
+    ws->device = -1;
+}
+
+inline void clear(blocked_ell_bucket_workspace *ws) {
+    if (ws == nullptr) return;
+    if (ws->device >= 0) cudaSetDevice(ws->device);
+    cudaFree(ws->d_sort_tmp);
+    cudaFree(ws->d_width_sorted);
+    cudaFree(ws->d_order);
+    cudaFree(ws->d_block_col_idx);
+    if (ws->stream != nullptr) cudaStreamDestroy(ws->stream);
+    init(ws);
+}
+
+inline int setup(blocked_ell_bucket_workspace *ws, int device) {
+    if (ws == nullptr) return 0;
+    init(ws);
+    ws->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return 0;
+    return cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) == cudaSuccess;
+}
+
+// build_plan (blocked_ell_bucket.cuh:149-210): uploads the block column
+// indices, orders the row blocks on the device and copies the plan back.
+inline int build_plan(const sparse::blocked_ell *src, blocked_ell_bucket_workspace *ws,
+                      blocked_ell_bucket_plan *out) {
+    if (src == nullptr || ws == nullptr || out == nullptr || (src->rows != 0u && src->block_size == 0u)) return 0;
+    const types::u32 rb = src->rows == 0u ? 0u : (src->rows + src->block_size - 1u) / src->block_size;
+    const std::size_t slots = (std::size_t) rb * (src->block_size ? src->ell_cols / src->block_size : 0u);
+    out->row_block_order.clear();
+    out->row_block_width_sorted.clear();
+    if (rb == 0u) return 1;
+    if (cudaSetDevice(ws->device >= 0 ? ws->device : 0) != cudaSuccess) return 0;
+    std::size_t need = 0u;
+    if (!cs_b200_blocked_ell_bucket_plan_scratch_bytes(src->rows, src->block_size, &need)) return 0;
+    if (slots > ws->slot_capacity) {
+        cudaFree(ws->d_block_col_idx);
+        ws->d_block_col_idx = nullptr;
+        if (cudaMalloc((void **) &ws->d_block_col_idx, slots * 4u) != cudaSuccess) return 0;
+        ws->slot_capacity = (std::uint32_t) slots;
+    }
+    if (rb > ws->row_block_capacity) {
+        cudaFree(ws->d_order);
+        cudaFree(ws->d_width_sorted);
+        ws->d_order = ws->d_width_sorted = nullptr;
+        if (cudaMalloc((void **) &ws->d_order, (std::size_t) rb * 4u) != cudaSuccess ||
+            cudaMalloc((void **) &ws->d_width_sorted, (std::size_t) rb * 4u) != cudaSuccess)
+            return 0;
+        ws->row_block_capacity = rb;
+    }
+    if (need > ws->sort_bytes) {
+        cudaFree(ws->d_sort_tmp);
+        ws->d_sort_tmp = nullptr;
+        if (cudaMalloc(&ws->d_sort_tmp, need) != cudaSuccess) return 0;
+        ws->sort_bytes = need;
+    }
+    if (slots != 0u && cudaMemcpyAsync(ws->d_block_col_idx, src->blockColIdx, slots * 4u, cudaMemcpyHostToDevice,
+                                       ws->stream) != cudaSuccess)
+        return 0;
+    const cs_blocked_ell_view v{src->rows, src->cols, src->nnz, src->block_size, src->ell_cols, ws->d_block_col_idx,
+                                nullptr};
+    if (!cs_b200_blocked_ell_bucket_plan(&v, ws->d_order, ws->d_width_sorted, ws->d_sort_tmp, ws->sort_bytes,
+                                         ws->stream))
+        return 0;
+    out->row_block_order.resize(rb);
+    out->row_block_width_sorted.resize(rb);
+    return cudaMemcpyAsync(out->row_block_order.data(), ws->d_order, (std::size_t) rb * 4u, cudaMemcpyDeviceToHost,
+                           ws->stream) == cudaSuccess &&
+           cudaMemcpyAsync(out->row_block_width_sorted.data(), ws->d_width_sorted, (std::size_t) rb * 4u,
+                           cudaMemcpyDeviceToHost, ws->stream) == cudaSuccess &&
+           cudaStreamSynchronize(ws->stream) == cudaSuccess;
+}
+
+} // namespace bucket
+
+namespace ingest {
+namespace dataset {
+
+// choose_bucket_count_for_part of the ingest path
+// (ingest/internal/dataset/internal/convert_layout_support_part.hh:143-181).
+inline int choose_bucket_count_for_part(const sparse::blocked_ell *part, int device, std::uint32_t *bucket_count_out) {
+    return cs_b200_choose_ingest_bucket_count_for_part(reinterpret_cast<const cs_host_blocked_ell *>(part), device,
+                                                       bucket_count_out);
+}
+
+} // namespace dataset
+} // namespace ingest
 } // namespace cellshard
 
 #endif /* CELLSHARD_B200_HPP_ */

@@ -1095,3 +1095,80 @@ int cso_sell_choose_bucket_count(uint32_t rows, uint32_t S_src, const uint32_t *
     *bytes = best_bytes;
     return 1;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Ingest-time bucket-count choice (bucket::build_plan,                      */
+/* src/bucket/operators/blocked_ell_bucket.cuh:70-95,149-210, and            */
+/* estimate_bucketed_bytes_from_gpu_plan / choose_bucket_count_for_part,     */
+/* include/CellShard/ingest/internal/dataset/internal/                       */
+/* convert_layout_support_part.hh:116-181).  Row blocks are ordered by the   */
+/* 64-bit key (valid width << 32 | hash of the valid block columns), stably. */
+/* ------------------------------------------------------------------------ */
+static const uint64_t *g_sort_keys64;
+static int cmp_by_key64_then_id(const void *a, const void *b) {
+    const uint32_t x = *(const uint32_t *) a, y = *(const uint32_t *) b;
+    const uint64_t kx = g_sort_keys64[x], ky = g_sort_keys64[y];
+    if (kx != ky) return kx < ky ? -1 : 1;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+void cso_bell_bucket_plan(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t *order,
+                          uint32_t *width_sorted) {
+    const uint32_t RB = B == 0u ? 0u : (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    uint64_t *keys = (uint64_t *) malloc(((size_t) RB + 1u) * sizeof(uint64_t));
+    if (keys == NULL) return;
+    for (uint32_t rb = 0; rb < RB; ++rb) {
+        uint32_t width = 0u, hash = 2166136261u;
+        for (uint32_t s = 0; s < W; ++s) {
+            const uint32_t c = bci[(size_t) rb * W + s];
+            if (c == CSO_INVALID) continue;
+            ++width;
+            hash ^= c + 0x9e3779b9u + (hash << 6) + (hash >> 2);
+            hash *= 16777619u;
+        }
+        keys[rb] = ((uint64_t) width << 32) | hash;
+        order[rb] = rb;
+    }
+    g_sort_keys64 = keys;
+    qsort(order, RB, sizeof(uint32_t), cmp_by_key64_then_id);
+    for (uint32_t i = 0; i < RB; ++i) width_sorted[i] = (uint32_t) (keys[order[i]] >> 32);
+    free(keys);
+}
+
+uint64_t cso_bell_estimate_bucketed_bytes(uint32_t rows, uint32_t B, const uint32_t *order,
+                                          const uint32_t *width_sorted, uint32_t RB, uint32_t buckets) {
+    uint64_t bytes = 0u;
+    if (RB == 0u || buckets == 0u) return 0u;
+    for (uint32_t b = 0; b < buckets; ++b) {
+        const uint32_t lo = (b * RB) / buckets, hi = ((b + 1u) * RB) / buckets;
+        if (hi <= lo) continue;
+        const uint32_t w = width_sorted[hi - 1u];
+        uint32_t seg_rows = 0u;
+        for (uint32_t p = lo; p < hi; ++p) seg_rows += bell_rb_rows(rows, B, order[p]);
+        bytes += (uint64_t) (hi - lo) * w * 4u;
+        bytes += (uint64_t) seg_rows * w * B * 2u;
+    }
+    bytes += (uint64_t) rows * 4u * 2u;
+    bytes += ((uint64_t) buckets + 1u) * 4u;
+    return bytes;
+}
+
+uint32_t cso_bell_choose_ingest_bucket_count(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci) {
+    const uint32_t RB = B == 0u ? 0u : (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    const uint32_t top = RB < 8u ? RB : 8u;
+    uint64_t best = cso_packed_blocked_ell_bytes(rows, W * B, B);
+    uint32_t best_b = 1u;
+    if (RB <= 1u) return 1u;
+    uint32_t *order = (uint32_t *) malloc((size_t) RB * 2u * sizeof(uint32_t));
+    if (order == NULL) return 0u;
+    cso_bell_bucket_plan(rows, B, W, bci, order, order + RB);
+    for (uint32_t b = 1; b <= (top < 1u ? 1u : top); ++b) {
+        const uint64_t x = cso_bell_estimate_bucketed_bytes(rows, B, order, order + RB, RB, b);
+        if (x < best || (x == best && b < best_b)) {
+            best = x;
+            best_b = b;
+        }
+    }
+    free(order);
+    return best_b;
+}

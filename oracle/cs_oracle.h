@@ -131,6 +131,12 @@ void cso_sell_exec_fill(uint32_t rows, uint32_t S_src, const uint32_t *offsets, 
                         uint32_t *exec_to_canonical, uint32_t *canonical_to_exec);
 int cso_sell_choose_bucket_count(uint32_t rows, uint32_t S_src, const uint32_t *offsets, const uint32_t *widths,
                                  const uint32_t *col_idx, uint32_t *count, uint64_t *bytes);
+/* Ingest-time choice (blocked_ell_bucket.cuh:70-210, convert_layout_support_part.hh:116-181). */
+void cso_bell_bucket_plan(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci, uint32_t *order,
+                          uint32_t *width_sorted);
+uint64_t cso_bell_estimate_bucketed_bytes(uint32_t rows, uint32_t B, const uint32_t *order,
+                                          const uint32_t *width_sorted, uint32_t RB, uint32_t buckets);
+uint32_t cso_bell_choose_ingest_bucket_count(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci);
 
 #ifdef __cplusplus
 }

@@ -347,6 +347,29 @@ def sell_choose_bucket_count(rows, offsets, widths, col_idx):
                                               C.byref(count), C.byref(nbytes)) == 1
     return count.value, nbytes.value
 
+
+def bell_bucket_plan(rows, B, ell_cols, bci):
+    """bucket::build_plan restated: (order, width_sorted) of the row blocks."""
+    RB = (rows + B - 1) // B if B else 0
+    order, ws = np.zeros(max(RB, 1), np.uint32), np.zeros(max(RB, 1), np.uint32)
+    lib().cso_bell_bucket_plan.restype = None
+    lib().cso_bell_bucket_plan(u32(rows), u32(B), u32(ell_cols // B if B else 0),
+                               _p(np.ascontiguousarray(bci, np.uint32)), _p(order), _p(ws))
+    return order[:RB], ws[:RB]
+
+
+def bell_estimate_bucketed_bytes(rows, B, order, width_sorted, buckets):
+    f = lib().cso_bell_estimate_bucketed_bytes
+    f.restype = C.c_uint64
+    return f(u32(rows), u32(B), _p(np.ascontiguousarray(order, np.uint32)),
+             _p(np.ascontiguousarray(width_sorted, np.uint32)), u32(len(order)), u32(buckets))
+
+
+def bell_choose_ingest_bucket_count(rows, B, ell_cols, bci):
+    f = lib().cso_bell_choose_ingest_bucket_count
+    f.restype = u32
+    return f(u32(rows), u32(B), u32(ell_cols // B if B else 0), _p(np.ascontiguousarray(bci, np.uint32)))
+
 # ---------------------------------------------------------------------------
 # the reference's own code (compiled from its sources into _ref/)
 # ---------------------------------------------------------------------------
@@ -672,6 +695,53 @@ def ref_choose_bucket_count_for_sliced_part(rows, cols, nnz, offsets, widths, co
     assert ref_bucket().csrefb_choose_bucket_count_for_sliced_part(C.byref(src), C.byref(count),
                                                                    C.byref(nbytes)) == 1
     return count.value, nbytes.value
+
+
+# ---------------------------------------------------------------------------
+# the reference's ingest-time chooser (_ref/libcs_ref_ingest.so; its plan runs on the GPU)
+# ---------------------------------------------------------------------------
+REF_INGEST_LIB = HERE / "_ref" / "libcs_ref_ingest.so"
+_ri = None
+
+
+def ref_ingest_available() -> bool:
+    return REF_INGEST_LIB.exists()
+
+
+def ref_ingest() -> C.CDLL:
+    global _ri
+    if _ri is None:
+        r = C.CDLL(str(REF_INGEST_LIB))
+        r.csrefi_bucket_plan.argtypes = [vp, vp, vp]
+        r.csrefi_estimate_bucketed_bytes.argtypes = [vp, vp, vp, u32, u32]
+        r.csrefi_estimate_bucketed_bytes.restype = C.c_ulonglong
+        r.csrefi_choose_bucket_count_for_part.argtypes = [vp, vp]
+        _ri = r
+    return _ri
+
+
+def ref_bucket_plan(rows, cols, nnz, B, ell_cols, bci, val):
+    bci, val = np.ascontiguousarray(bci, np.uint32), np.ascontiguousarray(val, np.uint16)
+    RB = (rows + B - 1) // B
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    order, ws = np.zeros(max(RB, 1), np.uint32), np.zeros(max(RB, 1), np.uint32)
+    assert ref_ingest().csrefi_bucket_plan(C.byref(src), _p(order), _p(ws)) == 1
+    return order[:RB], ws[:RB]
+
+
+def ref_estimate_bucketed_bytes(rows, cols, nnz, B, ell_cols, bci, val, order, ws, buckets):
+    bci, val = np.ascontiguousarray(bci, np.uint32), np.ascontiguousarray(val, np.uint16)
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    return ref_ingest().csrefi_estimate_bucketed_bytes(C.byref(src), _p(np.ascontiguousarray(order, np.uint32)),
+                                                       _p(np.ascontiguousarray(ws, np.uint32)), len(order), buckets)
+
+
+def ref_choose_ingest_bucket_count(rows, cols, nnz, B, ell_cols, bci, val):
+    bci, val = np.ascontiguousarray(bci, np.uint32), np.ascontiguousarray(val, np.uint16)
+    src = host_bell(rows, cols, nnz, B, ell_cols, bci, val)
+    count = C.c_uint32()
+    assert ref_ingest().csrefi_choose_bucket_count_for_part(C.byref(src), C.byref(count)) == 1
+    return count.value
 
 
 def cpu_count() -> int:

@@ -104,4 +104,12 @@ extern "C" int csrefb_choose_bucket_count_for_sliced_part(const cs_host_sliced_e
     return r;
 }
 
+// The public entry point the reference defines in src/io/csh5/runtime/fetch.cc:332-337
+// (a one-line forward to build_bucketed_execution_partition); that file needs the
+// whole .csh5 runtime, so the ingest bridge links this forward instead.
+int build_bucketed_blocked_ell_partition(bucketed_blocked_ell_partition *out, const sparse::blocked_ell *part,
+                                         std::uint32_t requested_bucket_count, std::uint64_t *bucketed_bytes_out) {
+    return build_bucketed_execution_partition(out, part, requested_bucket_count, bucketed_bytes_out);
+}
+
 } // namespace cellshard (opened by the reference's header chain)

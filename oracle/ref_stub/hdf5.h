@@ -9,6 +9,11 @@ typedef long long hid_t;
 typedef int herr_t;
 typedef int htri_t;
 typedef unsigned long long hsize_t;
+typedef long long hssize_t;
+typedef int H5T_class_t;
+typedef struct {
+    int type;
+} H5L_info_t;
 
 #define H5P_DEFAULT ((hid_t) 0)
 #define H5S_ALL ((hid_t) 0)
@@ -20,8 +25,15 @@ typedef unsigned long long hsize_t;
 #define H5T_NATIVE_DOUBLE ((hid_t) 6)
 #define H5T_NATIVE_CHAR ((hid_t) 7)
 #define H5T_C_S1 ((hid_t) 8)
+#define H5T_NATIVE_LLONG ((hid_t) 9)
+#define H5T_VARIABLE ((unsigned long) -1)
 #define H5F_ACC_RDONLY 0u
+#define H5E_BEGIN_TRY {
+#define H5E_END_TRY }
 enum { H5S_SCALAR = 0, H5S_SELECT_SET = 0 };
+enum { H5T_INTEGER = 0, H5T_FLOAT = 1, H5T_STRING = 3 };
+enum { H5T_SGN_2 = 1, H5T_CSET_ASCII = 0, H5T_CSET_UTF8 = 1 };
+enum { H5_INDEX_NAME = 0, H5_ITER_NATIVE = 2 };
 
 #define CS_H5_STANDIN(name)                  \
     template <class... A>                   \
@@ -56,4 +68,15 @@ CS_H5_STANDIN(H5Tclose)
 CS_H5_STANDIN(H5Tcopy)
 CS_H5_STANDIN(H5Tget_size)
 CS_H5_STANDIN(H5Tset_size)
+CS_H5_STANDIN(H5Aget_space)
+CS_H5_STANDIN(H5Dget_type)
+CS_H5_STANDIN(H5Dvlen_reclaim)
+CS_H5_STANDIN(H5Literate)
+CS_H5_STANDIN(H5Sget_simple_extent_ndims)
+CS_H5_STANDIN(H5Sget_simple_extent_npoints)
+CS_H5_STANDIN(H5Tget_class)
+CS_H5_STANDIN(H5Tget_cset)
+CS_H5_STANDIN(H5Tget_sign)
+CS_H5_STANDIN(H5Tis_variable_str)
+CS_H5_STANDIN(H5Tset_cset)
 #undef CS_H5_STANDIN

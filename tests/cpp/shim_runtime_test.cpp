@@ -267,7 +267,57 @@ int main(int argc, char **argv) {
         std::printf("\nconvert.sell_from_bell.val");
         for (unsigned i = 0; i < total; ++i) std::printf(" %g", __half2float(sconv.val[i]));
         std::printf("\n");
+        // execution bucketing of the Sliced-ELL (2 buckets) and its chooser
+        cs::bucketed_sliced_ell_partition sb;
+        cs::init(&sb);
+        std::uint64_t sbytes = 0u;
+        if (!cs::build_bucketed_sliced_ell_partition(&sb, &sconv, 2u, &sbytes)) return fail(25, "bucketed sliced");
+        std::printf("exec.sell %u %llu", sb.segment_count, (unsigned long long) sbytes);
+        for (unsigned s = 0; s < sb.segment_count; ++s)
+            std::printf(" %u %u %u", sb.segments[s].rows, sb.segments[s].slice_count ? sb.segments[s].slice_widths[0] : 0u,
+                        sb.segments[s].nnz);
+        std::printf("\nexec.sell.e2c");
+        for (unsigned r = 0; r < sb.rows; ++r) std::printf(" %u", sb.exec_to_canonical_rows[r]);
+        std::printf("\n");
+        cs::clear(&sb);
+        std::uint32_t sc = 0u;
+        if (!cs::choose_bucket_count_for_sliced_part(&sconv, &sc, &sbytes)) return fail(26, "choose sliced");
+        std::printf("exec.sell.choose %u %llu\n", sc, (unsigned long long) sbytes);
         cs::sparse::clear(&sconv);
+    }
+    {
+        // execution bucketing of the Blocked-ELL (2 buckets), both choosers, bucket::build_plan
+        cs::bucketed_blocked_ell_partition bb;
+        cs::init(&bb);
+        std::uint64_t bbytes = 0u;
+        if (!cs::build_bucketed_blocked_ell_partition(&bb, &conv, 2u, &bbytes)) return fail(27, "bucketed blocked");
+        std::printf("exec.bell %u %llu", bb.segment_count, (unsigned long long) bbytes);
+        for (unsigned s = 0; s < bb.segment_count; ++s)
+            std::printf(" %u %u %u", bb.segments[s].rows, bb.segments[s].ell_cols, bb.segments[s].nnz);
+        std::printf("\nexec.bell.block_cols");
+        for (unsigned s = 0; s < bb.segment_count; ++s) {
+            const cs::sparse::blocked_ell &g = bb.segments[s];
+            const unsigned n = ((g.rows + g.block_size - 1u) / g.block_size) * (g.ell_cols / g.block_size);
+            for (unsigned i = 0; i < n; ++i) std::printf(" %u", g.blockColIdx[i]);
+        }
+        std::printf("\nexec.bell.e2c");
+        for (unsigned r = 0; r < bb.rows; ++r) std::printf(" %u", bb.exec_to_canonical_rows[r]);
+        std::printf("\n");
+        cs::clear(&bb);
+        std::uint32_t bc = 0u, ic = 0u;
+        if (!cs::choose_bucket_count_for_part(&conv, &bc, &bbytes)) return fail(28, "choose blocked");
+        if (!cs::ingest::dataset::choose_bucket_count_for_part(&conv, 0, &ic)) return fail(29, "choose ingest");
+        std::printf("exec.bell.choose %u %llu %u\n", bc, (unsigned long long) bbytes, ic);
+        cs::bucket::blocked_ell_bucket_workspace pws;
+        cs::bucket::init(&pws);
+        cs::bucket::blocked_ell_bucket_plan plan;
+        if (!cs::bucket::setup(&pws, 0) || !cs::bucket::build_plan(&conv, &pws, &plan)) return fail(30, "build_plan");
+        std::printf("exec.plan.order");
+        for (auto x : plan.row_block_order) std::printf(" %u", x);
+        std::printf("\nexec.plan.width");
+        for (auto x : plan.row_block_width_sorted) std::printf(" %u", x);
+        std::printf("\n");
+        cs::bucket::clear(&pws);
     }
     cs::sparse::clear(&conv);
     const unsigned cands[3] = {16u, 32u, 64u};

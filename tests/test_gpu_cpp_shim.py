@@ -117,6 +117,31 @@ def test_shim_convert_bucket_transpose_reoptimize(shim_out, orc):
     assert list(o["convert.sell_from_bell"]) == [hb, sb["slice_count"], ref["nnz"]]
     assert np.array_equal(o["convert.sell_from_bell.col"].astype(np.uint32), sb["col_idx"])
     assert np.array_equal(o["convert.sell_from_bell.val"].astype(np.float16).view(np.uint16), sb["val"])
+    # execution bucketing of that Sliced-ELL and of the Blocked-ELL-2, both choosers, the ingest plan
+    eb = orc.sell_bucketed(rows, sb["offsets"], sb["widths"], sb["col_idx"], sb["val"], 2)
+    seg_nnz = [int(sum(eb["row_widths"][eb["order"][eb["seg_row"][k]:eb["seg_row"][k + 1]]]))
+               for k in range(eb["segment_count"])]
+    want = [eb["segment_count"], eb["bytes"]]
+    for k in range(eb["segment_count"]):
+        want += [int(eb["seg_row"][k + 1] - eb["seg_row"][k]), int(eb["seg_w"][k]), seg_nnz[k]]
+    assert list(o["exec.sell"]) == want
+    assert np.array_equal(o["exec.sell.e2c"].astype(np.uint32), eb["e2c"])
+    assert tuple(o["exec.sell.choose"]) == orc.sell_choose_bucket_count(rows, sb["offsets"], sb["widths"],
+                                                                         sb["col_idx"])
+    bb = orc.bell_bucketed(rows, 2, ref["ell_cols"], ref["bci"], ref["val"], 2)
+    want = [bb["segment_count"], bb["bytes"]]
+    for k in range(bb["segment_count"]):
+        rbs = bb["order"][bb["seg_rb"][k]:bb["seg_rb"][k + 1]]
+        nnz_k = int(sum(min(2, rows - 2 * int(r)) * int(bb["widths"][r]) * 2 for r in rbs))
+        want += [int(bb["seg_rows"][k]), int(bb["seg_w"][k]) * 2, nnz_k]
+    assert list(o["exec.bell"]) == want
+    assert np.array_equal(o["exec.bell.block_cols"].astype(np.uint32), bb["seg_bci"])
+    assert np.array_equal(o["exec.bell.e2c"].astype(np.uint32), bb["e2c"])
+    assert list(o["exec.bell.choose"]) == [*orc.bell_choose_bucket_count(rows, 2, ref["ell_cols"], ref["bci"]),
+                                          orc.bell_choose_ingest_bucket_count(rows, 2, ref["ell_cols"], ref["bci"])]
+    po, pw = orc.bell_bucket_plan(rows, 2, ref["ell_cols"], ref["bci"])
+    assert np.array_equal(o["exec.plan.order"].astype(np.uint32), po)
+    assert np.array_equal(o["exec.plan.width"].astype(np.uint32), pw)
     h, score, _ = orc.choose_sliced_slice_rows(rows, int(ptr[-1]), ptr, (16, 32, 64))
     assert o["convert.slice_choice"][0] == h and o["convert.slice_choice"][3] == score
     _nnz, _srt, order, offs = orc.major_nnz_plan(ptr, rows, 2)

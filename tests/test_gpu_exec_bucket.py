@@ -279,3 +279,60 @@ def test_synthetic_round_trip(cuda):
             keep = slot < cnt.repeat_interleave(B)[a:b, None]
             want = torch.where(keep[:, :, None], g, torch.zeros_like(g))
             assert torch.equal(seg.val.view(seg.rows, w, B)[a:b].view(torch.int16), want.view(torch.int16))
+
+
+@pytest.mark.parametrize("rows,cols,B,density,empty", [
+    (1000, 2000, 16, 0.01, 0.3),
+    (333, 500, 8, 0.05, 0.2),     # partial last row block, sorted with the others here
+    (200, 300, 5, 0.1, 0.1),
+    (96, 96, 8, 1.0, 0.0),        # equal widths: the hash orders the row blocks
+    (17, 40, 16, 0.2, 0.0),       # two row blocks
+])
+def test_ingest_plan_and_choice(cuda, orc, rows, cols, B, density, empty):
+    """bucket::build_plan and the ingest chooser: the device plan against the
+    restatement and the reference's own GPU plan, the device choice against
+    the restatement, the reference's chooser and its estimate."""
+    import torch
+
+    from cellshard_b200 import _abi
+    from cellshard_b200.device import blocked_ell_from_csr, ptr, stream_handle
+
+    ptr_, idx, val = random_csr(rows, cols, density, rows + 3 * B, empty)
+    bell = blocked_ell_from_csr(to_device_csr(rows, cols, ptr_, idx, val), B)
+    bci, bval = np_u32(bell.bci), np_u16(bell.val)
+    lib = _abi.load()
+    RB = bell.row_blocks
+    nb = C.c_size_t()
+    assert lib.cs_b200_blocked_ell_bucket_plan_scratch_bytes(rows, B, C.byref(nb)) == 1
+    scr = torch.empty(max(nb.value, 16), dtype=torch.uint8, device="cuda")
+    order = torch.empty(RB, dtype=torch.int32, device="cuda")
+    ws = torch.empty(RB, dtype=torch.int32, device="cuda")
+    out = torch.zeros(4, dtype=torch.int64, device="cuda")
+    v = bell.view()
+    assert lib.cs_b200_blocked_ell_bucket_plan(C.byref(v), ptr(order), ptr(ws), ptr(scr), nb.value,
+                                               stream_handle()) == 1
+    assert lib.cs_b200_choose_bucket_count_from_plan(C.byref(v), ptr(order), ptr(ws), out.data_ptr(),
+                                                     out.data_ptr() + 8, stream_handle()) == 1
+    o, w = np_u32(order), np_u32(ws)
+    ro, rw = orc.bell_bucket_plan(rows, B, bell.ell_cols, bci)
+    assert np.array_equal(o, ro) and np.array_equal(w, rw)
+    count = int(out[0].item()) & 0xFFFFFFFF
+    assert count == orc.bell_choose_ingest_bucket_count(rows, B, bell.ell_cols, bci)
+    est = [orc.bell_estimate_bucketed_bytes(rows, B, o, w, b) for b in range(1, min(8, RB) + 1)]
+    f = orc.lib().cso_packed_blocked_ell_bytes
+    f.restype = C.c_uint64
+    orig = f(C.c_uint32(rows), C.c_uint32(bell.ell_cols), C.c_uint32(B))
+    assert int(out[1].item()) == (min(orig, est[count - 1]) if est else orig)
+    h = _abi.HostBlockedEll()
+    h.rows, h.cols, h.nnz, h.block_size, h.ell_cols = rows, cols, bell.nnz, B, bell.ell_cols
+    hb = np.ascontiguousarray(bci)
+    h.blockColIdx = hb.ctypes.data
+    c = C.c_uint32()
+    assert lib.cs_b200_choose_ingest_bucket_count_for_part(C.byref(h), 0, C.byref(c)) == 1 and c.value == count
+    if orc.ref_ingest_available():
+        po, pw = orc.ref_bucket_plan(rows, cols, bell.nnz, B, bell.ell_cols, bci, bval)
+        assert np.array_equal(o, po) and np.array_equal(w, pw)
+        assert count == orc.ref_choose_ingest_bucket_count(rows, cols, bell.nnz, B, bell.ell_cols, bci, bval)
+        for b in range(1, min(8, RB) + 1):
+            assert est[b - 1] == orc.ref_estimate_bucketed_bytes(rows, cols, bell.nnz, B, bell.ell_cols, bci, bval,
+                                                                 po, pw, b)
