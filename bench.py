@@ -506,6 +506,69 @@ def bucket_lines(lib, timed, emit, bell, sell):
     torch.cuda.empty_cache()
 
 
+def coo_lines(lib, timed, emit, csr):
+    """COO -> Blocked-ELL-16 of the same matrix held as row-major COO: the plan (column
+    scan, keys, the stable radix sort, group heads and scans; two small device->host
+    reads) and the emit (block columns, zeroed values, one thread per block group),
+    timed separately; the reference's host routine on a row sample as the CPU line."""
+    import ctypes as C
+
+    import torch
+
+    from cellshard_b200 import _abi
+    from cellshard_b200.device import ptr, stream_handle
+
+    R, Cc, n = csr.rows, csr.cols, csr.nnz
+    counts = (csr.ptr[1:] - csr.ptr[:-1]).long()
+    row = torch.repeat_interleave(torch.arange(R, dtype=torch.int32, device="cuda"), counts)
+    v = _abi.CooView()
+    v.rows, v.cols, v.nnz = R, Cc, n
+    v.rowIdx, v.colIdx, v.val = ptr(row), ptr(csr.idx), ptr(csr.val)
+    nb = C.c_size_t()
+    lib.cs_b200_coo_blocked_ell_scratch_bytes(n, R, Cc, BLOCK, C.byref(nb))
+    scr = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+    width, total = C.c_uint32(), C.c_uint64()
+    plan_fn = lambda: lib.cs_b200_coo_blocked_ell_plan(C.byref(v), None, Cc, BLOCK, ptr(scr), nb.value, C.byref(width),
+                                                       C.byref(total), None, stream_handle())
+    _abi.check(plan_fn(), "coo plan")
+    W = width.value
+    RB = (R + BLOCK - 1) // BLOCK
+    bci = torch.empty(RB * W, dtype=torch.int32, device="cuda")
+    val = torch.empty(R * W * BLOCK, dtype=torch.float16, device="cuda")
+    nnz = torch.zeros(2, dtype=torch.int64, device="cuda")
+    dv = _abi.BlockedEllView()
+    dv.rows, dv.cols, dv.nnz, dv.block_size, dv.ell_cols = R, Cc, 0, BLOCK, W * BLOCK
+    dv.blockColIdx, dv.val = ptr(bci), ptr(val)
+    emit_fn = lambda: lib.cs_b200_coo_blocked_ell_emit(C.byref(v), None, Cc, ptr(scr), nb.value, C.byref(dv),
+                                                       ptr(nnz), stream_handle())
+    ms_plan = timed(plan_fn)
+    emit("coo_blocked_ell_plan", ms_plan, 0, {"ell_cols": W * BLOCK, "total_blocks": total.value,
+                                              "note": "time only: scan, keys, stable radix sort, heads, scans, "
+                                                      "two device->host reads"})
+    ms_emit = timed(emit_fn)
+    cpu = None
+    from oracle import oracle
+
+    if oracle.ref_available():
+        # the reference's host routine on the first rows (about 5 M entries)
+        S = int(torch.searchsorted(csr.ptr.long(), torch.tensor([5_000_000], device="cuda")).item())
+        S = max(1, min(R, S))
+        m = int(csr.ptr[S].item())
+        hr, hc, hv = row[:m].cpu().numpy().view(np.uint32), csr.idx[:m].cpu().numpy().view(np.uint32), \
+            csr.val[:m].cpu().numpy().view(np.uint16)
+        t0, k = time.perf_counter(), 0
+        while k < 3 and (k == 0 or time.perf_counter() - t0 < 10.0):
+            oracle.ref_blocked_ell_from_coo(S, Cc, Cc, hr, hc, hv, BLOCK)
+            k += 1
+        cpu = {"value": S / ((time.perf_counter() - t0) / k), "unit": "rows/s", "cores": 1, "kind": "reference",
+               "sample": f"first {S} rows ({m} entries), convert::blocked_ell_from_coo (host loops)"}
+    ex = {"ell_cols": W * BLOCK, "rows_per_s": R / ((ms_plan + ms_emit) * 1e-3)}
+    if cpu is not None:
+        ex["cpu_baseline"] = cpu
+    emit("coo_blocked_ell_emit", ms_emit, 12 * n + RB * W * 4 + R * W * BLOCK * 2 + 12 * total.value, ex)
+    del row, scr, bci, val
+
+
 def run_convert(args):
     """Conversion kernels on the same 500,000 x 32,768 matrix: CSR -> Blocked-ELL-16,
     Blocked-ELL-16 -> Sliced-ELL (h 32), CSR -> Sliced-ELL (h 32), stable transpose,
@@ -608,6 +671,8 @@ def run_convert(args):
     # execution bucketing of the Blocked-ELL-16 (bucket count chosen in 1..8, then the fill)
     bucket_lines(lib, timed, emit, bell, None)
     del bell
+    torch.cuda.empty_cache()
+    coo_lines(lib, timed, emit, csr)
     torch.cuda.empty_cache()
     # Sliced-ELL at h = 32: layout + emit (the layout's total needs one host read)
     sell = sliced_ell_from_csr(csr, 32)

@@ -51,6 +51,16 @@ class HostSlicedEll(C.Structure):
                 ("val", vp)]
 
 
+class HostCoo(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("storage", vp), ("rowIdx", vp), ("colIdx", vp),
+                ("val", vp)]
+
+
+class CooView(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("rowIdx", vp), ("colIdx", vp), ("val", vp),
+                ("_pad", C.c_uint64)]
+
+
 class HostBucketedBlockedEll(C.Structure):
     _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("segment_count", u32), ("segments", vp),
                 ("segment_row_offsets", vp), ("exec_to_canonical_rows", vp), ("canonical_to_exec_rows", vp),
@@ -187,6 +197,13 @@ PROTOTYPES: dict[str, tuple] = {
                                                     vp, sz, vp, vp]),
     "cs_b200_filter_blocked_ell_emit": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
                                                    vp, vp]),
+    "cs_b200_coo_blocked_ell_scratch_bytes": (C.c_int, [u32, u32, u32, u32, P(sz)]),
+    "cs_b200_coo_blocked_ell_plan": (C.c_int, [P(CooView), vp, u32, u32, vp, sz, P(u32), P(u64), vp, vp]),
+    "cs_b200_coo_blocked_ell_emit": (C.c_int, [P(CooView), vp, u32, vp, sz, P(BlockedEllView), vp, vp]),
+    "cs_b200_blocked_ell_from_coo": (C.c_int, [P(HostCoo), u32, vp, C.c_uint, P(HostBlockedEll)]),
+    "cs_b200_blocked_ell_from_coo_cuda": (C.c_int, [P(HostCoo), u32, vp, C.c_uint, P(HostBlockedEll), C.c_int]),
+    "cs_b200_choose_blocked_ell_block_size_from_coo": (C.c_int, [P(HostCoo), u32, vp, P(C.c_uint), C.c_uint,
+                                                                  P(BlockedEllTuneResult)]),
     "cs_b200_bucketed_blocked_ell_scratch_bytes": (C.c_int, [u32, u32, u32, P(sz)]),
     "cs_b200_bucketed_blocked_ell_plan": (C.c_int, [P(BlockedEllView), u32, vp, sz, P(ExecBucketPlan),
                                                      P(ExecBucketSegments), vp]),

@@ -521,7 +521,9 @@ int bell_fill(const cs_blocked_ell_view *part, const void *scratch, const cs_exe
     carve(const_cast<void *>(scratch), g.RB, 1u, &x);
     const bool vec = g.B % 8u == 0u && (reinterpret_cast<uintptr_t>(part->val) & 15u) == 0u &&
                      (reinterpret_cast<uintptr_t>(seg_val) & 15u) == 0u;
-    const std::size_t work = g.RB > part->cols ? g.RB : (part->cols + kFillThreads - 1u) / kFillThreads;
+    // blocks: one per destination row block, and enough to write the column maps
+    const std::size_t col_blocks = ((std::size_t) part->cols + kFillThreads - 1u) / kFillThreads;
+    const std::size_t work = g.RB > col_blocks ? g.RB : col_blocks;
     if (work == 0u) return 1;
     const void *k = vec ? (const void *) bell_exec_fill_kernel<true> : (const void *) bell_exec_fill_kernel<false>;
     const unsigned grid = resident_grid(k, kFillThreads, 0, work);

@@ -385,3 +385,40 @@ def bucketed_sliced_ell(sell: SlicedELL, requested: int, stream=None) -> Buckete
         o += n * w
     return BucketedPartition(_plan_dict(plan), segments, [int(x) for x in row_off[:S + 1]], e2c, c2e, None, None,
                              col, val)
+
+
+def blocked_ell_from_coo(rows: int, cols_src: int, row_idx: torch.Tensor, col_idx: torch.Tensor, val: torch.Tensor,
+                         block_size: int, cols: int, feature_to_global: torch.Tensor | None = None, stream=None):
+    """COO -> Blocked-ELL on the GPU (convert::blocked_ell_from_coo_cuda): plan (one host read of
+    the largest column, one of the width), then the emit.  Returns the Blocked-ELL and the two
+    nnz counts (the host routine's: stored nonzero values; the GPU routine's: those with
+    column < cols)."""
+    lib = _abi.load()
+    n = int(row_idx.numel())
+    v = _abi.CooView()
+    v.rows, v.cols, v.nnz = rows, cols_src, n
+    v.rowIdx, v.colIdx, v.val = ptr(row_idx), ptr(col_idx), ptr(val)
+    nbytes = C.c_size_t()
+    _abi.check(lib.cs_b200_coo_blocked_ell_scratch_bytes(n, rows, cols, block_size, C.byref(nbytes)), "coo scratch")
+    scratch = _scratch(nbytes.value)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    width, total = C.c_uint32(), C.c_uint64()
+    s = stream_handle(stream)
+    fm = ptr(feature_to_global) if feature_to_global is not None else None
+    _abi.check(lib.cs_b200_coo_blocked_ell_plan(C.byref(v), fm, cols, block_size, ptr(scratch), nbytes.value,
+                                                C.byref(width), C.byref(total), ptr(status), s), "coo plan")
+    W = width.value
+    RB = (rows + block_size - 1) // block_size
+    out = BlockedELL(rows, cols, block_size, W * block_size,
+                     torch.empty(max(RB * W, 1), dtype=torch.int32, device="cuda"),
+                     torch.empty(max(rows * W * block_size, 1), dtype=torch.float16, device="cuda"), 0)
+    nnz = torch.zeros(2, dtype=torch.int64, device="cuda")
+    dv = out.view()
+    dv.blockColIdx, dv.val = out.bci.data_ptr(), out.val.data_ptr()
+    _abi.check(lib.cs_b200_coo_blocked_ell_emit(C.byref(v), fm, cols, ptr(scratch), nbytes.value, C.byref(dv),
+                                                nnz.data_ptr(), s), "coo emit")
+    counts = [int(x) for x in nnz.cpu()]
+    out.nnz = counts[1]
+    out.bci = out.bci[:RB * W]
+    out.val = out.val[:rows * W * block_size]
+    return out, counts, int(status.item()), total.value

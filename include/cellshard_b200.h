@@ -207,6 +207,83 @@ CS_API int cs_b200_choose_blocked_ell_block_size(const cs_host_compressed *src,
                                           cs_blocked_ell_tune_result *out);
 
 /* ------------------------------------------------------------------------ */
+/* COO -> Blocked-ELL                                                         */
+/* replaces convert::blocked_ell_from_coo[_auto] and                          */
+/* choose_blocked_ell_block_size_from_coo (src/convert/                        */
+/* blocked_ell_from_compressed.cuh:105-257,349-478, host loops) and their GPU  */
+/* twins blocked_ell_from_coo_cuda[_auto] /                                   */
+/* choose_blocked_ell_block_size_from_coo_cuda (src/convert/                   */
+/* blocked_ell_from_coo_cuda.cuh:17-966).  Columns pass through the optional   */
+/* feature_to_global map first.  Each row block's distinct block columns are  */
+/* its slots, ascending; the width is the largest count.  Values land in COO  */
+/* order, so a repeated (row, column) keeps its last value (the host          */
+/* routine's rule; the reference's GPU scatter leaves the winner to the        */
+/* hardware).  Entries whose row is out of range are dropped and flagged      */
+/* CS_STATUS_INDEX_RANGE.                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* sparse::coo (formats/triplet.cuh:14-25) and device::coo_view
+ * (runtime/device/sharded_device.cuh:100-107) */
+typedef struct CS_ALIGN16 cs_host_coo {
+    uint32_t rows, cols, nnz;
+    void *storage;
+    uint32_t *rowIdx;
+    uint32_t *colIdx;
+    uint16_t *val;
+} cs_host_coo;
+
+typedef struct CS_ALIGN16 cs_coo_view {
+    uint32_t rows, cols, nnz;
+    uint32_t *rowIdx;
+    uint32_t *colIdx;
+    uint16_t *val;
+} cs_coo_view;
+
+/* Shape of one block size: width and the count of (row block, block column)
+ * pairs; the plan stays in the scratch for the emit of the same block size.
+ * Entries whose rows never decrease, with every mapped column below cols,
+ * take the CSR route (row pointers from the row runs, then the CSR ->
+ * Blocked-ELL shape and emit); others are sorted by (row block, block
+ * column).  Synchronises (two small reads of sizes). */
+CS_API int cs_b200_coo_blocked_ell_scratch_bytes(uint32_t nnz, uint32_t rows, uint32_t cols, uint32_t block_size,
+                                                 size_t *out_bytes);
+CS_API int cs_b200_coo_blocked_ell_plan(const cs_coo_view *src,
+                                        const uint32_t *d_feature_to_global,
+                                        uint32_t cols,
+                                        uint32_t block_size,
+                                        void *d_scratch,
+                                        size_t scratch_bytes,
+                                        uint32_t *ell_width_out,
+                                        uint64_t *total_blocks_out,
+                                        uint32_t *d_status,
+                                        cs_stream_t stream);
+/* dst: rows = src->rows, block_size, ell_cols = width * block_size, arrays
+ * allocated by the caller.  d_nnz (u64[2], zeroed by the caller) <- the
+ * stored values nonzero as floats, and those of them with column < cols
+ * (the host routine's and the GPU routine's nnz respectively). */
+CS_API int cs_b200_coo_blocked_ell_emit(const cs_coo_view *src,
+                                        const uint32_t *d_feature_to_global,
+                                        uint32_t cols,
+                                        const void *d_scratch,
+                                        size_t scratch_bytes,
+                                        const cs_blocked_ell_view *dst,
+                                        uint64_t *d_nnz,
+                                        cs_stream_t stream);
+
+/* Host signatures (host COO in, host Blocked-ELL out; synchronous).
+ * feature_to_global is a host array of src->cols entries or NULL. */
+CS_API int cs_b200_blocked_ell_from_coo(const cs_host_coo *src, uint32_t cols, const uint32_t *feature_to_global,
+                                        unsigned int block_size, cs_host_blocked_ell *dst);
+CS_API int cs_b200_blocked_ell_from_coo_cuda(const cs_host_coo *src, uint32_t cols,
+                                             const uint32_t *feature_to_global, unsigned int block_size,
+                                             cs_host_blocked_ell *dst, int device);
+CS_API int cs_b200_choose_blocked_ell_block_size_from_coo(const cs_host_coo *src, uint32_t cols,
+                                                          const uint32_t *feature_to_global,
+                                                          const unsigned int *candidates,
+                                                          unsigned int candidate_count,
+                                                          cs_blocked_ell_tune_result *out);
+
+/* ------------------------------------------------------------------------ */
 /* CSR -> Sliced-ELL                                                          */
 /* replaces convert::sliced_ell_from_compressed[_cuda] and                    */
 /* choose_sliced_ell_slice_rows[_from_compressed] (src/convert/                */

@@ -16,6 +16,8 @@
  *   src/convert/blocked_ell_from_compressed.cuh:157-190,258-347
  *   src/convert/sliced_ell_from_compressed.cuh:96-164,
  *       sliced_ell_from_blocked_ell.cuh:18-26,196-221
+ *   src/convert/blocked_ell_from_compressed.cuh:192-257,349-478 (COO),
+ *       blocked_ell_from_coo_cuda.cuh:604-966
  *   src/convert/compressed_transpose_raw.cuh:14-123
  *   src/bucket/major_nnz_raw.cuh:12-320, src/bucket/operators/major_nnz.cuh:11-213
  *   include/CellShard/runtime/mask_groups.cuh:14-224
@@ -24,8 +26,8 @@
  *       src/bucket/operators/blocked_ell_bucket.cuh:11-210,
  *       include/CellShard/ingest/internal/dataset/internal/convert_layout_support_part.hh:143-181
  * Not mirrored (out of this library's scope): the fleet (multi-GPU) entry
- * points, sharded<T> host containers and their shard-level staging, the COO
- * and DIA formats.
+ * points, sharded<T> host containers and their shard-level staging, COO
+ * staging and the DIA format.
  */
 #ifndef CELLSHARD_B200_HPP_
 #define CELLSHARD_B200_HPP_
@@ -100,6 +102,19 @@ struct alignas(16) sliced_ell {
     real::storage_t *val;
 };
 
+// formats/triplet.cuh:14-25
+struct alignas(16) coo {
+    types::dim_t rows;
+    types::dim_t cols;
+    types::nnz_t nnz;
+    void *storage;
+    types::idx_t *rowIdx;
+    types::idx_t *colIdx;
+    real::storage_t *val;
+};
+
+static_assert(sizeof(coo) == sizeof(cs_host_coo) && offsetof(coo, val) == offsetof(cs_host_coo, val),
+              "sparse::coo layout");
 static_assert(sizeof(compressed) == sizeof(cs_host_compressed) &&
                   offsetof(compressed, val) == offsetof(cs_host_compressed, val),
               "sparse::compressed layout");
@@ -247,6 +262,62 @@ inline int choose_blocked_ell_block_size(const sparse::compressed *src, const un
                                          unsigned int candidate_count, blocked_ell_tune_result *out) {
     return cs_b200_choose_blocked_ell_block_size(reinterpret_cast<const cs_host_compressed *>(src), candidates,
                                                  candidate_count, reinterpret_cast<cs_blocked_ell_tune_result *>(out));
+}
+
+// COO -> Blocked-ELL (blocked_ell_from_compressed.cuh:192-257,349-478;
+// blocked_ell_from_coo_cuda.cuh:604-966).  The _cuda forms take the device
+// ordinal; workspaces and streams of the reference's _cuda signatures are
+// replaced by the library's own.
+inline int blocked_ell_from_coo(const sparse::coo *src, types::dim_t cols, const types::u32 *feature_to_global,
+                                unsigned int block_size, sparse::blocked_ell *dst) {
+    return cs_b200_blocked_ell_from_coo(reinterpret_cast<const cs_host_coo *>(src), cols, feature_to_global,
+                                        block_size, reinterpret_cast<cs_host_blocked_ell *>(dst));
+}
+
+inline int blocked_ell_from_coo_cuda(const sparse::coo *src, types::dim_t cols, const types::u32 *feature_to_global,
+                                     unsigned int block_size, sparse::blocked_ell *dst, int device) {
+    return cs_b200_blocked_ell_from_coo_cuda(reinterpret_cast<const cs_host_coo *>(src), cols, feature_to_global,
+                                             block_size, reinterpret_cast<cs_host_blocked_ell *>(dst), device);
+}
+
+inline int choose_blocked_ell_block_size_from_coo(const sparse::coo *src, types::dim_t cols,
+                                                  const types::u32 *feature_to_global, const unsigned int *candidates,
+                                                  unsigned int candidate_count, blocked_ell_tune_result *out) {
+    return cs_b200_choose_blocked_ell_block_size_from_coo(reinterpret_cast<const cs_host_coo *>(src), cols,
+                                                          feature_to_global, candidates, candidate_count,
+                                                          reinterpret_cast<cs_blocked_ell_tune_result *>(out));
+}
+
+inline int choose_blocked_ell_block_size_from_coo_cuda(const sparse::coo *src, types::dim_t cols,
+                                                       const types::u32 *feature_to_global,
+                                                       const unsigned int *candidates, unsigned int candidate_count,
+                                                       int device, blocked_ell_tune_result *out) {
+    if (cudaSetDevice(device) != cudaSuccess) return 0;
+    return choose_blocked_ell_block_size_from_coo(src, cols, feature_to_global, candidates, candidate_count, out);
+}
+
+inline int blocked_ell_from_coo_auto(const sparse::coo *src, types::dim_t cols, const types::u32 *feature_to_global,
+                                     const unsigned int *candidates, unsigned int candidate_count,
+                                     sparse::blocked_ell *dst, blocked_ell_tune_result *picked = nullptr) {
+    blocked_ell_tune_result t{};
+    if (!choose_blocked_ell_block_size_from_coo(src, cols, feature_to_global, candidates, candidate_count, &t) ||
+        !blocked_ell_from_coo(src, cols, feature_to_global, t.block_size, dst))
+        return 0;
+    if (picked != nullptr) *picked = t;
+    return 1;
+}
+
+inline int blocked_ell_from_coo_cuda_auto(const sparse::coo *src, types::dim_t cols,
+                                          const types::u32 *feature_to_global, const unsigned int *candidates,
+                                          unsigned int candidate_count, sparse::blocked_ell *dst, int device,
+                                          blocked_ell_tune_result *picked = nullptr) {
+    blocked_ell_tune_result t{};
+    if (!choose_blocked_ell_block_size_from_coo_cuda(src, cols, feature_to_global, candidates, candidate_count, device,
+                                                     &t) ||
+        !blocked_ell_from_coo_cuda(src, cols, feature_to_global, t.block_size, dst, device))
+        return 0;
+    if (picked != nullptr) *picked = t;
+    return 1;
 }
 
 inline int sliced_ell_from_compressed(const sparse::compressed *src, unsigned int slice_rows,

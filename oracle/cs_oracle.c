@@ -1172,3 +1172,121 @@ uint32_t cso_bell_choose_ingest_bucket_count(uint32_t rows, uint32_t B, uint32_t
     free(order);
     return best_b;
 }
+
+/* ------------------------------------------------------------------------ */
+/* COO -> Blocked-ELL (convert::blocked_ell_from_coo and                     */
+/* choose_blocked_ell_block_size_from_coo, src/convert/                      */
+/* blocked_ell_from_compressed.cuh:105-257,349-437): row blocks' distinct    */
+/* block columns ascending, width = the largest count; values placed in      */
+/* COO order (a repeated (row, col) keeps the last); nnz[0] = stored values  */
+/* that are nonzero as floats (the host routine's count), nnz[1] = those     */
+/* also in a valid slot with column < cols (the CUDA routine's count,        */
+/* blocked_ell_from_coo_cuda.cuh:179-198).  Returns the width, or -1 when a  */
+/* row index is out of range.                                                */
+/* ------------------------------------------------------------------------ */
+static uint32_t coo_col(const uint32_t *col, const uint32_t *map, uint64_t i) {
+    return map != NULL ? map[col[i]] : col[i];
+}
+
+/* per row block: distinct block columns, ascending, into bc (offsets off[RB+1]) */
+static int coo_block_cols(uint32_t rows, uint32_t nnz, const uint32_t *row, const uint32_t *col, const uint32_t *map,
+                          uint32_t B, uint32_t *off, uint32_t *bc, uint32_t *width, uint64_t *total) {
+    const uint32_t RB = (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    uint32_t *cur = (uint32_t *) calloc((size_t) RB + 1u, sizeof(uint32_t));
+    if (cur == NULL) return 0;
+    memset(off, 0, ((size_t) RB + 1u) * sizeof(uint32_t));
+    for (uint32_t i = 0; i < nnz; ++i) ++off[row[i] / B + 1u];
+    for (uint32_t rb = 0; rb < RB; ++rb) {
+        off[rb + 1u] += off[rb];
+        cur[rb] = off[rb];
+    }
+    for (uint32_t i = 0; i < nnz; ++i) bc[cur[row[i] / B]++] = coo_col(col, map, i) / B;
+    *width = 0u;
+    *total = 0u;
+    for (uint32_t rb = 0; rb < RB; ++rb) {
+        uint32_t n = off[rb + 1u] - off[rb], u = 0u;
+        qsort(bc + off[rb], n, sizeof(uint32_t), cmp_u32);
+        for (uint32_t j = 0; j < n; ++j)
+            if (j == 0u || bc[off[rb] + j] != bc[off[rb] + j - 1u]) bc[off[rb] + u++] = bc[off[rb] + j];
+        cur[rb] = u; /* distinct count, compacted to the front */
+        if (u > *width) *width = u;
+        *total += u;
+    }
+    for (uint32_t rb = 0; rb < RB; ++rb) off[rb] = cur[rb]; /* reuse: distinct count per row block */
+    free(cur);
+    return 1;
+}
+
+long long cso_blocked_ell_from_coo(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row,
+                                   const uint32_t *col, const uint16_t *val, const uint32_t *map, uint32_t B,
+                                   uint32_t *bci, uint16_t *out_val, uint64_t *nnz_out, uint64_t *total_blocks) {
+    const uint32_t RB = (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    for (uint32_t i = 0; i < nnz; ++i)
+        if (row[i] >= rows) return -1;
+    uint32_t *off = (uint32_t *) malloc(((size_t) RB + 1u) * sizeof(uint32_t));
+    uint32_t *start = (uint32_t *) malloc(((size_t) RB + 1u) * sizeof(uint32_t));
+    uint32_t *bc = (uint32_t *) malloc(((size_t) nnz + 1u) * sizeof(uint32_t));
+    uint32_t W = 0u;
+    uint64_t tot = 0u;
+    if (!off || !start || !bc || !coo_block_cols(rows, nnz, row, col, map, B, off, bc, &W, &tot)) {
+        free(off);
+        free(start);
+        free(bc);
+        return -1;
+    }
+    /* recover each row block's start in bc: the counting pass order */
+    {
+        uint32_t *cnt = (uint32_t *) calloc((size_t) RB + 1u, sizeof(uint32_t));
+        for (uint32_t i = 0; i < nnz; ++i) ++cnt[row[i] / B + 1u];
+        for (uint32_t rb = 0; rb < RB; ++rb) cnt[rb + 1u] += cnt[rb];
+        memcpy(start, cnt, ((size_t) RB + 1u) * sizeof(uint32_t));
+        free(cnt);
+    }
+    const size_t ell = (size_t) W * B;
+    if (bci != NULL)
+        for (size_t i = 0; i < (size_t) RB * W; ++i) bci[i] = CSO_INVALID;
+    if (out_val != NULL) memset(out_val, 0, (size_t) rows * ell * sizeof(uint16_t));
+    for (uint32_t rb = 0; rb < RB && bci != NULL; ++rb)
+        for (uint32_t s = 0; s < off[rb]; ++s) bci[(size_t) rb * W + s] = bc[start[rb] + s];
+    uint64_t nz_all = 0u, nz_in = 0u;
+    for (uint32_t i = 0; i < nnz && out_val != NULL; ++i) {
+        const uint32_t c = coo_col(col, map, i), rb = row[i] / B, b = c / B;
+        /* binary search of the block column among the row block's slots */
+        uint32_t lo = 0u, hi = off[rb], slot = 0u;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2u;
+            if (bc[start[rb] + mid] < b)
+                lo = mid + 1u;
+            else
+                hi = mid;
+        }
+        slot = lo;
+        uint16_t *dst = out_val + (size_t) row[i] * ell + (size_t) slot * B + c % B;
+        const int prev = half_nonzero(*dst), next = half_nonzero(val[i]);
+        const int in = c < cols;
+        nz_all += (uint64_t) (next - prev);
+        if (in) nz_in += (uint64_t) (next - prev);
+        *dst = val[i];
+    }
+    if (nnz_out != NULL) {
+        nnz_out[0] = nz_all;
+        nnz_out[1] = nz_in;
+    }
+    if (total_blocks != NULL) *total_blocks = tot;
+    free(off);
+    free(start);
+    free(bc);
+    return W;
+}
+
+/* width and total blocks for one candidate (the chooser's inputs) */
+int cso_coo_block_shape(uint32_t rows, uint32_t nnz, const uint32_t *row, const uint32_t *col, const uint32_t *map,
+                        uint32_t B, uint32_t *width, uint64_t *total_blocks) {
+    const uint32_t RB = (uint32_t) (((uint64_t) rows + B - 1u) / B);
+    uint32_t *off = (uint32_t *) malloc(((size_t) RB + 1u) * sizeof(uint32_t));
+    uint32_t *bc = (uint32_t *) malloc(((size_t) nnz + 1u) * sizeof(uint32_t));
+    int ok = off && bc && coo_block_cols(rows, nnz, row, col, map, B, off, bc, width, total_blocks);
+    free(off);
+    free(bc);
+    return ok;
+}

@@ -137,6 +137,15 @@ void cso_bell_bucket_plan(uint32_t rows, uint32_t B, uint32_t W, const uint32_t 
 uint64_t cso_bell_estimate_bucketed_bytes(uint32_t rows, uint32_t B, const uint32_t *order,
                                           const uint32_t *width_sorted, uint32_t RB, uint32_t buckets);
 uint32_t cso_bell_choose_ingest_bucket_count(uint32_t rows, uint32_t B, uint32_t W, const uint32_t *bci);
+/* ---- COO -> Blocked-ELL (src/convert/blocked_ell_from_compressed.cuh:105-257,349-437,
+ *      src/convert/blocked_ell_from_coo_cuda.cuh:179-198) ---- */
+/* Returns the ell width (bci [RB x W], out_val [rows x W*B] when non-null), -1 on a
+ * row out of range; nnz_out[0] host count, nnz_out[1] CUDA-path count. */
+long long cso_blocked_ell_from_coo(uint32_t rows, uint32_t cols, uint32_t nnz, const uint32_t *row,
+                                   const uint32_t *col, const uint16_t *val, const uint32_t *map, uint32_t B,
+                                   uint32_t *bci, uint16_t *out_val, uint64_t *nnz_out, uint64_t *total_blocks);
+int cso_coo_block_shape(uint32_t rows, uint32_t nnz, const uint32_t *row, const uint32_t *col, const uint32_t *map,
+                        uint32_t B, uint32_t *width, uint64_t *total_blocks);
 
 #ifdef __cplusplus
 }

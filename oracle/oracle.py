@@ -370,6 +370,53 @@ def bell_choose_ingest_bucket_count(rows, B, ell_cols, bci):
     f.restype = u32
     return f(u32(rows), u32(B), u32(ell_cols // B if B else 0), _p(np.ascontiguousarray(bci, np.uint32)))
 
+
+class HostCoo(C.Structure):
+    _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("storage", vp), ("rowIdx", vp), ("colIdx", vp),
+                ("val", vp)]
+
+
+def blocked_ell_from_coo(rows, cols, row, col, val, B, fmap=None):
+    """Restated convert::blocked_ell_from_coo (blocked_ell_from_compressed.cuh:349-437): ell width,
+    block columns, values, nnz (host count, GPU-path count) and total blocks; None when a
+    row index is out of range."""
+    f = lib().cso_blocked_ell_from_coo
+    f.restype = C.c_longlong
+    row, col = np.ascontiguousarray(row, np.uint32), np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.uint16)
+    m = None if fmap is None else np.ascontiguousarray(fmap, np.uint32)
+    nz, tot = np.zeros(2, np.uint64), C.c_uint64()
+    W = f(u32(rows), u32(cols), u32(len(row)), _p(row), _p(col), _p(val), _p(m), u32(B), None, None, _p(nz),
+          C.byref(tot))
+    if W < 0:
+        return None
+    RB = (rows + B - 1) // B
+    bci, v = np.zeros(max(RB * W, 1), np.uint32), np.zeros(max(rows * W * B, 1), np.uint16)
+    f(u32(rows), u32(cols), u32(len(row)), _p(row), _p(col), _p(val), _p(m), u32(B), _p(bci), _p(v), _p(nz),
+      C.byref(tot))
+    return {"ell_width": int(W), "ell_cols": int(W) * B, "bci": bci[:RB * W], "val": v[:rows * W * B],
+            "nnz_host": int(nz[0]), "nnz_gpu": int(nz[1]), "total_blocks": tot.value}
+
+
+def choose_block_size_from_coo(rows, cols, row, col, B_candidates, fmap=None):
+    """choose_blocked_ell_block_size_from_coo restated: (block_size, fill_ratio, padded_bytes)."""
+    f = lib().cso_coo_block_shape
+    row, col = np.ascontiguousarray(row, np.uint32), np.ascontiguousarray(col, np.uint32)
+    m = None if fmap is None else np.ascontiguousarray(fmap, np.uint32)
+    best = None
+    for B in B_candidates:
+        if B == 0:
+            continue
+        w, tot = C.c_uint32(), C.c_uint64()
+        assert f(u32(rows), u32(len(row)), _p(row), _p(col), _p(m), u32(B), C.byref(w), C.byref(tot)) == 1
+        RB = (rows + B - 1) // B
+        padded = rows * w.value * B * 2
+        fill = 1.0 if (RB == 0 or w.value == 0) else tot.value / float(RB * w.value)
+        if (best is None or padded + 1 < best[2] or (padded == best[2] and fill > best[1] + 1e-9)
+                or (padded == best[2] and fill + 1e-9 >= best[1] and B > best[0])):
+            best = (B, fill, padded)
+    return best
+
 # ---------------------------------------------------------------------------
 # the reference's own code (compiled from its sources into _ref/)
 # ---------------------------------------------------------------------------
@@ -529,6 +576,82 @@ def ref_choose_sliced_ell_slice_rows(rows, cols, ptr, idx, val, candidates):
     if ok != 1:
         return None
     return {k: getattr(out, k) for k, _ in SlicedTune._fields_}
+
+
+def host_coo(rows, cols, row, col, val):
+    h = HostCoo()
+    h.rows, h.cols, h.nnz = rows, cols, len(row)
+    h.rowIdx, h.colIdx, h.val = _p(row), _p(col), _p(val)
+    return h
+
+
+def _bell_result(dst, B, free):
+    rb = (dst.rows + B - 1) // B
+    W = dst.ell_cols // B if B else 0
+    bci = np.ctypeslib.as_array(C.cast(dst.blockColIdx, C.POINTER(u32)), (rb * W,)).copy() if rb * W else \
+        np.zeros(0, np.uint32)
+    n = dst.rows * dst.ell_cols
+    v = np.ctypeslib.as_array(C.cast(dst.val, C.POINTER(C.c_uint16)), (n,)).copy() if n else np.zeros(0, np.uint16)
+    res = {"ell_cols": dst.ell_cols, "ell_width": W, "bci": bci, "val": v, "nnz": dst.nnz, "rows": dst.rows,
+           "cols": dst.cols}
+    if dst.storage:
+        free(dst.storage)
+    return res
+
+
+def ref_blocked_ell_from_coo(rows, cols_src, cols, row, col, val, B, fmap=None):
+    """convert::blocked_ell_from_coo of the reference (host loops)."""
+    row, col = np.ascontiguousarray(row, np.uint32), np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.uint16)
+    m = None if fmap is None else np.ascontiguousarray(fmap, np.uint32)
+    src = host_coo(rows, cols_src, row, col, val)
+    dst = HostBlockedEll()
+    r = ref()
+    r.csref_blocked_ell_from_coo.argtypes = [vp, u32, vp, C.c_uint, vp]
+    ok = r.csref_blocked_ell_from_coo(C.byref(src), cols, _p(m), B, C.byref(dst))
+    return _bell_result(dst, B, r.csref_free) if ok == 1 else None
+
+
+def ref_choose_block_size_from_coo(rows, cols_src, cols, row, col, val, candidates, fmap=None):
+    row, col = np.ascontiguousarray(row, np.uint32), np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.uint16)
+    m = None if fmap is None else np.ascontiguousarray(fmap, np.uint32)
+    src = host_coo(rows, cols_src, row, col, val)
+    c = (C.c_uint * len(candidates))(*candidates)
+    out = BlockedTune()
+    r = ref()
+    r.csref_choose_blocked_ell_block_size_from_coo.argtypes = [vp, u32, vp, vp, C.c_uint, vp]
+    ok = r.csref_choose_blocked_ell_block_size_from_coo(C.byref(src), cols, _p(m), c, len(candidates), C.byref(out))
+    return (out.block_size, out.fill_ratio, out.padded_bytes) if ok == 1 else None
+
+
+def ref_gpu_blocked_ell_from_coo_cuda(rows, cols_src, cols, row, col, val, B, fmap=None):
+    """convert::blocked_ell_from_coo_cuda of the reference, run on the GPU."""
+    row, col = np.ascontiguousarray(row, np.uint32), np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.uint16)
+    m = None if fmap is None else np.ascontiguousarray(fmap, np.uint32)
+    src = host_coo(rows, cols_src, row, col, val)
+    dst = HostBlockedEll()
+    g = ref_gpu()
+    g.csrefgpu_blocked_ell_from_coo_cuda.argtypes = [vp, u32, vp, C.c_uint, vp]
+    g.csrefgpu_free.argtypes = [vp]
+    g.csrefgpu_free.restype = None
+    ok = g.csrefgpu_blocked_ell_from_coo_cuda(C.byref(src), cols, _p(m), B, C.byref(dst))
+    return _bell_result(dst, B, g.csrefgpu_free) if ok == 1 else None
+
+
+def ref_gpu_choose_block_size_from_coo_cuda(rows, cols_src, cols, row, col, val, candidates, fmap=None):
+    row, col = np.ascontiguousarray(row, np.uint32), np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.uint16)
+    m = None if fmap is None else np.ascontiguousarray(fmap, np.uint32)
+    src = host_coo(rows, cols_src, row, col, val)
+    c = (C.c_uint * len(candidates))(*candidates)
+    out = BlockedTune()
+    g = ref_gpu()
+    g.csrefgpu_choose_blocked_ell_block_size_from_coo_cuda.argtypes = [vp, u32, vp, vp, C.c_uint, vp]
+    ok = g.csrefgpu_choose_blocked_ell_block_size_from_coo_cuda(C.byref(src), cols, _p(m), c, len(candidates),
+                                                                C.byref(out))
+    return (out.block_size, out.fill_ratio, out.padded_bytes) if ok == 1 else None
 
 
 _rg = None

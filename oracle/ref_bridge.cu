@@ -8,7 +8,9 @@
 // convert::sliced_ell_from_compressed (src/convert/sliced_ell_from_compressed.cuh:96),
 // convert::choose_sliced_ell_slice_rows_from_compressed (:86),
 // convert::sliced_ell_from_blocked_ell (src/convert/sliced_ell_from_blocked_ell.cuh:233) and
-// convert::choose_sliced_ell_slice_rows_from_blocked_ell (:223).
+// convert::choose_sliced_ell_slice_rows_from_blocked_ell (:223),
+// convert::blocked_ell_from_coo (src/convert/blocked_ell_from_compressed.cuh:349) and
+// convert::choose_blocked_ell_block_size_from_coo (:192).
 // The static_asserts pin the C ABI structs of include/cellshard_b200.h to the
 // reference's format structs and device views, field for field.
 #include "src/convert/blocked_ell_from_compressed.cuh"
@@ -19,6 +21,7 @@
 
 #include <cstddef>
 #include <cstdlib>
+#include <cstring>
 
 using namespace cellshard;
 
@@ -55,6 +58,13 @@ SAME_FIELD(cs_sliced_ell_view, device::sliced_ell_view, slice_rows, slice_rows);
 SAME_FIELD(cs_sliced_ell_view, device::sliced_ell_view, slice_slot_offsets, slice_slot_offsets);
 SAME_FIELD(cs_sliced_ell_view, device::sliced_ell_view, val, val);
 static_assert(sizeof(cs_blocked_ell_tune_result) == sizeof(convert::blocked_ell_tune_result), "tune size");
+static_assert(sizeof(cs_host_coo) == sizeof(sparse::coo), "coo size");
+SAME_FIELD(cs_host_coo, sparse::coo, storage, storage);
+SAME_FIELD(cs_host_coo, sparse::coo, rowIdx, rowIdx);
+SAME_FIELD(cs_host_coo, sparse::coo, val, val);
+static_assert(sizeof(cs_coo_view) == sizeof(device::coo_view), "coo_view size");
+SAME_FIELD(cs_coo_view, device::coo_view, rowIdx, rowIdx);
+SAME_FIELD(cs_coo_view, device::coo_view, val, val);
 static_assert(sizeof(cs_sliced_ell_tune_result) == sizeof(convert::sliced_ell_tune_result), "tune size");
 SAME_FIELD(cs_sliced_ell_tune_result, convert::sliced_ell_tune_result, score, score);
 
@@ -197,5 +207,31 @@ unsigned int csref_sliced_total_slots(const cs_host_sliced_ell *m) {
 }
 
 void csref_free(void *p) { std::free(p); }
+
+int csref_blocked_ell_from_coo(const cs_host_coo *src, uint32_t cols, const uint32_t *feature_to_global,
+                               unsigned int block_size, cs_host_blocked_ell *dst) {
+    sparse::coo s;
+    std::memcpy(&s, src, sizeof(s));
+    s.storage = nullptr;
+    sparse::blocked_ell d;
+    sparse::init(&d);
+    const int ok = convert::blocked_ell_from_coo(&s, cols, feature_to_global, block_size, &d);
+    std::memcpy(dst, &d, sizeof(d));
+    return ok;
+}
+
+int csref_choose_blocked_ell_block_size_from_coo(const cs_host_coo *src, uint32_t cols,
+                                                 const uint32_t *feature_to_global, const unsigned int *candidates,
+                                                 unsigned int count, cs_blocked_ell_tune_result *out) {
+    sparse::coo s;
+    std::memcpy(&s, src, sizeof(s));
+    s.storage = nullptr;
+    convert::blocked_ell_tune_result r{};
+    const int ok = convert::choose_blocked_ell_block_size_from_coo(&s, cols, feature_to_global, candidates, count, &r);
+    out->block_size = r.block_size;
+    out->fill_ratio = r.fill_ratio;
+    out->padded_bytes = r.padded_bytes;
+    return ok;
+}
 
 } // extern "C"

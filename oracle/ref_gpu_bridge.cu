@@ -20,9 +20,12 @@
 #include "src/convert/compressed_transpose_raw.cuh"
 #include "src/convert/sliced_ell_from_compressed.cuh"
 #include "src/convert/filtered_blocked_ell_to_compressed.cuh"
+#include "src/convert/blocked_ell_from_compressed.cuh"
+#include "src/convert/blocked_ell_from_coo_cuda.cuh"
 
 #include "cellshard_b200.h"
 
+#include <cstdlib>
 #include <cstring>
 
 using namespace cellshard;
@@ -383,5 +386,37 @@ int csrefgpu_group_reduce_compressed_timed(const cs_compressed_view *src, const 
     runtime::clear(&ws);
     return ok;
 }
+
+// convert::blocked_ell_from_coo_cuda / choose_blocked_ell_block_size_from_coo_cuda
+// (src/convert/blocked_ell_from_coo_cuda.cuh:666,604): host COO in, host Blocked-ELL out
+int csrefgpu_blocked_ell_from_coo_cuda(const cs_host_coo *src, uint32_t cols, const uint32_t *feature_to_global,
+                                       unsigned int block_size, cs_host_blocked_ell *dst) {
+    sparse::coo s;
+    std::memcpy(&s, src, sizeof(s));
+    s.storage = nullptr;
+    sparse::blocked_ell d;
+    sparse::init(&d);
+    const int ok = convert::blocked_ell_from_coo_cuda(&s, cols, feature_to_global, block_size, &d, 0);
+    std::memcpy(dst, &d, sizeof(d));
+    return ok;
+}
+
+int csrefgpu_choose_blocked_ell_block_size_from_coo_cuda(const cs_host_coo *src, uint32_t cols,
+                                                         const uint32_t *feature_to_global,
+                                                         const unsigned int *candidates, unsigned int count,
+                                                         cs_blocked_ell_tune_result *out) {
+    sparse::coo s;
+    std::memcpy(&s, src, sizeof(s));
+    s.storage = nullptr;
+    convert::blocked_ell_tune_result r{};
+    const int ok =
+        convert::choose_blocked_ell_block_size_from_coo_cuda(&s, cols, feature_to_global, candidates, count, 0, &r);
+    out->block_size = r.block_size;
+    out->fill_ratio = r.fill_ratio;
+    out->padded_bytes = r.padded_bytes;
+    return ok;
+}
+
+void csrefgpu_free(void *p) { std::free(p); }
 
 } // extern "C"

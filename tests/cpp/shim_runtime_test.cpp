@@ -320,6 +320,32 @@ int main(int argc, char **argv) {
         cs::bucket::clear(&pws);
     }
     cs::sparse::clear(&conv);
+    {
+        // the same matrix as COO (entries in reverse order), through the COO chooser and builder
+        std::vector<cs::types::idx_t> cr, cc;
+        std::vector<__half> cv;
+        for (unsigned r = 0; r < hc.rows; ++r)
+            for (unsigned k = hc.majorPtr[r]; k < hc.majorPtr[r + 1u]; ++k) {
+                cr.insert(cr.begin(), r);
+                cc.insert(cc.begin(), hc.minorIdx[k]);
+                cv.insert(cv.begin(), hc.val[k]);
+            }
+        cs::sparse::coo coo{hc.rows, hc.cols, (cs::types::nnz_t) cr.size(), nullptr, cr.data(), cc.data(), cv.data()};
+        const unsigned coo_cands[2] = {2u, 4u};
+        cs::convert::blocked_ell_tune_result ct;
+        cs::sparse::blocked_ell cb;
+        cs::sparse::init(&cb);
+        if (!cs::convert::blocked_ell_from_coo_cuda_auto(&coo, hc.cols, nullptr, coo_cands, 2u, &cb, 0, &ct))
+            return fail(31, "blocked_ell_from_coo_cuda_auto");
+        std::printf("coo.blocked %u %u %u", ct.block_size, cb.ell_cols, cb.nnz);
+        const unsigned cn = ((cb.rows + cb.block_size - 1u) / cb.block_size) * (cb.ell_cols / cb.block_size);
+        std::printf("\ncoo.block_cols");
+        for (unsigned i = 0; i < cn; ++i) std::printf(" %u", cb.blockColIdx[i]);
+        std::printf("\ncoo.values");
+        for (unsigned i = 0; i < cb.rows * cb.ell_cols; ++i) std::printf(" %g", __half2float(cb.val[i]));
+        std::printf("\n");
+        cs::sparse::clear(&cb);
+    }
     const unsigned cands[3] = {16u, 32u, 64u};
     cs::convert::sliced_ell_tune_result tune;
     if (!cs::convert::choose_sliced_ell_slice_rows_from_compressed(&hc, cands, 3u, &tune))

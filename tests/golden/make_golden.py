@@ -19,6 +19,10 @@
    choose_bucket_count_for_sliced_part, src/io/csh5/execution_builders_part.hh)
    compiled into oracle/_ref/libcs_ref_bucket.so, on the Blocked-ELL and
    Sliced-ELL matrices of the conversion cases.
+4. ref_coo.npz -- outputs of the reference's COO -> Blocked-ELL host routines
+   (convert::blocked_ell_from_coo, choose_blocked_ell_block_size_from_coo,
+   src/convert/blocked_ell_from_compressed.cuh) on the conversion cases as
+   shuffled COO, some with repeated (row, column) entries and a column map.
 """
 
 from __future__ import annotations
@@ -216,6 +220,47 @@ def ref_bucketing(conv: dict) -> dict:
     return out
 
 
+COO_BLOCKS = [2, 3, 8, 16]
+COO_CANDIDATES = [2, 4, 8, 16]
+
+
+def coo_case(name, rows, cols, ptr, idx, val, seed):
+    """The CSR case as COO: entries shuffled; every third case repeats a few
+    (row, column) pairs with other values, every second gets a column map."""
+    rng = np.random.default_rng(seed)
+    row = np.repeat(np.arange(rows, dtype=np.uint32), np.diff(ptr.astype(np.int64)))
+    col, v = idx.astype(np.uint32), val.astype(np.uint16)
+    if seed % 3 == 0 and len(row) > 4:
+        k = rng.integers(0, len(row), 4)
+        row, col = np.concatenate([row, row[k]]), np.concatenate([col, col[k]])
+        v = np.concatenate([v, (v[k] ^ 0x0400).astype(np.uint16)])
+    p = rng.permutation(len(row))
+    fmap = rng.permutation(cols).astype(np.uint32) if seed % 2 == 0 else None
+    return row[p].astype(np.uint32), col[p].astype(np.uint32), v[p].astype(np.uint16), fmap
+
+
+def ref_coo(conv: dict) -> dict:
+    from oracle import oracle
+
+    out = {}
+    names = sorted({k.split("/")[0] for k in conv})
+    for seed, name in enumerate(names):
+        rows, cols = (int(x) for x in conv[f"{name}/shape"])
+        row, col, val, fmap = coo_case(name, rows, cols, conv[f"{name}/ptr"], conv[f"{name}/idx"],
+                                       conv[f"{name}/val"], seed)
+        out[f"{name}/coo/row"], out[f"{name}/coo/col"], out[f"{name}/coo/val"] = row, col, val
+        if fmap is not None:
+            out[f"{name}/coo/map"] = fmap
+        for B in COO_BLOCKS:
+            r = oracle.ref_blocked_ell_from_coo(rows, cols, cols, row, col, val, B, fmap)
+            out[f"{name}/coo{B}/bci"], out[f"{name}/coo{B}/val"] = r["bci"], r["val"]
+            out[f"{name}/coo{B}/meta"] = np.array([r["ell_cols"], r["nnz"]], np.uint64)
+        t = oracle.ref_choose_block_size_from_coo(rows, cols, cols, row, col, val, COO_CANDIDATES, fmap)
+        out[f"{name}/coo_choose"] = np.array([t[0], t[2]], np.uint64)
+        out[f"{name}/coo_choose_fill"] = np.array([t[1]], np.float64)
+    return out
+
+
 def main() -> None:
     (HERE / "mask_groups_known_answers.json").write_text(json.dumps(known_answers(), indent=1) + "\n")
     from oracle import oracle
@@ -227,8 +272,9 @@ def main() -> None:
     if not oracle.ref_bucket_available():
         raise SystemExit("oracle/_ref/libcs_ref_bucket.so missing: run `make -C oracle ref`")
     np.savez_compressed(HERE / "ref_bucketing.npz", **ref_bucketing(conv))
+    np.savez_compressed(HERE / "ref_coo.npz", **ref_coo(conv))
     print("wrote", HERE / "mask_groups_known_answers.json", HERE / "ref_conversions.npz",
-          HERE / "ref_bucketing.npz")
+          HERE / "ref_bucketing.npz", HERE / "ref_coo.npz")
 
 
 if __name__ == "__main__":

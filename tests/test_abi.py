@@ -56,6 +56,7 @@ int main(void) {
   S(cs_host_bucketed_blocked_ell) O(cs_host_bucketed_blocked_ell, canonical_to_exec_cols)
   S(cs_host_bucketed_sliced_ell) O(cs_host_bucketed_sliced_ell, canonical_slice_widths)
   S(cs_exec_bucket_plan) O(cs_exec_bucket_plan, value_entries) S(cs_exec_bucket_segments)
+  S(cs_host_coo) O(cs_host_coo, val) S(cs_coo_view) O(cs_coo_view, val)
   return 0;
 }
 """
@@ -85,6 +86,8 @@ PAIRS = {
     "cs_host_bucketed_sliced_ell": _abi.HostBucketedSlicedEll,
     "cs_exec_bucket_plan": _abi.ExecBucketPlan,
     "cs_exec_bucket_segments": _abi.ExecBucketSegments,
+    "cs_host_coo": _abi.HostCoo,
+    "cs_coo_view": _abi.CooView,
 }
 
 
@@ -110,6 +113,7 @@ def test_ctypes_layouts_match_c(tmp_path):
     assert got["cs_host_bucketed_sliced_ell.canonical_slice_widths"] == \
         _abi.HostBucketedSlicedEll.canonical_slice_widths.offset
     assert got["cs_exec_bucket_plan.value_entries"] == _abi.ExecBucketPlan.value_entries.offset
+    assert got["cs_host_coo.val"] == _abi.HostCoo.val.offset and got["cs_coo_view.val"] == _abi.CooView.val.offset
     assert got["cs_batch_sliced_result.view"] == _abi.BatchSlicedResult.view.offset
     assert got["cs_serve_request.group_rows"] == _abi.ServeRequest.group_rows.offset
     assert got["cs_partition_record.host_view"] == _abi.PartitionRecord.host_view.offset

@@ -142,6 +142,14 @@ def test_shim_convert_bucket_transpose_reoptimize(shim_out, orc):
     po, pw = orc.bell_bucket_plan(rows, 2, ref["ell_cols"], ref["bci"])
     assert np.array_equal(o["exec.plan.order"].astype(np.uint32), po)
     assert np.array_equal(o["exec.plan.width"].astype(np.uint32), pw)
+    # the same matrix as reversed COO through the COO chooser (2 / 4) and builder
+    crow = np.repeat(np.arange(rows, dtype=np.uint32), np.diff(ptr.astype(np.int64)))[::-1].copy()
+    ccol, cval = idx[::-1].copy(), val[::-1].copy()
+    cb, _fill, _pad = orc.choose_block_size_from_coo(rows, cols, crow, ccol, (2, 4))
+    cref = orc.blocked_ell_from_coo(rows, cols, crow, ccol, cval, cb)
+    assert list(o["coo.blocked"]) == [cb, cref["ell_cols"], cref["nnz_gpu"]]
+    assert np.array_equal(o["coo.block_cols"].astype(np.uint32), cref["bci"])
+    assert np.array_equal(o["coo.values"].astype(np.float16).view(np.uint16), cref["val"])
     h, score, _ = orc.choose_sliced_slice_rows(rows, int(ptr[-1]), ptr, (16, 32, 64))
     assert o["convert.slice_choice"][0] == h and o["convert.slice_choice"][3] == score
     _nnz, _srt, order, offs = orc.major_nnz_plan(ptr, rows, 2)
