@@ -566,7 +566,18 @@ def coo_lines(lib, timed, emit, csr):
     if cpu is not None:
         ex["cpu_baseline"] = cpu
     emit("coo_blocked_ell_emit", ms_emit, 12 * n + RB * W * 4 + R * W * BLOCK * 2 + 12 * total.value, ex)
-    del row, scr, bci, val
+    # the same entries in random order: a stable sort by row first, then the same CSR kernels
+    perm = torch.randperm(n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(7))
+    row_s, col_s, val_s = row[perm], csr.idx[perm], csr.val[perm]
+    del perm
+    torch.cuda.empty_cache()
+    v.rowIdx, v.colIdx, v.val = ptr(row_s), ptr(col_s), ptr(val_s)
+    ms_plan_u = timed(plan_fn)
+    ms_emit_u = timed(emit_fn)
+    emit("coo_blocked_ell_unordered", ms_plan_u + ms_emit_u, 0,
+         {"plan_ms": ms_plan_u, "emit_ms": ms_emit_u, "rows_per_s": R / ((ms_plan_u + ms_emit_u) * 1e-3),
+          "note": "entries shuffled: stable radix sort by row + gather, then the CSR route; time only"})
+    del row, scr, bci, val, row_s, col_s, val_s
 
 
 def run_convert(args):

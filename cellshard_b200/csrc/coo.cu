@@ -6,10 +6,15 @@
 // (src/convert/blocked_ell_from_coo_cuda.cuh:17-966: 64-bit (row block, block
 // column) keys, CUB sort, head flags, scans, a thread per entry scattering).
 //
-// Here (entries whose rows never decrease -- COO written row by row -- with
-// every mapped column below `cols` take the CSR route instead: row pointers
-// from the row runs, then the library's CSR -> Blocked-ELL shape and emit,
-// which place values in the same order and count nnz the same way):
+// Here, when every mapped column is below `cols` (and the column-block
+// bitmaps of the CSR kernels stay small), the CSR route: entries whose rows
+// never decrease -- COO written row by row -- get row pointers from their row
+// runs; other entries are first stably sorted by column and then by row (rows
+// in order, columns ascending, a repeated (row, column) keeping its entries'
+// COO order) and their columns and values gathered; then the
+// library's CSR -> Blocked-ELL shape and emit, which place a row's values in
+// that order (a repeated column keeps its last value) and count nnz the same
+// way.  Otherwise:
 //   scan    one pass over the entries: rows in range and columns inside
 //           the column map (others dropped and flagged), the largest mapped
 //           column (one small read-back sizes the key)
@@ -37,12 +42,21 @@ constexpr uint32_t kInvalid = 0xffffffffu;
 // words: [0] largest mapped column, [1] dropped entries, [2] width, [3] route
 // (0 two sorts, 1 one sort, 2 CSR), [4] key shift, [5] kept entries, [6] rows
 // decrease somewhere, [7] the CSR route's nnz
-constexpr uint32_t kRouteTwoSorts = 0u, kRouteOneSort = 1u, kRouteCsr = 2u;
+constexpr uint32_t kRouteTwoSorts = 0u, kRouteOneSort = 1u, kRouteCsr = 2u, kRouteCsrSorted = 3u;
+
+// The CSR route's column-block bitmaps (one bit per column block per row
+// block) must stay small next to the entries themselves.
+bool csr_route_fits(uint32_t n, uint32_t rows, uint32_t cols, uint32_t B) {
+    std::size_t bytes = 0u;
+    cs_b200_blocked_ell_scratch_bytes(rows, cols, B, &bytes);
+    return bytes <= ((std::size_t) 64u << 20) || bytes <= (std::size_t) n * 16u;
+}
 
 struct coo_scratch {
     uint32_t *words;
     unsigned long long *shape;   // CSR route: width, pairs
-    uint32_t *csr_ptr, *mcol;    // CSR route: row pointers, mapped columns
+    uint32_t *csr_ptr, *mcol;    // CSR route: row pointers, mapped (and row-sorted) columns
+    uint16_t *sval;              // CSR route after the row sort: values in row order
     void *csr_tmp;
     uint32_t *keys, *rkeys, *skeys, *spos, *pos1, *flags, *gid, *gs, *rb_count, *rb_off;
     void *sort_tmp, *scan_tmp;
@@ -57,8 +71,9 @@ void carve(void *base, uint32_t n, uint32_t rows, uint32_t cols, uint32_t B, coo
     x->shape = c.take<unsigned long long>(2);
     x->csr_ptr = c.take<uint32_t>((std::size_t) rows + 1u);
     x->mcol = c.take<uint32_t>(n1);
+    x->sval = c.take<uint16_t>(n1);
     x->csr_bytes = 0u;
-    cs_b200_blocked_ell_scratch_bytes(rows, cols, B, &x->csr_bytes);
+    if (B != 0u && csr_route_fits(n, rows, cols, B)) cs_b200_blocked_ell_scratch_bytes(rows, cols, B, &x->csr_bytes);
     x->csr_tmp = c.take<char>(x->csr_bytes);
     x->keys = c.take<uint32_t>(n1);
     x->rkeys = c.take<uint32_t>(n1);
@@ -244,6 +259,20 @@ __global__ void __launch_bounds__(256) coo_map_cols_kernel(uint32_t n, const uin
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = map[col[i]];
 }
 
+// CSR route after the row sort: columns (mapped) and values in row order.
+__global__ void __launch_bounds__(256) coo_gather_rows_kernel(uint32_t n, const uint32_t *__restrict__ pos,
+                                                              const uint32_t *__restrict__ col,
+                                                              const uint32_t *__restrict__ map,
+                                                              const uint16_t *__restrict__ val,
+                                                              uint32_t *__restrict__ out_col,
+                                                              uint16_t *__restrict__ out_val) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = pos[i];
+        out_col[i] = mapped(col, map, p);
+        out_val[i] = val[p];
+    }
+}
+
 __global__ void coo_nnz_from_csr_kernel(const uint32_t *__restrict__ count, unsigned long long *__restrict__ nnz) {
     if (threadIdx.x == 0u && blockIdx.x == 0u && nnz != nullptr) {
         nnz[0] += *count;
@@ -292,8 +321,11 @@ coo_decode decoder(const cs_coo_view *src, const uint32_t *map, const coo_scratc
     return d;
 }
 
-// The CSR view of the CSR route (row pointers and mapped columns in the scratch).
-cs_compressed_view csr_of(const cs_coo_view *src, const uint32_t *map, uint32_t cols, const coo_scratch &x) {
+// The CSR view of the CSR route (row pointers and mapped or row-sorted columns
+// in the scratch).
+cs_compressed_view csr_of(const cs_coo_view *src, const uint32_t *map, uint32_t cols, const coo_scratch &x,
+                          bool sorted) {
+    if (sorted) return cs_compressed_view{src->rows, cols, src->nnz, CS_COMPRESSED_BY_ROW, x.csr_ptr, x.mcol, x.sval};
     return cs_compressed_view{src->rows, cols, src->nnz, CS_COMPRESSED_BY_ROW, x.csr_ptr,
                               map != nullptr ? x.mcol : src->colIdx, src->val};
 }
@@ -330,18 +362,39 @@ int coo_plan(const cs_coo_view *src, const uint32_t *map, uint32_t cols, uint32_
         return 0;
     s->n_valid = n - w[1];
     uint32_t route;
-    if (w[1] == 0u && w[6] == 0u && w[0] < cols) {
-        // rows never decrease and every column fits: the CSR route
-        route = kRouteCsr;
-        coo_row_ptr_kernel<<<grid_for((const void *) coo_row_ptr_kernel, n), 256, 0, stream>>>(n, src->rows,
-                                                                                              src->rowIdx, x.csr_ptr);
-        if (!launch_ok("coo_row_ptr_kernel")) return 0;
-        if (map != nullptr) {
+    if (w[1] == 0u && w[0] < cols && x.csr_bytes != 0u) {
+        // every column fits: the CSR route, after a stable sort by row when rows decrease somewhere
+        const bool sorted = w[6] != 0u;
+        route = sorted ? kRouteCsrSorted : kRouteCsr;
+        const uint32_t *rows_in_order = src->rowIdx;
+        if (sorted) {
+            // stable by (mapped) column, then stable by row: rows in order, columns ascending
+            // inside a row, repeated (row, column) entries next to each other in COO order
+            const uint32_t *ckeys = src->colIdx;
+            if (map != nullptr) {
+                coo_map_cols_kernel<<<grid_for((const void *) coo_map_cols_kernel, n), 256, 0, stream>>>(
+                    n, src->colIdx, map, x.keys);
+                if (!launch_ok("coo_map_cols_kernel")) return 0;
+                ckeys = x.keys;
+            }
+            if (!sort_pairs_u32(ckeys, nullptr, n, x.flags, x.pos1, x.sort_tmp, x.sort_bytes, stream)) return 0;
+            gather_kernel<<<grid_for((const void *) gather_kernel, n), 256, 0, stream>>>(n, src->rowIdx, x.pos1,
+                                                                                       x.keys);
+            if (!launch_ok("gather_kernel")) return 0;
+            if (!sort_pairs_u32(x.keys, x.pos1, n, x.skeys, x.spos, x.sort_tmp, x.sort_bytes, stream)) return 0;
+            coo_gather_rows_kernel<<<grid_for((const void *) coo_gather_rows_kernel, n), 256, 0, stream>>>(
+                n, x.spos, src->colIdx, map, src->val, x.mcol, x.sval);
+            if (!launch_ok("coo_gather_rows_kernel")) return 0;
+            rows_in_order = x.skeys;
+        } else if (map != nullptr) {
             coo_map_cols_kernel<<<grid_for((const void *) coo_map_cols_kernel, n), 256, 0, stream>>>(n, src->colIdx,
                                                                                                    map, x.mcol);
             if (!launch_ok("coo_map_cols_kernel")) return 0;
         }
-        const cs_compressed_view v = csr_of(src, map, cols, x);
+        coo_row_ptr_kernel<<<grid_for((const void *) coo_row_ptr_kernel, n), 256, 0, stream>>>(n, src->rows,
+                                                                                              rows_in_order, x.csr_ptr);
+        if (!launch_ok("coo_row_ptr_kernel")) return 0;
+        const cs_compressed_view v = csr_of(src, map, cols, x, sorted);
         unsigned long long shape[2] = {0, 0};
         if (!cuda_ok(cudaMemsetAsync(x.shape, 0, 16, stream), "shape clear") ||
             !cs_b200_blocked_ell_shape(&v, B, (uint64_t *) x.shape, x.csr_tmp, x.csr_bytes, status,
@@ -429,8 +482,8 @@ int coo_emit(const cs_coo_view *src, const uint32_t *map, uint32_t cols, const v
         set_error("coo_blocked_ell_emit: null destination arrays");
         return 0;
     }
-    if (route == kRouteCsr) {
-        const cs_compressed_view v = csr_of(src, map, cols, x);
+    if (route == kRouteCsr || route == kRouteCsrSorted) {
+        const cs_compressed_view v = csr_of(src, map, cols, x, route == kRouteCsrSorted);
         if (!cuda_ok(cudaMemsetAsync(x.words + 7, 0, 4, stream), "csr nnz clear") ||
             !cs_b200_blocked_ell_emit(&v, dst, x.words + 7, x.csr_tmp, x.csr_bytes, nullptr,
                                       reinterpret_cast<cs_stream_t>(stream)))

@@ -130,8 +130,10 @@ def test_wide_keys_take_two_sorts(cuda, orc):
 
 
 def test_rows_out_of_range_are_dropped_and_flagged(cuda, orc):
+    """Dropped rows send the entries through the (row block, block column) sort
+    route, here with repeated entries too."""
     rows, cols = 100, 120
-    row, col, val = _coo(rows, cols, 0.1, 5)
+    row, col, val = _coo(rows, cols, 0.1, 5, dups=6)
     bad = row.copy()
     bad[::17] = rows + 3
     out, counts, status, _ = _run(rows, cols, bad, col, val, 8)
