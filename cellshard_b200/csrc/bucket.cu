@@ -35,7 +35,7 @@ namespace {
 
 constexpr unsigned kSortThreads = 256;
 constexpr unsigned kSortWarps = kSortThreads / 32;
-constexpr unsigned kTileKeys = 2048; // 8 warps x 256 keys
+constexpr unsigned kTileKeys = 4096; // 8 warps x 512 keys
 constexpr unsigned kKeysPerWarp = kTileKeys / kSortWarps;
 constexpr unsigned kRadix = 256;
 
@@ -113,7 +113,11 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
 
 // One stable counting-sort pass over digit (key >> shift) & 255.  vals ==
 // nullptr means the identity (the row ids).  Tiles are taken in start order so
-// every look-back target belongs to a CTA that is already running.
+// every look-back target belongs to a CTA that is already running.  The tile
+// is ranked in registers, placed in shared memory grouped by digit, and
+// written from there: consecutive threads store consecutive positions of one
+// digit's run, so the global stores come out as runs instead of one sector
+// per key.
 __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
     const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, uint32_t n, uint32_t shift,
     const uint32_t *__restrict__ ghist, unsigned long long *__restrict__ look, uint32_t *__restrict__ tile_counter,
@@ -122,6 +126,8 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
     __shared__ uint32_t wc[kSortWarps][kRadix];
     __shared__ uint32_t scan33[33];
     __shared__ uint32_t tile_s;
+    __shared__ uint32_t dg_global[kRadix], dg_local[kRadix];
+    __shared__ uint32_t s_keys[kTileKeys], s_vals[kTileKeys];
     if (skip_below != 0u && *max_key < skip_below) return; // uniform: the pass changes nothing
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
@@ -129,11 +135,17 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
     __syncthreads();
     const uint32_t t = tile_s;
     const uint32_t wbase = t * kTileKeys + warp * kKeysPerWarp;
-    uint32_t kk[kKeysPerWarp / 32u], pk[kKeysPerWarp / 32u];
+    uint32_t kk[kKeysPerWarp / 32u], pk[kKeysPerWarp / 32u], vv[kKeysPerWarp / 32u];
+    // keys and values of the tile are loaded up front (all in flight together)
 #pragma unroll
     for (uint32_t b = 0; b < kKeysPerWarp / 32u; ++b) {
         const uint32_t k = wbase + b * 32u + lane;
-        kk[b] = k < n ? __ldcg(keys + k) : 0u;
+        kk[b] = k < n ? __ldcs(keys + k) : 0u;
+        vv[b] = vals != nullptr ? (k < n ? __ldcs(vals + k) : 0u) : k;
+    }
+#pragma unroll
+    for (uint32_t b = 0; b < kKeysPerWarp / 32u; ++b) {
+        const uint32_t k = wbase + b * 32u + lane;
         const uint32_t d = k < n ? (kk[b] >> shift) & 0xffu : kRadix;
         pk[b] = __match_any_sync(0xffffffffu, d);
         if (d < kRadix && lane == (unsigned) (__ffs(pk[b]) - 1)) wc[warp][d] += __popc(pk[b]);
@@ -169,10 +181,14 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
             if (!ok) atomicOr(status, 1u);
             st_release_u64(mine, kLookInclusive | (unsigned long long) (excl + cnt));
         }
-        // global base of digit d: exclusive scan of the pass's digit totals
-        uint32_t tot;
+        // global base of digit d: exclusive scan of the pass's digit totals;
+        // tile-local base: exclusive scan of this tile's digit counts
+        uint32_t tot, tile_tot;
         const uint32_t gbase = block_exclusive_scan(ghist[d], scan33, tot);
-        uint32_t run = gbase + excl;
+        const uint32_t lbase = block_exclusive_scan(cnt, scan33, tile_tot);
+        dg_global[d] = gbase + excl;
+        dg_local[d] = lbase;
+        uint32_t run = lbase;
 #pragma unroll
         for (unsigned w = 0; w < kSortWarps; ++w) {
             const uint32_t c = wc[w][d];
@@ -190,11 +206,20 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(
         if (d < kRadix) pos = wc[warp][d] + __popc(pk[b] & lt);
         __syncwarp();
         if (d < kRadix) {
-            out_keys[pos] = kk[b];
-            out_vals[pos] = vals != nullptr ? __ldcg(vals + k) : k;
+            s_keys[pos] = kk[b];
+            s_vals[pos] = vv[b];
             if (lane == (unsigned) (__ffs(pk[b]) - 1)) wc[warp][d] += __popc(pk[b]);
         }
         __syncwarp();
+    }
+    __syncthreads();
+    const uint32_t tile_n = n - t * kTileKeys < kTileKeys ? n - t * kTileKeys : kTileKeys;
+    for (uint32_t i = threadIdx.x; i < tile_n; i += kSortThreads) {
+        const uint32_t key = s_keys[i];
+        const uint32_t d = (key >> shift) & 0xffu;
+        const uint32_t g = dg_global[d] + (i - dg_local[d]);
+        out_keys[g] = key;
+        out_vals[g] = s_vals[i];
     }
 }
 
