@@ -61,6 +61,11 @@ class CooView(C.Structure):
                 ("_pad", C.c_uint64)]
 
 
+class CspackInfo(C.Structure):
+    _fields_ = [("format", u32), ("rows", u32), ("cols", u32), ("nnz", u32), ("axis", u32), ("block_size", u32),
+                ("ell_cols", u32), ("slice_count", u32), ("total_slots", u32)]
+
+
 class HostBucketedBlockedEll(C.Structure):
     _fields_ = [("rows", u32), ("cols", u32), ("nnz", u32), ("segment_count", u32), ("segments", vp),
                 ("segment_row_offsets", vp), ("exec_to_canonical_rows", vp), ("canonical_to_exec_rows", vp),
@@ -197,6 +202,15 @@ PROTOTYPES: dict[str, tuple] = {
                                                     vp, sz, vp, vp]),
     "cs_b200_filter_blocked_ell_emit": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
                                                    vp, vp]),
+    "cs_b200_cspack_peek": (C.c_int, [C.c_char_p, P(CspackInfo)]),
+    "cs_b200_cspack_store_blocked_ell": (C.c_int, [C.c_char_p, P(BlockedEllView)]),
+    "cs_b200_cspack_load_blocked_ell": (C.c_int, [C.c_char_p, P(BlockedEllView)]),
+    "cs_b200_cspack_store_sliced_ell": (C.c_int, [C.c_char_p, P(SlicedEllView)]),
+    "cs_b200_cspack_load_sliced_ell": (C.c_int, [C.c_char_p, P(SlicedEllView)]),
+    "cs_b200_cspack_store_compressed": (C.c_int, [C.c_char_p, P(CompressedView)]),
+    "cs_b200_cspack_load_compressed": (C.c_int, [C.c_char_p, P(CompressedView)]),
+    "cs_b200_cspack_store_coo": (C.c_int, [C.c_char_p, P(CooView)]),
+    "cs_b200_cspack_load_coo": (C.c_int, [C.c_char_p, P(CooView)]),
     "cs_b200_coo_blocked_ell_scratch_bytes": (C.c_int, [u32, u32, u32, u32, P(sz)]),
     "cs_b200_coo_blocked_ell_plan": (C.c_int, [P(CooView), vp, u32, u32, vp, sz, P(u32), P(u64), vp, vp]),
     "cs_b200_coo_blocked_ell_emit": (C.c_int, [P(CooView), vp, u32, vp, sz, P(BlockedEllView), vp, vp]),

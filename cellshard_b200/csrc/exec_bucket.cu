@@ -28,16 +28,19 @@
 //   wide as its last row, exactly `requested` non-empty segments before
 //   equal-width neighbours merge) with its monotone convex-hull and its tie
 //   rules.  The programme is sequential over the sorted widths: it runs on the
-//   host over the widths copied back (4 bytes per row), as in the reference;
-//   counting, sorting and copying run on the device.  One programme of 8
+//   host over the widths copied back (4 bytes per row), as in the reference,
+//   its levels pipelined over host threads; counting, sorting and copying run
+//   on the device.  One programme of 8
 //   levels serves all eight candidates of choose_bucket_count_for_sliced_part
 //   (:1572-1596): level k's costs and cuts do not depend on how many levels
 //   follow.
 #include "common.cuh"
 
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <thread>
 #include <vector>
 
 namespace csb {
@@ -645,51 +648,95 @@ struct sliced_split {
     uint32_t rows = 0, K = 0;
     std::unique_ptr<uint32_t[]> cuts; // (K + 1) x (rows + 1)
     std::vector<uint64_t> cost_at_rows; // level k's cost of all rows
-    bool run(const std::vector<uint32_t> &w, uint32_t levels) {
-        rows = (uint32_t) w.size();
-        K = levels;
-        const uint64_t fixed = packed_sell_bytes(1u, 0u), slot = 6u, inf = ~0ull / 4u;
-        struct line {
-            int64_t slope, icpt;
-            uint32_t cut;
-        };
+
+    static constexpr uint64_t kInf = ~0ull / 4u;
+    static constexpr uint32_t kBlockRows = 4096u;
+
+    struct line {
+        int64_t slope, icpt;
+        uint32_t cut;
+    };
+
+    // One level over rows k..rows: prev = level k-1's costs, curr = this
+    // level's.  When `ready` is set, level k-1 runs in another thread and
+    // `ready` holds the last row it has finished: rows are taken in blocks
+    // once the previous level has passed them (bounded only by its progress,
+    // which always advances).
+    void level(uint32_t k, const std::vector<uint32_t> &w, const uint64_t *prev, uint64_t *curr,
+               const std::atomic<uint32_t> *ready, std::atomic<uint32_t> *done) {
+        const uint64_t fixed = packed_sell_bytes(1u, 0u), slot = 6u;
         auto at = [](const line &l, uint32_t x) { return l.icpt + l.slope * (int64_t) x; };
         auto redundant = [](const line &a, const line &m, const line &b) {
             const __int128 left = (__int128) (b.icpt - a.icpt) * (__int128) (a.slope - m.slope);
             const __int128 right = (__int128) (m.icpt - a.icpt) * (__int128) (a.slope - b.slope);
             return left <= right;
         };
-        std::vector<uint64_t> prev((std::size_t) rows + 1u, inf), curr((std::size_t) rows + 1u, inf);
-        std::vector<line> hull((std::size_t) rows + 1u);
-        // entries (k, r < k) are never read; every (k, r >= k) is written below
-        cuts.reset(new uint32_t[((std::size_t) K + 1u) * ((std::size_t) rows + 1u)]);
-        cost_at_rows.assign((std::size_t) K + 1u, inf);
-        prev[0] = 0u;
-        for (uint32_t k = 1; k <= K; ++k) {
-            std::size_t n = 0u, h = 0u;
-            // only entries r >= k of this level are read by the next (its first line
-            // uses row k, its loop rows above k), and all of them are written below
-            if (prev[k - 1u] != inf) hull[n++] = line{-(int64_t) slot * (int64_t) (k - 1u), (int64_t) prev[k - 1u], k - 1u};
-            uint32_t *cut = cuts.get() + (std::size_t) k * (rows + 1u);
-            for (uint32_t r = k; r <= rows; ++r) {
+        std::unique_ptr<line[]> hull(new line[(std::size_t) rows + 1u]); // written before read
+        std::size_t n = 0u, h = 0u;
+        uint32_t *cut = cuts.get() + (std::size_t) k * (rows + 1u);
+        uint32_t avail = ready != nullptr ? ready->load(std::memory_order_acquire) : rows;
+        while (avail < k - 1u) {
+            std::this_thread::yield();
+            avail = ready->load(std::memory_order_acquire);
+        }
+        if (prev[k - 1u] != kInf) hull[n++] = line{-(int64_t) slot * (int64_t) (k - 1u), (int64_t) prev[k - 1u], k - 1u};
+        for (uint32_t r0 = k; r0 <= rows; r0 += kBlockRows) {
+            const uint32_t r1 = r0 + kBlockRows - 1u < rows ? r0 + kBlockRows - 1u : rows;
+            while (avail < r1) {
+                std::this_thread::yield();
+                avail = ready->load(std::memory_order_acquire);
+            }
+            for (uint32_t r = r0; r <= r1; ++r) {
                 const uint32_t x = w[r - 1u];
                 while (h + 1u < n && at(hull[h + 1u], x) < at(hull[h], x)) ++h;
                 if (h < n) {
                     curr[r] = fixed + slot * (uint64_t) x * (uint64_t) r + (uint64_t) at(hull[h], x);
                     cut[r] = hull[h].cut;
                 } else {
-                    curr[r] = inf;
+                    curr[r] = kInf;
                     cut[r] = 0u;
                 }
-                if (prev[r] != inf) {
+                if (prev[r] != kInf) {
                     const line l{-(int64_t) slot * (int64_t) r, (int64_t) prev[r], r};
                     while (n >= h + 2u && redundant(hull[n - 2u], hull[n - 1u], l)) --n;
                     hull[n++] = l;
                 }
             }
-            prev.swap(curr);
-            cost_at_rows[k] = prev[rows];
+            if (done != nullptr) done->store(r1, std::memory_order_release);
         }
+        if (done != nullptr) done->store(rows, std::memory_order_release);
+    }
+
+    // Levels 1..K.  Each level's loop is sequential (its hull depends on every
+    // earlier row), but level k only needs level k-1's costs of rows up to the
+    // one it is at, so the levels run as a pipeline, one thread each, level k
+    // a block of rows behind level k-1; every cost and cut is the one the
+    // sequential order computes.
+    bool run(const std::vector<uint32_t> &w, uint32_t levels) {
+        rows = (uint32_t) w.size();
+        K = levels;
+        // level 0: no rows cost 0, any row unreachable; a level k >= 1 writes
+        // every entry r >= k, the only ones level k + 1 reads
+        std::vector<std::unique_ptr<uint64_t[]>> cost((std::size_t) K + 1u);
+        for (auto &c : cost) c.reset(new uint64_t[(std::size_t) rows + 1u]);
+        for (uint32_t r = 0; r <= rows; ++r) cost[0][r] = r == 0u ? 0u : kInf;
+        cuts.reset(new uint32_t[((std::size_t) K + 1u) * ((std::size_t) rows + 1u)]);
+        cost_at_rows.assign((std::size_t) K + 1u, kInf);
+        const unsigned hw = std::thread::hardware_concurrency();
+        if (K <= 1u || rows < 2u * kBlockRows || K > 16u || hw < 2u) {
+            for (uint32_t k = 1; k <= K; ++k) level(k, w, cost[k - 1u].get(), cost[k].get(), nullptr, nullptr);
+        } else {
+            std::vector<std::atomic<uint32_t>> progress((std::size_t) K + 1u);
+            progress[0].store(rows);
+            for (uint32_t k = 1; k <= K; ++k) progress[k].store(0u);
+            std::vector<std::thread> th;
+            th.reserve(K);
+            for (uint32_t k = 1; k <= K; ++k)
+                th.emplace_back([&, k] { level(k, w, cost[k - 1u].get(), cost[k].get(), &progress[k - 1u],
+                                               &progress[k]); });
+            for (auto &t : th) t.join();
+        }
+        for (uint32_t k = 1; k <= K; ++k) cost_at_rows[k] = cost[k][rows];
         return true;
     }
     // Segments of the k-level split after equal-width neighbours merge.
@@ -698,7 +745,7 @@ struct sliced_split {
         offs->assign(1, 0u);
         widths->clear();
         if (rows == 0u) return true;
-        if (cost_at_rows[k] == ~0ull / 4u) return false;
+        if (cost_at_rows[k] == kInf) return false;
         std::vector<uint32_t> raw_off((std::size_t) k + 1u), raw_w(k);
         uint32_t r = rows;
         raw_off[k] = rows;

@@ -422,3 +422,85 @@ def blocked_ell_from_coo(rows: int, cols_src: int, row_idx: torch.Tensor, col_id
     out.bci = out.bci[:RB * W]
     out.val = out.val[:rows * W * block_size]
     return out, counts, int(status.item()), total.value
+
+
+def cspack_store(path, m) -> None:
+    """Writes a device CSR / Blocked-ELL / Sliced-ELL as one .cspack raw record
+    (the reference's store_*_raw layout, src/io/pack/packfile.cu)."""
+    lib = _abi.load()
+    torch.cuda.synchronize()
+    p = str(path).encode()
+    v = m.view()
+    fn = {CSR: lib.cs_b200_cspack_store_compressed, BlockedELL: lib.cs_b200_cspack_store_blocked_ell,
+          SlicedELL: lib.cs_b200_cspack_store_sliced_ell}[type(m)]
+    _abi.check(fn(p, C.byref(v)), "cspack store")
+
+
+def cspack_peek(path) -> _abi.CspackInfo:
+    info = _abi.CspackInfo()
+    _abi.check(_abi.load().cs_b200_cspack_peek(str(path).encode(), C.byref(info)), "cspack peek")
+    return info
+
+
+def cspack_load(path):
+    """Reads one .cspack raw record into device memory (CSR, Blocked-ELL or Sliced-ELL;
+    COO records come back as (rows, cols, row_idx, col_idx, val))."""
+    lib = _abi.load()
+    info = cspack_peek(path)
+    p = str(path).encode()
+    dev = dict(device="cuda")
+    if info.format == 6:
+        B = info.block_size
+        rb = (info.rows + B - 1) // B if B else 0
+        W = info.ell_cols // B if B else 0
+        m = BlockedELL(info.rows, info.cols, B, info.ell_cols, torch.empty(max(rb * W, 1), dtype=torch.int32, **dev),
+                       torch.empty(max(info.rows * info.ell_cols, 1), dtype=torch.float16, **dev), info.nnz)
+        v = m.view()
+        v.blockColIdx, v.val = m.bci.data_ptr(), m.val.data_ptr()
+        _abi.check(lib.cs_b200_cspack_load_blocked_ell(p, C.byref(v)), "cspack load")
+        m.bci, m.val = m.bci[:rb * W], m.val[:info.rows * info.ell_cols]
+        return m
+    if info.format == 7:
+        S, T = info.slice_count, info.total_slots
+        m = SlicedELL(info.rows, info.cols, info.nnz, 0, torch.empty(S + 1, dtype=torch.int32, **dev),
+                      torch.empty(max(S, 1), dtype=torch.int32, **dev), torch.empty(max(S, 1), dtype=torch.int32, **dev),
+                      torch.empty(max(T, 1), dtype=torch.int32, **dev), torch.empty(max(T, 1), dtype=torch.float16, **dev))
+        v = m.view()
+        v.slice_row_offsets, v.slice_widths, v.slice_slot_offsets = (m.slice_row_offsets.data_ptr(),
+                                                                     m.slice_widths.data_ptr(),
+                                                                     m.slice_slot_offsets.data_ptr())
+        v.col_idx, v.val = m.col_idx.data_ptr(), m.val.data_ptr()
+        _abi.check(lib.cs_b200_cspack_load_sliced_ell(p, C.byref(v)), "cspack load")
+        m.slice_widths, m.slice_slot_offsets = m.slice_widths[:S], m.slice_slot_offsets[:S]
+        m.col_idx, m.val = m.col_idx[:T], m.val[:T]
+        return m
+    if info.format == 2:
+        major = info.cols if info.axis == COMPRESSED_BY_COL else info.rows
+        m = CSR(info.rows, info.cols, torch.empty(major + 1, dtype=torch.int32, **dev),
+                torch.empty(max(info.nnz, 1), dtype=torch.int32, **dev),
+                torch.empty(max(info.nnz, 1), dtype=torch.float16, **dev), info.axis)
+        v = _abi.CompressedView()
+        v.rows, v.cols, v.nnz, v.axis = info.rows, info.cols, info.nnz, info.axis
+        v.majorPtr, v.minorIdx, v.val = m.ptr.data_ptr(), m.idx.data_ptr(), m.val.data_ptr()
+        _abi.check(lib.cs_b200_cspack_load_compressed(p, C.byref(v)), "cspack load")
+        m.idx, m.val = m.idx[:info.nnz], m.val[:info.nnz]
+        return m
+    if info.format == 3:
+        n = info.nnz
+        r, c = torch.empty(max(n, 1), dtype=torch.int32, **dev), torch.empty(max(n, 1), dtype=torch.int32, **dev)
+        val = torch.empty(max(n, 1), dtype=torch.float16, **dev)
+        v = _abi.CooView()
+        v.rows, v.cols, v.nnz = info.rows, info.cols, n
+        v.rowIdx, v.colIdx, v.val = r.data_ptr(), c.data_ptr(), val.data_ptr()
+        _abi.check(lib.cs_b200_cspack_load_coo(p, C.byref(v)), "cspack load")
+        return info.rows, info.cols, r[:n], c[:n], val[:n]
+    raise _abi.CellShardError(f"cspack: format {info.format} not handled")
+
+
+def cspack_store_coo(path, rows: int, cols: int, row_idx: torch.Tensor, col_idx: torch.Tensor,
+                     val: torch.Tensor) -> None:
+    torch.cuda.synchronize()
+    v = _abi.CooView()
+    v.rows, v.cols, v.nnz = rows, cols, int(row_idx.numel())
+    v.rowIdx, v.colIdx, v.val = ptr(row_idx), ptr(col_idx), ptr(val)
+    _abi.check(_abi.load().cs_b200_cspack_store_coo(str(path).encode(), C.byref(v)), "cspack store")

@@ -777,6 +777,36 @@ CS_API int cs_b200_choose_bucket_count_for_sliced_part(const cs_host_sliced_ell 
 CS_API void cs_b200_host_bucketed_sliced_ell_clear(cs_host_bucketed_sliced_ell *part);
 
 /* ------------------------------------------------------------------------ */
+/* .cspack raw partition records, file <-> device memory                       */
+/* replaces store_*_raw / load_*_raw of src/io/pack/packfile.cu:191-770 (and   */
+/* the host staging the reference does between them and device::upload):      */
+/* the same bytes on disk, the arrays moved through two pinned staging        */
+/* buffers so the file transfer and the PCIe copy overlap.  fp16 values.      */
+/* Synchronous; call once the stream that produced the arrays has finished.   */
+/* ------------------------------------------------------------------------ */
+
+/* disk_header (io/common/raw_format.hh:26-31) and each format's leading words. */
+typedef struct cs_cspack_info {
+    uint32_t format; /* 2 compressed, 3 COO, 6 Blocked-ELL, 7 Sliced-ELL */
+    uint32_t rows, cols, nnz;
+    uint32_t axis;                 /* compressed */
+    uint32_t block_size, ell_cols; /* Blocked-ELL */
+    uint32_t slice_count, total_slots; /* Sliced-ELL */
+} cs_cspack_info;
+
+CS_API int cs_b200_cspack_peek(const char *path, cs_cspack_info *info);
+CS_API int cs_b200_cspack_store_blocked_ell(const char *path, const cs_blocked_ell_view *part);
+/* dst: shape from cs_b200_cspack_peek, arrays allocated by the caller. */
+CS_API int cs_b200_cspack_load_blocked_ell(const char *path, const cs_blocked_ell_view *dst);
+CS_API int cs_b200_cspack_store_sliced_ell(const char *path, const cs_sliced_ell_view *part);
+/* also writes dst->slice_slot_offsets (when set) from the slice table. */
+CS_API int cs_b200_cspack_load_sliced_ell(const char *path, const cs_sliced_ell_view *dst);
+CS_API int cs_b200_cspack_store_compressed(const char *path, const cs_compressed_view *part);
+CS_API int cs_b200_cspack_load_compressed(const char *path, const cs_compressed_view *dst);
+CS_API int cs_b200_cspack_store_coo(const char *path, const cs_coo_view *part);
+CS_API int cs_b200_cspack_load_coo(const char *path, const cs_coo_view *dst);
+
+/* ------------------------------------------------------------------------ */
 /* Row-label grouped per-feature moments (no reference counterpart: the new   */
 /* entry point beside compute_sparse_group_reduce, same header style).        */
 /* ------------------------------------------------------------------------ */

@@ -417,6 +417,44 @@ def choose_block_size_from_coo(rows, cols, row, col, B_candidates, fmap=None):
             best = (B, fill, padded)
     return best
 
+
+# ---------------------------------------------------------------------------
+# .cspack raw records (src/io/pack/packfile.cu:13-47,265-272,351-369,597-621,715-721)
+# ---------------------------------------------------------------------------
+CSPACK_COMPRESSED, CSPACK_COO, CSPACK_BLOCKED_ELL, CSPACK_SLICED_ELL = 2, 3, 6, 7
+
+
+def cspack_record(fmt, rows, cols, nnz, parts):
+    """Bytes of one record: the 13-byte header (u8 format, u32 rows, cols, nnz)
+    then the format's words and arrays, little-endian, no padding."""
+    head = np.array([fmt], np.uint8).tobytes() + np.array([rows, cols, nnz], np.uint32).tobytes()
+    return head + b"".join(np.ascontiguousarray(p).tobytes() for p in parts)
+
+
+def cspack_blocked_ell(rows, cols, nnz, B, ell_cols, bci, val):
+    return cspack_record(CSPACK_BLOCKED_ELL, rows, cols, nnz,
+                         [np.array([B, ell_cols], np.uint32), np.asarray(bci, np.uint32), np.asarray(val, np.uint16)])
+
+
+def cspack_sliced_ell(rows, cols, nnz, offsets, widths, col_idx, val):
+    return cspack_record(CSPACK_SLICED_ELL, rows, cols, nnz,
+                         [np.array([len(widths)], np.uint32), np.asarray(offsets, np.uint32),
+                          np.asarray(widths, np.uint32), np.asarray(col_idx, np.uint32), np.asarray(val, np.uint16)])
+
+
+def cspack_compressed(rows, cols, nnz, axis, ptr, idx, val):
+    major = cols if axis == 1 else rows
+    parts = [np.array([axis], np.uint32), np.asarray(val, np.uint16)]
+    if major:
+        parts.append(np.asarray(ptr, np.uint32))
+    parts.append(np.asarray(idx, np.uint32))
+    return cspack_record(CSPACK_COMPRESSED, rows, cols, nnz, parts)
+
+
+def cspack_coo(rows, cols, row, col, val):
+    return cspack_record(CSPACK_COO, rows, cols, len(row),
+                         [np.asarray(val, np.uint16), np.asarray(row, np.uint32), np.asarray(col, np.uint32)])
+
 # ---------------------------------------------------------------------------
 # the reference's own code (compiled from its sources into _ref/)
 # ---------------------------------------------------------------------------
@@ -818,6 +856,33 @@ def ref_choose_bucket_count_for_sliced_part(rows, cols, nnz, offsets, widths, co
     assert ref_bucket().csrefb_choose_bucket_count_for_sliced_part(C.byref(src), C.byref(count),
                                                                    C.byref(nbytes)) == 1
     return count.value, nbytes.value
+
+
+
+def ref_cspack_store(fmt, path, rows, cols, nnz, *arrays):
+    """The reference's store_*_raw writing one record to `path`."""
+    b = ref_bucket()
+    a = [np.ascontiguousarray(x) for x in arrays]
+    s = str(path).encode()
+    if fmt == CSPACK_BLOCKED_ELL:
+        B, ell_cols, bci, val = arrays
+        bci, val = np.ascontiguousarray(bci, np.uint32), np.ascontiguousarray(val, np.uint16)
+        b.csrefb_store_blocked_ell_raw.argtypes = [C.c_char_p, u32, u32, u32, u32, u32, vp, vp]
+        return b.csrefb_store_blocked_ell_raw(s, rows, cols, nnz, B, ell_cols, _p(bci), _p(val))
+    if fmt == CSPACK_SLICED_ELL:
+        offs, widths, col, val = (np.ascontiguousarray(x, t) for x, t in zip(arrays, (np.uint32, np.uint32,
+                                                                                      np.uint32, np.uint16)))
+        b.csrefb_store_sliced_ell_raw.argtypes = [C.c_char_p, u32, u32, u32, u32, vp, vp, vp, vp]
+        return b.csrefb_store_sliced_ell_raw(s, rows, cols, nnz, len(widths), _p(offs), _p(widths), _p(col), _p(val))
+    if fmt == CSPACK_COMPRESSED:
+        axis, ptr, idx, val = arrays
+        ptr, idx, val = (np.ascontiguousarray(x, t) for x, t in zip((ptr, idx, val), (np.uint32, np.uint32,
+                                                                                        np.uint16)))
+        b.csrefb_store_compressed_raw.argtypes = [C.c_char_p, u32, u32, u32, u32, vp, vp, vp]
+        return b.csrefb_store_compressed_raw(s, rows, cols, nnz, axis, _p(ptr), _p(idx), _p(val))
+    row, col, val = (np.ascontiguousarray(x, t) for x, t in zip(arrays, (np.uint32, np.uint32, np.uint16)))
+    b.csrefb_store_coo_raw.argtypes = [C.c_char_p, u32, u32, u32, vp, vp, vp]
+    return b.csrefb_store_coo_raw(s, rows, cols, nnz, _p(row), _p(col), _p(val))
 
 
 # ---------------------------------------------------------------------------

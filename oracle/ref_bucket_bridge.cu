@@ -7,7 +7,8 @@
 // execution_builders_part.hh:1011-1596) and calls
 //   build_bucketed_execution_partition (:1206), choose_bucket_count_for_part (:1249),
 //   build_bucketed_sliced_execution_partition (:1529),
-//   choose_bucket_count_for_sliced_part (:1572).
+//   choose_bucket_count_for_sliced_part (:1572),
+// and the .cspack store_*_raw functions of src/io/pack/packfile.cu.
 // The header chain also reads and writes HDF5 files; oracle/ref_stub/hdf5.h
 // stands in for <hdf5.h> so it compiles without the library (none of those
 // paths is called).  The chain opens `namespace cellshard {` and leaves it
@@ -102,6 +103,32 @@ extern "C" int csrefb_choose_bucket_count_for_sliced_part(const cs_host_sliced_e
     const int r = choose_bucket_count_for_sliced_part(&p, count, &b);
     *bytes = b;
     return r;
+}
+
+// .cspack raw records written by the reference's own codec (src/io/pack/packfile.cu),
+// fp16 values.
+extern "C" int csrefb_store_blocked_ell_raw(const char *path, uint32_t rows, uint32_t cols, uint32_t nnz,
+                                            uint32_t block_size, uint32_t ell_cols, const uint32_t *bci,
+                                            const uint16_t *val) {
+    return store_blocked_ell_raw(path, rows, cols, nnz, block_size, ell_cols, bci, val, 2u);
+}
+
+extern "C" int csrefb_store_sliced_ell_raw(const char *path, uint32_t rows, uint32_t cols, uint32_t nnz,
+                                           uint32_t slice_count, const uint32_t *offsets, const uint32_t *widths,
+                                           const uint32_t *col_idx, const uint16_t *val) {
+    return store_sliced_ell_raw(path, rows, cols, nnz, slice_count, offsets, widths, col_idx, val, 2u);
+}
+
+extern "C" int csrefb_store_compressed_raw(const char *path, uint32_t rows, uint32_t cols, uint32_t nnz,
+                                           uint32_t axis, const uint32_t *ptr, const uint32_t *idx,
+                                           const uint16_t *val) {
+    const uint32_t major = axis == sparse::compressed_by_col ? cols : rows;
+    return store_compressed_raw(path, rows, cols, nnz, axis, major, ptr, idx, val, 2u);
+}
+
+extern "C" int csrefb_store_coo_raw(const char *path, uint32_t rows, uint32_t cols, uint32_t nnz,
+                                    const uint32_t *row, const uint32_t *col, const uint16_t *val) {
+    return store_coo_raw(path, rows, cols, nnz, row, col, val, 2u);
 }
 
 // The public entry point the reference defines in src/io/csh5/runtime/fetch.cc:332-337

@@ -56,7 +56,7 @@ int main(void) {
   S(cs_host_bucketed_blocked_ell) O(cs_host_bucketed_blocked_ell, canonical_to_exec_cols)
   S(cs_host_bucketed_sliced_ell) O(cs_host_bucketed_sliced_ell, canonical_slice_widths)
   S(cs_exec_bucket_plan) O(cs_exec_bucket_plan, value_entries) S(cs_exec_bucket_segments)
-  S(cs_host_coo) O(cs_host_coo, val) S(cs_coo_view) O(cs_coo_view, val)
+  S(cs_host_coo) O(cs_host_coo, val) S(cs_coo_view) O(cs_coo_view, val) S(cs_cspack_info)
   return 0;
 }
 """
@@ -88,6 +88,7 @@ PAIRS = {
     "cs_exec_bucket_segments": _abi.ExecBucketSegments,
     "cs_host_coo": _abi.HostCoo,
     "cs_coo_view": _abi.CooView,
+    "cs_cspack_info": _abi.CspackInfo,
 }
 
 
