@@ -43,9 +43,12 @@ struct staging {
         }
         if (s) cudaStreamDestroy(s);
     }
-    bool open() {
+    std::size_t chunk = kChunk;
+    // buffers no larger than the record's largest array needs
+    bool open(std::size_t largest = kChunk) {
+        chunk = largest < kChunk ? (largest < 4096u ? 4096u : largest) : kChunk;
         for (int i = 0; i < 2; ++i)
-            if (!cuda_ok(cudaMallocHost(&buf[i], kChunk), "pinned staging") ||
+            if (!cuda_ok(cudaMallocHost(&buf[i], chunk), "pinned staging") ||
                 !cuda_ok(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming), "staging event"))
                 return false;
         return cuda_ok(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "staging stream") != 0;
@@ -60,9 +63,9 @@ bool store_array(std::FILE *fp, staging &st, const void *dev, std::size_t bytes)
     const char *src = (const char *) dev;
     std::size_t prev_n = 0u;
     int prev = -1;
-    for (std::size_t off = 0, i = 0; off < bytes; off += kChunk, ++i) {
+    for (std::size_t off = 0, i = 0; off < bytes; off += st.chunk, ++i) {
         const int b = (int) (i & 1u);
-        const std::size_t n = bytes - off < kChunk ? bytes - off : kChunk;
+        const std::size_t n = bytes - off < st.chunk ? bytes - off : st.chunk;
         if (!cuda_ok(cudaMemcpyAsync(st.buf[b], src + off, n, cudaMemcpyDeviceToHost, st.s), "D2H chunk") ||
             !cuda_ok(cudaEventRecord(st.ev[b], st.s), "chunk event"))
             return false;
@@ -81,9 +84,9 @@ bool store_array(std::FILE *fp, staging &st, const void *dev, std::size_t bytes)
 bool load_array(std::FILE *fp, staging &st, void *dev, std::size_t bytes) {
     char *dst = (char *) dev;
     bool used[2] = {false, false};
-    for (std::size_t off = 0, i = 0; off < bytes; off += kChunk, ++i) {
+    for (std::size_t off = 0, i = 0; off < bytes; off += st.chunk, ++i) {
         const int b = (int) (i & 1u);
-        const std::size_t n = bytes - off < kChunk ? bytes - off : kChunk;
+        const std::size_t n = bytes - off < st.chunk ? bytes - off : st.chunk;
         if (used[b] && !cuda_ok(cudaEventSynchronize(st.ev[b]), "buffer wait")) return false;
         if (!get(fp, st.buf[b], n)) {
             set_error("cspack: file ends inside an array");
@@ -173,7 +176,10 @@ extern "C" int cs_b200_cspack_store_blocked_ell(const char *path, const cs_block
     const std::size_t w = B == 0u ? 0u : part->ell_cols / B;
     file_guard g;
     staging st;
-    if (!open_file(g, path, "wb", "cspack_store_blocked_ell") || !st.open()) return 0;
+    if (!open_file(g, path, "wb", "cspack_store_blocked_ell") ||
+        !st.open((std::size_t) part->rows * part->ell_cols * 2u > rb * w * 4u ? (std::size_t) part->rows * part->ell_cols * 2u
+                                                                              : rb * w * 4u))
+        return 0;
     if (!write_header(g.fp, kFmtBlockedEll, part->rows, part->cols, part->nnz) || !put(g.fp, &B, 4) ||
         !put(g.fp, &part->ell_cols, 4) || !store_array(g.fp, st, part->blockColIdx, rb * w * 4u) ||
         !store_array(g.fp, st, part->val, (std::size_t) part->rows * part->ell_cols * 2u)) {
@@ -199,7 +205,8 @@ extern "C" int cs_b200_cspack_load_blocked_ell(const char *path, const cs_blocke
     const uint32_t B = info.block_size;
     const std::size_t rb = B == 0u ? 0u : ((std::size_t) info.rows + B - 1u) / B;
     const std::size_t wd = B == 0u ? 0u : info.ell_cols / B;
-    return st.open() && load_array(g.fp, st, dst->blockColIdx, rb * wd * 4u) &&
+    const std::size_t vb = (std::size_t) info.rows * info.ell_cols * 2u, ib = rb * wd * 4u;
+    return st.open(vb > ib ? vb : ib) && load_array(g.fp, st, dst->blockColIdx, rb * wd * 4u) &&
            load_array(g.fp, st, dst->val, (std::size_t) info.rows * info.ell_cols * 2u);
 }
 
@@ -219,7 +226,7 @@ extern "C" int cs_b200_cspack_store_sliced_ell(const char *path, const cs_sliced
     for (uint32_t s = 0; s < S; ++s) total += (offs[s + 1u] - offs[s]) * widths[s];
     file_guard g;
     staging st;
-    if (!open_file(g, path, "wb", "cspack_store_sliced_ell") || !st.open()) return 0;
+    if (!open_file(g, path, "wb", "cspack_store_sliced_ell") || !st.open((std::size_t) total * 4u)) return 0;
     if (!write_header(g.fp, kFmtSlicedEll, part->rows, part->cols, part->nnz) || !put(g.fp, &S, 4) ||
         !put(g.fp, offs.data(), offs.size() * 4u) || !put(g.fp, widths.data(), widths.size() * 4u) ||
         !store_array(g.fp, st, part->col_idx, (std::size_t) total * 4u) ||
@@ -249,7 +256,7 @@ extern "C" int cs_b200_cspack_load_sliced_ell(const char *path, const cs_sliced_
         slots[s] = run;
         run += (offs[s + 1u] - offs[s]) * widths[s];
     }
-    if (!st.open()) return 0;
+    if (!st.open((std::size_t) info.total_slots * 4u)) return 0;
     if (info.slice_count != 0u &&
         (!cuda_ok(cudaMemcpyAsync(dst->slice_row_offsets, offs.data(), offs.size() * 4u, cudaMemcpyHostToDevice, st.s),
                   "H2D offsets") ||
@@ -272,7 +279,8 @@ extern "C" int cs_b200_cspack_store_compressed(const char *path, const cs_compre
     const uint32_t major = part->axis == CS_COMPRESSED_BY_COL ? part->cols : part->rows;
     file_guard g;
     staging st;
-    if (!open_file(g, path, "wb", "cspack_store_compressed") || !st.open()) return 0;
+    const std::size_t big = (std::size_t) (part->nnz > major + 1u ? part->nnz : major + 1u) * 4u;
+    if (!open_file(g, path, "wb", "cspack_store_compressed") || !st.open(big)) return 0;
     if (!write_header(g.fp, kFmtCompressed, part->rows, part->cols, part->nnz) || !put(g.fp, &part->axis, 4) ||
         !store_array(g.fp, st, part->val, (std::size_t) part->nnz * 2u) ||
         (major != 0u && !store_array(g.fp, st, part->majorPtr, ((std::size_t) major + 1u) * 4u)) ||
@@ -297,7 +305,8 @@ extern "C" int cs_b200_cspack_load_compressed(const char *path, const cs_compres
         return 0;
     }
     const uint32_t major = info.axis == CS_COMPRESSED_BY_COL ? info.cols : info.rows;
-    return st.open() && load_array(g.fp, st, dst->val, (std::size_t) info.nnz * 2u) &&
+    const std::size_t big = (std::size_t) (info.nnz > major + 1u ? info.nnz : major + 1u) * 4u;
+    return st.open(big) && load_array(g.fp, st, dst->val, (std::size_t) info.nnz * 2u) &&
            (major == 0u || load_array(g.fp, st, dst->majorPtr, ((std::size_t) major + 1u) * 4u)) &&
            load_array(g.fp, st, dst->minorIdx, (std::size_t) info.nnz * 4u);
 }
@@ -309,7 +318,7 @@ extern "C" int cs_b200_cspack_store_coo(const char *path, const cs_coo_view *par
     }
     file_guard g;
     staging st;
-    if (!open_file(g, path, "wb", "cspack_store_coo") || !st.open()) return 0;
+    if (!open_file(g, path, "wb", "cspack_store_coo") || !st.open((std::size_t) part->nnz * 4u)) return 0;
     if (!write_header(g.fp, kFmtCoo, part->rows, part->cols, part->nnz) ||
         !store_array(g.fp, st, part->val, (std::size_t) part->nnz * 2u) ||
         !store_array(g.fp, st, part->rowIdx, (std::size_t) part->nnz * 4u) ||
@@ -331,7 +340,7 @@ extern "C" int cs_b200_cspack_load_coo(const char *path, const cs_coo_view *dst)
                   info.nnz);
         return 0;
     }
-    return st.open() && load_array(g.fp, st, dst->val, (std::size_t) info.nnz * 2u) &&
+    return st.open((std::size_t) info.nnz * 4u) && load_array(g.fp, st, dst->val, (std::size_t) info.nnz * 2u) &&
            load_array(g.fp, st, dst->rowIdx, (std::size_t) info.nnz * 4u) &&
            load_array(g.fp, st, dst->colIdx, (std::size_t) info.nnz * 4u);
 }

@@ -731,9 +731,17 @@ struct sliced_split {
             for (uint32_t k = 1; k <= K; ++k) progress[k].store(0u);
             std::vector<std::thread> th;
             th.reserve(K);
-            for (uint32_t k = 1; k <= K; ++k)
-                th.emplace_back([&, k] { level(k, w, cost[k - 1u].get(), cost[k].get(), &progress[k - 1u],
-                                               &progress[k]); });
+            uint32_t started = 0u;
+            try {
+                for (uint32_t k = 1; k <= K; ++k, ++started)
+                    th.emplace_back([&, k] { level(k, w, cost[k - 1u].get(), cost[k].get(), &progress[k - 1u],
+                                                   &progress[k]); });
+            } catch (...) {
+                // no thread for level `started + 1`: the remaining levels run here,
+                // after the started ones (each still waits on its predecessor)
+            }
+            for (uint32_t k = started + 1u; k <= K; ++k)
+                level(k, w, cost[k - 1u].get(), cost[k].get(), &progress[k - 1u], &progress[k]);
             for (auto &t : th) t.join();
         }
         for (uint32_t k = 1; k <= K; ++k) cost_at_rows[k] = cost[k][rows];
