@@ -545,6 +545,14 @@ int bell_fill(const cs_blocked_ell_view *part, const void *scratch, const cs_exe
 // find_slice (formats/sliced_ell.cuh:80-87): the first slice whose end lies
 // past the row.
 __device__ __forceinline__ uint32_t slice_of(const cs_sliced_ell_view &v, uint32_t row) {
+    // slices of one height h (all but possibly the last): slice row / h, checked
+    // against the offsets; any other layout falls back to the binary search
+    if (v.slice_count > 1u) {
+        const uint32_t h = __ldg(v.slice_row_offsets + 1u) - __ldg(v.slice_row_offsets);
+        const uint32_t g = h != 0u ? row / h : v.slice_count;
+        if (g < v.slice_count && __ldg(v.slice_row_offsets + g) <= row && row < __ldg(v.slice_row_offsets + g + 1u))
+            return g;
+    }
     uint32_t lo = 0u, hi = v.slice_count;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -592,19 +600,26 @@ __global__ void __launch_bounds__(256) sell_exec_fill_kernel(const cs_sliced_ell
         if (s < src.slice_count) {
             const uint32_t sw = src.slice_widths[s];
             const std::size_t base = src.slice_slot_offsets[s] + (std::size_t) (row - src.slice_row_offsets[s]) * sw;
-            // 128 slots per step: four column loads per lane in flight, then the
-            // values of the live ones, then four ballot-ranked stores
+            // 128 slots per step: four column loads per lane; the live values of
+            // a step are loaded together with the next step's columns, then four
+            // ballot-ranked stores
+            uint32_t cn[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t k = 32u * u + lane;
+                cn[u] = k < sw ? __ldcs(src.col_idx + base + k) : kInvalid;
+            }
             for (uint32_t k0 = 0; k0 < sw; k0 += 128u) {
                 uint32_t c[4];
                 uint16_t x[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const uint32_t k = k0 + 32u * u + lane;
-                    c[u] = k < sw ? __ldcs(src.col_idx + base + k) : kInvalid;
-                }
+                for (int u = 0; u < 4; ++u) c[u] = cn[u];
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < 4; ++u) {
                     x[u] = c[u] != kInvalid ? __ldcs(src.val + base + k0 + 32u * u + lane) : (uint16_t) 0u;
+                    const uint32_t k = k0 + 128u + 32u * u + lane;
+                    cn[u] = k < sw ? __ldcs(src.col_idx + base + k) : kInvalid;
+                }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const unsigned m = __ballot_sync(0xffffffffu, c[u] != kInvalid);
