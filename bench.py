@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--chunk-rows", type=int, default=0,
+                   help="rows per accumulation chunk of the moments reduction (0 = the library default, 2048)")
     p.add_argument("--workload", choices=["moments", "convert", "mask_groups", "batched", "serving"],
                    default="moments",
                    help="moments: the headline reduction; convert: per-kernel conversion throughput; "
@@ -263,7 +265,8 @@ def run_product(args):
     out["status"] = torch.zeros(1, dtype=torch.int32, device="cuda")
 
     def step(phases=runtime.PHASE_ALL):
-        runtime.compute_sparse_group_moments(bell, GROUPS, d_rk, d_fk, d_lab, workspace=ws, out=out, phases=phases)
+        runtime.compute_sparse_group_moments(bell, GROUPS, d_rk, d_fk, d_lab, workspace=ws, out=out, phases=phases,
+                                             chunk_rows=args.chunk_rows)
 
     for _ in range(args.warmup):
         step()
@@ -308,7 +311,8 @@ def run_product(args):
             r_rk.copy_(h_rk, non_blocking=True)
             r_fk.copy_(h_fk, non_blocking=True)
             r_lab.copy_(h_lab, non_blocking=True)
-            runtime.compute_sparse_group_moments(bell, GROUPS, r_rk, r_fk, r_lab, workspace=ws, out=out)
+            runtime.compute_sparse_group_moments(bell, GROUPS, r_rk, r_fk, r_lab, workspace=ws, out=out,
+                                                 chunk_rows=args.chunk_rows)
             for k2, t2 in h_out.items():
                 t2.copy_(out[k2], non_blocking=True)
             torch.cuda.current_stream().synchronize()
@@ -338,7 +342,8 @@ def run_product(args):
 
     W = bell.ell_width
     rb_kept = int(np.unique(np.flatnonzero(rk) // BLOCK).size)
-    chunks_per_group = [(n + 2047) // 2048 for n in np.bincount(lab[rk == 1], minlength=GROUPS)]
+    cr = args.chunk_rows or 2048
+    chunks_per_group = [(n + cr - 1) // cr for n in np.bincount(lab[rk == 1], minlength=GROUPS)]
     n_chunks = int(sum(chunks_per_group))
     acc_bytes = kept_rows * bell.ell_cols * 2 + n_chunks * spec.cols * 16
     step_bytes = (kept_rows * bell.ell_cols * 2 + rb_kept * W * 4 + spec.rows + spec.cols + 4 * spec.rows
@@ -364,7 +369,8 @@ def run_product(args):
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "clocks": clk,
             "extra": {"kept_rows": kept_rows, "kept_nnz": kept_nnz, "ell_cols": bell.ell_cols, "ell_width": W,
-                      "conversion_csr_to_blocked_ell_ms": conversion_ms, "chunks": n_chunks},
+                      "conversion_csr_to_blocked_ell_ms": conversion_ms, "chunks": n_chunks,
+                      "chunk_rows": cr},
         }
         if e2e:
             result["e2e"] = {"value": world * kept_nnz / (e2e["ms"] * 1e-3), "unit": "nnz/s",
