@@ -141,6 +141,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of this rank's timings over all ranks (every rank gets it);
+    the values unchanged without a process group."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_rate(world: int, units_per_rank: int, ms: float) -> float:
+    """Units all ranks processed per second, over the slowest rank's time."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -333,12 +350,9 @@ def run_product(args):
         e2e = {"ms": e2e_ms, "h2d": h2d, "d2h": d2h}
     clk = clocks.stop()
 
-    if dist is not None:
-        t = torch.tensor([step_ms, acc_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, acc_ms = float(t[0]), float(t[1])
-        if e2e:
-            e2e["ms"] = float(t[2])
+    step_ms, acc_ms, e2e_max = max_over_ranks(dist, [step_ms, acc_ms, e2e["ms"] if e2e else 0.0], "cuda")
+    if e2e:
+        e2e["ms"] = e2e_max
 
     W = bell.ell_width
     rb_kept = int(np.unique(np.flatnonzero(rk) // BLOCK).size)
@@ -350,7 +364,7 @@ def run_product(args):
                   + GROUPS * spec.cols * 8)
     peak, peak_kind = measured_peak()
     achieved = acc_bytes / (acc_ms * 1e-3) / 1e9
-    value = world * kept_nnz / (step_ms * 1e-3)
+    value = whole_job_rate(world, kept_nnz, step_ms)
 
     result = None
     if rank == 0:
@@ -373,7 +387,7 @@ def run_product(args):
                       "chunk_rows": cr},
         }
         if e2e:
-            result["e2e"] = {"value": world * kept_nnz / (e2e["ms"] * 1e-3), "unit": "nnz/s",
+            result["e2e"] = {"value": whole_job_rate(world, kept_nnz, e2e["ms"]), "unit": "nnz/s",
                              "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                              "ms_per_step": e2e["ms"]}
         if world == 1 and not args.no_cpu_baseline:
