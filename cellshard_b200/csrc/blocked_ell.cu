@@ -96,8 +96,19 @@ __global__ void __launch_bounds__(kShapeWarps * 32) bell_shape_kernel(
                     }
                     if (m != 0u) atomicOr(bits + word, m);
                 };
-#pragma unroll 4
-                for (uint32_t k = lane; k < nvec; k += 32u) mark4(__ldg(v4 + k));
+                // eight vectors per lane loaded before any is marked
+                constexpr unsigned kV = 8;
+                for (uint32_t k0 = lane; k0 < nvec; k0 += 32u * kV) {
+                    uint4 q[kV];
+#pragma unroll
+                    for (unsigned u = 0; u < kV; ++u) {
+                        const uint32_t k = k0 + 32u * u;
+                        q[u] = k < nvec ? __ldg(v4 + k) : make_uint4(0u, 0u, 0u, 0u);
+                    }
+#pragma unroll
+                    for (unsigned u = 0; u < kV; ++u)
+                        if (k0 + 32u * u < nvec) mark4(q[u]);
+                }
                 for (uint32_t i = head_end + (nvec << 2) + lane; i < e; i += 32u) mark(idx[i]);
             }
         }
