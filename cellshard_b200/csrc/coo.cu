@@ -106,13 +106,30 @@ __device__ __forceinline__ bool entry_ok(const cs_coo_view &src, const uint32_t 
 __global__ void __launch_bounds__(256) coo_scan_kernel(const cs_coo_view src, const uint32_t *__restrict__ map,
                                                        uint32_t *__restrict__ words, uint32_t *__restrict__ status) {
     uint32_t mx = 0u, dropped = 0u, down = 0u;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < src.nnz; i += gridDim.x * blockDim.x) {
-        if (i != 0u && src.rowIdx[i] < src.rowIdx[i - 1u]) down = 1u;
-        if (!entry_ok(src, map, i)) {
-            ++dropped;
-            continue;
+    // four entries per thread, their row and column loads issued together
+    constexpr unsigned U = 4;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < src.nnz; i0 += stride * U) {
+        uint32_t r[U], rp[U], c[U];
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            const uint32_t i = i0 + u * stride;
+            const bool in = i < src.nnz && i >= i0; // i >= i0: no wrap past 2^32
+            r[u] = in ? __ldg(src.rowIdx + i) : 0u;
+            rp[u] = in && i != 0u ? __ldg(src.rowIdx + i - 1u) : 0u;
+            c[u] = in ? __ldg(src.colIdx + i) : 0u;
         }
-        mx = max(mx, mapped(src.colIdx, map, i));
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            const uint32_t i = i0 + u * stride;
+            if (i >= src.nnz || i < i0) continue;
+            if (i != 0u && r[u] < rp[u]) down = 1u;
+            if (!(r[u] < src.rows && (map == nullptr || c[u] < src.cols))) {
+                ++dropped;
+                continue;
+            }
+            mx = max(mx, map != nullptr ? __ldg(map + c[u]) : c[u]);
+        }
     }
     mx = __reduce_max_sync(0xffffffffu, mx);
     dropped = __reduce_add_sync(0xffffffffu, dropped);
@@ -245,12 +262,28 @@ __global__ void __launch_bounds__(256) coo_group_kernel(coo_decode d, const uint
 // runs get the next run's start) and the mapped columns.
 __global__ void __launch_bounds__(256) coo_row_ptr_kernel(uint32_t n, uint32_t rows, const uint32_t *__restrict__ row,
                                                           uint32_t *__restrict__ ptr) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t r = row[i];
-        const uint32_t lo = i == 0u ? 0u : row[i - 1u] + 1u;
-        for (uint32_t q = lo; q <= r && (i == 0u || r != row[i - 1u]); ++q) ptr[q] = i;
-        if (i == n - 1u)
-            for (uint32_t q = r + 1u; q <= rows; ++q) ptr[q] = n;
+    // four entries per thread, their loads issued together
+    constexpr unsigned U = 4;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * U) {
+        uint32_t rr[U], rp[U];
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            const uint32_t i = i0 + u * stride;
+            const bool in = i < n && i >= i0;
+            rr[u] = in ? __ldg(row + i) : 0u;
+            rp[u] = in && i != 0u ? __ldg(row + i - 1u) : 0u;
+        }
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            const uint32_t i = i0 + u * stride;
+            if (i >= n || i < i0) continue;
+            const uint32_t r = rr[u];
+            const uint32_t lo = i == 0u ? 0u : rp[u] + 1u;
+            for (uint32_t q = lo; q <= r && (i == 0u || r != rp[u]); ++q) ptr[q] = i;
+            if (i == n - 1u)
+                for (uint32_t q = r + 1u; q <= rows; ++q) ptr[q] = n;
+        }
     }
 }
 
