@@ -278,44 +278,67 @@ __global__ void __launch_bounds__(256) segment_copy_kernel(uint32_t n, const uin
                                                            uint32_t *__restrict__ dst_idx,
                                                            uint16_t *__restrict__ dst_val) {
     const unsigned lane = threadIdx.x & 31u;
-    for (uint32_t i = blockIdx.x * 8u + (threadIdx.x >> 5); i < n; i += gridDim.x * 8u) {
-        const uint32_t s = order[i];
+    const uint32_t step = gridDim.x * 8u;
+    // a row's source arrays and bounds, from its source row id s and position i
+    struct row_src {
+        const uint32_t *si;
+        const uint16_t *sv;
+        uint32_t a, len, d;
+    };
+    auto locate = [&](uint32_t s, uint32_t i) {
         const uint32_t *sp = ptr;
-        const uint32_t *si = idx;
-        const uint16_t *sv = val;
+        row_src r{idx, val, 0u, 0u, 0u};
         uint32_t local = s;
         if (part_ptr != nullptr) {
             const uint32_t p = find_part(s, part_offsets, part_count);
             local = s - part_offsets[p];
             sp = part_ptr[p];
-            si = part_idx[p];
-            sv = part_val[p];
+            r.si = part_idx[p];
+            r.sv = part_val[p];
         }
-        const uint32_t a = sp[local];
-        const uint32_t len = sp[local + 1u] - a;
-        const uint32_t d = dst_ptr[i];
+        r.a = sp[local];
+        r.len = sp[local + 1u] - r.a;
+        r.d = dst_ptr[i];
+        return r;
+    };
+    // pipelined: row i's bounds and row i + step's source id are known when
+    // row i is copied, so those lookups overlap the copy instead of preceding it
+    uint32_t i = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (i >= n) return;
+    row_src cur = locate(order[i], i);
+    uint32_t s_next = i + step > i && i + step < n ? order[i + step] : 0u;
+    for (; i < n; i += step) {
+        row_src nxt{idx, val, 0u, 0u, 0u};
+        uint32_t s_after = 0u;
+        if (i + step > i && i + step < n) {
+            nxt = locate(s_next, i + step);
+            if (i + 2u * step < n && i + 2u * step > i) s_after = order[i + 2u * step];
+        }
         // eight coalesced loads per array in flight per lane before the stores
         constexpr unsigned U = 8;
-        for (uint32_t j0 = 0; j0 < len; j0 += 32u * U) {
+        for (uint32_t j0 = 0; j0 < cur.len; j0 += 32u * U) {
             uint32_t iv[U];
             uint16_t vv[U];
 #pragma unroll
             for (unsigned u = 0; u < U; ++u) {
                 const uint32_t j = j0 + u * 32u + lane;
-                if (j < len) {
-                    iv[u] = __ldcs(si + a + j);
-                    vv[u] = __ldcs(reinterpret_cast<const unsigned short *>(sv) + a + j);
+                if (j < cur.len) {
+                    iv[u] = __ldcs(cur.si + cur.a + j);
+                    vv[u] = __ldcs(reinterpret_cast<const unsigned short *>(cur.sv) + cur.a + j);
                 }
             }
 #pragma unroll
             for (unsigned u = 0; u < U; ++u) {
                 const uint32_t j = j0 + u * 32u + lane;
-                if (j < len) {
-                    dst_idx[d + j] = iv[u];
-                    dst_val[d + j] = vv[u];
+                if (j < cur.len) {
+                    dst_idx[cur.d + j] = iv[u];
+                    dst_val[cur.d + j] = vv[u];
                 }
             }
         }
+        cur = nxt;
+        s_next = s_after;
+        if (i + step < i) break; // the next index would wrap past 2^32
     }
 }
 
