@@ -9,10 +9,12 @@ step computes per-(group, feature) sum and sum of squares (fp32 with two-sum
 compensation, fp64 cross-chunk combine) plus mean and variance.
 
   value  stored nnz of the kept rows / device time of the step, inputs resident
-  e2e    same metric through the one-shot C-ABI call with the request's masks
+  e2e    same metric through the one-shot C-ABI call that delivers results to
+         host memory (cs_b200_group_moments_to_host) with the request's masks
          and labels copied from pinned host memory and the four G x C result
-         arrays copied back every step (the partition itself is staged once,
-         as device::stage_partition does in the reference)
+         arrays copied back every step, each group range's rows while the next
+         range computes (the partition itself is staged once, as
+         device::stage_partition does in the reference)
 
 Multi-GPU: one process per GPU (torchrun), each rank an independent replica
 (the reduction needs no exchange for a single partition): weak scaling,
@@ -64,6 +66,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--e2e-parts", type=int, default=0,
+                   help="group ranges whose result copies overlap the next range's work (0 = library default)")
     p.add_argument("--chunk-rows", type=int, default=0,
                    help="rows per accumulation chunk of the moments reduction (0 = the library default, 2048)")
     p.add_argument("--workload", choices=["moments", "convert", "mask_groups", "batched", "serving"],
@@ -328,10 +332,10 @@ def run_product(args):
             r_rk.copy_(h_rk, non_blocking=True)
             r_fk.copy_(h_fk, non_blocking=True)
             r_lab.copy_(h_lab, non_blocking=True)
-            runtime.compute_sparse_group_moments(bell, GROUPS, r_rk, r_fk, r_lab, workspace=ws, out=out,
-                                                 chunk_rows=args.chunk_rows)
-            for k2, t2 in h_out.items():
-                t2.copy_(out[k2], non_blocking=True)
+            # results land in pinned host memory; each group range's rows copy while
+            # the next range computes
+            runtime.compute_sparse_group_moments_to_host(bell, GROUPS, h_out, r_rk, r_fk, r_lab, workspace=ws,
+                                                         out=out, chunk_rows=args.chunk_rows, parts=args.e2e_parts)
             torch.cuda.current_stream().synchronize()
 
         for _ in range(2):

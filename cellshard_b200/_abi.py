@@ -266,6 +266,8 @@ PROTOTYPES: dict[str, tuple] = {
                                                             P(GroupMomentsOut), vp]),
     "cs_b200_group_moments_phases": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
                                                P(GroupMomentsOut), vp, sz, u32, vp]),
+    "cs_b200_group_moments_to_host": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
+                                                P(GroupMomentsOut), P(GroupMomentsOut), vp, sz, u32, vp]),
     "cs_b200_synth_csr": (C.c_int, [u32, u32, vp, vp, vp, vp, u32, vp, u64, vp, vp, vp]),
     "cs_b200_batch_sliced_create": (C.c_int, [P(BatchPart), u32, P(u32), u32, vp, u64, P(BatchTiles), P(vp)]),
     "cs_b200_batch_sliced_autotune": (C.c_int, [vp, vp, P(BatchTiles)]),

@@ -285,10 +285,13 @@ template <int L, bool COMP>
 __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
     const uint16_t *__restrict__ val, uint32_t ell_cols, uint32_t block_size, uint32_t col_blocks, uint32_t words,
     uint32_t cols, const uint2 *__restrict__ index, const chunk_desc *__restrict__ chunks,
-    const uint32_t *__restrict__ num_chunks, const uint32_t *__restrict__ sorted_rows, float *__restrict__ partials) {
+    const uint32_t *__restrict__ num_chunks, const uint32_t *__restrict__ sorted_rows, float *__restrict__ partials,
+    const uint32_t *__restrict__ chunk_first, uint32_t g_lo, uint32_t g_hi) {
     extern __shared__ uint2 chunk_rows_smem[]; // (row, row_block * words)
     const uint32_t c = blockIdx.x;
     if (c >= *num_chunks) return;
+    // with chunk_first: only the chunks of groups [g_lo, g_hi)
+    if (chunk_first != nullptr && (c < chunk_first[g_lo] || c >= chunk_first[g_hi])) return;
     const chunk_desc d = chunks[c];
     const uint32_t n = d.end - d.begin;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
@@ -416,8 +419,9 @@ __global__ void __launch_bounds__(256) moments_combine_kernel(
     uint32_t cols, uint32_t G, uint32_t scheme, uint32_t ddof, const uint32_t *__restrict__ chunk_first,
     const uint32_t *__restrict__ group_rows, const float *__restrict__ partials, const uint8_t *__restrict__ feature_keep,
     float *__restrict__ out_sum, float *__restrict__ out_sumsq, float *__restrict__ out_mean, float *__restrict__ out_var,
-    double *__restrict__ out_mean64, double *__restrict__ out_var64, uint32_t *__restrict__ out_group_rows) {
-    const uint32_t g = blockIdx.y;
+    double *__restrict__ out_mean64, double *__restrict__ out_var64, uint32_t *__restrict__ out_group_rows,
+    uint32_t g_base) {
+    const uint32_t g = g_base + blockIdx.y;
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     if (f == 0 && out_group_rows != nullptr) out_group_rows[g] = group_rows[g];
@@ -485,7 +489,8 @@ __global__ void __launch_bounds__(256) moments_combine_kernel(
 }
 
 template <int L, bool COMP>
-int launch_accumulate(const cs_blocked_ell_view *src, const moments_layout &lay, cudaStream_t stream) {
+int launch_accumulate(const cs_blocked_ell_view *src, const moments_layout &lay, const uint32_t *chunk_first,
+                      uint32_t g_lo, uint32_t g_hi, cudaStream_t stream) {
     const uint32_t segs = lay.col_blocks * (src->block_size / L);
     dim3 grid(lay.max_chunks, (segs + kAccThreads - 1u) / kAccThreads);
     const std::size_t smem = (std::size_t) lay.chunk_rows * sizeof(uint2);
@@ -496,7 +501,7 @@ int launch_accumulate(const cs_blocked_ell_view *src, const moments_layout &lay,
         return 0;
     kern<<<grid, kAccThreads, smem, stream>>>(src->val, src->ell_cols, src->block_size, lay.col_blocks, lay.words,
                                               src->cols, lay.index, lay.chunks, lay.num_chunks, lay.sorted_rows,
-                                              lay.partials);
+                                              lay.partials, chunk_first, g_lo, g_hi);
     return launch_ok("moments_accumulate_kernel");
 }
 
@@ -549,7 +554,7 @@ extern "C" int cs_b200_group_moments_scratch_bytes(const cs_blocked_ell_view *sr
 static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep, const uint8_t *d_feature_keep,
                        const uint32_t *d_row_labels, const cs_group_moments_params *params,
                        const cs_group_moments_out *out, void *d_scratch, size_t scratch_bytes, cs_stream_t s,
-                       uint32_t phases) {
+                       uint32_t phases, uint32_t g_lo = 0u, uint32_t g_hi = 0xffffffffu) {
     if (!validate(src, params)) return 0;
     if (out == nullptr || out->sum == nullptr || out->sumsq == nullptr) {
         set_error("group_moments: sum and sumsq outputs are required");
@@ -567,6 +572,11 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
     cudaStream_t stream = as_stream(s);
     const uint32_t G = params->group_count;
     const uint32_t width = src->ell_cols / src->block_size;
+    // accumulate and combine may be restricted to groups [g_lo, g_hi)
+    if (g_hi > G) g_hi = G;
+    const bool all_groups = g_lo == 0u && g_hi == G;
+    if (g_lo >= g_hi) return 1;
+    const uint32_t *range_first = all_groups ? nullptr : lay.chunk_first;
 
     if ((phases & CS_MOMENTS_PHASE_PREPARE) && lay.row_blocks != 0u && lay.words != 0u) {
         if (width != 0u) {
@@ -623,23 +633,27 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
         const uint32_t B = src->block_size;
         const bool aligned16 = (reinterpret_cast<uintptr_t>(src->val) & 15u) == 0u;
         int ok;
+#define CS_ACC(L_)                                                                                     \
+    (comp ? launch_accumulate<L_, true>(src, lay, range_first, g_lo, g_hi, stream)                      \
+          : launch_accumulate<L_, false>(src, lay, range_first, g_lo, g_hi, stream))
         if (B % 8u == 0u && aligned16)
-            ok = comp ? launch_accumulate<8, true>(src, lay, stream) : launch_accumulate<8, false>(src, lay, stream);
+            ok = CS_ACC(8);
         else if (B % 4u == 0u && (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u)
-            ok = comp ? launch_accumulate<4, true>(src, lay, stream) : launch_accumulate<4, false>(src, lay, stream);
+            ok = CS_ACC(4);
         else if (B % 2u == 0u && (reinterpret_cast<uintptr_t>(src->val) & 3u) == 0u)
-            ok = comp ? launch_accumulate<2, true>(src, lay, stream) : launch_accumulate<2, false>(src, lay, stream);
+            ok = CS_ACC(2);
         else
-            ok = comp ? launch_accumulate<1, true>(src, lay, stream) : launch_accumulate<1, false>(src, lay, stream);
+            ok = CS_ACC(1);
+#undef CS_ACC
         if (!ok) return 0;
     }
 
     if ((phases & CS_MOMENTS_PHASE_COMBINE) && (src->cols != 0u || out->group_rows != nullptr)) {
-        dim3 grid((src->cols + 255u) / 256u == 0u ? 1u : (src->cols + 255u) / 256u, G);
+        dim3 grid((src->cols + 255u) / 256u == 0u ? 1u : (src->cols + 255u) / 256u, g_hi - g_lo);
         moments_combine_kernel<<<grid, 256, 0, stream>>>(src->cols, G, params->scheme, params->ddof, lay.chunk_first,
                                                          lay.group_rows, lay.partials, d_feature_keep, out->sum,
                                                          out->sumsq, out->mean, out->var, out->mean64, out->var64,
-                                                         out->group_rows);
+                                                         out->group_rows, g_lo);
         if (!launch_ok("moments_combine_kernel")) return 0;
     }
     return 1;
@@ -712,4 +726,95 @@ extern "C" int cs_b200_group_moments_phases(const cs_blocked_ell_view *src, cons
     }
     return moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, out, d_scratch, scratch_bytes, s,
                        phases);
+}
+
+namespace {
+
+// Copy stream and events of the host-delivery entry point, one set per host
+// thread and device (created on first use, kept for the thread's lifetime).
+struct host_copy_ctx {
+    int device = -1;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ready = nullptr, done = nullptr;
+};
+
+bool host_copy_setup(host_copy_ctx &c) {
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "get device")) return false;
+    if (c.device == dev && c.copy != nullptr) return true;
+    c = host_copy_ctx{};
+    if (!cuda_ok(cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking), "copy stream") ||
+        !cuda_ok(cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming), "copy event") ||
+        !cuda_ok(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "copy event"))
+        return false;
+    c.device = dev;
+    return true;
+}
+
+template <typename T>
+bool copy_rows(T *h, const T *d, uint32_t g0, uint32_t g1, std::size_t row_elems, cudaStream_t copy) {
+    if (h == nullptr || d == nullptr || g1 <= g0) return true;
+    return cuda_ok(cudaMemcpyAsync(h + (std::size_t) g0 * row_elems, d + (std::size_t) g0 * row_elems,
+                                   (std::size_t) (g1 - g0) * row_elems * sizeof(T), cudaMemcpyDeviceToHost, copy),
+                   "moments D2H") != 0;
+}
+
+} // namespace
+
+extern "C" int cs_b200_group_moments_to_host(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,
+                                             const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
+                                             const cs_group_moments_params *params, const cs_group_moments_out *d_out,
+                                             const cs_group_moments_out *h_out, void *d_scratch,
+                                             size_t scratch_bytes, uint32_t parts, cs_stream_t s) {
+    if (h_out == nullptr || d_out == nullptr) {
+        set_error("group_moments_to_host: null outputs");
+        return 0;
+    }
+    const struct {
+        const void *h, *d;
+        const char *name;
+    } fields[] = {{h_out->sum, d_out->sum, "sum"},          {h_out->sumsq, d_out->sumsq, "sumsq"},
+                  {h_out->mean, d_out->mean, "mean"},       {h_out->var, d_out->var, "var"},
+                  {h_out->mean64, d_out->mean64, "mean64"}, {h_out->var64, d_out->var64, "var64"},
+                  {h_out->group_rows, d_out->group_rows, "group_rows"}};
+    for (const auto &f : fields)
+        if (f.h != nullptr && f.d == nullptr) {
+            set_error("group_moments_to_host: host %s given without its device array", f.name);
+            return 0;
+        }
+    if (!validate(src, params)) return 0;
+    const uint32_t G = params->group_count;
+    if (parts == 0u) parts = 2u;
+    if (parts > G) parts = G;
+    cudaStream_t stream = as_stream(s);
+    if (!moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, d_out, d_scratch, scratch_bytes, s,
+                     CS_MOMENTS_PHASE_PREPARE))
+        return 0;
+    thread_local host_copy_ctx ctx;
+    if (!host_copy_setup(ctx)) return 0;
+    const std::size_t cols = src->cols;
+    for (uint32_t k = 0; k < parts; ++k) {
+        const uint32_t g0 = (uint32_t) ((uint64_t) k * G / parts), g1 = (uint32_t) ((uint64_t) (k + 1u) * G / parts);
+        if (g1 <= g0) continue;
+        // groups [g0, g1) accumulated and combined; their rows copy while the next part computes
+        if (!moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, d_out, d_scratch, scratch_bytes, s,
+                         CS_MOMENTS_PHASE_ACCUMULATE | CS_MOMENTS_PHASE_COMBINE, g0, g1) ||
+            !cuda_ok(cudaEventRecord(ctx.ready, stream), "part event") ||
+            !cuda_ok(cudaStreamWaitEvent(ctx.copy, ctx.ready, 0), "copy wait") ||
+            !copy_rows(h_out->sum, d_out->sum, g0, g1, cols, ctx.copy) ||
+            !copy_rows(h_out->sumsq, d_out->sumsq, g0, g1, cols, ctx.copy) ||
+            !copy_rows(h_out->mean, d_out->mean, g0, g1, cols, ctx.copy) ||
+            !copy_rows(h_out->var, d_out->var, g0, g1, cols, ctx.copy) ||
+            !copy_rows(h_out->mean64, d_out->mean64, g0, g1, cols, ctx.copy) ||
+            !copy_rows(h_out->var64, d_out->var64, g0, g1, cols, ctx.copy) ||
+            !copy_rows(h_out->group_rows, d_out->group_rows, g0, g1, 1u, ctx.copy))
+            return 0;
+    }
+    if (h_out->status != nullptr && d_out->status != nullptr &&
+        !cuda_ok(cudaMemcpyAsync(h_out->status, d_out->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.copy),
+                 "status D2H"))
+        return 0;
+    // the caller's stream waits for the copies, so a sync on it covers them
+    return cuda_ok(cudaEventRecord(ctx.done, ctx.copy), "copy done event") &&
+           cuda_ok(cudaStreamWaitEvent(stream, ctx.done, 0), "stream wait");
 }

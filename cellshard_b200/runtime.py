@@ -238,3 +238,45 @@ def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=Non
                                                     C.byref(p), C.byref(o), ptr(scratch), scratch.numel(), phases,
                                                     stream_handle(stream)), "group_moments_phases")
     return out
+
+
+def compute_sparse_group_moments_to_host(src: BlockedELL, group_count: int, host_out: dict, row_keep=None,
+                                         feature_keep=None, row_labels=None, scheme: int = TWOSUM_F64_COMBINE,
+                                         ddof: int = 1, chunk_rows: int = 0, parts: int = 0,
+                                         workspace: MomentsWorkspace | None = None, out=None, stream=None):
+    """compute_sparse_group_moments with the results copied into ``host_out`` (pinned CPU
+    tensors keyed like the device outputs: sum, sumsq, mean, var, mean64, var64,
+    group_rows, status), the groups split into ``parts`` ranges whose copies overlap the
+    next range's work (cs_b200_group_moments_to_host).  Synchronise the stream before
+    reading ``host_out``.  Returns the device outputs."""
+    lib = _abi.load()
+    G, cols = group_count, src.cols
+    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows)
+    v = src.view()
+    n = C.c_size_t()
+    _abi.check(lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(p), C.byref(n)), "moments scratch")
+    ws = workspace or MomentsWorkspace()
+    scratch = ws.reserve(n.value)
+    if out is None:
+        out = {k: torch.empty((G, cols), dtype=torch.float32, device="cuda") for k in ("sum", "sumsq", "mean", "var")}
+        out["group_rows"] = torch.empty(G, dtype=torch.int32, device="cuda")
+        out["status"] = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if "mean64" in host_out or "var64" in host_out:
+            out["mean64"] = torch.empty((G, cols), dtype=torch.float64, device="cuda")
+            out["var64"] = torch.empty((G, cols), dtype=torch.float64, device="cuda")
+
+    def hptr(k):
+        t = host_out.get(k)
+        if t is None:
+            return None
+        if t.is_cuda or t.numel() != out[k].numel() or t.dtype != out[k].dtype:
+            raise ValueError(f"host_out[{k!r}] must be a CPU tensor shaped and typed like the device output")
+        return t.data_ptr()
+
+    keys = ("sum", "sumsq", "mean", "var", "mean64", "var64", "group_rows", "status")
+    o = _abi.GroupMomentsOut(*[ptr(out.get(k)) for k in keys])
+    h = _abi.GroupMomentsOut(*[hptr(k) for k in keys])
+    _abi.check(lib.cs_b200_group_moments_to_host(C.byref(v), ptr(row_keep), ptr(feature_keep), ptr(row_labels),
+                                                 C.byref(p), C.byref(o), C.byref(h), ptr(scratch), scratch.numel(),
+                                                 parts, stream_handle(stream)), "group_moments_to_host")
+    return out

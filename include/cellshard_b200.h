@@ -908,6 +908,28 @@ CS_API int cs_b200_group_moments_phases(const cs_blocked_ell_view *src,
                                         uint32_t phases,
                                         cs_stream_t stream);
 
+/* No counterpart in the reference.  The one-shot reduction with its results
+ * delivered to host memory: h_out holds host pointers (pinned memory, for the
+ * copies to overlap) for the fields the caller wants back, each with its
+ * device array in d_out.  The groups are split into `parts` ranges (0 = 2,
+ * at most G): each range is accumulated and combined in turn, and its rows of
+ * every requested array are copied to the host on a library-owned copy stream
+ * while the next range computes.  Results equal the device-only call's bit
+ * for bit.  Stream-ordered: `stream` waits for the copies, so synchronising
+ * it makes h_out readable.  h_out->status, when given with d_out->status,
+ * receives the device status word. */
+CS_API int cs_b200_group_moments_to_host(const cs_blocked_ell_view *src,
+                                         const uint8_t *d_row_keep,
+                                         const uint8_t *d_feature_keep,
+                                         const uint32_t *d_row_labels,
+                                         const cs_group_moments_params *params,
+                                         const cs_group_moments_out *d_out,
+                                         const cs_group_moments_out *h_out,
+                                         void *d_scratch,
+                                         size_t scratch_bytes,
+                                         uint32_t parts,
+                                         cs_stream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* Synthetic cell x gene data (no reference counterpart; feeds tests and the  */
 /* benchmark with seeded NB counts on Zipf-popular columns).                  */

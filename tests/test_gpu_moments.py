@@ -166,3 +166,33 @@ def test_moments_generated_matrix(cuda, orc):
                                  nthreads=4)
     res = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab))
     _check(res, ref, G, spec.cols)
+
+
+@pytest.mark.parametrize("parts", [0, 1, 2, 3, 7])
+def test_moments_to_host_matches_device_call(cuda, orc, parts):
+    """The host-delivery entry point (groups in `parts` ranges, each range's rows copied
+    while the next computes) returns the device-only call's results bit for bit, in
+    pinned host memory, and both match the FP64 oracle."""
+    import torch
+
+    from cellshard_b200 import runtime
+
+    rows, cols, G = 3000, 203, 7
+    bell = _bell(cuda, rows, cols, 16, 0.06, seed=parts + 3, integer=False)
+    rk, fk, lab = _masks(rows, cols, G, parts + 11)
+    bci, val = _host(bell)
+    ref = orc.group_moments_bell(rows, cols, 16, bell.ell_cols, bci, val, rk, fk, lab, G, ddof=1)
+    want = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab), ddof=1, chunk_rows=128,
+                                                want_f64=True)
+    host = {k: torch.empty((G, cols), dtype=torch.float32).pin_memory() for k in ("sum", "sumsq", "mean", "var")}
+    host["mean64"] = torch.empty((G, cols), dtype=torch.float64).pin_memory()
+    host["group_rows"] = torch.empty(G, dtype=torch.int32).pin_memory()
+    host["status"] = torch.full((1,), -1, dtype=torch.int32).pin_memory()
+    runtime.compute_sparse_group_moments_to_host(bell, G, host, _dev(rk), _dev(fk), _dev(lab), ddof=1,
+                                                 chunk_rows=128, parts=parts)
+    torch.cuda.synchronize()
+    for k in ("sum", "sumsq", "mean", "var", "mean64", "group_rows"):
+        a, b = host[k].numpy(), want[k].cpu().numpy()
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), k
+    assert int(host["status"][0]) == 0
+    _check(host, ref, G, cols)
