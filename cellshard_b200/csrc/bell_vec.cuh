@@ -26,6 +26,20 @@ __device__ __forceinline__ uint32_t in_range8(uint32_t bc, uint32_t gene0, uint3
     return gene0 + 8u <= cols ? 0xffu : (1u << (cols - gene0)) - 1u;
 }
 
+// e / B and e % B for a block size B: a shift and a mask when B is a power
+// of two (every block size the choosers produce), a division otherwise.
+struct block_div {
+    uint32_t B;
+    int shift;
+    __device__ __forceinline__ explicit block_div(uint32_t b) : B(b), shift(-1) {
+#ifdef __CUDA_ARCH__
+        if (b != 0u && (b & (b - 1u)) == 0u) shift = __ffs((int) b) - 1;
+#endif
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t e) const { return shift >= 0 ? e >> shift : e / B; }
+    __device__ __forceinline__ uint32_t mod(uint32_t e) const { return shift >= 0 ? e & (B - 1u) : e % B; }
+};
+
 __device__ __forceinline__ uint16_t half_of(const uint4 &v, uint32_t q) {
     const uint32_t w = q < 4u ? (q < 2u ? v.x : v.y) : (q < 6u ? v.z : v.w);
     return (uint16_t) (w >> ((q & 1u) * 16u));
@@ -34,14 +48,14 @@ __device__ __forceinline__ uint16_t half_of(const uint4 &v, uint32_t q) {
 // N 16-byte value vectors of one lane (256 values apart) and their block
 // columns; positions past the row give zeros and CS_INVALID_COL.
 template <unsigned N>
-__device__ __forceinline__ void load_steps(const uint16_t *vrow, const uint32_t *bci, uint32_t B, uint32_t ell_cols,
-                                           uint32_t first, uint4 (&v)[N], uint32_t (&bc)[N]) {
+__device__ __forceinline__ void load_steps(const uint16_t *vrow, const uint32_t *bci, const block_div &bd,
+                                           uint32_t ell_cols, uint32_t first, uint4 (&v)[N], uint32_t (&bc)[N]) {
 #pragma unroll
     for (unsigned u = 0; u < N; ++u) {
         const uint32_t e0 = first + u * 256u;
         const bool in = e0 < ell_cols;
         v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
-        bc[u] = in ? __ldg(bci + e0 / B) : CS_INVALID_COL;
+        bc[u] = in ? __ldg(bci + bd.div(e0)) : CS_INVALID_COL;
     }
 }
 

@@ -243,6 +243,7 @@ __device__ __forceinline__ void bell_row(const cs_blocked_ell_view &src, uint32_
     row_acc<GR> a;
     init_acc(a);
     const uint32_t rb = B != 0u ? row / B : 0u;
+    const block_div bd(B);
     const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
     const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
     if (VEC) {
@@ -263,14 +264,14 @@ __device__ __forceinline__ void bell_row(const cs_blocked_ell_view &src, uint32_
                 const uint32_t e0 = base + u * 256u;
                 const bool in = e0 < src.ell_cols;
                 v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
-                bc[u] = in ? __ldg(bci + e0 / B) : CS_INVALID_COL;
+                bc[u] = in ? __ldg(bci + bd.div(e0)) : CS_INVALID_COL;
             }
             // the feature flags are checked per staged value, not per vector
             uint32_t nzall = 0u;
     #pragma unroll
             for (unsigned u = 0; u < U; ++u) {
                 const uint32_t e0 = base + u * 256u;
-                gene0[u] = bc[u] * B + (e0 % B);
+                gene0[u] = bc[u] * B + bd.mod(e0);
                 if (bc[u] == CS_INVALID_COL) continue;
                 uint32_t nz = nonzero_bits(v[u]);
                 if (nz != 0u && gene0[u] + 8u > src.cols) {
@@ -932,6 +933,7 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
         const uint32_t B = src.block_size;
         const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
         const uint32_t rb = B != 0u ? local / B : 0u;
+        const block_div bd(B);
         const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
         const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
         uint32_t run = EMIT ? major_ptr[out_row] : 0u;
@@ -947,10 +949,10 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
             for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
                 uint4 v[kRs];
                 uint32_t bcs[kRs];
-                load_steps(vrow, bci, B, src.ell_cols, b0, v, bcs);
+                load_steps(vrow, bci, bd, src.ell_cols, b0, v, bcs);
 #pragma unroll
                 for (unsigned u = 0; u < kRs; ++u) {
-                    const uint32_t gene0 = bcs[u] * B + (b0 + u * 256u) % B;
+                    const uint32_t gene0 = bcs[u] * B + bd.mod(b0 + u * 256u);
                     uint32_t live = live_bits8(v[u]) & in_range8(bcs[u], gene0, src.cols);
                     // gene0 is a multiple of 8: its 8 flags sit in one bitmap word
                     if (kbits != nullptr && live != 0u) live &= kbits[gene0 >> 5] >> (gene0 & 31u);

@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(kThreads) bell_row_live_kernel(cs_blocked_ell_
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t B = src.block_size;
     const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
+    const block_div bd(B);
     for (uint32_t row = blockIdx.x * kWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kWarps) {
         const uint32_t *bci = src.blockColIdx + (std::size_t) (row / B) * W;
         const uint16_t *vrow = src.val + (std::size_t) row * src.ell_cols;
@@ -51,13 +52,13 @@ __global__ void __launch_bounds__(kThreads) bell_row_live_kernel(cs_blocked_ell_
             // the next group of steps is loaded before the current one is counted
             uint4 v[kSteps], vn[kSteps];
             uint32_t bc[kSteps], bcn[kSteps];
-            load_steps(vrow, bci, B, src.ell_cols, lane * 8u, v, bc);
+            load_steps(vrow, bci, bd, src.ell_cols, lane * 8u, v, bc);
             for (uint32_t base = lane * 8u; base - lane * 8u < src.ell_cols; base += 256u * kSteps) {
-                load_steps(vrow, bci, B, src.ell_cols, base + 256u * kSteps, vn, bcn);
+                load_steps(vrow, bci, bd, src.ell_cols, base + 256u * kSteps, vn, bcn);
 #pragma unroll
                 for (unsigned u = 0; u < kSteps; ++u) {
                     const uint32_t e0 = base + u * 256u;
-                    n += __popc(live_bits8(v[u]) & in_range8(bc[u], bc[u] * B + e0 % B, src.cols));
+                    n += __popc(live_bits8(v[u]) & in_range8(bc[u], bc[u] * B + bd.mod(e0), src.cols));
                     v[u] = vn[u];
                     bc[u] = bcn[u];
                 }
@@ -85,6 +86,7 @@ __global__ void __launch_bounds__(kThreads) sell_from_bell_emit_kernel(cs_blocke
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t B = src.block_size;
     const uint32_t W = B != 0u ? src.ell_cols / B : 0u;
+    const block_div bd(B);
     for (uint32_t row = blockIdx.x * kWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kWarps) {
         const uint32_t slice = row / h;
         const uint32_t width = widths[slice];
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) sell_from_bell_emit_kernel(cs_blocke
             for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kSteps) {
                 uint4 v[kSteps];
                 uint32_t bc[kSteps];
-                load_steps(vrow, bci, B, src.ell_cols, b0, v, bc);
+                load_steps(vrow, bci, bd, src.ell_cols, b0, v, bc);
 #pragma unroll
                 for (unsigned u = 0; u < kSteps; u += 2u) {
                     // two 256-value steps in slot order (lanes in order, values in
@@ -104,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) sell_from_bell_emit_kernel(cs_blocke
                     uint32_t bits[2], gene0[2];
 #pragma unroll
                     for (unsigned k = 0; k < 2u; ++k) {
-                        gene0[k] = bc[u + k] * B + (b0 + (u + k) * 256u) % B;
+                        gene0[k] = bc[u + k] * B + bd.mod(b0 + (u + k) * 256u);
                         bits[k] = live_bits8(v[u + k]) & in_range8(bc[u + k], gene0[k], src.cols);
                     }
                     const uint32_t cnt = __popc(bits[0]) | (__popc(bits[1]) << 16);
