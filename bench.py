@@ -49,10 +49,10 @@ BLOCK = 16
 FALLBACK_HBM_GBS = 6650.0
 # launches per step: index, tile hist, group tiles, group scan, tile scatter, accumulate, combine
 LAUNCHES_PER_STEP = 7
-# DRAM bytes (read + write) of one moments_accumulate_kernel launch per kept row: the ncu capture
-# summarised in profiles/moments_accumulate_500k_x_32768.md read 924.15 MB and wrote 8.95 MB on a
-# 20,000-row case with 14,034 kept rows; traffic grows with the kept rows (each kept row's values
-# are read once), so a full launch's traffic = this x kept rows.
+# DRAM bytes (read + write) of one moments_accumulate_kernel launch per kept row, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of that kernel on the first 20,000 rows
+# of this workload: 924.15 MB read and 8.95 MB written for 14,034 kept rows.  Traffic grows with
+# the kept rows (each kept row's values are read once), so a full launch's traffic = this x kept rows.
 NCU_DRAM_BYTES_PER_KEPT_ROW = (924.15e6 + 8.95e6) / 14034
 
 
@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the check of the run's results against the FP64 restatement over all rows")
     p.add_argument("--e2e-parts", type=int, default=0,
                    help="group ranges whose result copies overlap the next range's work (0 = library default)")
     p.add_argument("--chunk-rows", type=int, default=0,
@@ -354,6 +356,13 @@ def run_product(args):
         e2e = {"ms": e2e_ms, "h2d": h2d, "d2h": d2h}
     clk = clocks.stop()
 
+    # parity of this very run: the last step's results against FP64 over all rows
+    parity = None
+    if rank == 0 and not args.no_parity:
+        step()
+        torch.cuda.synchronize()
+        parity = headline_parity(spec, bell, rk, fk, lab, out)
+
     step_ms, acc_ms, e2e_max = max_over_ranks(dist, [step_ms, acc_ms, e2e["ms"] if e2e else 0.0], "cuda")
     if e2e:
         e2e["ms"] = e2e_max
@@ -394,6 +403,8 @@ def run_product(args):
             result["e2e"] = {"value": whole_job_rate(world, kept_nnz, e2e["ms"]), "unit": "nnz/s",
                              "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                              "ms_per_step": e2e["ms"]}
+        if parity is not None:
+            result["parity"] = parity
         if world == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, args.cpu_seconds)
     if dist is not None:
@@ -401,6 +412,38 @@ def run_product(args):
         dist.destroy_process_group()
     if result is not None:
         print(json.dumps(result), flush=True)
+    if parity is not None and not parity["ok"]:
+        raise SystemExit(f"moments differ from FP64 by {parity['max_rel']:.3g} > {PARITY_RTOL:g}")
+
+
+PARITY_RTOL = 1e-6
+
+
+def headline_parity(spec, bell, rk, fk, lab, out):
+    """The step's sum, sumsq, mean and var (fp32 on the GPU) against the FP64 restatement
+    over every row of the partition: the Blocked-ELL is copied back in slabs of 32,768 rows
+    and the per-slab FP64 sums are added (exact for integer counts)."""
+    from oracle import oracle
+
+    threads = oracle.cpu_count()
+    W, E = bell.ell_width, bell.ell_cols
+
+    def fetch(r0, r1):
+        bci = bell.bci[(r0 // BLOCK) * W: ((r1 + BLOCK - 1) // BLOCK) * W].cpu().numpy().view(np.uint32)
+        val = bell.val[r0 * E: r1 * E].cpu().numpy().view(np.uint16)
+        return bci, val
+
+    t0 = time.perf_counter()
+    ref = oracle.group_moments_bell_slabs(fetch, spec.rows, spec.cols, BLOCK, E, rk, fk, lab, GROUPS, ddof=1,
+                                          nthreads=threads)
+    got = {k: out[k].cpu().numpy() for k in ("sum", "sumsq", "mean", "var")}
+    rows_ok = np.array_equal(out["group_rows"].cpu().numpy().astype(np.int64), ref["group_rows"].astype(np.int64))
+    err = oracle.moments_max_rel(got, ref)
+    worst = max(err.values())
+    return {"max_rel": worst, "per_output": err, "tolerance": PARITY_RTOL, "group_rows_equal": rows_ok,
+            "rows": spec.rows, "kept_rows": int(rk.sum()), "ok": bool(worst <= PARITY_RTOL and rows_ok),
+            "oracle": f"FP64 restatement over all rows in slabs of 32,768 on {threads} threads",
+            "oracle_s": round(time.perf_counter() - t0, 1)}
 
 
 def cpu_baseline_from_device(spec, bell, rk, fk, lab, row_nnz, seconds):

@@ -129,6 +129,58 @@ def group_moments_bell(rows, cols, B, ell_cols, bci, val, row_keep, feature_keep
             "group_rows": n}
 
 
+def group_moments_bell_slabs(fetch, rows, cols, B, ell_cols, row_keep, feature_keep, labels, G, ddof=1,
+                            slab_rows=32768, nthreads=1):
+    """FP64 moments of a Blocked-ELL matrix too large to hold on the host at once.
+
+    ``fetch(r0, r1)`` returns the host (bci, val) of rows [r0, r1) (r0 a multiple of B).
+    Per-slab FP64 sums and sums of squares are added; integer counts keep them exact,
+    so the totals equal one call over all rows.  The finishing rule is the one in
+    cs_oracle.c's moments worker: mean = S / n; var = max(Q - S * mean, 0) / (n - ddof)
+    when n > ddof; features the mask drops are all zero."""
+    slab_rows = max(B, slab_rows // B * B)
+    s = np.zeros((G, cols), np.float64)
+    q = np.zeros((G, cols), np.float64)
+    n = np.zeros(G, np.int64)
+    for r0 in range(0, rows, slab_rows):
+        r1 = min(rows, r0 + slab_rows)
+        bci, val = fetch(r0, r1)
+        part = group_moments_bell(r1 - r0, cols, B, ell_cols, bci, val, row_keep[r0:r1], None, labels[r0:r1], G,
+                                  ddof=ddof, nthreads=nthreads)
+        s += part["sum"]
+        q += part["sumsq"]
+        n += part["group_rows"].astype(np.int64)
+    keep = np.ones(cols, bool) if feature_keep is None else feature_keep.astype(bool)
+    s[:, ~keep] = 0.0
+    q[:, ~keep] = 0.0
+    nn = n.astype(np.float64)[:, None]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        mean = np.where(nn > 0, s / np.maximum(nn, 1.0), 0.0)
+        m2 = np.maximum(q - s * mean, 0.0)
+        var = np.where(nn > ddof, m2 / np.maximum(nn - ddof, 1.0), 0.0)
+    mean[:, ~keep] = 0.0
+    var[:, ~keep] = 0.0
+    return {"sum": s, "sumsq": q, "mean": mean, "var": var, "group_rows": n.astype(np.uint32)}
+
+
+def moments_max_rel(got: dict, ref: dict) -> dict:
+    """Largest relative error per output against the FP64 result: |got - ref| / |ref| for
+    sum, sumsq and mean (entries equal to the reference count as 0); variance relative to
+    max(|var|, 1e-12 * sumsq / n) so that exact zeros compare absolutely."""
+    out = {}
+    n = ref["group_rows"].astype(np.float64)
+    for k in ("sum", "sumsq", "mean", "var"):
+        g = np.asarray(got[k], np.float64)
+        e = ref[k]
+        d = np.abs(g - e)
+        scale = np.abs(e)
+        if k == "var":
+            scale = np.maximum(scale, 1e-12 * ref["sumsq"] / np.maximum(n, 1.0)[:, None])
+        err = np.where(d == 0.0, 0.0, d / np.maximum(scale, 1e-30))
+        out[k] = float(err.max(initial=0.0))
+    return out
+
+
 def group_moments_csr(rows, cols, ptr, idx, val, row_keep, feature_keep, labels, G, ddof=1, nthreads=1):
     gc = G * cols
     s, q, m, v = (np.zeros(gc, np.float64) for _ in range(4))

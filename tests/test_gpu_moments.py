@@ -196,3 +196,33 @@ def test_moments_to_host_matches_device_call(cuda, orc, parts):
         assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), k
     assert int(host["status"][0]) == 0
     _check(host, ref, G, cols)
+
+
+@pytest.mark.parametrize("chunk_rows", [64, 0])
+def test_moments_headline_layout(cuda, orc, chunk_rows):
+    """The headline workload's layout on 20,000 rows: 32,768 columns at ~4 % density as
+    Blocked-ELL-16 (ell_width near the 2,048 block columns), 64 uniform groups, a
+    Bernoulli(0.7) row mask and 20,000 kept features.  Chunks of 64 rows give every group
+    three or more chunks, so the fp64 cross-chunk combine is exercised; 0 is the library's
+    default chunking, as the headline runs it."""
+    from cellshard_b200 import runtime, synth
+    from cellshard_b200.device import blocked_ell_from_csr
+
+    G = 64
+    spec = synth.grouped_reduction_spec(20000)
+    csr = synth.make_csr(spec)
+    bell = blocked_ell_from_csr(csr, 16)
+    del csr
+    assert bell.cols == 32768 and bell.ell_width >= 1900
+    rk, fk, lab = synth.masks_and_labels(spec.rows, spec.cols, G, 0.7, 20000)
+    per_group = np.bincount(lab[rk == 1], minlength=G)
+    if chunk_rows:
+        assert int(per_group.min()) > 2 * chunk_rows
+    bci, val = _host(bell)
+    ref = orc.group_moments_bell(spec.rows, spec.cols, 16, bell.ell_cols, bci, val, rk, fk, lab, G, ddof=1,
+                                 nthreads=orc.cpu_count())
+    res = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab), ddof=1, chunk_rows=chunk_rows)
+    _check(res, ref, G, spec.cols)
+    err = orc.moments_max_rel({k: res[k].cpu().numpy() for k in ("sum", "sumsq", "mean", "var")}, ref)
+    assert max(err.values()) <= RTOL, err
+

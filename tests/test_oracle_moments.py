@@ -67,3 +67,25 @@ def test_bell_oracle_matches_csr_oracle(orc):
     b = orc.group_moments_bell(rows, cols, B, ell_cols, bci, bval, rk, None, lab, G, ddof=0, nthreads=4)
     for k in ("sum", "sumsq", "mean", "var", "group_rows"):
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_moments_slab_oracle_matches_one_call(orc):
+    """The slab-accumulated FP64 oracle the benchmark uses over its full partition equals
+    one oracle call over all rows (integer counts: exact sums)."""
+    rows, cols, B, G = 301, 70, 16, 4
+    ptr, idx, val = random_csr(rows, cols, 0.2, 3, 0.1, True)
+    oracle = orc
+    b = oracle.blocked_ell_from_csr(rows, cols, ptr, idx, val, B)
+    W = b["ell_cols"] // B
+    rng = np.random.default_rng(1)
+    rk = (rng.random(rows) < 0.7).astype(np.uint8)
+    fk = (rng.random(cols) < 0.8).astype(np.uint8)
+    lab = rng.integers(0, G, rows).astype(np.uint32)
+    one = oracle.group_moments_bell(rows, cols, B, b["ell_cols"], b["bci"], b["val"], rk, fk, lab, G, ddof=1)
+    fetch = lambda r0, r1: (b["bci"][(r0 // B) * W:((r1 + B - 1) // B) * W], b["val"][r0 * b["ell_cols"]:
+                                                                                     r1 * b["ell_cols"]])
+    slabs = oracle.group_moments_bell_slabs(fetch, rows, cols, B, b["ell_cols"], rk, fk, lab, G, ddof=1, slab_rows=64)
+    for k in ("sum", "sumsq", "mean", "var"):
+        assert np.allclose(slabs[k], one[k], rtol=1e-15, atol=0), k
+    assert np.array_equal(slabs["group_rows"], one["group_rows"])
+    assert max(oracle.moments_max_rel(slabs, one).values()) <= 1e-15
