@@ -142,6 +142,22 @@ class PartitionRecord(C.Structure):
                 ("a3", vp), ("device_id", C.c_int), ("format", u32), ("host_view", C.c_ubyte * 64)]
 
 
+class StagedPart(C.Structure):
+    """device::partition_record (one record of a sharded_device residency table)."""
+    _fields_ = [("allocation", vp), ("allocation_bytes", sz), ("storage", vp), ("view", vp), ("a0", vp), ("a1", vp),
+                ("a2", vp), ("a3", vp), ("group_begin", C.c_ulong), ("group_end", C.c_ulong), ("device_id", C.c_int),
+                ("_align16", C.c_ubyte * 12)]
+
+
+class CachedAllocation(C.Structure):
+    _fields_ = [("ptr", vp), ("bytes", sz), ("device_id", C.c_int)]
+
+
+class ShardedDevice(C.Structure):
+    _fields_ = [("capacity", C.c_ulong), ("parts", C.POINTER(StagedPart)), ("cache_count", C.c_ulong),
+                ("cache_capacity", C.c_ulong), ("cache", C.POINTER(CachedAllocation))]
+
+
 class ServeConfig(C.Structure):
     _fields_ = [("scratch_budget_bytes", u64), ("max_inflight", u32), ("chunk_rows", u32), ("idle_exit_us", u32),
                 ("ctas_per_sm", u32)]
@@ -284,6 +300,21 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_upload_blocked_ell": (C.c_int, [P(HostBlockedEll), P(PartitionRecord), vp]),
     "cs_b200_upload_sliced_ell": (C.c_int, [P(HostSlicedEll), P(PartitionRecord), vp]),
     "cs_b200_release_partition": (C.c_int, [P(PartitionRecord)]),
+    "cs_b200_sharded_device_reserve": (C.c_int, [P(ShardedDevice), C.c_ulong]),
+    "cs_b200_sharded_device_clear": (C.c_int, [P(ShardedDevice)]),
+    "cs_b200_stage_partition_compressed": (C.c_int, [P(ShardedDevice), C.c_ulong, P(HostCompressed), C.c_int, vp]),
+    "cs_b200_stage_partition_blocked_ell": (C.c_int, [P(ShardedDevice), C.c_ulong, P(HostBlockedEll), C.c_int, vp]),
+    "cs_b200_stage_partition_sliced_ell": (C.c_int, [P(ShardedDevice), C.c_ulong, P(HostSlicedEll), C.c_int, vp]),
+    "cs_b200_stage_shard_compressed": (C.c_int, [P(ShardedDevice), C.c_ulong, C.c_ulong, P(P(HostCompressed)),
+                                                 C.c_int, vp]),
+    "cs_b200_stage_shard_blocked_ell": (C.c_int, [P(ShardedDevice), C.c_ulong, C.c_ulong, P(P(HostBlockedEll)),
+                                                  C.c_int, vp]),
+    "cs_b200_stage_shard_sliced_ell": (C.c_int, [P(ShardedDevice), C.c_ulong, C.c_ulong, P(P(HostSlicedEll)),
+                                                 C.c_int, vp]),
+    "cs_b200_release_staged_partition": (C.c_int, [P(ShardedDevice), C.c_ulong]),
+    "cs_b200_staged_bytes_compressed": (C.c_int, [P(P(HostCompressed)), C.c_ulong, P(sz)]),
+    "cs_b200_staged_bytes_blocked_ell": (C.c_int, [P(P(HostBlockedEll)), C.c_ulong, P(sz)]),
+    "cs_b200_staged_bytes_sliced_ell": (C.c_int, [P(P(HostSlicedEll)), C.c_ulong, P(sz)]),
     "cs_b200_serve_open": (C.c_int, [P(BlockedEllView), u32, P(ServeConfig), P(vp)]),
     "cs_b200_serve_submit": (C.c_int, [vp, P(ServeRequest), P(u64)]),
     "cs_b200_serve_poll": (C.c_int, [vp, u64, P(u32), P(C.c_double)]),

@@ -987,6 +987,120 @@ CS_API int cs_b200_upload_sliced_ell(const cs_host_sliced_ell *src, cs_partition
 CS_API int cs_b200_release_partition(cs_partition_record *record);
 
 /* ------------------------------------------------------------------------ */
+/* Shard-level staging: the residency state of a sharded matrix on a device  */
+/* (device::sharded_device<MatrixT>, runtime/device/sharded_device.cuh:22-52, */
+/* 160-243, 992-1212, 1436-1721).  The three structs below are field for     */
+/* field the reference's partition_record, cached_allocation and              */
+/* sharded_device (one layout for every MatrixT), so a reference state table */
+/* crosses this ABI unchanged.                                               */
+/*                                                                          */
+/* Device layout of one staged group (a single partition, or every partition */
+/* of a shard in one packed allocation): the partitions' device views packed */
+/* back to back at the start (record.view points at its own), then each     */
+/* partition's arrays, every array on a 256-byte boundary.  Record arrays:   */
+/*   compressed   a0 majorPtr, a1 minorIdx, a2 val                          */
+/*   Blocked-ELL  a0 blockColIdx, a1 val                                    */
+/*   Sliced-ELL   a0 slice_row_offsets, a1 slice_widths, a2 col_idx, a3 val;*/
+/*                the u32 slot offsets of the device view sit at            */
+/*                a1 + round_up(4 * slice_count, 256)                      */
+/* The group's owner (its first partition) holds allocation /              */
+/* allocation_bytes / storage; the others hold 0 there.  A released group's */
+/* allocation goes to the state's cache (at most 16 entries; the smallest   */
+/* cached block that fits is reused by the next upload on that device)     */
+/* instead of cudaFree, as the reference's release_partition does.          */
+/*                                                                          */
+/* Stream order: payload arrays are copied with cudaMemcpyAsync on `stream`  */
+/* (pinned host parts give truly asynchronous copies); the device views and */
+/* the Sliced-ELL slot offsets are written by kernels on the same stream    */
+/* whose arguments carry the data, so nothing on the host stack is read    */
+/* after the call returns.  No call synchronises.  Like the reference, an   */
+/* upload leaves `device_id` current and a release leaves the record's      */
+/* device current.                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* device::partition_record<MatrixT> (sharded_device.cuh:22-35) */
+typedef struct CS_ALIGN16 cs_staged_part {
+    void *allocation;          /* packed device block (group owner only) */
+    size_t allocation_bytes;   /* bytes of that block (a cached block may be larger than needed) */
+    void *storage;             /* == allocation on the owner */
+    void *view;                /* device address of this partition's cs_*_view */
+    void *a0, *a1, *a2, *a3;   /* device arrays, per format as listed above */
+    unsigned long group_begin; /* partitions staged together: [group_begin, group_end) */
+    unsigned long group_end;
+    int device_id;             /* -1 when not resident */
+} cs_staged_part;
+
+/* device::cached_allocation (sharded_device.cuh:37-41) */
+typedef struct cs_cached_allocation {
+    void *ptr;
+    size_t bytes;
+    int device_id;
+} cs_cached_allocation;
+
+/* device::sharded_device<MatrixT> (sharded_device.cuh:44-51) */
+typedef struct cs_sharded_device {
+    unsigned long capacity;
+    cs_staged_part *parts;       /* malloc'd by cs_b200_sharded_device_reserve */
+    unsigned long cache_count;
+    unsigned long cache_capacity;
+    cs_cached_allocation *cache; /* malloc'd; at most 16 live entries */
+} cs_sharded_device;
+
+#define CS_STAGE_CACHE_ENTRIES 16u
+
+/* device::reserve (sharded_device.cuh:160-178): grows the record table to
+ * `capacity` records (new records zeroed, device_id -1); records move
+ * bitwise. */
+CS_API int cs_b200_sharded_device_reserve(cs_sharded_device *state, unsigned long capacity);
+/* device::clear (sharded_device.cuh:136-158): releases every resident
+ * partition, frees every cached block on its device and the tables. */
+CS_API int cs_b200_sharded_device_clear(cs_sharded_device *state);
+
+/* device::upload_partition_async (sharded_device.cuh:1019-1043, 1144-1166):
+ * stages one host partition as record `part_id` on `device_id` (its group is
+ * [part_id, part_id + 1)).  A partition already resident on that device is
+ * left as it is; one resident elsewhere is released first. */
+CS_API int cs_b200_stage_partition_compressed(cs_sharded_device *state, unsigned long part_id,
+                                              const cs_host_compressed *src, int device_id, cs_stream_t stream);
+CS_API int cs_b200_stage_partition_blocked_ell(cs_sharded_device *state, unsigned long part_id,
+                                               const cs_host_blocked_ell *src, int device_id, cs_stream_t stream);
+CS_API int cs_b200_stage_partition_sliced_ell(cs_sharded_device *state, unsigned long part_id,
+                                              const cs_host_sliced_ell *src, int device_id, cs_stream_t stream);
+
+/* device::upload_shard_async for the compressed and Blocked-ELL formats
+ * (upload_{compressed,blocked_ell}_shard_current_device_async,
+ * sharded_device.cuh:1223-1435): the `count` partitions `parts[0..count)`
+ * become records [first_part, first_part + count), all in ONE packed
+ * allocation with their views back to back (the reference does the same for
+ * compressed and Blocked-ELL; Sliced-ELL shards are packed here too, where
+ * the reference uploads them one partition at a time).  If every partition
+ * of the range is already resident on `device_id` nothing happens;
+ * otherwise the resident ones are released first. */
+CS_API int cs_b200_stage_shard_compressed(cs_sharded_device *state, unsigned long first_part, unsigned long count,
+                                          const cs_host_compressed *const *parts, int device_id, cs_stream_t stream);
+CS_API int cs_b200_stage_shard_blocked_ell(cs_sharded_device *state, unsigned long first_part, unsigned long count,
+                                           const cs_host_blocked_ell *const *parts, int device_id,
+                                           cs_stream_t stream);
+CS_API int cs_b200_stage_shard_sliced_ell(cs_sharded_device *state, unsigned long first_part, unsigned long count,
+                                          const cs_host_sliced_ell *const *parts, int device_id, cs_stream_t stream);
+
+/* device::release_partition (sharded_device.cuh:1168-1200): releases the
+ * whole group record `part_id` belongs to; the owner's block goes to the
+ * cache (cudaFree once 16 blocks are cached).  A record whose group range is
+ * empty (a standalone upload) is freed on its own.  Not resident: success. */
+CS_API int cs_b200_release_staged_partition(cs_sharded_device *state, unsigned long part_id);
+
+/* Bytes one packed group of `count` partitions takes on the device (views +
+ * arrays, 256-byte aligned): the shard-level counterpart of
+ * cs_b200_device_partition_bytes_* (which is this with count 1). */
+CS_API int cs_b200_staged_bytes_compressed(const cs_host_compressed *const *parts, unsigned long count,
+                                           size_t *out_bytes);
+CS_API int cs_b200_staged_bytes_blocked_ell(const cs_host_blocked_ell *const *parts, unsigned long count,
+                                            size_t *out_bytes);
+CS_API int cs_b200_staged_bytes_sliced_ell(const cs_host_sliced_ell *const *parts, unsigned long count,
+                                           size_t *out_bytes);
+
+/* ------------------------------------------------------------------------ */
 /* Batched conversion of many uneven partitions (no reference counterpart:  */
 /* the reference converts one partition per call, sliced_ell_from_          */
 /* compressed.cuh:96-254, and plans one per call, major_nnz_raw.cuh:64-120). */

@@ -37,6 +37,8 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -166,18 +168,99 @@ static_assert(sizeof(compressed_view) == sizeof(cs_compressed_view), "compressed
 static_assert(sizeof(blocked_ell_view) == sizeof(cs_blocked_ell_view), "blocked_ell_view layout");
 static_assert(sizeof(sliced_ell_view) == sizeof(cs_sliced_ell_view), "sliced_ell_view layout");
 
-// One staged partition: `view` is the device address of the view descriptor
-// at the start of the packed block; `host_view` its host copy.
+// device::partition_record<MatrixT> (sharded_device.cuh:22-35): field for
+// field the reference's record, the same for every MatrixT.  `view` is the
+// device address of the partition's view; a0..a3 its device arrays
+// (compressed: majorPtr, minorIdx, val; Blocked-ELL: blockColIdx, val;
+// Sliced-ELL: slice_row_offsets, slice_widths, col_idx, val, with the u32
+// slot offsets at a1 + round_up(4 * slice_count, 256)).
 template <typename MatrixT>
 struct alignas(16) partition_record {
-    cs_partition_record rec;
+    void *allocation;
+    std::size_t allocation_bytes;
+    void *storage;
+    void *view;
+    void *a0;
+    void *a1;
+    void *a2;
+    void *a3;
+    unsigned long group_begin;
+    unsigned long group_end;
+    int device_id;
 };
+
+// sharded_device.cuh:37-41
+struct cached_allocation {
+    void *ptr;
+    std::size_t bytes;
+    int device_id;
+};
+
+// sharded_device.cuh:44-51: the residency table of a sharded matrix
+template <typename MatrixT>
+struct sharded_device {
+    unsigned long capacity;
+    partition_record<MatrixT> *parts;
+    unsigned long cache_count;
+    unsigned long cache_capacity;
+    cached_allocation *cache;
+};
+
+static_assert(sizeof(partition_record<sparse::compressed>) == sizeof(cs_staged_part) &&
+                  offsetof(partition_record<sparse::compressed>, device_id) == offsetof(cs_staged_part, device_id) &&
+                  offsetof(partition_record<sparse::compressed>, group_begin) ==
+                      offsetof(cs_staged_part, group_begin),
+              "partition_record layout");
+static_assert(sizeof(cached_allocation) == sizeof(cs_cached_allocation), "cached_allocation layout");
+static_assert(sizeof(sharded_device<sparse::compressed>) == sizeof(cs_sharded_device) &&
+                  offsetof(sharded_device<sparse::compressed>, cache) == offsetof(cs_sharded_device, cache),
+              "sharded_device layout");
 
 namespace detail {
 inline cudaError_t staged(int ok) {
     if (ok) return cudaSuccess;
     const cudaError_t e = cudaGetLastError();
     return e != cudaSuccess ? e : cudaErrorInvalidValue;
+}
+template <typename MatrixT>
+inline cs_sharded_device *as_state(sharded_device<MatrixT> *s) {
+    return reinterpret_cast<cs_sharded_device *>(s);
+}
+inline const cs_host_compressed *host(const sparse::compressed *m) {
+    return reinterpret_cast<const cs_host_compressed *>(m);
+}
+inline const cs_host_blocked_ell *host(const sparse::blocked_ell *m) {
+    return reinterpret_cast<const cs_host_blocked_ell *>(m);
+}
+inline const cs_host_sliced_ell *host(const sparse::sliced_ell *m) {
+    return reinterpret_cast<const cs_host_sliced_ell *>(m);
+}
+inline int stage_one(cs_sharded_device *st, unsigned long part, const sparse::compressed *m, int dev,
+                     cudaStream_t s) {
+    return cs_b200_stage_partition_compressed(st, part, host(m), dev, reinterpret_cast<cs_stream_t>(s));
+}
+inline int stage_one(cs_sharded_device *st, unsigned long part, const sparse::blocked_ell *m, int dev,
+                     cudaStream_t s) {
+    return cs_b200_stage_partition_blocked_ell(st, part, host(m), dev, reinterpret_cast<cs_stream_t>(s));
+}
+inline int stage_one(cs_sharded_device *st, unsigned long part, const sparse::sliced_ell *m, int dev,
+                     cudaStream_t s) {
+    return cs_b200_stage_partition_sliced_ell(st, part, host(m), dev, reinterpret_cast<cs_stream_t>(s));
+}
+inline int stage_many(cs_sharded_device *st, unsigned long first, unsigned long n, sparse::compressed *const *m,
+                      int dev, cudaStream_t s) {
+    return cs_b200_stage_shard_compressed(st, first, n, reinterpret_cast<const cs_host_compressed *const *>(m), dev,
+                                          reinterpret_cast<cs_stream_t>(s));
+}
+inline int stage_many(cs_sharded_device *st, unsigned long first, unsigned long n, sparse::blocked_ell *const *m,
+                      int dev, cudaStream_t s) {
+    return cs_b200_stage_shard_blocked_ell(st, first, n, reinterpret_cast<const cs_host_blocked_ell *const *>(m),
+                                           dev, reinterpret_cast<cs_stream_t>(s));
+}
+inline int stage_many(cs_sharded_device *st, unsigned long first, unsigned long n, sparse::sliced_ell *const *m,
+                      int dev, cudaStream_t s) {
+    return cs_b200_stage_shard_sliced_ell(st, first, n, reinterpret_cast<const cs_host_sliced_ell *const *>(m), dev,
+                                          reinterpret_cast<cs_stream_t>(s));
 }
 } // namespace detail
 
@@ -195,35 +278,819 @@ inline std::size_t device_partition_bytes(const sparse::sliced_ell *src) {
     return cs_b200_device_partition_bytes_sliced_ell(reinterpret_cast<const cs_host_sliced_ell *>(src), &n) ? n : 0;
 }
 
-inline cudaError_t upload_async(const sparse::compressed *src, partition_record<sparse::compressed> *record,
-                                cudaStream_t stream) {
-    return detail::staged(cs_b200_upload_compressed(reinterpret_cast<const cs_host_compressed *>(src), &record->rec,
-                                                    reinterpret_cast<cs_stream_t>(stream)));
+template <typename MatrixT>
+inline void zero_record(partition_record<MatrixT> *record) {
+    std::memset(record, 0, sizeof(*record));
+    record->device_id = -1;
 }
-inline cudaError_t upload_async(const sparse::blocked_ell *src, partition_record<sparse::blocked_ell> *record,
-                                cudaStream_t stream) {
-    return detail::staged(cs_b200_upload_blocked_ell(reinterpret_cast<const cs_host_blocked_ell *>(src),
-                                                     &record->rec, reinterpret_cast<cs_stream_t>(stream)));
+
+// device::upload_async (sharded_device.cuh:400-756): one packed block on the
+// current device holding the view and the arrays; stream-ordered, no sync.
+// The record stands alone (empty group range), as the reference's upload
+// leaves it; release() frees it.
+template <typename MatrixT>
+inline cudaError_t upload_async(const MatrixT *src, partition_record<MatrixT> *record, cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    zero_record(record);
+    cs_sharded_device one{1ul, reinterpret_cast<cs_staged_part *>(record), 0ul, 0ul, nullptr};
+    if (!detail::stage_one(&one, 0ul, src, dev, stream)) return detail::staged(0);
+    record->group_begin = record->group_end = 0ul;
+    return cudaSuccess;
 }
-inline cudaError_t upload_async(const sparse::sliced_ell *src, partition_record<sparse::sliced_ell> *record,
-                                cudaStream_t stream) {
-    return detail::staged(cs_b200_upload_sliced_ell(reinterpret_cast<const cs_host_sliced_ell *>(src), &record->rec,
-                                                    reinterpret_cast<cs_stream_t>(stream)));
-}
+// device::upload: the same, then the stream is synchronised.
 template <typename MatrixT>
 inline cudaError_t upload(const MatrixT *src, partition_record<MatrixT> *record) {
-    return upload_async(src, record, (cudaStream_t) 0);
+    cudaError_t e = upload_async(src, record, (cudaStream_t) 0);
+    return e != cudaSuccess ? e : cudaStreamSynchronize((cudaStream_t) 0);
 }
+// device::release (sharded_device.cuh:959-991): frees a standalone record.
 template <typename MatrixT>
 inline cudaError_t release(partition_record<MatrixT> *record) {
-    return detail::staged(cs_b200_release_partition(&record->rec));
+    cs_sharded_device one{1ul, reinterpret_cast<cs_staged_part *>(record), 0ul, 0ul, nullptr};
+    record->group_begin = record->group_end = 0ul;
+    return detail::staged(cs_b200_release_staged_partition(&one, 0ul));
 }
-// The staged view, usable on the host side of a launch.
-template <typename ViewT, typename MatrixT>
-inline ViewT staged_view(const partition_record<MatrixT> *record) {
-    ViewT v;
-    std::memcpy(&v, record->rec.host_view, sizeof(v));
+
+// Host copy of a staged partition's device view, from its host part's
+// metadata and the record's arrays (what reference callers assemble by hand
+// from a0..a3, e.g. src/convert/sliced_ell_from_compressed.cuh:204-224).
+inline compressed_view staged_view(const sparse::compressed *m, const partition_record<sparse::compressed> *r) {
+    compressed_view v;
+    v.rows = m->rows;
+    v.cols = m->cols;
+    v.nnz = m->nnz;
+    v.axis = m->axis;
+    v.majorPtr = static_cast<unsigned int *>(r->a0);
+    v.minorIdx = static_cast<unsigned int *>(r->a1);
+    v.val = static_cast<__half *>(r->a2);
     return v;
+}
+inline blocked_ell_view staged_view(const sparse::blocked_ell *m, const partition_record<sparse::blocked_ell> *r) {
+    blocked_ell_view v;
+    v.rows = m->rows;
+    v.cols = m->cols;
+    v.nnz = m->nnz;
+    v.block_size = m->block_size;
+    v.ell_cols = m->ell_cols;
+    v.blockColIdx = static_cast<unsigned int *>(r->a0);
+    v.val = static_cast<__half *>(r->a1);
+    return v;
+}
+inline sliced_ell_view staged_view(const sparse::sliced_ell *m, const partition_record<sparse::sliced_ell> *r) {
+    sliced_ell_view v;
+    v.rows = m->rows;
+    v.cols = m->cols;
+    v.nnz = m->nnz;
+    v.slice_count = m->slice_count;
+    v.slice_rows = m->slice_count ? m->slice_row_offsets[1] - m->slice_row_offsets[0] : 0u;
+    v.slice_row_offsets = static_cast<unsigned int *>(r->a0);
+    v.slice_widths = static_cast<unsigned int *>(r->a1);
+    v.slice_slot_offsets = reinterpret_cast<unsigned int *>(static_cast<char *>(r->a1) +
+                                                           (((std::size_t) m->slice_count * 4u + 255u) / 256u) * 256u);
+    v.col_idx = static_cast<unsigned int *>(r->a2);
+    v.val = static_cast<__half *>(r->a3);
+    return v;
+}
+
+} // namespace device
+
+// ---------------------------------------------------------------------------
+// sharded<MatrixT>: the metadata-only stitched matrix (runtime/layout/sharded.cuh
+// :29-50, 52-362) and its host helpers (runtime/host/sharded_host.cuh:15-395,
+// 528-560).  parts[i] may be null (not materialised on the host);
+// partition_rows / partition_nnz / partition_aux stay valid as metadata;
+// shard_offsets group whole partitions into shards; shard_parts[s] is the
+// first partition of shard s.  The cut rules of the re-sharding helpers are
+// the reference's, so the same partitions give the same shards.
+// ---------------------------------------------------------------------------
+template <typename MatrixT>
+struct alignas(16) sharded {
+    unsigned long rows;
+    unsigned long cols;
+    unsigned long nnz;
+    unsigned long num_partitions;
+    unsigned long partition_capacity;
+    MatrixT **parts;
+    unsigned long *partition_offsets;
+    unsigned long *partition_rows;
+    unsigned long *partition_nnz;
+    unsigned long *partition_aux;
+    unsigned long num_shards;
+    unsigned long shard_capacity;
+    unsigned long *shard_offsets;
+    unsigned long *shard_parts;
+};
+
+// runtime/storage/shard_storage.cuh:33-41.  The only backend the reference
+// fetches partitions from is its `.csh5` (HDF5) dataset, which this library
+// does not read: parts must be materialised on the host before they are
+// staged, and fetch_partition / fetch_shard report failure with a message.
+struct shard_storage;
+typedef int (*shard_storage_open_fn)(shard_storage *s);
+typedef void (*shard_storage_close_fn)(shard_storage *s);
+enum { shard_storage_backend_none = 0, shard_storage_backend_dataset_h5 = 1 };
+struct shard_storage {
+    unsigned int backend;
+    std::uint32_t role;
+    std::uint32_t capability_flags;
+    char *source_path;
+    void *backend_state;
+    shard_storage_open_fn open_backend;
+    shard_storage_close_fn close_backend;
+};
+inline void init(shard_storage *s) { std::memset(s, 0, sizeof(*s)); }
+inline void clear(shard_storage *s) {
+    if (s->close_backend != nullptr) s->close_backend(s);
+    std::free(s->source_path);
+    std::memset(s, 0, sizeof(*s));
+}
+
+namespace sparse {
+// formats/blocked_ell.cuh:43-57, sliced_ell.cuh:30-40
+inline unsigned long pack_blocked_ell_aux(types::u32 block_size, unsigned long ell_width) {
+    return (ell_width << 16u) | (unsigned long) block_size;
+}
+inline types::u32 unpack_blocked_ell_block_size(unsigned long aux) { return (types::u32) (aux & 0xfffful); }
+inline unsigned long unpack_blocked_ell_ell_width(unsigned long aux) { return aux >> 16u; }
+inline unsigned long pack_sliced_ell_aux(types::u32 slice_count, types::u32 total_slots) {
+    return ((unsigned long) total_slots << 32u) | (unsigned long) slice_count;
+}
+inline types::u32 unpack_sliced_ell_slice_count(unsigned long aux) { return (types::u32) (aux & 0xfffffffful); }
+inline types::u32 unpack_sliced_ell_total_slots(unsigned long aux) { return (types::u32) (aux >> 32u); }
+inline types::u32 total_slots(const sliced_ell *m) {
+    types::u32 t = 0u;
+    for (types::u32 s = 0; s < m->slice_count; ++s)
+        t += (m->slice_row_offsets[s + 1u] - m->slice_row_offsets[s]) * m->slice_widths[s];
+    return t;
+}
+} // namespace sparse
+
+template <typename MatrixT>
+inline void init(sharded<MatrixT> *m) {
+    std::memset(m, 0, sizeof(*m));
+}
+
+inline unsigned long partition_nnz(const sparse::compressed *m) { return m->nnz; }
+inline unsigned long partition_nnz(const sparse::blocked_ell *m) { return m->nnz; }
+inline unsigned long partition_nnz(const sparse::sliced_ell *m) { return m->nnz; }
+inline unsigned long partition_aux(const sparse::compressed *m) { return m->axis; }
+inline unsigned long partition_aux(const sparse::blocked_ell *m) {
+    return sparse::pack_blocked_ell_aux(m->block_size, m->block_size ? m->ell_cols / m->block_size : 0u);
+}
+inline unsigned long partition_aux(const sparse::sliced_ell *m) {
+    return sparse::pack_sliced_ell_aux(m->slice_count, sparse::total_slots(m));
+}
+
+// destroy(): the part's packed storage, then the part itself (parts are new'ed)
+template <typename MatrixT>
+inline void destroy(MatrixT *m) {
+    if (m == nullptr) return;
+    sparse::clear(m);
+    delete m;
+}
+
+template <typename MatrixT>
+inline void clear(sharded<MatrixT> *m) {
+    for (unsigned long i = 0; m->parts != nullptr && i < m->num_partitions; ++i) destroy(m->parts[i]);
+    std::free(m->parts);
+    std::free(m->partition_offsets);
+    std::free(m->partition_rows);
+    std::free(m->partition_nnz);
+    std::free(m->partition_aux);
+    std::free(m->shard_offsets);
+    std::free(m->shard_parts);
+    init(m);
+}
+
+template <typename MatrixT>
+inline int reserve_partitions(sharded<MatrixT> *m, unsigned long capacity) {
+    if (capacity <= m->partition_capacity) return 1;
+    auto *parts = static_cast<MatrixT **>(std::calloc(capacity, sizeof(MatrixT *)));
+    auto *offs = static_cast<unsigned long *>(std::calloc(capacity + 1u, sizeof(unsigned long)));
+    auto *rows = static_cast<unsigned long *>(std::calloc(capacity, sizeof(unsigned long)));
+    auto *nnz = static_cast<unsigned long *>(std::calloc(capacity, sizeof(unsigned long)));
+    auto *aux = static_cast<unsigned long *>(std::calloc(capacity, sizeof(unsigned long)));
+    if (!parts || !offs || !rows || !nnz || !aux) {
+        std::free(parts);
+        std::free(offs);
+        std::free(rows);
+        std::free(nnz);
+        std::free(aux);
+        return 0;
+    }
+    const unsigned long n = m->num_partitions;
+    if (n != 0u) {
+        std::memcpy(parts, m->parts, n * sizeof(MatrixT *));
+        std::memcpy(offs, m->partition_offsets, (n + 1u) * sizeof(unsigned long));
+        std::memcpy(rows, m->partition_rows, n * sizeof(unsigned long));
+        std::memcpy(nnz, m->partition_nnz, n * sizeof(unsigned long));
+        std::memcpy(aux, m->partition_aux, n * sizeof(unsigned long));
+    }
+    std::free(m->parts);
+    std::free(m->partition_offsets);
+    std::free(m->partition_rows);
+    std::free(m->partition_nnz);
+    std::free(m->partition_aux);
+    m->parts = parts;
+    m->partition_offsets = offs;
+    m->partition_rows = rows;
+    m->partition_nnz = nnz;
+    m->partition_aux = aux;
+    m->partition_capacity = capacity;
+    return 1;
+}
+
+template <typename MatrixT>
+inline int reserve_shards(sharded<MatrixT> *m, unsigned long capacity) {
+    if (capacity <= m->shard_capacity) return 1;
+    auto *offs = static_cast<unsigned long *>(std::calloc(capacity + 1u, sizeof(unsigned long)));
+    auto *sp = static_cast<unsigned long *>(std::calloc(capacity + 1u, sizeof(unsigned long)));
+    if (!offs || !sp) {
+        std::free(offs);
+        std::free(sp);
+        return 0;
+    }
+    if (m->shard_offsets != nullptr && m->num_shards != 0u) {
+        std::memcpy(offs, m->shard_offsets, (m->num_shards + 1u) * sizeof(unsigned long));
+        if (m->shard_parts != nullptr) std::memcpy(sp, m->shard_parts, (m->num_shards + 1u) * sizeof(unsigned long));
+    }
+    std::free(m->shard_offsets);
+    std::free(m->shard_parts);
+    m->shard_offsets = offs;
+    m->shard_parts = sp;
+    m->shard_capacity = capacity;
+    return 1;
+}
+
+// shard s starts at the first partition whose first row is >= its first row
+template <typename MatrixT>
+inline void rebuild_shard_parts(sharded<MatrixT> *m) {
+    if (!m->shard_parts || !m->shard_offsets || !m->partition_offsets) return;
+    unsigned long part = 0;
+    for (unsigned long s = 0; s < m->num_shards; ++s) {
+        while (part < m->num_partitions && m->partition_offsets[part] < m->shard_offsets[s]) ++part;
+        m->shard_parts[s] = part;
+    }
+    m->shard_parts[m->num_shards] = m->num_partitions;
+}
+
+template <typename MatrixT>
+inline void rebuild_partition_offsets(sharded<MatrixT> *m) {
+    m->rows = 0;
+    m->nnz = 0;
+    if (!m->partition_offsets) return;
+    m->partition_offsets[0] = 0;
+    for (unsigned long i = 0; i < m->num_partitions; ++i) {
+        m->partition_offsets[i + 1u] = m->partition_offsets[i] + m->partition_rows[i];
+        m->nnz += m->partition_nnz[i];
+    }
+    m->rows = m->partition_offsets[m->num_partitions];
+}
+
+template <typename MatrixT>
+inline int set_shards_to_partitions(sharded<MatrixT> *m) {
+    if (!reserve_shards(m, m->num_partitions)) return 0;
+    m->num_shards = m->num_partitions;
+    for (unsigned long i = 0; i <= m->num_partitions; ++i) {
+        m->shard_offsets[i] = m->partition_offsets ? m->partition_offsets[i] : 0u;
+        m->shard_parts[i] = i;
+    }
+    return 1;
+}
+
+// metadata-only partitions (parts left null): sharded_host.cuh:145-168
+template <typename MatrixT>
+inline int define_partitions(sharded<MatrixT> *m, unsigned long cols, unsigned long num_partitions,
+                             const unsigned long *partition_rows, const unsigned long *partition_nnz,
+                             const unsigned long *partition_aux_in) {
+    clear(m);
+    if (!reserve_partitions(m, num_partitions)) return 0;
+    m->cols = cols;
+    m->num_partitions = num_partitions;
+    for (unsigned long i = 0; i < num_partitions; ++i) {
+        m->parts[i] = nullptr;
+        m->partition_rows[i] = partition_rows ? partition_rows[i] : 0u;
+        m->partition_nnz[i] = partition_nnz ? partition_nnz[i] : 0u;
+        m->partition_aux[i] = partition_aux_in ? partition_aux_in[i] : 0u;
+    }
+    rebuild_partition_offsets(m);
+    return set_shards_to_partitions(m);
+}
+
+// takes ownership of `part` (not copied); one shard per partition afterwards
+template <typename MatrixT>
+inline int append_partition(sharded<MatrixT> *m, MatrixT *part) {
+    if (m->num_partitions == m->partition_capacity &&
+        !reserve_partitions(m, m->partition_capacity == 0u ? 4u : m->partition_capacity * 2u))
+        return 0;
+    const unsigned long i = m->num_partitions;
+    m->parts[i] = part;
+    m->partition_rows[i] = part ? part->rows : 0u;
+    m->partition_nnz[i] = part ? partition_nnz(part) : 0u;
+    m->partition_aux[i] = part ? partition_aux(part) : 0u;
+    ++m->num_partitions;
+    if (part && m->cols == 0u) m->cols = part->cols;
+    rebuild_partition_offsets(m);
+    return set_shards_to_partitions(m);
+}
+
+// moves every partition of src to the end of dst (pointers, not payloads)
+template <typename MatrixT>
+inline int concatenate(sharded<MatrixT> *dst, sharded<MatrixT> *src) {
+    if (src->num_partitions == 0u) return 1;
+    if (!reserve_partitions(dst, dst->num_partitions + src->num_partitions)) return 0;
+    for (unsigned long i = 0; i < src->num_partitions; ++i) {
+        const unsigned long d = dst->num_partitions + i;
+        dst->parts[d] = src->parts[i];
+        dst->partition_rows[d] = src->partition_rows[i];
+        dst->partition_nnz[d] = src->partition_nnz[i];
+        dst->partition_aux[d] = src->partition_aux[i];
+        src->parts[i] = nullptr;
+        src->partition_rows[i] = src->partition_nnz[i] = src->partition_aux[i] = 0u;
+    }
+    dst->num_partitions += src->num_partitions;
+    src->num_partitions = 0;
+    if (dst->cols == 0u) dst->cols = src->cols;
+    rebuild_partition_offsets(dst);
+    set_shards_to_partitions(dst);
+    rebuild_partition_offsets(src);
+    src->rows = src->nnz = src->num_shards = 0u;
+    if (src->shard_parts) src->shard_parts[0] = 0u;
+    return 1;
+}
+
+template <typename MatrixT>
+inline unsigned long find_partition(const sharded<MatrixT> *m, unsigned long row) {
+    if (!m->partition_offsets || m->num_partitions == 0u) return m->num_partitions;
+    unsigned long lo = 0, hi = m->num_partitions;
+    while (lo < hi) {
+        const unsigned long mid = lo + (hi - lo) / 2u;
+        if (row < m->partition_offsets[mid]) hi = mid;
+        else if (row >= m->partition_offsets[mid + 1u]) lo = mid + 1u;
+        else return mid;
+    }
+    return m->num_partitions;
+}
+
+template <typename MatrixT>
+inline unsigned long find_shard(const sharded<MatrixT> *m, unsigned long row) {
+    if (!m->shard_offsets || m->num_shards == 0u) return m->num_shards;
+    unsigned long lo = 0, hi = m->num_shards;
+    while (lo < hi) {
+        const unsigned long mid = lo + (hi - lo) / 2u;
+        if (row < m->shard_offsets[mid]) hi = mid;
+        else if (row >= m->shard_offsets[mid + 1u]) lo = mid + 1u;
+        else return mid;
+    }
+    return m->num_shards;
+}
+
+template <typename MatrixT>
+inline unsigned long first_row_in_partition(const sharded<MatrixT> *m, unsigned long p) {
+    return (p >= m->num_partitions || !m->partition_offsets) ? m->rows : m->partition_offsets[p];
+}
+template <typename MatrixT>
+inline unsigned long last_row_in_partition(const sharded<MatrixT> *m, unsigned long p) {
+    return (p >= m->num_partitions || !m->partition_offsets) ? m->rows : m->partition_offsets[p + 1u];
+}
+
+template <typename MatrixT>
+inline int row_is_partition_boundary(const sharded<MatrixT> *m, unsigned long row) {
+    if (row == 0u || row == m->rows) return 1;
+    if (!m->partition_offsets || m->num_partitions == 0u) return 0;
+    const unsigned long hit = find_partition(m, row);
+    return hit < m->num_partitions && m->partition_offsets[hit] == row;
+}
+
+template <typename MatrixT>
+inline unsigned long first_partition_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    if (m->shard_parts && s < m->num_shards) return m->shard_parts[s];
+    if (s >= m->num_shards || m->num_partitions == 0u) return m->num_partitions;
+    return find_partition(m, m->shard_offsets[s]);
+}
+template <typename MatrixT>
+inline unsigned long last_partition_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    if (m->shard_parts && s < m->num_shards) return m->shard_parts[s + 1u];
+    if (s >= m->num_shards) return m->num_partitions;
+    const unsigned long end = m->shard_offsets[s + 1u];
+    return end == 0u ? 0u : find_partition(m, end - 1u) + 1u;
+}
+template <typename MatrixT>
+inline unsigned long first_row_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    return (s >= m->num_shards || !m->shard_offsets) ? m->rows : m->shard_offsets[s];
+}
+template <typename MatrixT>
+inline unsigned long last_row_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    return (s >= m->num_shards || !m->shard_offsets) ? m->rows : m->shard_offsets[s + 1u];
+}
+template <typename MatrixT>
+inline unsigned long partition_count_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    const unsigned long b = first_partition_in_shard(m, s), e = last_partition_in_shard(m, s);
+    return b >= e ? 0u : e - b;
+}
+template <typename MatrixT>
+inline unsigned long rows_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    const unsigned long b = first_row_in_shard(m, s), e = last_row_in_shard(m, s);
+    return b >= e ? 0u : e - b;
+}
+template <typename MatrixT>
+inline int partition_loaded(const sharded<MatrixT> *m, unsigned long p) {
+    return p < m->num_partitions && m->parts[p] != nullptr;
+}
+template <typename MatrixT>
+inline int shard_loaded(const sharded<MatrixT> *m, unsigned long s) {
+    if (s >= m->num_shards) return 0;
+    for (unsigned long i = first_partition_in_shard(m, s); i < last_partition_in_shard(m, s); ++i)
+        if (!partition_loaded(m, i)) return 0;
+    return 1;
+}
+template <typename MatrixT>
+inline unsigned long nnz_in_shard(const sharded<MatrixT> *m, unsigned long s) {
+    if (s >= m->num_shards) return 0;
+    unsigned long t = 0;
+    for (unsigned long i = first_partition_in_shard(m, s); i < last_partition_in_shard(m, s); ++i)
+        t += m->partition_nnz[i];
+    return t;
+}
+
+// host footprint of one partition (sharded.cuh:236-330): the packed host
+// block when materialised, else rebuilt from the metadata
+inline std::size_t partition_bytes(const sharded<sparse::compressed> *m, unsigned long p) {
+    if (p >= m->num_partitions) return 0;
+    const sparse::compressed *h = m->parts[p];
+    const unsigned long ptr_dim = m->partition_aux[p] == sparse::compressed_by_col ? m->cols : m->partition_rows[p];
+    if (h) {
+        const std::size_t major = h->axis == sparse::compressed_by_col ? h->cols : h->rows;
+        return sizeof(sparse::compressed) + (major + 1u) * 4u + (std::size_t) h->nnz * 6u;
+    }
+    return sizeof(sparse::compressed) + (ptr_dim + 1u) * 4u + (std::size_t) m->partition_nnz[p] * 6u;
+}
+inline std::size_t partition_bytes(const sharded<sparse::blocked_ell> *m, unsigned long p) {
+    if (p >= m->num_partitions) return 0;
+    const unsigned long aux = m->partition_aux[p];
+    const std::size_t B = sparse::unpack_blocked_ell_block_size(aux), W = sparse::unpack_blocked_ell_ell_width(aux);
+    const std::size_t rows = m->partition_rows[p];
+    return sizeof(sparse::blocked_ell) + (B ? (rows + B - 1u) / B : 0u) * W * 4u + rows * W * B * 2u;
+}
+inline std::size_t partition_bytes(const sharded<sparse::sliced_ell> *m, unsigned long p) {
+    if (p >= m->num_partitions) return 0;
+    const unsigned long aux = m->partition_aux[p];
+    const std::size_t S = sparse::unpack_sliced_ell_slice_count(aux), T = sparse::unpack_sliced_ell_total_slots(aux);
+    return sizeof(sparse::sliced_ell) + (S + 1u) * 4u + S * 4u + T * 6u;
+}
+template <typename MatrixT>
+inline std::size_t bytes(const sharded<MatrixT> *m) {
+    std::size_t t = sizeof(*m) + m->partition_capacity * (sizeof(MatrixT *) + 4u * sizeof(unsigned long)) +
+                    sizeof(unsigned long) + 2u * (m->shard_capacity + 1u) * sizeof(unsigned long);
+    for (unsigned long i = 0; i < m->num_partitions; ++i) t += partition_bytes(m, i);
+    return t;
+}
+template <typename MatrixT>
+inline std::size_t shard_bytes(const sharded<MatrixT> *m, unsigned long s) {
+    if (s >= m->num_shards) return 0;
+    std::size_t t = 0;
+    for (unsigned long i = first_partition_in_shard(m, s); i < last_partition_in_shard(m, s); ++i)
+        t += partition_bytes(m, i);
+    return t;
+}
+
+// sharded_host.cuh:232-268: about rows / count rows per shard, cutting only
+// where enough partitions remain for the shards still to come
+template <typename MatrixT>
+inline int set_equal_shards(sharded<MatrixT> *m, unsigned long count) {
+    if (count == 0u || m->num_partitions == 0u) {
+        m->num_shards = 0;
+        return 1;
+    }
+    if (count >= m->num_partitions) return set_shards_to_partitions(m);
+    if (!reserve_shards(m, count)) return 0;
+    const unsigned long target = (m->rows + count - 1u) / count;
+    unsigned long n = 0, rows = 0;
+    m->shard_offsets[0] = 0;
+    for (unsigned long i = 0; i < m->num_partitions; ++i) {
+        const unsigned long parts_left = m->num_partitions - (i + 1u), shards_left = count - (n + 1u);
+        rows += m->partition_rows[i];
+        if (shards_left == 0u) continue;
+        if (rows >= target && parts_left >= shards_left) {
+            m->shard_offsets[++n] = m->partition_offsets[i + 1u];
+            rows = 0;
+        }
+    }
+    m->shard_offsets[++n] = m->rows;
+    m->num_shards = n;
+    rebuild_shard_parts(m);
+    return 1;
+}
+
+namespace detail {
+// greedy cut: a new shard starts at partition i when the running total is
+// non-zero and adding i's weight would pass `limit`; zero-weight partitions
+// are skipped when `skip_zero` (sharded_host.cuh:335-395,
+// sharded_device.cuh:1113-1142)
+template <typename MatrixT, typename Weight>
+inline int cut_shards(sharded<MatrixT> *m, std::size_t limit, bool skip_zero, Weight w) {
+    if (limit == 0u) return set_shards_to_partitions(m);
+    if (!reserve_shards(m, m->num_partitions)) return 0;
+    std::size_t used = 0;
+    unsigned long n = 0;
+    m->shard_offsets[0] = 0;
+    for (unsigned long i = 0; i < m->num_partitions; ++i) {
+        const std::size_t b = w(i);
+        if (skip_zero && b == 0u) continue;
+        if (used != 0u && used + b > limit) {
+            m->shard_offsets[++n] = m->partition_offsets[i];
+            used = 0;
+        }
+        used += b;
+    }
+    if (m->num_partitions != 0u) m->shard_offsets[++n] = m->rows;
+    m->num_shards = n;
+    rebuild_shard_parts(m);
+    return 1;
+}
+} // namespace detail
+
+template <typename MatrixT>
+inline int set_shards_by_nnz(sharded<MatrixT> *m, unsigned long max_nnz) {
+    return detail::cut_shards(m, max_nnz, true, [m](unsigned long i) { return (std::size_t) m->partition_nnz[i]; });
+}
+template <typename MatrixT>
+inline int set_shards_by_part_bytes(sharded<MatrixT> *m, std::size_t max_bytes) {
+    return detail::cut_shards(m, max_bytes, true, [m](unsigned long i) { return partition_bytes(m, i); });
+}
+
+// shard offsets of about target rows each (sharded_host.cuh:270-311); the
+// array is calloc'd for the caller
+template <typename MatrixT>
+inline int build_shard_offsets_by_rows(const sharded<MatrixT> *m, unsigned long target, unsigned long **out_offsets,
+                                       unsigned long *out_count) {
+    if (!out_offsets || !out_count) return 0;
+    *out_offsets = nullptr;
+    *out_count = 0;
+    if (m->num_partitions == 0u) return 1;
+    auto *o = static_cast<unsigned long *>(std::calloc(m->num_partitions + 1u, sizeof(unsigned long)));
+    if (!o) return 0;
+    unsigned long n = 0, used = 0;
+    if (target == 0u) {
+        for (unsigned long i = 0; i <= m->num_partitions; ++i) o[i] = m->partition_offsets[i];
+        n = m->num_partitions;
+    } else {
+        for (unsigned long i = 0; i < m->num_partitions; ++i) {
+            if (used != 0u && used + m->partition_rows[i] > target) {
+                o[++n] = m->partition_offsets[i];
+                used = 0;
+            }
+            used += m->partition_rows[i];
+        }
+        o[++n] = m->rows;
+    }
+    *out_offsets = o;
+    *out_count = n;
+    return 1;
+}
+
+// explicit shard offsets, each a partition boundary (sharded_host.cuh:313-332)
+template <typename MatrixT>
+inline int reshard(sharded<MatrixT> *m, unsigned long count, const unsigned long *offsets) {
+    if (count == 0u || !offsets) {
+        m->num_shards = 0;
+        return 1;
+    }
+    if (offsets[0] != 0u || offsets[count] != m->rows) return 0;
+    for (unsigned long i = 0; i < count; ++i)
+        if (offsets[i] > offsets[i + 1u] || !row_is_partition_boundary(m, offsets[i])) return 0;
+    if (!row_is_partition_boundary(m, offsets[count]) || !reserve_shards(m, count)) return 0;
+    m->num_shards = count;
+    for (unsigned long i = 0; i <= count; ++i) m->shard_offsets[i] = offsets[i];
+    rebuild_shard_parts(m);
+    return 1;
+}
+
+// host materialisation: drop frees a part (metadata stays); fetch needs a
+// file backend this library does not have
+template <typename MatrixT>
+inline int drop_partition(sharded<MatrixT> *m, unsigned long p) {
+    if (p >= m->num_partitions) return 0;
+    destroy(m->parts[p]);
+    m->parts[p] = nullptr;
+    return 1;
+}
+template <typename MatrixT>
+inline int drop_all_partitions(sharded<MatrixT> *m) {
+    for (unsigned long i = 0; i < m->num_partitions; ++i)
+        if (!drop_partition(m, i)) return 0;
+    return 1;
+}
+template <typename MatrixT>
+inline int drop_shard(sharded<MatrixT> *m, unsigned long s) {
+    if (s >= m->num_shards) return 0;
+    for (unsigned long i = first_partition_in_shard(m, s); i < last_partition_in_shard(m, s); ++i)
+        if (!drop_partition(m, i)) return 0;
+    return 1;
+}
+template <typename MatrixT>
+inline int fetch_partition(sharded<MatrixT> *m, const shard_storage *, unsigned long p) {
+    if (p < m->num_partitions && m->parts[p] != nullptr) return 1;
+    std::fprintf(stderr,
+                 "Error: partition %lu is not materialised on the host and file-backed (.csh5) fetch is not part "
+                 "of this library\n",
+                 p);
+    return 0;
+}
+template <typename MatrixT>
+inline int fetch_shard(sharded<MatrixT> *m, const shard_storage *s, unsigned long shard) {
+    if (shard >= m->num_shards) return 0;
+    for (unsigned long i = first_partition_in_shard(m, shard); i < last_partition_in_shard(m, shard); ++i)
+        if (!fetch_partition(m, s, i)) return 0;
+    return 1;
+}
+
+namespace device {
+
+template <typename MatrixT>
+inline void init(sharded_device<MatrixT> *state) {
+    std::memset(state, 0, sizeof(*state));
+}
+// releases every resident partition and frees the cached blocks
+template <typename MatrixT>
+inline void clear(sharded_device<MatrixT> *state) {
+    cs_b200_sharded_device_clear(detail::as_state(state));
+}
+template <typename MatrixT>
+inline int reserve(sharded_device<MatrixT> *state, unsigned long capacity) {
+    return cs_b200_sharded_device_reserve(detail::as_state(state), capacity);
+}
+
+template <typename MatrixT>
+inline cudaError_t release_partition(sharded_device<MatrixT> *state, unsigned long part_id) {
+    return detail::staged(cs_b200_release_staged_partition(detail::as_state(state), part_id));
+}
+
+// sharded_device.cuh:1144-1166: the host part must be materialised
+template <typename MatrixT>
+inline cudaError_t upload_partition_async(sharded_device<MatrixT> *state, const sharded<MatrixT> *view,
+                                          unsigned long part_id, int device_id, cudaStream_t stream) {
+    if (part_id >= view->num_partitions || part_id >= state->capacity || view->parts[part_id] == nullptr)
+        return cudaErrorInvalidValue;
+    return detail::staged(detail::stage_one(detail::as_state(state), part_id, view->parts[part_id], device_id,
+                                            stream));
+}
+template <typename MatrixT>
+inline cudaError_t upload_partition(sharded_device<MatrixT> *state, const sharded<MatrixT> *view,
+                                    unsigned long part_id, int device_id) {
+    cudaError_t e = upload_partition_async(state, view, part_id, device_id, (cudaStream_t) 0);
+    return e != cudaSuccess ? e : cudaStreamSynchronize((cudaStream_t) 0);
+}
+
+// sharded_device.cuh:1437-1539: every partition of the shard in one packed
+// block (all three formats)
+template <typename MatrixT>
+inline cudaError_t upload_shard_async(sharded_device<MatrixT> *state, const sharded<MatrixT> *view,
+                                      unsigned long shard_id, int device_id, cudaStream_t stream) {
+    if (shard_id >= view->num_shards) return cudaErrorInvalidValue;
+    const unsigned long b = first_partition_in_shard(view, shard_id), e = last_partition_in_shard(view, shard_id);
+    if (b >= e) return cudaSuccess;
+    for (unsigned long i = b; i < e; ++i)
+        if (i >= state->capacity || view->parts[i] == nullptr) return cudaErrorInvalidValue;
+    return detail::staged(detail::stage_many(detail::as_state(state), b, e - b, view->parts + b, device_id, stream));
+}
+template <typename MatrixT>
+inline cudaError_t upload_shard(sharded_device<MatrixT> *state, const sharded<MatrixT> *view, unsigned long shard_id,
+                                int device_id) {
+    cudaError_t e = upload_shard_async(state, view, shard_id, device_id, (cudaStream_t) 0);
+    return e != cudaSuccess ? e : cudaStreamSynchronize((cudaStream_t) 0);
+}
+
+// sharded_device.cuh:1541-1559
+template <typename MatrixT>
+inline cudaError_t release_shard(sharded_device<MatrixT> *state, const sharded<MatrixT> *view,
+                                 unsigned long shard_id) {
+    if (shard_id >= view->num_shards) return cudaErrorInvalidValue;
+    for (unsigned long i = first_partition_in_shard(view, shard_id); i < last_partition_in_shard(view, shard_id);
+         ++i) {
+        if (i >= state->capacity || state->parts[i].view == nullptr) continue;
+        const cudaError_t e = release_partition(state, i);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// sharded_device.cuh:1569-1630: fetch when absent on the host (needs a
+// file backend), upload, optionally drop the host part
+template <typename MatrixT>
+inline cudaError_t stage_partition_async(sharded_device<MatrixT> *state, sharded<MatrixT> *view,
+                                         const shard_storage *files, unsigned long part_id, int device_id,
+                                         cudaStream_t stream, int drop_host_after_upload) {
+    if (part_id >= view->num_partitions || part_id >= state->capacity) return cudaErrorInvalidValue;
+    if (state->parts[part_id].view != nullptr && state->parts[part_id].device_id == device_id) {
+        if (drop_host_after_upload && view->parts[part_id] != nullptr && !drop_partition(view, part_id))
+            return cudaErrorInvalidValue;
+        return cudaSuccess;
+    }
+    if (view->parts[part_id] == nullptr && !fetch_partition(view, files, part_id)) return cudaErrorInvalidValue;
+    cudaError_t e = upload_partition_async(state, view, part_id, device_id, stream);
+    if (e != cudaSuccess) return e;
+    if (drop_host_after_upload) {
+        // the copies read the host part: wait for them before it is freed
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return e;
+        if (!drop_partition(view, part_id)) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+template <typename MatrixT>
+inline cudaError_t stage_partition(sharded_device<MatrixT> *state, sharded<MatrixT> *view, const shard_storage *files,
+                                   unsigned long part_id, int device_id, int drop_host_after_upload) {
+    cudaError_t e = stage_partition_async(state, view, files, part_id, device_id, (cudaStream_t) 0,
+                                          drop_host_after_upload);
+    return e != cudaSuccess ? e : cudaStreamSynchronize((cudaStream_t) 0);
+}
+
+// sharded_device.cuh:1632-1677
+template <typename MatrixT>
+inline cudaError_t stage_shard_async(sharded_device<MatrixT> *state, sharded<MatrixT> *view,
+                                     const shard_storage *files, unsigned long shard_id, int device_id,
+                                     cudaStream_t stream, int drop_host_after_upload) {
+    if (shard_id >= view->num_shards) return cudaErrorInvalidValue;
+    if (!shard_loaded(view, shard_id) && !fetch_shard(view, files, shard_id)) return cudaErrorInvalidValue;
+    cudaError_t e = upload_shard_async(state, view, shard_id, device_id, stream);
+    if (e != cudaSuccess) return e;
+    if (drop_host_after_upload) {
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return e;
+        if (!drop_shard(view, shard_id)) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+template <typename MatrixT>
+inline cudaError_t stage_shard(sharded_device<MatrixT> *state, sharded<MatrixT> *view, const shard_storage *files,
+                               unsigned long shard_id, int device_id, int drop_host_after_upload) {
+    cudaError_t e = stage_shard_async(state, view, files, shard_id, device_id, (cudaStream_t) 0,
+                                      drop_host_after_upload);
+    return e != cudaSuccess ? e : cudaStreamSynchronize((cudaStream_t) 0);
+}
+
+// sharded_device.cuh:1679-1721: the incoming shard is staged before the
+// outgoing one is released, so both are resident for a moment
+template <typename MatrixT>
+inline cudaError_t swap_shard_async(sharded_device<MatrixT> *state, sharded<MatrixT> *view, const shard_storage *files,
+                                    unsigned long out_shard, unsigned long in_shard, int device_id, cudaStream_t stream,
+                                    int drop_host_after_upload, int drop_host_after_release) {
+    cudaError_t e = stage_shard_async(state, view, files, in_shard, device_id, stream, drop_host_after_upload);
+    if (e != cudaSuccess) return e;
+    e = release_shard(state, view, out_shard);
+    if (e != cudaSuccess) return e;
+    if (drop_host_after_release && !drop_shard(view, out_shard)) return cudaErrorInvalidValue;
+    return cudaSuccess;
+}
+template <typename MatrixT>
+inline cudaError_t swap_shard(sharded_device<MatrixT> *state, sharded<MatrixT> *view, const shard_storage *files,
+                              unsigned long out_shard, unsigned long in_shard, int device_id,
+                              int drop_host_after_upload, int drop_host_after_release) {
+    cudaError_t e = swap_shard_async(state, view, files, out_shard, in_shard, device_id, (cudaStream_t) 0,
+                                     drop_host_after_upload, drop_host_after_release);
+    return e != cudaSuccess ? e : cudaStreamSynchronize((cudaStream_t) 0);
+}
+
+// Resident device bytes of one partition after upload_partition, from the
+// metadata alone (sharded_device.cuh:1050-1095): the view's 256 bytes, then
+// each array rounded up to 256 bytes (this library's layout).
+namespace detail {
+inline std::size_t r256(std::size_t x) { return (x + 255u) / 256u * 256u; }
+} // namespace detail
+inline std::size_t device_partition_bytes(const sharded<sparse::compressed> *view, unsigned long p) {
+    const std::size_t ptr_dim =
+        view->partition_aux[p] == sparse::compressed_by_col ? view->cols : view->partition_rows[p];
+    const std::size_t nnz = view->partition_nnz[p];
+    return 256u + detail::r256((ptr_dim + 1u) * 4u) + detail::r256(nnz * 4u) + detail::r256(nnz * 2u);
+}
+inline std::size_t device_partition_bytes(const sharded<sparse::blocked_ell> *view, unsigned long p) {
+    const unsigned long aux = view->partition_aux[p];
+    const std::size_t B = sparse::unpack_blocked_ell_block_size(aux), W = sparse::unpack_blocked_ell_ell_width(aux);
+    const std::size_t rows = view->partition_rows[p];
+    return 256u + detail::r256((B ? (rows + B - 1u) / B : 0u) * W * 4u) + detail::r256(rows * W * B * 2u);
+}
+inline std::size_t device_partition_bytes(const sharded<sparse::sliced_ell> *view, unsigned long p) {
+    const unsigned long aux = view->partition_aux[p];
+    const std::size_t S = sparse::unpack_sliced_ell_slice_count(aux), T = sparse::unpack_sliced_ell_total_slots(aux);
+    return 256u + detail::r256(S ? (S + 1u) * 4u : 0u) + 2u * detail::r256(S * 4u) + detail::r256(T * 4u) +
+           detail::r256(T * 2u);
+}
+template <typename MatrixT>
+inline std::size_t device_shard_bytes(const sharded<MatrixT> *view, unsigned long shard_id) {
+    if (shard_id >= view->num_shards) return 0;
+    std::size_t t = 0;
+    for (unsigned long i = first_partition_in_shard(view, shard_id); i < last_partition_in_shard(view, shard_id); ++i)
+        t += device_partition_bytes(view, i);
+    return t;
+}
+// sharded_device.cuh:1113-1142: shards cut so each fits max_bytes of device memory
+template <typename MatrixT>
+inline int set_shards_by_device_bytes(sharded<MatrixT> *view, std::size_t max_bytes) {
+    return ::cellshard::detail::cut_shards(view, max_bytes, true,
+                                           [view](unsigned long i) { return device_partition_bytes(view, i); });
 }
 
 } // namespace device

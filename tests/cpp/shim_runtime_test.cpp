@@ -1,5 +1,7 @@
 // Drives the C++ shim (include/cellshard_b200.hpp) the way reference host
-// code drives the reference API: stage host partitions with device::upload,
+// code drives the reference API: stage host partitions with device::upload
+// and whole shards of a sharded<T> through a sharded_device<T> (upload_shard,
+// swap_shard, stage_partition, the allocation cache),
 // run runtime::compute_sparse_group_reduce over Blocked-ELL, Sliced-ELL and
 // compressed views, runtime::manual_reoptimize_masked_sparse, the
 // convert:: host conversion and chooser, bucket::build_bucketed_major_view and
@@ -9,6 +11,8 @@
 #include <cellshard_b200.hpp>
 
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <map>
 #include <sstream>
@@ -70,6 +74,96 @@ T *to_device(const std::vector<T> &v) {
     return d;
 }
 
+template <typename T>
+void print_host(const std::string &name, const T *v, size_t n) {
+    std::printf("%s", name.c_str());
+    for (size_t i = 0; i < n; ++i) std::printf(" %.9g", (double) v[i]);
+    std::printf("\n");
+}
+
+void print_host_half(const std::string &name, const __half *v, size_t n) {
+    std::printf("%s", name.c_str());
+    for (size_t i = 0; i < n; ++i) std::printf(" %.9g", (double) __half2float(v[i]));
+    std::printf("\n");
+}
+
+struct lcg {
+    std::uint32_t s;
+    std::uint32_t next() {
+        s = s * 1664525u + 1013904223u;
+        return s >> 8;
+    }
+};
+
+// A Blocked-ELL host partition owning one malloc'd block (as sparse::allocate
+// packs it), so cellshard::clear(sharded*) can destroy it: random ascending
+// block columns per row block with trailing padding, about a third of the
+// valid cells nonzero.
+cs::sparse::blocked_ell *make_bell_part(lcg &g, unsigned rows, unsigned cols, unsigned B, unsigned W) {
+    auto *m = new cs::sparse::blocked_ell;
+    cs::sparse::init(m);
+    const unsigned rb = (rows + B - 1u) / B, nb = (cols + B - 1u) / B;
+    const std::size_t ib = (std::size_t) rb * W * 4u, vb = (std::size_t) rows * W * B * 2u;
+    char *st = static_cast<char *>(std::malloc(ib + vb + 16u));
+    m->rows = rows;
+    m->cols = cols;
+    m->block_size = B;
+    m->ell_cols = W * B;
+    m->storage = st;
+    m->blockColIdx = reinterpret_cast<cs::types::idx_t *>(st);
+    m->val = reinterpret_cast<__half *>(st + ib);
+    for (unsigned r = 0; r < rb; ++r) {
+        const unsigned valid = 1u + g.next() % W;
+        unsigned c = g.next() % 3u;
+        for (unsigned k = 0; k < W; ++k) {
+            unsigned bc = 0xffffffffu;
+            if (k < valid && c < nb) {
+                bc = c;
+                c += 1u + g.next() % 3u;
+            }
+            m->blockColIdx[(std::size_t) r * W + k] = bc;
+        }
+    }
+    for (unsigned r = 0; r < rows; ++r)
+        for (unsigned k = 0; k < W * B; ++k) {
+            const unsigned bc = m->blockColIdx[(std::size_t) (r / B) * W + k / B];
+            float v = 0.0f;
+            if (bc != 0xffffffffu && bc * B + k % B < cols && g.next() % 3u == 0u) v = (float) (1u + g.next() % 7u);
+            m->val[(std::size_t) r * W * B + k] = __float2half(v);
+            m->nnz += v != 0.0f ? 1u : 0u;
+        }
+    return m;
+}
+
+// The same kind of matrix as a compressed partition (sorted distinct columns).
+cs::sparse::compressed *make_csr_part(lcg &g, unsigned rows, unsigned cols) {
+    auto *m = new cs::sparse::compressed;
+    cs::sparse::init(m);
+    std::vector<unsigned> ptr(rows + 1u, 0u), idx;
+    std::vector<__half> val;
+    for (unsigned r = 0; r < rows; ++r) {
+        for (unsigned c = g.next() % 4u; c < cols; c += 1u + g.next() % 6u) {
+            idx.push_back(c);
+            val.push_back(__float2half((float) (1u + g.next() % 9u)));
+        }
+        ptr[r + 1u] = (unsigned) idx.size();
+    }
+    const std::size_t pb = (rows + 1u) * 4u, ib = idx.size() * 4u, vb = val.size() * 2u;
+    char *st = static_cast<char *>(std::malloc(pb + ib + vb + 16u));
+    m->rows = rows;
+    m->cols = cols;
+    m->nnz = (unsigned) idx.size();
+    m->axis = cs::sparse::compressed_by_row;
+    m->storage = st;
+    m->majorPtr = reinterpret_cast<cs::types::ptr_t *>(st);
+    m->minorIdx = reinterpret_cast<cs::types::idx_t *>(st + pb);
+    m->val = reinterpret_cast<__half *>(st + pb + ib);
+    std::memcpy(m->majorPtr, ptr.data(), pb);
+    std::memcpy(m->minorIdx, idx.data(), ib);
+    std::memcpy(m->val, val.data(), vb);
+    return m;
+}
+
 int fail(int code, const char *what) {
     std::fprintf(stderr, "%s failed: %s\n", what, cs_b200_last_error());
     return code;
@@ -124,9 +218,8 @@ int main(int argc, char **argv) {
     for (const auto &x : bval) hb.nnz += __half2float(x) != 0.0f ? 1u : 0u; // the stored nonzeros
     cs::device::partition_record<cs::sparse::blocked_ell> rb;
     if (cs::device::upload(&hb, &rb) != cudaSuccess) return fail(5, "upload blocked_ell");
-    std::printf("blocked.partition_bytes %zu %zu\n", cs::device::device_partition_bytes(&hb),
-                rb.rec.allocation_bytes);
-    auto bview = cs::device::staged_view<cs::device::blocked_ell_view>(&rb);
+    std::printf("blocked.partition_bytes %zu %zu\n", cs::device::device_partition_bytes(&hb), rb.allocation_bytes);
+    auto bview = cs::device::staged_view(&hb, &rb);
     if (!cs::runtime::compute_sparse_group_reduce(&bview, &ws, &groups, &masks, &filter, &res))
         return fail(6, "reduce blocked_ell");
     dump("blocked");
@@ -153,7 +246,7 @@ int main(int argc, char **argv) {
     hc.val = cval.data();
     cs::device::partition_record<cs::sparse::compressed> rc;
     if (cs::device::upload(&hc, &rc) != cudaSuccess) return fail(8, "upload compressed");
-    auto cview = cs::device::staged_view<cs::device::compressed_view>(&rc);
+    auto cview = cs::device::staged_view(&hc, &rc);
     if (!cs::runtime::compute_sparse_group_reduce_compressed_fallback(&cview, &ws, &groups, &masks, &filter, &res))
         return fail(9, "reduce compressed");
     dump("compressed");
@@ -175,7 +268,7 @@ int main(int argc, char **argv) {
     hs.val = sval.data();
     cs::device::partition_record<cs::sparse::sliced_ell> rs;
     if (cs::device::upload(&hs, &rs) != cudaSuccess) return fail(10, "upload sliced_ell");
-    auto sview = cs::device::staged_view<cs::device::sliced_ell_view>(&rs);
+    auto sview = cs::device::staged_view(&hs, &rs);
     std::printf("sliced.view %u %u\n", sview.slice_rows, sview.slice_count);
     print_dev("sliced.slot_offsets", sview.slice_slot_offsets, sview.slice_count);
     if (!cs::runtime::compute_sparse_group_reduce(&sview, &ws, &groups, &masks, &filter, &res))
@@ -381,6 +474,190 @@ int main(int argc, char **argv) {
     print_dev("transpose.ptr", tptr, cols + 1u);
     print_dev("transpose.idx", tidx, hc.nnz);
     print_dev_half("transpose.val", tval, hc.nnz);
+
+
+    // ---------------------------------------------------------------------
+    // Shard-level staging: a sharded<blocked_ell> of five uneven partitions
+    // cut into two shards, staged through a sharded_device (one packed block
+    // per shard), swapped, restaged from the allocation cache; every staged
+    // partition reduced through runtime::compute_sparse_group_reduce.
+    // ---------------------------------------------------------------------
+    {
+        const unsigned scols = 48u, SB = 4u, SG = 4u;
+        lcg g{12345u};
+        std::vector<std::uint32_t> smask(scols);
+        for (auto &x : smask) x = g.next() & 0xfu;
+        print_host("shard.group_masks", smask.data(), smask.size());
+        cs::runtime::sparse_group_reduce_workspace ws2;
+        cs::runtime::init(&ws2);
+        if (!cs::runtime::setup(&ws2, 0) || !cs::runtime::upload_feature_group_masks(&ws2, scols, smask.data()))
+            return fail(40, "shard workspace");
+        cs::runtime::group_mask_config_view g2{SG, nullptr, ws2.feature_group_masks};
+        cs::runtime::sparse_group_filter_params f2{1.0f, 1u, 0.9f, 0u};
+        cs::runtime::sparse_group_reduce_result r2;
+        auto dump2 = [&](const std::string &t) {
+            cudaStreamSynchronize(ws2.stream);
+            print_dev((t + ".row_totals").c_str(), r2.row_totals, r2.rows);
+            print_dev((t + ".detected").c_str(), r2.detected_features, r2.rows);
+            print_dev((t + ".max").c_str(), r2.max_values, r2.rows);
+            print_dev((t + ".keep").c_str(), r2.row_keep, r2.rows);
+            print_dev((t + ".group_counts").c_str(), r2.group_counts, (size_t) r2.rows * SG);
+        };
+
+        const unsigned prow[5] = {37u, 64u, 21u, 50u, 9u}, pw[5] = {3u, 5u, 2u, 4u, 1u};
+        cs::sharded<cs::sparse::blocked_ell> m;
+        cs::init(&m);
+        for (unsigned p = 0; p < 5u; ++p) {
+            cs::sparse::blocked_ell *part = make_bell_part(g, prow[p], scols, SB, pw[p]);
+            const std::string t = "shard.part" + std::to_string(p);
+            std::printf("%s.meta %u %u %u %u\n", t.c_str(), part->rows, part->ell_cols, part->nnz, SB);
+            print_host(t + ".bci", part->blockColIdx, (size_t) ((part->rows + SB - 1u) / SB) * pw[p]);
+            print_host_half(t + ".val", part->val, (size_t) part->rows * part->ell_cols);
+            if (!cs::append_partition(&m, part)) return fail(41, "append_partition");
+        }
+        if (!cs::set_equal_shards(&m, 2u)) return fail(42, "set_equal_shards");
+        print_host("shard.offsets", m.shard_offsets, m.num_shards + 1u);
+        print_host("shard.parts", m.shard_parts, m.num_shards + 1u);
+
+        cs::device::sharded_device<cs::sparse::blocked_ell> st;
+        cs::device::init(&st);
+        if (!cs::device::reserve(&st, m.num_partitions)) return fail(43, "reserve");
+        auto reduce_resident = [&](const std::string &tag) -> int {
+            for (unsigned long p = 0; p < m.num_partitions; ++p) {
+                if (st.parts[p].view == nullptr) continue;
+                auto v = cs::device::staged_view(m.parts[p], &st.parts[p]);
+                if (!cs::runtime::compute_sparse_group_reduce(&v, &ws2, &g2, nullptr, &f2, &r2)) return 0;
+                dump2(tag + ".p" + std::to_string(p));
+            }
+            return 1;
+        };
+        auto records = [&](const std::string &tag) {
+            std::printf("%s", tag.c_str());
+            for (unsigned long p = 0; p < m.num_partitions; ++p) {
+                const auto &r = st.parts[p];
+                const long vo = r.view ? (long) ((char *) r.view - (char *) st.parts[r.group_begin].view) : -1;
+                std::printf(" %lu %lu %d %d %ld", r.group_begin, r.group_end, r.allocation != nullptr ? 1 : 0,
+                            r.device_id, vo);
+            }
+            std::printf(" cache %lu\n", st.cache_count);
+        };
+        if (cs::device::stage_shard(&st, &m, nullptr, 0ul, 0, 0) != cudaSuccess) return fail(44, "stage_shard 0");
+        records("shard.records.s0");
+        if (!reduce_resident("shard.s0")) return fail(45, "reduce shard 0");
+        void *block0 = st.parts[0].allocation;
+        const std::size_t bytes0 = st.parts[0].allocation_bytes;
+        if (cs::device::swap_shard(&st, &m, nullptr, 0ul, 1ul, 0, 0, 0) != cudaSuccess) return fail(46, "swap_shard");
+        records("shard.records.swapped");
+        if (!reduce_resident("shard.s1")) return fail(47, "reduce shard 1");
+        // shard 0 again: its block comes back from the cache
+        if (cs::device::stage_shard(&st, &m, nullptr, 0ul, 0, 0) != cudaSuccess) return fail(48, "restage shard 0");
+        records("shard.records.restaged");
+        std::printf("shard.reuse %d %d\n", st.parts[0].allocation == block0 ? 1 : 0,
+                    st.parts[0].allocation_bytes == bytes0 ? 1 : 0);
+        if (!reduce_resident("shard.both")) return fail(49, "reduce both shards");
+        // staging a resident shard again does nothing
+        void *b1 = st.parts[m.shard_parts[1]].allocation;
+        if (cs::device::upload_shard(&st, &m, 1ul, 0) != cudaSuccess || st.parts[m.shard_parts[1]].allocation != b1)
+            return fail(50, "upload resident shard");
+        // footprints: per-partition bytes from the metadata equal the C ABI's for the materialised part
+        std::printf("shard.bytes");
+        for (unsigned long p = 0; p < m.num_partitions; ++p)
+            std::printf(" %zu %zu", cs::device::device_partition_bytes(&m, p),
+                        cs::device::device_partition_bytes(m.parts[p]));
+        std::printf(" %zu %zu %zu\n", cs::device::device_shard_bytes(&m, 0ul), cs::device::device_shard_bytes(&m, 1ul),
+                    bytes0);
+        // shards by device bytes, by nnz, by host bytes; explicit offsets
+        const std::size_t lim = cs::device::device_partition_bytes(&m, 0ul) + cs::device::device_partition_bytes(&m, 1ul);
+        cs::device::release_shard(&st, &m, 0ul);
+        cs::device::release_shard(&st, &m, 1ul);
+        if (!cs::device::set_shards_by_device_bytes(&m, lim)) return fail(51, "set_shards_by_device_bytes");
+        print_host("shard.by_device_bytes", m.shard_offsets, m.num_shards + 1u);
+        if (!cs::set_shards_by_nnz(&m, 400ul)) return fail(52, "set_shards_by_nnz");
+        print_host("shard.by_nnz", m.shard_offsets, m.num_shards + 1u);
+        const unsigned long cuts[3] = {0ul, m.partition_offsets[3], m.rows};
+        std::printf("shard.reshard %d %d\n", cs::reshard(&m, 2ul, cuts), cs::reshard(&m, 1ul, cuts + 1));
+        // stage_partition with the host part dropped after upload; a dropped,
+        // non-resident part cannot be fetched (no file backend)
+        if (cs::device::stage_partition(&st, &m, nullptr, 4ul, 0, 1) != cudaSuccess) return fail(53, "stage_partition");
+        std::printf("shard.dropped %d %lu %lu\n", m.parts[4] == nullptr ? 1 : 0, st.parts[4].group_begin,
+                    st.parts[4].group_end);
+        const cudaError_t again = cs::device::stage_partition(&st, &m, nullptr, 4ul, 0, 0);
+        cs::device::release_partition(&st, 4ul);
+        const cudaError_t absent = cs::device::stage_partition(&st, &m, nullptr, 4ul, 0, 0);
+        std::printf("shard.stage_codes %d %d\n", (int) again, absent == cudaSuccess ? 0 : 1);
+        cs::device::clear(&st);
+        cs::clear(&m);
+        cs::runtime::clear(&ws2);
+    }
+
+    // compressed and Sliced-ELL shards: one packed block each, the Sliced-ELL
+    // slot offsets computed on the device per partition
+    {
+        const unsigned scols = 48u, SG = 4u;
+        lcg g{777u};
+        std::vector<std::uint32_t> smask(scols);
+        for (auto &x : smask) x = g.next() & 0xfu;
+        print_host("cshard.group_masks", smask.data(), smask.size());
+        cs::runtime::sparse_group_reduce_workspace ws3;
+        cs::runtime::init(&ws3);
+        if (!cs::runtime::setup(&ws3, 0) || !cs::runtime::upload_feature_group_masks(&ws3, scols, smask.data()))
+            return fail(60, "cshard workspace");
+        cs::runtime::group_mask_config_view g3{SG, nullptr, ws3.feature_group_masks};
+        cs::runtime::sparse_group_filter_params f3{1.0f, 1u, 0.9f, 0u};
+        cs::runtime::sparse_group_reduce_result r3;
+        auto dump3 = [&](const std::string &t) {
+            cudaStreamSynchronize(ws3.stream);
+            print_dev((t + ".row_totals").c_str(), r3.row_totals, r3.rows);
+            print_dev((t + ".detected").c_str(), r3.detected_features, r3.rows);
+            print_dev((t + ".group_counts").c_str(), r3.group_counts, (size_t) r3.rows * SG);
+        };
+        const unsigned crow[3] = {29u, 70u, 13u};
+        cs::sharded<cs::sparse::compressed> mc;
+        cs::sharded<cs::sparse::sliced_ell> ms;
+        cs::init(&mc);
+        cs::init(&ms);
+        for (unsigned p = 0; p < 3u; ++p) {
+            cs::sparse::compressed *c = make_csr_part(g, crow[p], scols);
+            const std::string t = "cshard.part" + std::to_string(p);
+            print_host(t + ".ptr", c->majorPtr, c->rows + 1u);
+            print_host(t + ".idx", c->minorIdx, c->nnz);
+            print_host_half(t + ".val", c->val, c->nnz);
+            auto *sl = new cs::sparse::sliced_ell;
+            cs::sparse::init(sl);
+            if (!cs::convert::sliced_ell_from_compressed(c, 8u, sl)) return fail(61, "sliced_ell_from_compressed");
+            if (!cs::append_partition(&mc, c) || !cs::append_partition(&ms, sl)) return fail(62, "append");
+        }
+        cs::set_equal_shards(&mc, 1u);
+        cs::set_equal_shards(&ms, 1u);
+        cs::device::sharded_device<cs::sparse::compressed> sc;
+        cs::device::sharded_device<cs::sparse::sliced_ell> ss;
+        cs::device::init(&sc);
+        cs::device::init(&ss);
+        if (!cs::device::reserve(&sc, 3ul) || !cs::device::reserve(&ss, 3ul)) return fail(63, "reserve");
+        if (cs::device::upload_shard_async(&sc, &mc, 0ul, 0, ws3.stream) != cudaSuccess ||
+            cs::device::upload_shard_async(&ss, &ms, 0ul, 0, ws3.stream) != cudaSuccess)
+            return fail(64, "upload_shard_async");
+        for (unsigned long p = 0; p < 3ul; ++p) {
+            auto cv = cs::device::staged_view(mc.parts[p], &sc.parts[p]);
+            if (!cs::runtime::compute_sparse_group_reduce_compressed_fallback(&cv, &ws3, &g3, nullptr, &f3, &r3))
+                return fail(65, "reduce staged compressed");
+            dump3("cshard.c" + std::to_string(p));
+            auto sv = cs::device::staged_view(ms.parts[p], &ss.parts[p]);
+            cudaStreamSynchronize(ws3.stream);
+            print_dev(("cshard.s" + std::to_string(p) + ".slot_offsets").c_str(), sv.slice_slot_offsets,
+                      sv.slice_count);
+            if (!cs::runtime::compute_sparse_group_reduce(&sv, &ws3, &g3, nullptr, &f3, &r3))
+                return fail(66, "reduce staged sliced");
+            dump3("cshard.s" + std::to_string(p));
+            std::printf("cshard.group %lu %lu %lu %lu\n", sc.parts[p].group_begin, sc.parts[p].group_end,
+                        ss.parts[p].group_begin, ss.parts[p].group_end);
+        }
+        cs::device::clear(&sc);
+        cs::device::clear(&ss);
+        cs::clear(&mc);
+        cs::clear(&ms);
+        cs::runtime::clear(&ws3);
+    }
 
     cs::bucket::clear(&bws);
     cs::runtime::clear(&rws);

@@ -53,6 +53,8 @@ int main(void) {
   S(cs_batch_tiles) S(cs_batch_sliced_result) O(cs_batch_sliced_result, view)
   S(cs_serve_config) S(cs_serve_request) O(cs_serve_request, group_rows) S(cs_serve_stats)
   S(cs_partition_record) O(cs_partition_record, host_view)
+  S(cs_staged_part) O(cs_staged_part, group_begin) O(cs_staged_part, device_id)
+  S(cs_cached_allocation) S(cs_sharded_device) O(cs_sharded_device, cache)
   S(cs_host_bucketed_blocked_ell) O(cs_host_bucketed_blocked_ell, canonical_to_exec_cols)
   S(cs_host_bucketed_sliced_ell) O(cs_host_bucketed_sliced_ell, canonical_slice_widths)
   S(cs_exec_bucket_plan) O(cs_exec_bucket_plan, value_entries) S(cs_exec_bucket_segments)
@@ -82,6 +84,9 @@ PAIRS = {
     "cs_serve_request": _abi.ServeRequest,
     "cs_serve_stats": _abi.ServeStats,
     "cs_partition_record": _abi.PartitionRecord,
+    "cs_staged_part": _abi.StagedPart,
+    "cs_cached_allocation": _abi.CachedAllocation,
+    "cs_sharded_device": _abi.ShardedDevice,
     "cs_host_bucketed_blocked_ell": _abi.HostBucketedBlockedEll,
     "cs_host_bucketed_sliced_ell": _abi.HostBucketedSlicedEll,
     "cs_exec_bucket_plan": _abi.ExecBucketPlan,
@@ -118,6 +123,9 @@ def test_ctypes_layouts_match_c(tmp_path):
     assert got["cs_batch_sliced_result.view"] == _abi.BatchSlicedResult.view.offset
     assert got["cs_serve_request.group_rows"] == _abi.ServeRequest.group_rows.offset
     assert got["cs_partition_record.host_view"] == _abi.PartitionRecord.host_view.offset
+    assert got["cs_staged_part.group_begin"] == _abi.StagedPart.group_begin.offset
+    assert got["cs_staged_part.device_id"] == _abi.StagedPart.device_id.offset
+    assert got["cs_sharded_device.cache"] == _abi.ShardedDevice.cache.offset
 
 
 def test_abi_version_and_host_validation(cs_lib):
@@ -154,3 +162,53 @@ def test_missing_library_fails_loudly(tmp_path):
             _abi.load(tmp_path / "absent.so")
     finally:
         _abi._lib = saved
+
+
+def test_sharded_device_table_on_the_host(cs_lib):
+    """The residency table of device::sharded_device grows on the host with no device
+    work: records start empty (device -1), keep their contents when the table grows,
+    and staging outside the table is refused with a message before any CUDA call."""
+    st = _abi.ShardedDevice()
+    assert cs_lib.cs_b200_sharded_device_reserve(C.byref(st), 3) == 1
+    assert st.capacity == 3 and all(st.parts[i].device_id == -1 and not st.parts[i].view for i in range(3))
+    st.parts[1].group_begin, st.parts[1].group_end = 7, 9
+    assert cs_lib.cs_b200_sharded_device_reserve(C.byref(st), 2) == 1 and st.capacity == 3
+    assert cs_lib.cs_b200_sharded_device_reserve(C.byref(st), 8) == 1 and st.capacity == 8
+    assert (st.parts[1].group_begin, st.parts[1].group_end) == (7, 9) and st.parts[7].device_id == -1
+    st.parts[1].group_begin = st.parts[1].group_end = 0
+    h = _abi.HostBlockedEll()
+    h.rows, h.cols, h.block_size, h.ell_cols = 16, 16, 16, 16
+    assert cs_lib.cs_b200_stage_partition_blocked_ell(C.byref(st), 8, C.byref(h), 0, None) == 0
+    assert b"outside" in cs_lib.cs_b200_last_error()
+    arr = (C.POINTER(_abi.HostBlockedEll) * 2)(C.pointer(h), C.pointer(h))
+    assert cs_lib.cs_b200_stage_shard_blocked_ell(C.byref(st), 7, 2, arr, 0, None) == 0
+    # not resident: releasing is a no-op success
+    assert cs_lib.cs_b200_release_staged_partition(C.byref(st), 2) == 1
+    assert cs_lib.cs_b200_sharded_device_clear(C.byref(st)) == 1
+    assert st.capacity == 0 and not st.parts and st.cache_count == 0
+
+
+def test_staged_group_bytes(cs_lib):
+    """A packed group: the views back to back in one 256-byte-rounded block, then each
+    partition's arrays rounded to 256 bytes; one partition alone is the single-upload
+    footprint."""
+    import numpy as np
+
+    def bell(rows, W, B=4):
+        h = _abi.HostBlockedEll()
+        h.rows, h.cols, h.block_size, h.ell_cols = rows, 64, B, W * B
+        return h
+
+    parts = [bell(37, 3), bell(64, 5), bell(21, 2)]
+    arr = (C.POINTER(_abi.HostBlockedEll) * 3)(*[C.pointer(p) for p in parts])
+    n = C.c_size_t()
+    assert cs_lib.cs_b200_staged_bytes_blocked_ell(arr, 3, C.byref(n)) == 1
+    r = lambda x: (x + 255) // 256 * 256
+    want = r(3 * C.sizeof(_abi.BlockedEllView)) + sum(
+        r(((p.rows + 3) // 4) * (p.ell_cols // 4) * 4) + r(p.rows * p.ell_cols * 2) for p in parts)
+    assert n.value == want
+    one = C.c_size_t()
+    assert cs_lib.cs_b200_staged_bytes_blocked_ell(arr, 1, C.byref(n)) == 1
+    assert cs_lib.cs_b200_device_partition_bytes_blocked_ell(C.byref(parts[0]), C.byref(one)) == 1
+    assert n.value == one.value
+    assert np.int64(n.value) > 0

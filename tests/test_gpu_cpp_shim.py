@@ -186,3 +186,116 @@ def test_shim_convert_bucket_transpose_reoptimize(shim_out, orc):
     assert np.array_equal(o["reoptimize.ptr"].astype(np.uint32), major)
     assert np.array_equal(o["reoptimize.idx"].astype(np.uint32), ridx)
     assert np.array_equal(o["reoptimize.val"].astype(np.float16).view(np.uint16), rval)
+
+
+SHARD_FILTER = (1.0, 1, 0.9, 0)
+BELL_VIEW_BYTES = 48  # sizeof(device::blocked_ell_view)
+
+
+def _r256(x):
+    return (int(x) + 255) // 256 * 256
+
+
+def _shard_parts(o):
+    parts = []
+    for p in range(5):
+        rows, ell_cols, nnz, B = (int(x) for x in o[f"shard.part{p}.meta"])
+        bci = o[f"shard.part{p}.bci"].astype(np.uint32)
+        val = o[f"shard.part{p}.val"].astype(np.float16).view(np.uint16)
+        parts.append((rows, ell_cols, nnz, B, bci, val))
+    return parts
+
+
+def test_shim_shard_staging_records_and_swap(shim_out):
+    """sharded<blocked_ell> of five partitions (37/64/21/50/9 rows) cut into two shards
+    by set_equal_shards; stage_shard packs a shard's partitions into one block (views
+    48 bytes apart, the first partition owning the block); swap_shard stages shard 1
+    and hands shard 0's block to the cache; restaging shard 0 takes that same block."""
+    o = shim_out
+    assert list(o["shard.offsets"]) == [0, 101, 181] and list(o["shard.parts"]) == [0, 2, 5]
+    empty = [0, 0, 0, -1, -1]
+    s0 = [0, 2, 1, 0, 0, 0, 2, 0, 0, BELL_VIEW_BYTES]
+    s1 = [2, 5, 1, 0, 0, 2, 5, 0, 0, BELL_VIEW_BYTES, 2, 5, 0, 0, 2 * BELL_VIEW_BYTES]
+    assert list(o["shard.records.s0"][:25]) == s0 + empty * 3
+    assert list(o["shard.records.swapped"][:25]) == empty * 2 + s1
+    assert list(o["shard.records.restaged"][:25]) == s0 + s1
+    assert [o[f"shard.records.{k}.cache"][0] for k in ("s0", "swapped", "restaged")] == [0, 1, 0]
+    assert o["shard.records.s0"].size == 25 and o["shard.reuse"].tolist() == [1, 1]
+
+
+def test_shim_shard_staged_reduces_match_oracle(shim_out, orc):
+    """Every partition staged as part of a shard (first staging, after the swap, after
+    restaging from the cache) reduces to the restatement's per-row results."""
+    o = shim_out
+    masks = o["shard.group_masks"].astype(np.uint32)
+    parts = _shard_parts(o)
+    seen = 0
+    for tag in ("shard.s0", "shard.s1", "shard.both"):
+        for p, (rows, ell_cols, _nnz, B, bci, val) in enumerate(parts):
+            key = f"{tag}.p{p}"
+            if key + ".row_totals" not in o:
+                continue
+            ref = orc.group_reduce_bell(rows, 48, B, ell_cols, bci, val, masks, 4, None, None, SHARD_FILTER)
+            assert np.array_equal(o[key + ".row_totals"].astype(np.float32), ref["row_totals"]), key
+            assert np.array_equal(o[key + ".detected"].astype(np.uint32), ref["detected_features"]), key
+            assert np.array_equal(o[key + ".max"].astype(np.float32), ref["max_values"]), key
+            assert np.array_equal(o[key + ".keep"].astype(np.uint8), ref["row_keep"]), key
+            assert np.array_equal(o[key + ".group_counts"].astype(np.float32), ref["group_counts"]), key
+            seen += 1
+    assert seen == 2 + 3 + 5
+
+
+def test_shim_shard_bytes_and_cuts(shim_out):
+    """Metadata-only device bytes equal the C ABI's for the materialised part; a packed
+    shard takes one 256-byte view block plus each partition's arrays; the byte, nnz and
+    explicit cuts follow the reference's rules; a host part dropped after upload stays
+    staged, and once released cannot be staged again without a file backend."""
+    o = shim_out
+    parts = _shard_parts(o)
+    b = o["shard.bytes"].astype(np.int64)
+    per = b[:10].reshape(5, 2)
+    assert np.array_equal(per[:, 0], per[:, 1])
+    arrays = [_r256(((r + B - 1) // B) * (e // B) * 4) + _r256(r * e * 2) for (r, e, _n, B, _b, _v) in parts]
+    assert list(per[:, 0]) == [256 + a for a in arrays]
+    assert b[10] == per[0, 0] + per[1, 0] and b[11] == per[2:, 0].sum()
+    assert b[12] == _r256(2 * BELL_VIEW_BYTES) + arrays[0] + arrays[1]
+
+    def cut(weights, limit):
+        offs, used, row, rows = [0], 0, 0, [p[0] for p in parts]
+        for w, r in zip(weights, rows):
+            if w and used and used + w > limit:
+                offs.append(row)
+                used = 0
+            used += w
+            row += r
+        return offs + [sum(rows)]
+
+    assert list(o["shard.by_device_bytes"]) == cut(list(per[:, 0]), per[0, 0] + per[1, 0])
+    assert list(o["shard.by_nnz"]) == cut([p[2] for p in parts], 400)
+    assert o["shard.reshard"].tolist() == [1, 0]
+    assert o["shard.dropped"].tolist() == [1, 4, 5]
+    assert o["shard.stage_codes"].tolist() == [0, 1]
+
+
+def test_shim_compressed_and_sliced_shards(shim_out, orc):
+    """A compressed and a Sliced-ELL shard of three partitions each, staged as one
+    packed block apiece (the Sliced-ELL slot offsets computed on the device per
+    partition); every staged partition reduces to the restatement's results."""
+    o = shim_out
+    masks = o["cshard.group_masks"].astype(np.uint32)
+    for p in range(3):
+        ptr = o[f"cshard.part{p}.ptr"].astype(np.uint32)
+        idx = o[f"cshard.part{p}.idx"].astype(np.uint32)
+        val = o[f"cshard.part{p}.val"].astype(np.float16).view(np.uint16)
+        rows = len(ptr) - 1
+        rc = orc.group_reduce_csr(rows, 48, ptr, idx, val, masks, 4, None, None, SHARD_FILTER)
+        assert np.array_equal(o[f"cshard.c{p}.row_totals"].astype(np.float32), rc["row_totals"])
+        assert np.array_equal(o[f"cshard.c{p}.detected"].astype(np.uint32), rc["detected_features"])
+        assert np.array_equal(o[f"cshard.c{p}.group_counts"].astype(np.float32), rc["group_counts"])
+        sl = orc.sliced_ell_from_csr(rows, ptr, idx, val, 8)
+        assert np.array_equal(o[f"cshard.s{p}.slot_offsets"].astype(np.uint32), sl["slot_offsets"])
+        rs = orc.group_reduce_sell(rows, 48, 8, sl["offsets"], sl["widths"], sl["slot_offsets"], sl["col_idx"],
+                                   sl["val"], masks, 4, None, None, SHARD_FILTER)
+        assert np.array_equal(o[f"cshard.s{p}.row_totals"].astype(np.float32), rs["row_totals"])
+        assert np.array_equal(o[f"cshard.s{p}.group_counts"].astype(np.float32), rs["group_counts"])
+        assert o[f"cshard.group"].tolist() == [0, 3, 0, 3]
