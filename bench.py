@@ -47,8 +47,9 @@ KEEP_FRAC = 0.7
 KEPT_FEATURES = 20_000
 BLOCK = 16
 FALLBACK_HBM_GBS = 6650.0
-# launches per step: index, tile hist, group tiles, group scan, tile scatter, accumulate, combine
-LAUNCHES_PER_STEP = 7
+# launches per step: tile hist, group tiles, group scan, tile scatter, accumulate, combine (the
+# column-block index is built once when the partition is staged)
+LAUNCHES_PER_STEP = 6
 # DRAM bytes (read + write) of one moments_accumulate_kernel launch per kept row, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of that kernel on the first 20,000 rows
 # of this workload: 924.15 MB read and 8.95 MB written for 14,034 kept rows.  Traffic grows with
@@ -77,6 +78,9 @@ def parse():
                    help="moments: the headline reduction; convert: per-kernel conversion throughput; "
                         "mask_groups: the masked group reduce over the compressed, Sliced-ELL and Blocked-ELL "
                         "forms; batched: 256 uneven partitions -> Sliced-ELL + nnz plans in one persistent launch")
+    p.add_argument("--config", choices=["c1", "c2"], default="c2",
+                   help="convert / mask_groups: c1 = the plain 8,192 x 2,000 conversion matrix, c2 = the "
+                        "500,000 x 32,768 grouped-reduction matrix (--rows rows)")
     p.add_argument("--parts", type=int, default=256, help="batched: partitions")
     p.add_argument("--total-rows", type=int, default=8_000_000, help="batched: rows over all partitions")
     p.add_argument("--resident-gb", type=float, default=135.0, help="serving: resident Blocked-ELL bytes")
@@ -239,7 +243,7 @@ def workload_config(spec):
             "rows": spec.rows, "cols": spec.cols, "density": 0.04, "block_size": BLOCK, "groups": GROUPS,
             "row_keep": KEEP_FRAC, "kept_features": KEPT_FEATURES,
             "scheme": "fp32 two-sum, fp64 combine", "l2": "inputs larger than L2 (no flush needed)",
-            "parallelism": "replicas"}
+            "staged": "partition and its column-block index resident (built once)", "parallelism": "replicas"}
 
 
 # ---------------------------------------------------------------------------
@@ -286,10 +290,13 @@ def run_product(args):
            for k in ("sum", "sumsq", "mean", "var")}
     out["group_rows"] = torch.empty(GROUPS, dtype=torch.int32, device="cuda")
     out["status"] = torch.zeros(1, dtype=torch.int32, device="cuda")
+    # the partition's column-block index depends on blockColIdx alone: built once with the
+    # staged partition, as its row pointers would be, not per request
+    index = runtime.build_moments_index(bell, out["status"])
 
     def step(phases=runtime.PHASE_ALL):
         runtime.compute_sparse_group_moments(bell, GROUPS, d_rk, d_fk, d_lab, workspace=ws, out=out, phases=phases,
-                                             chunk_rows=args.chunk_rows)
+                                             chunk_rows=args.chunk_rows, index=index)
 
     for _ in range(args.warmup):
         step()
@@ -337,7 +344,8 @@ def run_product(args):
             # results land in pinned host memory; each group range's rows copy while
             # the next range computes
             runtime.compute_sparse_group_moments_to_host(bell, GROUPS, h_out, r_rk, r_fk, r_lab, workspace=ws,
-                                                         out=out, chunk_rows=args.chunk_rows, parts=args.e2e_parts)
+                                                         out=out, chunk_rows=args.chunk_rows, parts=args.e2e_parts,
+                                                         index=index)
             torch.cuda.current_stream().synchronize()
 
         for _ in range(2):
@@ -656,26 +664,66 @@ def coo_lines(lib, timed, emit, csr):
     del row, scr, bci, val, row_s, col_s, val_s
 
 
+def host_csr_rows(csr, r0: int, r1: int):
+    """(rows, cols, ptr, idx, val) numpy copy of device CSR rows [r0, r1), pointers rebased to 0."""
+    a, b = int(csr.ptr[r0].item()), int(csr.ptr[r1].item())
+    ptr = (csr.ptr[r0:r1 + 1].long() - a).to(dtype=__import__("torch").int32).cpu().numpy().view(np.uint32)
+    return (r1 - r0, csr.cols, ptr, csr.idx[a:b].cpu().numpy().view(np.uint32),
+            csr.val[a:b].cpu().numpy().view(np.uint16))
+
+
+def conversion_cpu_baseline(csr, rows_per_part: int, run, seconds: float, what: str, kind: str = "reference"):
+    """CPU baseline of one conversion: `run(parts, threads, seconds)` -> (s per pass, passes) on
+    one partition of `rows_per_part` rows at 1 thread and on one such partition per host core
+    over all cores (independent partitions, as the reference converts them).  nnz/s."""
+    from oracle import oracle
+
+    n = oracle.cpu_count()
+    rpp = max(1, min(rows_per_part, csr.rows))
+    one = [host_csr_rows(csr, 0, rpp)]
+    many = [host_csr_rows(csr, k * rpp, min(csr.rows, (k + 1) * rpp)) for k in range(n) if k * rpp < csr.rows]
+    nnz1 = sum(len(x[3]) for x in one)
+    nnzn = sum(len(x[3]) for x in many)
+    t1, p1 = run(one, 1, seconds)
+    tn, pn = run(many, n, seconds)
+    return {"value": nnzn / tn, "unit": "nnz/s", "cores": n, "kind": kind,
+            "sample": f"{len(many)} partitions of {rpp} rows ({nnzn} nnz) on {n} host threads, mean of {pn} passes: "
+                      f"{what}",
+            "one_thread": {"value": nnz1 / t1, "unit": "nnz/s", "cores": 1,
+                           "sample": f"one partition of {rpp} rows ({nnz1} nnz), mean of {p1} passes"}}
+
+
+def workload_spec(args):
+    from cellshard_b200 import synth
+
+    return synth.plain_conversion_spec() if args.config == "c1" else synth.grouped_reduction_spec(args.rows)
+
+
 def run_convert(args):
-    """Conversion kernels on the same 500,000 x 32,768 matrix: CSR -> Blocked-ELL-16,
-    Blocked-ELL-16 -> Sliced-ELL (h 32), CSR -> Sliced-ELL (h 32), stable transpose,
-    nnz plan + rebuild.  One JSON line per
-    operation with device time (CUDA events, mean of --steps after --warmup) and
-    algorithmic GB/s."""
+    """Conversion kernels on one matrix (--config c2: 500,000 x 32,768; c1: 8,192 x 2,000):
+    CSR -> Blocked-ELL-16, Blocked-ELL-16 -> Sliced-ELL (h 32), CSR -> Sliced-ELL (h 32),
+    stable transpose, nnz plan + rebuild, execution bucketing, COO.  One JSON line per
+    operation with device time (CUDA events, mean of --steps after --warmup), algorithmic
+    GB/s against the measured copy peak, the clocks sampled over the run and, where the
+    reference has a host routine for it, that routine timed on the host cores."""
     import ctypes as C
 
     import torch
 
-    from cellshard_b200 import _abi, synth
+    from cellshard_b200 import _abi
     from cellshard_b200.device import (blocked_ell_from_csr, blocked_ell_shape, major_nnz_plan,
                                        rebuild_major_order, sliced_ell_from_csr, transpose, ptr, stream_handle)
+    from cellshard_b200 import synth
+    from oracle import oracle
 
     torch.cuda.set_device(0)
-    spec = synth.grouped_reduction_spec(args.rows)
+    spec = workload_spec(args)
     csr = synth.make_csr(spec)
     R, Cc, nnz = spec.rows, spec.cols, csr.nnz
-    peak, _ = measured_peak()
+    peak, peak_kind = measured_peak()
     lib = _abi.load()
+    cpu_rows = 8192 if args.config == "c1" else 2048
+    ref_ok = oracle.ref_available() and not args.no_cpu_baseline
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -693,13 +741,35 @@ def run_convert(args):
 
     def emit(op, ms, nbytes, extra=None):
         gbs = nbytes / (ms * 1e-3) / 1e9
-        d = {"workload": "convert", "op": op, "ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs,
-             "peak_gbs": peak, "frac": gbs / peak, "nnz_per_s": nnz / (ms * 1e-3), "rows": R, "cols": Cc, "nnz": nnz}
+        d = {"workload": "convert", "config": args.config, "op": op, "ms": ms, "algorithmic_bytes": nbytes,
+             "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": peak_kind, "frac": gbs / peak,
+             "nnz_per_s": nnz / (ms * 1e-3), "rows": R, "cols": Cc, "nnz": nnz}
         if extra:
             d.update(extra)
         lines.append(d)
-        print(json.dumps(d), flush=True)
 
+    clocks = ClockSampler(0)
+    try:
+        convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok)
+    finally:
+        clk = clocks.stop()
+        for d in lines:
+            d["clocks"] = clk
+            print(json.dumps(d), flush=True)
+
+
+def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
+    import ctypes as C
+
+    import torch
+
+    from cellshard_b200 import _abi
+    from cellshard_b200.device import (blocked_ell_from_csr, blocked_ell_shape, major_nnz_plan,
+                                       rebuild_major_order, sliced_ell_from_csr, ptr, stream_handle)
+    from oracle import oracle
+
+    R, Cc, nnz = spec.rows, spec.cols, csr.nnz
+    secs = max(2.0, args.cpu_seconds / 4)
     # Blocked-ELL: shape (with bitmaps) and emit timed separately
     B = BLOCK
     width, _tot, scratch, status = blocked_ell_shape(csr, B)
@@ -714,8 +784,14 @@ def run_convert(args):
     nnz_t = torch.zeros(1, dtype=torch.int32, device="cuda")
     ms_emit = timed(lambda: lib.cs_b200_blocked_ell_emit(C.byref(v), C.byref(dv), ptr(nnz_t), ptr(scratch),
                                                          scratch.numel(), ptr(status), stream_handle()))
-    emit("blocked_ell_emit", ms_emit, 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4,
-         {"ell_cols": bell.ell_cols})
+    ex = {"ell_cols": bell.ell_cols, "shape_ms": ms_shape,
+          "conversion_ms": ms_shape + ms_emit,
+          "note": "emit only; shape_ms is the bitmap / width pass the emit needs (conversion = both)"}
+    if ref_ok:
+        ex["cpu_baseline"] = conversion_cpu_baseline(
+            csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_blocked_ell_from_compressed(parts, B, th, sec), secs,
+            "the reference's convert::blocked_ell_from_compressed (block 16) compiled from its sources")
+    emit("blocked_ell_emit", ms_emit, 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4, ex)
     # Blocked-ELL -> Sliced-ELL (h 32): live-entry row pointers (count + scan), then the emit;
     # both read the whole value array (the layout needs every row's count before any slot)
     from cellshard_b200.device import blocked_ell_row_ptr, sliced_ell_from_blocked_ell
@@ -761,15 +837,49 @@ def run_convert(args):
     torch.cuda.empty_cache()
     coo_lines(lib, timed, emit, csr)
     torch.cuda.empty_cache()
-    # Sliced-ELL at h = 32: layout + emit (the layout's total needs one host read)
+    # Sliced-ELL at h = 32: the whole conversion (layout + emit, device only, into arrays sized
+    # by a first run) and the emit alone; the slice-height candidates (16 / 32 / 64) of the chooser
     sell = sliced_ell_from_csr(csr, 32)
     S = sell.slice_count
     total = int(sell.col_idx.numel())
     sv = sell.view()
+    nbs = C.c_size_t()
+    lib.cs_b200_sliced_ell_scratch_bytes(R, 32, C.byref(nbs))
+    sscr = torch.empty(max(nbs.value, 16), dtype=torch.uint8, device="cuda")
+    stot = torch.zeros(1, dtype=torch.int64, device="cuda")
+    sell_bytes = 4 * (R + 1) + 6 * nnz + 6 * total + 4 * (2 * S + 1)
+
+    def sell_full():
+        lib.cs_b200_sliced_ell_layout(C.byref(v), 32, ptr(sell.slice_row_offsets), ptr(sell.slice_widths),
+                                      ptr(sell.slice_slot_offsets), ptr(stot), ptr(sscr), nbs.value, stream_handle())
+        lib.cs_b200_sliced_ell_emit(C.byref(v), C.byref(sv), stream_handle())
+
+    ms_full = timed(sell_full)
+    assert int(stot.item()) == total
+    ex = {"total_slots": total, "slice_rows": 32,
+          "note": "layout (row nnz, slice widths, slot offsets, total) + emit; bytes: CSR read once, Sliced-ELL "
+                  "written (the layout's own pass over the row pointers is not credited)"}
+    if ref_ok:
+        ex["cpu_baseline"] = conversion_cpu_baseline(
+            csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_sliced_ell_from_compressed(parts, 32, th, sec), secs,
+            "the reference's convert::sliced_ell_from_compressed (h 32) compiled from its sources")
+    emit("sliced_ell_from_csr", ms_full, sell_bytes, ex)
     ms_sell = timed(lambda: lib.cs_b200_sliced_ell_emit(C.byref(v), C.byref(sv), stream_handle()))
-    emit("sliced_ell_emit", ms_sell, 4 * (R + 1) + 6 * nnz + 6 * total + 4 * (2 * S + 1), {"total_slots": total})
+    emit("sliced_ell_emit", ms_sell, sell_bytes, {"total_slots": total})
+    cands = (C.c_uint32 * 3)(16, 32, 64)
+    padded = torch.zeros(3, dtype=torch.int64, device="cuda")
+    ms_c = timed(lambda: lib.cs_b200_sliced_ell_candidates(C.byref(v), cands, 3, ptr(padded), stream_handle()))
+    ex = {"candidates": [16, 32, 64], "padded_slots": [int(x) for x in padded.cpu()],
+          "note": "padded slots of every candidate height (the device half of the chooser); time only"}
+    if ref_ok:
+        ex["cpu_baseline"] = conversion_cpu_baseline(
+            csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_sliced_ell_from_compressed(
+                parts, 0, th, sec, candidates=(16, 32, 64)), secs,
+            "the reference's choose_sliced_ell_slice_rows_from_compressed (16 / 32 / 64) + "
+            "sliced_ell_from_compressed at its choice")
+    emit("sliced_ell_candidates", ms_c, 4 * (R + 1), ex)
     bucket_lines(lib, timed, emit, None, sell)
-    del sell
+    del sell, sscr
     torch.cuda.empty_cache()
     # transpose
     nb = C.c_size_t()
@@ -781,12 +891,27 @@ def run_convert(args):
     ms_t = timed(lambda: lib.cs_b200_build_compressed_transpose(R, Cc, nnz, ptr(csr.ptr), ptr(csr.idx), ptr(csr.val),
                                                                ptr(optr), None, ptr(oidx), ptr(oval), ptr(tscr),
                                                                nb.value, stream_handle()))
-    emit("transpose", ms_t, 4 * (R + 1) + 6 * nnz + 4 * (Cc + 1) + 6 * nnz)
+    ex = {}
+    if not args.no_cpu_baseline:
+        ex["cpu_baseline"] = conversion_cpu_baseline(
+            csr, cpu_rows, lambda parts, th, sec: oracle.time_restated(
+                lambda q: oracle.csr_transpose(q[0], q[1], q[2], q[3], q[4]), parts, th, sec), secs,
+            "restated stable counting-sort transpose (oracle/cs_oracle.c; the reference transposes on the GPU "
+            "only, through cuSPARSE), one independent partition per thread", kind="port")
+    emit("transpose", ms_t, 4 * (R + 1) + 6 * nnz + 4 * (Cc + 1) + 6 * nnz, ex)
     del oidx, oval, tscr
     torch.cuda.empty_cache()
     # nnz plan (+ pow2 bins) and rebuild
     ms_p = timed(lambda: major_nnz_plan(csr.ptr, R, 64))
-    emit("nnz_plan", ms_p, 4 * (R + 1) + 12 * R + 4 * 65)
+    ex = {}
+    if not args.no_cpu_baseline:
+        hp = csr.ptr.cpu().numpy().view(np.uint32)
+        t, k = oracle.time_restated(lambda q: oracle.major_nnz_plan(q, R, 64), [hp], 1, secs)
+        ex["cpu_baseline"] = {"value": R / t, "unit": "rows/s", "cores": 1, "kind": "port",
+                              "sample": f"all {R} rows, restated stable sort by nnz + equal-count offsets "
+                                        f"(the reference plans on the GPU only, with CUB), mean of {k} passes"}
+    ex["rows_per_s"] = R / (ms_p * 1e-3)
+    emit("nnz_plan", ms_p, 4 * (R + 1) + 12 * R + 4 * 65, ex)
     plan = major_nnz_plan(csr.ptr, R, 64)
     ms_r = timed(lambda: rebuild_major_order(csr, plan["order"]))
     emit("rebuild", ms_r, 6 * nnz + 4 * (R + 1) + 6 * nnz + 4 * (R + 1) + 4 * R)
@@ -794,32 +919,40 @@ def run_convert(args):
 
 def run_mask_groups(args):
     """mask_groups reduce (row totals, maxima, detected counts, 8 feature-group sums,
-    keep decision) over the grouped-reduction matrix held as CSR, Sliced-ELL (h 32) and
-    Blocked-ELL-16, with 70 % of rows and 60 % of features kept.  One JSON line per
-    format: device time (CUDA events, mean of --steps after --warmup) and algorithmic
-    GB/s = the stored entries / slots of the kept rows, each row's metadata and flag,
-    the column tables and the outputs, each counted once."""
+    keep decision) over one matrix (--config c2: 500,000 x 32,768; c1: 8,192 x 2,000) held
+    as CSR, Sliced-ELL (h 32) and Blocked-ELL-16, with 70 % of rows and 60 % of features
+    kept.  One JSON line per format: device time (CUDA events, mean of --steps after
+    --warmup), algorithmic GB/s = the stored entries / slots of the kept rows, each row's
+    metadata and flag, the column tables and the outputs, each counted once; the clocks
+    sampled over the run; and the restated CPU reduce (the reference's is GPU-only) timed on
+    the host cores over independent row slices."""
     import torch
 
     from cellshard_b200 import runtime, synth
     from cellshard_b200.device import blocked_ell_from_csr, sliced_ell_from_csr
+    from oracle import oracle
 
     torch.cuda.set_device(0)
-    spec = synth.grouped_reduction_spec(args.rows)
+    spec = workload_spec(args)
     csr = synth.make_csr(spec)
     R, Cc, nnz = spec.rows, spec.cols, csr.nnz
-    peak, _ = measured_peak()
+    peak, peak_kind = measured_peak()
     rng = np.random.default_rng(5)
     G = 8
     masks = (rng.integers(0, 1 << G, Cc) & rng.integers(0, 2, Cc) * 0xFF).astype(np.uint32)
     gm = torch.from_numpy(masks.view(np.int32)).cuda()
     rk_h = rng.random(R) < 0.7
     rk = torch.from_numpy(rk_h.astype(np.uint8)).cuda()
-    fk = torch.from_numpy((rng.random(Cc) < 0.6).astype(np.uint8)).cuda()
+    fk_h = (rng.random(Cc) < 0.6).astype(np.uint8)
+    fk = torch.from_numpy(fk_h).cuda()
     filt = runtime.FilterParams(10.0, 5, 0.9, 0)
+    fl = (10.0, 5, 0.9, 0)
     kept = torch.from_numpy(rk_h).cuda()
     row_nnz = (csr.ptr[1:] - csr.ptr[:-1]).long()
     common = R + Cc * 5 + R * 13 + R * G * 8  # row flags, column tables, outputs
+    threads = oracle.cpu_count()
+    slice_rows = 8192 if args.config == "c1" else 2048
+    secs = max(2.0, args.cpu_seconds / 4)
 
     def timed(fn):
         for _ in range(args.warmup):
@@ -833,33 +966,88 @@ def run_mask_groups(args):
         torch.cuda.synchronize()
         return float(np.mean([a.elapsed_time(b) for a, b in ev]))
 
+    lines = []
+
     def emit(fmt, ms, nbytes, extra=None):
         gbs = nbytes / (ms * 1e-3) / 1e9
-        d = {"workload": "mask_groups", "format": fmt, "ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs,
-             "peak_gbs": peak, "frac": gbs / peak, "rows": R, "cols": Cc, "nnz": nnz, "groups": G,
-             "kept_rows": int(rk_h.sum())}
+        d = {"workload": "mask_groups", "config": args.config, "format": fmt, "ms": ms, "algorithmic_bytes": nbytes,
+             "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": peak_kind, "frac": gbs / peak, "rows": R,
+             "cols": Cc, "nnz": nnz, "groups": G, "kept_rows": int(rk_h.sum()), "rows_per_s": R / (ms * 1e-3)}
         if extra:
             d.update(extra)
-        print(json.dumps(d), flush=True)
+        lines.append(d)
 
-    ms = timed(lambda: runtime.compute_sparse_group_reduce(csr, gm, G, rk, fk, filt))
-    emit("compressed", ms, common + 4 * (R + 1) + 6 * int(row_nnz[kept].sum()))
-    sell = sliced_ell_from_csr(csr, 32)
-    widths = sell.slice_widths.long().repeat_interleave(32)[:R]
-    ms = timed(lambda: runtime.compute_sparse_group_reduce(sell, gm, G, rk, fk, filt))
-    emit("sliced_ell", ms, common + 4 * 3 * sell.slice_count + 6 * int(widths[kept].sum()),
-         {"total_slots": int(sell.col_idx.numel())})
-    del sell
-    torch.cuda.empty_cache()
-    bell = blocked_ell_from_csr(csr, BLOCK)
-    del csr
-    torch.cuda.empty_cache()
-    W = bell.ell_cols // BLOCK
-    kept_blocks = int(kept.view(-1)[: (R // BLOCK) * BLOCK].view(-1, BLOCK).any(1).sum()) + (
-        int(kept[(R // BLOCK) * BLOCK:].any()) if R % BLOCK else 0)
-    ms = timed(lambda: runtime.compute_sparse_group_reduce(bell, gm, G, rk, fk, filt))
-    emit("blocked_ell", ms, common + 2 * bell.ell_cols * int(rk_h.sum()) + 4 * W * kept_blocks,
-         {"ell_cols": bell.ell_cols})
+    def cpu(run, what):
+        """restated reduce over one independent row slice per host thread; rows/s"""
+        if args.no_cpu_baseline:
+            return None
+        n = min(threads, max(1, R // slice_rows))
+        parts = [(k * slice_rows, min(R, (k + 1) * slice_rows)) for k in range(n)]
+        t, k = oracle.time_restated(run, parts, threads, secs)
+        rows = sum(b - a for a, b in parts)
+        return {"value": rows / t, "unit": "rows/s", "cores": threads, "kind": "port",
+                "sample": f"{n} row slices of {slice_rows} rows, one per thread, mean of {k} passes: restated "
+                          f"{what} (oracle/cs_oracle.c; the reference's reduce runs on the GPU only)"}
+
+    clocks = ClockSampler(0)
+    try:
+        ms = timed(lambda: runtime.compute_sparse_group_reduce(csr, gm, G, rk, fk, filt))
+        hp = csr.ptr.cpu().numpy().view(np.uint32)
+        # slices are copied to the host once, outside the timed passes
+        host_slices = {}
+        for k in range(min(threads, max(1, R // slice_rows))):
+            a, b = k * slice_rows, min(R, (k + 1) * slice_rows)
+            lo, hi_ = int(hp[a]), int(hp[b])
+            host_slices[(a, b)] = (hp[a:b + 1] - hp[a], csr.idx[lo:hi_].cpu().numpy().view(np.uint32),
+                                   csr.val[lo:hi_].cpu().numpy().view(np.uint16))
+
+        def run_csr_h(ab):
+            a, b = ab
+            p_, i_, v_ = host_slices[ab]
+            oracle.group_reduce_csr(b - a, Cc, p_, i_, v_, masks, G, rk_h[a:b].astype(np.uint8), fk_h, fl)
+
+        emit("compressed", ms, common + 4 * (R + 1) + 6 * int(row_nnz[kept].sum()),
+             {"cpu_baseline": cpu(run_csr_h, "compressed reduce")})
+        sell = sliced_ell_from_csr(csr, 32)
+        widths = sell.slice_widths.long().repeat_interleave(32)[:R]
+        ms = timed(lambda: runtime.compute_sparse_group_reduce(sell, gm, G, rk, fk, filt))
+        hs = {ab: oracle.sliced_ell_from_csr(ab[1] - ab[0], p_, i_, v_, 32) for ab, (p_, i_, v_) in host_slices.items()}
+
+        def run_sell(ab):
+            a, b = ab
+            q = hs[ab]
+            oracle.group_reduce_sell(b - a, Cc, 32, q["offsets"], q["widths"], q["slot_offsets"], q["col_idx"],
+                                     q["val"], masks, G, rk_h[a:b].astype(np.uint8), fk_h, fl)
+
+        emit("sliced_ell", ms, common + 4 * 3 * sell.slice_count + 6 * int(widths[kept].sum()),
+             {"total_slots": int(sell.col_idx.numel()), "cpu_baseline": cpu(run_sell, "Sliced-ELL (h 32) reduce")})
+        del sell
+        torch.cuda.empty_cache()
+        bell = blocked_ell_from_csr(csr, BLOCK)
+        del csr
+        torch.cuda.empty_cache()
+        W = bell.ell_cols // BLOCK
+        kept_blocks = int(kept.view(-1)[: (R // BLOCK) * BLOCK].view(-1, BLOCK).any(1).sum()) + (
+            int(kept[(R // BLOCK) * BLOCK:].any()) if R % BLOCK else 0)
+        ms = timed(lambda: runtime.compute_sparse_group_reduce(bell, gm, G, rk, fk, filt))
+        hb = {}
+        for (a, b) in host_slices:
+            hb[(a, b)] = (bell.bci[(a // BLOCK) * W:((b + BLOCK - 1) // BLOCK) * W].cpu().numpy().view(np.uint32),
+                          bell.val[a * bell.ell_cols:b * bell.ell_cols].cpu().numpy().view(np.uint16))
+
+        def run_bell(ab):
+            a, b = ab
+            bci, val = hb[ab]
+            oracle.group_reduce_bell(b - a, Cc, BLOCK, bell.ell_cols, bci, val, masks, G,
+                                     rk_h[a:b].astype(np.uint8), fk_h, fl)
+
+        emit("blocked_ell", ms, common + 2 * bell.ell_cols * int(rk_h.sum()) + 4 * W * kept_blocks,
+             {"ell_cols": bell.ell_cols, "cpu_baseline": cpu(run_bell, "Blocked-ELL-16 reduce")})
+    finally:
+        clk = clocks.stop()
+        for d in lines:
+            d["clocks"] = clk
+            print(json.dumps(d), flush=True)
 
 
 BATCH_CANDIDATES = (16, 32, 64)

@@ -113,7 +113,8 @@ class GroupReduceOut(C.Structure):
 
 
 class GroupMomentsParams(C.Structure):
-    _fields_ = [("group_count", u32), ("scheme", u32), ("ddof", u32), ("chunk_rows", u32)]
+    _fields_ = [("group_count", u32), ("scheme", u32), ("ddof", u32), ("chunk_rows", u32), ("index", vp),
+                ("_align16", C.c_ubyte * 8)]
 
 
 class GroupMomentsOut(C.Structure):
@@ -276,6 +277,8 @@ PROTOTYPES: dict[str, tuple] = {
                                            vp]),
     "cs_b200_reoptimize_emit": (C.c_int, [P(BlockedEllView), P(RowFeatureMaskView), u32, u32, vp, vp, vp, vp]),
     "cs_b200_group_moments_scratch_bytes": (C.c_int, [P(BlockedEllView), P(GroupMomentsParams), P(sz)]),
+    "cs_b200_group_moments_index_bytes": (C.c_int, [P(BlockedEllView), P(sz)]),
+    "cs_b200_group_moments_build_index": (C.c_int, [P(BlockedEllView), vp, vp, vp]),
     "cs_b200_group_moments_blocked_ell": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
                                                     P(GroupMomentsOut), vp, sz, vp]),
     "cs_b200_group_moments_blocked_ell_noalloc": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),

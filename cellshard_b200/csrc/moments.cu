@@ -572,13 +572,16 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
     cudaStream_t stream = as_stream(s);
     const uint32_t G = params->group_count;
     const uint32_t width = src->ell_cols / src->block_size;
+    // a column-block index the caller built once for this partition replaces the scratch one
+    const bool prebuilt = params->index != nullptr;
+    if (prebuilt) lay.index = static_cast<uint2 *>(const_cast<void *>(params->index));
     // accumulate and combine may be restricted to groups [g_lo, g_hi)
     if (g_hi > G) g_hi = G;
     const bool all_groups = g_lo == 0u && g_hi == G;
     if (g_lo >= g_hi) return 1;
     const uint32_t *range_first = all_groups ? nullptr : lay.chunk_first;
 
-    if ((phases & CS_MOMENTS_PHASE_PREPARE) && lay.row_blocks != 0u && lay.words != 0u) {
+    if ((phases & CS_MOMENTS_PHASE_PREPARE) && !prebuilt && lay.row_blocks != 0u && lay.words != 0u) {
         if (width != 0u) {
             const uint32_t blocks = (lay.row_blocks + kIndexWarps - 1u) / kIndexWarps;
             const std::size_t smem = (std::size_t) kIndexWarps * lay.words * sizeof(uint32_t);
@@ -687,6 +690,13 @@ int build_column_block_index(const cs_blocked_ell_view *src, uint2 *index, uint3
     return launch_ok("moments_index_kernel");
 }
 
+std::size_t column_block_index_bytes(const cs_blocked_ell_view *src) {
+    const uint32_t B = src->block_size;
+    const std::size_t row_blocks = (src->rows + B - 1u) / B;
+    const std::size_t words = (((std::size_t) src->cols + B - 1u) / B + 31u) / 32u;
+    return (row_blocks * words + 1u) * sizeof(uint2);
+}
+
 // Scratch bytes the moments reduction needs for (src, params); 0 when the
 // arguments are invalid (the error message is set).
 std::size_t group_moments_scratch_needed(const cs_blocked_ell_view *src, const cs_group_moments_params *params) {
@@ -714,6 +724,30 @@ extern "C" int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
                                                   size_t scratch_bytes, cs_stream_t s) {
     return moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, out, d_scratch, scratch_bytes, s,
                        CS_MOMENTS_PHASE_ALL);
+}
+
+extern "C" int cs_b200_group_moments_index_bytes(const cs_blocked_ell_view *src, size_t *out_bytes) {
+    if (src == nullptr || out_bytes == nullptr || src->block_size == 0u) {
+        set_error("group_moments_index_bytes: null argument or zero block size");
+        return 0;
+    }
+    *out_bytes = column_block_index_bytes(src);
+    return 1;
+}
+
+extern "C" int cs_b200_group_moments_build_index(const cs_blocked_ell_view *src, void *d_index, uint32_t *d_status,
+                                                  cs_stream_t s) {
+    if (src == nullptr || d_index == nullptr || src->block_size == 0u || src->ell_cols % src->block_size != 0u ||
+        (src->rows != 0u && src->ell_cols != 0u && src->blockColIdx == nullptr)) {
+        set_error("group_moments_build_index: null argument, zero block size or block size not dividing ell_cols");
+        return 0;
+    }
+    const uint32_t col_blocks = (src->cols + src->block_size - 1u) / src->block_size;
+    if ((col_blocks + 31u) / 32u > kMaxIndexWords) {
+        set_error("group_moments_build_index: %u column blocks exceed the index limit", col_blocks);
+        return 0;
+    }
+    return build_column_block_index(src, static_cast<uint2 *>(d_index), d_status, as_stream(s));
 }
 
 extern "C" int cs_b200_group_moments_phases(const cs_blocked_ell_view *src, const uint8_t *d_row_keep,

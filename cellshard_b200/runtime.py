@@ -199,15 +199,30 @@ def group_moments_scratch_bytes(src: BlockedELL, group_count: int, scheme: int =
     return n.value
 
 
+def build_moments_index(src: BlockedELL, status: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """The partition's column-block index (cs_b200_group_moments_build_index), built once
+    and passed as ``index=`` to later reductions over the same partition, which then skip
+    rebuilding it.  Order errors in blockColIdx go to ``status`` (int32[1]) when given."""
+    lib = _abi.load()
+    v = src.view()
+    n = C.c_size_t()
+    _abi.check(lib.cs_b200_group_moments_index_bytes(C.byref(v), C.byref(n)), "moments index bytes")
+    index = torch.empty(max(n.value, 16), dtype=torch.uint8, device="cuda")
+    _abi.check(lib.cs_b200_group_moments_build_index(C.byref(v), ptr(index), ptr(status), stream_handle(stream)),
+               "moments index")
+    return index
+
+
 def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=None, feature_keep=None,
                                  row_labels=None, scheme: int = TWOSUM_F64_COMBINE, ddof: int = 1,
                                  chunk_rows: int = 0, workspace: MomentsWorkspace | None = None, out=None,
-                                 want_f64: bool = False, phases: int = 7, stream=None):
+                                 want_f64: bool = False, phases: int = 7, stream=None, index=None):
     """Per-(group, feature) sum / sum of squares / mean / variance over kept rows of a
-    Blocked-ELL partition; returns a dict of device tensors ([G, cols])."""
+    Blocked-ELL partition; returns a dict of device tensors ([G, cols]).  ``index``: the
+    partition's column-block index from build_moments_index (None = rebuilt by this call)."""
     lib = _abi.load()
     G, cols = group_count, src.cols
-    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows)
+    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows, ptr(index))
     v = src.view()
     n = C.c_size_t()
     _abi.check(lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(p), C.byref(n)), "moments scratch")
@@ -243,15 +258,17 @@ def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=Non
 def compute_sparse_group_moments_to_host(src: BlockedELL, group_count: int, host_out: dict, row_keep=None,
                                          feature_keep=None, row_labels=None, scheme: int = TWOSUM_F64_COMBINE,
                                          ddof: int = 1, chunk_rows: int = 0, parts: int = 0,
-                                         workspace: MomentsWorkspace | None = None, out=None, stream=None):
+                                         workspace: MomentsWorkspace | None = None, out=None, stream=None,
+                                         index=None):
     """compute_sparse_group_moments with the results copied into ``host_out`` (pinned CPU
     tensors keyed like the device outputs: sum, sumsq, mean, var, mean64, var64,
     group_rows, status), the groups split into ``parts`` ranges whose copies overlap the
     next range's work (cs_b200_group_moments_to_host).  Synchronise the stream before
-    reading ``host_out``.  Returns the device outputs."""
+    reading ``host_out``.  Returns the device outputs.  ``index`` as in
+    compute_sparse_group_moments."""
     lib = _abi.load()
     G, cols = group_count, src.cols
-    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows)
+    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows, ptr(index))
     v = src.view()
     n = C.c_size_t()
     _abi.check(lib.cs_b200_group_moments_scratch_bytes(C.byref(v), C.byref(p), C.byref(n)), "moments scratch")

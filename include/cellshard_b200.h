@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define CS_B200_ABI_VERSION 1
+#define CS_B200_ABI_VERSION 2
 #define CS_ALIGN16 __attribute__((aligned(16)))
 #define CS_API __attribute__((visibility("default")))
 
@@ -822,6 +822,12 @@ typedef struct CS_ALIGN16 cs_group_moments_params {
     uint32_t scheme;      /* CS_MOMENTS_* */
     uint32_t ddof;        /* variance divisor is n - ddof (0 or 1) */
     uint32_t chunk_rows;  /* rows per work chunk, 0 = default */
+    /* Optional (NULL = built by every call): device address of the partition's
+     * column-block index, built once by cs_b200_group_moments_build_index for
+     * this partition (it depends only on blockColIdx, so it stays valid while
+     * the staged partition does).  The prepare phase then skips the index pass
+     * and the accumulation reads this one. */
+    const void *index;
 } cs_group_moments_params;
 
 /* All arrays are device memory, [G x cols] row-major unless noted.  Only sum
@@ -840,6 +846,15 @@ typedef struct CS_ALIGN16 cs_group_moments_out {
 CS_API int cs_b200_group_moments_scratch_bytes(const cs_blocked_ell_view *src,
                                         const cs_group_moments_params *params,
                                         size_t *out_bytes);
+
+/* The column-block index of a Blocked-ELL partition, kept with the staged
+ * partition so repeated reductions over it skip rebuilding it: one
+ * (occupancy bitmap of 32 column blocks, slots before them) pair per row block
+ * and 32 column blocks.  The build validates blockColIdx order into *d_status
+ * (CS_STATUS_BLOCK_COL_ORDER; nullable) and is stream-ordered. */
+CS_API int cs_b200_group_moments_index_bytes(const cs_blocked_ell_view *src, size_t *out_bytes);
+CS_API int cs_b200_group_moments_build_index(const cs_blocked_ell_view *src, void *d_index, uint32_t *d_status,
+                                             cs_stream_t stream);
 
 /* For every kept row r (d_row_keep[r] != 0, or all rows when NULL) with label
  * g = d_row_labels[r] < G (all rows in group 0 when NULL), and every stored

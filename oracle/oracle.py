@@ -989,3 +989,65 @@ def cpu_count() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:  # pragma: no cover
         return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines: the reference's host conversions (and the restated CPU paths
+# where the reference has none) timed over independent partitions on a pool
+# of host threads.  ctypes releases the GIL inside the foreign call, so the
+# threads run in parallel.  Outputs are freed, not copied back.
+# ---------------------------------------------------------------------------
+def _pool_time(parts, one, threads, seconds):
+    """Runs one(part) over `parts` on `threads` threads, repeating the list until
+    `seconds` of wall time have passed (at least once); returns (seconds, passes)."""
+    import time
+    from concurrent.futures import ThreadPoolExecutor
+
+    t0 = time.perf_counter()
+    passes = 0
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        while True:
+            list(ex.map(one, parts))
+            passes += 1
+            if time.perf_counter() - t0 >= seconds or passes >= 50:
+                break
+    return (time.perf_counter() - t0) / passes, passes
+
+
+def ref_time_blocked_ell_from_compressed(parts, B, threads, seconds=3.0):
+    """convert::blocked_ell_from_compressed (the reference's host routine) on every
+    (rows, cols, ptr, idx, val) partition; seconds per pass over all partitions."""
+    def one(p):
+        rows, cols, ptr, idx, val = p
+        src = host_csr(rows, cols, ptr, idx, val)
+        dst = HostBlockedEll()
+        assert ref().csref_blocked_ell_from_compressed(C.byref(src), C.c_uint(B), C.byref(dst)) == 1
+        ref().csref_free(dst.storage)
+
+    return _pool_time(parts, one, threads, seconds)
+
+
+def ref_time_sliced_ell_from_compressed(parts, slice_rows, threads, seconds=3.0, candidates=None):
+    """convert::sliced_ell_from_compressed (host) at `slice_rows`, or, with
+    `candidates`, choose_sliced_ell_slice_rows_from_compressed first and convert at
+    its choice; seconds per pass over all partitions."""
+    def one(p):
+        rows, cols, ptr, idx, val = p
+        src = host_csr(rows, cols, ptr, idx, val)
+        h = slice_rows
+        if candidates:
+            c = (C.c_uint * len(candidates))(*candidates)
+            out = SlicedTune()
+            assert ref().csref_choose_sliced_ell_slice_rows_from_compressed(C.byref(src), c, C.c_uint(len(candidates)),
+                                                                            C.byref(out)) == 1
+            h = out.slice_rows
+        dst = HostSlicedEll()
+        assert ref().csref_sliced_ell_from_compressed(C.byref(src), C.c_uint(h), C.byref(dst)) == 1
+        ref().csref_free(dst.storage)
+
+    return _pool_time(parts, one, threads, seconds)
+
+
+def time_restated(fn, parts, threads, seconds=3.0):
+    """Seconds per pass of a restated CPU routine fn(part) over `parts`."""
+    return _pool_time(parts, fn, threads, seconds)

@@ -129,7 +129,7 @@ def test_ctypes_layouts_match_c(tmp_path):
 
 
 def test_abi_version_and_host_validation(cs_lib):
-    assert cs_lib.cs_b200_abi_version() == 1
+    assert cs_lib.cs_b200_abi_version() == 2
     v = _abi.BlockedEllView()
     v.rows, v.cols, v.block_size, v.ell_cols = 100, 64, 16, 64
     n = C.c_size_t()

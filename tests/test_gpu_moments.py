@@ -226,3 +226,37 @@ def test_moments_headline_layout(cuda, orc, chunk_rows):
     err = orc.moments_max_rel({k: res[k].cpu().numpy() for k in ("sum", "sumsq", "mean", "var")}, ref)
     assert max(err.values()) <= RTOL, err
 
+
+
+def test_moments_prebuilt_index_matches(cuda, orc):
+    """A column-block index built once for the partition (build_moments_index) gives the
+    same bits as the index each call builds, for the one-shot call, the phases and the
+    host-delivery call, over repeated requests."""
+    import torch
+
+    from cellshard_b200 import runtime
+
+    rows, cols, G = 3000, 203, 7
+    bell = _bell(cuda, rows, cols, 16, 0.06, seed=21, integer=False)
+    idx = runtime.build_moments_index(bell)
+    for seed in (1, 2):
+        rk, fk, lab = _masks(rows, cols, G, seed)
+        a = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=128)
+        b = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=128, index=idx)
+        ws = runtime.MomentsWorkspace()
+        c = None
+        for ph in (runtime.PHASE_PREPARE, runtime.PHASE_ACCUMULATE, runtime.PHASE_COMBINE):
+            c = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=128,
+                                                     index=idx, workspace=ws, out=c, phases=ph)
+        host = {k: torch.empty((G, cols), dtype=torch.float32).pin_memory() for k in ("sum", "sumsq", "mean", "var")}
+        runtime.compute_sparse_group_moments_to_host(bell, G, host, _dev(rk), _dev(fk), _dev(lab), chunk_rows=128,
+                                                     index=idx)
+        torch.cuda.synchronize()
+        for k in ("sum", "sumsq", "mean", "var"):
+            want = a[k].cpu().numpy().view(np.uint32)
+            assert np.array_equal(b[k].cpu().numpy().view(np.uint32), want), k
+            assert np.array_equal(c[k].cpu().numpy().view(np.uint32), want), k
+            assert np.array_equal(host[k].numpy().view(np.uint32), want), k
+        bci, val = _host(bell)
+        ref = orc.group_moments_bell(rows, cols, 16, bell.ell_cols, bci, val, rk, fk, lab, G, ddof=1)
+        _check(b, ref, G, cols)
