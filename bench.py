@@ -86,7 +86,9 @@ def parse():
     p.add_argument("--resident-gb", type=float, default=135.0, help="serving: resident Blocked-ELL bytes")
     p.add_argument("--rates", type=str, default="100,300,1000,3000,5000", help="serving: arrival rates (req/s)")
     p.add_argument("--requests", type=int, default=200, help="serving: requests per rate")
-    p.add_argument("--plain-requests", type=int, default=40, help="serving: requests timed on the plain path")
+    p.add_argument("--plain-requests", type=int, default=40,
+                   help="serving: requests timed one by one on the plain path (service times)")
+    p.add_argument("--distinct", type=int, default=96, help="serving: distinct requests replayed by the traces")
     return p.parse_args()
 
 
@@ -1286,7 +1288,7 @@ def run_serving(args):
         torch.cuda.empty_cache()
     total_rows = rows_per_part * SERVE_PARTS
     resident = sum(p.rows * p.ell_cols * 2 + p.bci.numel() * 4 for p in parts)
-    n_distinct = 24
+    n_distinct = args.distinct
     rq = serving_requests(total_rows, cols, n_distinct)
     reqs = [Request(G, rk, lab, fk, cols, want_moments=False) for (G, rk, lab, fk) in rq]
     kept = [int(r[1].sum()) for r in rq]
@@ -1320,41 +1322,82 @@ def run_serving(args):
             best = line
     st = srv.stats()
     srv.close()
-    clk = clocks.stop()
 
-    # plain per-call path: per request, every partition through the single-partition entry
-    # point (one launch sequence per partition) -> sync -> partition sums added in fp64 -> D2H
+    # plain per-call path (the serving baseline): per request, the masks and labels copied in
+    # from pinned memory, ONE launch sequence of the moments reduction over all 64 resident
+    # partitions (cs_b200_group_moments_blocked_ell_parts, each partition's column-block
+    # index built once at open, as the server's is), one synchronisation, sum and sumsq
+    # copied back; buffers sized once for the largest request; requests strictly one after
+    # another, replayed against the same Poisson arrivals as the served path.
+    idxs = [runtime.build_moments_index(p) for p in parts]
+    gmax = max(G for (G, _rk, _lab, _fk) in rq)
     ws = runtime.MomentsWorkspace()
-    offs = np.cumsum([0] + [p.rows for p in parts])
-    plain_ms = []
+    d_rk = torch.empty(total_rows, dtype=torch.uint8, device="cuda")
+    d_lab = torch.empty(total_rows, dtype=torch.int32, device="cuda")
+    d_fk = torch.empty(cols, dtype=torch.uint8, device="cuda")
+    big = {k: torch.empty((gmax, cols), dtype=torch.float32, device="cuda") for k in ("sum", "sumsq")}
+    big_rows = torch.empty(gmax, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ws.reserve(max(runtime.group_moments_parts_scratch_bytes(parts, G) for (G, _a, _b, _c) in rq))
+
+    def plain(k):
+        G = rq[k][0]
+        r = reqs[k]
+        d_rk.copy_(r.row_keep, non_blocking=True)
+        d_lab.copy_(r.row_labels, non_blocking=True)
+        d_fk.copy_(r.feature_keep, non_blocking=True)
+        out = {"sum": big["sum"][:G], "sumsq": big["sumsq"][:G], "group_rows": big_rows[:G], "status": status}
+        runtime.compute_sparse_group_moments_parts(parts, G, d_rk, d_fk, d_lab, indexes=idxs, workspace=ws, out=out)
+        r.sum.copy_(out["sum"], non_blocking=True)
+        r.sumsq.copy_(out["sumsq"], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for k in range(min(4, n_distinct)):
+        plain(k)
+    # accuracy check on one request: the plain path's sums equal the served path's within 1e-6
+    srv2 = Server(parts, scratch_budget_bytes=SERVE_BUDGET, max_inflight=32)
+    chk = Request(rq[0][0], rq[0][1], rq[0][2], rq[0][3], cols, want_moments=False)
+    srv2.wait(srv2.submit(chk), 120000)
+    srv2.close()
+    plain(0)
+    served_sum, plain_sum = chk.sum.numpy().astype(np.float64), reqs[0].sum.numpy().astype(np.float64)
+    agree = float((np.abs(served_sum - plain_sum) / np.maximum(np.abs(served_sum), 1e-30)).max())
+    service_ms = []
     for k in range(args.plain_requests):
-        G, rk, lab, fk = rq[k % n_distinct]
-        r = reqs[k % n_distinct]
         t0 = time.perf_counter()
-        d_rk = r.row_keep.cuda(non_blocking=True)
-        d_lab = r.row_labels.cuda(non_blocking=True)
-        d_fk = r.feature_keep.cuda(non_blocking=True)
-        s64 = torch.zeros((G, cols), dtype=torch.float64, device="cuda")
-        q64 = torch.zeros((G, cols), dtype=torch.float64, device="cuda")
-        out = {"sum": torch.empty((G, cols), dtype=torch.float32, device="cuda"),
-               "sumsq": torch.empty((G, cols), dtype=torch.float32, device="cuda"),
-               "group_rows": torch.empty(G, dtype=torch.int32, device="cuda"),
-               "status": torch.zeros(1, dtype=torch.int32, device="cuda")}
-        for i, p in enumerate(parts):
-            a, b = int(offs[i]), int(offs[i + 1])
-            runtime.compute_sparse_group_moments(p, G, d_rk[a:b], d_fk, d_lab[a:b], workspace=ws, out=out)
-            s64 += out["sum"]
-            q64 += out["sumsq"]
-        r.sum.copy_(s64.float(), non_blocking=True)
-        r.sumsq.copy_(q64.float(), non_blocking=True)
-        torch.cuda.synchronize()
-        plain_ms.append((time.perf_counter() - t0) * 1e3)
-    plain_rps = 1e3 / float(np.mean(plain_ms))
+        plain(k % n_distinct)
+        service_ms.append((time.perf_counter() - t0) * 1e3)
+    plain_lines = []
+    rng2 = np.random.default_rng(7)
+    for rate in [float(x) for x in args.rates.split(",")]:
+        n = args.requests
+        idx = rng2.integers(0, n_distinct, n)
+        arr = np.cumsum(rng2.exponential(1.0 / rate, n))
+        arr -= arr[0]
+        lat = []
+        t0 = time.perf_counter()
+        for i in range(n):
+            while time.perf_counter() - t0 < arr[i]:
+                pass
+            plain(int(idx[i]))
+            lat.append((time.perf_counter() - t0 - arr[i]) * 1e3)
+        mk = time.perf_counter() - t0
+        pl = {"workload": "serving_plain", "rate_rps": rate, "requests": n, "p50_ms": float(np.percentile(lat, 50)),
+              "p99_ms": float(np.percentile(lat, 99)), "throughput_rps": n / mk, "makespan_s": mk}
+        print(json.dumps(pl), flush=True)
+        plain_lines.append(pl)
+    clk = clocks.stop()
+    plain_rps = max(x["throughput_rps"] for x in plain_lines)
+    plain_ms = service_ms
     summary = {
         "workload": "serving", "metric": "served throughput (req/s) and p50/p99 latency vs plain per-call path",
         "value": best["throughput_rps"], "unit": "req/s", "n_gpus": 1, "higher_is_better": True,
         "served_best": best, "plain_rps": plain_rps, "plain_p50_ms": float(np.percentile(plain_ms, 50)),
         "plain_p99_ms": float(np.percentile(plain_ms, 99)), "served_over_plain": best["throughput_rps"] / plain_rps,
+        "plain_service_ms_mean": float(np.mean(plain_ms)), "plain_rates": plain_lines,
+        "plain_vs_served_max_rel": agree,
+        "plain_path": "per request: H2D of masks and labels, one cs_b200_group_moments_blocked_ell_parts call over "
+                      "the 64 partitions (indexes built once), one sync, D2H of sum and sumsq; serial",
         "data": "synthetic NB(mean 2, dispersion 0.5) counts on Zipf(1.1) genes, seeded, generated in HBM",
         "config": {"workload": "serving masked grouped moments requests over 64 resident Blocked-ELL-16 partitions",
                    "partitions": SERVE_PARTS, "rows": total_rows, "cols": cols, "density": 0.02, "nnz": nnz,

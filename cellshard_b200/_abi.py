@@ -278,6 +278,9 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_reoptimize_emit": (C.c_int, [P(BlockedEllView), P(RowFeatureMaskView), u32, u32, vp, vp, vp, vp]),
     "cs_b200_group_moments_scratch_bytes": (C.c_int, [P(BlockedEllView), P(GroupMomentsParams), P(sz)]),
     "cs_b200_group_moments_index_bytes": (C.c_int, [P(BlockedEllView), P(sz)]),
+    "cs_b200_group_moments_parts_scratch_bytes": (C.c_int, [P(BlockedEllView), u32, P(GroupMomentsParams), P(sz)]),
+    "cs_b200_group_moments_blocked_ell_parts": (C.c_int, [P(BlockedEllView), u32, P(vp), vp, vp, vp,
+                                                          P(GroupMomentsParams), P(GroupMomentsOut), vp, sz, vp]),
     "cs_b200_group_moments_build_index": (C.c_int, [P(BlockedEllView), vp, vp, vp]),
     "cs_b200_group_moments_blocked_ell": (C.c_int, [P(BlockedEllView), vp, vp, vp, P(GroupMomentsParams),
                                                     P(GroupMomentsOut), vp, sz, vp]),

@@ -281,23 +281,53 @@ __global__ void __launch_bounds__(kSortThreads) moments_tile_scatter_kernel(uint
 // ---------------------------------------------------------------------------
 // 3. Accumulation.
 // ---------------------------------------------------------------------------
-template <int L, bool COMP>
+// Where a sorted row's values and index entries live.  One partition: the
+// row id and its row block's index offset, kept in shared memory as a uint2.
+struct one_partition_rows {
+    using entry = uint2;
+    const uint16_t *__restrict__ val;
+    const uint2 *__restrict__ index;
+    const uint32_t *__restrict__ sorted_rows;
+    uint32_t ell_cols, block_size, words;
+    __device__ __forceinline__ entry fetch(uint32_t pos) const {
+        const uint32_t r = sorted_rows[pos];
+        return make_uint2(r, (r / block_size) * words);
+    }
+    __device__ __forceinline__ uint2 index_entry(const entry &e, uint32_t w) const { return __ldg(index + e.y + w); }
+    __device__ __forceinline__ const uint16_t *row(const entry &e) const {
+        return val + (std::size_t) e.x * ell_cols;
+    }
+};
+
+// Several partitions (a shard): each sorted row's value row and index row
+// addresses, precomputed by moments_row_ptrs_kernel.
+struct many_partition_rows {
+    using entry = ulonglong2;
+    const ulonglong2 *__restrict__ row_ptrs;
+    __device__ __forceinline__ entry fetch(uint32_t pos) const { return row_ptrs[pos]; }
+    __device__ __forceinline__ uint2 index_entry(const entry &e, uint32_t w) const {
+        return __ldg(reinterpret_cast<const uint2 *>(e.y) + w);
+    }
+    __device__ __forceinline__ const uint16_t *row(const entry &e) const {
+        return reinterpret_cast<const uint16_t *>(e.x);
+    }
+};
+
+template <int L, bool COMP, typename Rows>
 __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
-    const uint16_t *__restrict__ val, uint32_t ell_cols, uint32_t block_size, uint32_t col_blocks, uint32_t words,
-    uint32_t cols, const uint2 *__restrict__ index, const chunk_desc *__restrict__ chunks,
-    const uint32_t *__restrict__ num_chunks, const uint32_t *__restrict__ sorted_rows, float *__restrict__ partials,
-    const uint32_t *__restrict__ chunk_first, uint32_t g_lo, uint32_t g_hi) {
-    extern __shared__ uint2 chunk_rows_smem[]; // (row, row_block * words)
+    Rows rows_of, uint32_t block_size, uint32_t col_blocks, uint32_t cols, const chunk_desc *__restrict__ chunks,
+    const uint32_t *__restrict__ num_chunks, float *__restrict__ partials, const uint32_t *__restrict__ chunk_first,
+    uint32_t g_lo, uint32_t g_hi) {
+    using entry = typename Rows::entry;
+    extern __shared__ __align__(16) unsigned char acc_smem[];
+    entry *chunk_rows_smem = reinterpret_cast<entry *>(acc_smem);
     const uint32_t c = blockIdx.x;
     if (c >= *num_chunks) return;
     // with chunk_first: only the chunks of groups [g_lo, g_hi)
     if (chunk_first != nullptr && (c < chunk_first[g_lo] || c >= chunk_first[g_hi])) return;
     const chunk_desc d = chunks[c];
     const uint32_t n = d.end - d.begin;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint32_t r = sorted_rows[d.begin + i];
-        chunk_rows_smem[i] = make_uint2(r, (r / block_size) * words);
-    }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) chunk_rows_smem[i] = rows_of.fetch(d.begin + i);
     __syncthreads();
 
     const uint32_t segs_per_block = block_size / L;
@@ -319,7 +349,7 @@ __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
     uint2 e_next[kBatch];
 #pragma unroll
     for (unsigned u = 0; u < kBatch; ++u)
-        e_next[u] = u < n ? __ldg(index + (std::size_t) chunk_rows_smem[u].y + w) : make_uint2(0u, 0u);
+        e_next[u] = u < n ? rows_of.index_entry(chunk_rows_smem[u], w) : make_uint2(0u, 0u);
     uint32_t i = 0;
     for (; i + kBatch <= n; i += kBatch) {
         raw_vec<L> raw[kBatch];
@@ -328,8 +358,7 @@ __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
             const uint2 e = e_next[u];
             if (e.x & bitmask) {
                 const uint32_t slot = e.y + __popc(e.x & below);
-                load_raw<L>(val + (std::size_t) chunk_rows_smem[i + u].x * ell_cols + (std::size_t) slot * block_size +
-                                lane_off,
+                load_raw<L>(rows_of.row(chunk_rows_smem[i + u]) + (std::size_t) slot * block_size + lane_off,
                             raw[u]);
             } else {
                 zero_raw<L>(raw[u]);
@@ -338,7 +367,7 @@ __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
 #pragma unroll
         for (unsigned u = 0; u < kBatch; ++u) {
             const uint32_t k = i + kBatch + u;
-            e_next[u] = k < n ? __ldg(index + (std::size_t) chunk_rows_smem[k].y + w) : make_uint2(0u, 0u);
+            e_next[u] = k < n ? rows_of.index_entry(chunk_rows_smem[k], w) : make_uint2(0u, 0u);
         }
         if (COMP) {
             float bs[L], bq[L];
@@ -380,8 +409,7 @@ __global__ void __launch_bounds__(kAccThreads, 2) moments_accumulate_kernel(
             if (e.x & bitmask) {
                 raw_vec<L> raw;
                 const uint32_t slot = e.y + __popc(e.x & below);
-                load_raw<L>(val + (std::size_t) chunk_rows_smem[i + u].x * ell_cols + (std::size_t) slot * block_size +
-                                lane_off,
+                load_raw<L>(rows_of.row(chunk_rows_smem[i + u]) + (std::size_t) slot * block_size + lane_off,
                             raw);
                 float x[L];
                 unpack<L>(raw, x);
@@ -488,21 +516,28 @@ __global__ void __launch_bounds__(256) moments_combine_kernel(
     if (out_var64 != nullptr) out_var64[o] = dv;
 }
 
-template <int L, bool COMP>
-int launch_accumulate(const cs_blocked_ell_view *src, const moments_layout &lay, const uint32_t *chunk_first,
-                      uint32_t g_lo, uint32_t g_hi, cudaStream_t stream) {
-    const uint32_t segs = lay.col_blocks * (src->block_size / L);
+template <int L, bool COMP, typename Rows>
+int launch_accumulate_rows(const Rows &rows_of, uint32_t block_size, uint32_t cols, const moments_layout &lay,
+                           const uint32_t *chunk_first, uint32_t g_lo, uint32_t g_hi, cudaStream_t stream) {
+    const uint32_t segs = lay.col_blocks * (block_size / L);
     dim3 grid(lay.max_chunks, (segs + kAccThreads - 1u) / kAccThreads);
-    const std::size_t smem = (std::size_t) lay.chunk_rows * sizeof(uint2);
-    auto kern = moments_accumulate_kernel<L, COMP>;
+    const std::size_t smem = (std::size_t) lay.chunk_rows * sizeof(typename Rows::entry);
+    auto kern = moments_accumulate_kernel<L, COMP, Rows>;
     if (smem > 48u * 1024u &&
         !cuda_ok(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem),
                  "moments smem attribute"))
         return 0;
-    kern<<<grid, kAccThreads, smem, stream>>>(src->val, src->ell_cols, src->block_size, lay.col_blocks, lay.words,
-                                              src->cols, lay.index, lay.chunks, lay.num_chunks, lay.sorted_rows,
+    kern<<<grid, kAccThreads, smem, stream>>>(rows_of, block_size, lay.col_blocks, cols, lay.chunks, lay.num_chunks,
                                               lay.partials, chunk_first, g_lo, g_hi);
     return launch_ok("moments_accumulate_kernel");
+}
+
+template <int L, bool COMP>
+int launch_accumulate(const cs_blocked_ell_view *src, const moments_layout &lay, const uint32_t *chunk_first,
+                      uint32_t g_lo, uint32_t g_hi, cudaStream_t stream) {
+    const one_partition_rows rows_of{reinterpret_cast<const uint16_t *>(src->val), lay.index, lay.sorted_rows,
+                                     src->ell_cols, src->block_size, lay.words};
+    return launch_accumulate_rows<L, COMP>(rows_of, src->block_size, src->cols, lay, chunk_first, g_lo, g_hi, stream);
 }
 
 int validate(const cs_blocked_ell_view *src, const cs_group_moments_params *p) {
@@ -532,6 +567,90 @@ int validate(const cs_blocked_ell_view *src, const cs_group_moments_params *p) {
         return 0;
     }
     return 1;
+}
+
+// A shard's partitions, passed to moments_row_ptrs_kernel by value (the
+// table travels in the launch, so nothing of the host call outlives it).
+struct moment_part {
+    const uint16_t *val;
+    const uint2 *index;
+    uint32_t row0;     // first global row of the partition
+    uint32_t ell_cols;
+};
+struct moment_part_table {
+    moment_part p[CS_MOMENTS_MAX_PARTS];
+    uint32_t count, block_size, words, pad;
+};
+
+// row_ptrs[i] = (address of sorted row i's values, address of its row
+// block's index entries) for the kept rows of all groups.
+__global__ void __launch_bounds__(256) moments_row_ptrs_kernel(moment_part_table T,
+                                                              const uint32_t *__restrict__ sorted_rows,
+                                                              const uint32_t *__restrict__ group_offsets, uint32_t G,
+                                                              ulonglong2 *__restrict__ row_ptrs) {
+    __shared__ uint32_t row0[CS_MOMENTS_MAX_PARTS];
+    for (uint32_t k = threadIdx.x; k < T.count; k += blockDim.x) row0[k] = T.p[k].row0;
+    __syncthreads();
+    const uint32_t total = group_offsets[G];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const uint32_t r = sorted_rows[i];
+        uint32_t lo = 0u, hi = T.count - 1u; // last partition whose first row is <= r
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (row0[mid] <= r)
+                lo = mid;
+            else
+                hi = mid - 1u;
+        }
+        const uint32_t local = r - row0[lo];
+        const uint16_t *v = T.p[lo].val + (std::size_t) local * T.p[lo].ell_cols;
+        const uint2 *x = T.p[lo].index + (std::size_t) (local / T.block_size) * T.words;
+        row_ptrs[i] = make_ulonglong2((unsigned long long) v, (unsigned long long) x);
+    }
+}
+
+// Stable sort of the kept rows [0, rows) by label into lay.sorted_rows, with
+// each group's rows cut into chunks (prepare phase, after the index).
+int sort_rows_by_label(const moments_layout &lay, uint32_t rows, const uint8_t *d_row_keep,
+                       const uint32_t *d_row_labels, uint32_t G, cudaStream_t stream) {
+    const std::size_t sort_smem = (std::size_t) kSortWarps * G * sizeof(uint32_t);
+    if (lay.tiles != 0u) {
+        const std::size_t hist_smem = (std::size_t) G * sizeof(uint32_t);
+        moments_tile_hist_kernel<<<lay.tiles, kSortThreads, hist_smem, stream>>>(rows, d_row_keep, d_row_labels, G,
+                                                                                lay.tile_counts);
+        if (!launch_ok("moments_tile_hist_kernel")) return 0;
+        moments_group_tiles_kernel<<<(G + 7u) / 8u, 256, 0, stream>>>(lay.tiles, G, lay.tile_counts, lay.group_rows);
+        if (!launch_ok("moments_group_tiles_kernel")) return 0;
+    } else if (!cuda_ok(cudaMemsetAsync(lay.group_rows, 0, (std::size_t) G * sizeof(uint32_t), stream),
+                        "group rows memset")) {
+        return 0;
+    }
+    moments_group_scan_kernel<<<1, 1024, 0, stream>>>(G, lay.chunk_rows, lay.max_chunks, lay.group_rows,
+                                                      lay.group_offsets, lay.chunk_first, lay.num_chunks, lay.chunks);
+    if (!launch_ok("moments_group_scan_kernel")) return 0;
+    if (lay.tiles != 0u) {
+        if (sort_smem > 48u * 1024u &&
+            !cuda_ok(cudaFuncSetAttribute(moments_tile_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) sort_smem),
+                     "scatter smem attribute"))
+            return 0;
+        moments_tile_scatter_kernel<<<lay.tiles, kSortThreads, sort_smem, stream>>>(
+            rows, d_row_keep, d_row_labels, G, lay.tile_counts, lay.group_offsets, lay.sorted_rows);
+        if (!launch_ok("moments_tile_scatter_kernel")) return 0;
+    }
+    return 1;
+}
+
+// Combine phase for groups [g_lo, g_hi).
+int combine_groups(const moments_layout &lay, uint32_t cols, const cs_group_moments_params *params,
+                   const uint8_t *d_feature_keep, const cs_group_moments_out *out, uint32_t g_lo, uint32_t g_hi,
+                   cudaStream_t stream) {
+    dim3 grid((cols + 255u) / 256u == 0u ? 1u : (cols + 255u) / 256u, g_hi - g_lo);
+    moments_combine_kernel<<<grid, 256, 0, stream>>>(cols, params->group_count, params->scheme, params->ddof,
+                                                     lay.chunk_first, lay.group_rows, lay.partials, d_feature_keep,
+                                                     out->sum, out->sumsq, out->mean, out->var, out->mean64,
+                                                     out->var64, out->group_rows, g_lo);
+    return launch_ok("moments_combine_kernel");
 }
 
 } // namespace
@@ -601,35 +720,8 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
         }
     }
 
-    const std::size_t sort_smem = (std::size_t) kSortWarps * G * sizeof(uint32_t);
-    if (phases & CS_MOMENTS_PHASE_PREPARE) {
-    if (lay.tiles != 0u) {
-        const std::size_t hist_smem = (std::size_t) G * sizeof(uint32_t);
-        moments_tile_hist_kernel<<<lay.tiles, kSortThreads, hist_smem, stream>>>(src->rows, d_row_keep, d_row_labels,
-                                                                                G, lay.tile_counts);
-        if (!launch_ok("moments_tile_hist_kernel")) return 0;
-    }
-    if (lay.tiles != 0u) {
-        moments_group_tiles_kernel<<<(G + 7u) / 8u, 256, 0, stream>>>(lay.tiles, G, lay.tile_counts, lay.group_rows);
-        if (!launch_ok("moments_group_tiles_kernel")) return 0;
-    } else if (!cuda_ok(cudaMemsetAsync(lay.group_rows, 0, (std::size_t) G * sizeof(uint32_t), stream),
-                        "group rows memset")) {
+    if ((phases & CS_MOMENTS_PHASE_PREPARE) && !sort_rows_by_label(lay, src->rows, d_row_keep, d_row_labels, G, stream))
         return 0;
-    }
-    moments_group_scan_kernel<<<1, 1024, 0, stream>>>(G, lay.chunk_rows, lay.max_chunks, lay.group_rows,
-                                                      lay.group_offsets, lay.chunk_first, lay.num_chunks, lay.chunks);
-    if (!launch_ok("moments_group_scan_kernel")) return 0;
-    if (lay.tiles != 0u) {
-        if (sort_smem > 48u * 1024u &&
-            !cuda_ok(cudaFuncSetAttribute(moments_tile_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int) sort_smem),
-                     "scatter smem attribute"))
-            return 0;
-        moments_tile_scatter_kernel<<<lay.tiles, kSortThreads, sort_smem, stream>>>(
-            src->rows, d_row_keep, d_row_labels, G, lay.tile_counts, lay.group_offsets, lay.sorted_rows);
-        if (!launch_ok("moments_tile_scatter_kernel")) return 0;
-    }
-    }
 
     if ((phases & CS_MOMENTS_PHASE_ACCUMULATE) && lay.col_blocks != 0u && lay.max_chunks != 0u && src->cols != 0u) {
         const bool comp = params->scheme != CS_MOMENTS_PLAIN_F32;
@@ -651,14 +743,9 @@ static int moments_run(const cs_blocked_ell_view *src, const uint8_t *d_row_keep
         if (!ok) return 0;
     }
 
-    if ((phases & CS_MOMENTS_PHASE_COMBINE) && (src->cols != 0u || out->group_rows != nullptr)) {
-        dim3 grid((src->cols + 255u) / 256u == 0u ? 1u : (src->cols + 255u) / 256u, g_hi - g_lo);
-        moments_combine_kernel<<<grid, 256, 0, stream>>>(src->cols, G, params->scheme, params->ddof, lay.chunk_first,
-                                                         lay.group_rows, lay.partials, d_feature_keep, out->sum,
-                                                         out->sumsq, out->mean, out->var, out->mean64, out->var64,
-                                                         out->group_rows, g_lo);
-        if (!launch_ok("moments_combine_kernel")) return 0;
-    }
+    if ((phases & CS_MOMENTS_PHASE_COMBINE) && (src->cols != 0u || out->group_rows != nullptr) &&
+        !combine_groups(lay, src->cols, params, d_feature_keep, out, g_lo, g_hi, stream))
+        return 0;
     return 1;
 }
 
@@ -760,6 +847,155 @@ extern "C" int cs_b200_group_moments_phases(const cs_blocked_ell_view *src, cons
     }
     return moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, out, d_scratch, scratch_bytes, s,
                        phases);
+}
+
+// ---------------------------------------------------------------------------
+// The reduction over a shard given as its partitions' views, in one call.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct parts_layout {
+    moments_layout base;    // over all rows of the shard
+    uint2 *part_index;      // per-partition column-block indexes built by the call
+    ulonglong2 *row_ptrs;   // [rows]
+    std::size_t bytes;
+    uint32_t rows;
+};
+
+int validate_parts(const cs_blocked_ell_view *parts, uint32_t count, const cs_group_moments_params *params,
+                   cs_blocked_ell_view *whole) {
+    if (parts == nullptr || count == 0u || count > CS_MOMENTS_MAX_PARTS) {
+        set_error("group_moments_parts: %u partitions (need 1..%u)", count, CS_MOMENTS_MAX_PARTS);
+        return 0;
+    }
+    uint64_t rows = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (!validate(&parts[k], params)) return 0;
+        if (parts[k].cols != parts[0].cols || parts[k].block_size != parts[0].block_size) {
+            set_error("group_moments_parts: partition %u has cols %u / block size %u, partition 0 %u / %u", k,
+                      parts[k].cols, parts[k].block_size, parts[0].cols, parts[0].block_size);
+            return 0;
+        }
+        if (parts[k].rows != 0u && parts[k].ell_cols != 0u &&
+            (parts[k].val == nullptr || parts[k].blockColIdx == nullptr)) {
+            set_error("group_moments_parts: partition %u has null arrays", k);
+            return 0;
+        }
+        rows += parts[k].rows;
+    }
+    if (rows >= 0xffffffffull) {
+        set_error("group_moments_parts: %llu rows exceed the u32 row ids", (unsigned long long) rows);
+        return 0;
+    }
+    *whole = parts[0];
+    whole->rows = (uint32_t) rows;
+    return 1;
+}
+
+bool make_parts_layout(const cs_blocked_ell_view *parts, uint32_t count, const cs_blocked_ell_view &whole,
+                       const cs_group_moments_params *params, void *base, std::size_t cap, parts_layout *pl) {
+    make_layout(&whole, params, base, cap, &pl->base);
+    const uint32_t B = whole.block_size;
+    std::size_t blocks = 0;
+    for (uint32_t k = 0; k < count; ++k) blocks += (parts[k].rows + B - 1u) / B;
+    scratch_carver c(base, cap);
+    c.used = pl->base.bytes;
+    pl->part_index = c.take<uint2>(blocks * pl->base.words + 1u);
+    pl->row_ptrs = c.take<ulonglong2>((std::size_t) whole.rows + 1u);
+    pl->bytes = c.used;
+    pl->rows = whole.rows;
+    return c.fits();
+}
+
+} // namespace
+
+extern "C" int cs_b200_group_moments_parts_scratch_bytes(const cs_blocked_ell_view *parts, uint32_t count,
+                                                          const cs_group_moments_params *params, size_t *out_bytes) {
+    cs_blocked_ell_view whole;
+    if (out_bytes == nullptr) {
+        set_error("group_moments_parts_scratch_bytes: null output");
+        return 0;
+    }
+    if (!validate_parts(parts, count, params, &whole)) return 0;
+    parts_layout pl;
+    make_parts_layout(parts, count, whole, params, nullptr, 0, &pl);
+    *out_bytes = pl.bytes;
+    return 1;
+}
+
+extern "C" int cs_b200_group_moments_blocked_ell_parts(const cs_blocked_ell_view *parts, uint32_t count,
+                                                       const void *const *d_indexes, const uint8_t *d_row_keep,
+                                                       const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
+                                                       const cs_group_moments_params *params,
+                                                       const cs_group_moments_out *out, void *d_scratch,
+                                                       size_t scratch_bytes, cs_stream_t s) {
+    cs_blocked_ell_view whole;
+    if (!validate_parts(parts, count, params, &whole)) return 0;
+    if (out == nullptr || out->sum == nullptr || out->sumsq == nullptr) {
+        set_error("group_moments_parts: sum and sumsq outputs are required");
+        return 0;
+    }
+    parts_layout pl;
+    if (!make_parts_layout(parts, count, whole, params, d_scratch, scratch_bytes, &pl) || d_scratch == nullptr) {
+        set_error("group_moments_parts: scratch too small (%zu bytes, need %zu)", scratch_bytes, pl.bytes);
+        return 0;
+    }
+    cudaStream_t stream = as_stream(s);
+    const moments_layout &lay = pl.base;
+    const uint32_t G = params->group_count, B = whole.block_size;
+    moment_part_table T{};
+    T.count = count;
+    T.block_size = B;
+    T.words = lay.words;
+    uint32_t row0 = 0u;
+    std::size_t built = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint2 *idx = d_indexes != nullptr ? static_cast<const uint2 *>(d_indexes[k]) : nullptr;
+        if (idx == nullptr) {
+            uint2 *mine = pl.part_index + built * lay.words;
+            built += (parts[k].rows + B - 1u) / B;
+            if (!build_column_block_index(&parts[k], mine, out->status, stream)) return 0;
+            idx = mine;
+        }
+        T.p[k] = moment_part{reinterpret_cast<const uint16_t *>(parts[k].val), idx, row0, parts[k].ell_cols};
+        row0 += parts[k].rows;
+    }
+    if (!sort_rows_by_label(lay, whole.rows, d_row_keep, d_row_labels, G, stream)) return 0;
+    if (whole.rows != 0u) {
+        const unsigned grid = resident_grid(reinterpret_cast<const void *>(moments_row_ptrs_kernel), 256, 0,
+                                            (whole.rows + 255u) / 256u);
+        moments_row_ptrs_kernel<<<grid, 256, 0, stream>>>(T, lay.sorted_rows, lay.group_offsets, G, pl.row_ptrs);
+        if (!launch_ok("moments_row_ptrs_kernel")) return 0;
+    }
+    if (lay.col_blocks != 0u && lay.max_chunks != 0u && whole.cols != 0u) {
+        const bool comp = params->scheme != CS_MOMENTS_PLAIN_F32;
+        bool a16 = true, a8 = true, a4 = true;
+        for (uint32_t k = 0; k < count; ++k) {
+            const uintptr_t v = reinterpret_cast<uintptr_t>(parts[k].val);
+            const uint32_t rowb = parts[k].ell_cols * 2u; // a row's bytes: every row start keeps the base alignment
+            a16 = a16 && (v & 15u) == 0u && rowb % 16u == 0u;
+            a8 = a8 && (v & 7u) == 0u && rowb % 8u == 0u;
+            a4 = a4 && (v & 3u) == 0u && rowb % 4u == 0u;
+        }
+        const many_partition_rows rows_of{pl.row_ptrs};
+        int ok;
+#define CS_ACCM(L_)                                                                                       \
+    (comp ? launch_accumulate_rows<L_, true>(rows_of, B, whole.cols, lay, nullptr, 0u, G, stream)         \
+          : launch_accumulate_rows<L_, false>(rows_of, B, whole.cols, lay, nullptr, 0u, G, stream))
+        if (B % 8u == 0u && a16)
+            ok = CS_ACCM(8);
+        else if (B % 4u == 0u && a8)
+            ok = CS_ACCM(4);
+        else if (B % 2u == 0u && a4)
+            ok = CS_ACCM(2);
+        else
+            ok = CS_ACCM(1);
+#undef CS_ACCM
+        if (!ok) return 0;
+    }
+    if (whole.cols != 0u || out->group_rows != nullptr)
+        return combine_groups(lay, whole.cols, params, d_feature_keep, out, 0u, G, stream);
+    return 1;
 }
 
 namespace {

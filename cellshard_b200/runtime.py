@@ -255,6 +255,53 @@ def compute_sparse_group_moments(src: BlockedELL, group_count: int, row_keep=Non
     return out
 
 
+def group_moments_parts_scratch_bytes(parts, group_count: int, scheme: int = TWOSUM_F64_COMBINE, ddof: int = 1,
+                                      chunk_rows: int = 0) -> int:
+    lib = _abi.load()
+    p = _abi.GroupMomentsParams(group_count, scheme, ddof, chunk_rows)
+    views = (_abi.BlockedEllView * len(parts))(*[q.view() for q in parts])
+    n = C.c_size_t()
+    _abi.check(lib.cs_b200_group_moments_parts_scratch_bytes(views, len(parts), C.byref(p), C.byref(n)),
+               "moments parts scratch")
+    return n.value
+
+
+def compute_sparse_group_moments_parts(parts, group_count: int, row_keep=None, feature_keep=None, row_labels=None,
+                                       scheme: int = TWOSUM_F64_COMBINE, ddof: int = 1, chunk_rows: int = 0,
+                                       indexes=None, workspace: MomentsWorkspace | None = None, out=None,
+                                       want_f64: bool = False, stream=None):
+    """The moments reduction over a shard given as its Blocked-ELL partitions, in one call
+    (cs_b200_group_moments_blocked_ell_parts).  ``row_keep`` / ``row_labels`` cover the rows of
+    all partitions in order; ``indexes``: each partition's column-block index from
+    build_moments_index (None, or a None entry, = built by the call)."""
+    lib = _abi.load()
+    G, cols = group_count, parts[0].cols
+    p = _abi.GroupMomentsParams(G, scheme, ddof, chunk_rows)
+    views = (_abi.BlockedEllView * len(parts))(*[q.view() for q in parts])
+    n = C.c_size_t()
+    _abi.check(lib.cs_b200_group_moments_parts_scratch_bytes(views, len(parts), C.byref(p), C.byref(n)),
+               "moments parts scratch")
+    ws = workspace or MomentsWorkspace()
+    scratch = ws.reserve(n.value)
+    if out is None:
+        out = {k: torch.empty((G, cols), dtype=torch.float32, device="cuda") for k in ("sum", "sumsq", "mean", "var")}
+        out["group_rows"] = torch.empty(G, dtype=torch.int32, device="cuda")
+        out["status"] = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if want_f64:
+            out["mean64"] = torch.empty((G, cols), dtype=torch.float64, device="cuda")
+            out["var64"] = torch.empty((G, cols), dtype=torch.float64, device="cuda")
+    keys = ("sum", "sumsq", "mean", "var", "mean64", "var64", "group_rows", "status")
+    o = _abi.GroupMomentsOut(*[ptr(out.get(k)) for k in keys])
+    idx = None
+    if indexes is not None:
+        idx = (C.c_void_p * len(parts))(*[ptr(x) for x in indexes])
+    _abi.check(lib.cs_b200_group_moments_blocked_ell_parts(views, len(parts), idx, ptr(row_keep), ptr(feature_keep),
+                                                           ptr(row_labels), C.byref(p), C.byref(o), ptr(scratch),
+                                                           scratch.numel(), stream_handle(stream)),
+               "group_moments_blocked_ell_parts")
+    return out
+
+
 def compute_sparse_group_moments_to_host(src: BlockedELL, group_count: int, host_out: dict, row_keep=None,
                                          feature_keep=None, row_labels=None, scheme: int = TWOSUM_F64_COMBINE,
                                          ddof: int = 1, chunk_rows: int = 0, parts: int = 0,

@@ -853,6 +853,26 @@ CS_API int cs_b200_group_moments_scratch_bytes(const cs_blocked_ell_view *src,
  * and 32 column blocks.  The build validates blockColIdx order into *d_status
  * (CS_STATUS_BLOCK_COL_ORDER; nullable) and is stream-ordered. */
 CS_API int cs_b200_group_moments_index_bytes(const cs_blocked_ell_view *src, size_t *out_bytes);
+
+/* No counterpart in the reference: the same reduction over a whole shard
+ * given as its partitions' views, in one call (one label sort, one
+ * accumulation launch over every partition's rows, one combine).  Rows are
+ * numbered across the partitions in order (row r of partition k is global row
+ * rows_0 + ... + rows_{k-1} + r), so d_row_keep and d_row_labels cover all
+ * of them.  The partitions share cols and block_size; at most
+ * CS_MOMENTS_MAX_PARTS.  d_indexes: nullable host array of each partition's
+ * column-block index (cs_b200_group_moments_build_index); a NULL array or
+ * entry is built in scratch by the call.  params->index is not used.
+ * Stream-ordered, no synchronisation. */
+#define CS_MOMENTS_MAX_PARTS 64u
+CS_API int cs_b200_group_moments_parts_scratch_bytes(const cs_blocked_ell_view *parts, uint32_t count,
+                                                     const cs_group_moments_params *params, size_t *out_bytes);
+CS_API int cs_b200_group_moments_blocked_ell_parts(const cs_blocked_ell_view *parts, uint32_t count,
+                                                   const void *const *d_indexes, const uint8_t *d_row_keep,
+                                                   const uint8_t *d_feature_keep, const uint32_t *d_row_labels,
+                                                   const cs_group_moments_params *params,
+                                                   const cs_group_moments_out *out, void *d_scratch,
+                                                   size_t scratch_bytes, cs_stream_t stream);
 CS_API int cs_b200_group_moments_build_index(const cs_blocked_ell_view *src, void *d_index, uint32_t *d_status,
                                              cs_stream_t stream);
 

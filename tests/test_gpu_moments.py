@@ -260,3 +260,62 @@ def test_moments_prebuilt_index_matches(cuda, orc):
         bci, val = _host(bell)
         ref = orc.group_moments_bell(rows, cols, 16, bell.ell_cols, bci, val, rk, fk, lab, G, ddof=1)
         _check(b, ref, G, cols)
+
+
+@pytest.mark.parametrize("prebuilt", [False, True])
+def test_moments_over_shard_partitions(cuda, orc, prebuilt):
+    """One call over a shard of uneven partitions (rows not multiples of the block size,
+    different ell_cols): the FP64 oracle over the partitions stacked row-wise; prebuilt
+    per-partition indexes give the same bits as indexes built by the call."""
+    import torch
+
+    from cellshard_b200 import runtime
+
+    cols, G, B = 203, 6, 16
+    rows = [301, 64, 17, 540]
+    parts = [_bell(cuda, r, cols, B, 0.03 + 0.02 * k, seed=50 + k, integer=(k % 2 == 0)) for k, r in enumerate(rows)]
+    R = sum(rows)
+    rk, fk, lab = _masks(R, cols, G, 9)
+    idx = [runtime.build_moments_index(q) for q in parts] if prebuilt else None
+    res = runtime.compute_sparse_group_moments_parts(parts, G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=64,
+                                                     indexes=idx)
+    # the oracle over the stacked partitions: FP64 sums per partition, added
+    s = np.zeros((G, cols))
+    q = np.zeros((G, cols))
+    n = np.zeros(G, np.int64)
+    r0 = 0
+    for part, r in zip(parts, rows):
+        bci, val = _host(part)
+        o = orc.group_moments_bell(r, cols, B, part.ell_cols, bci, val, rk[r0:r0 + r], None, lab[r0:r0 + r], G)
+        s += o["sum"]
+        q += o["sumsq"]
+        n += o["group_rows"].astype(np.int64)
+        r0 += r
+    keep = fk.astype(bool)
+    s[:, ~keep] = 0.0
+    q[:, ~keep] = 0.0
+    nn = n[:, None].astype(np.float64)
+    mean = np.where(nn > 0, s / np.maximum(nn, 1), 0.0)
+    var = np.where(nn > 1, np.maximum(q - s * mean, 0.0) / np.maximum(nn - 1, 1), 0.0)
+    mean[:, ~keep] = 0.0
+    var[:, ~keep] = 0.0
+    ref = {"sum": s, "sumsq": q, "mean": mean, "var": var, "group_rows": n.astype(np.uint32)}
+    _check(res, ref, G, cols)
+    again = runtime.compute_sparse_group_moments_parts(parts, G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=64,
+                                                       indexes=[runtime.build_moments_index(q_) for q_ in parts])
+    torch.cuda.synchronize()
+    for k in ("sum", "sumsq", "mean", "var"):
+        assert np.array_equal(res[k].cpu().numpy().view(np.uint32), again[k].cpu().numpy().view(np.uint32)), k
+
+
+def test_moments_one_partition_shard_matches_single_call(cuda):
+    """A shard of one partition is the single-partition reduction, bit for bit."""
+    from cellshard_b200 import runtime
+
+    rows, cols, G = 1000, 150, 5
+    bell = _bell(cuda, rows, cols, 16, 0.05, seed=77, integer=False)
+    rk, fk, lab = _masks(rows, cols, G, 4)
+    a = runtime.compute_sparse_group_moments(bell, G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=128)
+    b = runtime.compute_sparse_group_moments_parts([bell], G, _dev(rk), _dev(fk), _dev(lab), chunk_rows=128)
+    for k in ("sum", "sumsq", "mean", "var", "group_rows"):
+        assert np.array_equal(a[k].cpu().numpy().view(np.uint32), b[k].cpu().numpy().view(np.uint32)), k
