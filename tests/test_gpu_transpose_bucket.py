@@ -209,3 +209,21 @@ def test_plan_vs_reference_cub_and_reference_rebuild_shift(cuda, orc):
     shifted = np.concatenate([[0, 0], np.cumsum(counts)[:-1]]).astype(np.uint32)
     assert np.array_equal(np_u32(rptr), shifted)
     assert np.array_equal(np_u32(rinv), np.argsort(np_u32(ref["order"])).astype(np.uint32))
+
+
+@pytest.mark.parametrize("rows,cols,density,seed", [
+    (600, 64, 0.9, 31),     # a tile's panel overflows the shared-memory stage: direct stores
+    (1000, 5000, 0.5, 32),  # many rows with more than 32 entries in one panel
+    (4097, 257, 0.08, 33),  # ragged last tile and panel
+    (70000, 300, 0.02, 34), # many tiles
+])
+def test_transpose_panel_path_edges(cuda, orc, rows, cols, density, seed):
+    """The panel transpose (sorted rows) on its edge cases, bit-exact vs the restatement."""
+    from cellshard_b200.device import transpose
+
+    ptr, idx, val = random_csr(rows, cols, density, seed, 0.1, integer=False)
+    t = transpose(to_device_csr(rows, cols, ptr, idx, val))
+    rptr, ridx, rval = orc.csr_transpose(rows, cols, ptr, idx, val)
+    assert np.array_equal(np_u32(t.ptr), rptr)
+    assert np.array_equal(np_u32(t.idx), ridx)
+    assert np.array_equal(np_u16(t.val), rval)
