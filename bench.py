@@ -825,11 +825,16 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     fk = torch.from_numpy((g.random(Cc) < 0.6).astype(np.uint8)).cuda()
     filt_csr, fstats = runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk)
     del filt_csr
-    ms_f = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk))
-    emit("filter_blocked_ell_to_compressed", ms_f,
-         2 * int(rk_h.sum()) * bell.ell_cols + rb * width * 4 + R + Cc + 4 * (R + 1) + 6 * fstats["live_nnz"],
-         {"live_nnz": fstats["live_nnz"], "note": "count + emit with one host read of the live nnz; bytes are the "
-                                                  "kept rows' values, tables, row pointers and the CSR written"})
+    filt_bytes = 2 * int(rk_h.sum()) * bell.ell_cols + rb * width * 4 + R + Cc + 4 * (R + 1) + 6 * fstats["live_nnz"]
+    ms_f = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk, method="onepass"))
+    emit("filter_blocked_ell_to_compressed", ms_f, filt_bytes,
+         {"live_nnz": fstats["live_nnz"], "note": "one pass: count, look-back over rows, emit from L2, then one host "
+                                                  "read of the live nnz; bytes are the kept rows' values, tables, row "
+                                                  "pointers and the CSR written"})
+    ms_f2 = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk, method="two_pass"))
+    emit("filter_blocked_ell_count_emit", ms_f2, filt_bytes,
+         {"live_nnz": fstats["live_nnz"], "note": "the count + emit route (remaps, other block sizes): both passes "
+                                                  "read the kept rows' values"})
     ms_rp2 = timed(lambda: runtime.build_repacked_blocked_ell([bell], R, Cc, BLOCK, 64, rk, fk))
     emit("repack_blocked_ell", ms_rp2, 0, {"note": "filter + nnz plan + rebuild + CSR -> Blocked-ELL-16 with host "
                                                    "reads of sizes between stages; time only"})

@@ -1020,6 +1020,156 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
     }
 }
 
+// ---------------------------------------------------------------------------
+// One-pass filter: count, decoupled look-back over rows, emit while the row's
+// values are still in L2.  Rows are claimed in order from a global counter by
+// resident warps, so every row a warp waits for is held by a running warp.
+// row_state[r]: (flag << 32) | value, flag 1 = the row's count, 2 = the
+// inclusive prefix through the row.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kLbCount = 1ull << 32, kLbPrefix = 2ull << 32;
+constexpr uint32_t kLbSpinLimit = 1u << 22; // ~0.3 s of 64 ns sleeps
+
+__device__ __forceinline__ unsigned long long lb_load(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void lb_store(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Kept entries among the 8 values of one vector (no feature remap).
+__device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, uint32_t gene0, uint32_t cols,
+                                                 uint32_t output_cols, const uint32_t *kbits) {
+    uint32_t live = live_bits8(v) & in_range8(bc, gene0, cols);
+    if (kbits != nullptr && live != 0u) live &= kbits[gene0 >> 5] >> (gene0 & 31u);
+    return live & in_range8(bc, gene0, output_cols);
+}
+
+__global__ void __launch_bounds__(kRowThreads) filter_onepass_kernel(
+    const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
+    uint32_t *__restrict__ major_ptr, uint32_t *__restrict__ minor_idx, uint16_t *__restrict__ out_val,
+    unsigned long long capacity, unsigned long long *__restrict__ row_state, uint32_t *__restrict__ row_counter,
+    uint32_t *status, unsigned long long *__restrict__ kept, uint32_t keep_words) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t rows = parts.row_off[parts.count];
+    extern __shared__ uint32_t onepass_keep_bits[];
+    const uint32_t *kbits = keep_words != 0u ? onepass_keep_bits : nullptr;
+    uint32_t kcols = 0u;
+    for (uint32_t k = 0; k < parts.count; ++k) kcols = max(kcols, parts.v[k].cols);
+    for (uint32_t w = threadIdx.x; w < keep_words; w += blockDim.x) {
+        uint32_t word = 0u;
+        const uint32_t c0 = w * 32u;
+#pragma unroll 4
+        for (uint32_t k = 0; k < 32u; ++k)
+            if (c0 + k < kcols) word |= (masks.feature_keep[c0 + k] != 0u ? 1u : 0u) << k;
+        onepass_keep_bits[w] = word;
+    }
+    if (keep_words != 0u) __syncthreads();
+    uint32_t warp_kept_rows = 0u;
+    unsigned long long warp_kept_slots = 0u;
+    bool gave_up = false;
+    for (;;) {
+        uint32_t row = 0u;
+        if (lane == 0u) row = atomicAdd(row_counter, 1u);
+        row = __shfl_sync(0xffffffffu, row, 0);
+        if (row >= rows) break;
+        const bool kept_row = masks.row_keep == nullptr || masks.row_keep[row] != 0u;
+        const uint32_t part = part_of_row(parts, row);
+        const cs_blocked_ell_view &src = parts.v[part];
+        const uint32_t local = row - parts.row_off[part];
+        const uint32_t B = src.block_size, W = src.ell_cols / B;
+        const block_div bd(B);
+        const uint32_t *bci = src.blockColIdx + (std::size_t) (local / B) * W;
+        const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
+        constexpr unsigned kRs = 4;
+        // count
+        uint32_t lane_count = 0u;
+        if (kept_row) {
+            warp_kept_rows += 1u;
+            warp_kept_slots += src.ell_cols;
+            for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
+                uint4 v[kRs];
+                uint32_t bcs[kRs];
+                load_steps(vrow, bci, bd, src.ell_cols, b0, v, bcs);
+#pragma unroll
+                for (unsigned u = 0; u < kRs; ++u)
+                    lane_count += __popc(onepass_keep(v[u], bcs[u], bcs[u] * B + bd.mod(b0 + u * 256u), src.cols,
+                                                      output_cols, kbits));
+            }
+        }
+        const uint32_t count = __reduce_add_sync(0xffffffffu, lane_count);
+        // publish the count, then the prefix once the rows before it are known
+        uint32_t excl = 0u;
+        if (lane == 0u) {
+            lb_store(row_state + row, kLbCount | count);
+            uint32_t j = row;
+            while (j > 0u && !gave_up) {
+                --j;
+                unsigned long long st = lb_load(row_state + j);
+                for (uint32_t spins = 0; (st >> 32) == 0ull; st = lb_load(row_state + j)) {
+                    if (++spins > kLbSpinLimit) {
+                        gave_up = true;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                if (gave_up) break;
+                excl += (uint32_t) st;
+                if ((st & ~0xffffffffull) == kLbPrefix) break;
+            }
+            if (!gave_up) {
+                lb_store(row_state + row, kLbPrefix | (excl + count));
+                major_ptr[row] = excl;
+            }
+        }
+        gave_up = __shfl_sync(0xffffffffu, gave_up ? 1u : 0u, 0) != 0u;
+        if (gave_up) break;
+        excl = __shfl_sync(0xffffffffu, excl, 0);
+        if (count == 0u) continue;
+        if ((unsigned long long) excl + count > capacity) {
+            if (lane == 0u) status_or(status, CS_STATUS_CAPACITY);
+            continue;
+        }
+        // emit, re-reading the row (now in L2) in slot order
+        uint32_t run = excl;
+        for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
+            uint4 v[kRs];
+            uint32_t bcs[kRs];
+            load_steps(vrow, bci, bd, src.ell_cols, b0, v, bcs);
+#pragma unroll
+            for (unsigned u = 0; u < kRs; ++u) {
+                const uint32_t gene0 = bcs[u] * B + bd.mod(b0 + u * 256u);
+                const uint32_t keep = onepass_keep(v[u], bcs[u], gene0, src.cols, output_cols, kbits);
+                const uint32_t cnt = __popc(keep);
+                const uint32_t incl = warp_inclusive_scan(cnt);
+                uint32_t pos = run + incl - cnt;
+                for (uint32_t bb = keep; bb != 0u; bb &= bb - 1u, ++pos) {
+                    const uint32_t q = __ffs(bb) - 1u;
+                    minor_idx[pos] = gene0 + q;
+                    out_val[pos] = half_of(v[u], q);
+                }
+                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+    }
+    if (gave_up && lane == 0u) status_or(status, CS_STATUS_WAIT_LIMIT);
+    if (kept != nullptr && lane == 0u && warp_kept_rows != 0u) {
+        atomicAdd(kept, (unsigned long long) warp_kept_rows);
+        atomicAdd(kept + 1, warp_kept_slots);
+    }
+}
+
+// major_ptr[r] for r in [rows, output_rows]: the total (the last row's prefix).
+__global__ void filter_onepass_tail_kernel(const unsigned long long *__restrict__ row_state, uint32_t rows,
+                                           uint32_t output_rows, uint32_t *__restrict__ major_ptr) {
+    const uint32_t total = rows != 0u ? (uint32_t) row_state[rows - 1u] : 0u;
+    for (uint32_t r = rows + blockIdx.x * blockDim.x + threadIdx.x; r <= output_rows; r += gridDim.x * blockDim.x)
+        major_ptr[r] = total;
+}
+
 // Group accumulator registers a call needs: none, 8, 16 or 32.
 unsigned group_regs(const uint32_t *masks, uint32_t group_count) {
     if (masks == nullptr || group_count == 0u) return 0u;
@@ -1318,4 +1468,78 @@ extern "C" int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts,
     reopt_parts p;
     if (!make_parts(parts, part_count, &p, "filter_blocked_ell_emit")) return 0;
     return reopt_emit_launch(p, masks, output_rows, output_cols, d_major_ptr, d_minor_idx, d_val, as_stream(s));
+}
+
+extern "C" int cs_b200_filter_blocked_ell_onepass_scratch_bytes(uint32_t shard_rows, size_t *out_bytes) {
+    if (out_bytes == nullptr) {
+        set_error("filter_blocked_ell_onepass_scratch_bytes: null output");
+        return 0;
+    }
+    *out_bytes = align_up(((std::size_t) shard_rows + 1u) * 8u + 16u, 256);
+    return 1;
+}
+
+extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *parts, uint32_t part_count,
+                                                  const cs_row_feature_mask_view *masks, uint32_t output_rows,
+                                                  uint32_t output_cols, uint32_t *d_major_ptr, uint32_t *d_minor_idx,
+                                                  uint16_t *d_val, uint64_t capacity, uint64_t *d_kept,
+                                                  void *d_scratch, size_t scratch_bytes, uint32_t *d_status,
+                                                  cs_stream_t s) {
+    static const char *who = "filter_blocked_ell_onepass";
+    if (d_major_ptr == nullptr || (capacity != 0u && (d_minor_idx == nullptr || d_val == nullptr))) {
+        set_error("%s: null output array", who);
+        return 0;
+    }
+    reopt_parts p;
+    if (!make_parts(parts, part_count, &p, who)) return 0;
+    const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
+    const uint32_t rows = p.row_off[p.count];
+    if (m.row_remap != nullptr || m.feature_remap != nullptr) {
+        set_error("%s: row or feature remaps need the count + emit path", who);
+        return 0;
+    }
+    if (output_rows < rows) {
+        set_error("%s: output_rows %u below the shard's %u rows", who, output_rows, rows);
+        return 0;
+    }
+    for (uint32_t k = 0; k < p.count; ++k) {
+        const cs_blocked_ell_view &v = p.v[k];
+        if (v.rows == 0u || v.ell_cols == 0u) continue;
+        if (v.block_size % 8u != 0u || (reinterpret_cast<uintptr_t>(v.val) & 15u) != 0u || v.val == nullptr ||
+            v.blockColIdx == nullptr) {
+            set_error("%s: partition %u needs a block size that is a multiple of 8 and 16-byte aligned values", who,
+                      k);
+            return 0;
+        }
+    }
+    const uint32_t kw = keep_bitmap_words(p, m);
+    if (m.feature_keep != nullptr && kw == 0u) {
+        set_error("%s: too many columns for the shared feature bitmap", who);
+        return 0;
+    }
+    size_t need = 0;
+    cs_b200_filter_blocked_ell_onepass_scratch_bytes(rows, &need);
+    if (d_scratch == nullptr || scratch_bytes < need) {
+        set_error("%s: scratch %zu < %zu", who, scratch_bytes, need);
+        return 0;
+    }
+    cudaStream_t stream = as_stream(s);
+    auto *state = static_cast<unsigned long long *>(d_scratch);
+    auto *counter = reinterpret_cast<uint32_t *>(state + rows + 1u);
+    if (!cuda_ok(cudaMemsetAsync(d_scratch, 0, need, stream), "onepass scratch memset") ||
+        (d_kept != nullptr && !cuda_ok(cudaMemsetAsync(d_kept, 0, 16, stream), "memset kept")))
+        return 0;
+    if (rows != 0u) {
+        const auto k = filter_onepass_kernel;
+        const unsigned grid =
+            resident_grid(reinterpret_cast<const void *>(k), kRowThreads, kw * 4u, (rows + kRowWarps - 1u) / kRowWarps);
+        k<<<grid, kRowThreads, kw * 4u, stream>>>(p, m, output_cols, d_major_ptr, d_minor_idx, d_val, capacity, state,
+                                                  counter, d_status, reinterpret_cast<unsigned long long *>(d_kept),
+                                                  kw);
+        if (!launch_ok("filter_onepass_kernel")) return 0;
+    }
+    const uint32_t tail = output_rows - rows + 1u;
+    filter_onepass_tail_kernel<<<(tail + 255u) / 256u > 1024u ? 1024u : (tail + 255u) / 256u, 256, 0, stream>>>(
+        state, rows, output_rows, d_major_ptr);
+    return launch_ok("filter_onepass_tail_kernel");
 }

@@ -120,34 +120,67 @@ def manual_reoptimize_masked_sparse(src: BlockedELL, row_keep=None, feature_keep
     return CSR(out_rows, out_cols, major, idx, val), meta
 
 
+STATUS_CAPACITY = 1 << 5
+
+
 def filter_blocked_ell_to_compressed(parts, output_rows: int, output_cols: int, keep_rows=None, keep_cols=None,
-                                     row_remap=None, col_remap=None, stream=None):
+                                     row_remap=None, col_remap=None, stream=None, method: str = "auto"):
     """Filtered Blocked-ELL -> CSR over the partitions of one shard, rows concatenated in
     order (convert::filter_blocked_ell_to_compressed, src/convert/
     filtered_blocked_ell_to_compressed.cuh:264-382, and the filter stage of
     repack::build_repacked_shard_blocked_ell).  Synchronises once to size the output.
     Returns (CSR, stats) with the reference's stats fields; kept_rows / kept_row_slots
-    count every kept source row (the repack operator's figures)."""
+    count every kept source row (the repack operator's figures).
+
+    method "auto": one pass over the values (cs_b200_filter_blocked_ell_onepass) when the
+    shard qualifies (no remaps, block sizes multiples of 8, output_rows >= its rows), into
+    arrays sized by the parts' stored nnz; otherwise, or if those prove too small, count +
+    emit.  "onepass" / "two_pass" force one route ("onepass" raises if it does not apply)."""
     lib = _abi.load()
     parts = list(parts) if isinstance(parts, (list, tuple)) else [parts]
     views = (_abi.BlockedEllView * len(parts))(*[p.view() for p in parts])
     shard_rows = sum(p.rows for p in parts)
     m = _mask_view(keep_rows, keep_cols, row_remap, col_remap)
-    nbytes = C.c_size_t()
-    _abi.check(lib.cs_b200_filter_blocked_ell_scratch_bytes(shard_rows, output_rows, C.byref(nbytes)), "scratch")
-    scratch = torch.empty(max(nbytes.value, 16), dtype=torch.uint8, device="cuda")
     major = torch.empty(output_rows + 1, dtype=torch.int32, device="cuda")
     kept = torch.zeros(2, dtype=torch.int64, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     s = stream_handle(stream)
-    _abi.check(lib.cs_b200_filter_blocked_ell_count(views, len(parts), C.byref(m), output_rows, output_cols,
-                                                    ptr(major), ptr(kept), ptr(scratch), nbytes.value, ptr(status),
-                                                    s), "filter_blocked_ell_count")
-    nnz = int(major[output_rows].item()) & 0xFFFFFFFF
-    idx = torch.empty(nnz, dtype=torch.int32, device="cuda")
-    val = torch.empty(nnz, dtype=torch.float16, device="cuda")
-    _abi.check(lib.cs_b200_filter_blocked_ell_emit(views, len(parts), C.byref(m), output_rows, output_cols,
-                                                   ptr(major), ptr(idx), ptr(val), s), "filter_blocked_ell_emit")
+    idx = val = None
+    nnz = None
+    qualifies = (row_remap is None and col_remap is None and output_rows >= shard_rows
+                 and all(p.rows == 0 or (p.block_size % 8 == 0 and p.val.data_ptr() % 16 == 0) for p in parts))
+    if method == "onepass" and not qualifies:
+        raise _abi.CellShardError("the one-pass filter needs no remaps, block sizes multiple of 8 and "
+                                  "output_rows >= the shard's rows")
+    if method != "two_pass" and qualifies:
+        cap = sum(int(p.nnz) for p in parts)
+        nb = C.c_size_t()
+        _abi.check(lib.cs_b200_filter_blocked_ell_onepass_scratch_bytes(shard_rows, C.byref(nb)), "onepass scratch")
+        scratch = torch.empty(max(nb.value, 16), dtype=torch.uint8, device="cuda")
+        idx = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
+        val = torch.empty(max(cap, 1), dtype=torch.float16, device="cuda")
+        _abi.check(lib.cs_b200_filter_blocked_ell_onepass(views, len(parts), C.byref(m), output_rows, output_cols,
+                                                          ptr(major), ptr(idx), ptr(val), cap, ptr(kept), ptr(scratch),
+                                                          nb.value, ptr(status), s), "filter_blocked_ell_onepass")
+        st = int(status.item())
+        if st & STATUS_CAPACITY and method != "onepass":
+            status.zero_()
+            idx = val = None  # the stored nnz under-counts: count + emit below
+        else:
+            nnz = int(major[output_rows].item()) & 0xFFFFFFFF
+            idx, val = idx[:nnz], val[:nnz]
+    if idx is None:
+        nbytes = C.c_size_t()
+        _abi.check(lib.cs_b200_filter_blocked_ell_scratch_bytes(shard_rows, output_rows, C.byref(nbytes)), "scratch")
+        scratch = torch.empty(max(nbytes.value, 16), dtype=torch.uint8, device="cuda")
+        _abi.check(lib.cs_b200_filter_blocked_ell_count(views, len(parts), C.byref(m), output_rows, output_cols,
+                                                        ptr(major), ptr(kept), ptr(scratch), nbytes.value,
+                                                        ptr(status), s), "filter_blocked_ell_count")
+        nnz = int(major[output_rows].item()) & 0xFFFFFFFF
+        idx = torch.empty(nnz, dtype=torch.int32, device="cuda")
+        val = torch.empty(nnz, dtype=torch.float16, device="cuda")
+        _abi.check(lib.cs_b200_filter_blocked_ell_emit(views, len(parts), C.byref(m), output_rows, output_cols,
+                                                       ptr(major), ptr(idx), ptr(val), s), "filter_blocked_ell_emit")
     st = int(status.item())
     if st:
         raise _abi.CellShardError(f"filter flagged invalid input (status 0x{st:x})")

@@ -52,7 +52,9 @@ enum {
     CS_STATUS_DUPLICATE_COL = 1u << 1,      /* a row repeats a column index */
     CS_STATUS_INDEX_RANGE = 1u << 2,        /* an index is >= its dimension */
     CS_STATUS_REMAP_COLLISION = 1u << 3,    /* two kept rows remap to one output row */
-    CS_STATUS_BAD_POINTERS = 1u << 4        /* a CSR row pointer decreases or exceeds nnz */
+    CS_STATUS_BAD_POINTERS = 1u << 4,       /* a CSR row pointer decreases or exceeds nnz */
+    CS_STATUS_CAPACITY = 1u << 5,           /* the caller's output arrays are too small (nothing written past them) */
+    CS_STATUS_WAIT_LIMIT = 1u << 6          /* a device-side wait gave up: the result is incomplete */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -609,6 +611,33 @@ CS_API int cs_b200_filter_blocked_ell_count(const cs_blocked_ell_view *parts,
                                             size_t scratch_bytes,
                                             uint32_t *d_status,
                                             cs_stream_t stream);
+
+/* The same filter in ONE pass over the kept rows' values, for shards without
+ * row or feature remaps whose block sizes are multiples of 8 (16-byte aligned
+ * values) and output_rows >= the shard's rows: each row is counted, its output
+ * offset found by a decoupled look-back over the rows before it, and its
+ * entries written while its values are still in L2, so the values cross HBM
+ * once instead of twice (count + emit).  The output arrays hold `capacity`
+ * entries (the stored nnz of the parts bounds the live entries); a shard that
+ * needs more sets CS_STATUS_CAPACITY in *d_status and writes nothing past
+ * them (run count + emit instead).  d_major_ptr, d_kept as for count.
+ * Returns 0 with a message (and launches nothing) when the shard does not
+ * qualify.  Scratch: cs_b200_filter_blocked_ell_onepass_scratch_bytes. */
+CS_API int cs_b200_filter_blocked_ell_onepass_scratch_bytes(uint32_t shard_rows, size_t *out_bytes);
+CS_API int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *parts,
+                                              uint32_t part_count,
+                                              const cs_row_feature_mask_view *masks,
+                                              uint32_t output_rows,
+                                              uint32_t output_cols,
+                                              uint32_t *d_major_ptr,
+                                              uint32_t *d_minor_idx,
+                                              uint16_t *d_val,
+                                              uint64_t capacity,
+                                              uint64_t *d_kept,
+                                              void *d_scratch,
+                                              size_t scratch_bytes,
+                                              uint32_t *d_status,
+                                              cs_stream_t stream);
 
 CS_API int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts,
                                            uint32_t part_count,

@@ -142,3 +142,56 @@ def test_reference_filter_row_pointers_are_shifted(cuda, orc):
     shifted = np.concatenate([[0, 0], np.cumsum(counts)[:-1]]).astype(np.uint32)
     assert np.array_equal(np_u32(rptr), shifted)
     assert live.value == int(shifted[-1])
+
+
+@pytest.mark.parametrize("part_specs,cols,out_rows", [
+    ([(300, 16)], 257, 300),
+    ([(130, 16), (77, 8), (2000, 16)], 3000, 2500),   # output rows past the shard's stay empty
+    ([(64, 32), (1, 16), (9000, 8)], 500, 9065),
+])
+def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows):
+    """The one-pass filter (count, look-back over rows, emit while in L2) gives the count +
+    emit CSR bit for bit, with the same kept-row statistics, and both equal the
+    restatement's masked reoptimize without remaps."""
+    from cellshard_b200 import runtime
+
+    parts, host = _shard(61, part_specs, cols)
+    shard_rows = sum(r for r, _ in part_specs)
+    rng = np.random.default_rng(5)
+    keep_rows = (rng.random(shard_rows) < 0.7).astype(np.uint8)
+    keep_cols = (rng.random(cols) < 0.6).astype(np.uint8)
+    import torch
+
+    rk, fk = torch.from_numpy(keep_rows).cuda(), torch.from_numpy(keep_cols).cuda()
+    a, sa = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="onepass")
+    b, sb = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="two_pass")
+    assert sa == sb
+    assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr))
+    assert np.array_equal(np_u32(a.idx), np_u32(b.idx))
+    assert np.array_equal(np_u16(a.val), np_u16(b.val))
+    ident = np.arange(shard_rows, dtype=np.uint32)
+    ptr, idx, val = _oracle_filter(orc, host, cols, keep_rows, keep_cols, ident, np.arange(cols, dtype=np.uint32),
+                                   out_rows, cols)
+    assert np.array_equal(np_u32(a.ptr), ptr) and np.array_equal(np_u32(a.idx), idx)
+    assert np.array_equal(np_u16(a.val), val)
+
+
+def test_filter_onepass_capacity_falls_back(cuda):
+    """A view whose stored nnz under-counts its nonzeros gives the one-pass filter too
+    little room: it flags CS_STATUS_CAPACITY (forced one pass raises) and the default
+    route reruns count + emit with the same result as always."""
+    import torch
+
+    from cellshard_b200 import _abi, runtime
+    from cellshard_b200.device import BlockedELL
+
+    parts, _host = _shard(71, [(500, 16)], 400)
+    p = parts[0]
+    short = BlockedELL(p.rows, p.cols, p.block_size, p.ell_cols, p.bci, p.val, nnz=p.nnz // 3)
+    rk = torch.ones(p.rows, dtype=torch.uint8, device="cuda")
+    with pytest.raises(_abi.CellShardError):
+        runtime.filter_blocked_ell_to_compressed([short], p.rows, p.cols, rk, None, method="onepass")
+    a, _ = runtime.filter_blocked_ell_to_compressed([short], p.rows, p.cols, rk, None)
+    b, _ = runtime.filter_blocked_ell_to_compressed([p], p.rows, p.cols, rk, None, method="two_pass")
+    assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr)) and np.array_equal(np_u32(a.idx), np_u32(b.idx))
+    assert np.array_equal(np_u16(a.val), np_u16(b.val))
