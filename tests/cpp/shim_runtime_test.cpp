@@ -539,7 +539,7 @@ int main(int argc, char **argv) {
                 std::printf(" %lu %lu %d %d %ld", r.group_begin, r.group_end, r.allocation != nullptr ? 1 : 0,
                             r.device_id, vo);
             }
-            std::printf(" cache %lu\n", st.cache_count);
+            std::printf("\n%s.cache %lu\n", tag.c_str(), st.cache_count);
         };
         if (cs::device::stage_shard(&st, &m, nullptr, 0ul, 0, 0) != cudaSuccess) return fail(44, "stage_shard 0");
         records("shard.records.s0");
