@@ -1001,24 +1001,34 @@ extern "C" int cs_b200_group_moments_blocked_ell_parts(const cs_blocked_ell_view
 namespace {
 
 // Copy stream and events of the host-delivery entry point, one set per host
-// thread and device (created on first use, kept for the thread's lifetime).
+// thread and device ordinal (created on first use on that device, kept for the
+// thread's lifetime, so a thread that moves between devices creates nothing
+// new after its first call on each).
 struct host_copy_ctx {
-    int device = -1;
     cudaStream_t copy = nullptr;
     cudaEvent_t ready = nullptr, done = nullptr;
 };
 
-bool host_copy_setup(host_copy_ctx &c) {
+constexpr int kCopyDevices = 64;
+
+host_copy_ctx *host_copy_setup() {
+    thread_local host_copy_ctx ctxs[kCopyDevices];
     int dev = 0;
-    if (!cuda_ok(cudaGetDevice(&dev), "get device")) return false;
-    if (c.device == dev && c.copy != nullptr) return true;
-    c = host_copy_ctx{};
-    if (!cuda_ok(cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking), "copy stream") ||
-        !cuda_ok(cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming), "copy event") ||
-        !cuda_ok(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "copy event"))
-        return false;
-    c.device = dev;
-    return true;
+    if (!cuda_ok(cudaGetDevice(&dev), "get device")) return nullptr;
+    if (dev < 0 || dev >= kCopyDevices) {
+        set_error("group_moments_to_host: device ordinal %d outside the supported range", dev);
+        return nullptr;
+    }
+    host_copy_ctx &c = ctxs[dev];
+    if (c.copy != nullptr && c.ready != nullptr && c.done != nullptr) return &c;
+    // a set-up that failed partway keeps what it created and completes it now
+    if (c.copy == nullptr && !cuda_ok(cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking), "copy stream"))
+        return nullptr;
+    if (c.ready == nullptr && !cuda_ok(cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming), "copy event"))
+        return nullptr;
+    if (c.done == nullptr && !cuda_ok(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "copy event"))
+        return nullptr;
+    return &c;
 }
 
 template <typename T>
@@ -1060,8 +1070,9 @@ extern "C" int cs_b200_group_moments_to_host(const cs_blocked_ell_view *src, con
     if (!moments_run(src, d_row_keep, d_feature_keep, d_row_labels, params, d_out, d_scratch, scratch_bytes, s,
                      CS_MOMENTS_PHASE_PREPARE))
         return 0;
-    thread_local host_copy_ctx ctx;
-    if (!host_copy_setup(ctx)) return 0;
+    host_copy_ctx *cp = host_copy_setup();
+    if (cp == nullptr) return 0;
+    host_copy_ctx &ctx = *cp;
     const std::size_t cols = src->cols;
     for (uint32_t k = 0; k < parts; ++k) {
         const uint32_t g0 = (uint32_t) ((uint64_t) k * G / parts), g1 = (uint32_t) ((uint64_t) (k + 1u) * G / parts);

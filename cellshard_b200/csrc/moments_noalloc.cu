@@ -15,7 +15,10 @@
 // name is only a host-side stand-in, never a device address: the device
 // address is obtained once per device with cudaGetSymbolAddress (with that
 // device current) and cached.  The first call on each device performs that
-// set-up, so that first call should come before any stream capture.
+// set-up, so that first call should come before any stream capture.  The
+// cached address belongs to the device's primary context: after
+// cudaDeviceReset the module is loaded again and the array may move, so a
+// process that resets a device must not use this entry point on it again.
 //
 // All calls share the one array and the array keeps the previous call's
 // contents.  The reduction writes every scratch byte it reads during the same

@@ -939,7 +939,8 @@ CS_API int cs_b200_group_moments_blocked_ell(const cs_blocked_ell_view *src,
  * return 0 with a message.  All calls share the array and it keeps the last
  * call's contents (nothing needs clearing: every byte read is written earlier
  * in the same call); calls that overlap on the GPU race on it, so the caller
- * serialises them. */
+ * serialises them.  The located address is kept for the life of the process:
+ * do not call this again on a device after cudaDeviceReset. */
 CS_API int cs_b200_group_moments_blocked_ell_noalloc(const cs_blocked_ell_view *src,
                                                      const uint8_t *d_row_keep,
                                                      const uint8_t *d_feature_keep,

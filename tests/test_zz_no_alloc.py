@@ -80,13 +80,15 @@ def test_noalloc_matches_caller_scratch_entry_point_on_two_calls(cuda):
         ref = runtime.compute_sparse_group_moments(bell, G, rk, fk, lab, ddof=1)
         out = _outputs(G, cols)
         torch.cuda.synchronize()
-        free_before = torch.cuda.mem_get_info()[0]
-        _noalloc(bell, G, rk, fk, lab, out)
-        torch.cuda.synchronize()
-        free_after = torch.cuda.mem_get_info()[0]
+        free = [torch.cuda.mem_get_info()[0]]
+        for _ in range(3 if n > 0 else 1):
+            _noalloc(bell, G, rk, fk, lab, out)
+            torch.cuda.synchronize()
+            free.append(torch.cuda.mem_get_info()[0])
         if n > 0:
-            # once the first call has located the static scratch, a call allocates nothing
-            assert free_after == free_before
+            # once the first call has located the static scratch, repeated calls allocate nothing:
+            # the device's free memory stays the same across all of them
+            assert len(set(free)) == 1, free
         assert int(out["status"].item()) == 0
         assert torch.equal(out["group_rows"], ref["group_rows"])
         for k in ("sum", "sumsq", "mean", "var"):
