@@ -793,7 +793,14 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
         ex["cpu_baseline"] = conversion_cpu_baseline(
             csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_blocked_ell_from_compressed(parts, B, th, sec), secs,
             "the reference's convert::blocked_ell_from_compressed (block 16) compiled from its sources")
-    emit("blocked_ell_emit", ms_emit, 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4, ex)
+    bell_bytes_alg = 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4
+    emit("blocked_ell_emit", ms_emit, bell_bytes_alg, ex)
+    # the whole conversion through the public call, warm (shape, one read of the width, the output
+    # from the allocator's cache, emit, status read): what a caller converting repeatedly sees
+    ms_api = timed(lambda: blocked_ell_from_csr(csr, B))
+    emit("blocked_ell_from_csr_api", ms_api, bell_bytes_alg,
+         {"ell_cols": bell.ell_cols, "note": "device.blocked_ell_from_csr end to end on device data, warm; bytes "
+                                             "as the emit's (the shape pass's read of the indices is not credited)"})
     # Blocked-ELL -> Sliced-ELL (h 32): live-entry row pointers (count + scan), then the emit;
     # both read the whole value array (the layout needs every row's count before any slot)
     from cellshard_b200.device import blocked_ell_row_ptr, sliced_ell_from_blocked_ell
