@@ -227,6 +227,76 @@ __device__ __forceinline__ void reduce_span(const uint32_t *__restrict__ idx, co
     }
 }
 
+// Column codes in shared memory for the compressed and Sliced-ELL reduces
+// with at most 15 groups: bit 15 = the column is kept, bits 0..14 its groups
+// (bits at or above the group count cleared).  One 2-byte shared read per
+// entry replaces two global gathers (the feature flag and the group mask) that
+// touch ~32 distinct cache lines per warp for a row's sorted columns.
+__device__ __forceinline__ void build_col_codes(uint16_t *tbl, uint32_t cols, const uint8_t *__restrict__ feature_keep,
+                                                const uint32_t *__restrict__ group_masks, uint32_t gmask) {
+    for (uint32_t c = threadIdx.x; c < cols; c += blockDim.x) {
+        uint32_t e = 0u;
+        if (feature_kept(feature_keep, c)) e = 0x8000u | (group_masks != nullptr ? __ldg(group_masks + c) & gmask : 0u);
+        tbl[c] = (uint16_t) e;
+    }
+    __syncthreads();
+}
+
+// reduce_span with the column codes: same quads, loads in flight and
+// head / tail handling.
+template <unsigned U, unsigned GR>
+__device__ __forceinline__ void reduce_span_codes(const uint32_t *__restrict__ idx, const uint16_t *__restrict__ val,
+                                                  std::size_t b, std::size_t e, uint32_t cols,
+                                                  const uint16_t *__restrict__ tbl, row_acc<GR> &a) {
+    const unsigned lane = threadIdx.x & 31u;
+    const std::size_t a4 = min(e, (b + 3u) & ~(std::size_t) 3u);
+    const std::size_t e4 = max(a4, e & ~(std::size_t) 3u);
+    {
+        const std::size_t i = lane < 3u ? b + lane : e4 + (lane - 3u);
+        if (lane < 3u ? i < a4 : (lane < 6u && i < e)) {
+            const uint32_t col = __ldg(idx + i);
+            const uint32_t h = __ldg(val + i);
+            if (col < cols && (h & 0x7fffu) != 0u) {
+                const uint32_t code = tbl[col];
+                if (code & 0x8000u) add_value_masked(a, h2f((uint16_t) h), code & 0x7fffu);
+            }
+        }
+    }
+    const std::size_t q_end = e4 >> 2;
+    for (std::size_t q = (a4 >> 2) + lane; q < q_end; q += 32u * U) {
+        uint4 c[U];
+        uint2 h[U];
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            const std::size_t qi = q + 32u * u;
+            const bool in = qi < q_end;
+            c[u] = in ? ld_stream_v4(idx + qi * 4u) : make_uint4(cols, cols, cols, cols);
+            h[u] = in ? ld_stream_v2(val + qi * 4u) : make_uint2(0u, 0u);
+        }
+        uint32_t col[4 * U], hv[4 * U], code[4 * U];
+        bool any = false;
+#pragma unroll
+        for (unsigned u = 0; u < U; ++u) {
+            col[4 * u + 0] = c[u].x;
+            col[4 * u + 1] = c[u].y;
+            col[4 * u + 2] = c[u].z;
+            col[4 * u + 3] = c[u].w;
+            hv[4 * u + 0] = h[u].x & 0xffffu;
+            hv[4 * u + 1] = h[u].x >> 16;
+            hv[4 * u + 2] = h[u].y & 0xffffu;
+            hv[4 * u + 3] = h[u].y >> 16;
+            any = any || ((h[u].x | h[u].y) & 0x7fff7fffu) != 0u;
+        }
+        if (!any) continue;
+#pragma unroll
+        for (unsigned j = 0; j < 4 * U; ++j)
+            code[j] = (col[j] < cols && (hv[j] & 0x7fffu) != 0u) ? (uint32_t) tbl[col[j]] : 0u;
+#pragma unroll
+        for (unsigned j = 0; j < 4 * U; ++j)
+            if (code[j] & 0x8000u) add_value_masked(a, h2f((uint16_t) hv[j]), code[j] & 0x7fffu);
+    }
+}
+
 // One Blocked-ELL row, warp-wide (reads, accumulation and outputs).
 template <bool VEC, unsigned GR>
 __device__ __forceinline__ void bell_row(const cs_blocked_ell_view &src, uint32_t row,
@@ -422,6 +492,97 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_kernel(cs_compre
         __syncwarp();
         finish_row(row, a, acc_col, group_count, filter, out);
     }
+}
+
+// The compressed and Sliced-ELL reduces over shared-memory column codes (at
+// most 15 groups, the code table in shared memory after the accumulators;
+// col_idx / minorIdx 16-byte and val 8-byte aligned).
+template <unsigned GR, unsigned U = 2>
+__global__ void __launch_bounds__(kRowThreads) group_reduce_csr_codes_kernel(cs_compressed_view src,
+                                                                              const uint32_t *__restrict__ group_masks,
+                                                                              uint32_t group_count,
+                                                                              cs_row_feature_mask_view masks,
+                                                                              cs_group_filter_params filter,
+                                                                              cs_group_reduce_out out) {
+    extern __shared__ __align__(16) float gr_smem[];
+    float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
+    uint16_t *tbl = reinterpret_cast<uint16_t *>(gr_smem + (GR != 0u ? kRowWarps * group_count * 32u : 0u));
+    build_col_codes(tbl, src.cols, masks.feature_keep, GR != 0u ? group_masks : nullptr,
+                    GR != 0u ? (1u << group_count) - 1u : 0u);
+    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
+        if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
+            empty_row(row, group_count, out);
+            continue;
+        }
+        row_acc<GR> a;
+        init_acc(a);
+        reduce_span_codes<U>(src.minorIdx, src.val, src.majorPtr[row], src.majorPtr[row + 1u], src.cols, tbl, a);
+        __syncwarp();
+        finish_row(row, a, acc_col, group_count, filter, out);
+    }
+}
+
+template <unsigned GR, unsigned U = 2>
+__global__ void __launch_bounds__(kRowThreads) group_reduce_sell_codes_kernel(cs_sliced_ell_view src,
+                                                                               const uint32_t *__restrict__ group_masks,
+                                                                               uint32_t group_count,
+                                                                               cs_row_feature_mask_view masks,
+                                                                               cs_group_filter_params filter,
+                                                                               cs_group_reduce_out out) {
+    extern __shared__ __align__(16) float gr_smem[];
+    float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
+    uint16_t *tbl = reinterpret_cast<uint16_t *>(gr_smem + (GR != 0u ? kRowWarps * group_count * 32u : 0u));
+    build_col_codes(tbl, src.cols, masks.feature_keep, GR != 0u ? group_masks : nullptr,
+                    GR != 0u ? (1u << group_count) - 1u : 0u);
+    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
+        if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
+            empty_row(row, group_count, out);
+            continue;
+        }
+        row_acc<GR> a;
+        init_acc(a);
+        uint32_t width = 0u;
+        std::size_t slot_base = 0u;
+        if (src.slice_count != 0u) {
+            const uint32_t slice = find_slice(src, row);
+            width = src.slice_widths[slice];
+            slot_base = (std::size_t) src.slice_slot_offsets[slice] +
+                        (std::size_t) (row - src.slice_row_offsets[slice]) * width;
+        }
+        reduce_span_codes<U>(src.col_idx, src.val, slot_base, slot_base + width, src.cols, tbl, a);
+        __syncwarp();
+        finish_row(row, a, acc_col, group_count, filter, out);
+    }
+}
+
+std::size_t group_smem(const uint32_t *masks, uint32_t group_count);
+
+// Shared bytes of the code-table kernels, 0 when they do not apply (more than
+// 15 groups, or a table above 96 KB).
+std::size_t codes_smem(const uint32_t *masks, uint32_t group_count, uint32_t cols) {
+    const bool groups = masks != nullptr && group_count != 0u;
+    if (groups && group_count > 15u) return 0u;
+    if ((std::size_t) cols * 2u > 96u * 1024u) return 0u;
+    return align_up(group_smem(masks, group_count), 16u) + align_up((std::size_t) cols * 2u, 16u);
+}
+
+template <typename View>
+using reduce_codes_kernel_t = void (*)(View, const uint32_t *, uint32_t, cs_row_feature_mask_view,
+                                       cs_group_filter_params, cs_group_reduce_out);
+
+template <typename View>
+int launch_codes(reduce_codes_kernel_t<View> k, const View &src, const uint32_t *masks, uint32_t group_count,
+                 const cs_row_feature_mask_view &m, const cs_group_filter_params &filter,
+                 const cs_group_reduce_out &out, std::size_t smem, cudaStream_t stream, const char *name) {
+    if (smem > 48u * 1024u &&
+        !cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(k), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) smem),
+                 name))
+        return 0;
+    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, smem,
+                                        (src.rows + kRowWarps - 1u) / kRowWarps);
+    k<<<grid, kRowThreads, smem, stream>>>(src, masks, group_count, m, filter, out);
+    return launch_ok(name);
 }
 
 // ---------------------------------------------------------------------------
@@ -1276,6 +1437,15 @@ extern "C" int cs_b200_group_reduce_sliced_ell(const cs_sliced_ell_view *src, co
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
     const bool vec = (reinterpret_cast<uintptr_t>(src->col_idx) & 15u) == 0u &&
                      (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u;
+    const std::size_t csmem = vec ? codes_smem(d_feature_group_masks, group_count, src->cols) : 0u;
+    if (csmem != 0u) {
+        const unsigned g = group_regs(d_feature_group_masks, group_count);
+        return launch_codes<cs_sliced_ell_view>(g == 0u ? group_reduce_sell_codes_kernel<0u>
+                                                        : g == 8u ? group_reduce_sell_codes_kernel<8u>
+                                                                  : group_reduce_sell_codes_kernel<16u>,
+                                                *src, d_feature_group_masks, group_count, m, *filter, *out, csmem,
+                                                as_stream(s), "group_reduce_sell_codes_kernel");
+    }
     const std::size_t smem = group_smem(d_feature_group_masks, group_count);
     const unsigned gr = group_regs(d_feature_group_masks, group_count);
     const reduce_kernel_t<cs_sliced_ell_view> k = vec ? CS_PICK_REDUCE(group_reduce_sell_kernel, true, gr)
@@ -1302,6 +1472,15 @@ extern "C" int cs_b200_group_reduce_compressed(const cs_compressed_view *src, co
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
     const bool vec = (reinterpret_cast<uintptr_t>(src->minorIdx) & 15u) == 0u &&
                      (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u;
+    const std::size_t csmem = vec ? codes_smem(d_feature_group_masks, group_count, src->cols) : 0u;
+    if (csmem != 0u) {
+        const unsigned g = group_regs(d_feature_group_masks, group_count);
+        return launch_codes<cs_compressed_view>(g == 0u ? group_reduce_csr_codes_kernel<0u>
+                                                        : g == 8u ? group_reduce_csr_codes_kernel<8u>
+                                                                  : group_reduce_csr_codes_kernel<16u>,
+                                                *src, d_feature_group_masks, group_count, m, *filter, *out, csmem,
+                                                as_stream(s), "group_reduce_csr_codes_kernel");
+    }
     const std::size_t smem = group_smem(d_feature_group_masks, group_count);
     const unsigned gr = group_regs(d_feature_group_masks, group_count);
     const reduce_kernel_t<cs_compressed_view> k = vec ? CS_PICK_REDUCE(group_reduce_csr_kernel, true, gr)
