@@ -1209,14 +1209,23 @@ __device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, ui
     return live & in_range8(bc, gene0, output_cols);
 }
 
-__global__ void __launch_bounds__(kRowThreads) filter_onepass_kernel(
+// One CTA per row at a time (rows claimed in order): the row's values are read
+// once to count, and read again from L2 to emit -- with a few CTAs per SM the
+// rows in flight stay well inside L2.  Each thread owns kOpVecs consecutive
+// 16-byte vectors of a 256 x kOpVecs-vector step, so one block scan per step
+// gives every thread its output position in slot order.
+constexpr unsigned kOpThreads = 256;
+constexpr unsigned kOpVecs = 4;
+constexpr unsigned kOpCtasPerSm = 3;
+
+__global__ void __launch_bounds__(kOpThreads) filter_onepass_kernel(
     const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
     uint32_t *__restrict__ major_ptr, uint32_t *__restrict__ minor_idx, uint16_t *__restrict__ out_val,
     unsigned long long capacity, unsigned long long *__restrict__ row_state, uint32_t *__restrict__ row_counter,
     uint32_t *status, unsigned long long *__restrict__ kept, uint32_t keep_words) {
-    const unsigned lane = threadIdx.x & 31u;
     const uint32_t rows = parts.row_off[parts.count];
     extern __shared__ uint32_t onepass_keep_bits[];
+    __shared__ uint32_t s_row, s_excl, s_stop, scan33[33];
     const uint32_t *kbits = keep_words != 0u ? onepass_keep_bits : nullptr;
     uint32_t kcols = 0u;
     for (uint32_t k = 0; k < parts.count; ++k) kcols = max(kcols, parts.v[k].cols);
@@ -1228,14 +1237,16 @@ __global__ void __launch_bounds__(kRowThreads) filter_onepass_kernel(
             if (c0 + k < kcols) word |= (masks.feature_keep[c0 + k] != 0u ? 1u : 0u) << k;
         onepass_keep_bits[w] = word;
     }
-    if (keep_words != 0u) __syncthreads();
-    uint32_t warp_kept_rows = 0u;
-    unsigned long long warp_kept_slots = 0u;
-    bool gave_up = false;
+    uint32_t cta_kept_rows = 0u;
+    unsigned long long cta_kept_slots = 0u;
+    constexpr uint32_t kStep = kOpThreads * kOpVecs * 8u; // values per step
     for (;;) {
-        uint32_t row = 0u;
-        if (lane == 0u) row = atomicAdd(row_counter, 1u);
-        row = __shfl_sync(0xffffffffu, row, 0);
+        if (threadIdx.x == 0u) {
+            s_row = atomicAdd(row_counter, 1u);
+            s_stop = 0u;
+        }
+        __syncthreads();
+        const uint32_t row = s_row;
         if (row >= rows) break;
         const bool kept_row = masks.row_keep == nullptr || masks.row_keep[row] != 0u;
         const uint32_t part = part_of_row(parts, row);
@@ -1245,29 +1256,41 @@ __global__ void __launch_bounds__(kRowThreads) filter_onepass_kernel(
         const block_div bd(B);
         const uint32_t *bci = src.blockColIdx + (std::size_t) (local / B) * W;
         const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
-        constexpr unsigned kRs = 4;
-        // count
-        uint32_t lane_count = 0u;
-        if (kept_row) {
-            warp_kept_rows += 1u;
-            warp_kept_slots += src.ell_cols;
-            for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
-                uint4 v[kRs];
-                uint32_t bcs[kRs];
-                load_steps(vrow, bci, bd, src.ell_cols, b0, v, bcs);
+        // keep bits of this thread's vectors of one step
+        auto step_keep = [&](uint32_t base, uint4 (&v)[kOpVecs], uint32_t (&keep)[kOpVecs], uint32_t (&gene0)[kOpVecs]) {
 #pragma unroll
-                for (unsigned u = 0; u < kRs; ++u)
-                    lane_count += __popc(onepass_keep(v[u], bcs[u], bcs[u] * B + bd.mod(b0 + u * 256u), src.cols,
-                                                      output_cols, kbits));
+            for (unsigned u = 0; u < kOpVecs; ++u) {
+                const uint32_t e0 = base + (threadIdx.x * kOpVecs + u) * 8u;
+                const bool in = e0 < src.ell_cols;
+                v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
+                const uint32_t bc = in ? __ldg(bci + bd.div(e0)) : CS_INVALID_COL;
+                gene0[u] = bc * B + bd.mod(e0);
+                keep[u] = in ? onepass_keep(v[u], bc, gene0[u], src.cols, output_cols, kbits) : 0u;
+            }
+        };
+        // count
+        uint32_t my = 0u;
+        if (kept_row) {
+            if (threadIdx.x == 0u) {
+                cta_kept_rows += 1u;
+                cta_kept_slots += src.ell_cols;
+            }
+            for (uint32_t base = 0u; base < src.ell_cols; base += kStep) {
+                uint4 v[kOpVecs];
+                uint32_t keep[kOpVecs], gene0[kOpVecs];
+                step_keep(base, v, keep, gene0);
+#pragma unroll
+                for (unsigned u = 0; u < kOpVecs; ++u) my += __popc(keep[u]);
             }
         }
-        const uint32_t count = __reduce_add_sync(0xffffffffu, lane_count);
+        uint32_t count;
+        (void) block_exclusive_scan(my, scan33, count);
         // publish the count, then the prefix once the rows before it are known
-        uint32_t excl = 0u;
-        if (lane == 0u) {
+        if (threadIdx.x == 0u) {
             lb_store(row_state + row, kLbCount | count);
-            uint32_t j = row;
-            while (j > 0u && !gave_up) {
+            uint32_t excl = 0u, j = row;
+            bool gave_up = false;
+            while (j > 0u) {
                 --j;
                 unsigned long long st = lb_load(row_state + j);
                 for (uint32_t spins = 0; (st >> 32) == 0ull; st = lb_load(row_state + j)) {
@@ -1281,45 +1304,48 @@ __global__ void __launch_bounds__(kRowThreads) filter_onepass_kernel(
                 excl += (uint32_t) st;
                 if ((st & ~0xffffffffull) == kLbPrefix) break;
             }
-            if (!gave_up) {
+            if (gave_up) {
+                s_stop = 1u;
+                status_or(status, CS_STATUS_WAIT_LIMIT);
+            } else {
                 lb_store(row_state + row, kLbPrefix | (excl + count));
                 major_ptr[row] = excl;
-            }
-        }
-        gave_up = __shfl_sync(0xffffffffu, gave_up ? 1u : 0u, 0) != 0u;
-        if (gave_up) break;
-        excl = __shfl_sync(0xffffffffu, excl, 0);
-        if (count == 0u) continue;
-        if ((unsigned long long) excl + count > capacity) {
-            if (lane == 0u) status_or(status, CS_STATUS_CAPACITY);
-            continue;
-        }
-        // emit, re-reading the row (now in L2) in slot order
-        uint32_t run = excl;
-        for (uint32_t b0 = lane * 8u; b0 - lane * 8u < src.ell_cols; b0 += 256u * kRs) {
-            uint4 v[kRs];
-            uint32_t bcs[kRs];
-            load_steps(vrow, bci, bd, src.ell_cols, b0, v, bcs);
-#pragma unroll
-            for (unsigned u = 0; u < kRs; ++u) {
-                const uint32_t gene0 = bcs[u] * B + bd.mod(b0 + u * 256u);
-                const uint32_t keep = onepass_keep(v[u], bcs[u], gene0, src.cols, output_cols, kbits);
-                const uint32_t cnt = __popc(keep);
-                const uint32_t incl = warp_inclusive_scan(cnt);
-                uint32_t pos = run + incl - cnt;
-                for (uint32_t bb = keep; bb != 0u; bb &= bb - 1u, ++pos) {
-                    const uint32_t q = __ffs(bb) - 1u;
-                    minor_idx[pos] = gene0 + q;
-                    out_val[pos] = half_of(v[u], q);
+                if (count != 0u && (unsigned long long) excl + count > capacity) {
+                    s_stop = 2u; // this row does not fit: skip its emission
+                    status_or(status, CS_STATUS_CAPACITY);
                 }
-                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            s_excl = excl;
+        }
+        __syncthreads();
+        if (s_stop == 1u) break;
+        if (count != 0u && s_stop == 0u) {
+            // emit, re-reading the row (now in L2) in slot order
+            uint32_t run = s_excl;
+            for (uint32_t base = 0u; base < src.ell_cols; base += kStep) {
+                uint4 v[kOpVecs];
+                uint32_t keep[kOpVecs], gene0[kOpVecs];
+                step_keep(base, v, keep, gene0);
+                uint32_t n = 0u;
+#pragma unroll
+                for (unsigned u = 0; u < kOpVecs; ++u) n += __popc(keep[u]);
+                uint32_t total;
+                uint32_t pos = run + block_exclusive_scan(n, scan33, total);
+#pragma unroll
+                for (unsigned u = 0; u < kOpVecs; ++u)
+                    for (uint32_t bb = keep[u]; bb != 0u; bb &= bb - 1u, ++pos) {
+                        const uint32_t q = __ffs(bb) - 1u;
+                        minor_idx[pos] = gene0[u] + q;
+                        out_val[pos] = half_of(v[u], q);
+                    }
+                run += total;
             }
         }
+        __syncthreads(); // s_row / s_excl are rewritten by the next claim
     }
-    if (gave_up && lane == 0u) status_or(status, CS_STATUS_WAIT_LIMIT);
-    if (kept != nullptr && lane == 0u && warp_kept_rows != 0u) {
-        atomicAdd(kept, (unsigned long long) warp_kept_rows);
-        atomicAdd(kept + 1, warp_kept_slots);
+    if (threadIdx.x == 0u && kept != nullptr && cta_kept_rows != 0u) {
+        atomicAdd(kept, (unsigned long long) cta_kept_rows);
+        atomicAdd(kept + 1, cta_kept_slots);
     }
 }
 
@@ -1710,11 +1736,12 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
         return 0;
     if (rows != 0u) {
         const auto k = filter_onepass_kernel;
-        const unsigned grid =
-            resident_grid(reinterpret_cast<const void *>(k), kRowThreads, kw * 4u, (rows + kRowWarps - 1u) / kRowWarps);
-        k<<<grid, kRowThreads, kw * 4u, stream>>>(p, m, output_cols, d_major_ptr, d_minor_idx, d_val, capacity, state,
-                                                  counter, d_status, reinterpret_cast<unsigned long long *>(d_kept),
-                                                  kw);
+        // a few CTAs per SM: enough bytes in flight, few enough rows in flight to stay in L2
+        unsigned grid = (unsigned) sm_count() * kOpCtasPerSm;
+        if (grid > rows) grid = rows;
+        k<<<grid, kOpThreads, kw * 4u, stream>>>(p, m, output_cols, d_major_ptr, d_minor_idx, d_val, capacity, state,
+                                                 counter, d_status, reinterpret_cast<unsigned long long *>(d_kept),
+                                                 kw);
         if (!launch_ok("filter_onepass_kernel")) return 0;
     }
     const uint32_t tail = output_rows - rows + 1u;
