@@ -50,16 +50,8 @@ constexpr unsigned kScanThreads = 256;
 constexpr unsigned kScanItems = 16;
 constexpr unsigned kScanTile = kScanThreads * kScanItems;
 
-// A scan whose `gate` is given runs only when gate[0] has a bit of `gate_bits`
-// set (a device-side decision taken by an earlier kernel on the stream).
-__device__ __forceinline__ bool scan_gated_off(const uint32_t *gate, uint32_t gate_bits) {
-    return gate != nullptr && (*gate & gate_bits) == 0u;
-}
-
 __global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(const uint32_t *__restrict__ in, std::size_t n,
-                                                                       uint32_t *__restrict__ tile_sums,
-                                                                       const uint32_t *gate, uint32_t gate_bits) {
-    if (scan_gated_off(gate, gate_bits)) return;
+                                                                       uint32_t *__restrict__ tile_sums) {
     __shared__ uint32_t smem[33];
     uint32_t total;
     const std::size_t base = (std::size_t) blockIdx.x * kScanTile + (std::size_t) threadIdx.x * kScanItems;
@@ -74,9 +66,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(const uint
 }
 
 __global__ void __launch_bounds__(1024) scan_of_tile_sums_kernel(uint32_t *__restrict__ tile_sums, std::size_t tiles,
-                                                                 uint32_t *__restrict__ total_out, const uint32_t *gate,
-                                                                 uint32_t gate_bits) {
-    if (scan_gated_off(gate, gate_bits)) return;
+                                                                 uint32_t *__restrict__ total_out) {
     __shared__ uint32_t smem[33];
     uint32_t total;
     uint32_t carry = 0;
@@ -91,9 +81,7 @@ __global__ void __launch_bounds__(1024) scan_of_tile_sums_kernel(uint32_t *__res
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t *in, uint32_t *out, std::size_t n,
-                                                                   const uint32_t *__restrict__ tile_offsets,
-                                                                   const uint32_t *gate, uint32_t gate_bits) {
-    if (scan_gated_off(gate, gate_bits)) return;
+                                                                   const uint32_t *__restrict__ tile_offsets) {
     __shared__ uint32_t smem[33];
     uint32_t total;
     const std::size_t base = (std::size_t) blockIdx.x * kScanTile + (std::size_t) threadIdx.x * kScanItems;
@@ -122,7 +110,7 @@ std::size_t scan_u32_scratch_bytes(std::size_t n) {
 }
 
 int scan_exclusive_u32(const uint32_t *in, uint32_t *out, std::size_t n, bool write_total, void *scratch,
-                       std::size_t scratch_bytes, cudaStream_t stream, const uint32_t *gate, uint32_t gate_bits) {
+                       std::size_t scratch_bytes, cudaStream_t stream) {
     const std::size_t tiles = (n + kScanTile - 1) / kScanTile;
     if (n == 0) {
         if (write_total) return cuda_ok(cudaMemsetAsync(out, 0, sizeof(uint32_t), stream), "scan empty total");
@@ -137,12 +125,11 @@ int scan_exclusive_u32(const uint32_t *in, uint32_t *out, std::size_t n, bool wr
         return 0;
     }
     uint32_t *tile_sums = (uint32_t *) scratch;
-    scan_tile_sums_kernel<<<(unsigned) tiles, kScanThreads, 0, stream>>>(in, n, tile_sums, gate, gate_bits);
+    scan_tile_sums_kernel<<<(unsigned) tiles, kScanThreads, 0, stream>>>(in, n, tile_sums);
     if (!launch_ok("scan_tile_sums_kernel")) return 0;
-    scan_of_tile_sums_kernel<<<1, 1024, 0, stream>>>(tile_sums, tiles, write_total ? out + n : nullptr, gate,
-                                                     gate_bits);
+    scan_of_tile_sums_kernel<<<1, 1024, 0, stream>>>(tile_sums, tiles, write_total ? out + n : nullptr);
     if (!launch_ok("scan_of_tile_sums_kernel")) return 0;
-    scan_apply_kernel<<<(unsigned) tiles, kScanThreads, 0, stream>>>(in, out, n, tile_sums, gate, gate_bits);
+    scan_apply_kernel<<<(unsigned) tiles, kScanThreads, 0, stream>>>(in, out, n, tile_sums);
     return launch_ok("scan_apply_kernel");
 }
 

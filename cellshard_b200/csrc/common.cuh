@@ -191,14 +191,11 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // ---------------------------------------------------------------------------
 // Device-wide exclusive scan of uint32 (three launches: tile sums, scan of
 // tile sums, tile-local scan + add).  out may alias in.  out[n] receives the
-// total when write_total is set (so out must hold n + 1 entries).  With a
-// `gate`, the kernels do nothing unless gate[0] & gate_bits is non-zero (a
-// decision an earlier kernel on the stream wrote to device memory).
+// total when write_total is set (so out must hold n + 1 entries).
 // ---------------------------------------------------------------------------
 std::size_t scan_u32_scratch_bytes(std::size_t n);
 int scan_exclusive_u32(const uint32_t *in, uint32_t *out, std::size_t n, bool write_total, void *scratch,
-                       std::size_t scratch_bytes, cudaStream_t stream, const uint32_t *gate = nullptr,
-                       uint32_t gate_bits = 0u);
+                       std::size_t scratch_bytes, cudaStream_t stream);
 
 // Stable ascending sort of n uint32 keys carrying uint32 values (vals nullptr:
 // the indices 0..n-1), LSD radix in 8-bit digit passes (bucket.cu).  Word 0

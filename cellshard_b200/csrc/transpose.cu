@@ -4,22 +4,6 @@
 // (src/convert/compressed_transpose_raw.cuh:43-81).  Its atomic fallback
 // (:84-121) is order-nondeterministic and is not reproduced.
 //
-// Three routes, chosen by shape on the host and by content on the device:
-//   panel     (default: uDim <= 98,304 and cDim < 2^24) rows cut into tiles,
-//             columns into panels; each (tile, panel) block is counted, ranked
-//             and staged in shared memory and leaves as one run per column.
-//             Needs every row's columns strictly ascending, which its count
-//             pass checks; otherwise it leaves the work to
-//   two-pass  a stable counting sort on the column key in two passes
-//             (column >> 8, then column & 255), gated on the device by the
-//             panel path's check (and the route on its own for
-//             98,304 < uDim <= 262,144); it keeps repeated columns in row order.
-//   one-pass  (uDim > 262,144) the tile-histogram scatter directly below;
-//             a row that repeats a column sets CS_STATUS_DUPLICATE_COL.
-// The status word at the start of the caller's scratch gets CS_STATUS_* bits;
-// the word after it is the route decision.
-//
-// one-pass details:
 //   hist     rows are cut into T tiles; each CTA counts its tile's entries
 //            per column in shared memory -> H[t][c].
 //   colscan  per column, exclusive scan of H over tiles (in place) and the
@@ -30,6 +14,10 @@
 //            entry (r, c) at out_ptr[c] + H[t][c] + count + popc(mask below r);
 //            round C advances the count.  Placement is therefore fixed by
 //            (tile, row) order alone -- deterministic and stable.
+// The one-pass path below is used only where the two-pass path (further down,
+// the default) does not apply.  On the one-pass path a row that repeats a
+// column sets CS_STATUS_DUPLICATE_COL in the status word at the start of the
+// caller's scratch; the two-pass path keeps repeated entries, in row order.
 #include "common.cuh"
 
 namespace csb {
@@ -247,19 +235,8 @@ void tp2_make_layout(uint32_t cDim, uint32_t uDim, uint32_t nnz, void *base, std
 
 // gran_row[j] = the row holding entry j * kTpGran (rows own the granules that
 // start inside them).
-// The two-pass kernels below also serve as the fallback of the panel path:
-// given a gate (the word after the caller-visible status word), they run only
-// when the panel path's count pass found a row whose columns do not ascend
-// strictly (kTqFallback in gate[0]).
-constexpr uint32_t kTqFallback = 1u << 31;
-
-__device__ __forceinline__ bool tp_gated_off(const uint32_t *gate) {
-    return gate != nullptr && (*gate & kTqFallback) == 0u;
-}
-
 __global__ void __launch_bounds__(256) tp_gran_rows_kernel(const uint32_t *__restrict__ ptr, uint32_t cDim,
-                                                          uint32_t *__restrict__ gran_row, const uint32_t *gate) {
-    if (tp_gated_off(gate)) return;
+                                                          uint32_t *__restrict__ gran_row) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= cDim) return;
     const uint32_t lo = ptr[r], hi = ptr[r + 1u];
@@ -269,9 +246,7 @@ __global__ void __launch_bounds__(256) tp_gran_rows_kernel(const uint32_t *__res
 // Pass-1 histogram: tile t is entries [t * kTpTile1, (t + 1) * kTpTile1).
 __global__ void __launch_bounds__(kTpThreads) tp_hist1_kernel(const uint32_t *__restrict__ idx, uint32_t nnz,
                                                              uint32_t uDim, uint32_t K, uint32_t tiles1,
-                                                             uint32_t *__restrict__ hist1, uint32_t *status,
-                                                             const uint32_t *gate) {
-    if (tp_gated_off(gate)) return;
+                                                             uint32_t *__restrict__ hist1, uint32_t *status) {
     extern __shared__ uint32_t tp_h[];
     for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) tp_h[k] = 0u;
     __syncthreads();
@@ -386,8 +361,7 @@ __global__ void __launch_bounds__(kTpThreads) tp_scatter1_kernel(const uint32_t 
                                                                 uint32_t tiles1, const uint32_t *__restrict__ hist1,
                                                                 const uint32_t *__restrict__ gran_row,
                                                                 uint32_t *__restrict__ tmp_key,
-                                                                uint16_t *__restrict__ tmp_val, const uint32_t *gate) {
-    if (tp_gated_off(gate)) return;
+                                                                uint16_t *__restrict__ tmp_val) {
     extern __shared__ __align__(16) uint32_t tp_s[];
     __shared__ uint32_t scan33[33];
     // staged entry: key | value << 32 | bucket << 48
@@ -511,8 +485,7 @@ __global__ void __launch_bounds__(1024) tp_chunks_kernel(const uint32_t *__restr
                                                          uint32_t *__restrict__ chunk_bucket,
                                                          uint32_t *__restrict__ chunk_begin,
                                                          uint32_t *__restrict__ chunk_end,
-                                                         uint32_t *__restrict__ chunk_first, const uint32_t *gate) {
-    if (tp_gated_off(gate)) return;
+                                                         uint32_t *__restrict__ chunk_first) {
     __shared__ uint32_t smem[33];
     const uint32_t total = hist1[(std::size_t) K * tiles1];
     uint32_t carry = 0u;
@@ -552,9 +525,7 @@ __global__ void __launch_bounds__(1024) tp_chunks_kernel(const uint32_t *__restr
 __global__ void __launch_bounds__(kTpThreads) tp_hist2_kernel(const uint32_t *__restrict__ tmp_key,
                                                              const uint32_t *__restrict__ chunk_begin,
                                                              const uint32_t *__restrict__ chunk_end,
-                                                             uint32_t max_chunks, uint32_t *__restrict__ hist2,
-                                                             const uint32_t *gate) {
-    if (tp_gated_off(gate)) return;
+                                                             uint32_t max_chunks, uint32_t *__restrict__ hist2) {
     __shared__ uint32_t h[kTpWarps][256];
     const unsigned warp = threadIdx.x >> 5;
     for (uint32_t d = threadIdx.x; d < kTpWarps * 256u; d += blockDim.x) (&h[0][0])[d] = 0u;
@@ -600,8 +571,7 @@ __global__ void __launch_bounds__(kTpThreads) tp_scatter2_kernel(const uint32_t 
                                                                 uint32_t max_chunks, const uint32_t *__restrict__ hist2,
                                                                 const uint32_t *__restrict__ out_ptr, uint32_t uDim,
                                                                 uint32_t *__restrict__ out_idx,
-                                                                uint16_t *__restrict__ out_val, const uint32_t *gate) {
-    if (tp_gated_off(gate)) return;
+                                                                uint16_t *__restrict__ out_val) {
     extern __shared__ __align__(16) uint32_t tp_s2[];
     __shared__ uint32_t gbase[256];
     __shared__ uint32_t lb[257];
@@ -702,12 +672,9 @@ __global__ void __launch_bounds__(kTpThreads) tp_scatter2_kernel(const uint32_t 
 
 constexpr std::size_t kTpScatter2Smem = (std::size_t) kTpChunk * 6u + (std::size_t) 2u * kTpWarps * 256u * 2u;
 
-// With a gate, the path is the panel path's fallback: its kernels and scans
-// run only if the gate says so, and out_ptr (the column counts, scanned) is
-// already the panel path's.
 int transpose2_launch(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uint32_t *ptr, const uint32_t *idx,
                       const uint16_t *val, uint32_t *out_ptr, uint32_t *out_idx, uint16_t *out_val,
-                      const tp2_layout &l, cudaStream_t stream, const uint32_t *gate = nullptr) {
+                      const tp2_layout &l, cudaStream_t stream) {
     const std::size_t h1_smem = (std::size_t) l.K * 4u;
     const std::size_t s1_smem = tp_scatter1_smem(l.K);
     auto s1 = tp_scatter1_kernel;
@@ -717,401 +684,31 @@ int transpose2_launch(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uint32_t
                                       (int) kTpScatter2Smem),
                  "scatter2 smem attribute"))
         return 0;
-    tp_gran_rows_kernel<<<(cDim + 255u) / 256u, 256, 0, stream>>>(ptr, cDim, l.gran_row, gate);
+    tp_gran_rows_kernel<<<(cDim + 255u) / 256u, 256, 0, stream>>>(ptr, cDim, l.gran_row);
     if (!launch_ok("tp_gran_rows_kernel")) return 0;
-    tp_hist1_kernel<<<l.tiles1, kTpThreads, h1_smem, stream>>>(idx, nnz, uDim, l.K, l.tiles1, l.hist1, l.status, gate);
+    tp_hist1_kernel<<<l.tiles1, kTpThreads, h1_smem, stream>>>(idx, nnz, uDim, l.K, l.tiles1, l.hist1, l.status);
     if (!launch_ok("tp_hist1_kernel")) return 0;
-    if (!scan_exclusive_u32(l.hist1, l.hist1, (std::size_t) l.K * l.tiles1, true, l.scan_tmp, l.scan_bytes, stream,
-                            gate, kTqFallback))
+    if (!scan_exclusive_u32(l.hist1, l.hist1, (std::size_t) l.K * l.tiles1, true, l.scan_tmp, l.scan_bytes, stream))
         return 0;
     s1<<<l.tiles1, kTpThreads, s1_smem, stream>>>(ptr, idx, val, cDim, uDim, nnz, l.K, l.tiles1, l.hist1,
-                                                  l.gran_row, l.tmp_key, l.tmp_val, gate);
+                                                  l.gran_row, l.tmp_key, l.tmp_val);
     if (!launch_ok("tp_scatter1_kernel")) return 0;
     tp_chunks_kernel<<<1, 1024, 0, stream>>>(l.hist1, l.tiles1, l.K, l.max_chunks, l.chunk_bucket, l.chunk_begin,
-                                             l.chunk_end, l.chunk_first, gate);
+                                             l.chunk_end, l.chunk_first);
     if (!launch_ok("tp_chunks_kernel")) return 0;
     tp_hist2_kernel<<<l.max_chunks, kTpThreads, 0, stream>>>(l.tmp_key, l.chunk_begin, l.chunk_end, l.max_chunks,
-                                                             l.hist2, gate);
+                                                             l.hist2);
     if (!launch_ok("tp_hist2_kernel")) return 0;
     if (!scan_exclusive_u32(l.hist2, l.hist2, (std::size_t) 256u * l.max_chunks, true, l.scan_tmp, l.scan_bytes,
-                            stream, gate, kTqFallback))
+                            stream))
         return 0;
-    if (gate == nullptr) {
-        tp_colcount_kernel<<<l.K, 256, 0, stream>>>(l.hist2, l.max_chunks, l.chunk_first, uDim, out_ptr);
-        if (!launch_ok("tp_colcount_kernel")) return 0;
-        if (!scan_exclusive_u32(out_ptr, out_ptr, uDim, true, l.scan_tmp, l.scan_bytes, stream)) return 0;
-    }
+    tp_colcount_kernel<<<l.K, 256, 0, stream>>>(l.hist2, l.max_chunks, l.chunk_first, uDim, out_ptr);
+    if (!launch_ok("tp_colcount_kernel")) return 0;
+    if (!scan_exclusive_u32(out_ptr, out_ptr, uDim, true, l.scan_tmp, l.scan_bytes, stream)) return 0;
     tp_scatter2_kernel<<<l.max_chunks, kTpThreads, kTpScatter2Smem, stream>>>(l.tmp_key, l.tmp_val, l.chunk_bucket, l.chunk_begin,
                                                                 l.chunk_end, l.chunk_first, l.max_chunks, l.hist2,
-                                                                out_ptr, uDim, out_idx, out_val, gate);
+                                                                out_ptr, uDim, out_idx, out_val);
     return launch_ok("tp_scatter2_kernel");
-}
-
-// ---------------------------------------------------------------------------
-// Panel transpose (default where rows have strictly ascending columns).
-//
-// Rows are cut into tiles of <= 256 consecutive rows (8 warps x 32 rows) and
-// columns into panels of P (a power of two, chosen so a row holds about 20
-// entries per panel).  Three passes:
-//   count    one CTA per tile: per-column counts of the tile in shared memory
-//            (u16 pairs) -> hist[t][c]; also checks that every row's columns
-//            ascend strictly (else the two-pass path above runs instead).
-//   colscan  per column, exclusive prefix of hist over tiles and the column
-//            total; one device scan of the totals gives out_ptr.
-//   scatter  one CTA per tile walks the panels in order.  For each panel:
-//            (A) every warp loads the next 32 entries of each of its 32 rows
-//            at once (a row's panel entries are contiguous and come first)
-//            and counts them per (warp, column); (B) the counts become
-//            per-(warp, column) ranks and per-column staging offsets; (C) the
-//            entries are placed in shared memory grouped by column, in row
-//            order; (D) each column's run leaves as consecutive stores at
-//            out_ptr[c] + hist[t][c].  Placement depends on (tile, row) only:
-//            the result is the stable transpose, deterministic.
-// DRAM traffic: the column indices twice (count, scatter), the values once,
-// the CSC once, plus the tile histogram (tiles x cols u32 written, scanned,
-// read).
-// ---------------------------------------------------------------------------
-constexpr unsigned kTqWarps = 8;
-constexpr unsigned kTqThreads = kTqWarps * 32;
-constexpr unsigned kTqRowsPerWarp = 32;
-constexpr uint32_t kTqMaxTileRows = kTqWarps * kTqRowsPerWarp; // 256
-constexpr uint32_t kTqStage = 8192;                              // staged entries per (tile, panel)
-constexpr uint32_t kTqMaxPanel = 1024;
-constexpr uint32_t kTqMaxCols = 98304;                           // count pass: u16 pairs in 192 KB
-constexpr unsigned kTqCountThreads = 1024;
-
-struct tq_layout {
-    uint32_t *status; // [4]; status[0] gets CS_STATUS_* bits, status[1] kTqFallback
-    uint32_t *hist;   // [tiles * uDim]
-    void *scan_tmp;
-    std::size_t scan_bytes, bytes;
-    uint32_t tiles, tile_rows, panel;
-};
-
-// (the two-pass path must exist as the fallback)
-bool tq_applicable(uint32_t cDim, uint32_t uDim) { return uDim <= kTqMaxCols && tp2_applicable(cDim, uDim); }
-
-void tq_make_layout(uint32_t cDim, uint32_t uDim, uint32_t nnz, void *base, std::size_t cap, tq_layout *l) {
-    const uint32_t sms = (uint32_t) sm_count();
-    // tiles of up to 256 rows; at least two tiles per SM where the rows allow it
-    uint32_t tr = kTqMaxTileRows;
-    const uint32_t want = 2u * sms;
-    if (cDim / want < tr) tr = cDim / want;
-    if (tr < 1u) tr = 1u;
-    l->tile_rows = tr;
-    l->tiles = cDim == 0u ? 1u : (cDim + tr - 1u) / tr;
-    // panel: about 20 entries per (row, panel) on average
-    const double per_col = cDim == 0u || uDim == 0u ? 0.0 : (double) nnz / ((double) cDim * (double) uDim);
-    uint32_t P = 64u;
-    while (P < kTqMaxPanel && per_col * (double) (2u * P) <= 24.0) P <<= 1;
-    l->panel = P;
-    scratch_carver c(base, cap);
-    l->status = c.take<uint32_t>(4);
-    l->hist = c.take<uint32_t>((std::size_t) l->tiles * uDim + 1u);
-    l->scan_bytes = scan_u32_scratch_bytes(uDim);
-    l->scan_tmp = c.take<char>(l->scan_bytes);
-    l->bytes = c.used;
-}
-
-__global__ void __launch_bounds__(kTqCountThreads) tq_count_kernel(const uint32_t *__restrict__ ptr,
-                                                                   const uint32_t *__restrict__ idx, uint32_t cDim,
-                                                                   uint32_t uDim, uint32_t tile_rows,
-                                                                   uint32_t *__restrict__ hist, uint32_t *status) {
-    extern __shared__ uint32_t tq_h[]; // column c's count in the (c & 1) half of word c >> 1
-    const uint32_t words = (uDim + 1u) >> 1;
-    for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) tq_h[k] = 0u;
-    __syncthreads();
-    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
-    const uint32_t r0 = blockIdx.x * tile_rows, r1 = min(cDim, r0 + tile_rows);
-    uint32_t bad = 0u;
-    constexpr unsigned U = 4;
-    for (uint32_t r = r0 + warp; r < r1; r += nw) {
-        const uint32_t a = __ldg(ptr + r), e = __ldg(ptr + r + 1u);
-        uint32_t prev = 0u; // last column of the previous 32 entries (valid once i0 > a)
-        for (uint32_t i0 = a; i0 < e; i0 += U * 32u) {
-            uint32_t c[U];
-#pragma unroll
-            for (unsigned u = 0; u < U; ++u) {
-                const uint32_t i = i0 + u * 32u + lane;
-                c[u] = i < e ? __ldg(idx + i) : 0u;
-            }
-#pragma unroll
-            for (unsigned u = 0; u < U; ++u) {
-                const uint32_t i = i0 + u * 32u + lane;
-                uint32_t before = __shfl_up_sync(0xffffffffu, c[u], 1);
-                if (lane == 0u) before = prev;
-                if (i < e) {
-                    if (c[u] >= uDim)
-                        bad |= CS_STATUS_INDEX_RANGE;
-                    else
-                        atomicAdd(tq_h + (c[u] >> 1), 1u << ((c[u] & 1u) << 4));
-                    if (i > a && c[u] <= before) bad |= kTqFallback;
-                }
-                prev = __shfl_sync(0xffffffffu, c[u], 31);
-            }
-        }
-    }
-    __syncthreads();
-    uint32_t *hrow = hist + (std::size_t) blockIdx.x * uDim;
-    for (uint32_t k = threadIdx.x; k < uDim; k += blockDim.x) hrow[k] = (tq_h[k >> 1] >> ((k & 1u) << 4)) & 0xffffu;
-    if (bad & kTqFallback) atomicOr(status + 1, kTqFallback);
-    if (bad & ~kTqFallback) status_or(status, bad & ~kTqFallback);
-}
-
-// per column: exclusive prefix of hist over tiles (in place) and the total.
-// A block takes 32 columns; its 8 warps each scan one range of tiles.
-__global__ void __launch_bounds__(256) tq_colscan_kernel(uint32_t uDim, uint32_t tiles, uint32_t *__restrict__ hist,
-                                                         uint32_t *__restrict__ totals) {
-    __shared__ uint32_t seg[8][32];
-    const uint32_t cl = threadIdx.x & 31u, sg = threadIdx.x >> 5;
-    const uint32_t c = blockIdx.x * 32u + cl;
-    const uint32_t per = (tiles + 7u) / 8u;
-    const uint32_t t0 = min(tiles, sg * per), t1 = min(tiles, t0 + per);
-    uint32_t sum = 0u;
-    if (c < uDim) {
-        uint32_t t = t0;
-        for (; t + 4u <= t1; t += 4u) {
-            uint32_t v[4];
-#pragma unroll
-            for (unsigned u = 0; u < 4u; ++u) v[u] = hist[(std::size_t) (t + u) * uDim + c];
-            sum += v[0] + v[1] + v[2] + v[3];
-        }
-        for (; t < t1; ++t) sum += hist[(std::size_t) t * uDim + c];
-    }
-    seg[sg][cl] = sum;
-    __syncthreads();
-    uint32_t run = 0u;
-    for (uint32_t k = 0; k < sg; ++k) run += seg[k][cl];
-    if (c < uDim) {
-        for (uint32_t t = t0; t < t1; ++t) {
-            const std::size_t k = (std::size_t) t * uDim + c;
-            const uint32_t v = hist[k];
-            hist[k] = run;
-            run += v;
-        }
-        if (sg == 7u) totals[c] = run;
-    }
-}
-
-struct tq_smem {
-    uint32_t *st_key;  // [kTqStage] (row in tile << 16) | column in panel
-    uint16_t *st_val;  // [kTqStage]
-    uint16_t *cnt;     // [kTqWarps][P] counts, then ranks
-    uint32_t *colofs;  // [P + 1] staging offsets
-    uint32_t *gbase;   // [P] global slot of the tile's first entry per column
-    uint32_t *cursor;  // [kTqMaxTileRows] next entry of each row
-    uint32_t *rend;    // [kTqMaxTileRows]
-    uint16_t *seglen;  // [kTqMaxTileRows] the row's entries in this panel
-};
-
-__host__ __device__ inline std::size_t tq_scatter_smem(uint32_t P) {
-    return (std::size_t) kTqStage * 6u + (std::size_t) kTqWarps * P * 2u + ((std::size_t) 2u * P + 1u) * 4u +
-           (std::size_t) kTqMaxTileRows * 10u + 16u;
-}
-
-__global__ void __launch_bounds__(kTqThreads, 2) tq_scatter_kernel(
-    const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ idx, const uint16_t *__restrict__ val,
-    uint32_t cDim, uint32_t uDim, uint32_t tile_rows, uint32_t P, const uint32_t *__restrict__ hist,
-    const uint32_t *__restrict__ out_ptr, uint32_t *__restrict__ out_idx, uint16_t *__restrict__ out_val,
-    const uint32_t *status) {
-    if (status[1] & kTqFallback) return; // the two-pass path transposes this input
-    extern __shared__ __align__(16) unsigned char tq_raw[];
-    __shared__ uint32_t scan33[33];
-    __shared__ uint32_t staged;
-    tq_smem S;
-    S.st_key = reinterpret_cast<uint32_t *>(tq_raw);
-    S.st_val = reinterpret_cast<uint16_t *>(S.st_key + kTqStage);
-    S.cnt = S.st_val + kTqStage;
-    S.colofs = reinterpret_cast<uint32_t *>(S.cnt + kTqWarps * P);
-    S.gbase = S.colofs + P + 1u;
-    S.cursor = S.gbase + P;
-    S.rend = S.cursor + kTqMaxTileRows;
-    S.seglen = reinterpret_cast<uint16_t *>(S.rend + kTqMaxTileRows);
-    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t r0 = blockIdx.x * tile_rows;
-    if (r0 >= cDim) return;
-    const uint32_t nrows = min(tile_rows, cDim - r0);
-    for (uint32_t i = threadIdx.x; i < nrows; i += blockDim.x) {
-        S.cursor[i] = __ldg(ptr + r0 + i);
-        S.rend[i] = __ldg(ptr + r0 + i + 1u);
-    }
-    for (uint32_t k = threadIdx.x; k < kTqWarps * P; k += blockDim.x) S.cnt[k] = 0u;
-    __syncthreads();
-    const uint32_t *hrow = hist + (std::size_t) blockIdx.x * uDim;
-    uint16_t *my_cnt = S.cnt + warp * P;
-    const uint32_t panels = (uDim + P - 1u) / P;
-    for (uint32_t p = 0; p < panels; ++p) {
-        const uint32_t c0 = p * P, c1 = min(uDim, c0 + P);
-        // (A) count: the first 32 entries of every row of the warp in flight at once
-        {
-            uint32_t cc[kTqRowsPerWarp];
-#pragma unroll
-            for (unsigned j = 0; j < kTqRowsPerWarp; ++j) {
-                const uint32_t i = warp * kTqRowsPerWarp + j;
-                uint32_t c = 0xffffffffu;
-                if (i < nrows) {
-                    const uint32_t st = S.cursor[i] + lane;
-                    if (st < S.rend[i]) c = __ldg(idx + st);
-                }
-                cc[j] = c;
-            }
-#pragma unroll
-            for (unsigned j = 0; j < kTqRowsPerWarp; ++j) {
-                const uint32_t i = warp * kTqRowsPerWarp + j;
-                const bool in = cc[j] < c1;
-                const uint32_t n = __popc(__ballot_sync(0xffffffffu, in));
-                if (in) my_cnt[cc[j] - c0] += 1u;
-                uint32_t tot = n;
-                if (n == 32u) { // a row with more than 32 entries in this panel
-                    uint32_t st = S.cursor[i] + 32u;
-                    const uint32_t en = S.rend[i];
-                    for (;;) {
-                        __syncwarp();
-                        const uint32_t c = st + lane < en ? __ldg(idx + st + lane) : 0xffffffffu;
-                        const bool in2 = c < c1;
-                        const uint32_t n2 = __popc(__ballot_sync(0xffffffffu, in2));
-                        if (in2) my_cnt[c - c0] += 1u;
-                        tot += n2;
-                        if (n2 < 32u) break;
-                        st += 32u;
-                    }
-                }
-                if (lane == 0u && i < nrows) S.seglen[i] = (uint16_t) tot;
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        // (B) ranks per (warp, column), staging offsets per column, global bases
-        {
-            uint32_t tot[4], sum = 0u;
-#pragma unroll
-            for (unsigned q = 0; q < 4u; ++q) {
-                const uint32_t k = threadIdx.x * 4u + q;
-                uint32_t run = 0u;
-                if (k < P) {
-#pragma unroll
-                    for (unsigned w = 0; w < kTqWarps; ++w) {
-                        const uint32_t v = S.cnt[w * P + k];
-                        S.cnt[w * P + k] = (uint16_t) run;
-                        run += v;
-                    }
-                    S.gbase[k] = c0 + k < uDim ? __ldg(out_ptr + c0 + k) + __ldg(hrow + c0 + k) : 0u;
-                }
-                tot[q] = run;
-                sum += run;
-            }
-            uint32_t all;
-            uint32_t ex = block_exclusive_scan(sum, scan33, all);
-#pragma unroll
-            for (unsigned q = 0; q < 4u; ++q) {
-                const uint32_t k = threadIdx.x * 4u + q;
-                if (k < P) S.colofs[k] = ex;
-                ex += tot[q];
-            }
-            if (threadIdx.x == 0u) {
-                S.colofs[P] = all;
-                staged = all;
-            }
-        }
-        __syncthreads();
-        const bool direct = staged > kTqStage; // more entries than the stage holds: straight to the CSC
-        // (C) place, rows in order
-        {
-            uint32_t cc[kTqRowsPerWarp];
-            uint16_t vv[kTqRowsPerWarp];
-#pragma unroll
-            for (unsigned j = 0; j < kTqRowsPerWarp; ++j) {
-                const uint32_t i = warp * kTqRowsPerWarp + j;
-                uint32_t c = 0xffffffffu;
-                uint16_t v = 0u;
-                if (i < nrows && lane < S.seglen[i]) {
-                    const uint32_t st = S.cursor[i] + lane;
-                    c = __ldg(idx + st);
-                    v = __ldg(reinterpret_cast<const unsigned short *>(val) + st);
-                }
-                cc[j] = c;
-                vv[j] = v;
-            }
-#pragma unroll
-            for (unsigned j = 0; j < kTqRowsPerWarp; ++j) {
-                const uint32_t i = warp * kTqRowsPerWarp + j;
-                if (i >= nrows) break;
-                const uint32_t n = S.seglen[i];
-                if (cc[j] != 0xffffffffu) {
-                    const uint32_t k = cc[j] - c0;
-                    const uint32_t rk = my_cnt[k];
-                    my_cnt[k] = (uint16_t) (rk + 1u);
-                    if (!direct) {
-                        const uint32_t pos = S.colofs[k] + rk;
-                        S.st_key[pos] = (i << 16) | k;
-                        S.st_val[pos] = vv[j];
-                    } else {
-                        const uint32_t g = S.gbase[k] + rk;
-                        out_idx[g] = r0 + i;
-                        out_val[g] = vv[j];
-                    }
-                }
-                if (n > 32u) { // the rest of a long row segment
-                    for (uint32_t o = 32u; o < n; o += 32u) {
-                        __syncwarp();
-                        const uint32_t st = S.cursor[i] + o + lane;
-                        if (o + lane < n) {
-                            const uint32_t c = __ldg(idx + st);
-                            const uint16_t v = __ldg(reinterpret_cast<const unsigned short *>(val) + st);
-                            const uint32_t k = c - c0;
-                            const uint32_t rk = my_cnt[k];
-                            my_cnt[k] = (uint16_t) (rk + 1u);
-                            if (!direct) {
-                                const uint32_t pos = S.colofs[k] + rk;
-                                S.st_key[pos] = (i << 16) | k;
-                                S.st_val[pos] = v;
-                            } else {
-                                const uint32_t g = S.gbase[k] + rk;
-                                out_idx[g] = r0 + i;
-                                out_val[g] = v;
-                            }
-                        }
-                    }
-                }
-                __syncwarp();
-                if (lane == 0u) S.cursor[i] += n;
-            }
-        }
-        __syncthreads();
-        // (D) the staged runs leave column by column
-        if (!direct) {
-            const uint32_t total = staged;
-            for (uint32_t j = threadIdx.x; j < total; j += blockDim.x) {
-                const uint32_t key = S.st_key[j];
-                const uint32_t k = key & 0xffffu;
-                const uint32_t g = S.gbase[k] + (j - S.colofs[k]);
-                out_idx[g] = r0 + (key >> 16);
-                out_val[g] = S.st_val[j];
-            }
-        }
-        for (uint32_t k = threadIdx.x; k < kTqWarps * P; k += blockDim.x) S.cnt[k] = 0u;
-        __syncthreads();
-    }
-}
-
-int transpose_panel_launch(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uint32_t *ptr, const uint32_t *idx,
-                           const uint16_t *val, uint32_t *out_ptr, uint32_t *out_idx, uint16_t *out_val,
-                           const tq_layout &l, cudaStream_t stream) {
-    const std::size_t csmem = (std::size_t) ((uDim + 1u) >> 1) * 4u;
-    const std::size_t ssmem = tq_scatter_smem(l.panel);
-    if (!cuda_ok(cudaFuncSetAttribute(tq_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) csmem),
-                 "tq count smem attribute") ||
-        !cuda_ok(cudaFuncSetAttribute(tq_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) ssmem),
-                 "tq scatter smem attribute"))
-        return 0;
-    tq_count_kernel<<<l.tiles, kTqCountThreads, csmem, stream>>>(ptr, idx, cDim, uDim, l.tile_rows, l.hist, l.status);
-    if (!launch_ok("tq_count_kernel")) return 0;
-    tq_colscan_kernel<<<(uDim + 31u) / 32u, 256, 0, stream>>>(uDim, l.tiles, l.hist, out_ptr);
-    if (!launch_ok("tq_colscan_kernel")) return 0;
-    if (!scan_exclusive_u32(out_ptr, out_ptr, uDim, true, l.scan_tmp, l.scan_bytes, stream)) return 0;
-    tq_scatter_kernel<<<l.tiles, kTqThreads, ssmem, stream>>>(ptr, idx, val, cDim, uDim, l.tile_rows, l.panel, l.hist,
-                                                             out_ptr, out_idx, out_val, l.status);
-    return launch_ok("tq_scatter_kernel");
 }
 
 } // namespace
@@ -1119,30 +716,6 @@ int transpose_panel_launch(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uin
 int transpose_launch(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uint32_t *ptr, const uint32_t *idx,
                      const uint16_t *val, uint32_t *out_ptr, uint32_t *out_idx, uint16_t *out_val, void *scratch,
                      std::size_t scratch_bytes, cudaStream_t stream) {
-    if (tq_applicable(cDim, uDim)) {
-        // the panel path, and the two-pass path behind it for rows whose columns
-        // do not ascend strictly (decided on the device by the count pass)
-        tq_layout lq;
-        tq_make_layout(cDim, uDim, nnz, scratch, scratch_bytes, &lq);
-        // the fallback's scratch follows on a 256-byte boundary
-        const std::size_t q = align_up(lq.bytes, 256);
-        tp2_layout l2;
-        tp2_make_layout(cDim, uDim, nnz, scratch != nullptr ? static_cast<char *>(scratch) + q : nullptr,
-                        scratch_bytes > q ? scratch_bytes - q : 0u, &l2);
-        const std::size_t need = q + l2.bytes;
-        if (scratch == nullptr || need > scratch_bytes) {
-            set_error("compressed_transpose: scratch %zu < %zu bytes", scratch_bytes, need);
-            return 0;
-        }
-        if (!cuda_ok(cudaMemsetAsync(lq.status, 0, 16, stream), "transpose status memset") ||
-            !cuda_ok(cudaMemsetAsync(out_ptr, 0, ((std::size_t) uDim + 1u) * 4u, stream), "transpose out_ptr memset"))
-            return 0;
-        if (nnz == 0u || cDim == 0u || uDim == 0u) return 1;
-        if (!transpose_panel_launch(cDim, uDim, nnz, ptr, idx, val, out_ptr, out_idx, out_val, lq, stream)) return 0;
-        l2.status = lq.status; // one status word for the caller
-        return transpose2_launch(cDim, uDim, nnz, ptr, idx, val, out_ptr, out_idx, out_val, l2, stream,
-                                 lq.status + 1);
-    }
     if (tp2_applicable(cDim, uDim)) {
         tp2_layout l2;
         tp2_make_layout(cDim, uDim, nnz, scratch, scratch_bytes, &l2);
@@ -1184,13 +757,6 @@ int transpose_launch(uint32_t cDim, uint32_t uDim, uint32_t nnz, const uint32_t 
 }
 
 std::size_t transpose_scratch(uint32_t cDim, uint32_t uDim, uint32_t nnz) {
-    if (tq_applicable(cDim, uDim)) {
-        tq_layout lq;
-        tq_make_layout(cDim, uDim, nnz, nullptr, 0, &lq);
-        tp2_layout l2;
-        tp2_make_layout(cDim, uDim, nnz, nullptr, 0, &l2);
-        return align_up(lq.bytes, 256) + l2.bytes;
-    }
     if (tp2_applicable(cDim, uDim)) {
         tp2_layout l2;
         tp2_make_layout(cDim, uDim, nnz, nullptr, 0, &l2);
