@@ -46,6 +46,7 @@ GROUPS = 64
 KEEP_FRAC = 0.7
 KEPT_FEATURES = 20_000
 BLOCK = 16
+BELL_CPU_ROWS = 1024  # rows per Blocked-ELL partition of the CPU baselines (64 MB of values at 32,768 columns)
 FALLBACK_HBM_GBS = 6650.0
 # launches per step: tile hist, group tiles, group scan, tile scatter, accumulate, combine (the
 # column-block index is built once when the partition is staged)
@@ -525,7 +526,7 @@ def bucket_cpu_baseline(bell, sell, chosen: int, seconds: float = 10.0):
     return {"value": rows / dt, "unit": "rows/s", "cores": 1, "kind": "reference", "sample": sample}
 
 
-def bucket_lines(lib, timed, emit, bell, sell):
+def bucket_lines(lib, timed, emit, bell, sell, no_cpu=False):
     """Execution bucketing lines: the plan (counts, sort, cuts, choice of 1..8 buckets;
     ends with one small device->host read) and the fill, timed separately; the fill's
     algorithmic bytes are the source's index array, its valid values, the segments
@@ -579,11 +580,13 @@ def bucket_lines(lib, timed, emit, bell, sell):
     ms_plan = timed(plan_fn)
     extra = {"segments": plan.segment_count, "bucket_count": plan.bucket_count, "bytes": plan.bytes,
              "original_bytes": plan.original_bytes}
-    emit(name + "_plan", ms_plan, 0, dict(extra, note="time only: counts, stable sort, cuts and the 1..8 choice, "
-                                                      "one device->host read"))
+    cpu = None if no_cpu else bucket_cpu_baseline(bell, sell, plan.bucket_count)
+    ex = dict(extra, note="time only: counts, stable sort, cuts and the 1..8 choice, one device->host read")
+    if cpu is not None:
+        ex["cpu_baseline"] = dict(cpu, note="the reference's builder plans and fills in one routine")
+    emit(name + "_plan", ms_plan, 0, ex)
     _abi.check(fill_fn(), "bucketed fill")
     ms_fill = timed(fill_fn)
-    cpu = bucket_cpu_baseline(bell, sell, plan.bucket_count)
     ex = dict(extra, rows_per_s=R / ((ms_plan + ms_fill) * 1e-3), cols=cols)
     if cpu is not None:
         ex["cpu_baseline"] = cpu
@@ -592,7 +595,7 @@ def bucket_lines(lib, timed, emit, bell, sell):
     torch.cuda.empty_cache()
 
 
-def coo_lines(lib, timed, emit, csr):
+def coo_lines(lib, timed, emit, csr, no_cpu=False):
     """COO -> Blocked-ELL-16 of the same matrix held as row-major COO: the plan (column
     scan, keys, the stable radix sort, group heads and scans; two small device->host
     reads) and the emit (block columns, zeroed values, one thread per block group),
@@ -628,26 +631,35 @@ def coo_lines(lib, timed, emit, csr):
     emit_fn = lambda: lib.cs_b200_coo_blocked_ell_emit(C.byref(v), None, Cc, ptr(scr), nb.value, C.byref(dv),
                                                        ptr(nnz), stream_handle())
     ms_plan = timed(plan_fn)
-    emit("coo_blocked_ell_plan", ms_plan, 0, {"ell_cols": W * BLOCK, "total_blocks": total.value,
-                                              "note": "time only: scan, keys, stable radix sort, heads, scans, "
-                                                      "two device->host reads"})
     ms_emit = timed(emit_fn)
-    cpu = None
+    cpu = cpu_u = None
     from oracle import oracle
 
-    if oracle.ref_available():
-        # the reference's host routine on the first rows (about 5 M entries)
+    if oracle.ref_available() and not no_cpu:
+        # the reference's host routine on the first rows (about 5 M entries), in row order and shuffled
         S = int(torch.searchsorted(csr.ptr.long(), torch.tensor([5_000_000], device="cuda")).item())
         S = max(1, min(R, S))
         m = int(csr.ptr[S].item())
         hr, hc, hv = row[:m].cpu().numpy().view(np.uint32), csr.idx[:m].cpu().numpy().view(np.uint32), \
             csr.val[:m].cpu().numpy().view(np.uint16)
-        t0, k = time.perf_counter(), 0
-        while k < 3 and (k == 0 or time.perf_counter() - t0 < 10.0):
-            oracle.ref_blocked_ell_from_coo(S, Cc, Cc, hr, hc, hv, BLOCK)
-            k += 1
-        cpu = {"value": S / ((time.perf_counter() - t0) / k), "unit": "rows/s", "cores": 1, "kind": "reference",
+
+        def ref_rate(hr, hc, hv):
+            t0, k = time.perf_counter(), 0
+            while k < 3 and (k == 0 or time.perf_counter() - t0 < 10.0):
+                oracle.ref_blocked_ell_from_coo(S, Cc, Cc, hr, hc, hv, BLOCK)
+                k += 1
+            return S / ((time.perf_counter() - t0) / k)
+
+        cpu = {"value": ref_rate(hr, hc, hv), "unit": "rows/s", "cores": 1, "kind": "reference",
                "sample": f"first {S} rows ({m} entries), convert::blocked_ell_from_coo (host loops)"}
+        sh = np.random.default_rng(7).permutation(m)
+        cpu_u = {"value": ref_rate(hr[sh], hc[sh], hv[sh]), "unit": "rows/s", "cores": 1, "kind": "reference",
+                 "sample": f"first {S} rows ({m} entries) in random order, convert::blocked_ell_from_coo (host loops)"}
+    ex = {"ell_cols": W * BLOCK, "total_blocks": total.value,
+          "note": "time only: scan, keys, stable radix sort, heads, scans, two device->host reads"}
+    if cpu is not None:
+        ex["cpu_baseline"] = dict(cpu, note="the reference converts in one routine (no separate plan)")
+    emit("coo_blocked_ell_plan", ms_plan, 0, ex)
     ex = {"ell_cols": W * BLOCK, "rows_per_s": R / ((ms_plan + ms_emit) * 1e-3)}
     if cpu is not None:
         ex["cpu_baseline"] = cpu
@@ -660,9 +672,11 @@ def coo_lines(lib, timed, emit, csr):
     v.rowIdx, v.colIdx, v.val = ptr(row_s), ptr(col_s), ptr(val_s)
     ms_plan_u = timed(plan_fn)
     ms_emit_u = timed(emit_fn)
-    emit("coo_blocked_ell_unordered", ms_plan_u + ms_emit_u, 0,
-         {"plan_ms": ms_plan_u, "emit_ms": ms_emit_u, "rows_per_s": R / ((ms_plan_u + ms_emit_u) * 1e-3),
-          "note": "entries shuffled: stable radix sort by row + gather, then the CSR route; time only"})
+    ex = {"plan_ms": ms_plan_u, "emit_ms": ms_emit_u, "rows_per_s": R / ((ms_plan_u + ms_emit_u) * 1e-3),
+          "note": "entries shuffled: stable radix sort by row + gather, then the CSR route; time only"}
+    if cpu_u is not None:
+        ex["cpu_baseline"] = cpu_u
+    emit("coo_blocked_ell_unordered", ms_plan_u + ms_emit_u, 0, ex)
     del row, scr, bci, val, row_s, col_s, val_s
 
 
@@ -672,6 +686,41 @@ def host_csr_rows(csr, r0: int, r1: int):
     ptr = (csr.ptr[r0:r1 + 1].long() - a).to(dtype=__import__("torch").int32).cpu().numpy().view(np.uint32)
     return (r1 - r0, csr.cols, ptr, csr.idx[a:b].cpu().numpy().view(np.uint32),
             csr.val[a:b].cpu().numpy().view(np.uint16))
+
+
+def host_bell_rows(bell, r0: int, r1: int):
+    """(rows, cols, B, ell_cols, bci, val) numpy copy of Blocked-ELL rows [r0, r1); r0 a multiple of the block size."""
+    B, W = bell.block_size, bell.ell_width
+    b0, b1 = r0 // B, (r1 + B - 1) // B
+    return (r1 - r0, bell.cols, B, bell.ell_cols, bell.bci[b0 * W:b1 * W].cpu().numpy().view(np.uint32),
+            bell.val[r0 * bell.ell_cols:r1 * bell.ell_cols].cpu().numpy().view(np.uint16))
+
+
+def bell_cpu_baseline(bell, rows_per_part: int, run, seconds: float, what: str, kind: str, extra=None):
+    """CPU baseline over Blocked-ELL partitions of `rows_per_part` rows: one partition on
+    one thread and one partition per host core on all cores; `extra(r0, r1)` appends
+    per-partition arguments (masks).  Units: stored nnz of the sample per second."""
+    from oracle import oracle
+
+    n = oracle.cpu_count()
+    B = bell.block_size
+    rpp = max(B, min(rows_per_part, bell.rows) // B * B)
+
+    def part(k):
+        r0, r1 = k * rpp, min(bell.rows, (k + 1) * rpp)
+        return host_bell_rows(bell, r0, r1) + (tuple(extra(r0, r1)) if extra else ())
+
+    many = [part(k) for k in range(n) if k * rpp < bell.rows]
+    one = many[:1]
+    live = lambda ps: sum(int(np.count_nonzero(q[5] & 0x7fff)) for q in ps)
+    nnz1, nnzn = live(one), live(many)
+    t1, p1 = run(one, 1, seconds)
+    tn, pn = run(many, n, seconds)
+    return {"value": nnzn / tn, "unit": "nnz/s", "cores": n, "kind": kind,
+            "sample": f"{len(many)} partitions of {rpp} rows ({nnzn} stored nnz) on {n} host threads, mean of {pn} "
+                      f"passes: {what}",
+            "one_thread": {"value": nnz1 / t1, "unit": "nnz/s", "cores": 1,
+                           "sample": f"one partition of {rpp} rows ({nnz1} stored nnz), mean of {p1} passes"}}
 
 
 def conversion_cpu_baseline(csr, rows_per_part: int, run, seconds: float, what: str, kind: str = "reference"):
@@ -781,7 +830,13 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     shape_t = torch.zeros(2, dtype=torch.int64, device="cuda")
     ms_shape = timed(lambda: lib.cs_b200_blocked_ell_shape(C.byref(v), B, ptr(shape_t), ptr(scratch), scratch.numel(),
                                                            ptr(status), stream_handle()))
-    emit("blocked_ell_shape", ms_shape, 4 * (R + 1) + 4 * nnz)
+    conv_cpu = None
+    if ref_ok:
+        conv_cpu = conversion_cpu_baseline(
+            csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_blocked_ell_from_compressed(parts, B, th, sec), secs,
+            "the reference's convert::blocked_ell_from_compressed (block 16) compiled from its sources")
+    whole = lambda: dict(conv_cpu, note="the whole conversion (the reference has no separate shape pass)")
+    emit("blocked_ell_shape", ms_shape, 4 * (R + 1) + 4 * nnz, {"cpu_baseline": whole()} if conv_cpu else None)
     dv = bell.view()
     nnz_t = torch.zeros(1, dtype=torch.int32, device="cuda")
     ms_emit = timed(lambda: lib.cs_b200_blocked_ell_emit(C.byref(v), C.byref(dv), ptr(nnz_t), ptr(scratch),
@@ -789,18 +844,18 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     ex = {"ell_cols": bell.ell_cols, "shape_ms": ms_shape,
           "conversion_ms": ms_shape + ms_emit,
           "note": "emit only; shape_ms is the bitmap / width pass the emit needs (conversion = both)"}
-    if ref_ok:
-        ex["cpu_baseline"] = conversion_cpu_baseline(
-            csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_blocked_ell_from_compressed(parts, B, th, sec), secs,
-            "the reference's convert::blocked_ell_from_compressed (block 16) compiled from its sources")
+    if conv_cpu:
+        ex["cpu_baseline"] = conv_cpu
     bell_bytes_alg = 4 * (R + 1) + 6 * nnz + R * bell.ell_cols * 2 + rb * width * 4
     emit("blocked_ell_emit", ms_emit, bell_bytes_alg, ex)
     # the whole conversion through the public call, warm (shape, one read of the width, the output
     # from the allocator's cache, emit, status read): what a caller converting repeatedly sees
     ms_api = timed(lambda: blocked_ell_from_csr(csr, B))
-    emit("blocked_ell_from_csr_api", ms_api, bell_bytes_alg,
-         {"ell_cols": bell.ell_cols, "note": "device.blocked_ell_from_csr end to end on device data, warm; bytes "
-                                             "as the emit's (the shape pass's read of the indices is not credited)"})
+    ex = {"ell_cols": bell.ell_cols, "note": "device.blocked_ell_from_csr end to end on device data, warm; bytes "
+                                            "as the emit's (the shape pass's read of the indices is not credited)"}
+    if conv_cpu:
+        ex["cpu_baseline"] = whole()
+    emit("blocked_ell_from_csr_api", ms_api, bell_bytes_alg, ex)
     # Blocked-ELL -> Sliced-ELL (h 32): live-entry row pointers (count + scan), then the emit;
     # both read the whole value array (the layout needs every row's count before any slot)
     from cellshard_b200.device import blocked_ell_row_ptr, sliced_ell_from_blocked_ell
@@ -813,13 +868,22 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     rp = torch.empty(R + 1, dtype=torch.int32, device="cuda")
     ms_rp = timed(lambda: lib.cs_b200_blocked_ell_row_ptr(C.byref(bv), ptr(rp), ptr(rscr), rbytes.value,
                                                           stream_handle()))
-    emit("blocked_ell_row_ptr", ms_rp, bell_bytes + 4 * (R + 1))
+    b2s_cpu = None
+    if ref_ok:
+        b2s_cpu = bell_cpu_baseline(
+            bell, BELL_CPU_ROWS, lambda parts, th, sec: oracle.ref_time_sliced_ell_from_blocked_ell(parts, 32, th, sec),
+            secs, "the reference's convert::sliced_ell_from_blocked_ell (h 32) compiled from its sources",
+            "reference")
+    ex = {"cpu_baseline": dict(b2s_cpu, note="the whole conversion (row pointers and emit)")} if b2s_cpu else None
+    emit("blocked_ell_row_ptr", ms_rp, bell_bytes + 4 * (R + 1), ex)
     sfb = sliced_ell_from_blocked_ell(bell, 32)
     sfv = sfb.view()
     total_fb = int(sfb.col_idx.numel())
     ms_sfb = timed(lambda: lib.cs_b200_sliced_ell_emit_from_blocked_ell(C.byref(bv), C.byref(sfv), stream_handle()))
-    emit("sliced_ell_emit_from_blocked_ell", ms_sfb, bell_bytes + 6 * total_fb + 4 * (2 * sfb.slice_count + 1),
-         {"total_slots": total_fb})
+    ex = {"total_slots": total_fb}
+    if b2s_cpu:
+        ex["cpu_baseline"] = dict(b2s_cpu, note="the whole conversion (row pointers and emit)")
+    emit("sliced_ell_emit_from_blocked_ell", ms_sfb, bell_bytes + 6 * total_fb + 4 * (2 * sfb.slice_count + 1), ex)
     del sfb, rscr, rp
     torch.cuda.empty_cache()
     # filtered Blocked-ELL -> CSR (70 % rows, 60 % features kept) and the whole repack
@@ -833,23 +897,44 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     filt_csr, fstats = runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk)
     del filt_csr
     filt_bytes = 2 * int(rk_h.sum()) * bell.ell_cols + rb * width * 4 + R + Cc + 4 * (R + 1) + 6 * fstats["live_nnz"]
+    fk_h = fk.cpu().numpy()
+    masks = lambda r0, r1: (rk_h[r0:r1].astype(np.uint8), fk_h)
+    filt_cpu = repack_cpu = None
+    if not args.no_cpu_baseline:
+        filt_cpu = bell_cpu_baseline(
+            bell, BELL_CPU_ROWS, lambda parts, th, sec: oracle.time_filter_bell(parts, th, sec), secs,
+            "restated filtered Blocked-ELL -> CSR (oracle/cs_oracle.c; the reference filters on the GPU only)",
+            "port", masks)
+        if ref_ok:
+            repack_cpu = bell_cpu_baseline(
+                bell, BELL_CPU_ROWS, lambda parts, th, sec: oracle.time_repack_bell(parts, BLOCK, 64, th, sec), secs,
+                "restated filter, nnz plan (64 buckets) and rebuild, then the reference's "
+                "convert::blocked_ell_from_compressed (block 16)", "port", masks)
     ms_f = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk, method="onepass"))
-    emit("filter_blocked_ell_to_compressed", ms_f, filt_bytes,
-         {"live_nnz": fstats["live_nnz"], "note": "one pass: count, look-back over rows, emit from L2, then one host "
-                                                  "read of the live nnz; bytes are the kept rows' values, tables, row "
-                                                  "pointers and the CSR written"})
+    ex = {"live_nnz": fstats["live_nnz"],
+          "note": "one pass: each row counted, placed by a look-back over rows and written from L2, then one "
+                  "host read of the live nnz; bytes are the kept rows' values, tables, row pointers and the CSR "
+                  "written"}
+    if filt_cpu:
+        ex["cpu_baseline"] = filt_cpu
+    emit("filter_blocked_ell_to_compressed", ms_f, filt_bytes, ex)
     ms_f2 = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk, method="two_pass"))
-    emit("filter_blocked_ell_count_emit", ms_f2, filt_bytes,
-         {"live_nnz": fstats["live_nnz"], "note": "the count + emit route (remaps, other block sizes): both passes "
-                                                  "read the kept rows' values"})
+    ex = {"live_nnz": fstats["live_nnz"], "note": "the count + emit route (remaps, other block sizes): both passes "
+                                                  "read the kept rows' values"}
+    if filt_cpu:
+        ex["cpu_baseline"] = filt_cpu
+    emit("filter_blocked_ell_count_emit", ms_f2, filt_bytes, ex)
     ms_rp2 = timed(lambda: runtime.build_repacked_blocked_ell([bell], R, Cc, BLOCK, 64, rk, fk))
-    emit("repack_blocked_ell", ms_rp2, 0, {"note": "filter + nnz plan + rebuild + CSR -> Blocked-ELL-16 with host "
-                                                   "reads of sizes between stages; time only"})
+    ex = {"note": "filter + nnz plan + rebuild + CSR -> Blocked-ELL-16 with host reads of sizes between stages; "
+                  "time only"}
+    if repack_cpu:
+        ex["cpu_baseline"] = repack_cpu
+    emit("repack_blocked_ell", ms_rp2, 0, ex)
     # execution bucketing of the Blocked-ELL-16 (bucket count chosen in 1..8, then the fill)
-    bucket_lines(lib, timed, emit, bell, None)
+    bucket_lines(lib, timed, emit, bell, None, args.no_cpu_baseline)
     del bell
     torch.cuda.empty_cache()
-    coo_lines(lib, timed, emit, csr)
+    coo_lines(lib, timed, emit, csr, args.no_cpu_baseline)
     torch.cuda.empty_cache()
     # Sliced-ELL at h = 32: the whole conversion (layout + emit, device only, into arrays sized
     # by a first run) and the emit alone; the slice-height candidates (16 / 32 / 64) of the chooser
@@ -878,8 +963,12 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
             csr, cpu_rows, lambda parts, th, sec: oracle.ref_time_sliced_ell_from_compressed(parts, 32, th, sec), secs,
             "the reference's convert::sliced_ell_from_compressed (h 32) compiled from its sources")
     emit("sliced_ell_from_csr", ms_full, sell_bytes, ex)
+    sell_cpu = ex.get("cpu_baseline")
     ms_sell = timed(lambda: lib.cs_b200_sliced_ell_emit(C.byref(v), C.byref(sv), stream_handle()))
-    emit("sliced_ell_emit", ms_sell, sell_bytes, {"total_slots": total})
+    ex = {"total_slots": total}
+    if sell_cpu:
+        ex["cpu_baseline"] = dict(sell_cpu, note="the whole conversion (the reference has no separate layout pass)")
+    emit("sliced_ell_emit", ms_sell, sell_bytes, ex)
     cands = (C.c_uint32 * 3)(16, 32, 64)
     padded = torch.zeros(3, dtype=torch.int64, device="cuda")
     ms_c = timed(lambda: lib.cs_b200_sliced_ell_candidates(C.byref(v), cands, 3, ptr(padded), stream_handle()))
@@ -892,7 +981,7 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
             "the reference's choose_sliced_ell_slice_rows_from_compressed (16 / 32 / 64) + "
             "sliced_ell_from_compressed at its choice")
     emit("sliced_ell_candidates", ms_c, 4 * (R + 1), ex)
-    bucket_lines(lib, timed, emit, None, sell)
+    bucket_lines(lib, timed, emit, None, sell, args.no_cpu_baseline)
     del sell, sscr
     torch.cuda.empty_cache()
     # transpose
@@ -928,7 +1017,13 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     emit("nnz_plan", ms_p, 4 * (R + 1) + 12 * R + 4 * 65, ex)
     plan = major_nnz_plan(csr.ptr, R, 64)
     ms_r = timed(lambda: rebuild_major_order(csr, plan["order"]))
-    emit("rebuild", ms_r, 6 * nnz + 4 * (R + 1) + 6 * nnz + 4 * (R + 1) + 4 * R)
+    ex = {}
+    if not args.no_cpu_baseline:
+        ex["cpu_baseline"] = conversion_cpu_baseline(
+            csr, cpu_rows, lambda parts, th, sec: oracle.time_rebuild(parts, th, sec), secs,
+            "restated row rebuild in nnz-plan order (oracle/cs_oracle.c; the reference rebuilds on the GPU only)",
+            kind="port")
+    emit("rebuild", ms_r, 6 * nnz + 4 * (R + 1) + 6 * nnz + 4 * (R + 1) + 4 * R, ex)
 
 
 def run_mask_groups(args):

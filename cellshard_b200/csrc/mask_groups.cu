@@ -785,6 +785,13 @@ constexpr unsigned kPipeSlots = 8;
 constexpr unsigned kPipeRowStride = kPipeSlots * 32u + 32u;
 constexpr unsigned kPipeStageBytes = 16u * kPipeRowStride;
 constexpr unsigned kPipeStages = 2;
+constexpr unsigned kPipePieces = kPipeSlots * 2u;     // 16-byte pieces of one row of a stage
+constexpr unsigned kPipeRowsPerCopy = 32u / kPipePieces; // stage rows one copy instruction covers
+constexpr unsigned kPipeStagesPerWindow = 32u / kPipeSlots; // stages per 32-slot window of block columns
+static_assert(kPipeSlots >= 2u && kPipeSlots <= 16u && (kPipeSlots & (kPipeSlots - 1u)) == 0u,
+              "a stage holds 2, 4, 8 or 16 slots");
+static_assert(kPipeStages * kPipeStageBytes >= 16u * 32u * sizeof(float) + kStagePairs * 8u,
+              "the per-row fallback's accumulators and pairs fit in a warp's stage buffers");
 
 template <unsigned STAGES>
 constexpr std::size_t pipe_warp_bytes() { return (std::size_t) STAGES * kPipeStageBytes; }
@@ -836,22 +843,23 @@ __global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_k
         if (keep16 != 0u) {
             const uint32_t *bci = src.blockColIdx + (std::size_t) rb * W;
             // rows the mask drops are never copied: zero them in every stage once
-            for (unsigned i = lane; i < STAGES * 16u * 16u; i += 32u) {
-                const unsigned r = (i >> 4) & 15u;
+            for (unsigned i = lane; i < STAGES * 16u * kPipePieces; i += 32u) {
+                const unsigned r = (i / kPipePieces) % 16u;
                 if (!((keep16 >> r) & 1u))
-                    *reinterpret_cast<uint4 *>(buf + (i >> 8) * kPipeStageBytes + r * RS + (i & 15u) * 16u) =
-                        make_uint4(0u, 0u, 0u, 0u);
+                    *reinterpret_cast<uint4 *>(buf + (i / (16u * kPipePieces)) * kPipeStageBytes + r * RS +
+                                               (i % kPipePieces) * 16u) = make_uint4(0u, 0u, 0u, 0u);
             }
-            // this lane's copies: 16-byte piece (lane & 15) of stage rows (lane >> 4) + 2i
-            const unsigned piece = lane & 15u;
+            // this lane's copies: 16-byte piece (lane % kPipePieces) of stage rows
+            // lane / kPipePieces + kPipeRowsPerCopy * i
+            const unsigned piece = lane % kPipePieces;
             const uint16_t *gsrc = src.val + (std::size_t) rb * 16u * src.ell_cols + piece * 8u;
             auto issue = [&](uint32_t k) {
                 if (k < nstages && k * kPipeSlots + piece / 2u < W) {
                     unsigned char *dst = buf + (k % STAGES) * kPipeStageBytes + piece * 16u;
                     const uint16_t *from = gsrc + (std::size_t) k * kPipeSlots * 16u;
 #pragma unroll
-                    for (unsigned i = 0; i < 8u; ++i) {
-                        const unsigned r = (lane >> 4) + 2u * i;
+                    for (unsigned i = 0; i < 16u / kPipeRowsPerCopy; ++i) {
+                        const unsigned r = lane / kPipePieces + kPipeRowsPerCopy * i;
                         if ((keep16 >> r) & 1u) cp_async_16(dst + r * RS, from + (std::size_t) r * src.ell_cols);
                     }
                 }
@@ -868,14 +876,15 @@ __global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_k
                 __syncwarp();
                 const unsigned char *sb = buf + (k % STAGES) * kPipeStageBytes + 8u * t;
                 const uint32_t nslots = min(kPipeSlots, W - k * kPipeSlots);
-                if (k % 4u == 0u && k != 0u) {
+                if (k % kPipeStagesPerWindow == 0u && k != 0u) {
                     my_bc = next_bc;
                     const uint32_t s = k * kPipeSlots + 32u + lane;
                     next_bc = s < W ? __ldg(bci + s) : CS_INVALID_COL;
                 }
 #pragma unroll
                 for (unsigned j = 0; j < kPipeSlots; ++j) {
-                    const uint32_t bc = __shfl_sync(0xffffffffu, my_bc, ((k % 4u) * kPipeSlots + j) & 31u);
+                    const uint32_t bc =
+                        __shfl_sync(0xffffffffu, my_bc, ((k % kPipeStagesPerWindow) * kPipeSlots + j) & 31u);
                     if (j >= nslots || bc >= col_blocks) continue; // warp-uniform (padding or outside)
                     // this lane's 4 columns: two u16 entries per word (columns 4t, 4t+1 and 4t+2, 4t+3)
                     const uint2 te = *reinterpret_cast<const uint2 *>(table + bc * 16u + 4u * t);
@@ -1153,21 +1162,45 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
 // ---------------------------------------------------------------------------
 // One-pass filter: count, decoupled look-back over rows, emit while the row's
 // values are still in L2.  Rows are claimed in order from a global counter by
-// resident warps, so every row a warp waits for is held by a running warp.
+// resident CTAs, so every row a CTA waits for is held by a running CTA.
 // row_state[r]: (flag << 32) | value, flag 1 = the row's count, 2 = the
-// inclusive prefix through the row.
+// inclusive prefix through the row.  The state word is all a reader needs, so
+// it is published and read with relaxed 64-bit accesses (no fence).
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kLbCount = 1ull << 32, kLbPrefix = 2ull << 32;
 constexpr uint32_t kLbSpinLimit = 1u << 22; // ~0.3 s of 64 ns sleeps
 
 __device__ __forceinline__ unsigned long long lb_load(const unsigned long long *p) {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
 __device__ __forceinline__ void lb_store(unsigned long long *p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// 16-byte value loads with an L2 eviction priority (createpolicy): the count
+// pass marks a row's values evict_last so they stay in L2 for the emit's
+// re-read, which marks them evict_first again.
+__device__ __forceinline__ unsigned long long l2_evict_last_policy() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ unsigned long long l2_evict_first_policy() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ uint4 ld_policy_v4(const void *p, unsigned long long pol) {
+    uint4 r;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(p), "l"(pol));
+    return r;
 }
 
 // Kept entries among the 8 values of one vector (no feature remap).
@@ -1179,15 +1212,16 @@ __device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, ui
 }
 
 // One CTA per row at a time (rows claimed in order): the row's values are read
-// once to count, and read again from L2 to emit -- with a few CTAs per SM the
-// rows in flight stay well inside L2.  Each thread owns kOpVecs consecutive
+// once to count, and read again from L2 to emit -- the count's loads mark them
+// evict_last, and the rows in flight (a few CTAs per SM) stay well inside L2.  Each thread owns kOpVecs consecutive
 // 16-byte vectors of a 256 x kOpVecs-vector step, so one block scan per step
 // gives every thread its output position in slot order.
 constexpr unsigned kOpThreads = 256;
 constexpr unsigned kOpVecs = 4;
-constexpr unsigned kOpCtasPerSm = 3;
+constexpr unsigned kOpCtasPerSm = 5;
+constexpr bool kOpPrefetch = false; // the next step's loads issued before this step's work
 
-__global__ void __launch_bounds__(kOpThreads) filter_onepass_kernel(
+__global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kernel(
     const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
     uint32_t *__restrict__ major_ptr, uint32_t *__restrict__ minor_idx, uint16_t *__restrict__ out_val,
     unsigned long long capacity, unsigned long long *__restrict__ row_state, uint32_t *__restrict__ row_counter,
@@ -1225,16 +1259,33 @@ __global__ void __launch_bounds__(kOpThreads) filter_onepass_kernel(
         const block_div bd(B);
         const uint32_t *bci = src.blockColIdx + (std::size_t) (local / B) * W;
         const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
-        // keep bits of this thread's vectors of one step
-        auto step_keep = [&](uint32_t base, uint4 (&v)[kOpVecs], uint32_t (&keep)[kOpVecs], uint32_t (&gene0)[kOpVecs]) {
+        // this thread's vectors of one step, and their keep bits
+        auto load_vecs = [&](uint32_t base, uint4 (&v)[kOpVecs], unsigned long long pol) {
+#pragma unroll
+            for (unsigned u = 0; u < kOpVecs; ++u) {
+                const uint32_t e0 = base + (threadIdx.x * kOpVecs + u) * 8u;
+                v[u] = e0 < src.ell_cols ? ld_policy_v4(vrow + e0, pol) : make_uint4(0u, 0u, 0u, 0u);
+            }
+        };
+        auto keep_of = [&](uint32_t base, const uint4 (&v)[kOpVecs], uint32_t (&keep)[kOpVecs],
+                           uint32_t (&gene0)[kOpVecs]) {
 #pragma unroll
             for (unsigned u = 0; u < kOpVecs; ++u) {
                 const uint32_t e0 = base + (threadIdx.x * kOpVecs + u) * 8u;
                 const bool in = e0 < src.ell_cols;
-                v[u] = in ? ld_stream_v4(vrow + e0) : make_uint4(0u, 0u, 0u, 0u);
                 const uint32_t bc = in ? __ldg(bci + bd.div(e0)) : CS_INVALID_COL;
                 gene0[u] = bc * B + bd.mod(e0);
                 keep[u] = in ? onepass_keep(v[u], bc, gene0[u], src.cols, output_cols, kbits) : 0u;
+            }
+        };
+        // the next step's loads go out before this step's work (kOpPrefetch) or after it
+        auto next_step = [&](uint32_t base, uint4 (&v)[kOpVecs], uint4 (&nv)[kOpVecs], unsigned long long pol) {
+            if (base + kStep >= src.ell_cols) return;
+            if (kOpPrefetch) {
+#pragma unroll
+                for (unsigned u = 0; u < kOpVecs; ++u) v[u] = nv[u];
+            } else {
+                load_vecs(base + kStep, v, pol);
             }
         };
         // count
@@ -1244,57 +1295,75 @@ __global__ void __launch_bounds__(kOpThreads) filter_onepass_kernel(
                 cta_kept_rows += 1u;
                 cta_kept_slots += src.ell_cols;
             }
+            const unsigned long long pol = l2_evict_last_policy();
+            uint4 v[kOpVecs], nv[kOpVecs];
+            load_vecs(0u, v, pol);
             for (uint32_t base = 0u; base < src.ell_cols; base += kStep) {
-                uint4 v[kOpVecs];
+                if (kOpPrefetch && base + kStep < src.ell_cols) load_vecs(base + kStep, nv, pol);
                 uint32_t keep[kOpVecs], gene0[kOpVecs];
-                step_keep(base, v, keep, gene0);
+                keep_of(base, v, keep, gene0);
 #pragma unroll
                 for (unsigned u = 0; u < kOpVecs; ++u) my += __popc(keep[u]);
+                next_step(base, v, nv, pol);
             }
         }
         uint32_t count;
         (void) block_exclusive_scan(my, scan33, count);
-        // publish the count, then the prefix once the rows before it are known
-        if (threadIdx.x == 0u) {
-            lb_store(row_state + row, kLbCount | count);
+        // publish the count, then the prefix once the rows before it are known:
+        // warp 0 reads the states of the 32 rows before row j at once and stops
+        // at the nearest one that holds its prefix (rows before row 0 count as
+        // a zero prefix)
+        if (threadIdx.x < 32u) {
+            const unsigned lane = threadIdx.x;
+            if (lane == 0u) lb_store(row_state + row, kLbCount | count);
             uint32_t excl = 0u, j = row;
             bool gave_up = false;
             while (j > 0u) {
-                --j;
-                unsigned long long st = lb_load(row_state + j);
-                for (uint32_t spins = 0; (st >> 32) == 0ull; st = lb_load(row_state + j)) {
+                const bool real = lane < j;
+                const uint32_t q = real ? j - 1u - lane : 0u;
+                unsigned long long st = real ? lb_load(row_state + q) : kLbPrefix;
+                for (uint32_t spins = 0; !__all_sync(0xffffffffu, (st >> 32) != 0ull);) {
                     if (++spins > kLbSpinLimit) {
                         gave_up = true;
                         break;
                     }
                     __nanosleep(64);
+                    if ((st >> 32) == 0ull) st = lb_load(row_state + q);
                 }
                 if (gave_up) break;
-                excl += (uint32_t) st;
-                if ((st & ~0xffffffffull) == kLbPrefix) break;
+                const uint32_t pm = __ballot_sync(0xffffffffu, (st & ~0xffffffffull) == kLbPrefix);
+                const uint32_t first = pm != 0u ? (uint32_t) __ffs(pm) - 1u : 31u;
+                excl += __reduce_add_sync(0xffffffffu, lane <= first ? (uint32_t) st : 0u);
+                if (pm != 0u) break;
+                j -= 32u; // pm == 0 means all 32 rows before j are real
             }
-            if (gave_up) {
-                s_stop = 1u;
-                status_or(status, CS_STATUS_WAIT_LIMIT);
-            } else {
-                lb_store(row_state + row, kLbPrefix | (excl + count));
-                major_ptr[row] = excl;
-                if (count != 0u && (unsigned long long) excl + count > capacity) {
-                    s_stop = 2u; // this row does not fit: skip its emission
-                    status_or(status, CS_STATUS_CAPACITY);
+            if (lane == 0u) {
+                if (gave_up) {
+                    s_stop = 1u;
+                    status_or(status, CS_STATUS_WAIT_LIMIT);
+                } else {
+                    lb_store(row_state + row, kLbPrefix | (excl + count));
+                    major_ptr[row] = excl;
+                    if (count != 0u && (unsigned long long) excl + count > capacity) {
+                        s_stop = 2u; // this row does not fit: skip its emission
+                        status_or(status, CS_STATUS_CAPACITY);
+                    }
                 }
+                s_excl = excl;
             }
-            s_excl = excl;
         }
         __syncthreads();
         if (s_stop == 1u) break;
         if (count != 0u && s_stop == 0u) {
             // emit, re-reading the row (now in L2) in slot order
             uint32_t run = s_excl;
+            const unsigned long long pol = l2_evict_first_policy();
+            uint4 v[kOpVecs], nv[kOpVecs];
+            load_vecs(0u, v, pol);
             for (uint32_t base = 0u; base < src.ell_cols; base += kStep) {
-                uint4 v[kOpVecs];
+                if (kOpPrefetch && base + kStep < src.ell_cols) load_vecs(base + kStep, nv, pol);
                 uint32_t keep[kOpVecs], gene0[kOpVecs];
-                step_keep(base, v, keep, gene0);
+                keep_of(base, v, keep, gene0);
                 uint32_t n = 0u;
 #pragma unroll
                 for (unsigned u = 0; u < kOpVecs; ++u) n += __popc(keep[u]);
@@ -1308,6 +1377,7 @@ __global__ void __launch_bounds__(kOpThreads) filter_onepass_kernel(
                         out_val[pos] = half_of(v[u], q);
                     }
                 run += total;
+                next_step(base, v, nv, pol);
             }
         }
         __syncthreads(); // s_row / s_excl are rewritten by the next claim
@@ -1635,12 +1705,16 @@ extern "C" int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts,
     return reopt_emit_launch(p, masks, output_rows, output_cols, d_major_ptr, d_minor_idx, d_val, as_stream(s));
 }
 
-extern "C" int cs_b200_filter_blocked_ell_onepass_scratch_bytes(uint32_t shard_rows, size_t *out_bytes) {
+extern "C" int cs_b200_filter_blocked_ell_onepass_scratch_bytes(const cs_blocked_ell_view *parts, uint32_t part_count,
+                                                                size_t *out_bytes) {
+    static const char *who = "filter_blocked_ell_onepass_scratch_bytes";
     if (out_bytes == nullptr) {
-        set_error("filter_blocked_ell_onepass_scratch_bytes: null output");
+        set_error("%s: null output", who);
         return 0;
     }
-    *out_bytes = align_up(((std::size_t) shard_rows + 1u) * 8u + 16u, 256);
+    reopt_parts p;
+    if (!make_parts(parts, part_count, &p, who)) return 0;
+    *out_bytes = align_up(((std::size_t) p.row_off[p.count] + 1u) * 8u + 16u, 256);
     return 1;
 }
 
@@ -1682,8 +1756,7 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
         set_error("%s: too many columns for the shared feature bitmap", who);
         return 0;
     }
-    size_t need = 0;
-    cs_b200_filter_blocked_ell_onepass_scratch_bytes(rows, &need);
+    const std::size_t need = align_up(((std::size_t) rows + 1u) * 8u + 16u, 256);
     if (d_scratch == nullptr || scratch_bytes < need) {
         set_error("%s: scratch %zu < %zu", who, scratch_bytes, need);
         return 0;

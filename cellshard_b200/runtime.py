@@ -132,7 +132,8 @@ def filter_blocked_ell_to_compressed(parts, output_rows: int, output_cols: int, 
     Returns (CSR, stats) with the reference's stats fields; kept_rows / kept_row_slots
     count every kept source row (the repack operator's figures).
 
-    method "auto": one pass over the values (cs_b200_filter_blocked_ell_onepass) when the
+    method "auto": one pass over the values (cs_b200_filter_blocked_ell_onepass: each row
+    counted, placed by a decoupled look-back and written from L2) when the
     shard qualifies (no remaps, block sizes multiples of 8, output_rows >= its rows), into
     arrays sized by the parts' stored nnz; otherwise, or if those prove too small, count +
     emit.  "onepass" / "two_pass" force one route ("onepass" raises if it does not apply)."""
@@ -155,7 +156,8 @@ def filter_blocked_ell_to_compressed(parts, output_rows: int, output_cols: int, 
     if method != "two_pass" and qualifies:
         cap = sum(int(p.nnz) for p in parts)
         nb = C.c_size_t()
-        _abi.check(lib.cs_b200_filter_blocked_ell_onepass_scratch_bytes(shard_rows, C.byref(nb)), "onepass scratch")
+        _abi.check(lib.cs_b200_filter_blocked_ell_onepass_scratch_bytes(views, len(parts), C.byref(nb)),
+                   "onepass scratch")
         scratch = torch.empty(max(nb.value, 16), dtype=torch.uint8, device="cuda")
         idx = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
         val = torch.empty(max(cap, 1), dtype=torch.float16, device="cuda")

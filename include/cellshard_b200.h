@@ -616,14 +616,18 @@ CS_API int cs_b200_filter_blocked_ell_count(const cs_blocked_ell_view *parts,
  * row or feature remaps whose block sizes are multiples of 8 (16-byte aligned
  * values) and output_rows >= the shard's rows: each row is counted, its output
  * offset found by a decoupled look-back over the rows before it, and its
- * entries written while its values are still in L2, so the values cross HBM
- * once instead of twice (count + emit).  The output arrays hold `capacity`
- * entries (the stored nnz of the parts bounds the live entries); a shard that
- * needs more sets CS_STATUS_CAPACITY in *d_status and writes nothing past
- * them (run count + emit instead).  d_major_ptr, d_kept as for count.
- * Returns 0 with a message (and launches nothing) when the shard does not
- * qualify.  Scratch: cs_b200_filter_blocked_ell_onepass_scratch_bytes. */
-CS_API int cs_b200_filter_blocked_ell_onepass_scratch_bytes(uint32_t shard_rows, size_t *out_bytes);
+ * entries written while its values are still in L2 (the count's loads mark
+ * them evict_last), so the values cross HBM once instead of twice (count +
+ * emit).  The output arrays hold
+ * `capacity` entries (the stored nnz of the parts bounds the live entries); a
+ * shard that needs more sets CS_STATUS_CAPACITY in *d_status and writes
+ * nothing past them (run count + emit instead).  d_major_ptr, d_kept as for
+ * count.  Returns 0 with a message (and launches nothing) when the shard does
+ * not qualify.  Scratch: cs_b200_filter_blocked_ell_onepass_scratch_bytes
+ * (8 bytes per row). */
+CS_API int cs_b200_filter_blocked_ell_onepass_scratch_bytes(const cs_blocked_ell_view *parts,
+                                                            uint32_t part_count,
+                                                            size_t *out_bytes);
 CS_API int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *parts,
                                               uint32_t part_count,
                                               const cs_row_feature_mask_view *masks,

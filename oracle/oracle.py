@@ -1051,3 +1051,85 @@ def ref_time_sliced_ell_from_compressed(parts, slice_rows, threads, seconds=3.0,
 def time_restated(fn, parts, threads, seconds=3.0):
     """Seconds per pass of a restated CPU routine fn(part) over `parts`."""
     return _pool_time(parts, fn, threads, seconds)
+
+
+def ref_time_sliced_ell_from_blocked_ell(parts, slice_rows, threads, seconds=3.0):
+    """convert::sliced_ell_from_blocked_ell (the reference's host routine) on every
+    (rows, cols, B, ell_cols, bci, val) Blocked-ELL partition; seconds per pass."""
+    def one(p):
+        rows, cols, B, ell_cols, bci, val = p
+        src = host_bell(rows, cols, 0, B, ell_cols, bci, val)
+        dst = HostSlicedEll()
+        assert ref().csref_sliced_ell_from_blocked_ell(C.byref(src), C.c_uint(slice_rows), C.byref(dst)) == 1
+        if dst.storage:
+            ref().csref_free(dst.storage)
+
+    return _pool_time(parts, one, threads, seconds)
+
+
+class _FilterOut:
+    """Output arrays of the restated filter for one partition, allocated once so
+    the timed passes run the filter alone."""
+
+    def __init__(self, rows, ell_cols):
+        cap = max(rows * ell_cols, 1)
+        self.major = np.zeros(rows + 1, np.uint32)
+        self.idx = np.zeros(cap, np.uint32)
+        self.val = np.zeros(cap, np.uint16)
+
+
+def _filter_one(p, out):
+    rows, cols, B, ell_cols, bci, val, row_keep, feature_keep = p
+    f = lib().cso_reoptimize_bell
+    f.restype = C.c_longlong
+    n = f(u32(rows), u32(cols), u32(B), u32(ell_cols), _p(bci), _p(val), _p(row_keep), _p(feature_keep), None, None,
+          u32(rows), u32(cols), _p(out.major), _p(out.idx), _p(out.val))
+    assert n >= 0
+    return n
+
+
+def time_filter_bell(parts, threads, seconds=3.0):
+    """The restated filtered Blocked-ELL -> CSR (cso_reoptimize_bell: kept rows,
+    kept features, no remaps) on every (rows, cols, B, ell_cols, bci, val,
+    row_keep, feature_keep) partition; seconds per pass."""
+    outs = {id(p): _FilterOut(p[0], p[3]) for p in parts}
+    return _pool_time(parts, lambda p: _filter_one(p, outs[id(p)]), threads, seconds)
+
+
+def time_repack_bell(parts, B_out, buckets, threads, seconds=3.0):
+    """The restated repack of every Blocked-ELL partition: filter to CSR, nnz plan
+    over `buckets` buckets, row rebuild in plan order (all restated), then the
+    reference's convert::blocked_ell_from_compressed at block B_out; seconds per pass."""
+    outs = {id(p): _FilterOut(p[0], p[3]) for p in parts}
+
+    def one(p):
+        o = outs[id(p)]
+        rows, cols = p[0], p[1]
+        n = _filter_one(p, o)
+        ptr, idx, val = o.major, o.idx[:n], o.val[:n]
+        _, _, order, _ = major_nnz_plan(ptr, rows, buckets)
+        dptr, didx, dval, _ = rebuild(ptr, idx, val, rows, order)
+        src = host_csr(rows, cols, dptr, didx, dval)
+        dst = HostBlockedEll()
+        assert ref().csref_blocked_ell_from_compressed(C.byref(src), C.c_uint(B_out), C.byref(dst)) == 1
+        ref().csref_free(dst.storage)
+
+    return _pool_time(parts, one, threads, seconds)
+
+
+def time_rebuild(parts, threads, seconds=3.0):
+    """The restated row rebuild (cso_rebuild) of every (rows, cols, ptr, idx, val)
+    partition in its nnz-plan order (the plan made once, outside the timing);
+    seconds per pass."""
+    prepared = []
+    for rows, cols, ptr, idx, val in parts:
+        _, _, order, _ = major_nnz_plan(ptr, rows, 64)
+        nnz = int(ptr[rows]) if rows else 0
+        prepared.append((rows, ptr, idx, val, order, np.zeros(rows + 1, np.uint32), np.zeros(max(nnz, 1), np.uint32),
+                         np.zeros(max(nnz, 1), np.uint16), np.zeros(max(rows, 1), np.uint32)))
+
+    def one(q):
+        rows, ptr, idx, val, order, dptr, didx, dval, inv = q
+        lib().cso_rebuild(_p(ptr), _p(idx), _p(val), u32(rows), _p(order), _p(dptr), _p(didx), _p(dval), _p(inv))
+
+    return _pool_time(prepared, one, threads, seconds)

@@ -74,6 +74,12 @@ def test_blocked_ell_generated_plain_conversion(cuda, orc):
     assert out.ell_cols == ref["ell_cols"] and out.nnz == ref["nnz"] == len(idx)
     assert np.array_equal(np_u32(out.bci), ref["bci"])
     assert np.array_equal(np_u16(out.val), ref["val"])
+    if orc.ref_available():
+        # the reference's own convert::blocked_ell_from_compressed on the whole matrix
+        live = orc.ref_blocked_ell_from_compressed(8192, 2000, ptr, idx, val, 16)
+        assert live["ell_cols"] == out.ell_cols and live["nnz"] == out.nnz
+        assert np.array_equal(np_u32(out.bci), live["bci"])
+        assert np.array_equal(np_u16(out.val), live["val"])
 
 
 def test_blocked_ell_host_api_and_chooser(cuda, orc):

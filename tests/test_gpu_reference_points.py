@@ -24,6 +24,17 @@ pytestmark = pytest.mark.gpu
 REPS = 5
 
 
+def _percent_ulps(ours, ref):
+    """group_percentages within 2 ulp of the reference kernels' (they divide with
+    --use_fast_math); every value is a non-negative float, so the ulp distance is
+    the difference of the bit patterns."""
+    import torch
+
+    a = ours["group_percentages"].view(torch.int32).long()
+    b = ref["group_percentages"].view(torch.int32).long()
+    assert int((a - b).abs().max()) <= 2
+
+
 def _time_ours(fn, reps=REPS, warmup=2):
     import torch
 
@@ -110,6 +121,7 @@ def test_reference_gpu_points(cuda, orc):
         torch.cuda.synchronize()
         for k in ("row_totals", "detected_features", "max_values", "row_keep", "group_counts"):
             assert torch.equal(ours[k], ref[k]), k
+        _percent_ulps(ours, ref)
 
     ours = runtime.compute_sparse_group_reduce(csr, d_masks, G, rk, fk, filt)
     ms = _time_ours(lambda: runtime.compute_sparse_group_reduce(csr, d_masks, G, rk, fk, filt))
@@ -149,6 +161,7 @@ def test_reference_gpu_points(cuda, orc):
     torch.cuda.synchronize()
     for k in ("row_totals", "detected_features", "max_values", "row_keep", "group_counts"):
         assert torch.equal(ours[k], ref[k]), k
+    _percent_ulps(ours, ref)
     bytes_read = R * bell.ell_cols * 2 + bell.row_blocks * bell.ell_width * 4
     out["mask_groups_reduce_ms"] = {"ours": ms, "reference": ms_ref.value, "bytes_read": bytes_read}
     print(json.dumps({"reference_gpu_points": out}))

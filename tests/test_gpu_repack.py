@@ -150,8 +150,8 @@ def test_reference_filter_row_pointers_are_shifted(cuda, orc):
     ([(64, 32), (1, 16), (9000, 8)], 500, 9065),
 ])
 def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows):
-    """The one-pass filter (count, look-back over rows, emit while in L2) gives the count +
-    emit CSR bit for bit, with the same kept-row statistics, and both equal the
+    """The one-pass filter (rows counted, placed by a look-back, emitted from L2) gives the
+    count + emit CSR bit for bit, with the same kept-row statistics, and both equal the
     restatement's masked reoptimize without remaps."""
     from cellshard_b200 import runtime
 
@@ -169,6 +169,41 @@ def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows
     assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr))
     assert np.array_equal(np_u32(a.idx), np_u32(b.idx))
     assert np.array_equal(np_u16(a.val), np_u16(b.val))
+    ident = np.arange(shard_rows, dtype=np.uint32)
+    ptr, idx, val = _oracle_filter(orc, host, cols, keep_rows, keep_cols, ident, np.arange(cols, dtype=np.uint32),
+                                   out_rows, cols)
+    assert np.array_equal(np_u32(a.ptr), ptr) and np.array_equal(np_u32(a.idx), idx)
+    assert np.array_equal(np_u16(a.val), val)
+
+
+@pytest.mark.parametrize("drop", ["last_row", "last_partition"])
+def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop):
+    """Rows of 9,000 columns (two 8,192-slot steps of the one-pass kernel, the
+    last ragged) and a dropped final row or partition, which carry no entries but
+    must still give every row pointer and the total: bit-exact vs count + emit and
+    the restatement."""
+    import torch
+
+    from cellshard_b200 import runtime
+
+    cols = 9000
+    specs = [(40, 16), (33, 8)]
+    parts, host = _shard(81, specs, cols)
+    shard_rows = sum(r for r, _ in specs)
+    rng = np.random.default_rng(9)
+    keep_rows = (rng.random(shard_rows) < 0.7).astype(np.uint8)
+    if drop == "last_row":
+        keep_rows[-1] = 0
+    else:
+        keep_rows[specs[0][0]:] = 0
+    keep_cols = (rng.random(cols) < 0.6).astype(np.uint8)
+    out_rows = shard_rows + 5
+    rk, fk = torch.from_numpy(keep_rows).cuda(), torch.from_numpy(keep_cols).cuda()
+    a, sa = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="onepass")
+    b, sb = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="two_pass")
+    assert sa == sb
+    assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr))
+    assert np.array_equal(np_u32(a.idx), np_u32(b.idx)) and np.array_equal(np_u16(a.val), np_u16(b.val))
     ident = np.arange(shard_rows, dtype=np.uint32)
     ptr, idx, val = _oracle_filter(orc, host, cols, keep_rows, keep_cols, ident, np.arange(cols, dtype=np.uint32),
                                    out_rows, cols)

@@ -47,6 +47,18 @@ def test_transpose_generated_and_roundtrip(cuda, orc):
     back = transpose(CSR(csr.cols, csr.rows, t.ptr, t.idx, t.val))
     assert np.array_equal(np_u32(back.ptr), ptr) and np.array_equal(np_u32(back.idx), idx)
     assert np.array_equal(np_u16(back.val), val)
+    if (ROOT / "oracle" / "_ref" / "libcs_ref_gpu.so").exists():
+        # the reference's own cuSPARSE route on the whole 8,192 x 2,000 matrix
+        import torch
+
+        optr = torch.empty(csr.cols + 1, dtype=torch.int32, device="cuda")
+        oidx = torch.empty(csr.nnz, dtype=torch.int32, device="cuda")
+        oval = torch.empty(csr.nnz, dtype=torch.float16, device="cuda")
+        assert orc.ref_gpu().csrefgpu_transpose(csr.rows, csr.cols, csr.nnz, csr.ptr.data_ptr(), csr.idx.data_ptr(),
+                                                csr.val.data_ptr(), optr.data_ptr(), oidx.data_ptr(),
+                                                oval.data_ptr()) == 1
+        assert np.array_equal(np_u32(t.ptr), np_u32(optr)) and np.array_equal(np_u32(t.idx), np_u32(oidx))
+        assert np.array_equal(np_u16(t.val), np_u16(oval))
 
 
 def test_transpose_keeps_repeated_columns_in_row_order(cuda, orc):
@@ -212,16 +224,51 @@ def test_plan_vs_reference_cub_and_reference_rebuild_shift(cuda, orc):
 
 
 @pytest.mark.parametrize("rows,cols,density,seed", [
-    (600, 64, 0.9, 31),     # a tile's panel overflows the shared-memory stage: direct stores
-    (1000, 5000, 0.5, 32),  # many rows with more than 32 entries in one panel
+    (600, 64, 0.9, 31),     # dense, narrow panels
+    (1000, 5000, 0.5, 32),  # dense rows, hundreds of panels
     (4097, 257, 0.08, 33),  # ragged last tile and panel
     (70000, 300, 0.02, 34), # many tiles
 ])
-def test_transpose_panel_path_edges(cuda, orc, rows, cols, density, seed):
-    """The panel transpose (sorted rows) on its edge cases, bit-exact vs the restatement."""
+def test_transpose_sorted_row_edges(cuda, orc, rows, cols, density, seed):
+    """The stable transpose of sorted rows at dense, ragged and many-tile shapes, bit-exact vs the restatement."""
     from cellshard_b200.device import transpose
 
     ptr, idx, val = random_csr(rows, cols, density, seed, 0.1, integer=False)
+    t = transpose(to_device_csr(rows, cols, ptr, idx, val))
+    rptr, ridx, rval = orc.csr_transpose(rows, cols, ptr, idx, val)
+    assert np.array_equal(np_u32(t.ptr), rptr)
+    assert np.array_equal(np_u32(t.idx), ridx)
+    assert np.array_equal(np_u16(t.val), rval)
+
+
+def _stack_csr(parts):
+    """Row-wise concatenation of (rows, ptr, idx, val) CSR pieces with the same column count."""
+    ptrs, idxs, vals, base = [np.zeros(1, np.uint32)], [], [], 0
+    for _, ptr, idx, val in parts:
+        ptrs.append(ptr[1:].astype(np.uint64) + base)
+        idxs.append(idx)
+        vals.append(val)
+        base += int(ptr[-1])
+    return (sum(p[0] for p in parts), np.concatenate(ptrs).astype(np.uint32), np.concatenate(idxs).astype(np.uint32),
+            np.concatenate(vals).astype(np.uint16))
+
+
+@pytest.mark.parametrize("case", ["dense_first_tile", "long_rows_among_short"])
+def test_transpose_uneven_rows(cuda, orc, case):
+    """A block of rows far denser than the rest, and single near-dense rows among
+    sparse ones, bit-exact vs the restatement."""
+    from cellshard_b200.device import transpose
+
+    cols = 3000
+    if case == "dense_first_tile":
+        pieces = [(512, *random_csr(512, cols, 0.9, 41, 0.0, integer=False)),
+                  (6000, *random_csr(6000, cols, 0.002, 42, 0.3, integer=False))]
+    else:
+        pieces = []
+        for k in range(12):
+            pieces.append((300, *random_csr(300, cols, 0.01, 50 + k, 0.1, integer=False)))
+            pieces.append((3, *random_csr(3, cols, 0.95, 70 + k, 0.0, integer=False)))
+    rows, ptr, idx, val = _stack_csr(pieces)
     t = transpose(to_device_csr(rows, cols, ptr, idx, val))
     rptr, ridx, rval = orc.csr_transpose(rows, cols, ptr, idx, val)
     assert np.array_equal(np_u32(t.ptr), rptr)
