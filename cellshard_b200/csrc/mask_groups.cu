@@ -24,6 +24,9 @@ namespace {
 constexpr unsigned kRowWarps = 8;
 constexpr unsigned kRowThreads = kRowWarps * 32;
 constexpr uint32_t kStagePairs = 128; // per-warp (feature, value) staging in the Blocked-ELL reduce
+#ifndef PIPE_WIDE_WARPS
+#define PIPE_WIDE_WARPS 24u // warps of the many-warp Blocked-ELL-16 pipe
+#endif
 
 // Per-lane running values of one row.  The group sums live in registers:
 // GR (8, 16 or 32, or 0 without groups) accumulators updated with one
@@ -499,8 +502,13 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_kernel(cs_compre
 // and val 8-byte aligned).  (Sliced-ELL keeps the global gathers: its padding
 // quads skip them, and the table's smaller occupancy cost it more than the
 // gathers saved, 1.93 -> 2.10 ms on the 500,000-row matrix.)
+#ifndef CODES_WARPS
+#define CODES_WARPS 8u
+#endif
+constexpr unsigned kCodesWarps = CODES_WARPS; // warps of a code-table CTA (they share one table)
+
 template <unsigned GR, unsigned U = 2>
-__global__ void __launch_bounds__(kRowThreads) group_reduce_csr_codes_kernel(cs_compressed_view src,
+__global__ void __launch_bounds__(kCodesWarps * 32) group_reduce_csr_codes_kernel(cs_compressed_view src,
                                                                               const uint32_t *__restrict__ group_masks,
                                                                               uint32_t group_count,
                                                                               cs_row_feature_mask_view masks,
@@ -508,10 +516,11 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_codes_kernel(cs_
                                                                               cs_group_reduce_out out) {
     extern __shared__ __align__(16) float gr_smem[];
     float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
-    uint16_t *tbl = reinterpret_cast<uint16_t *>(gr_smem + (GR != 0u ? kRowWarps * group_count * 32u : 0u));
+    uint16_t *tbl = reinterpret_cast<uint16_t *>(gr_smem + (GR != 0u ? kCodesWarps * group_count * 32u : 0u));
     build_col_codes(tbl, src.cols, masks.feature_keep, GR != 0u ? group_masks : nullptr,
                     GR != 0u ? (1u << group_count) - 1u : 0u);
-    for (uint32_t row = blockIdx.x * kRowWarps + (threadIdx.x >> 5); row < src.rows; row += gridDim.x * kRowWarps) {
+    for (uint32_t row = blockIdx.x * kCodesWarps + (threadIdx.x >> 5); row < src.rows;
+         row += gridDim.x * kCodesWarps) {
         if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
             empty_row(row, group_count, out);
             continue;
@@ -532,7 +541,8 @@ std::size_t codes_smem(const uint32_t *masks, uint32_t group_count, uint32_t col
     const bool groups = masks != nullptr && group_count != 0u;
     if (groups && group_count > 15u) return 0u;
     if ((std::size_t) cols * 2u > 96u * 1024u) return 0u;
-    return align_up(group_smem(masks, group_count), 16u) + align_up((std::size_t) cols * 2u, 16u);
+    const std::size_t acc = groups ? (std::size_t) kCodesWarps * group_count * 32u * sizeof(float) : 0u;
+    return align_up(acc, 16u) + align_up((std::size_t) cols * 2u, 16u);
 }
 
 template <typename View>
@@ -548,9 +558,9 @@ int launch_codes(reduce_codes_kernel_t<View> k, const View &src, const uint32_t 
                                       (int) smem),
                  name))
         return 0;
-    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kRowThreads, smem,
-                                        (src.rows + kRowWarps - 1u) / kRowWarps);
-    k<<<grid, kRowThreads, smem, stream>>>(src, masks, group_count, m, filter, out);
+    const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kCodesWarps * 32u, smem,
+                                        (src.rows + kCodesWarps - 1u) / kCodesWarps);
+    k<<<grid, kCodesWarps * 32u, smem, stream>>>(src, masks, group_count, m, filter, out);
     return launch_ok(name);
 }
 
@@ -774,44 +784,51 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_bell16_mma_kernel(
 // memory.  Each CTA first builds a u16 entry per column in shared memory
 // (bit 15: in the matrix and kept; bits 0..G-1: the column's groups if
 // kept), so the per-slot column lookups are shared-memory reads.  The values
-// reach shared memory through 16-byte asynchronous copies, STAGES stages of 8
-// slots (16 rows x 256 bytes) per warp, so the bytes in flight do not depend
-// on registers; rows the row mask drops are not copied.  A stage row is
-// padded by 32 bytes, which puts the 8-byte fragment reads of a half-warp on
-// distinct banks.  Row blocks with non-finite values use the per-row path,
-// its shared memory taken from the warp's (then idle) stage buffers.
-constexpr unsigned kPipeWarps = 16;
-constexpr unsigned kPipeSlots = 8;
-constexpr unsigned kPipeRowStride = kPipeSlots * 32u + 32u;
-constexpr unsigned kPipeStageBytes = 16u * kPipeRowStride;
-constexpr unsigned kPipeStages = 2;
-constexpr unsigned kPipePieces = kPipeSlots * 2u;     // 16-byte pieces of one row of a stage
-constexpr unsigned kPipeRowsPerCopy = 32u / kPipePieces; // stage rows one copy instruction covers
-constexpr unsigned kPipeStagesPerWindow = 32u / kPipeSlots; // stages per 32-slot window of block columns
-static_assert(kPipeSlots >= 2u && kPipeSlots <= 16u && (kPipeSlots & (kPipeSlots - 1u)) == 0u,
-              "a stage holds 2, 4, 8 or 16 slots");
-static_assert(kPipeStages * kPipeStageBytes >= 16u * 32u * sizeof(float) + kStagePairs * 8u,
-              "the per-row fallback's accumulators and pairs fit in a warp's stage buffers");
-
-template <unsigned STAGES>
-constexpr std::size_t pipe_warp_bytes() { return (std::size_t) STAGES * kPipeStageBytes; }
+// reach shared memory through 16-byte asynchronous copies, STAGES stages of
+// SLOTS slots (16 rows x 32 * SLOTS bytes) per warp, so the bytes in flight do
+// not depend on registers; rows the row mask drops are not copied.  A stage
+// row is padded by 32 bytes, which puts the 8-byte fragment reads of a
+// half-warp on distinct banks.  Row blocks with non-finite values use the
+// per-row path, its shared memory taken from the warp's (then idle) stage
+// buffers.  Stages of 4 slots, so more warps fit beside the table and hide
+// the copies' latency (24 warps: 5.34 ms against 5.75 ms for 16 warps of
+// 8-slot stages on 500,000 x 32,768); 16 warps where the table of a wider
+// matrix leaves less room.
+template <unsigned SLOTS, unsigned WARPS, unsigned STAGES>
+struct pipe_cfg {
+    static constexpr unsigned slots = SLOTS, warps = WARPS, stages = STAGES;
+    static constexpr unsigned row_stride = SLOTS * 32u + 32u;
+    static constexpr unsigned stage_bytes = 16u * row_stride;
+    static constexpr unsigned pieces = SLOTS * 2u;            // 16-byte pieces of one row of a stage
+    static constexpr unsigned rows_per_copy = 32u / pieces;   // stage rows one copy instruction covers
+    static constexpr unsigned stages_per_window = 32u / SLOTS; // stages per 32-slot window of block columns
+    static constexpr std::size_t warp_bytes = (std::size_t) STAGES * stage_bytes;
+    static_assert(SLOTS >= 2u && SLOTS <= 16u && (SLOTS & (SLOTS - 1u)) == 0u, "a stage holds 2, 4, 8 or 16 slots");
+    static_assert(warp_bytes >= 16u * 32u * sizeof(float) + kStagePairs * 8u,
+                  "the per-row fallback's accumulators and pairs fit in a warp's stage buffers");
+};
+using pipe_wide = pipe_cfg<4u, PIPE_WIDE_WARPS, 2u>;
+using pipe_narrow = pipe_cfg<4u, 16u, 2u>; // a column table of up to ~75,000 columns
 
 std::size_t pipe_table_bytes(uint32_t cols) { return align_up(((std::size_t) cols + 15u) / 16u * 32u, 16u); }
 
-template <unsigned STAGES>
-std::size_t pipe_smem_bytes(uint32_t cols) { return kPipeWarps * pipe_warp_bytes<STAGES>() + pipe_table_bytes(cols); }
+template <class CFG>
+std::size_t pipe_smem_bytes(uint32_t cols) { return CFG::warps * CFG::warp_bytes + pipe_table_bytes(cols); }
 
-template <unsigned NT, unsigned GR, unsigned STAGES>
-__global__ void __launch_bounds__(kPipeWarps * 32, 1) group_reduce_bell16_pipe_kernel(
+template <unsigned NT, unsigned GR, class CFG>
+__global__ void __launch_bounds__(CFG::warps * 32, 1) group_reduce_bell16_pipe_kernel(
     cs_blocked_ell_view src, const uint32_t *__restrict__ group_masks, uint32_t group_count,
     cs_row_feature_mask_view masks, cs_group_filter_params filter, cs_group_reduce_out out) {
     extern __shared__ __align__(16) unsigned char pipe_smem[];
-    constexpr unsigned RS = kPipeRowStride;
+    constexpr unsigned STAGES = CFG::stages, kPipeSlots = CFG::slots, kPipeWarps = CFG::warps;
+    constexpr unsigned kPipeStageBytes = CFG::stage_bytes, kPipePieces = CFG::pieces;
+    constexpr unsigned kPipeRowsPerCopy = CFG::rows_per_copy, kPipeStagesPerWindow = CFG::stages_per_window;
+    constexpr unsigned RS = CFG::row_stride;
     const bool groups = GR != 0u;
     const uint32_t G = groups ? group_count : 0u;
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    unsigned char *buf = pipe_smem + (std::size_t) warp * pipe_warp_bytes<STAGES>();
-    uint16_t *table = reinterpret_cast<uint16_t *>(pipe_smem + kPipeWarps * pipe_warp_bytes<STAGES>());
+    unsigned char *buf = pipe_smem + (std::size_t) warp * CFG::warp_bytes;
+    uint16_t *table = reinterpret_cast<uint16_t *>(pipe_smem + kPipeWarps * CFG::warp_bytes);
     // per-row fallback: accumulator block and pair staging inside this warp's stage buffers
     float *acc_col = groups ? reinterpret_cast<float *>(buf) + lane : nullptr;
     uint2 *stage = reinterpret_cast<uint2 *>(buf + (std::size_t) G * 32u * sizeof(float));
@@ -1453,25 +1470,29 @@ extern "C" int cs_b200_group_reduce_blocked_ell(const cs_blocked_ell_view *src, 
     if (vec && src->block_size == 16u && G <= 15u) {
         // pipelined tensor-core kernel when the column table fits shared memory
         int dev = 0, optin = 0;
-        const std::size_t psmem = pipe_smem_bytes<kPipeStages>(src->cols);
         if (cuda_ok(cudaGetDevice(&dev), "group_reduce_blocked_ell device") &&
             cuda_ok(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
-                    "group_reduce_blocked_ell shared memory limit") &&
-            psmem <= (std::size_t) optin) {
-            const reduce_kernel_t<cs_blocked_ell_view> k =
-                G == 0u ? group_reduce_bell16_pipe_kernel<0u, 0u, kPipeStages>
-                        : G <= 8u ? group_reduce_bell16_pipe_kernel<1u, 8u, kPipeStages>
-                                  : group_reduce_bell16_pipe_kernel<2u, 16u, kPipeStages>;
-            if (!cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(k),
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int) psmem),
-                         "group_reduce_bell16_pipe_kernel shared memory"))
-                return 0;
-            const uint32_t row_blocks = (src->rows + 15u) / 16u;
-            const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), kPipeWarps * 32u, psmem,
-                                                (row_blocks + kPipeWarps - 1u) / kPipeWarps);
-            k<<<grid, kPipeWarps * 32u, psmem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m, *filter,
-                                                                *out);
-            return launch_ok("group_reduce_bell16_pipe_kernel");
+                    "group_reduce_blocked_ell shared memory limit")) {
+            auto launch = [&](auto cfg) -> int {
+                using CFG = decltype(cfg);
+                const std::size_t psmem = pipe_smem_bytes<CFG>(src->cols);
+                const reduce_kernel_t<cs_blocked_ell_view> k =
+                    G == 0u ? group_reduce_bell16_pipe_kernel<0u, 0u, CFG>
+                            : G <= 8u ? group_reduce_bell16_pipe_kernel<1u, 8u, CFG>
+                                      : group_reduce_bell16_pipe_kernel<2u, 16u, CFG>;
+                if (!cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(k),
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int) psmem),
+                             "group_reduce_bell16_pipe_kernel shared memory"))
+                    return 0;
+                const uint32_t row_blocks = (src->rows + 15u) / 16u;
+                const unsigned grid = resident_grid(reinterpret_cast<const void *>(k), CFG::warps * 32u, psmem,
+                                                    (row_blocks + CFG::warps - 1u) / CFG::warps);
+                k<<<grid, CFG::warps * 32u, psmem, as_stream(s)>>>(*src, d_feature_group_masks, group_count, m,
+                                                                    *filter, *out);
+                return launch_ok("group_reduce_bell16_pipe_kernel");
+            };
+            if (pipe_smem_bytes<pipe_wide>(src->cols) <= (std::size_t) optin) return launch(pipe_wide{});
+            if (pipe_smem_bytes<pipe_narrow>(src->cols) <= (std::size_t) optin) return launch(pipe_narrow{});
         }
     }
     if (mma) {

@@ -334,7 +334,9 @@ def _cmp_nan(r, o, exact=True):
     (24, 333, 333, True, True),
     (32, 700, 300, True, True),
     (32, 700, 300, False, True),
-    (8, 48, 50000, True, True),     # column table too large for shared memory
+    (8, 48, 50000, True, True),     # a wide column table beside the many-warp pipeline
+    (8, 48, 70000, True, True),     # the table leaves room for 16 warps only
+    (8, 48, 90000, True, True),     # column table too large for shared memory
 ])
 def test_bell16_tensor_core_paths(cuda, orc, G, rows, cols, integer, masked):
     """Blocked-ELL-16 reduces on the tensor-core kernels (every group-count
