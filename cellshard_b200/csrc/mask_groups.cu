@@ -499,13 +499,10 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_kernel(cs_compre
 
 // The compressed reduce over shared-memory column codes (at most 15 groups,
 // the code table in shared memory after the accumulators; minorIdx 16-byte
-// and val 8-byte aligned).  (Sliced-ELL keeps the global gathers: its padding
-// quads skip them, and the table's smaller occupancy cost it more than the
-// gathers saved, 1.93 -> 2.10 ms on the 500,000-row matrix.)
-#ifndef CODES_WARPS
-#define CODES_WARPS 8u
-#endif
-constexpr unsigned kCodesWarps = CODES_WARPS; // warps of a code-table CTA (they share one table)
+// and val 8-byte aligned).  A CTA of kCodesWarps warps shares one table:
+// 32 warps per SM instead of the 24 that 8-warp CTAs with a table each allow
+// (CSR on 500,000 x 32,768: 0.86 ms against 1.18 ms).
+constexpr unsigned kCodesWarps = 32; // warps of a code-table CTA (they share one table)
 
 template <unsigned GR, unsigned U = 2>
 __global__ void __launch_bounds__(kCodesWarps * 32) group_reduce_csr_codes_kernel(cs_compressed_view src,
@@ -532,6 +529,46 @@ __global__ void __launch_bounds__(kCodesWarps * 32) group_reduce_csr_codes_kerne
         finish_row(row, a, acc_col, group_count, filter, out);
     }
 }
+
+// The Sliced-ELL twin (slots of the row's slice; padding quads skip the table).
+template <unsigned GR, unsigned U = 2>
+__global__ void __launch_bounds__(kCodesWarps * 32) group_reduce_sell_codes_kernel(cs_sliced_ell_view src,
+                                                                               const uint32_t *__restrict__ group_masks,
+                                                                               uint32_t group_count,
+                                                                               cs_row_feature_mask_view masks,
+                                                                               cs_group_filter_params filter,
+                                                                               cs_group_reduce_out out) {
+    extern __shared__ __align__(16) float gr_smem[];
+    float *acc_col = warp_acc_column(gr_smem, GR != 0u, group_count);
+    uint16_t *tbl = reinterpret_cast<uint16_t *>(gr_smem + (GR != 0u ? kCodesWarps * group_count * 32u : 0u));
+    build_col_codes(tbl, src.cols, masks.feature_keep, GR != 0u ? group_masks : nullptr,
+                    GR != 0u ? (1u << group_count) - 1u : 0u);
+    for (uint32_t row = blockIdx.x * kCodesWarps + (threadIdx.x >> 5); row < src.rows;
+         row += gridDim.x * kCodesWarps) {
+        if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
+            empty_row(row, group_count, out);
+            continue;
+        }
+        row_acc<GR> a;
+        init_acc(a);
+        uint32_t width = 0u;
+        std::size_t slot_base = 0u;
+        if (src.slice_count != 0u) {
+            const uint32_t slice = find_slice(src, row);
+            width = src.slice_widths[slice];
+            slot_base = (std::size_t) src.slice_slot_offsets[slice] +
+                        (std::size_t) (row - src.slice_row_offsets[slice]) * width;
+        }
+        reduce_span_codes<U>(src.col_idx, src.val, slot_base, slot_base + width, src.cols, tbl, a);
+        __syncwarp();
+        finish_row(row, a, acc_col, group_count, filter, out);
+    }
+}
+
+#ifndef SELL_CODES
+#define SELL_CODES 1
+#endif
+constexpr bool kSellCodes = SELL_CODES != 0; // the Sliced-ELL reduce over the shared code table
 
 std::size_t group_smem(const uint32_t *masks, uint32_t group_count);
 
@@ -1523,6 +1560,15 @@ extern "C" int cs_b200_group_reduce_sliced_ell(const cs_sliced_ell_view *src, co
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
     const bool vec = (reinterpret_cast<uintptr_t>(src->col_idx) & 15u) == 0u &&
                      (reinterpret_cast<uintptr_t>(src->val) & 7u) == 0u;
+    const std::size_t csmem = kSellCodes && vec ? codes_smem(d_feature_group_masks, group_count, src->cols) : 0u;
+    if (csmem != 0u) {
+        const unsigned g = group_regs(d_feature_group_masks, group_count);
+        return launch_codes<cs_sliced_ell_view>(g == 0u ? group_reduce_sell_codes_kernel<0u>
+                                                        : g == 8u ? group_reduce_sell_codes_kernel<8u>
+                                                                  : group_reduce_sell_codes_kernel<16u>,
+                                                *src, d_feature_group_masks, group_count, m, *filter, *out, csmem,
+                                                as_stream(s), "group_reduce_sell_codes_kernel");
+    }
     const std::size_t smem = group_smem(d_feature_group_masks, group_count);
     const unsigned gr = group_regs(d_feature_group_masks, group_count);
     const reduce_kernel_t<cs_sliced_ell_view> k = vec ? CS_PICK_REDUCE(group_reduce_sell_kernel, true, gr)
