@@ -1219,7 +1219,9 @@ __global__ void __launch_bounds__(kRowThreads) reopt_kernel(const __grid_constan
 // resident CTAs, so every row a CTA waits for is held by a running CTA.
 // row_state[r]: (flag << 32) | value, flag 1 = the row's count, 2 = the
 // inclusive prefix through the row.  The state word is all a reader needs, so
-// it is published and read with relaxed 64-bit accesses (no fence).
+// it is published and read with relaxed 64-bit accesses (no fence).  A row the
+// mask drops is published as count 0 by the thread that claims it, which then
+// claims the next row; the kept row before it writes its row pointer.
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kLbCount = 1ull << 32, kLbPrefix = 2ull << 32;
 constexpr uint32_t kLbSpinLimit = 1u << 22; // ~0.3 s of 64 ns sleeps
@@ -1270,8 +1272,41 @@ __device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, ui
 // evict_last, and the rows in flight (a few CTAs per SM) stay well inside L2.  Each thread owns kOpVecs consecutive
 // 16-byte vectors of a 256 x kOpVecs-vector step, so one block scan per step
 // gives every thread its output position in slot order.
+// Block-wide exclusive scan of 64-bit values (the packed per-step counts);
+// every thread calls it; smem holds 33 words.
+__device__ __forceinline__ unsigned long long block_exclusive_scan_u64(unsigned long long v,
+                                                                       unsigned long long *smem,
+                                                                       unsigned long long &total) {
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned long long incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned) o) incl += t;
+    }
+    if (lane == 31u) smem[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned long long w = lane < nw ? smem[lane] : 0ull;
+        unsigned long long wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= (unsigned) o) wi += t;
+        }
+        if (lane < nw) smem[lane] = wi - w;
+        if (lane == 31u) smem[32] = wi;
+    }
+    __syncthreads();
+    const unsigned long long r = smem[warp] + incl - v;
+    total = smem[32];
+    __syncthreads();
+    return r;
+}
+
 constexpr unsigned kOpThreads = 256;
 constexpr unsigned kOpVecs = 4;
+constexpr uint32_t kOpPackedSteps = 4; // rows of up to 4 steps keep their per-step counts for one scan
 constexpr unsigned kOpCtasPerSm = 5;
 constexpr bool kOpPrefetch = false; // the next step's loads issued before this step's work
 
@@ -1283,6 +1318,7 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
     const uint32_t rows = parts.row_off[parts.count];
     extern __shared__ uint32_t onepass_keep_bits[];
     __shared__ uint32_t s_row, s_excl, s_stop, scan33[33];
+    __shared__ unsigned long long scan33w[33];
     const uint32_t *kbits = keep_words != 0u ? onepass_keep_bits : nullptr;
     uint32_t kcols = 0u;
     for (uint32_t k = 0; k < parts.count; ++k) kcols = max(kcols, parts.v[k].cols);
@@ -1299,13 +1335,20 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
     constexpr uint32_t kStep = kOpThreads * kOpVecs * 8u; // values per step
     for (;;) {
         if (threadIdx.x == 0u) {
-            s_row = atomicAdd(row_counter, 1u);
+            // rows the mask drops are published as empty at once (their row
+            // pointers come from the kept row before them) and not worked on
+            uint32_t r;
+            for (;;) {
+                r = atomicAdd(row_counter, 1u);
+                if (r >= rows || masks.row_keep == nullptr || masks.row_keep[r] != 0u) break;
+                lb_store(row_state + r, kLbCount);
+            }
+            s_row = r;
             s_stop = 0u;
         }
         __syncthreads();
         const uint32_t row = s_row;
         if (row >= rows) break;
-        const bool kept_row = masks.row_keep == nullptr || masks.row_keep[row] != 0u;
         const uint32_t part = part_of_row(parts, row);
         const cs_blocked_ell_view &src = parts.v[part];
         const uint32_t local = row - parts.row_off[part];
@@ -1342,9 +1385,12 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
                 load_vecs(base + kStep, v, pol);
             }
         };
-        // count
+        // count (a row of at most kOpPackedSteps steps keeps each step's count,
+        // 16 bits per step, so one scan orders the whole emit)
+        const bool packed = src.ell_cols <= kOpPackedSteps * kStep;
         uint32_t my = 0u;
-        if (kept_row) {
+        unsigned long long my_steps = 0ull;
+        {
             if (threadIdx.x == 0u) {
                 cta_kept_rows += 1u;
                 cta_kept_slots += src.ell_cols;
@@ -1352,17 +1398,27 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
             const unsigned long long pol = l2_evict_last_policy();
             uint4 v[kOpVecs], nv[kOpVecs];
             load_vecs(0u, v, pol);
-            for (uint32_t base = 0u; base < src.ell_cols; base += kStep) {
+            for (uint32_t base = 0u, st = 0u; base < src.ell_cols; base += kStep, ++st) {
                 if (kOpPrefetch && base + kStep < src.ell_cols) load_vecs(base + kStep, nv, pol);
                 uint32_t keep[kOpVecs], gene0[kOpVecs];
                 keep_of(base, v, keep, gene0);
+                uint32_t n = 0u;
 #pragma unroll
-                for (unsigned u = 0; u < kOpVecs; ++u) my += __popc(keep[u]);
+                for (unsigned u = 0; u < kOpVecs; ++u) n += __popc(keep[u]);
+                my += n;
+                if (packed) my_steps += (unsigned long long) n << (16u * st);
                 next_step(base, v, nv, pol);
             }
         }
         uint32_t count;
-        (void) block_exclusive_scan(my, scan33, count);
+        unsigned long long step_excl = 0ull, step_tot = 0ull;
+        if (packed) {
+            step_excl = block_exclusive_scan_u64(my_steps, scan33w, step_tot);
+            count = (uint32_t) (step_tot & 0xffffu) + (uint32_t) ((step_tot >> 16) & 0xffffu) +
+                    (uint32_t) ((step_tot >> 32) & 0xffffu) + (uint32_t) (step_tot >> 48);
+        } else {
+            (void) block_exclusive_scan(my, scan33, count);
+        }
         // publish the count, then the prefix once the rows before it are known:
         // warp 0 reads the states of the 32 rows before row j at once and stops
         // at the nearest one that holds its prefix (rows before row 0 count as
@@ -1405,10 +1461,52 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
                 }
                 s_excl = excl;
             }
+            // the row pointers of the dropped rows after this one (up to the
+            // next kept row, or the shard's end: then major_ptr[rows]) are this
+            // row's inclusive prefix; 32 rows per step
+            if (!gave_up) {
+                const uint32_t incl = excl + count;
+                for (uint32_t k0 = row + 1u;; k0 += 32u) {
+                    const uint32_t k = k0 + lane;
+                    const bool dropped = k < rows && masks.row_keep != nullptr && masks.row_keep[k] == 0u;
+                    const uint32_t stop = __ballot_sync(0xffffffffu, !dropped);
+                    const uint32_t first = stop != 0u ? (uint32_t) __ffs(stop) - 1u : 32u;
+                    if (lane < first) major_ptr[k] = incl;
+                    if (stop != 0u) {
+                        if (lane == 0u && k0 + first >= rows) major_ptr[rows] = incl;
+                        break;
+                    }
+                }
+            }
         }
         __syncthreads();
         if (s_stop == 1u) break;
-        if (count != 0u && s_stop == 0u) {
+        if (packed && my != 0u && s_stop == 0u) {
+            // emit, re-reading the row (now in L2) in slot order: step st's
+            // entries of this thread start after the earlier steps' entries and
+            // the earlier threads' entries of step st -- no further barrier
+            const unsigned long long pol = l2_evict_first_policy();
+            uint32_t step_base = s_excl;
+            for (uint32_t base = 0u, st = 0u; base < src.ell_cols; base += kStep, ++st) {
+                const uint32_t sh = 16u * st;
+                if (((my_steps >> sh) & 0xffffull) != 0ull) {
+                    uint4 v[kOpVecs];
+                    load_vecs(base, v, pol);
+                    uint32_t keep[kOpVecs], gene0[kOpVecs];
+                    keep_of(base, v, keep, gene0);
+                    uint32_t pos = step_base + (uint32_t) ((step_excl >> sh) & 0xffffull);
+#pragma unroll
+                    for (unsigned u = 0; u < kOpVecs; ++u)
+                        for (uint32_t bb = keep[u]; bb != 0u; bb &= bb - 1u, ++pos) {
+                            const uint32_t q = __ffs(bb) - 1u;
+                            minor_idx[pos] = gene0[u] + q;
+                            out_val[pos] = half_of(v[u], q);
+                        }
+                }
+                step_base += (uint32_t) ((step_tot >> sh) & 0xffffull);
+            }
+        }
+        if (!packed && count != 0u && s_stop == 0u) {
             // emit, re-reading the row (now in L2) in slot order
             uint32_t run = s_excl;
             const unsigned long long pol = l2_evict_first_policy();
@@ -1442,11 +1540,12 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
     }
 }
 
-// major_ptr[r] for r in [rows, output_rows]: the total (the last row's prefix).
-__global__ void filter_onepass_tail_kernel(const unsigned long long *__restrict__ row_state, uint32_t rows,
-                                           uint32_t output_rows, uint32_t *__restrict__ major_ptr) {
-    const uint32_t total = rows != 0u ? (uint32_t) row_state[rows - 1u] : 0u;
-    for (uint32_t r = rows + blockIdx.x * blockDim.x + threadIdx.x; r <= output_rows; r += gridDim.x * blockDim.x)
+// major_ptr[r] for r in (rows, output_rows]: the total, major_ptr[rows] (the
+// last kept row's inclusive prefix, or the zero set before the kernel).
+__global__ void filter_onepass_tail_kernel(uint32_t rows, uint32_t output_rows, uint32_t *__restrict__ major_ptr) {
+    const uint32_t total = major_ptr[rows];
+    for (uint32_t r = rows + 1u + blockIdx.x * blockDim.x + threadIdx.x; r <= output_rows;
+         r += gridDim.x * blockDim.x)
         major_ptr[r] = total;
 }
 
@@ -1831,7 +1930,9 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
     cudaStream_t stream = as_stream(s);
     auto *state = static_cast<unsigned long long *>(d_scratch);
     auto *counter = reinterpret_cast<uint32_t *>(state + rows + 1u);
+    // row pointers start at zero: dropped rows before the first kept row keep it
     if (!cuda_ok(cudaMemsetAsync(d_scratch, 0, need, stream), "onepass scratch memset") ||
+        !cuda_ok(cudaMemsetAsync(d_major_ptr, 0, ((std::size_t) rows + 1u) * 4u, stream), "onepass row pointers") ||
         (d_kept != nullptr && !cuda_ok(cudaMemsetAsync(d_kept, 0, 16, stream), "memset kept")))
         return 0;
     if (rows != 0u) {
@@ -1846,6 +1947,6 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
     }
     const uint32_t tail = output_rows - rows + 1u;
     filter_onepass_tail_kernel<<<(tail + 255u) / 256u > 1024u ? 1024u : (tail + 255u) / 256u, 256, 0, stream>>>(
-        state, rows, output_rows, d_major_ptr);
+        rows, output_rows, d_major_ptr);
     return launch_ok("filter_onepass_tail_kernel");
 }

@@ -176,26 +176,33 @@ def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows
     assert np.array_equal(np_u16(a.val), val)
 
 
-@pytest.mark.parametrize("drop", ["last_row", "last_partition"])
-def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop):
+@pytest.mark.parametrize("cols", [9000, 40000])
+@pytest.mark.parametrize("drop", ["last_row", "last_partition", "first_rows", "all"])
+def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop, cols):
     """Rows of 9,000 columns (two 8,192-slot steps of the one-pass kernel, the
-    last ragged) and a dropped final row or partition, which carry no entries but
-    must still give every row pointer and the total: bit-exact vs count + emit and
-    the restatement."""
+    last ragged: the per-step counts of the whole row go through one scan) and of
+    40,000 columns (more steps than that: one scan per step), and a dropped final
+    row or partition, the first rows, or every row dropped (dropped rows carry no
+    entries but must still get their row pointers and the total): bit-exact vs
+    count + emit and the restatement."""
     import torch
 
     from cellshard_b200 import runtime
 
-    cols = 9000
     specs = [(40, 16), (33, 8)]
     parts, host = _shard(81, specs, cols)
+    assert cols < 32768 or max(p.ell_cols for p in parts) > 32768
     shard_rows = sum(r for r, _ in specs)
     rng = np.random.default_rng(9)
     keep_rows = (rng.random(shard_rows) < 0.7).astype(np.uint8)
     if drop == "last_row":
         keep_rows[-1] = 0
-    else:
+    elif drop == "last_partition":
         keep_rows[specs[0][0]:] = 0
+    elif drop == "first_rows":
+        keep_rows[:7] = 0
+    else:
+        keep_rows[:] = 0
     keep_cols = (rng.random(cols) < 0.6).astype(np.uint8)
     out_rows = shard_rows + 5
     rk, fk = torch.from_numpy(keep_rows).cuda(), torch.from_numpy(keep_cols).cuda()
