@@ -1317,6 +1317,9 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
     uint32_t *status, unsigned long long *__restrict__ kept, uint32_t keep_words) {
     const uint32_t rows = parts.row_off[parts.count];
     extern __shared__ uint32_t onepass_keep_bits[];
+    // after the feature bitmap: the keep bits of this thread's 4 vectors of each
+    // step of the current row (packed rows), read back by the same thread
+    uint32_t *row_keep32 = onepass_keep_bits + ((keep_words + 3u) & ~3u) + threadIdx.x;
     __shared__ uint32_t s_row, s_excl, s_stop, scan33[33];
     __shared__ unsigned long long scan33w[33];
     const uint32_t *kbits = keep_words != 0u ? onepass_keep_bits : nullptr;
@@ -1406,7 +1409,10 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
 #pragma unroll
                 for (unsigned u = 0; u < kOpVecs; ++u) n += __popc(keep[u]);
                 my += n;
-                if (packed) my_steps += (unsigned long long) n << (16u * st);
+                if (packed) {
+                    my_steps += (unsigned long long) n << (16u * st);
+                    row_keep32[st * kOpThreads] = keep[0] | (keep[1] << 8) | (keep[2] << 16) | (keep[3] << 24);
+                }
                 next_step(base, v, nv, pol);
             }
         }
@@ -1489,19 +1495,23 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
             uint32_t step_base = s_excl;
             for (uint32_t base = 0u, st = 0u; base < src.ell_cols; base += kStep, ++st) {
                 const uint32_t sh = 16u * st;
-                if (((my_steps >> sh) & 0xffffull) != 0ull) {
-                    uint4 v[kOpVecs];
-                    load_vecs(base, v, pol);
-                    uint32_t keep[kOpVecs], gene0[kOpVecs];
-                    keep_of(base, v, keep, gene0);
+                // only the vectors the count found kept entries in are re-read
+                const uint32_t kw4 = row_keep32[st * kOpThreads];
+                if (kw4 != 0u) {
                     uint32_t pos = step_base + (uint32_t) ((step_excl >> sh) & 0xffffull);
 #pragma unroll
-                    for (unsigned u = 0; u < kOpVecs; ++u)
-                        for (uint32_t bb = keep[u]; bb != 0u; bb &= bb - 1u, ++pos) {
+                    for (unsigned u = 0; u < kOpVecs; ++u) {
+                        const uint32_t kb = (kw4 >> (8u * u)) & 0xffu;
+                        if (kb == 0u) continue;
+                        const uint32_t e0 = base + (threadIdx.x * kOpVecs + u) * 8u;
+                        const uint4 v = ld_policy_v4(vrow + e0, pol);
+                        const uint32_t gene0 = __ldg(bci + bd.div(e0)) * B + bd.mod(e0);
+                        for (uint32_t bb = kb; bb != 0u; bb &= bb - 1u, ++pos) {
                             const uint32_t q = __ffs(bb) - 1u;
-                            minor_idx[pos] = gene0[u] + q;
-                            out_val[pos] = half_of(v[u], q);
+                            minor_idx[pos] = gene0 + q;
+                            out_val[pos] = half_of(v, q);
                         }
+                    }
                 }
                 step_base += (uint32_t) ((step_tot >> sh) & 0xffffull);
             }
@@ -1940,7 +1950,13 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
         // a few CTAs per SM: enough bytes in flight, few enough rows in flight to stay in L2
         unsigned grid = (unsigned) sm_count() * kOpCtasPerSm;
         if (grid > rows) grid = rows;
-        k<<<grid, kOpThreads, kw * 4u, stream>>>(p, m, output_cols, d_major_ptr, d_minor_idx, d_val, capacity, state,
+        const std::size_t smem = ((std::size_t) ((kw + 3u) & ~3u) + kOpPackedSteps * kOpThreads) * 4u;
+        if (smem > 48u * 1024u &&
+            !cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(k),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem),
+                     "onepass shared memory"))
+            return 0;
+        k<<<grid, kOpThreads, smem, stream>>>(p, m, output_cols, d_major_ptr, d_minor_idx, d_val, capacity, state,
                                                  counter, d_status, reinterpret_cast<unsigned long long *>(d_kept),
                                                  kw);
         if (!launch_ok("filter_onepass_kernel")) return 0;
