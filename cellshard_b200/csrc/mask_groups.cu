@@ -1260,11 +1260,25 @@ __device__ __forceinline__ uint4 ld_policy_v4(const void *p, unsigned long long 
 }
 
 // Kept entries among the 8 values of one vector (no feature remap).
-__device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, uint32_t gene0, uint32_t cols,
-                                                 uint32_t output_cols, const uint32_t *kbits) {
-    uint32_t live = live_bits8(v) & in_range8(bc, gene0, cols);
+// Bit q set when fp16 value q of the 8 in v is nonzero as a float (NaN
+// counts): (w & 0x7fff7fff) + 0x7fff7fff sets bit 15 (31) exactly when the low
+// (high) half has a nonzero magnitude, with no carry between the halves; the
+// eight flags are gathered by a byte permute and a multiply.
+__device__ __forceinline__ uint32_t live_bits8_add(const uint4 &v) {
+    const uint32_t m0 = (v.x & 0x7fff7fffu) + 0x7fff7fffu, m1 = (v.y & 0x7fff7fffu) + 0x7fff7fffu;
+    const uint32_t m2 = (v.z & 0x7fff7fffu) + 0x7fff7fffu, m3 = (v.w & 0x7fff7fffu) + 0x7fff7fffu;
+    const uint32_t f01 = __byte_perm(m0, m1, 0x7531u), f23 = __byte_perm(m2, m3, 0x7531u);
+    const uint32_t lo = (((f01 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
+    const uint32_t hi = (((f23 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
+    return (lo & 0xfu) | ((hi & 0xfu) << 4);
+}
+
+// lim = min(cols, output_cols): the columns that exist and have an output slot.
+__device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, uint32_t gene0, uint32_t lim,
+                                                 const uint32_t *kbits) {
+    uint32_t live = live_bits8_add(v) & in_range8(bc, gene0, lim);
     if (kbits != nullptr && live != 0u) live &= kbits[gene0 >> 5] >> (gene0 & 31u);
-    return live & in_range8(bc, gene0, output_cols);
+    return live;
 }
 
 // One CTA per row at a time (rows claimed in order): the row's values are read
@@ -1375,7 +1389,7 @@ __global__ void __launch_bounds__(kOpThreads, kOpCtasPerSm) filter_onepass_kerne
                 const bool in = e0 < src.ell_cols;
                 const uint32_t bc = in ? __ldg(bci + bd.div(e0)) : CS_INVALID_COL;
                 gene0[u] = bc * B + bd.mod(e0);
-                keep[u] = in ? onepass_keep(v[u], bc, gene0[u], src.cols, output_cols, kbits) : 0u;
+                keep[u] = in ? onepass_keep(v[u], bc, gene0[u], min(src.cols, output_cols), kbits) : 0u;
             }
         };
         // the next step's loads go out before this step's work (kOpPrefetch) or after it
