@@ -7,16 +7,17 @@
 
 namespace csb {
 
-// Bit q set when fp16 value q of the 8 in v is nonzero as a float (NaN counts).
+// Bit q set when fp16 value q of the 8 in v is nonzero as a float (NaN
+// counts): (w & 0x7fff7fff) + 0x7fff7fff sets bit 15 (31) exactly when the low
+// (high) half has a nonzero magnitude, with no carry between the halves; the
+// eight flags are gathered by a byte permute and a multiply.
 __device__ __forceinline__ uint32_t live_bits8(const uint4 &v) {
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    uint32_t b = 0u;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const uint32_t m = __vsetne2(w[i] & 0x7fff7fffu, 0u);
-        b |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * i);
-    }
-    return b;
+    const uint32_t m0 = (v.x & 0x7fff7fffu) + 0x7fff7fffu, m1 = (v.y & 0x7fff7fffu) + 0x7fff7fffu;
+    const uint32_t m2 = (v.z & 0x7fff7fffu) + 0x7fff7fffu, m3 = (v.w & 0x7fff7fffu) + 0x7fff7fffu;
+    const uint32_t f01 = __byte_perm(m0, m1, 0x7531u), f23 = __byte_perm(m2, m3, 0x7531u);
+    const uint32_t lo = (((f01 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
+    const uint32_t hi = (((f23 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
+    return (lo & 0xfu) | ((hi & 0xfu) << 4);
 }
 
 // Columns gene0 .. gene0 + 7 of a vector inside slot bc: the mask of those

@@ -54,19 +54,6 @@ __device__ __forceinline__ bool feature_kept(const uint8_t *feature_keep, uint32
     return feature_keep == nullptr || feature_keep[c] != 0u;
 }
 
-// Bit q set when fp16 value q of the 8 packed in v (low half first) is
-// nonzero (either sign of zero counts as zero).
-__device__ __forceinline__ uint32_t nonzero_bits(const uint4 &v) {
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    uint32_t b = 0u;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const uint32_t m = __vsetne2(w[i] & 0x7fff7fffu, 0u); // 1 in each nonzero half
-        b |= ((m & 1u) | ((m >> 15) & 2u)) << (2 * i);
-    }
-    return b;
-}
-
 // Adds one participating value whose column has group mask m.  Bits at or
 // above the call's group count land in accumulators that are never written
 // out, so they are ignored as the reference ignores them.
@@ -346,7 +333,7 @@ __device__ __forceinline__ void bell_row(const cs_blocked_ell_view &src, uint32_
                 const uint32_t e0 = base + u * 256u;
                 gene0[u] = bc[u] * B + bd.mod(e0);
                 if (bc[u] == CS_INVALID_COL) continue;
-                uint32_t nz = nonzero_bits(v[u]);
+                uint32_t nz = live_bits8(v[u]);
                 if (nz != 0u && gene0[u] + 8u > src.cols) {
                     const uint32_t lim = gene0[u] < src.cols ? src.cols - gene0[u] : 0u; // < 8 here
                     nz &= (1u << lim) - 1u;
@@ -1260,23 +1247,10 @@ __device__ __forceinline__ uint4 ld_policy_v4(const void *p, unsigned long long 
 }
 
 // Kept entries among the 8 values of one vector (no feature remap).
-// Bit q set when fp16 value q of the 8 in v is nonzero as a float (NaN
-// counts): (w & 0x7fff7fff) + 0x7fff7fff sets bit 15 (31) exactly when the low
-// (high) half has a nonzero magnitude, with no carry between the halves; the
-// eight flags are gathered by a byte permute and a multiply.
-__device__ __forceinline__ uint32_t live_bits8_add(const uint4 &v) {
-    const uint32_t m0 = (v.x & 0x7fff7fffu) + 0x7fff7fffu, m1 = (v.y & 0x7fff7fffu) + 0x7fff7fffu;
-    const uint32_t m2 = (v.z & 0x7fff7fffu) + 0x7fff7fffu, m3 = (v.w & 0x7fff7fffu) + 0x7fff7fffu;
-    const uint32_t f01 = __byte_perm(m0, m1, 0x7531u), f23 = __byte_perm(m2, m3, 0x7531u);
-    const uint32_t lo = (((f01 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
-    const uint32_t hi = (((f23 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
-    return (lo & 0xfu) | ((hi & 0xfu) << 4);
-}
-
 // lim = min(cols, output_cols): the columns that exist and have an output slot.
 __device__ __forceinline__ uint32_t onepass_keep(const uint4 &v, uint32_t bc, uint32_t gene0, uint32_t lim,
                                                  const uint32_t *kbits) {
-    uint32_t live = live_bits8_add(v) & in_range8(bc, gene0, lim);
+    uint32_t live = live_bits8(v) & in_range8(bc, gene0, lim);
     if (kbits != nullptr && live != 0u) live &= kbits[gene0 >> 5] >> (gene0 & 31u);
     return live;
 }
