@@ -614,11 +614,12 @@ CS_API int cs_b200_filter_blocked_ell_count(const cs_blocked_ell_view *parts,
 
 /* The same filter in ONE pass over the kept rows' values, for shards without
  * row or feature remaps whose block sizes are multiples of 8 (16-byte aligned
- * values) and output_rows >= the shard's rows: each row is counted, its output
- * offset found by a decoupled look-back over the rows before it, and its
- * entries written while its values are still in L2 (the count's loads mark
- * them evict_last), so the values cross HBM once instead of twice (count +
- * emit).  The output arrays hold
+ * values) and output_rows >= the shard's rows: each kept row is counted, its
+ * output offset found by a decoupled look-back over the rows before it, and
+ * its entries written while its values are still in L2 (the count's loads
+ * mark them evict_last; only the 8-value groups holding kept entries are read
+ * again), so the values cross HBM once instead of twice (count + emit).  Rows
+ * the row mask drops cost no pass over their values.  The output arrays hold
  * `capacity` entries (the stored nnz of the parts bounds the live entries); a
  * shard that needs more sets CS_STATUS_CAPACITY in *d_status and writes
  * nothing past them (run count + emit instead).  d_major_ptr, d_kept as for
