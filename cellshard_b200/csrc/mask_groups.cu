@@ -17,6 +17,7 @@
 #include "bell_vec.cuh"
 
 #include <cstring>
+#include <type_traits>
 
 namespace csb {
 namespace {
@@ -911,6 +912,8 @@ __global__ void __launch_bounds__(CFG::warps * 32, 1) group_reduce_bell16_pipe_k
             // block columns of slots [32w, 32w + 32) one per lane, the next window loaded ahead
             uint32_t my_bc = lane < W ? __ldg(bci + lane) : CS_INVALID_COL;
             uint32_t next_bc = 32u + lane < W ? __ldg(bci + 32u + lane) : CS_INVALID_COL;
+            // slots of the window whose block column lies inside the table (bit = slot)
+            uint32_t valid_bc = __ballot_sync(0xffffffffu, my_bc < col_blocks);
             for (uint32_t k = 0; k < nstages; ++k) {
                 issue(k + STAGES - 1u);
                 cp_async_wait<STAGES - 1>();
@@ -921,30 +924,41 @@ __global__ void __launch_bounds__(CFG::warps * 32, 1) group_reduce_bell16_pipe_k
                     my_bc = next_bc;
                     const uint32_t s = k * kPipeSlots + 32u + lane;
                     next_bc = s < W ? __ldg(bci + s) : CS_INVALID_COL;
+                    valid_bc = __ballot_sync(0xffffffffu, my_bc < col_blocks);
                 }
-#pragma unroll
-                for (unsigned j = 0; j < kPipeSlots; ++j) {
-                    const uint32_t bc =
-                        __shfl_sync(0xffffffffu, my_bc, ((k % kPipeStagesPerWindow) * kPipeSlots + j) & 31u);
-                    if (j >= nslots || bc >= col_blocks) continue; // warp-uniform (padding or outside)
+                const uint32_t wbase = (k % kPipeStagesPerWindow) * kPipeSlots;
+                // one slot: the values of the columns the table does not keep are
+                // zeroed once (the masked fragments give the totals, the detected
+                // counts and the maxima against a constant B; the group bits of a
+                // dropped column are zero in the table already)
+                auto slot = [&](unsigned j, auto check) {
+                    const uint32_t bc = __shfl_sync(0xffffffffu, my_bc, (wbase + j) & 31u);
+                    if constexpr (decltype(check)::value)
+                        if (bc >= col_blocks) return; // warp-uniform (padding or outside)
                     // this lane's 4 columns: two u16 entries per word (columns 4t, 4t+1 and 4t+2, 4t+3)
                     const uint2 te = *reinterpret_cast<const uint2 *>(table + bc * 16u + 4u * t);
                     const uint32_t km_lo = half_sign_mask(te.x), km_hi = half_sign_mask(te.y);
-                    const uint32_t bt_lo = km_lo & unit_n0, bt_hi = km_hi & unit_n0;
                     const uint2 lo = *reinterpret_cast<const uint2 *>(sb + g * RS + j * 32u);
                     const uint2 hi = *reinterpret_cast<const uint2 *>(sb + (g + 8u) * RS + j * 32u);
-                    const uint32_t a0 = lo.x, a1 = hi.x, a2 = lo.y, a3 = hi.y;
-                    mma_16816(dt, a0, a1, a2, a3, bt_lo, bt_hi);
+                    const uint32_t a0 = lo.x & km_lo, a1 = hi.x & km_lo, a2 = lo.y & km_hi, a3 = hi.y & km_hi;
+                    mma_16816(dt, a0, a1, a2, a3, unit_n0, unit_n0);
                     mma_16816(dd, nonzero_unit_pair(a0), nonzero_unit_pair(a1), nonzero_unit_pair(a2),
-                              nonzero_unit_pair(a3), bt_lo, bt_hi);
+                              nonzero_unit_pair(a3), unit_n0, unit_n0);
                     if constexpr (NT > 0u)
                         mma_16816(dg[0], a0, a1, a2, a3, ((te.x >> g) & 0x00010001u) * 0x3c00u,
                                   ((te.y >> g) & 0x00010001u) * 0x3c00u);
                     if constexpr (NT > 1u)
                         mma_16816(dg[NT - 1u], a0, a1, a2, a3, ((te.x >> (g + 8u)) & 0x00010001u) * 0x3c00u,
                                   ((te.y >> (g + 8u)) & 0x00010001u) * 0x3c00u);
-                    mx[0] = hmax2_bits(mx[0], hmax2_bits(a0 & km_lo, a2 & km_hi));
-                    mx[1] = hmax2_bits(mx[1], hmax2_bits(a1 & km_lo, a3 & km_hi));
+                    mx[0] = hmax2_bits(mx[0], hmax2_bits(a0, a2));
+                    mx[1] = hmax2_bits(mx[1], hmax2_bits(a1, a3));
+                };
+                constexpr uint32_t kStageSlotsMask = (1u << kPipeSlots) - 1u;
+                if (nslots == kPipeSlots && ((valid_bc >> wbase) & kStageSlotsMask) == kStageSlotsMask) {
+#pragma unroll
+                    for (unsigned j = 0; j < kPipeSlots; ++j) slot(j, std::false_type{});
+                } else {
+                    for (unsigned j = 0; j < nslots; ++j) slot(j, std::true_type{});
                 }
                 __syncwarp();
             }
