@@ -918,6 +918,14 @@ def convert_lines(args, lib, timed, emit, csr, spec, cpu_rows, ref_ok):
     if filt_cpu:
         ex["cpu_baseline"] = filt_cpu
     emit("filter_blocked_ell_to_compressed", ms_f, filt_bytes, ex)
+    ms_fm = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk, method="marked"))
+    ex = {"live_nnz": fstats["live_nnz"],
+          "note": "marked: one pass counts each kept row and marks its 8-value groups holding kept entries, a "
+                  "device scan places the rows, a second pass re-reads only the marked groups; then one host "
+                  "read of the live nnz; bytes as the one-pass line (the marks and the re-read groups not counted)"}
+    if filt_cpu:
+        ex["cpu_baseline"] = filt_cpu
+    emit("filter_blocked_ell_marked", ms_fm, filt_bytes, ex)
     ms_f2 = timed(lambda: runtime.filter_blocked_ell_to_compressed([bell], R, Cc, rk, fk, method="two_pass"))
     ex = {"live_nnz": fstats["live_nnz"], "note": "the count + emit route (remaps, other block sizes): both passes "
                                                   "read the kept rows' values"}

@@ -220,6 +220,9 @@ PROTOTYPES: dict[str, tuple] = {
     "cs_b200_filter_blocked_ell_onepass_scratch_bytes": (C.c_int, [P(BlockedEllView), u32, P(sz)]),
     "cs_b200_filter_blocked_ell_onepass": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
                                                      vp, u64, vp, vp, sz, vp, vp]),
+    "cs_b200_filter_blocked_ell_marked_scratch_bytes": (C.c_int, [P(BlockedEllView), u32, P(sz)]),
+    "cs_b200_filter_blocked_ell_marked": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
+                                                    vp, u64, vp, vp, sz, vp, vp]),
     "cs_b200_filter_blocked_ell_emit": (C.c_int, [P(BlockedEllView), u32, P(RowFeatureMaskView), u32, u32, vp, vp,
                                                    vp, vp]),
     "cs_b200_cspack_peek": (C.c_int, [C.c_char_p, P(CspackInfo)]),

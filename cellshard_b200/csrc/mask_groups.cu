@@ -1561,6 +1561,167 @@ __global__ void filter_onepass_tail_kernel(uint32_t rows, uint32_t output_rows, 
         major_ptr[r] = total;
 }
 
+// ---------------------------------------------------------------------------
+// Marked filter, two passes with no waits between CTAs.  Pass 1: one warp per
+// kept row counts its kept entries (eight 16-byte value loads per lane in
+// flight) and marks, one bit per 8-value vector, the vectors that hold any; a
+// device scan turns the counts (0 for dropped rows) into the row pointers.
+// Pass 2: one warp per kept row compacts the indices of its marked vectors
+// into shared memory (slot order), reads only those vectors again and writes
+// their entries, a warp scan ranking each round.  The values cross HBM once,
+// the marked vectors (those holding kept entries) a second time.
+// ---------------------------------------------------------------------------
+constexpr unsigned kMkWarps = 8;
+constexpr unsigned kMkSteps = 4;        // 256-value steps per lane per group; two groups in flight
+constexpr uint32_t kMkChunkWords = 64;  // mark words compacted per list fill (2,048 vectors)
+constexpr unsigned kMkRound = 4;        // marked vectors per lane in flight in pass 2
+
+__device__ __forceinline__ void fill_keep_bitmap(uint32_t *bits, uint32_t words, const reopt_parts &parts,
+                                                 const cs_row_feature_mask_view &masks) {
+    uint32_t kcols = 0u;
+    for (uint32_t k = 0; k < parts.count; ++k) kcols = max(kcols, parts.v[k].cols);
+    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+        uint32_t word = 0u;
+        const uint32_t c0 = w * 32u;
+#pragma unroll 4
+        for (uint32_t k = 0; k < 32u; ++k)
+            if (c0 + k < kcols) word |= (masks.feature_keep[c0 + k] != 0u ? 1u : 0u) << k;
+        bits[w] = word;
+    }
+}
+
+__global__ void __launch_bounds__(kMkWarps * 32) filter_mark_kernel(
+    const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
+    uint32_t *__restrict__ counts, uint32_t *__restrict__ marks, uint32_t mark_words,
+    unsigned long long *__restrict__ kept, uint32_t keep_words) {
+    extern __shared__ __align__(16) uint32_t mark_smem[];
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t rows = parts.row_off[parts.count];
+    const uint32_t *kbits = keep_words != 0u ? mark_smem : nullptr;
+    fill_keep_bitmap(mark_smem, keep_words, parts, masks);
+    __syncthreads();
+    uint32_t warp_kept_rows = 0u;
+    unsigned long long warp_kept_slots = 0u;
+    for (uint32_t row = blockIdx.x * kMkWarps + (threadIdx.x >> 5); row < rows; row += gridDim.x * kMkWarps) {
+        if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) {
+            if (lane == 0u) counts[row] = 0u;
+            continue;
+        }
+        const uint32_t part = part_of_row(parts, row);
+        const cs_blocked_ell_view &src = parts.v[part];
+        const uint32_t local = row - parts.row_off[part];
+        warp_kept_rows += 1u;
+        warp_kept_slots += src.ell_cols;
+        const uint32_t B = src.block_size, W = src.ell_cols / B;
+        const block_div bd(B);
+        const uint32_t *bci = src.blockColIdx + (std::size_t) (local / B) * W;
+        const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
+        uint32_t *mrow = marks + (std::size_t) row * mark_words;
+        const uint32_t lim = min(src.cols, output_cols);
+        uint32_t n = 0u;
+        uint4 v[kMkSteps], vn[kMkSteps];
+        uint32_t bc[kMkSteps], bcn[kMkSteps];
+        load_steps(vrow, bci, bd, src.ell_cols, lane * 8u, v, bc);
+        for (uint32_t s0 = 0u; s0 * 256u < src.ell_cols; s0 += kMkSteps) {
+            load_steps(vrow, bci, bd, src.ell_cols, (s0 + kMkSteps) * 256u + lane * 8u, vn, bcn);
+            uint32_t word = 0u; // lane u keeps step s0 + u's mark word
+#pragma unroll
+            for (unsigned u = 0; u < kMkSteps; ++u) {
+                const uint32_t e0 = (s0 + u) * 256u + lane * 8u;
+                const uint32_t keep =
+                    e0 < src.ell_cols ? onepass_keep(v[u], bc[u], bc[u] * B + bd.mod(e0), lim, kbits) : 0u;
+                n += __popc(keep);
+                const uint32_t m = __ballot_sync(0xffffffffu, keep != 0u);
+                if (lane == u) word = m;
+                v[u] = vn[u];
+                bc[u] = bcn[u];
+            }
+            if (lane < kMkSteps && s0 + lane < mark_words) mrow[s0 + lane] = word;
+        }
+        n = __reduce_add_sync(0xffffffffu, n);
+        if (lane == 0u) counts[row] = n;
+    }
+    if (kept != nullptr && lane == 0u && warp_kept_rows != 0u) {
+        atomicAdd(kept, (unsigned long long) warp_kept_rows);
+        atomicAdd(kept + 1, warp_kept_slots);
+    }
+}
+
+__global__ void __launch_bounds__(kMkWarps * 32) filter_marked_emit_kernel(
+    const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
+    const uint32_t *__restrict__ major_ptr, const uint32_t *__restrict__ marks, uint32_t mark_words,
+    uint32_t *__restrict__ minor_idx, uint16_t *__restrict__ out_val, unsigned long long capacity,
+    uint32_t *status, uint32_t keep_words) {
+    extern __shared__ __align__(16) uint32_t mark_smem[];
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t rows = parts.row_off[parts.count];
+    const uint32_t *kbits = keep_words != 0u ? mark_smem : nullptr;
+    // after the feature bitmap: each warp's list of marked vectors (offsets in
+    // the current chunk of kMkChunkWords mark words)
+    uint16_t *list = reinterpret_cast<uint16_t *>(mark_smem + ((keep_words + 3u) & ~3u)) +
+                     (threadIdx.x >> 5) * (kMkChunkWords * 32u);
+    fill_keep_bitmap(mark_smem, keep_words, parts, masks);
+    __syncthreads();
+    if (blockIdx.x == 0u && threadIdx.x == 0u && major_ptr[rows] > capacity) status_or(status, CS_STATUS_CAPACITY);
+    for (uint32_t row = blockIdx.x * kMkWarps + (threadIdx.x >> 5); row < rows; row += gridDim.x * kMkWarps) {
+        if (masks.row_keep != nullptr && masks.row_keep[row] == 0u) continue;
+        uint32_t run = major_ptr[row];
+        if (major_ptr[row + 1u] == run || run >= capacity) continue; // nothing kept, or nothing that fits
+        const uint32_t part = part_of_row(parts, row);
+        const cs_blocked_ell_view &src = parts.v[part];
+        const uint32_t local = row - parts.row_off[part];
+        const uint32_t B = src.block_size, W = src.ell_cols / B;
+        const block_div bd(B);
+        const uint32_t *bci = src.blockColIdx + (std::size_t) (local / B) * W;
+        const uint16_t *vrow = src.val + (std::size_t) local * src.ell_cols;
+        const uint32_t *mrow = marks + (std::size_t) row * mark_words;
+        const uint32_t lim = min(src.cols, output_cols);
+        const uint32_t nwords = (src.ell_cols + 255u) / 256u;
+        for (uint32_t w0 = 0u; w0 < nwords; w0 += kMkChunkWords) {
+            // two mark words per lane; their set bits, in order, fill the list
+            const uint32_t wa = w0 + 2u * lane;
+            const uint32_t m0 = wa < nwords ? mrow[wa] : 0u;
+            const uint32_t m1 = wa + 1u < nwords ? mrow[wa + 1u] : 0u;
+            const uint32_t c = __popc(m0) + __popc(m1);
+            const uint32_t incl = warp_inclusive_scan(c);
+            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+            uint32_t at = incl - c;
+            for (uint32_t bb = m0; bb != 0u; bb &= bb - 1u) list[at++] = (uint16_t) (64u * lane + __ffs(bb) - 1u);
+            for (uint32_t bb = m1; bb != 0u; bb &= bb - 1u) list[at++] = (uint16_t) (64u * lane + 31u + __ffs(bb));
+            __syncwarp();
+            for (uint32_t i0 = 0u; i0 < total; i0 += 32u * kMkRound) {
+                uint4 v[kMkRound];
+                uint32_t bc[kMkRound], e0[kMkRound];
+#pragma unroll
+                for (unsigned k = 0; k < kMkRound; ++k) {
+                    const uint32_t i = i0 + k * 32u + lane;
+                    const bool in = i < total;
+                    e0[k] = (w0 * 32u + (in ? (uint32_t) list[i] : 0u)) * 8u;
+                    v[k] = in ? ld_stream_v4(vrow + e0[k]) : make_uint4(0u, 0u, 0u, 0u);
+                    bc[k] = in ? __ldg(bci + bd.div(e0[k])) : CS_INVALID_COL;
+                }
+#pragma unroll
+                for (unsigned k = 0; k < kMkRound; ++k) {
+                    const uint32_t gene0 = bc[k] * B + bd.mod(e0[k]);
+                    const uint32_t keep = onepass_keep(v[k], bc[k], gene0, lim, kbits);
+                    const uint32_t cnt = __popc(keep);
+                    const uint32_t inc = warp_inclusive_scan(cnt);
+                    uint32_t pos = run + inc - cnt;
+                    for (uint32_t bb = keep; bb != 0u; bb &= bb - 1u, ++pos) {
+                        const uint32_t q = __ffs(bb) - 1u;
+                        if (pos < capacity) {
+                            minor_idx[pos] = gene0 + q;
+                            out_val[pos] = half_of(v[k], q);
+                        }
+                    }
+                    run += __shfl_sync(0xffffffffu, inc, 31);
+                }
+            }
+            __syncwarp(); // the list is refilled by the next chunk
+        }
+    }
+}
+
 // Group accumulator registers a call needs: none, 8, 16 or 32.
 unsigned group_regs(const uint32_t *masks, uint32_t group_count) {
     if (masks == nullptr || group_count == 0u) return 0u;
@@ -1775,6 +1936,38 @@ uint32_t keep_bitmap_words(const reopt_parts &parts, const cs_row_feature_mask_v
     return words <= 12288u ? words : 0u;
 }
 
+// The vector filters (one pass, marked): no remaps, output_rows >= the
+// shard's rows, block sizes multiples of 8 with 16-byte aligned values, and a
+// feature bitmap that fits in shared memory (*kw words).
+int vector_filter_qualifies(const reopt_parts &p, const cs_row_feature_mask_view &m, uint32_t output_rows,
+                            uint32_t *kw, const char *who) {
+    const uint32_t rows = p.row_off[p.count];
+    if (m.row_remap != nullptr || m.feature_remap != nullptr) {
+        set_error("%s: row or feature remaps need the count + emit path", who);
+        return 0;
+    }
+    if (output_rows < rows) {
+        set_error("%s: output_rows %u below the shard's %u rows", who, output_rows, rows);
+        return 0;
+    }
+    for (uint32_t k = 0; k < p.count; ++k) {
+        const cs_blocked_ell_view &v = p.v[k];
+        if (v.rows == 0u || v.ell_cols == 0u) continue;
+        if (v.block_size % 8u != 0u || (reinterpret_cast<uintptr_t>(v.val) & 15u) != 0u || v.val == nullptr ||
+            v.blockColIdx == nullptr) {
+            set_error("%s: partition %u needs a block size that is a multiple of 8 and 16-byte aligned values", who,
+                      k);
+            return 0;
+        }
+    }
+    *kw = keep_bitmap_words(p, m);
+    if (m.feature_keep != nullptr && *kw == 0u) {
+        set_error("%s: too many columns for the shared feature bitmap", who);
+        return 0;
+    }
+    return 1;
+}
+
 int reopt_count_launch(const reopt_parts &parts, const cs_row_feature_mask_view *masks, uint32_t output_rows,
                        uint32_t output_cols, uint32_t *d_major_ptr, uint64_t *d_kept, void *d_scratch,
                        std::size_t scratch_bytes, uint32_t *d_status, cudaStream_t stream, const char *who) {
@@ -1911,29 +2104,8 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
     if (!make_parts(parts, part_count, &p, who)) return 0;
     const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
     const uint32_t rows = p.row_off[p.count];
-    if (m.row_remap != nullptr || m.feature_remap != nullptr) {
-        set_error("%s: row or feature remaps need the count + emit path", who);
-        return 0;
-    }
-    if (output_rows < rows) {
-        set_error("%s: output_rows %u below the shard's %u rows", who, output_rows, rows);
-        return 0;
-    }
-    for (uint32_t k = 0; k < p.count; ++k) {
-        const cs_blocked_ell_view &v = p.v[k];
-        if (v.rows == 0u || v.ell_cols == 0u) continue;
-        if (v.block_size % 8u != 0u || (reinterpret_cast<uintptr_t>(v.val) & 15u) != 0u || v.val == nullptr ||
-            v.blockColIdx == nullptr) {
-            set_error("%s: partition %u needs a block size that is a multiple of 8 and 16-byte aligned values", who,
-                      k);
-            return 0;
-        }
-    }
-    const uint32_t kw = keep_bitmap_words(p, m);
-    if (m.feature_keep != nullptr && kw == 0u) {
-        set_error("%s: too many columns for the shared feature bitmap", who);
-        return 0;
-    }
+    uint32_t kw = 0u;
+    if (!vector_filter_qualifies(p, m, output_rows, &kw, who)) return 0;
     const std::size_t need = align_up(((std::size_t) rows + 1u) * 8u + 16u, 256);
     if (d_scratch == nullptr || scratch_bytes < need) {
         set_error("%s: scratch %zu < %zu", who, scratch_bytes, need);
@@ -1962,6 +2134,91 @@ extern "C" int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *par
                                                  counter, d_status, reinterpret_cast<unsigned long long *>(d_kept),
                                                  kw);
         if (!launch_ok("filter_onepass_kernel")) return 0;
+    }
+    const uint32_t tail = output_rows - rows + 1u;
+    filter_onepass_tail_kernel<<<(tail + 255u) / 256u > 1024u ? 1024u : (tail + 255u) / 256u, 256, 0, stream>>>(
+        rows, output_rows, d_major_ptr);
+    return launch_ok("filter_onepass_tail_kernel");
+}
+
+namespace {
+// Mark words per row: one per 256 values of the widest partition.
+uint32_t mark_words_of(const csb::reopt_parts &p) {
+    uint32_t w = 0u;
+    for (uint32_t k = 0; k < p.count; ++k) w = std::max(w, (p.v[k].ell_cols + 255u) / 256u);
+    return w;
+}
+std::size_t marked_scan_bytes(uint32_t rows) { return align_up(scan_u32_scratch_bytes(rows), 256); }
+} // namespace
+
+extern "C" int cs_b200_filter_blocked_ell_marked_scratch_bytes(const cs_blocked_ell_view *parts, uint32_t part_count,
+                                                               size_t *out_bytes) {
+    static const char *who = "filter_blocked_ell_marked_scratch_bytes";
+    if (out_bytes == nullptr) {
+        set_error("%s: null output", who);
+        return 0;
+    }
+    reopt_parts p;
+    if (!make_parts(parts, part_count, &p, who)) return 0;
+    const uint32_t rows = p.row_off[p.count];
+    *out_bytes = marked_scan_bytes(rows) + align_up((std::size_t) rows * mark_words_of(p) * 4u + 4u, 256);
+    return 1;
+}
+
+extern "C" int cs_b200_filter_blocked_ell_marked(const cs_blocked_ell_view *parts, uint32_t part_count,
+                                                 const cs_row_feature_mask_view *masks, uint32_t output_rows,
+                                                 uint32_t output_cols, uint32_t *d_major_ptr, uint32_t *d_minor_idx,
+                                                 uint16_t *d_val, uint64_t capacity, uint64_t *d_kept,
+                                                 void *d_scratch, size_t scratch_bytes, uint32_t *d_status,
+                                                 cs_stream_t s) {
+    static const char *who = "filter_blocked_ell_marked";
+    if (d_major_ptr == nullptr || (capacity != 0u && (d_minor_idx == nullptr || d_val == nullptr))) {
+        set_error("%s: null output array", who);
+        return 0;
+    }
+    reopt_parts p;
+    if (!make_parts(parts, part_count, &p, who)) return 0;
+    const cs_row_feature_mask_view m = masks != nullptr ? *masks : cs_row_feature_mask_view{};
+    const uint32_t rows = p.row_off[p.count];
+    uint32_t kw = 0u;
+    if (!vector_filter_qualifies(p, m, output_rows, &kw, who)) return 0;
+    const uint32_t mw = mark_words_of(p);
+    std::size_t need = 0;
+    if (!cs_b200_filter_blocked_ell_marked_scratch_bytes(parts, part_count, &need)) return 0;
+    if (d_scratch == nullptr || scratch_bytes < need) {
+        set_error("%s: scratch %zu < %zu", who, scratch_bytes, need);
+        return 0;
+    }
+    cudaStream_t stream = as_stream(s);
+    void *scan_tmp = d_scratch;
+    auto *marks = reinterpret_cast<uint32_t *>(static_cast<char *>(d_scratch) + marked_scan_bytes(rows));
+    if (d_kept != nullptr && !cuda_ok(cudaMemsetAsync(d_kept, 0, 16, stream), "memset kept")) return 0;
+    const std::size_t smem_mark = (std::size_t) kw * 4u;
+    const std::size_t smem_emit = (std::size_t) ((kw + 3u) & ~3u) * 4u + (std::size_t) kMkWarps * kMkChunkWords * 32u * 2u;
+    if (rows != 0u) {
+        unsigned grid = (rows + kMkWarps - 1u) / kMkWarps;
+        const unsigned cap = (unsigned) sm_count() * 16u;
+        if (grid > cap) grid = cap;
+        if (smem_mark > 48u * 1024u &&
+            !cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(filter_mark_kernel),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_mark),
+                     "mark shared memory"))
+            return 0;
+        filter_mark_kernel<<<grid, kMkWarps * 32, smem_mark, stream>>>(
+            p, m, output_cols, d_major_ptr, marks, mw, reinterpret_cast<unsigned long long *>(d_kept), kw);
+        if (!launch_ok("filter_mark_kernel")) return 0;
+        if (!scan_exclusive_u32(d_major_ptr, d_major_ptr, rows, true, scan_tmp, marked_scan_bytes(rows), stream))
+            return 0;
+        if (smem_emit > 48u * 1024u &&
+            !cuda_ok(cudaFuncSetAttribute(reinterpret_cast<const void *>(filter_marked_emit_kernel),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_emit),
+                     "marked emit shared memory"))
+            return 0;
+        filter_marked_emit_kernel<<<grid, kMkWarps * 32, smem_emit, stream>>>(
+            p, m, output_cols, d_major_ptr, marks, mw, d_minor_idx, d_val, capacity, d_status, kw);
+        if (!launch_ok("filter_marked_emit_kernel")) return 0;
+    } else if (!cuda_ok(cudaMemsetAsync(d_major_ptr, 0, 4, stream), "marked row pointer")) {
+        return 0;
     }
     const uint32_t tail = output_rows - rows + 1u;
     filter_onepass_tail_kernel<<<(tail + 255u) / 256u > 1024u ? 1024u : (tail + 255u) / 256u, 256, 0, stream>>>(

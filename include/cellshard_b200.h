@@ -644,6 +644,33 @@ CS_API int cs_b200_filter_blocked_ell_onepass(const cs_blocked_ell_view *parts,
                                               uint32_t *d_status,
                                               cs_stream_t stream);
 
+/* The same filter for the same shards as the one-pass entry, in two passes
+ * with no waits between CTAs: pass 1 reads every kept row's values once,
+ * counts its kept entries and marks (one bit per 8-value group, in scratch)
+ * the groups that hold any; a device scan turns the counts into d_major_ptr;
+ * pass 2 reads only the marked groups again and writes their entries in slot
+ * order.  Arguments, capacity, CS_STATUS_CAPACITY, d_major_ptr and d_kept as
+ * for cs_b200_filter_blocked_ell_onepass.  Scratch:
+ * cs_b200_filter_blocked_ell_marked_scratch_bytes (4 bytes per 256 slots of
+ * the widest partition per row, plus the scan's). */
+CS_API int cs_b200_filter_blocked_ell_marked_scratch_bytes(const cs_blocked_ell_view *parts,
+                                                           uint32_t part_count,
+                                                           size_t *out_bytes);
+CS_API int cs_b200_filter_blocked_ell_marked(const cs_blocked_ell_view *parts,
+                                             uint32_t part_count,
+                                             const cs_row_feature_mask_view *masks,
+                                             uint32_t output_rows,
+                                             uint32_t output_cols,
+                                             uint32_t *d_major_ptr,
+                                             uint32_t *d_minor_idx,
+                                             uint16_t *d_val,
+                                             uint64_t capacity,
+                                             uint64_t *d_kept,
+                                             void *d_scratch,
+                                             size_t scratch_bytes,
+                                             uint32_t *d_status,
+                                             cs_stream_t stream);
+
 CS_API int cs_b200_filter_blocked_ell_emit(const cs_blocked_ell_view *parts,
                                            uint32_t part_count,
                                            const cs_row_feature_mask_view *masks,

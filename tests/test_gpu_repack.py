@@ -144,14 +144,16 @@ def test_reference_filter_row_pointers_are_shifted(cuda, orc):
     assert live.value == int(shifted[-1])
 
 
+@pytest.mark.parametrize("method", ["onepass", "marked"])
 @pytest.mark.parametrize("part_specs,cols,out_rows", [
     ([(300, 16)], 257, 300),
     ([(130, 16), (77, 8), (2000, 16)], 3000, 2500),   # output rows past the shard's stay empty
     ([(64, 32), (1, 16), (9000, 8)], 500, 9065),
 ])
-def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows):
-    """The one-pass filter (rows counted, placed by a look-back, emitted from L2) gives the
-    count + emit CSR bit for bit, with the same kept-row statistics, and both equal the
+def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows, method):
+    """The vector filters -- one pass (rows counted, placed by a look-back, emitted from
+    L2) and marked (count + mark, scan, re-read of the marked groups) -- give the count +
+    emit CSR bit for bit, with the same kept-row statistics, and both equal the
     restatement's masked reoptimize without remaps."""
     from cellshard_b200 import runtime
 
@@ -163,7 +165,7 @@ def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows
     import torch
 
     rk, fk = torch.from_numpy(keep_rows).cuda(), torch.from_numpy(keep_cols).cuda()
-    a, sa = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="onepass")
+    a, sa = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method=method)
     b, sb = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="two_pass")
     assert sa == sb
     assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr))
@@ -176,15 +178,17 @@ def test_filter_onepass_matches_count_emit(cuda, orc, part_specs, cols, out_rows
     assert np.array_equal(np_u16(a.val), val)
 
 
-@pytest.mark.parametrize("cols", [9000, 40000])
+@pytest.mark.parametrize("method", ["onepass", "marked"])
+@pytest.mark.parametrize("cols", [9000, 40000, 70000])
 @pytest.mark.parametrize("drop", ["last_row", "last_partition", "first_rows", "all"])
-def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop, cols):
+def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop, cols, method):
     """Rows of 9,000 columns (two 8,192-slot steps of the one-pass kernel, the
     last ragged: the per-step counts of the whole row go through one scan) and of
-    40,000 columns (more steps than that: one scan per step), and a dropped final
+    40,000 columns (more steps than that: one scan per step), of 70,000 columns (the
+    marked route's emit compacts its mark words in five chunks), and a dropped final
     row or partition, the first rows, or every row dropped (dropped rows carry no
     entries but must still get their row pointers and the total): bit-exact vs
-    count + emit and the restatement."""
+    count + emit and the restatement, for both vector routes."""
     import torch
 
     from cellshard_b200 import runtime
@@ -206,7 +210,7 @@ def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop, cols):
     keep_cols = (rng.random(cols) < 0.6).astype(np.uint8)
     out_rows = shard_rows + 5
     rk, fk = torch.from_numpy(keep_rows).cuda(), torch.from_numpy(keep_cols).cuda()
-    a, sa = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="onepass")
+    a, sa = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method=method)
     b, sb = runtime.filter_blocked_ell_to_compressed(parts, out_rows, cols, rk, fk, method="two_pass")
     assert sa == sb
     assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr))
@@ -218,10 +222,11 @@ def test_filter_onepass_long_rows_and_dropped_tail(cuda, orc, drop, cols):
     assert np.array_equal(np_u16(a.val), val)
 
 
-def test_filter_onepass_capacity_falls_back(cuda):
-    """A view whose stored nnz under-counts its nonzeros gives the one-pass filter too
-    little room: it flags CS_STATUS_CAPACITY (forced one pass raises) and the default
-    route reruns count + emit with the same result as always."""
+@pytest.mark.parametrize("method", ["onepass", "marked"])
+def test_filter_onepass_capacity_falls_back(cuda, method):
+    """A view whose stored nnz under-counts its nonzeros gives the vector filters too
+    little room: they flag CS_STATUS_CAPACITY (a forced vector route raises) and the
+    default route reruns count + emit with the same result as always."""
     import torch
 
     from cellshard_b200 import _abi, runtime
@@ -232,7 +237,7 @@ def test_filter_onepass_capacity_falls_back(cuda):
     short = BlockedELL(p.rows, p.cols, p.block_size, p.ell_cols, p.bci, p.val, nnz=p.nnz // 3)
     rk = torch.ones(p.rows, dtype=torch.uint8, device="cuda")
     with pytest.raises(_abi.CellShardError):
-        runtime.filter_blocked_ell_to_compressed([short], p.rows, p.cols, rk, None, method="onepass")
+        runtime.filter_blocked_ell_to_compressed([short], p.rows, p.cols, rk, None, method=method)
     a, _ = runtime.filter_blocked_ell_to_compressed([short], p.rows, p.cols, rk, None)
     b, _ = runtime.filter_blocked_ell_to_compressed([p], p.rows, p.cols, rk, None, method="two_pass")
     assert np.array_equal(np_u32(a.ptr), np_u32(b.ptr)) and np.array_equal(np_u32(a.idx), np_u32(b.idx))
