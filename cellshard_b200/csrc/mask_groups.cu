@@ -1647,6 +1647,16 @@ __global__ void __launch_bounds__(kMkWarps * 32) filter_mark_kernel(
     }
 }
 
+// 16-byte load of a scattered vector: no L1 line and no L2 prefetch beyond
+// its own sector (the streaming loads ask for 256-byte L2 fills).
+__device__ __forceinline__ uint4 ld_gather_v4(const void *p) {
+    uint4 r;
+    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p));
+    return r;
+}
+
 __global__ void __launch_bounds__(kMkWarps * 32) filter_marked_emit_kernel(
     const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
     const uint32_t *__restrict__ major_ptr, const uint32_t *__restrict__ marks, uint32_t mark_words,
@@ -1697,7 +1707,7 @@ __global__ void __launch_bounds__(kMkWarps * 32) filter_marked_emit_kernel(
                     const uint32_t i = i0 + k * 32u + lane;
                     const bool in = i < total;
                     e0[k] = (w0 * 32u + (in ? (uint32_t) list[i] : 0u)) * 8u;
-                    v[k] = in ? ld_stream_v4(vrow + e0[k]) : make_uint4(0u, 0u, 0u, 0u);
+                    v[k] = in ? ld_gather_v4(vrow + e0[k]) : make_uint4(0u, 0u, 0u, 0u);
                     bc[k] = in ? __ldg(bci + bd.div(e0[k])) : CS_INVALID_COL;
                 }
 #pragma unroll
