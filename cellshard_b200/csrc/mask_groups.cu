@@ -1575,6 +1575,7 @@ constexpr unsigned kMkWarps = 8;
 constexpr unsigned kMkSteps = 4;        // 256-value steps per lane per group; two groups in flight
 constexpr uint32_t kMkChunkWords = 64;  // mark words compacted per list fill (2,048 vectors)
 constexpr unsigned kMkRound = 4;        // marked vectors per lane in flight in pass 2
+constexpr unsigned kMkCtasPerSm = 4;    // pass 1 at <= 64 registers: four CTAs per SM
 
 __device__ __forceinline__ void fill_keep_bitmap(uint32_t *bits, uint32_t words, const reopt_parts &parts,
                                                  const cs_row_feature_mask_view &masks) {
@@ -1590,7 +1591,7 @@ __device__ __forceinline__ void fill_keep_bitmap(uint32_t *bits, uint32_t words,
     }
 }
 
-__global__ void __launch_bounds__(kMkWarps * 32) filter_mark_kernel(
+__global__ void __launch_bounds__(kMkWarps * 32, kMkCtasPerSm) filter_mark_kernel(
     const __grid_constant__ reopt_parts parts, cs_row_feature_mask_view masks, uint32_t output_cols,
     uint32_t *__restrict__ counts, uint32_t *__restrict__ marks, uint32_t mark_words,
     unsigned long long *__restrict__ kept, uint32_t keep_words) {
