@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_csr_kernel(cs_compre
 // (CSR on 500,000 x 32,768: 0.86 ms against 1.18 ms).
 constexpr unsigned kCodesWarps = 32; // warps of a code-table CTA (they share one table)
 
-template <unsigned GR, unsigned U = 2>
+template <unsigned GR, unsigned U = 4>
 __global__ void __launch_bounds__(kCodesWarps * 32) group_reduce_csr_codes_kernel(cs_compressed_view src,
                                                                               const uint32_t *__restrict__ group_masks,
                                                                               uint32_t group_count,
@@ -1628,9 +1628,9 @@ __global__ void __launch_bounds__(kMkWarps * 32, kMkCtasPerSm) filter_mark_kerne
             uint32_t word = 0u; // lane u keeps step s0 + u's mark word
 #pragma unroll
             for (unsigned u = 0; u < kMkSteps; ++u) {
+                // a vector past the row is zeros in an invalid slot: no kept entries
                 const uint32_t e0 = (s0 + u) * 256u + lane * 8u;
-                const uint32_t keep =
-                    e0 < src.ell_cols ? onepass_keep(v[u], bc[u], bc[u] * B + bd.mod(e0), lim, kbits) : 0u;
+                const uint32_t keep = onepass_keep(v[u], bc[u], bc[u] * B + bd.mod(e0), lim, kbits);
                 n += __popc(keep);
                 const uint32_t m = __ballot_sync(0xffffffffu, keep != 0u);
                 if (lane == u) word = m;
