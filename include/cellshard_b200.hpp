@@ -1584,6 +1584,37 @@ inline int filter_parts(const cs_blocked_ell_view *views, std::uint32_t part_cou
     cs_row_feature_mask_view m{d_keep_rows, d_keep_cols, d_row_remap, d_col_remap};
     const cs_stream_t s = reinterpret_cast<cs_stream_t>(ws->stream);
     if (cudaMemsetAsync(ws->d_status, 0, 4, ws->stream) != cudaSuccess) return 0;
+    // without remaps, block sizes multiples of 8 and 16-byte aligned values: the
+    // marked route (one full read of the kept values, a re-read of the 8-value
+    // groups holding kept entries); count + emit otherwise, or when max_nnz is short
+    bool vec = d_row_remap == nullptr && d_col_remap == nullptr && output_rows >= rows;
+    for (std::uint32_t k = 0; vec && k < part_count; ++k)
+        vec = views[k].rows == 0u ||
+              (views[k].block_size % 8u == 0u && (reinterpret_cast<std::uintptr_t>(views[k].val) & 15u) == 0u);
+    std::size_t need = 0;
+    if (vec && cs_b200_filter_blocked_ell_marked_scratch_bytes(views, part_count, &need) && need > 0u) {
+        if (need > ws->d_scan_tmp_bytes) {
+            cudaFree(ws->d_scan_tmp);
+            ws->d_scan_tmp = nullptr;
+            ws->d_scan_tmp_bytes = 0u;
+            if (cudaMalloc(&ws->d_scan_tmp, need) != cudaSuccess) return 0;
+            ws->d_scan_tmp_bytes = need;
+        }
+        std::uint32_t status = 0u;
+        if (!cs_b200_filter_blocked_ell_marked(views, part_count, &m, output_rows, output_cols,
+                                               ws->d_filtered_major_ptr, ws->d_filtered_minor_idx,
+                                               reinterpret_cast<std::uint16_t *>(ws->d_filtered_val), max_nnz,
+                                               reinterpret_cast<std::uint64_t *>(ws->d_kept), ws->d_scan_tmp,
+                                               ws->d_scan_tmp_bytes, ws->d_status, s) ||
+            cudaMemcpyAsync(live_nnz, ws->d_filtered_major_ptr + output_rows, 4, cudaMemcpyDeviceToHost,
+                            ws->stream) != cudaSuccess ||
+            cudaMemcpyAsync(kept, ws->d_kept, 16, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+            cudaMemcpyAsync(&status, ws->d_status, 4, cudaMemcpyDeviceToHost, ws->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ws->stream) != cudaSuccess)
+            return 0;
+        if (status == 0u) return 1;
+        if (status != CS_STATUS_CAPACITY || cudaMemsetAsync(ws->d_status, 0, 4, ws->stream) != cudaSuccess) return 0;
+    }
     if (!cs_b200_filter_blocked_ell_count(views, part_count, &m, output_rows, output_cols, ws->d_filtered_major_ptr,
                                           reinterpret_cast<std::uint64_t *>(ws->d_kept), ws->d_scan_tmp,
                                           ws->d_scan_tmp_bytes, ws->d_status, s))
