@@ -21,10 +21,13 @@ __device__ __forceinline__ uint32_t live_bits8(const uint4 &v) {
 }
 
 // Columns gene0 .. gene0 + 7 of a vector inside slot bc: the mask of those
-// that exist (valid block column, column < cols).
+// that exist (valid block column, column < cols).  gene0 = bc * B + offset:
+// for a padding slot (bc = CS_INVALID_COL) it wraps to 2^32 - B + offset,
+// past any column count, so one clamp covers both tests.
 __device__ __forceinline__ uint32_t in_range8(uint32_t bc, uint32_t gene0, uint32_t cols) {
-    if (bc == CS_INVALID_COL || gene0 >= cols) return 0u;
-    return gene0 + 8u <= cols ? 0xffu : (1u << (cols - gene0)) - 1u;
+    (void) bc;
+    const uint32_t d = min(max(cols, gene0) - gene0, 8u);
+    return (1u << d) - 1u;
 }
 
 // e / B and e % B for a block size B: a shift and a mask when B is a power
