@@ -15,9 +15,11 @@ __device__ __forceinline__ uint32_t live_bits8(const uint4 &v) {
     const uint32_t m0 = (v.x & 0x7fff7fffu) + 0x7fff7fffu, m1 = (v.y & 0x7fff7fffu) + 0x7fff7fffu;
     const uint32_t m2 = (v.z & 0x7fff7fffu) + 0x7fff7fffu, m3 = (v.w & 0x7fff7fffu) + 0x7fff7fffu;
     const uint32_t f01 = __byte_perm(m0, m1, 0x7531u), f23 = __byte_perm(m2, m3, 0x7531u);
-    const uint32_t lo = (((f01 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
-    const uint32_t hi = (((f23 >> 7) & 0x01010101u) * 0x01020408u) >> 24;
-    return (lo & 0xfu) | ((hi & 0xfu) << 4);
+    // the flags of values 0-3 at bit 8k + 3, of values 4-7 at bit 8k + 7; shifted
+    // down by 3, one multiply gathers bit 8k into bit 24 + k and bit 8k + 4 into
+    // bit 28 + k (no two partial products meet)
+    const uint32_t g = (f23 & 0x80808080u) | ((f01 >> 4) & 0x08080808u);
+    return ((g >> 3) * 0x01020408u) >> 24;
 }
 
 // Columns gene0 .. gene0 + 7 of a vector inside slot bc: the mask of those
