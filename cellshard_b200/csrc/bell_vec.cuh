@@ -7,19 +7,25 @@
 
 namespace csb {
 
+// 1.0 in each half of w that is nonzero as a float or NaN (either sign of
+// zero gives 0.0): one packed-half compare.
+__device__ __forceinline__ uint32_t nonzero_halves(uint32_t w) {
+    uint32_t d;
+    asm("set.neu.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(w), "r"(0u));
+    return d;
+}
+
 // Bit q set when fp16 value q of the 8 in v is nonzero as a float (NaN
-// counts): (w & 0x7fff7fff) + 0x7fff7fff sets bit 15 (31) exactly when the low
-// (high) half has a nonzero magnitude, with no carry between the halves; the
-// eight flags are gathered by a byte permute and a multiply.
+// counts).  Each half becomes 1.0 (0x3c00) or 0 by a packed compare; a byte
+// permute keeps the high byte of every half (bit 5 set for a nonzero value),
+// the flags of values 0-3 land at bit 8k + 1 and those of values 4-7 at bit
+// 8k + 5, and after a shift one multiply gathers bit 8k into bit 24 + k and
+// bit 8k + 4 into bit 28 + k (no two partial products meet).
 __device__ __forceinline__ uint32_t live_bits8(const uint4 &v) {
-    const uint32_t m0 = (v.x & 0x7fff7fffu) + 0x7fff7fffu, m1 = (v.y & 0x7fff7fffu) + 0x7fff7fffu;
-    const uint32_t m2 = (v.z & 0x7fff7fffu) + 0x7fff7fffu, m3 = (v.w & 0x7fff7fffu) + 0x7fff7fffu;
-    const uint32_t f01 = __byte_perm(m0, m1, 0x7531u), f23 = __byte_perm(m2, m3, 0x7531u);
-    // the flags of values 0-3 at bit 8k + 3, of values 4-7 at bit 8k + 7; shifted
-    // down by 3, one multiply gathers bit 8k into bit 24 + k and bit 8k + 4 into
-    // bit 28 + k (no two partial products meet)
-    const uint32_t g = (f23 & 0x80808080u) | ((f01 >> 4) & 0x08080808u);
-    return ((g >> 3) * 0x01020408u) >> 24;
+    const uint32_t f01 = __byte_perm(nonzero_halves(v.x), nonzero_halves(v.y), 0x7531u);
+    const uint32_t f23 = __byte_perm(nonzero_halves(v.z), nonzero_halves(v.w), 0x7531u);
+    const uint32_t g = (f23 & 0x20202020u) | ((f01 >> 4) & 0x02020202u);
+    return ((g >> 1) * 0x01020408u) >> 24;
 }
 
 // Columns gene0 .. gene0 + 7 of a vector inside slot bc: the mask of those

@@ -633,13 +633,6 @@ __device__ __forceinline__ uint32_t half_sign_mask(uint32_t x) {
     return d;
 }
 
-// 1.0 in each half that is nonzero or NaN (either sign of zero gives 0.0).
-__device__ __forceinline__ uint32_t nonzero_unit_pair(uint32_t x) {
-    uint32_t d;
-    asm("set.neu.f16x2.f16x2 %0, %1, %2;" : "=r"(d) : "r"(x), "r"(0u));
-    return d;
-}
-
 // (without groups, G is the constant 0 and its comparisons fold away)
 #pragma nv_diag_suppress 186
 // NT: tiles of 8 groups (0 without groups); GR: accumulators of the per-row
@@ -723,8 +716,8 @@ __global__ void __launch_bounds__(kRowThreads) group_reduce_bell16_mma_kernel(
                         const uint32_t km_lo = kb_lo * 0xffffu, km_hi = kb_hi * 0xffffu;
                         const uint32_t a0 = x[u][0].x, a1 = x[u][1].x, a2 = x[u][0].y, a3 = x[u][1].y;
                         mma_16816(dt, a0, a1, a2, a3, kb_lo * unit_n0, kb_hi * unit_n0);
-                        mma_16816(dd, nonzero_unit_pair(a0), nonzero_unit_pair(a1), nonzero_unit_pair(a2),
-                                  nonzero_unit_pair(a3), kb_lo * unit_n0, kb_hi * unit_n0);
+                        mma_16816(dd, nonzero_halves(a0), nonzero_halves(a1), nonzero_halves(a2),
+                                  nonzero_halves(a3), kb_lo * unit_n0, kb_hi * unit_n0);
 #pragma unroll
                         for (unsigned nt = 0; nt < NT; ++nt) {
                             // group 8nt + g of columns (4t, 4t+1) and (4t+2, 4t+3), as bits 0 and 16
@@ -942,8 +935,8 @@ __global__ void __launch_bounds__(CFG::warps * 32, 1) group_reduce_bell16_pipe_k
                     const uint2 hi = *reinterpret_cast<const uint2 *>(sb + (g + 8u) * RS + j * 32u);
                     const uint32_t a0 = lo.x & km_lo, a1 = hi.x & km_lo, a2 = lo.y & km_hi, a3 = hi.y & km_hi;
                     mma_16816(dt, a0, a1, a2, a3, unit_n0, unit_n0);
-                    mma_16816(dd, nonzero_unit_pair(a0), nonzero_unit_pair(a1), nonzero_unit_pair(a2),
-                              nonzero_unit_pair(a3), unit_n0, unit_n0);
+                    mma_16816(dd, nonzero_halves(a0), nonzero_halves(a1), nonzero_halves(a2),
+                              nonzero_halves(a3), unit_n0, unit_n0);
                     if constexpr (NT > 0u)
                         mma_16816(dg[0], a0, a1, a2, a3, ((te.x >> g) & 0x00010001u) * 0x3c00u,
                                   ((te.y >> g) & 0x00010001u) * 0x3c00u);
