@@ -863,6 +863,9 @@ __global__ void __launch_bounds__(CFG::warps * 32, 1) group_reduce_bell16_pipe_k
     const uint32_t nstages = (W + kPipeSlots - 1u) / kPipeSlots;
     const uint32_t row_blocks = (src.rows + 15u) >> 4;
     const uint32_t unit_n0 = g == 0u ? 0x3c003c00u : 0u; // 1.0 pairs in B column 0 only
+    // group g's bit of two table entries times 0x3c00 >> g is 1.0 (0x3c00) per
+    // member half: 0x3c00 = 15 << 10, so the shift is exact for g < 8
+    const uint32_t gsel = 0x00010001u << g, gmul = 0x3c00u >> g;
     for (uint32_t rb = blockIdx.x * kPipeWarps + warp; rb < row_blocks; rb += gridDim.x * kPipeWarps) {
         // rows of the block the row mask keeps (bit r = block row r)
         const uint32_t r16 = rb * 16u + (lane & 15u);
@@ -938,8 +941,7 @@ __global__ void __launch_bounds__(CFG::warps * 32, 1) group_reduce_bell16_pipe_k
                     mma_16816(dd, nonzero_halves(a0), nonzero_halves(a1), nonzero_halves(a2),
                               nonzero_halves(a3), unit_n0, unit_n0);
                     if constexpr (NT > 0u)
-                        mma_16816(dg[0], a0, a1, a2, a3, ((te.x >> g) & 0x00010001u) * 0x3c00u,
-                                  ((te.y >> g) & 0x00010001u) * 0x3c00u);
+                        mma_16816(dg[0], a0, a1, a2, a3, (te.x & gsel) * gmul, (te.y & gsel) * gmul);
                     if constexpr (NT > 1u)
                         mma_16816(dg[NT - 1u], a0, a1, a2, a3, ((te.x >> (g + 8u)) & 0x00010001u) * 0x3c00u,
                                   ((te.y >> (g + 8u)) & 0x00010001u) * 0x3c00u);
